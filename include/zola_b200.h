@@ -1,0 +1,135 @@
+/*
+ * zola_b200.h — C-ABI of the B200-native ZOLA-3D localization library.
+ *
+ * This is the whole boundary: plain pointers and sizes, no C++ or torch types.
+ * It replaces the JCuda object API that ZOLA-3D's Java classes drive (paths are
+ * relative to the reference's src/main/java/org/pasteur/imagej/):
+ *
+ *   MyCudaStream.init / destroy                 cuda/MyCudaStream.java:36-132
+ *   DataPhase_ (+ PSFmany_float_ construction)  process/gpu/DataPhase_.java,
+ *                                               process/gpu/PSFmany_float_.java:186-500
+ *   PSFmany_float_.computePSF                   process/gpu/PSFmany_float_.java:1626-1720
+ *   Modelmany_double_.getLikelihood / Fisher    process/gpu/Modelmany_double_.java:545-791,865-940
+ *   Localization_.localize (per-ROI MLE)        process/gpu/Localization_.java:633-798
+ *
+ * Conventions (all functions):
+ *   - return 0 on success, a negative ZOLA_E* code on failure; zola_last_error()
+ *     gives a message.  The reference logged and continued (IJ.log); here every
+ *     failure is reported to the caller.
+ *   - x, y, z, pixel size and wavelength are in micrometres; Zernike
+ *     coefficients are in radians, un-normalised, in the reference's index order
+ *     (n = 0,1,2,..., m = -n,-n+2,...,n; utils/Zernike.java:26-60).
+ *   - images and ROIs are stored [x][y] (first index x), as the reference's
+ *     double[][] arrays (process/cpu/LocalizationPipeline.java:588-606).
+ *   - "host" entry points take host buffers and copy in and out inside the call;
+ *     "_dev" entry points take device pointers and a cudaStream_t (as void*).
+ *   - a context is not thread-safe; use one per host thread (the reference's
+ *     "part"/stream), exactly as the reference used one DataPhase_ per stream.
+ */
+#ifndef ZOLA_B200_H
+#define ZOLA_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define ZOLA_API __attribute__((visibility("default")))
+#else
+#define ZOLA_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ZOLA_OK 0
+#define ZOLA_E_ARG -1       /* invalid argument (size, null pointer, range) */
+#define ZOLA_E_CUDA -2      /* CUDA runtime error */
+#define ZOLA_E_NODEV -3     /* no usable sm_100 device */
+#define ZOLA_E_UNSUPPORTED -4
+#define ZOLA_E_TIMEOUT -5   /* a bounded device wait ran out (kernel status word) */
+
+typedef struct zola_ctx zola_ctx;
+typedef struct zola_psf zola_psf;
+
+/* Optical parameters of one calibration (the calibration JSON keys of
+ * process/cpu/DataPhase.java:587-679 plus the localization command's n_wat). */
+typedef struct {
+    int size_fft;        /* "sizeFFT": pupil grid; made even and rounded up to a
+                            power of two as the CPU path does (PhaseParameters.java:296) */
+    double xystep;       /* "sizePix", um */
+    double na;           /* "NA" */
+    double wavelength;   /* "wavelength", um */
+    double n_oil;        /* "index" (immersion) */
+    double n_wat;        /* sample index (DataPhase.setNwat) */
+    double sigma;        /* "sigmaGaussianKernel", px */
+    int with_apo;        /* "withApoFactor" */
+    double zfocus;       /* Zfocus: the zoil the localization model uses, um */
+    int kz_reset;        /* 1: evanescent kz = 2 pi sqrt|.| as PSFPhase.resetKz
+                            (detection library); 0: kz = 0 (fit model, PSFPhaseMany) */
+} zola_optics;
+
+/* Levenberg-Marquardt fit controls. */
+typedef struct {
+    double zmin, zmax;   /* z box, um (reference: minZ-0.3, maxZ+0.3) */
+    double xymax;        /* |x|,|y| box, um */
+    int max_iter;        /* model evaluations per ROI (config: 30) */
+    double tol_xyz;      /* convergence: accepted step below this, um */
+    double step_xy;      /* per-iteration step caps, um */
+    double step_z;
+    int precision;       /* ZOLA_PREC_* */
+} zola_fit_params;
+
+#define ZOLA_PREC_FP64 0     /* plain FP64 GPU form (CUDA cores, one CTA per ROI) */
+#define ZOLA_PREC_SPLIT 1    /* split-precision tcgen05 partial DFT, FP32 sums, FP64 solve */
+
+/* Per-ROI status codes written by the fits. */
+#define ZOLA_FIT_CONVERGED 1
+#define ZOLA_FIT_MAXITER 2
+#define ZOLA_FIT_STALLED 3
+#define ZOLA_FIT_NAN -1
+
+/* --- context (replaces MyCudaStream.init / destroy, cuda/MyCudaStream.java:36-132) */
+ZOLA_API int zola_ctx_create(int device, zola_ctx** out);
+ZOLA_API int zola_ctx_destroy(zola_ctx* ctx);
+ZOLA_API const char* zola_last_error(const zola_ctx* ctx);
+/* Stream the context launches on (cudaStream_t as void*). */
+ZOLA_API void* zola_ctx_stream(zola_ctx* ctx);
+
+/* --- PSF (replaces DataPhase_ + PSFmany_float_ construction; the Java side
+ * parses the unchanged calibration JSON and passes its fields here).
+ * zernike: nz coefficients in radians (DataPhase.java:641-660). */
+ZOLA_API int zola_psf_load(zola_ctx* ctx, const zola_optics* optics, const double* zernike, int nz,
+                  zola_psf** out);
+ZOLA_API int zola_psf_free(zola_psf* psf);
+/* Grid facts: rounded pupil grid N and disk pixel count K. */
+ZOLA_API int zola_psf_info(const zola_psf* psf, int* N, int* K);
+
+/* --- PSF model (replaces PSFmany_float_.computePSF, PSFmany_float_.java:1626-1720,
+ * and PSFPhase.computePSF, process/cpu/PSFPhase.java:557-629).
+ * xyz: n triples (x, y, zwat) um, zoil = optics.zfocus.  out_psf: n*R*R FP64,
+ * normalised to sum 1.  out_dpsf (nullable): n*3*R*R, d psi / d{x,y,z}.
+ * FP64 on the device. */
+ZOLA_API int zola_psf_model(zola_psf* psf, int R, const double* xyz, int n, double* out_psf, double* out_dpsf);
+ZOLA_API int zola_psf_model_dev(zola_psf* psf, int R, const double* d_xyz, int n, double* d_out_psf,
+                       double* d_out_dpsf, void* stream);
+
+/* --- batched Poisson MLE fit (replaces Localization_.localize with its
+ * Modelmany_double_ likelihood batches, process/gpu/Localization_.java:633-798).
+ * rois: n*R*R photon counts [x][y]; init5/out5: n*(x, y, z, A, B);
+ * crlb5 (nullable): sqrt(diag(F^-1)) at the optimum, n*5; nll: n (deviance
+ * form sum mu - d - d ln(mu/d)); status/iters: n (model evaluations). */
+ZOLA_API int zola_fit_batch(zola_ctx* ctx, zola_psf* psf, int R, const float* rois, const double* init5, int n,
+                   const zola_fit_params* prm, double* out5, double* crlb5, double* nll, int* status,
+                   int* iters);
+ZOLA_API int zola_fit_batch_dev(zola_ctx* ctx, zola_psf* psf, int R, const float* d_rois, const double* d_init5,
+                       int n, const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll,
+                       int* d_status, int* d_iters, void* stream);
+
+/* Number of kernel launches the library issued since the context was created
+ * (bench bookkeeping). */
+ZOLA_API long long zola_ctx_launches(const zola_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ZOLA_B200_H */

@@ -1,0 +1,183 @@
+"""ORACLE — test infrastructure only (never imported by the product path).
+
+ctypes wrapper over ``zola_oracle.cpp``, the FP64 CPU restatement of ZOLA-3D's
+localization hot path (see the header of that file for the reference file:line
+each function follows).  Only ``tests/``, ``__graft_entry__.smoke()`` and
+``bench.py``'s CPU-baseline leg may import this module.
+
+PARITY UNPINNED: the reference has no tests or golden vectors for this path and
+cannot run here (Java plugin, no JVM); the oracle is pinned by known-answer
+tests only.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_SO = os.path.join(_HERE, "liboracle.so")
+_SRC = os.path.join(_HERE, "zola_oracle.cpp")
+
+
+def build(force=False):
+    """Compile the oracle with g++ (the recipe lives here and in Makefile)."""
+    if force or not os.path.exists(_SO) or os.path.getmtime(_SO) < os.path.getmtime(_SRC):
+        subprocess.check_call(["g++", "-O3", "-std=c++17", "-fPIC", "-shared", "-o", _SO, _SRC, "-lpthread"])
+    return _SO
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(_SO)
+        d, i, vp = ctypes.c_double, ctypes.c_int, ctypes.c_void_p
+        P = ctypes.POINTER
+        L.orc_psf_create.restype = vp
+        L.orc_psf_create.argtypes = [i, d, d, d, d, d, d, i, d, i, i, i, vp]
+        L.orc_psf_destroy.argtypes = [vp]
+        L.orc_psf_info.argtypes = [vp, vp, vp]
+        L.orc_psf_tables.argtypes = [vp] + [vp] * 6
+        L.orc_window_size.argtypes = [i, i]
+        L.orc_psf_model.argtypes = [vp, i, i, vp, vp, vp]
+        L.orc_psf_model_oil.argtypes = [vp, i, d, d, d, d, vp]
+        L.orc_localize_cd.argtypes = [vp, i, i, vp, vp, d, d, i, d, vp, vp, vp, vp, i]
+        L.orc_fit_lm.argtypes = [vp, i, i, vp, vp, vp, i, vp, vp, vp, vp, vp, i]
+        L.orc_nll_grad.restype = d
+        L.orc_nll_grad.argtypes = [vp, i, vp, vp, vp, vp]
+        L.orc_crlb_fd.argtypes = [vp, i, vp, vp]
+        L.orc_det_create.restype = vp
+        L.orc_det_create.argtypes = [vp, i, i, i, d, d, d, d]
+        L.orc_det_destroy.argtypes = [vp]
+        L.orc_det_nslices.argtypes = [vp]
+        L.orc_det_library.argtypes = [vp, vp, vp]
+        L.orc_detect.argtypes = [vp, i, vp, i, vp, vp, i]
+        L.orc_calib_nll.restype = d
+        L.orc_calib_nll.argtypes = [vp, i, i, vp, vp, d, d, d, d, d]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class OraclePSF:
+    """PSFPhase + ZernikePhase (process/cpu/PSFPhase.java, ZernikePhase.java)."""
+
+    def __init__(self, N, dx, na, wavelength, n_oil, n_wat, sigma, zernike, apo=False,
+                 zfocus=0.0, kz_reset=False, gauss_f32=True):
+        self.zernike = _f64(zernike)
+        self.h = lib().orc_psf_create(int(N), dx, na, wavelength, n_oil, n_wat, sigma, int(apo), zfocus,
+                                      int(kz_reset), int(gauss_f32), len(self.zernike), _p(self.zernike))
+        n = ctypes.c_int()
+        k = ctypes.c_int()
+        lib().orc_psf_info(self.h, ctypes.byref(n), ctypes.byref(k))
+        self.N, self.K = n.value, k.value
+        self.dx = dx
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.orc_psf_destroy(self.h)
+            self.h = None
+
+    def tables(self):
+        out = [np.zeros(self.K) for _ in range(6)]
+        lib().orc_psf_tables(self.h, *[_p(o) for o in out])
+        return dict(zip(["kx", "ky", "kz", "kzoil", "pupil", "phase"], out))
+
+    def model(self, R, xyz, derivs=False):
+        xyz = _f64(np.atleast_2d(xyz))
+        n = xyz.shape[0]
+        out = np.zeros((n, R, R))
+        d = np.zeros((n, 3, R, R)) if derivs else None
+        lib().orc_psf_model(self.h, R, n, _p(xyz), _p(out), _p(d) if derivs else None)
+        return (out, d) if derivs else out
+
+    def model_oil(self, R, x, y, zoil, zwat):
+        out = np.zeros((R, R))
+        lib().orc_psf_model_oil(self.h, R, x, y, zoil, zwat, _p(out))
+        return out
+
+    def localize_cd(self, patches, init_abxyz, minZ, maxZ, iter_max=20, photon_thr=0.0, threads=1):
+        patches = _f64(patches)
+        n, R = patches.shape[0], patches.shape[1]
+        init = _f64(init_abxyz)
+        out = np.zeros((n, 5))
+        crlb = np.zeros((n, 3))
+        st = np.zeros(n, np.int32)
+        ev = np.zeros(n, np.int32)
+        lib().orc_localize_cd(self.h, R, n, _p(patches), _p(init), minZ, maxZ, iter_max, photon_thr,
+                              _p(out), _p(crlb), _p(st), _p(ev), threads)
+        return out, crlb, st, ev
+
+    def fit_lm(self, patches, init_xyzab, zmin, zmax, xymax, tol_xyz=1e-5, step_xy=0.11, step_z=0.22,
+               max_iter=30, threads=1, crlb=False):
+        patches = _f64(patches)
+        n, R = patches.shape[0], patches.shape[1]
+        init = _f64(init_xyzab)
+        prm = _f64([zmin, zmax, xymax, tol_xyz, step_xy, step_z])
+        out = np.zeros((n, 5))
+        nll = np.zeros(n)
+        st = np.zeros(n, np.int32)
+        ev = np.zeros(n, np.int32)
+        cr = np.zeros((n, 5)) if crlb else None
+        lib().orc_fit_lm(self.h, R, n, _p(patches), _p(init), _p(prm), max_iter, _p(out), _p(nll), _p(st),
+                         _p(ev), _p(cr) if crlb else None, threads)
+        return (out, nll, st, ev, cr) if crlb else (out, nll, st, ev)
+
+    def nll_grad(self, patch, theta):
+        patch = _f64(patch)
+        th = _f64(theta)
+        g = np.zeros(5)
+        H = np.zeros(25)
+        v = lib().orc_nll_grad(self.h, patch.shape[0], _p(patch), _p(th), _p(g), _p(H))
+        return v, g, H.reshape(5, 5)
+
+    def crlb_fd(self, R, theta):
+        th = _f64(theta)
+        out = np.zeros(3)
+        lib().orc_crlb_fd(self.h, R, _p(th), _p(out))
+        return out
+
+    def calib_nll(self, R, dz, stack, x, y, z, A, B):
+        dz = _f64(dz)
+        stack = _f64(stack)
+        return lib().orc_calib_nll(self.h, R, len(dz), _p(dz), _p(stack), x, y, z, A, B)
+
+
+class OracleDetector:
+    """Predetection (process/cpu/Predetection.java) for frames [X][Y]."""
+
+    def __init__(self, psf, SX, SY, R, minZ, maxZ, step, thr=0.1):
+        self.psf = psf
+        self.SX, self.SY, self.R = SX, SY, R
+        self.h = lib().orc_det_create(psf.h, SX, SY, R, minZ, maxZ, step, thr)
+        self.nz = lib().orc_det_nslices(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.orc_det_destroy(self.h)
+            self.h = None
+
+    def library(self):
+        rng = np.zeros(self.nz)
+        psfs = np.zeros((self.nz, self.R, self.R))
+        lib().orc_det_library(self.h, _p(rng), _p(psfs))
+        return rng, psfs
+
+    def detect(self, frames, cap=4096, threads=1):
+        frames = _f64(frames)
+        nf = frames.shape[0]
+        out = np.zeros((nf, cap, 7))
+        counts = np.zeros(nf, np.int32)
+        lib().orc_detect(self.h, nf, _p(frames), cap, _p(out), _p(counts), threads)
+        return [out[f, :min(cap, counts[f])] for f in range(nf)]

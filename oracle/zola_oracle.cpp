@@ -1,0 +1,894 @@
+// ORACLE — test infrastructure only.
+//
+// FP64 CPU restatement of ZOLA-3D's localization hot path, written from the
+// reference's Java sources (paths relative to src/main/java/org/pasteur/imagej/).
+// It is the checker for the CUDA library: only tests/, __graft_entry__.smoke()
+// and bench.py's cpu_baseline leg may load it.  The product never links it.
+//
+// PARITY UNPINNED: the reference ships no tests, golden vectors or fixtures for
+// this path, and it is a Java/ImageJ plugin that cannot be built or run in this
+// environment (no JVM).  This restatement is therefore pinned only by
+// known-answer tests derived from the mathematics (FFT round trip, Zernike
+// orthogonality, symmetric in-focus PSF, translation equivariance).
+//
+// What is restated, function by function:
+//   geometry          process/PhaseParameters.java:265-366
+//   Zernike basis     utils/Zernike.java:26-79, 540-608, 818-836
+//   phase combination process/cpu/ZernikePhase.java:200-224
+//   pupil tables      process/cpu/PSFPhase.java:96-269 (constructor),
+//                     :417-464 (resetKz)
+//   PSF model         process/cpu/PSFPhase.java:361-378 (Gaussian), :557-629
+//   unitary FFT       utils/FastFourierTransform.java:628-796 (convention only:
+//                     every 1-D pass divided by sqrt(n), forward exponent -i)
+//   likelihood        process/cpu/Localization.java:1125-1143
+//   coordinate descent process/cpu/Localization.java:491-1058
+//   Fisher / CRLB     process/cpu/Localization.java:317-451
+//   detection         process/cpu/Predetection.java:63-593
+//   calibration NLL   process/cpu/ZernikePhaseRetrieval.java:1843-1874
+// plus the FP64 Levenberg-Marquardt fit of the same Poisson NLL with analytic
+// x/y/z derivatives (no reference counterpart: the "FP64 oracle of the same
+// fit" that the GPU fits are compared against).
+
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+#include <thread>
+#include <atomic>
+#include <array>
+#include <functional>
+
+namespace {
+
+typedef std::complex<double> cplx;
+
+int pow2ceil(int n) {
+    int p = 1;
+    while (p < n) p <<= 1;
+    return p;
+}
+
+// ---------------------------------------------------------------- FFT ------
+// Radix-2 in-place complex FFT with exact twiddles, unitary scaling per pass.
+// sign = -1 forward, +1 inverse (FastFourierTransform.java:700-790 convention).
+void fft1d(cplx* a, int n, int sign) {
+    for (int i = 1, j = 0; i < n; ++i) {
+        int bit = n >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) std::swap(a[i], a[j]);
+    }
+    for (int len = 2; len <= n; len <<= 1) {
+        int half = len >> 1;
+        for (int k = 0; k < half; ++k) {
+            double ang = sign * 2.0 * M_PI * (double)k / (double)len;
+            cplx w(std::cos(ang), std::sin(ang));
+            for (int i = 0; i < n; i += len) {
+                cplx u = a[i + k];
+                cplx v = a[i + k + half] * w;
+                a[i + k] = u + v;
+                a[i + k + half] = u - v;
+            }
+        }
+    }
+    double s = 1.0 / std::sqrt((double)n);
+    for (int i = 0; i < n; ++i) a[i] *= s;
+}
+
+// 2-D unitary FFT over a row-major n x n array.
+void fft2d(std::vector<cplx>& a, int n, int sign) {
+    std::vector<cplx> col(n);
+    for (int i = 0; i < n; ++i) fft1d(&a[(size_t)i * n], n, sign);
+    for (int j = 0; j < n; ++j) {
+        for (int i = 0; i < n; ++i) col[i] = a[(size_t)i * n + j];
+        fft1d(col.data(), n, sign);
+        for (int i = 0; i < n; ++i) a[(size_t)i * n + j] = col[i];
+    }
+}
+
+// ------------------------------------------------------------- Zernike -----
+double factorial(int n) {  // Zernike.java:818-836 (long table to 19, then double)
+    double f = 1.0;
+    for (int i = 2; i <= n; ++i) f *= i;
+    return f;
+}
+
+// Un-normalised Zernike polynomial, Zernike.java:574-608.
+double zernike_value(int n, int m, double theta, double rho) {
+    int am = m < 0 ? -m : m;
+    double som = 0.0;
+    for (int k = 0; k <= (n - am) / 2; ++k) {
+        double truc = ((k & 1) ? -1.0 : 1.0) * factorial(n - k);
+        double trac = factorial(k) * factorial((n + am) / 2 - k) * factorial((n - am) / 2 - k);
+        som += (truc / trac) * std::pow(rho, n - 2 * k);
+    }
+    return m >= 0 ? som * std::cos(theta * am) : som * std::sin(theta * am);
+}
+
+// Index order of Zernike.java:31-47: n = 0,1,2..., m = -n, -n+2, ..., n.
+void zernike_nm(int idx, int* n_out, int* m_out) {
+    int i = 0;
+    for (int n = 0;; ++n)
+        for (int m = -n; m <= n; m += 2) {
+            if (i == idx) { *n_out = n; *m_out = m; return; }
+            ++i;
+        }
+}
+
+// ----------------------------------------------------------------- PSF -----
+struct Psf {
+    int N;                 // pupil grid (power of two, size_cpu)
+    double dx, na, lambda, n_oil, n_wat, sigma, zfocus;
+    int apo, kz_reset, gauss_f32;
+    int K;                 // disk pixels
+    std::vector<int> di, dj;
+    std::vector<double> kx, ky, kz, kzoil, isim, isimoil, pupil, phase;
+};
+
+// PhaseParameters.java:300-362 + PSFPhase.java:140-220 (+ resetKz :417-464).
+Psf* psf_build(int N_in, double dx, double na, double lambda, double n_oil, double n_wat,
+               double sigma, int apo, double zfocus, int kz_reset, int gauss_f32,
+               int nz, const double* zern) {
+    Psf* p = new Psf();
+    int N = N_in;
+    if (N % 2) N--;
+    N = pow2ceil(N);
+    p->N = N; p->dx = dx; p->na = na; p->lambda = lambda; p->n_oil = n_oil; p->n_wat = n_wat;
+    p->sigma = sigma; p->apo = apo; p->zfocus = zfocus; p->kz_reset = kz_reset; p->gauss_f32 = gauss_f32;
+    double ringsize = (na / lambda) * (na / lambda);
+    double c = (double)(N / 2) - 0.5;
+    double radius = std::sqrt(ringsize) * (N * dx);
+    double left = (n_wat / lambda) * (n_wat / lambda);
+    double left_oil = (n_oil / lambda) * (n_oil / lambda);
+    std::vector<double> zn(nz), zm(nz);
+    for (int i = 0; i < N; ++i)
+        for (int ii = 0; ii < N; ++ii) {
+            double a = (i - c) / (N * dx), b = (ii - c) / (N * dx);
+            double disk = a * a + b * b;
+            if (!(disk <= ringsize)) continue;
+            p->di.push_back(i); p->dj.push_back(ii);
+            p->kx.push_back((i - c) * (2 * M_PI) / (dx * N));
+            p->ky.push_back((ii - c) * (2 * M_PI) / (dx * N));
+            double kxx = ((i - c) / (dx * N)) * ((i - c) / (dx * N));
+            double kyy = ((ii - c) / (dx * N)) * ((ii - c) / (dx * N));
+            double right = kxx + kyy;
+            if (left > right) { p->kz.push_back(2 * M_PI * std::sqrt(left - right)); p->isim.push_back(1); }
+            else { p->kz.push_back(kz_reset ? 2 * M_PI * std::sqrt(std::fabs(left - right)) : 0.0); p->isim.push_back(0); }
+            if (left_oil > right) { p->kzoil.push_back(2 * M_PI * std::sqrt(left_oil - right)); p->isimoil.push_back(1); }
+            else { p->kzoil.push_back(0.0); p->isimoil.push_back(0); }
+            // phase: sum_i a_i Z_i, Zernike evaluated where rho < 1 (Zernike.java:553-560)
+            double x = (i - c) / radius, y = (ii - c) / radius;
+            double rho = std::sqrt(x * x + y * y), theta = std::atan2(y, x);
+            double ph = 0.0;
+            for (int z = 0; z < nz; ++z) {
+                int n, m;
+                zernike_nm(z, &n, &m);
+                double v = rho < 1 ? zernike_value(n, m, theta, rho) : 0.0;
+                ph += v * zern[z];
+            }
+            p->phase.push_back(ph);
+        }
+    p->K = (int)p->di.size();
+    for (int k = 0; k < p->K; ++k) {
+        if (apo) {
+            double kxx = p->kx[k] / (2 * M_PI), kyy = p->ky[k] / (2 * M_PI);
+            double right = kxx * kxx + kyy * kyy;
+            p->pupil.push_back(left_oil > right ? (double)(float)(1.0 / std::pow(1 - right / left_oil, .25)) : 0.0);
+        } else {
+            p->pupil.push_back(1.0 / std::sqrt((double)p->K));
+        }
+    }
+    return p;
+}
+
+int window_size(int R, int N) {  // PSFPhase.java:100-108
+    int w = 2 * R;
+    if (w > N) w = N;
+    return pow2ceil(w);
+}
+
+// Separable spectral Gaussian g(f) for the W-grid blur, PSFPhase.java:361-378.
+double gauss_value(const Psf* p, int W, int a, int b) {
+    double sigF = (1.0 / p->sigma) * W / (M_PI * 2);
+    double sigpow = sigF * sigF;
+    double cc = W / 2;
+    double v = std::exp(-.5 * ((a - cc) * (a - cc) + (b - cc) * (b - cc)) / sigpow);
+    return p->gauss_f32 ? (double)(float)v : v;
+}
+
+// Pupil field with an optional per-pixel multiplier (used for derivatives).
+// deriv: 0 none, 1 x, 2 y, 3 z (zwat).  For deriv != 0 the field is the
+// derivative of the field with respect to that coordinate.
+void pupil_field(const Psf* p, double x, double y, double zoil, double zwat, int deriv,
+                 std::vector<cplx>& grid) {
+    int N = p->N;
+    grid.assign((size_t)N * N, cplx(0, 0));
+    for (int k = 0; k < p->K; ++k) {
+        double pp = p->kx[k] * x + p->ky[k] * y + p->phase[k];
+        double q = pp + p->kz[k] * zwat - p->kzoil[k] * zoil;
+        double r = pp + p->kz[k] * zwat * p->isim[k] - p->kzoil[k] * zoil * p->isimoil[k];
+        cplx v;
+        if (deriv == 0) v = cplx(p->pupil[k] * std::cos(q), p->pupil[k] * std::sin(r));
+        else {
+            double dq, dr;
+            if (deriv == 1) { dq = p->kx[k]; dr = p->kx[k]; }
+            else if (deriv == 2) { dq = p->ky[k]; dr = p->ky[k]; }
+            else { dq = p->kz[k]; dr = p->kz[k] * p->isim[k]; }
+            v = cplx(-p->pupil[k] * std::sin(q) * dq, p->pupil[k] * std::cos(r) * dr);
+        }
+        grid[(size_t)((p->di[k] + N / 2) % N) * N + (p->dj[k] + N / 2) % N] = v;
+    }
+}
+
+// Blur of a real W x W intensity window laid out as in PSFPhase.computePSF
+// (centre at W/2), returning the complex blurred window (unitary FFTs).
+void blur_window(const Psf* p, int W, const std::vector<double>& I, std::vector<cplx>& out) {
+    out.assign((size_t)W * W, cplx(0, 0));
+    for (int i = 0; i < W; ++i)
+        for (int ii = 0; ii < W; ++ii)
+            out[(size_t)((i + W / 2) % W) * W + (ii + W / 2) % W] = cplx(I[(size_t)i * W + ii], 0);
+    fft2d(out, W, -1);
+    for (int i = 0; i < W; ++i)
+        for (int ii = 0; ii < W; ++ii)
+            out[(size_t)i * W + ii] *= gauss_value(p, W, (i + W / 2) % W, (ii + W / 2) % W);
+    fft2d(out, W, +1);
+}
+
+// PSFPhase.computePSF (PSFPhase.java:557-629): psi[R][R], first index <-> x.
+// With derivs != nullptr also the analytic derivatives d psi / d{x,y,zwat}
+// (3 * R * R), obtained through the same FFT route.
+void psf_model(const Psf* p, int R, double x, double y, double zoil, double zwat,
+               double* psi, double* derivs) {
+    int N = p->N, W = window_size(R, N);
+    std::vector<cplx> E, Ed[3];
+    pupil_field(p, x, y, zoil, zwat, 0, E);
+    fft2d(E, N, +1);
+    int nd = derivs ? 3 : 0;
+    for (int d = 0; d < nd; ++d) {
+        pupil_field(p, x, y, zoil, zwat, d + 1, Ed[d]);
+        fft2d(Ed[d], N, +1);
+    }
+    std::vector<double> I((size_t)W * W), Id[3];
+    for (int d = 0; d < nd; ++d) Id[d].resize((size_t)W * W);
+    for (int i = 0; i < W; ++i)
+        for (int ii = 0; ii < W; ++ii) {
+            size_t src = (size_t)((N / 2 - W / 2 + i + N / 2) % N) * N + (N / 2 - W / 2 + ii + N / 2) % N;
+            cplx e = E[src];
+            I[(size_t)i * W + ii] = e.real() * e.real() + e.imag() * e.imag();
+            for (int d = 0; d < nd; ++d)
+                Id[d][(size_t)i * W + ii] = 2.0 * (std::conj(e) * Ed[d][src]).real();
+        }
+    std::vector<cplx> B, Bd[3];
+    blur_window(p, W, I, B);
+    for (int d = 0; d < nd; ++d) blur_window(p, W, Id[d], Bd[d]);
+    double sum = 0.0;
+    std::vector<double> m((size_t)R * R), dm[3];
+    for (int d = 0; d < nd; ++d) dm[d].resize((size_t)R * R);
+    double dsum[3] = {0, 0, 0};
+    for (int i = 0; i < R; ++i)
+        for (int ii = 0; ii < R; ++ii) {
+            size_t src = (size_t)((W / 2 - R / 2 + i + W / 2) % W) * W + (W / 2 - R / 2 + ii + W / 2) % W;
+            cplx b = B[src];
+            double mag = std::sqrt(b.real() * b.real() + b.imag() * b.imag());
+            m[(size_t)i * R + ii] = mag;
+            sum += mag;
+            for (int d = 0; d < nd; ++d) {
+                // d|b| = Re(conj(b) db)/|b|; the blurred window is real up to rounding.
+                double v = mag > 0 ? (std::conj(b) * Bd[d][src]).real() / mag : 0.0;
+                dm[d][(size_t)i * R + ii] = v;
+                dsum[d] += v;
+            }
+        }
+    for (int k = 0; k < R * R; ++k) psi[k] = m[k] / sum;
+    for (int d = 0; d < nd; ++d)
+        for (int k = 0; k < R * R; ++k)
+            derivs[(size_t)d * R * R + k] = (dm[d][k] - psi[k] * dsum[d]) / sum;
+}
+
+// ------------------------------------------------- coordinate descent ------
+// Localization.java (single camera, single frame), with Zfocus as zoil.
+struct CD {
+    const Psf* p;
+    int R;
+    const double* d;   // patch R*R (photons), [x][y]
+    double minZ, maxZ;
+    int iterMax;
+    double photonThreshold;
+    double h = .0005, eps = .0001, maxShift;
+    double tx, ty, tz, ta, tb;
+    std::vector<double> psi, mu;
+    int nevals = 0;
+
+    double lik(double x, double y, double z, double a, double b) {  // :1125-1143
+        psf_model(p, R, x, y, p->zfocus, z, psi.data(), nullptr);
+        ++nevals;
+        double l = 0;
+        for (int k = 0; k < R * R; ++k) {
+            double m = psi[k] * a + b;
+            mu[k] = m;
+            l += m - d[k] * std::log(m);
+        }
+        return l;
+    }
+    void clampAB() { ta = std::max(1.0, ta); tb = std::max(.01, tb); }  // testPhotonNumber
+    static double newton(double l1, double l2, double l3, double h) {
+        double curv = std::fabs((l3 + l1 - 2 * l2) / (h * h));
+        if (curv == 0) return (l3 - l1) * (2 * h);
+        return ((l3 - l1) / (2 * h)) / curv;
+    }
+    // minimizeX/Y/Z (:672-916): Newton step capped at maxShift, gamma 1, .1, .01.
+    double minCoord(double* t, double prev, int which) {
+        double save = *t;
+        double l1, l3;
+        double sv = *t;
+        *t = sv - h; l1 = lik(tx, ty, tz, ta, tb);
+        *t = sv + h; l3 = lik(tx, ty, tz, ta, tb);
+        *t = sv;
+        (void)which;
+        double l2 = prev;
+        double g = newton(l1, l2, l3, h);
+        if (g > maxShift) g = maxShift;
+        else if (g < -maxShift) g = -maxShift;
+        for (double gamma = 1; gamma > .02; gamma /= 10) {
+            *t -= gamma * g;
+            double l = lik(tx, ty, tz, ta, tb);
+            if (l < l2) { prev = l; break; }
+            *t = save;
+        }
+        return prev;
+    }
+    // minimizeA (:919-970) and minimizeB (:974-1036): no early break.
+    double minAB(double* t, double hh) {
+        double save = *t;
+        double sv = *t;
+        *t = sv - hh; double l1 = lik(tx, ty, tz, ta, tb);
+        *t = sv; double l2 = lik(tx, ty, tz, ta, tb);
+        *t = sv + hh; double l3 = lik(tx, ty, tz, ta, tb);
+        *t = save;
+        double g = newton(l1, l2, l3, hh);
+        for (double gamma = 1; gamma > .02; gamma /= 10) {
+            *t -= gamma * g;
+            double l = lik(tx, ty, tz, ta, tb);
+            if (l < l2) { l2 = l; save = *t; }
+            else *t = save;
+        }
+        return lik(tx, ty, tz, ta, tb);
+    }
+    // localize (:491-653); returns false on the photon-count break or NaN.
+    int run() {
+        clampAB();
+        double likelihood = lik(tx, ty, tz, ta, tb);
+        double oX = 1e300, oY = 1e300, oZ = 1e300;
+        bool brk4 = false;
+        likelihood = minAB(&ta, h * 1000); clampAB();
+        likelihood = minAB(&tb, h * 10); clampAB();
+        int it = 0;
+        for (int i = 0; i < iterMax; ++i) {
+            it = i + 1;
+            likelihood = minCoord(&tz, likelihood, 2);
+            if (tz < minZ) tz = minZ;
+            if (tz > maxZ) tz = maxZ;
+            likelihood = minCoord(&tx, likelihood, 0);
+            likelihood = minCoord(&ty, likelihood, 1);
+            likelihood = minAB(&ta, h * 1000); clampAB();
+            likelihood = minAB(&tb, h * 10); clampAB();
+            double dist = std::sqrt((tx - oX) * (tx - oX) + (ty - oY) * (ty - oY) + (tz - oZ) * (tz - oZ));
+            bool breaking = false;
+            if (i > 4) { breaking = !(ta > photonThreshold); if (breaking) brk4 = true; }
+            if (dist < eps || breaking) break;
+            if (std::isnan(likelihood)) return -1;
+            oX = tx; oY = ty; oZ = tz;
+        }
+        (void)it;
+        return brk4 ? 0 : 1;
+    }
+};
+
+// Finite-difference Fisher matrix and CRLB, Localization.java:317-451,
+// including its A-derivative, which differentiates mu*(a+-h)+b (mu, not psi).
+void fisher_crlb_fd(const Psf* p, int R, double x, double y, double z, double a, double b,
+                    double* crlb3) {
+    int n = R * R;
+    double h = .0005;
+    std::vector<double> f(n), f1(n), f0[5], f2[5], tmp(n);
+    for (int q = 0; q < 5; ++q) { f0[q].resize(n); f2[q].resize(n); }
+    psf_model(p, R, x, y, p->zfocus, z, f.data(), nullptr);
+    for (int k = 0; k < n; ++k) f1[k] = f[k] * a + b;
+    double sh[3][2][3] = {{{x + h, y, z}, {x - h, y, z}}, {{x, y + h, z}, {x, y - h, z}}, {{x, y, z + h}, {x, y, z - h}}};
+    for (int q = 0; q < 3; ++q) {
+        psf_model(p, R, sh[q][0][0], sh[q][0][1], p->zfocus, sh[q][0][2], tmp.data(), nullptr);
+        for (int k = 0; k < n; ++k) f2[q][k] = tmp[k] * a + b;
+        psf_model(p, R, sh[q][1][0], sh[q][1][1], p->zfocus, sh[q][1][2], tmp.data(), nullptr);
+        for (int k = 0; k < n; ++k) f0[q][k] = tmp[k] * a + b;
+    }
+    for (int k = 0; k < n; ++k) {
+        f0[3][k] = f1[k] * (a - h) + b; f2[3][k] = f1[k] * (a + h) + b;
+        f0[4][k] = f1[k] * a + (b - h); f2[4][k] = f1[k] * a + (b + h);
+    }
+    double F[5][5];
+    for (int q = 0; q < 5; ++q)
+        for (int qq = 0; qq < 5; ++qq) {
+            double s = 0;
+            for (int k = 0; k < n; ++k) {
+                double d1 = (f2[q][k] - f0[q][k]) / (2 * std::fabs(h));
+                double d2 = (f2[qq][k] - f0[qq][k]) / (2 * std::fabs(h));
+                s += (1 / f1[k]) * d1 * d2;
+            }
+            F[q][qq] = s;
+        }
+    // Gauss-Jordan inverse with partial pivoting; on failure fall back to 1/F_ii.
+    double M[5][10];
+    for (int i = 0; i < 5; ++i)
+        for (int j = 0; j < 10; ++j) M[i][j] = j < 5 ? F[i][j] : (j - 5 == i ? 1 : 0);
+    bool ok = true;
+    for (int c = 0; c < 5 && ok; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < 5; ++r) if (std::fabs(M[r][c]) > std::fabs(M[piv][c])) piv = r;
+        if (M[piv][c] == 0) { ok = false; break; }
+        for (int j = 0; j < 10; ++j) std::swap(M[c][j], M[piv][j]);
+        double dv = M[c][c];
+        for (int j = 0; j < 10; ++j) M[c][j] /= dv;
+        for (int r = 0; r < 5; ++r) if (r != c) {
+            double fct = M[r][c];
+            for (int j = 0; j < 10; ++j) M[r][j] -= fct * M[c][j];
+        }
+    }
+    for (int i = 0; i < 3; ++i) {
+        if (ok) crlb3[i] = std::sqrt(M[i][5 + i]);
+        else crlb3[i] = F[i][i] != 0 ? std::sqrt(1 / F[i][i]) : 1.79769313486231570e308;
+    }
+}
+
+// ------------------------------------------------------------ LM fit -------
+// The FP64 Levenberg-Marquardt fit shared (as an algorithm) with the GPU
+// library.  theta = x, y, z (um), A (photons), B (photons/px).
+struct LMParams {
+    double zmin, zmax, xymax;  // box: |x|,|y| <= xymax, zmin <= z <= zmax
+    int max_iter;              // model evaluations
+    double tol_xyz;            // um
+    double step_xy, step_z;    // per-iteration caps (um)
+};
+
+// Deviance-form Poisson NLL: sum mu - d - d ln(mu/d) (mu - d ln mu + const).
+// Returns +inf if any mu <= 0.
+double model_eval(const Psf* p, int R, const double* d, const double* th, double* g, double H[5][5],
+                  std::vector<double>& psi, std::vector<double>& dpsi) {
+    int n = R * R;
+    psf_model(p, R, th[0], th[1], p->zfocus, th[2], psi.data(), dpsi.data());
+    double nll = 0;
+    for (int q = 0; q < 5; ++q) { g[q] = 0; for (int r = 0; r < 5; ++r) H[q][r] = 0; }
+    for (int k = 0; k < n; ++k) {
+        double mu = th[3] * psi[k] + th[4];
+        if (!(mu > 0)) return INFINITY;
+        double dk = d[k];
+        nll += dk > 0 ? mu - dk - dk * std::log(mu / dk) : mu;
+        double j[5] = {th[3] * dpsi[k], th[3] * dpsi[n + k], th[3] * dpsi[2 * n + k], psi[k], 1.0};
+        double w = 1.0 - dk / mu, w2 = dk / (mu * mu);
+        for (int q = 0; q < 5; ++q) {
+            g[q] += w * j[q];
+            for (int r = 0; r <= q; ++r) H[q][r] += w2 * j[q] * j[r];
+        }
+    }
+    for (int q = 0; q < 5; ++q) for (int r = q + 1; r < 5; ++r) H[q][r] = H[r][q];
+    return nll;
+}
+
+// Cholesky solve of (H + lambda diag H) delta = -g; false if not positive definite.
+bool damped_solve(const double H[5][5], const double* g, double lambda, double* delta) {
+    double L[5][5] = {};
+    for (int i = 0; i < 5; ++i)
+        for (int j = 0; j <= i; ++j) {
+            double s = H[i][j] + (i == j ? lambda * H[i][i] : 0.0);
+            for (int k = 0; k < j; ++k) s -= L[i][k] * L[j][k];
+            if (i == j) {
+                if (!(s > 0)) return false;
+                L[i][i] = std::sqrt(s);
+            } else L[i][j] = s / L[j][j];
+        }
+    double yv[5];
+    for (int i = 0; i < 5; ++i) {
+        double s = -g[i];
+        for (int k = 0; k < i; ++k) s -= L[i][k] * yv[k];
+        yv[i] = s / L[i][i];
+    }
+    for (int i = 4; i >= 0; --i) {
+        double s = yv[i];
+        for (int k = i + 1; k < 5; ++k) s -= L[k][i] * delta[k];
+        delta[i] = s / L[i][i];
+    }
+    return true;
+}
+
+void clamp_theta(double* th, const LMParams& P) {
+    th[0] = std::min(std::max(th[0], -P.xymax), P.xymax);
+    th[1] = std::min(std::max(th[1], -P.xymax), P.xymax);
+    th[2] = std::min(std::max(th[2], P.zmin), P.zmax);
+    th[3] = std::max(th[3], 1.0);
+    th[4] = std::max(th[4], 0.01);
+}
+
+// status: 1 converged, 2 max evaluations, 3 stalled (lambda at bound), -1 NaN.
+int lm_fit(const Psf* p, int R, const double* d, const double* init, const LMParams& P,
+           double* out, double* nll_out, int* evals_out, double* crlb5) {
+    int n = R * R;
+    std::vector<double> psi(n), dpsi(3 * n), psi2(n), dpsi2(3 * n);
+    double th[5], g[5], H[5][5];
+    for (int q = 0; q < 5; ++q) th[q] = init[q];
+    clamp_theta(th, P);
+    double nll = model_eval(p, R, d, th, g, H, psi, dpsi);
+    int evals = 1;
+    double lambda = 1e-3;
+    int status = 2;
+    if (!std::isfinite(nll)) status = -1;
+    while (status == 2 && evals < P.max_iter) {
+        double delta[5];
+        if (!damped_solve(H, g, lambda, delta)) {
+            lambda *= 10;
+            if (lambda > 1e7) { status = 3; break; }
+            continue;
+        }
+        double sxy = std::max(std::fabs(delta[0]), std::fabs(delta[1]));
+        double scale = 1.0;
+        if (sxy > P.step_xy) scale = P.step_xy / sxy;
+        if (std::fabs(delta[2]) * scale > P.step_z) scale = P.step_z / std::fabs(delta[2]);
+        double t2[5], g2[5], H2[5][5];
+        for (int q = 0; q < 5; ++q) t2[q] = th[q] + scale * delta[q];
+        clamp_theta(t2, P);
+        double step = std::max(std::fabs(t2[0] - th[0]), std::max(std::fabs(t2[1] - th[1]), std::fabs(t2[2] - th[2])));
+        double nll2 = model_eval(p, R, d, t2, g2, H2, psi2, dpsi2);
+        ++evals;
+        if (nll2 <= nll) {
+            for (int q = 0; q < 5; ++q) { th[q] = t2[q]; g[q] = g2[q]; for (int r = 0; r < 5; ++r) H[q][r] = H2[q][r]; }
+            nll = nll2;
+            lambda = std::max(lambda * 0.1, 1e-7);
+            if (step < P.tol_xyz) status = 1;
+        } else {
+            lambda *= 10;
+            if (step < P.tol_xyz) status = 1;
+            else if (lambda > 1e7) status = 3;
+        }
+    }
+    for (int q = 0; q < 5; ++q) out[q] = th[q];
+    *nll_out = nll;
+    *evals_out = evals;
+    if (crlb5) {  // sqrt(diag(F^-1)) from the analytic Fisher matrix at the optimum
+        model_eval(p, R, d, th, g, H, psi, dpsi);
+        double F[5][5] = {};
+        for (int k = 0; k < n; ++k) {
+            double mu = th[3] * psi[k] + th[4];
+            double j[5] = {th[3] * dpsi[k], th[3] * dpsi[n + k], th[3] * dpsi[2 * n + k], psi[k], 1.0};
+            for (int q = 0; q < 5; ++q) for (int r = 0; r < 5; ++r) F[q][r] += j[q] * j[r] / mu;
+        }
+        for (int c = 0; c < 5; ++c) {
+            double e[5] = {0, 0, 0, 0, 0}, col[5];
+            e[c] = 1;
+            double G[5] = {-e[0], -e[1], -e[2], -e[3], -e[4]};
+            if (damped_solve(F, G, 0.0, col)) crlb5[c] = std::sqrt(col[c]);
+            else crlb5[c] = NAN;
+        }
+    }
+    return status;
+}
+
+// ----------------------------------------------------------- detection ----
+// Predetection.java:63-593 (one frame).  image is [X][Y] (first index x).
+struct Detector {
+    const Psf* p;
+    int SX, SY, R, MX, MY, nz;
+    double thr, zstep;
+    std::vector<double> range, varPSF, normImage;
+    std::vector<std::vector<cplx>> dict;
+    std::vector<std::vector<double>> libpsf;
+};
+
+void fft2d_rect(std::vector<cplx>& a, int nx, int ny, int sign) {
+    std::vector<cplx> col(nx);
+    for (int i = 0; i < nx; ++i) fft1d(&a[(size_t)i * ny], ny, sign);
+    for (int j = 0; j < ny; ++j) {
+        for (int i = 0; i < nx; ++i) col[i] = a[(size_t)i * ny + j];
+        fft1d(col.data(), nx, sign);
+        for (int i = 0; i < nx; ++i) a[(size_t)i * ny + j] = col[i];
+    }
+}
+
+Detector* det_build(const Psf* p, int SX, int SY, int R, double minZ, double maxZ, double step, double thr) {
+    Detector* D = new Detector();
+    D->p = p; D->SX = SX; D->SY = SY; D->R = R; D->thr = thr; D->zstep = step;
+    D->MX = pow2ceil(2 * SX); D->MY = pow2ceil(2 * SY);
+    D->normImage.resize((size_t)SX * SY);
+    for (int i = 0; i < SX; ++i)          // Predetection.java:95-116, verbatim index rules
+        for (int ii = 0; ii < SY; ++ii) {
+            int vx1 = R / 2, vx2 = R / 2;
+            if (i < R / 2 - 1) vx1 = i + 1;
+            if (i > SX - R / 2 - 2) vx2 = SY - i - 1;
+            int vy1 = R / 2, vy2 = R / 2;
+            if (ii < R / 2 - 1) vy1 = ii + 1;
+            if (ii > SX - R / 2 - 2) vy2 = SY - ii - 2;
+            D->normImage[(size_t)i * SY + ii] = (double)((vx1 + vx2) * (vy1 + vy2));
+        }
+    int number = (int)std::ceil((maxZ - minZ) / step);
+    double z = minZ;
+    for (int i = 0; i < number; ++i) { D->range.push_back(z); z += step; }
+    D->nz = number;
+    std::vector<double> psf((size_t)R * R);
+    for (int i = 0; i < number; ++i) {
+        psf_model(p, R, 0, 0, p->zfocus, D->range[i], psf.data(), nullptr);
+        D->libpsf.push_back(psf);
+        double mean = 0;
+        for (int k = 0; k < R * R; ++k) mean += psf[k];
+        mean /= (double)R * R;
+        double var = 0;
+        std::vector<double> pd(psf);
+        for (int k = 0; k < R * R; ++k) { pd[k] -= mean; var += pd[k] * pd[k]; }
+        var /= (double)(R * R);
+        D->varPSF.push_back(var);
+        std::vector<cplx> g((size_t)D->MX * D->MY, cplx(0, 0));
+        for (int u = 0; u < R; ++u)
+            for (int uu = 0; uu < R; ++uu) {
+                int x = (u - R / 2 + D->MX / 2 + D->MX / 2) % D->MX;
+                int y = (uu - R / 2 + D->MY / 2 + D->MY / 2) % D->MY;
+                g[(size_t)x * D->MY + y] = cplx(pd[(size_t)u * R + uu], 0);
+            }
+        fft2d_rect(g, D->MX, D->MY, -1);
+        D->dict.push_back(g);
+    }
+    return D;
+}
+
+double top_of_parabola(double xa, double ya, double xb, double yb, double xc, double yc) {
+    double a = (yc - ya) / ((xc - xa) * (xc - xb)) - (yb - ya) / ((xb - xa) * (xc - xb));
+    double b = ((yb - ya) / (xb - xa)) - a * (xb + xa);
+    return -b / (2 * a);
+}
+
+// Candidate rows: score, r, i, j, topZ, topX, topY (Predetection.java:520-540).
+void det_frame(const Detector* D, const double* image, std::vector<std::array<double, 7>>& out) {
+    int SX = D->SX, SY = D->SY, R = D->R, MX = D->MX, MY = D->MY;
+    std::vector<double> full((size_t)SX * SY);
+    std::vector<cplx> X((size_t)MX * MY, cplx(0, 0));
+    for (int i = 0; i < SX; ++i)
+        for (int ii = 0; ii < SY; ++ii) {
+            full[(size_t)i * SY + ii] = (double)(float)image[(size_t)i * SY + ii];
+            int x = (i - SX / 2 + MX / 2 + MX / 2) % MX;
+            int y = (ii - SY / 2 + MY / 2 + MY / 2) % MY;
+            X[(size_t)x * MY + y] = cplx(image[(size_t)i * SY + ii], 0);
+        }
+    fft2d_rect(X, MX, MY, -1);
+    // running sums (Predetection.java:337-405)
+    std::vector<double> s1((size_t)SX * SY), s2((size_t)SX * SY), t1((size_t)SX * SY), t2((size_t)SX * SY);
+    auto F = [&](int i, int j) { return full[(size_t)i * SY + j]; };
+    for (int i = 0; i < SX; ++i) {
+        double a = 0, b = 0;
+        for (int t = 0; t < R / 2 + 1; ++t) if (t < SY) { a += F(i, t); b += F(i, t) * F(i, t); }
+        s1[(size_t)i * SY] = a; s2[(size_t)i * SY] = b;
+        for (int ii = 1; ii < SY; ++ii) {
+            double v = s1[(size_t)i * SY + ii - 1];
+            if (ii - R / 2 >= 0) v -= F(i, ii - R / 2);
+            if (ii + R / 2 < SY) v += F(i, ii + R / 2);
+            s1[(size_t)i * SY + ii] = v;
+            double w = s2[(size_t)i * SY + ii - 1];
+            if (ii - R / 2 >= 0) w -= F(i, ii - R / 2) * F(i, ii - R / 2);
+            if (ii + R / 2 < SY) w += F(i, ii + R / 2) * F(i, ii + R / 2);
+            s2[(size_t)i * SY + ii] = w;
+        }
+    }
+    std::vector<double> var((size_t)SX * SY);
+    for (int ii = 0; ii < SY; ++ii) {
+        double a = 0, b = 0;
+        for (int t = 0; t < R / 2 + 1; ++t) if (t < SX) { a += s1[(size_t)t * SY + ii]; b += s2[(size_t)t * SY + ii]; }
+        t1[ii] = a; t2[ii] = b;
+        for (int i = 1; i < SX; ++i) {
+            double v = t1[(size_t)(i - 1) * SY + ii];
+            if (i - R / 2 >= 0) v -= s1[(size_t)(i - R / 2) * SY + ii];
+            if (i + R / 2 < SX) v += s1[(size_t)(i + R / 2) * SY + ii];
+            t1[(size_t)i * SY + ii] = v;
+            double w = t2[(size_t)(i - 1) * SY + ii];
+            if (i - R / 2 >= 0) w -= s2[(size_t)(i - R / 2) * SY + ii];
+            if (i + R / 2 < SX) w += s2[(size_t)(i + R / 2) * SY + ii];
+            t2[(size_t)i * SY + ii] = w;
+        }
+        for (int i = 0; i < SX; ++i) {
+            double nrm = D->normImage[(size_t)i * SY + ii];
+            double mean = t1[(size_t)i * SY + ii] / nrm;
+            var[(size_t)i * SY + ii] = (t2[(size_t)i * SY + ii] / nrm) - mean * mean;
+        }
+    }
+    // correlation maps
+    int nz = D->nz;
+    std::vector<double> res((size_t)nz * SX * SY, 0.0);
+    std::vector<cplx> P((size_t)MX * MY);
+    for (int r = 0; r < nz; ++r) {
+        const std::vector<cplx>& Dz = D->dict[r];
+        for (size_t k = 0; k < P.size(); ++k)
+            P[k] = cplx(X[k].imag() * Dz[k].imag() + X[k].real() * Dz[k].real(),
+                        X[k].imag() * Dz[k].real() - X[k].real() * Dz[k].imag());
+        fft2d_rect(P, MX, MY, +1);
+        for (int ii = 0; ii < SX; ++ii)
+            for (int iii = 0; iii < SY; ++iii) {
+                int x = (ii - SX / 2 + MX / 2 + MX / 2) % MX;
+                int y = (iii - SY / 2 + MY / 2 + MY / 2) % MY;
+                double v = var[(size_t)ii * SY + iii];
+                double s = std::sqrt(D->varPSF[r] * v);
+                double o;
+                if (s > 0) o = P[(size_t)x * MY + y].real() / s;
+                else if (D->varPSF[r] <= 0) o = -1;
+                else o = -2;  // v <= 0 (or NaN product)
+                res[((size_t)r * SX + ii) * SY + iii] = o;
+            }
+    }
+    // local maxima (getVectMaxPosition, Predetection.java:480-560)
+    int dec = 3, lo = std::max(dec, R / 2);
+    std::vector<double> tmp((size_t)SX * SY, 0.0);
+    auto RC = [&](int r, int i, int j) { return res[((size_t)r * SX + i) * SY + j]; };
+    out.clear();
+    for (int r = 0; r < nz; ++r) {
+        for (int i = lo; i < SX - lo; ++i)
+            for (int j = lo; j < SY - lo; ++j)
+                if (RC(r, i, j) > 0) {
+                    double t = -INFINITY;
+                    for (int a = -dec; a <= dec; ++a) t = std::max(RC(r, i, j + a), t);
+                    tmp[(size_t)i * SY + j] = t;
+                }
+        for (int j = lo; j < SY - lo; ++j)
+            for (int i = lo; i < SX - lo; ++i) {
+                double v = RC(r, i, j);
+                if (!(v > D->thr)) continue;
+                if (v != tmp[(size_t)i * SY + j]) continue;
+                double mx = -INFINITY;
+                for (int a = -dec; a <= dec; ++a) mx = std::max(tmp[(size_t)(i + a) * SY + j], mx);
+                if (mx != v) continue;
+                double tz = 0, tx = 0, ty = 0;
+                if (r > 1 && r < nz - 1) tz = top_of_parabola(-D->zstep, RC(r - 1, i, j), 0, v, D->zstep, RC(r + 1, i, j));
+                if (i > 1 && i < SX - 1) tx = top_of_parabola(-D->p->dx, RC(r, i - 1, j), 0, v, D->p->dx, RC(r, i + 1, j));
+                if (j > 1 && j < SY - 1) ty = top_of_parabola(-D->p->dx, RC(r, i, j - 1), 0, v, D->p->dx, RC(r, i, j + 1));
+                out.push_back({v, (double)r, (double)i, (double)j, tz, tx, ty});
+            }
+    }
+    std::stable_sort(out.begin(), out.end(), [](const std::array<double, 7>& a, const std::array<double, 7>& b) { return a[0] > b[0]; });
+}
+
+}  // namespace
+
+// ================================================================ C ABI ====
+extern "C" {
+
+void* orc_psf_create(int N, double dx, double na, double lambda, double n_oil, double n_wat,
+                     double sigma, int apo, double zfocus, int kz_reset, int gauss_f32,
+                     int nz, const double* zern) {
+    return psf_build(N, dx, na, lambda, n_oil, n_wat, sigma, apo, zfocus, kz_reset, gauss_f32, nz, zern);
+}
+void orc_psf_destroy(void* h) { delete (Psf*)h; }
+int orc_psf_info(void* h, int* N, int* K) { Psf* p = (Psf*)h; *N = p->N; *K = p->K; return 0; }
+int orc_psf_tables(void* h, double* kx, double* ky, double* kz, double* kzoil, double* pupil, double* phase) {
+    Psf* p = (Psf*)h;
+    for (int k = 0; k < p->K; ++k) {
+        kx[k] = p->kx[k]; ky[k] = p->ky[k]; kz[k] = p->kz[k]; kzoil[k] = p->kzoil[k];
+        pupil[k] = p->pupil[k]; phase[k] = p->phase[k];
+    }
+    return 0;
+}
+int orc_window_size(int R, int N) { return window_size(R, N); }
+
+// n models at (x, y, z) with zoil = zfocus; out n*R*R (+ derivs n*3*R*R).
+void orc_psf_model(void* h, int R, int n, const double* xyz, double* out, double* derivs) {
+    const Psf* p = (const Psf*)h;
+    for (int i = 0; i < n; ++i)
+        psf_model(p, R, xyz[3 * i], xyz[3 * i + 1], p->zfocus, xyz[3 * i + 2], out + (size_t)i * R * R,
+                  derivs ? derivs + (size_t)i * 3 * R * R : nullptr);
+}
+
+// Explicit zoil/zwat form (calibration uses zoil = slice depth, zwat = 0).
+void orc_psf_model_oil(void* h, int R, double x, double y, double zoil, double zwat, double* out) {
+    psf_model((const Psf*)h, R, x, y, zoil, zwat, out, nullptr);
+}
+
+}
+
+static void parallel_for(int n, int threads, const std::function<void(int)>& f) {
+    if (threads <= 1) { for (int i = 0; i < n; ++i) f(i); return; }
+    std::atomic<int> next(0);
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t)
+        pool.emplace_back([&]() { for (int i; (i = next.fetch_add(1)) < n;) f(i); });
+    for (auto& th : pool) th.join();
+}
+
+extern "C" {
+
+// Reference coordinate-descent localisation (+ finite-difference CRLB) of n
+// patches.  init: n*5 (A, B, x, y, z) in the order Localization.init takes.
+// out: n*5 (x, y, z, A, B); crlb: n*3 (um); status: 1 ok, 0 photon break, -1 NaN.
+void orc_localize_cd(void* h, int R, int n, const double* patches, const double* init,
+                     double minZ, double maxZ, int iterMax, double photonThr,
+                     double* out, double* crlb, int* status, int* evals, int threads) {
+    const Psf* p = (const Psf*)h;
+    parallel_for(n, threads, [&](int i) {
+        CD cd;
+        cd.p = p; cd.R = R; cd.d = patches + (size_t)i * R * R;
+        cd.minZ = minZ; cd.maxZ = maxZ; cd.iterMax = iterMax; cd.photonThreshold = photonThr;
+        cd.maxShift = p->dx / 2.;
+        cd.psi.resize(R * R); cd.mu.resize(R * R);
+        cd.ta = init[5 * i]; cd.tb = init[5 * i + 1]; cd.tx = init[5 * i + 2]; cd.ty = init[5 * i + 3]; cd.tz = init[5 * i + 4];
+        int st = cd.run();
+        out[5 * i] = cd.tx; out[5 * i + 1] = cd.ty; out[5 * i + 2] = cd.tz; out[5 * i + 3] = cd.ta; out[5 * i + 4] = cd.tb;
+        if (crlb) fisher_crlb_fd(p, R, cd.tx, cd.ty, cd.tz, cd.ta, cd.tb, crlb + 3 * i);
+        status[i] = st;
+        if (evals) evals[i] = cd.nevals;
+    });
+}
+
+// FP64 LM fit of n patches.  init/out: n*5 (x, y, z, A, B).  params:
+// zmin, zmax, xymax, tol_xyz, step_xy, step_z; max_iter evaluations.
+void orc_fit_lm(void* h, int R, int n, const double* patches, const double* init, const double* params,
+                int max_iter, double* out, double* nll, int* status, int* evals, double* crlb5, int threads) {
+    const Psf* p = (const Psf*)h;
+    LMParams P{params[0], params[1], params[2], max_iter, params[3], params[4], params[5]};
+    parallel_for(n, threads, [&](int i) {
+        status[i] = lm_fit(p, R, patches + (size_t)i * R * R, init + 5 * i, P, out + 5 * i, nll + i,
+                           evals + i, crlb5 ? crlb5 + 5 * i : nullptr);
+    });
+}
+
+// Deviance-form NLL and its analytic gradient / Gauss-Newton Hessian at theta.
+double orc_nll_grad(void* h, int R, const double* patch, const double* th, double* g, double* H25) {
+    const Psf* p = (const Psf*)h;
+    std::vector<double> psi(R * R), dpsi(3 * R * R);
+    double H[5][5];
+    double v = model_eval(p, R, patch, th, g, H, psi, dpsi);
+    for (int q = 0; q < 5; ++q) for (int r = 0; r < 5; ++r) H25[5 * q + r] = H[q][r];
+    return v;
+}
+
+void orc_crlb_fd(void* h, int R, const double* th, double* crlb3) {
+    const Psf* p = (const Psf*)h;
+    fisher_crlb_fd(p, R, th[0], th[1], th[2], th[3], th[4], crlb3);
+}
+
+void* orc_det_create(void* h, int SX, int SY, int R, double minZ, double maxZ, double step, double thr) {
+    return det_build((const Psf*)h, SX, SY, R, minZ, maxZ, step, thr);
+}
+void orc_det_destroy(void* d) { delete (Detector*)d; }
+int orc_det_nslices(void* d) { return ((Detector*)d)->nz; }
+void orc_det_library(void* d, double* range, double* psfs) {
+    Detector* D = (Detector*)d;
+    for (int i = 0; i < D->nz; ++i) {
+        range[i] = D->range[i];
+        std::memcpy(psfs + (size_t)i * D->R * D->R, D->libpsf[i].data(), sizeof(double) * D->R * D->R);
+    }
+}
+// Detect on nframes frames [f][X][Y]; out rows of 7 doubles, capacity cap per
+// frame; counts[f] = number of candidates (may exceed cap: then truncated).
+void orc_detect(void* d, int nframes, const double* frames, int cap, double* out, int* counts, int threads) {
+    Detector* D = (Detector*)d;
+    parallel_for(nframes, threads, [&](int f) {
+        std::vector<std::array<double, 7>> rows;
+        det_frame(D, frames + (size_t)f * D->SX * D->SY, rows);
+        counts[f] = (int)rows.size();
+        for (int k = 0; k < (int)rows.size() && k < cap; ++k)
+            for (int c = 0; c < 7; ++c) out[((size_t)f * cap + k) * 7 + c] = rows[k][c];
+    });
+}
+
+// Calibration stack NLL (ZernikePhaseRetrieval.java:1843-1874) for one bead:
+// slices s at zoil = dz[s] + bz, zwat = 0; mu = A*psi + B clamped at 1e-8;
+// NLL = sum mu - d ln mu.  Registration x/y/z enter as the kx, ky, kz_oil
+// phase modes (ZernikePhaseRetrieval.java:93-95), i.e. as the coordinates.
+double orc_calib_nll(void* h, int R, int nslice, const double* dz, const double* stack,
+                     double bx, double by, double bz, double A, double B) {
+    const Psf* p = (const Psf*)h;
+    std::vector<double> psi(R * R);
+    double nll = 0;
+    for (int s = 0; s < nslice; ++s) {
+        psf_model(p, R, bx, by, dz[s] + bz, 0.0, psi.data(), nullptr);
+        for (int k = 0; k < R * R; ++k) {
+            double mu = psi[k] * A + B;
+            if (mu <= 0) mu = 0.00000001;
+            nll += mu - stack[(size_t)s * R * R + k] * std::log(mu);
+        }
+    }
+    return nll;
+}
+
+}  // extern "C"

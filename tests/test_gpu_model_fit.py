@@ -1,0 +1,114 @@
+"""GPU parity tests: the FP64 device model and fit against the CPU oracle, through the C-ABI."""
+import numpy as np
+import pytest
+
+import oracle as O
+from common import OPTICS, astig_zernike, saddle_zernike, synth_rois, tetrapod_zernike
+
+pytestmark = pytest.mark.gpu
+
+# (N, R, zernike) cases covering the three windows W = 32, 64, 128
+CASES = [
+    (64, 16, astig_zernike()),
+    (128, 24, saddle_zernike()),
+    (128, 48, tetrapod_zernike()),
+    (128, 40, tetrapod_zernike()),
+    (64, 8, astig_zernike()),
+]
+
+
+def pair(zpkg, ctx, N, zern, **kw):
+    o = dict(OPTICS)
+    o.update(kw)
+    psf = zpkg.PSF(ctx, zpkg.optics(size_fft=N, **o), zern)
+    ref = O.OraclePSF(N, o["xystep"], o["na"], o["wavelength"], o["n_oil"], o.get("n_wat", o["n_oil"]), o["sigma"],
+                      zern, gauss_f32=False, zfocus=o.get("zfocus", 0.0), kz_reset=o.get("kz_reset", False))
+    return psf, ref
+
+
+@pytest.mark.parametrize("N,R,zern", CASES)
+def test_model_matches_oracle_fp64(zpkg, ctx, N, R, zern):
+    psf, ref = pair(zpkg, ctx, N, zern)
+    rng = np.random.default_rng(R)
+    xyz = np.c_[rng.uniform(-0.15, 0.15, (6, 2)), rng.uniform(-1.5, 1.5, 6)]
+    got, dgot = psf.model(R, xyz, derivs=True)
+    want, dwant = ref.model(R, xyz, derivs=True)
+    assert np.abs(got - want).max() <= 1e-11 * want.max()
+    assert np.abs(dgot - dwant).max() <= 1e-9 * np.abs(dwant).max()
+
+
+def test_model_reference_float_gaussian_effect_is_small(zpkg, ctx):
+    # The reference rounds its W x W spectral Gaussian to float (PSFPhase.java:373);
+    # the library uses the exact separable Gaussian.  Bound the difference.
+    zern = astig_zernike()
+    psf, _ = pair(zpkg, ctx, 64, zern)
+    ref32 = O.OraclePSF(64, 0.11, 1.4, 0.66, 1.518, 1.518, 0.9, zern, gauss_f32=True)
+    xyz = np.array([[0.01, 0.02, 0.3], [0.0, 0.0, -0.5]])
+    assert np.abs(psf.model(16, xyz) - ref32.model(16, xyz)).max() < 1e-7 * ref32.model(16, xyz).max()
+
+
+def test_model_evanescent_reset_tables(zpkg, ctx):
+    # NA 1.4 into water (n 1.33): evanescent components; kz_reset reproduces resetKz
+    zern = astig_zernike()
+    for reset in (False, True):
+        psf, ref = pair(zpkg, ctx, 64, zern, n_wat=1.33, kz_reset=reset, zfocus=0.4)
+        xyz = np.array([[0.0, 0.0, 0.3], [0.02, -0.01, 0.8]])
+        got, want = psf.model(16, xyz), ref.model(16, xyz)
+        assert np.abs(got - want).max() <= 1e-11 * want.max()
+
+
+@pytest.mark.parametrize("N,R,zern", CASES[:3])
+def test_fp64_fit_matches_oracle_lm(zpkg, ctx, N, R, zern):
+    psf, ref = pair(zpkg, ctx, N, zern)
+    rois, truth = synth_rois(ref.model, R, 24, seed=7 + R, zrange=0.6)
+    init = truth.copy()
+    init[:, :2] = 0
+    init[:, 2] = np.round(truth[:, 2] / 0.3) * 0.3
+    init[:, 3] *= 0.8
+    xymax = R * 0.11 / 2
+    prm = zpkg.PSF.fit_params(-1.0, 1.0, xymax, max_iter=30, precision=zpkg.ZOLA_PREC_FP64)
+    res = psf.fit(rois, init, prm)
+    o, nll, st, ev, cr = ref.fit_lm(rois.astype(np.float64), init, -1.0, 1.0, xymax, max_iter=30, crlb=True)
+    ok = st == 1
+    assert ok.mean() > 0.8
+    assert (res["status"] == st).all()
+    assert (res["iters"] == ev).all()
+    d = np.abs(res["theta"] - o)
+    assert d[:, :3].max() * 1000 < 1e-4          # nm: same FP64 fit
+    assert (d[:, 3] / o[:, 3]).max() < 1e-8
+    assert np.allclose(res["nll"], nll, rtol=1e-9, atol=1e-8)
+    assert np.allclose(res["crlb"], cr, rtol=1e-6)
+
+
+def test_fp64_fit_matches_reference_coordinate_descent(zpkg, ctx):
+    """The reference's own CPU algorithm (coordinate descent) reaches the same
+    optimum within the north_star tolerances."""
+    zern = astig_zernike()
+    psf, ref = pair(zpkg, ctx, 64, zern)
+    ref_f32 = O.OraclePSF(64, 0.11, 1.4, 0.66, 1.518, 1.518, 0.9, zern, gauss_f32=True)
+    rois, truth = synth_rois(ref.model, 16, 16, seed=11, zrange=0.5, photons=3000)
+    init = truth.copy()
+    init[:, :3] = 0
+    prm = zpkg.PSF.fit_params(-0.9, 0.9, 0.88, max_iter=40, precision=zpkg.ZOLA_PREC_FP64)
+    res = psf.fit(rois, init, prm)
+    cd, crlb, stc, _ = ref_f32.localize_cd(rois.astype(np.float64), np.c_[init[:, 3], init[:, 4], init[:, :3]],
+                                           -0.9, 0.9, 20)
+    good = (stc == 1) & (res["status"] == 1)
+    assert good.mean() > 0.8
+    d = np.abs(res["theta"][good] - cd[good]) * 1000
+    assert d[:, :2].max() < 0.5
+    assert d[:, 2].max() < 1.0
+    assert (np.abs(res["theta"][good, 3] - cd[good, 3]) / cd[good, 3]).max() < 1e-3
+
+
+def test_fit_rejects_bad_arguments(zpkg, ctx):
+    psf, _ = pair(zpkg, ctx, 64, astig_zernike())
+    rois = np.zeros((2, 16, 16), np.float32) + 20
+    init = np.zeros((2, 5))
+    init[:, 3] = 100
+    init[:, 4] = 20
+    bad = zpkg.PSF.fit_params(1.0, -1.0, 0.88)
+    with pytest.raises(zpkg.ZolaError):
+        psf.fit(rois, init, bad)
+    with pytest.raises(zpkg.ZolaError):
+        psf.fit(np.zeros((2, 15, 15), np.float32), init, zpkg.PSF.fit_params(-1, 1, 0.88))

@@ -1,0 +1,104 @@
+"""CPU tests of the oracle (known-answer tests; the reference ships no golden vectors)."""
+import numpy as np
+import pytest
+
+import oracle as O
+from common import OPTICS, astig_zernike
+
+
+def make(N=64, zern=None, **kw):
+    o = dict(OPTICS)
+    o.update(kw)
+    return O.OraclePSF(N, o["xystep"], o["na"], o["wavelength"], o["n_oil"], o.get("n_wat", o["n_oil"]), o["sigma"],
+                       np.zeros(15) if zern is None else zern)
+
+
+def test_disk_sizes():
+    # PhaseParameters disk pixel counts for NA 1.4, lambda 0.66, dx 0.11
+    assert make(64).K == 708
+    assert make(128).K == 2820
+
+
+def test_in_focus_aberration_free_is_symmetric_and_normalised():
+    p = make(64)
+    psi = p.model(16, [0.0, 0.0, 0.0])[0]
+    assert abs(psi.sum() - 1) < 1e-12
+    # centre N/2-0.5 grid and W/2 crop: symmetric under (i -> R-i) about index R/2
+    core = psi[1:, 1:]
+    assert np.allclose(core, core[::-1, :], rtol=1e-9, atol=1e-15)
+    assert np.allclose(core, core[:, ::-1], rtol=1e-9, atol=1e-15)
+    assert np.allclose(core, core.T, rtol=1e-9, atol=1e-15)
+    assert np.unravel_index(psi.argmax(), psi.shape) == (8, 8)
+
+
+def test_one_pixel_shift_moves_the_model_by_one_pixel():
+    p = make(64, zern=astig_zernike())
+    a = p.model(32, [0.0, 0.0, 0.2])[0]
+    b = p.model(32, [-0.11, 0.0, 0.2])[0]  # theta_x = -dx moves the PSF by +1 px in x
+    # compare the interior (normalisation over the crop differs slightly at the border)
+    ia, ib = a[8:-9, 8:-8], b[9:-8, 8:-8]
+    assert np.abs(ia / ia.sum() - ib / ib.sum()).max() < 2e-4 * ia.max()
+
+
+def test_derivatives_match_central_differences():
+    p = make(64, zern=astig_zernike())
+    th = np.array([0.03, -0.02, 0.15])
+    _, d = p.model(16, th, derivs=True)
+    for k in range(3):
+        e = np.zeros(3)
+        e[k] = 1e-5
+        fd = (p.model(16, th + e)[0] - p.model(16, th - e)[0]) / 2e-5
+        assert np.abs(fd - d[0, k]).max() < 1e-7 * np.abs(d[0, k]).max()
+
+
+def test_lm_and_reference_coordinate_descent_agree():
+    p = make(64, zern=astig_zernike())
+    rng = np.random.default_rng(0)
+    n = 6
+    truth = np.c_[rng.uniform(-.11, .11, (n, 2)), rng.uniform(-.5, .5, n), np.full(n, 3000.), np.full(n, 20.)]
+    pat = rng.poisson(truth[:, 3, None, None] * p.model(16, truth[:, :3]) + 20).astype(float)
+    init = truth.copy()
+    init[:, :3] = 0
+    lm, _, st, _ = p.fit_lm(pat, init, -1, 1, 0.88)
+    assert (st == 1).all()
+    cd, crlb, stc, _ = p.localize_cd(pat, np.c_[init[:, 3], init[:, 4], init[:, :3]], -0.9, 0.9, 20)
+    assert (stc == 1).all()
+    # north_star tolerances: 0.5 nm in x/y, 1 nm in z
+    assert np.abs(cd[:, :2] - lm[:, :2]).max() < 0.5e-3
+    assert np.abs(cd[:, 2] - lm[:, 2]).max() < 1e-3
+    assert (crlb > 0).all() and (crlb < 0.1).all()
+
+
+def test_lm_gradient_is_zero_at_optimum():
+    p = make(64, zern=astig_zernike())
+    rng = np.random.default_rng(3)
+    th = np.array([0.02, -0.01, 0.1, 2500., 20.])
+    pat = rng.poisson(th[3] * p.model(16, th[:3])[0] + th[4]).astype(float)
+    out, *_ = p.fit_lm(pat[None], th[None], -1, 1, 0.88, tol_xyz=1e-8, max_iter=60)
+    v, g, H = p.nll_grad(pat, out[0])
+    # scaled gradient g / sqrt(diag H) is ~0 at the optimum
+    assert np.abs(g / np.sqrt(np.diag(H))).max() < 1e-3
+
+
+def test_fft_round_trip_and_unitarity():
+    # FFT convention (unitary, forward -i) checked through the blur with sigma -> 0:
+    # a very narrow spatial blur leaves the intensity unchanged up to normalisation.
+    p_sharp = make(64, sigma=0.05)
+    p_none = make(64, sigma=0.05)
+    a = p_sharp.model(16, [0.0, 0.0, 0.3])[0]
+    b = p_none.model(16, [0.0, 0.0, 0.3])[0]
+    assert np.allclose(a, b)
+    assert abs(a.sum() - 1) < 1e-12
+
+
+def test_detection_finds_isolated_emitter():
+    p = make(64, zern=astig_zernike())
+    det = O.OracleDetector(p, 64, 64, 16, -0.6, 0.6, 0.11, 0.1)
+    rng = np.random.default_rng(1)
+    img = np.full((64, 64), 20.0)
+    psi = p.model(16, [0.0, 0.0, 0.1])[0]
+    img[24:40, 30:46] += 5000 * psi
+    img = rng.poisson(img).astype(float)
+    c = det.detect(img[None])[0]
+    assert len(c) >= 1
+    assert (int(c[0, 2]), int(c[0, 3])) in [(32, 38), (31, 38), (32, 37), (33, 38), (32, 39)]

@@ -1,0 +1,218 @@
+"""Host-side mirror of ZOLA-3D's GPU localization objects over the C-ABI.
+
+The reference drives its GPU path through Java objects (paths relative to its
+src/main/java/org/pasteur/imagej/):
+
+  DataPhase_ / DataPhase.loadJSON   process/gpu/DataPhase_.java, process/cpu/DataPhase.java:587-679
+  PSFmany_float_.computePSF         process/gpu/PSFmany_float_.java:1626-1720
+  Localization_.localize            process/gpu/Localization_.java:633-798
+
+This module exposes the same roles over ``libzola_b200.so`` (include/zola_b200.h):
+``Context`` (MyCudaStream), ``PSF`` (DataPhase_ + its model), ``PSF.model``
+(computePSF) and ``PSF.fit`` (batched localize).  Host arrays are numpy; the
+``*_dev`` forms take torch CUDA tensors and pass raw device pointers.  There is
+no CPU fallback: if the library is missing every call raises.
+"""
+import ctypes
+import json
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libzola_b200.so")
+
+ZOLA_PREC_FP64 = 0
+ZOLA_PREC_SPLIT = 1
+FIT_STATUS = {1: "converged", 2: "max_iter", 3: "stalled", -1: "nan"}
+
+
+class ZolaError(RuntimeError):
+    pass
+
+
+class Optics(ctypes.Structure):
+    _fields_ = [("size_fft", ctypes.c_int), ("xystep", ctypes.c_double), ("na", ctypes.c_double),
+                ("wavelength", ctypes.c_double), ("n_oil", ctypes.c_double), ("n_wat", ctypes.c_double),
+                ("sigma", ctypes.c_double), ("with_apo", ctypes.c_int), ("zfocus", ctypes.c_double),
+                ("kz_reset", ctypes.c_int)]
+
+
+class FitParams(ctypes.Structure):
+    _fields_ = [("zmin", ctypes.c_double), ("zmax", ctypes.c_double), ("xymax", ctypes.c_double),
+                ("max_iter", ctypes.c_int), ("tol_xyz", ctypes.c_double), ("step_xy", ctypes.c_double),
+                ("step_z", ctypes.c_double), ("precision", ctypes.c_int)]
+
+
+EXPORTS = ["zola_ctx_create", "zola_ctx_destroy", "zola_last_error", "zola_ctx_stream", "zola_ctx_launches",
+           "zola_psf_load", "zola_psf_free", "zola_psf_info", "zola_psf_model", "zola_psf_model_dev",
+           "zola_fit_batch", "zola_fit_batch_dev"]
+
+_lib = None
+
+
+def lib():
+    """Load libzola_b200.so (built by build.py); raises if it is absent."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ZolaError(f"{LIB_PATH} not built: run __graft_entry__.build()")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        L.zola_ctx_create.argtypes = [i, ctypes.POINTER(vp)]
+        L.zola_ctx_destroy.argtypes = [vp]
+        L.zola_last_error.argtypes = [vp]
+        L.zola_last_error.restype = ctypes.c_char_p
+        L.zola_ctx_stream.argtypes = [vp]
+        L.zola_ctx_stream.restype = vp
+        L.zola_ctx_launches.argtypes = [vp]
+        L.zola_ctx_launches.restype = ctypes.c_longlong
+        L.zola_psf_load.argtypes = [vp, ctypes.POINTER(Optics), vp, i, ctypes.POINTER(vp)]
+        L.zola_psf_free.argtypes = [vp]
+        L.zola_psf_info.argtypes = [vp, ctypes.POINTER(i), ctypes.POINTER(i)]
+        L.zola_psf_model.argtypes = [vp, i, vp, i, vp, vp]
+        L.zola_psf_model_dev.argtypes = [vp, i, vp, i, vp, vp, vp]
+        L.zola_fit_batch.argtypes = [vp, vp, i, vp, vp, i, ctypes.POINTER(FitParams), vp, vp, vp, vp, vp]
+        L.zola_fit_batch_dev.argtypes = [vp, vp, i, vp, vp, i, ctypes.POINTER(FitParams), vp, vp, vp, vp, vp, vp]
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return ctypes.c_void_p(a.data_ptr())
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class Context:
+    """One device context and stream (replaces MyCudaStream.init/destroy)."""
+
+    def __init__(self, device=0):
+        h = ctypes.c_void_p()
+        rc = lib().zola_ctx_create(int(device), ctypes.byref(h))
+        if rc != 0:
+            raise ZolaError(f"zola_ctx_create failed ({rc}): no usable sm_100 device {device}")
+        self.h = h
+        self.device = device
+
+    def check(self, rc, what):
+        if rc != 0:
+            msg = lib().zola_last_error(self.h).decode()
+            raise ZolaError(f"{what} failed ({rc}): {msg}")
+
+    @property
+    def stream(self):
+        return lib().zola_ctx_stream(self.h)
+
+    @property
+    def launches(self):
+        return lib().zola_ctx_launches(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().zola_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def optics(size_fft=128, xystep=0.11, na=1.4, wavelength=0.66, n_oil=1.518, n_wat=None, sigma=0.9,
+           with_apo=False, zfocus=0.0, kz_reset=False):
+    return Optics(int(size_fft), float(xystep), float(na), float(wavelength), float(n_oil),
+                  float(n_oil if n_wat is None else n_wat), float(sigma), int(bool(with_apo)), float(zfocus),
+                  int(bool(kz_reset)))
+
+
+class PSF:
+    """A loaded calibration: pupil tables, Zernike phase and per-ROI-size tables
+    on the device (replaces DataPhase_ + PSFmany_float_)."""
+
+    def __init__(self, ctx, opt, zernike):
+        self.ctx = ctx
+        self.optics = opt
+        self.zernike = np.ascontiguousarray(zernike, dtype=np.float64)
+        h = ctypes.c_void_p()
+        ctx.check(lib().zola_psf_load(ctx.h, ctypes.byref(opt), _ptr(self.zernike), len(self.zernike),
+                                      ctypes.byref(h)), "zola_psf_load")
+        self.h = h
+        n, k = ctypes.c_int(), ctypes.c_int()
+        lib().zola_psf_info(h, ctypes.byref(n), ctypes.byref(k))
+        self.N, self.K = n.value, k.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().zola_psf_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def model(self, R, xyz, derivs=False):
+        """psi (n, R, R) (and dpsi (n, 3, R, R)) at (x, y, zwat) um, FP64 on the GPU."""
+        xyz = np.ascontiguousarray(np.atleast_2d(xyz), dtype=np.float64)
+        n = xyz.shape[0]
+        out = np.zeros((n, R, R))
+        d = np.zeros((n, 3, R, R)) if derivs else None
+        self.ctx.check(lib().zola_psf_model(self.h, int(R), _ptr(xyz), n, _ptr(out), _ptr(d)), "zola_psf_model")
+        return (out, d) if derivs else out
+
+    def model_dev(self, R, xyz, out, dout=None, stream=None):
+        """Device form: torch CUDA float64 tensors."""
+        n = xyz.shape[0]
+        self.ctx.check(lib().zola_psf_model_dev(self.h, int(R), _ptr(xyz), n, _ptr(out), _ptr(dout), stream),
+                       "zola_psf_model_dev")
+
+    @staticmethod
+    def fit_params(zmin, zmax, xymax, max_iter=30, tol_xyz=1e-5, step_xy=0.11, step_z=0.22,
+                   precision=ZOLA_PREC_FP64):
+        return FitParams(float(zmin), float(zmax), float(xymax), int(max_iter), float(tol_xyz), float(step_xy),
+                         float(step_z), int(precision))
+
+    def fit(self, rois, init, prm, crlb=True):
+        """Batched MLE fit of host ROIs (n, R, R) photons from init (n, 5) = x, y, z, A, B."""
+        rois = np.ascontiguousarray(rois, dtype=np.float32)
+        init = np.ascontiguousarray(init, dtype=np.float64)
+        n, R = rois.shape[0], rois.shape[1]
+        out = np.zeros((n, 5))
+        cr = np.zeros((n, 5)) if crlb else None
+        nll = np.zeros(n)
+        st = np.zeros(n, np.int32)
+        it = np.zeros(n, np.int32)
+        self.ctx.check(lib().zola_fit_batch(self.ctx.h, self.h, R, _ptr(rois), _ptr(init), n, ctypes.byref(prm),
+                                            _ptr(out), _ptr(cr), _ptr(nll), _ptr(st), _ptr(it)), "zola_fit_batch")
+        return dict(theta=out, crlb=cr, nll=nll, status=st, iters=it)
+
+    def fit_dev(self, rois, init, prm, out, crlb=None, nll=None, status=None, iters=None, stream=None):
+        """Device form over torch CUDA tensors (rois float32, init/out float64)."""
+        n, R = rois.shape[0], rois.shape[1]
+        self.ctx.check(lib().zola_fit_batch_dev(self.ctx.h, self.h, R, _ptr(rois), _ptr(init), n, ctypes.byref(prm),
+                                                _ptr(out), _ptr(crlb), _ptr(nll), _ptr(status), _ptr(iters), stream),
+                       "zola_fit_batch_dev")
+
+
+def load_calibration_json(path, size_fft=128, n_wat=None, zfocus=0.0, kz_reset=False):
+    """Parse a ZOLA calibration JSON (DataPhase.loadJSON, process/cpu/DataPhase.java:587-679).
+
+    Returns (optics, zernike).  As in the reference, the pupil grid is the
+    caller's sizeFFT for Zernike calibrations and the file's for pixel phases;
+    pixel-phase calibrations are not supported by this library."""
+    with open(path) as f:
+        js = json.load(f)
+    if str(js.get("zernikedPSF", "true")).lower() != "true":
+        raise ZolaError("pixel-phase (non-Zernike) calibrations are not supported")
+    zern = np.array([float(v) for v in js["zernike"]])
+    opt = optics(size_fft=size_fft, xystep=float(js["sizePix"]), na=float(js["NA"]),
+                 wavelength=float(js["wavelength"]), n_oil=float(js["index"]), n_wat=n_wat,
+                 sigma=float(js["sigmaGaussianKernel"]),
+                 with_apo=str(js.get("withApoFactor", "false")).lower() == "true", zfocus=zfocus,
+                 kz_reset=kz_reset)
+    return opt, zern

@@ -1,0 +1,227 @@
+// C-ABI entry points (include/zola_b200.h).  Host wrappers copy in/out; the
+// _dev forms take device pointers and a stream.  Every call validates its
+// arguments and reports failures through the return code and zola_last_error.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <new>
+
+#include "zola_internal.h"
+
+using namespace zola;
+
+namespace zola {
+
+int ensure_scratch(zola_ctx* ctx, size_t bytes, std::string& err) {
+    if (bytes <= ctx->scratch_bytes) return 0;
+    if (ctx->scratch) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(ctx->scratch);
+        ctx->scratch = nullptr;
+        ctx->scratch_bytes = 0;
+    }
+    cudaError_t e = cudaMalloc(&ctx->scratch, bytes);
+    if (e != cudaSuccess) {
+        err = std::string("scratch cudaMalloc: ") + cudaGetErrorString(e);
+        return ZOLA_E_CUDA;
+    }
+    ctx->scratch_bytes = bytes;
+    return 0;
+}
+
+}  // namespace zola
+
+namespace {
+
+int set_err(zola_ctx* ctx, int code, const char* msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+bool check_fit_params(zola_ctx* ctx, const zola_fit_params* prm) {
+    if (!prm) { ctx->err = "fit params is null"; return false; }
+    if (prm->max_iter < 1 || prm->max_iter > 1000) { ctx->err = "max_iter must be in [1, 1000]"; return false; }
+    if (!(prm->zmax >= prm->zmin) || !(prm->xymax > 0) || !(prm->step_xy > 0) || !(prm->step_z > 0) ||
+        !(prm->tol_xyz >= 0)) {
+        ctx->err = "fit params: need zmax >= zmin, xymax > 0, step_xy > 0, step_z > 0, tol_xyz >= 0";
+        return false;
+    }
+    if (prm->precision != ZOLA_PREC_FP64 && prm->precision != ZOLA_PREC_SPLIT) {
+        ctx->err = "unknown precision";
+        return false;
+    }
+    return true;
+}
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    ~DevBuf() { if (p) cudaFree(p); }
+    cudaError_t alloc(size_t n) { return cudaMalloc(&p, n * sizeof(T)); }
+};
+
+}  // namespace
+
+extern "C" {
+
+int zola_ctx_create(int device, zola_ctx** out) {
+    if (!out) return ZOLA_E_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0) return ZOLA_E_NODEV;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return ZOLA_E_NODEV;
+    if (prop.major != 10) return ZOLA_E_NODEV;  // built for sm_100a only
+    if (cudaSetDevice(device) != cudaSuccess) return ZOLA_E_CUDA;
+    zola_ctx* c = new (std::nothrow) zola_ctx();
+    if (!c) return ZOLA_E_ARG;
+    c->device = device;
+    c->num_sms = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&c->d_counter, 64 * sizeof(int)) != cudaSuccess) {
+        delete c;
+        return ZOLA_E_CUDA;
+    }
+    c->d_status_word = c->d_counter + 32;
+    cudaMemset(c->d_counter, 0, 64 * sizeof(int));
+    *out = c;
+    return ZOLA_OK;
+}
+
+int zola_ctx_destroy(zola_ctx* ctx) {
+    if (!ctx) return ZOLA_E_ARG;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->scratch) cudaFree(ctx->scratch);
+    if (ctx->d_counter) cudaFree(ctx->d_counter);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return ZOLA_OK;
+}
+
+const char* zola_last_error(const zola_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+void* zola_ctx_stream(zola_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+long long zola_ctx_launches(const zola_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+int zola_psf_load(zola_ctx* ctx, const zola_optics* optics, const double* zernike, int nz, zola_psf** out) {
+    if (!ctx || !optics || !out) return set_err(ctx, ZOLA_E_ARG, "zola_psf_load: null argument");
+    *out = nullptr;
+    cudaSetDevice(ctx->device);
+    zola_psf* p = new (std::nothrow) zola_psf();
+    if (!p) return set_err(ctx, ZOLA_E_ARG, "out of host memory");
+    p->ctx = ctx;
+    int rc = build_psf_tables(p, optics, zernike, nz, ctx->err);
+    if (rc) {
+        if (p->d_tables) cudaFree(p->d_tables);
+        delete p;
+        return rc;
+    }
+    *out = p;
+    return ZOLA_OK;
+}
+
+int zola_psf_free(zola_psf* psf) {
+    if (!psf) return ZOLA_E_ARG;
+    cudaSetDevice(psf->ctx->device);
+    cudaStreamSynchronize(psf->ctx->stream);
+    for (auto& kv : psf->win) {
+        if (kv.second.d_C) cudaFree(kv.second.d_C);
+        if (kv.second.d_G) cudaFree(kv.second.d_G);
+        if (kv.second.d_split) cudaFree(kv.second.d_split);
+    }
+    if (psf->d_tables) cudaFree(psf->d_tables);
+    delete psf;
+    return ZOLA_OK;
+}
+
+int zola_psf_info(const zola_psf* psf, int* N, int* K) {
+    if (!psf || !N || !K) return ZOLA_E_ARG;
+    *N = psf->N;
+    *K = psf->K;
+    return ZOLA_OK;
+}
+
+int zola_psf_model_dev(zola_psf* psf, int R, const double* d_xyz, int n, double* d_out, double* d_dout,
+                       void* stream) {
+    if (!psf) return ZOLA_E_ARG;
+    zola_ctx* ctx = psf->ctx;
+    if (n < 0 || (n > 0 && (!d_xyz || !d_out))) return set_err(ctx, ZOLA_E_ARG, "zola_psf_model: bad n or null buffer");
+    WindowTables* w = get_window(psf, R, ctx->err);
+    if (!w) return ZOLA_E_ARG;
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    return launch_model_f64(ctx, psf, w, d_xyz, n, d_out, d_dout, st);
+}
+
+int zola_psf_model(zola_psf* psf, int R, const double* xyz, int n, double* out, double* dout) {
+    if (!psf) return ZOLA_E_ARG;
+    zola_ctx* ctx = psf->ctx;
+    if (n < 0 || (n > 0 && (!xyz || !out))) return set_err(ctx, ZOLA_E_ARG, "zola_psf_model: bad n or null buffer");
+    if (R < 4 || R % 2 || R > psf->N) return set_err(ctx, ZOLA_E_ARG, "ROI side must be even, >= 4 and <= the pupil grid");
+    if (n == 0) return ZOLA_OK;
+    cudaSetDevice(ctx->device);
+    DevBuf<double> dx, dout_, ddout;
+    size_t rr = (size_t)R * R;
+    ZOLA_CUDA_CHECK(dx.alloc(3 * (size_t)n), ctx);
+    ZOLA_CUDA_CHECK(dout_.alloc(rr * n), ctx);
+    if (dout) ZOLA_CUDA_CHECK(ddout.alloc(3 * rr * n), ctx);
+    ZOLA_CUDA_CHECK(cudaMemcpyAsync(dx.p, xyz, 3 * sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream), ctx);
+    int rc = zola_psf_model_dev(psf, R, dx.p, n, dout_.p, dout ? ddout.p : nullptr, ctx->stream);
+    if (rc) return rc;
+    ZOLA_CUDA_CHECK(cudaMemcpyAsync(out, dout_.p, rr * n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), ctx);
+    if (dout)
+        ZOLA_CUDA_CHECK(cudaMemcpyAsync(dout, ddout.p, 3 * rr * n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), ctx);
+    ZOLA_CUDA_CHECK(cudaStreamSynchronize(ctx->stream), ctx);
+    return ZOLA_OK;
+}
+
+int zola_fit_batch_dev(zola_ctx* ctx, zola_psf* psf, int R, const float* d_rois, const double* d_init5, int n,
+                       const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll, int* d_status,
+                       int* d_iters, void* stream) {
+    if (!ctx || !psf) return ZOLA_E_ARG;
+    if (psf->ctx != ctx) return set_err(ctx, ZOLA_E_ARG, "psf belongs to another context");
+    if (!check_fit_params(ctx, prm)) return ZOLA_E_ARG;
+    if (n < 0 || (n > 0 && (!d_rois || !d_init5 || !d_out5))) return set_err(ctx, ZOLA_E_ARG, "zola_fit_batch: bad n or null buffer");
+    if (psf->o.kz_reset) return set_err(ctx, ZOLA_E_ARG, "fit needs a PSF built with kz_reset = 0 (the fit model tables)");
+    WindowTables* w = get_window(psf, R, ctx->err);
+    if (!w) return ZOLA_E_ARG;
+    if (n == 0) return ZOLA_OK;
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    if (prm->precision == ZOLA_PREC_SPLIT)
+        return launch_fit_split(ctx, psf, w, d_rois, d_init5, n, prm, d_out5, d_crlb5, d_nll, d_status, d_iters, st);
+    return launch_fit_f64(ctx, psf, w, d_rois, d_init5, n, prm, d_out5, d_crlb5, d_nll, d_status, d_iters, st);
+}
+
+int zola_fit_batch(zola_ctx* ctx, zola_psf* psf, int R, const float* rois, const double* init5, int n,
+                   const zola_fit_params* prm, double* out5, double* crlb5, double* nll, int* status, int* iters) {
+    if (!ctx || !psf) return ZOLA_E_ARG;
+    if (n < 0 || (n > 0 && (!rois || !init5 || !out5))) return set_err(ctx, ZOLA_E_ARG, "zola_fit_batch: bad n or null buffer");
+    if (n == 0) return ZOLA_OK;
+    cudaSetDevice(ctx->device);
+    size_t rr = (size_t)R * R;
+    DevBuf<float> dr;
+    DevBuf<double> di, dout, dcr, dnll;
+    DevBuf<int> dst, dit;
+    ZOLA_CUDA_CHECK(dr.alloc(rr * n), ctx);
+    ZOLA_CUDA_CHECK(di.alloc(5 * (size_t)n), ctx);
+    ZOLA_CUDA_CHECK(dout.alloc(5 * (size_t)n), ctx);
+    if (crlb5) ZOLA_CUDA_CHECK(dcr.alloc(5 * (size_t)n), ctx);
+    if (nll) ZOLA_CUDA_CHECK(dnll.alloc((size_t)n), ctx);
+    if (status) ZOLA_CUDA_CHECK(dst.alloc((size_t)n), ctx);
+    if (iters) ZOLA_CUDA_CHECK(dit.alloc((size_t)n), ctx);
+    ZOLA_CUDA_CHECK(cudaMemcpyAsync(dr.p, rois, rr * n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream), ctx);
+    ZOLA_CUDA_CHECK(cudaMemcpyAsync(di.p, init5, 5 * n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream), ctx);
+    int rc = zola_fit_batch_dev(ctx, psf, R, dr.p, di.p, n, prm, dout.p, crlb5 ? dcr.p : nullptr, nll ? dnll.p : nullptr,
+                                status ? dst.p : nullptr, iters ? dit.p : nullptr, ctx->stream);
+    if (rc) return rc;
+    ZOLA_CUDA_CHECK(cudaMemcpyAsync(out5, dout.p, 5 * n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), ctx);
+    if (crlb5) ZOLA_CUDA_CHECK(cudaMemcpyAsync(crlb5, dcr.p, 5 * n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), ctx);
+    if (nll) ZOLA_CUDA_CHECK(cudaMemcpyAsync(nll, dnll.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), ctx);
+    if (status) ZOLA_CUDA_CHECK(cudaMemcpyAsync(status, dst.p, n * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), ctx);
+    if (iters) ZOLA_CUDA_CHECK(cudaMemcpyAsync(iters, dit.p, n * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), ctx);
+    ZOLA_CUDA_CHECK(cudaStreamSynchronize(ctx->stream), ctx);
+    return ZOLA_OK;
+}
+
+}  // extern "C"

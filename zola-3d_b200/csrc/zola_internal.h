@@ -1,0 +1,116 @@
+// Internal types shared by the host set-up, the kernels and the C-ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/zola_b200.h"
+
+namespace zola {
+
+// Per-PSF pupil tables on the disk's bounding square (D x D, row a <-> kx,
+// column b <-> ky), zero outside the disk.  Built on the host in FP64 from
+// the optics (process/PhaseParameters.java:300-362, process/cpu/PSFPhase.java:140-220).
+struct PsfView {
+    int N;          // pupil grid (power of two)
+    int D;          // disk bounding-square side
+    int a0;         // first disk row / column index in the N grid
+    double dx;      // um
+    double zfocus;  // zoil of the localization model, um
+    const double* pupil;    // D*D amplitude (0 outside the disk)
+    const double* phase;    // D*D Zernike phase, radians
+    const double* kz;       // D*D
+    const double* kzoil;    // D*D
+    const double* isim;     // D*D (1: propagating in the sample)
+    const double* isimoil;  // D*D
+    const double* kx;       // D   (kx of row a)
+    const double* ky;       // D   (ky of column b)
+};
+
+// Per-ROI-size tables: the partial-DFT twiddles and the circular blur.
+struct WinView {
+    int R;          // ROI side
+    int W;          // intensity window, pow2(min(2R, N)) (PSFPhase.java:100-108)
+    const double2* C;   // W x D: C[w][a] = exp(+2 pi i ((a0+a+N/2)(w-W/2) mod N) / N)
+    const double* G;    // R x W: blur row i' <- window row i (circulant, see optics.cpp)
+};
+
+struct FitParamsDev {
+    double zmin, zmax, xymax, tol_xyz, step_xy, step_z;
+    int max_iter;
+};
+
+// Host-side tables of one window size (FP64 and the split-precision packs).
+struct WindowTables {
+    int R = 0, W = 0;
+    std::vector<double> C;     // W*D*2 interleaved
+    std::vector<double> G;     // R*W
+    double2* d_C = nullptr;
+    double* d_G = nullptr;
+    // split-precision operand packs (tcgen05 path), built lazily
+    void* d_split = nullptr;
+    size_t split_bytes = 0;
+};
+
+}  // namespace zola
+
+struct zola_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    long long launches = 0;
+    int num_sms = 0;
+    // reusable device scratch (FP64 fit work areas, counters)
+    void* scratch = nullptr;
+    size_t scratch_bytes = 0;
+    int* d_counter = nullptr;
+    int* d_status_word = nullptr;
+};
+
+struct zola_psf {
+    zola_ctx* ctx = nullptr;
+    zola_optics o{};
+    int N = 0, K = 0, D = 0, a0 = 0;
+    std::vector<double> zern;
+    // host copies of the D x D tables
+    std::vector<double> pupil, phase, kz, kzoil, isim, isimoil, kx, ky;
+    double* d_tables = nullptr;  // one allocation holding the arrays below
+    zola::PsfView view{};
+    std::map<int, zola::WindowTables> win;
+};
+
+namespace zola {
+
+// optics.cpp
+int build_psf_tables(zola_psf* p, const zola_optics* o, const double* zern, int nz, std::string& err);
+int window_size(int R, int N);
+WindowTables* get_window(zola_psf* p, int R, std::string& err);
+
+// fit_f64.cu
+int launch_model_f64(zola_ctx* ctx, zola_psf* p, WindowTables* w, const double* d_xyz, int n,
+                     double* d_out, double* d_dout, cudaStream_t st);
+int launch_fit_f64(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_rois, const double* d_init,
+                   int n, const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll,
+                   int* d_status, int* d_iters, cudaStream_t st);
+
+// fit_split.cu
+int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_rois, const double* d_init,
+                     int n, const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll,
+                     int* d_status, int* d_iters, cudaStream_t st);
+
+int ensure_scratch(zola_ctx* ctx, size_t bytes, std::string& err);
+
+}  // namespace zola
+
+#define ZOLA_CUDA_CHECK(call, ctxp)                                                 \
+    do {                                                                            \
+        cudaError_t e_ = (call);                                                    \
+        if (e_ != cudaSuccess) {                                                    \
+            (ctxp)->err = std::string(#call) + ": " + cudaGetErrorString(e_);       \
+            return ZOLA_E_CUDA;                                                     \
+        }                                                                           \
+    } while (0)
