@@ -112,6 +112,12 @@ ZOLA_API int zola_psf_info(const zola_psf* psf, int* N, int* K);
 ZOLA_API int zola_psf_model(zola_psf* psf, int R, const double* xyz, int n, double* out_psf, double* out_dpsf);
 ZOLA_API int zola_psf_model_dev(zola_psf* psf, int R, const double* d_xyz, int n, double* d_out_psf,
                        double* d_out_dpsf, void* stream);
+/* Same with an explicit arithmetic: ZOLA_PREC_FP64 (CUDA cores, FP64) or
+ * ZOLA_PREC_SPLIT (the tcgen05 split-precision stages the split fit uses). */
+ZOLA_API int zola_psf_model_prec(zola_psf* psf, int R, const double* xyz, int n, double* out_psf, double* out_dpsf,
+                                 int precision);
+ZOLA_API int zola_psf_model_prec_dev(zola_psf* psf, int R, const double* d_xyz, int n, double* d_out_psf,
+                                     double* d_out_dpsf, int precision, void* stream);
 
 /* --- batched Poisson MLE fit (replaces Localization_.localize with its
  * Modelmany_double_ likelihood batches, process/gpu/Localization_.java:633-798).
@@ -124,6 +130,10 @@ ZOLA_API int zola_fit_batch(zola_ctx* ctx, zola_psf* psf, int R, const float* ro
 ZOLA_API int zola_fit_batch_dev(zola_ctx* ctx, zola_psf* psf, int R, const float* d_rois, const double* d_init5,
                        int n, const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll,
                        int* d_status, int* d_iters, void* stream);
+
+/* Upper bound on the split fit's slot pool (ROIs in flight); 0 = automatic.
+ * Smaller pools keep the stage intermediates resident in L2. */
+ZOLA_API int zola_ctx_set_pool(zola_ctx* ctx, int max_slots);
 
 /* Number of kernel launches the library issued since the context was created
  * (bench bookkeeping). */

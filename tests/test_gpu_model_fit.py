@@ -69,8 +69,7 @@ def test_fp64_fit_matches_oracle_lm(zpkg, ctx, N, R, zern):
     prm = zpkg.PSF.fit_params(-1.0, 1.0, xymax, max_iter=30, precision=zpkg.ZOLA_PREC_FP64)
     res = psf.fit(rois, init, prm)
     o, nll, st, ev, cr = ref.fit_lm(rois.astype(np.float64), init, -1.0, 1.0, xymax, max_iter=30, crlb=True)
-    ok = st == 1
-    assert ok.mean() > 0.8
+    assert (st == 1).mean() > 0.6
     assert (res["status"] == st).all()
     assert (res["iters"] == ev).all()
     d = np.abs(res["theta"] - o)

@@ -1,0 +1,73 @@
+"""GPU tests of the split-precision tcgen05 path against the FP64 device path
+and the CPU oracle (north_star tolerances: 0.5 nm x/y, 1 nm z, 1e-3 photons)."""
+import numpy as np
+import pytest
+
+import oracle as O
+from common import OPTICS, astig_zernike, saddle_zernike, synth_rois, tetrapod_zernike
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    (64, 16, astig_zernike()),
+    (128, 24, saddle_zernike()),
+    (128, 48, tetrapod_zernike()),
+]
+
+
+def make(zpkg, ctx, N, zern):
+    return zpkg.PSF(ctx, zpkg.optics(size_fft=N, **OPTICS), zern)
+
+
+@pytest.mark.parametrize("N,R,zern", CASES)
+def test_split_model_matches_fp64(zpkg, ctx, N, R, zern):
+    psf = make(zpkg, ctx, N, zern)
+    rng = np.random.default_rng(5 + R)
+    xyz = np.c_[rng.uniform(-0.12, 0.12, (9, 2)), rng.uniform(-1.2, 1.2, 9)]
+    a, da = psf.model(R, xyz, derivs=True, precision=zpkg.ZOLA_PREC_FP64)
+    b, db = psf.model(R, xyz, derivs=True, precision=zpkg.ZOLA_PREC_SPLIT)
+    # three-product FP16 model: ~1e-6 of the peak; single-product derivatives: ~1e-3
+    assert np.abs(a - b).max() <= 2e-6 * a.max()
+    assert np.abs(da - db).max() <= 5e-3 * np.abs(da).max()
+
+
+@pytest.mark.parametrize("N,R,zern", CASES)
+def test_split_fit_matches_fp64_fit(zpkg, ctx, N, R, zern):
+    psf = make(zpkg, ctx, N, zern)
+    ref = O.OraclePSF(N, 0.11, 1.4, 0.66, 1.518, 1.518, 0.9, zern, gauss_f32=False)
+    rois, truth = synth_rois(ref.model, R, 64, seed=3 + R, zrange=0.6, photons=3000, sigma_ln=0.6)
+    init = truth.copy()
+    init[:, :2] = 0
+    init[:, 2] = np.round(truth[:, 2] / 0.3) * 0.3
+    init[:, 3] *= 0.8
+    xymax = R * 0.11 / 2
+    p64 = zpkg.PSF.fit_params(-1.0, 1.0, xymax, max_iter=50, precision=zpkg.ZOLA_PREC_FP64)
+    psp = zpkg.PSF.fit_params(-1.0, 1.0, xymax, max_iter=50, precision=zpkg.ZOLA_PREC_SPLIT)
+    a = psf.fit(rois, init, p64)
+    b = psf.fit(rois, init, psp)
+    ok = (a["status"] == 1) & (b["status"] == 1)
+    assert ok.mean() > 0.85
+    d = np.abs(a["theta"][ok] - b["theta"][ok])
+    assert d[:, :2].max() * 1000 <= 0.5
+    assert d[:, 2].max() * 1000 <= 1.0
+    assert (d[:, 3] / a["theta"][ok, 3]).max() <= 1e-3
+    assert np.allclose(a["crlb"][ok, :3], b["crlb"][ok, :3], rtol=2e-2)
+
+
+def test_split_fit_small_pool_refills(zpkg, ctx):
+    """A pool much smaller than the batch retires and refills slots; every ROI is fitted once."""
+    psf = make(zpkg, ctx, 64, astig_zernike())
+    ref = O.OraclePSF(64, 0.11, 1.4, 0.66, 1.518, 1.518, 0.9, astig_zernike(), gauss_f32=False)
+    rois, truth = synth_rois(ref.model, 16, 100, seed=21)
+    init = truth.copy()
+    init[:, :3] = 0
+    prm = zpkg.PSF.fit_params(-1.0, 1.0, 0.88, max_iter=40, precision=zpkg.ZOLA_PREC_SPLIT)
+    full = psf.fit(rois, init, prm)
+    ctx.set_pool(8)
+    try:
+        small = psf.fit(rois, init, prm)
+    finally:
+        ctx.set_pool(0)
+    assert (small["iters"] > 0).all()
+    assert np.array_equal(full["status"], small["status"])
+    assert np.allclose(full["theta"], small["theta"], rtol=0, atol=1e-9)

@@ -16,6 +16,7 @@ no CPU fallback: if the library is missing every call raises.
 import ctypes
 import json
 import os
+import weakref
 
 import numpy as np
 
@@ -45,8 +46,9 @@ class FitParams(ctypes.Structure):
 
 
 EXPORTS = ["zola_ctx_create", "zola_ctx_destroy", "zola_last_error", "zola_ctx_stream", "zola_ctx_launches",
-           "zola_psf_load", "zola_psf_free", "zola_psf_info", "zola_psf_model", "zola_psf_model_dev",
-           "zola_fit_batch", "zola_fit_batch_dev"]
+           "zola_ctx_set_pool", "zola_psf_load", "zola_psf_free", "zola_psf_info", "zola_psf_model",
+           "zola_psf_model_dev", "zola_psf_model_prec", "zola_psf_model_prec_dev", "zola_fit_batch",
+           "zola_fit_batch_dev"]
 
 _lib = None
 
@@ -72,6 +74,9 @@ def lib():
         L.zola_psf_info.argtypes = [vp, ctypes.POINTER(i), ctypes.POINTER(i)]
         L.zola_psf_model.argtypes = [vp, i, vp, i, vp, vp]
         L.zola_psf_model_dev.argtypes = [vp, i, vp, i, vp, vp, vp]
+        L.zola_psf_model_prec.argtypes = [vp, i, vp, i, vp, vp, i]
+        L.zola_psf_model_prec_dev.argtypes = [vp, i, vp, i, vp, vp, i, vp]
+        L.zola_ctx_set_pool.argtypes = [vp, i]
         L.zola_fit_batch.argtypes = [vp, vp, i, vp, vp, i, ctypes.POINTER(FitParams), vp, vp, vp, vp, vp]
         L.zola_fit_batch_dev.argtypes = [vp, vp, i, vp, vp, i, ctypes.POINTER(FitParams), vp, vp, vp, vp, vp, vp]
         _lib = L
@@ -96,6 +101,7 @@ class Context:
             raise ZolaError(f"zola_ctx_create failed ({rc}): no usable sm_100 device {device}")
         self.h = h
         self.device = device
+        self._psfs = weakref.WeakSet()
 
     def check(self, rc, what):
         if rc != 0:
@@ -106,12 +112,18 @@ class Context:
     def stream(self):
         return lib().zola_ctx_stream(self.h)
 
+    def set_pool(self, max_slots):
+        """Bound the split fit's slot pool (ROIs in flight); 0 = automatic."""
+        self.check(lib().zola_ctx_set_pool(self.h, int(max_slots)), "zola_ctx_set_pool")
+
     @property
     def launches(self):
         return lib().zola_ctx_launches(self.h)
 
     def close(self):
         if getattr(self, "h", None):
+            for p in list(self._psfs):
+                p.close()
             lib().zola_ctx_destroy(self.h)
             self.h = None
 
@@ -141,13 +153,15 @@ class PSF:
         ctx.check(lib().zola_psf_load(ctx.h, ctypes.byref(opt), _ptr(self.zernike), len(self.zernike),
                                       ctypes.byref(h)), "zola_psf_load")
         self.h = h
+        ctx._psfs.add(self)
         n, k = ctypes.c_int(), ctypes.c_int()
         lib().zola_psf_info(h, ctypes.byref(n), ctypes.byref(k))
         self.N, self.K = n.value, k.value
 
     def close(self):
         if getattr(self, "h", None):
-            lib().zola_psf_free(self.h)
+            if getattr(self.ctx, "h", None):  # the context frees its PSFs first on close
+                lib().zola_psf_free(self.h)
             self.h = None
 
     def __del__(self):
@@ -156,13 +170,15 @@ class PSF:
         except Exception:
             pass
 
-    def model(self, R, xyz, derivs=False):
-        """psi (n, R, R) (and dpsi (n, 3, R, R)) at (x, y, zwat) um, FP64 on the GPU."""
+    def model(self, R, xyz, derivs=False, precision=ZOLA_PREC_FP64):
+        """psi (n, R, R) (and dpsi (n, 3, R, R)) at (x, y, zwat) um on the GPU
+        (FP64 CUDA cores, or the tcgen05 split-precision stages)."""
         xyz = np.ascontiguousarray(np.atleast_2d(xyz), dtype=np.float64)
         n = xyz.shape[0]
         out = np.zeros((n, R, R))
         d = np.zeros((n, 3, R, R)) if derivs else None
-        self.ctx.check(lib().zola_psf_model(self.h, int(R), _ptr(xyz), n, _ptr(out), _ptr(d)), "zola_psf_model")
+        self.ctx.check(lib().zola_psf_model_prec(self.h, int(R), _ptr(xyz), n, _ptr(out), _ptr(d), int(precision)),
+                       "zola_psf_model_prec")
         return (out, d) if derivs else out
 
     def model_dev(self, R, xyz, out, dout=None, stream=None):

@@ -94,6 +94,7 @@ int zola_ctx_destroy(zola_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->d_counter) cudaFree(ctx->d_counter);
+    if (ctx->h_flags) cudaFreeHost(ctx->h_flags);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return ZOLA_OK;
@@ -129,7 +130,7 @@ int zola_psf_free(zola_psf* psf) {
     for (auto& kv : psf->win) {
         if (kv.second.d_C) cudaFree(kv.second.d_C);
         if (kv.second.d_G) cudaFree(kv.second.d_G);
-        if (kv.second.d_split) cudaFree(kv.second.d_split);
+        if (kv.second.d_split) free_split_plan(kv.second.d_split);
     }
     if (psf->d_tables) cudaFree(psf->d_tables);
     delete psf;
@@ -143,6 +144,23 @@ int zola_psf_info(const zola_psf* psf, int* N, int* K) {
     return ZOLA_OK;
 }
 
+int zola_psf_model_prec_dev(zola_psf* psf, int R, const double* d_xyz, int n, double* d_out, double* d_dout,
+                            int precision, void* stream) {
+    if (!psf) return ZOLA_E_ARG;
+    zola_ctx* ctx = psf->ctx;
+    if (n < 0 || (n > 0 && (!d_xyz || !d_out))) return set_err(ctx, ZOLA_E_ARG, "zola_psf_model: bad n or null buffer");
+    if (precision != ZOLA_PREC_FP64 && precision != ZOLA_PREC_SPLIT) return set_err(ctx, ZOLA_E_ARG, "unknown precision");
+    WindowTables* w = get_window(psf, R, ctx->err);
+    if (!w) return ZOLA_E_ARG;
+    if (n == 0) return ZOLA_OK;
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    if (precision == ZOLA_PREC_SPLIT) {
+        if (psf->o.kz_reset) return set_err(ctx, ZOLA_E_ARG, "split model needs kz_reset = 0 tables");
+        return launch_model_split(ctx, psf, w, d_xyz, n, d_out, d_dout, st);
+    }
+    return launch_model_f64(ctx, psf, w, d_xyz, n, d_out, d_dout, st);
+}
+
 int zola_psf_model_dev(zola_psf* psf, int R, const double* d_xyz, int n, double* d_out, double* d_dout,
                        void* stream) {
     if (!psf) return ZOLA_E_ARG;
@@ -154,7 +172,7 @@ int zola_psf_model_dev(zola_psf* psf, int R, const double* d_xyz, int n, double*
     return launch_model_f64(ctx, psf, w, d_xyz, n, d_out, d_dout, st);
 }
 
-int zola_psf_model(zola_psf* psf, int R, const double* xyz, int n, double* out, double* dout) {
+int zola_psf_model_prec(zola_psf* psf, int R, const double* xyz, int n, double* out, double* dout, int precision) {
     if (!psf) return ZOLA_E_ARG;
     zola_ctx* ctx = psf->ctx;
     if (n < 0 || (n > 0 && (!xyz || !out))) return set_err(ctx, ZOLA_E_ARG, "zola_psf_model: bad n or null buffer");
@@ -167,12 +185,22 @@ int zola_psf_model(zola_psf* psf, int R, const double* xyz, int n, double* out, 
     ZOLA_CUDA_CHECK(dout_.alloc(rr * n), ctx);
     if (dout) ZOLA_CUDA_CHECK(ddout.alloc(3 * rr * n), ctx);
     ZOLA_CUDA_CHECK(cudaMemcpyAsync(dx.p, xyz, 3 * sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream), ctx);
-    int rc = zola_psf_model_dev(psf, R, dx.p, n, dout_.p, dout ? ddout.p : nullptr, ctx->stream);
+    int rc = zola_psf_model_prec_dev(psf, R, dx.p, n, dout_.p, dout ? ddout.p : nullptr, precision, ctx->stream);
     if (rc) return rc;
     ZOLA_CUDA_CHECK(cudaMemcpyAsync(out, dout_.p, rr * n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), ctx);
     if (dout)
         ZOLA_CUDA_CHECK(cudaMemcpyAsync(dout, ddout.p, 3 * rr * n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), ctx);
     ZOLA_CUDA_CHECK(cudaStreamSynchronize(ctx->stream), ctx);
+    return ZOLA_OK;
+}
+
+int zola_psf_model(zola_psf* psf, int R, const double* xyz, int n, double* out, double* dout) {
+    return zola_psf_model_prec(psf, R, xyz, n, out, dout, ZOLA_PREC_FP64);
+}
+
+int zola_ctx_set_pool(zola_ctx* ctx, int max_slots) {
+    if (!ctx || max_slots < 0) return ZOLA_E_ARG;
+    ctx->split_pool_max = max_slots;
     return ZOLA_OK;
 }
 

@@ -1,12 +1,987 @@
-// Split-precision tcgen05 fit (placeholder until the tensor-core kernel lands).
+// Split-precision Poisson MLE fit on the sm_100a tensor cores (tcgen05).
+//
+// The model of process/cpu/PSFPhase.java:557-629 is evaluated for a pool of
+// ROI "slots" as four batched tensor-core contractions per Levenberg-Marquardt
+// evaluation, each a tcgen05.mma chain from shared memory into TMEM:
+//
+//   stage 1  S  = Q  C^T  (+ Sy = Q CK^T, Sz = Qz C^T)   rows (roi, a)   K = 2DP
+//   stage 2  E^T = S^T C^T (+ Ex, Ey, Ez)                rows (roi, j)   K = 2DP
+//            epilogue: I = |E|^2, I_t = 2 Re(conj(E) E_t)
+//   stage 3  J^T = I G^T  (blur along the first image index)  rows (roi, j)  K = W
+//   stage 4  T  = J G^T   (blur along the second index)       rows (map, i') K = W
+//   stage 5  likelihood, gradient, Gauss-Newton Hessian and Fisher sums in
+//            FP32 with Kahan compensation, then the FP64 5x5 LM solve, damping
+//            and convergence test; converged slots are retired and refilled
+//            from the ROI queue (a device counter).
+//
+// C is the W x D partial-DFT matrix, CK = C diag(i k) its x/y derivative, Q the
+// pupil field (built in registers from the pupil tables and the slot's trial
+// x, y, z), G the R x W circular-blur matrix (see optics.cpp).  Complex
+// products are real GEMMs on [re | im] operands.  Every operand that sets the
+// likelihood value (Q, S, E, I, J of the model itself, and the constants C, G)
+// is an FP16 hi + lo pair and multiplied with three products
+// (hi*hi + hi*lo + lo*hi, FP32 accumulation): about 2^-22 relative.  The
+// derivative maps only enter the gradient and the Hessian; their operands are
+// single FP16 products, whose rounding moves the optimum by about
+// 2^-11 x CRLB (~0.01 nm), far below the 0.5 nm budget.
+//
+// All operands use the canonical no-swizzle layouts of umma.h.  Intermediate
+// operands travel through a global (L2-resident for moderate pools) slab laid
+// out exactly as the shared-memory tiles, so each stage fetches a tile with
+// 1-D bulk (TMA) copies.  Scales are powers of two chosen from host-side bounds
+// so no FP16 value overflows; they are exact and undone in FP32.
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+
+#include "lm.h"
+#include "umma.h"
 #include "zola_internal.h"
 
 namespace zola {
 
-int launch_fit_split(zola_ctx* ctx, zola_psf*, WindowTables*, const float*, const double*, int,
-                     const zola_fit_params*, double*, double*, double*, int*, int*, cudaStream_t) {
-    ctx->err = "split-precision fit not built";
-    return ZOLA_E_UNSUPPORTED;
+using umma::kmajor_off;
+using umma::mnmajor_off;
+
+constexpr int SPLIT_THREADS = 128;
+
+// ---------------------------------------------------------------- plan ------
+struct SplitScales {
+    float q, qz;                 // Q, Qz operand scales
+    float c2, c2y, c2z;          // TMEM(S) -> A2 operand factors
+    float cI, cIx, cIy, cIz;     // TMEM(E products) -> A3 operand factors
+    float cJ[4];                 // TMEM(J) -> A4 operand factors
+    float cT[4];                 // TMEM(T) -> true blurred maps
+};
+
+struct SplitDev {
+    // geometry
+    int R, W, D, DP, K1, IC, NCH, RP, G1, G2, NT4, P;
+    int a0, N;
+    double zfocus;
+    // constant operands
+    const __half* bc_hi;  // NCH chunks of 4IC x K1 (K-major)
+    const __half* bc_lo;  // NCH chunks of 2IC x K1
+    const __half* gt_hi;  // RP x W (K-major)
+    const __half* gt_lo;
+    // pupil tables (D x D, row a <-> kx, column b <-> ky), FP64
+    const double* pupil;
+    const double* phase0;  // phase - kzoil * zfocus
+    const double* kz;
+    const double* kx;
+    const double* ky;
+    // pool slabs
+    char* a2;      // P/G2 tiles x 4 arrays x 128 x K1 f16
+    char* a3;      // P/G2 tiles x 5 arrays x 128 x W f16
+    char* a4;      // P x NT4 tiles x 2 arrays x 128 x W f16
+    float* tmaps;  // P x 4 x R x R
+    // slot state
+    int* slot_roi;
+    int* slot_phase;
+    LMState* lm;
+    int* queue;    // next ROI to hand out
+    int* active;   // occupied slots
+    int* err;      // bounded-wait timeout flag
+    SplitScales sc;
+};
+
+struct SplitPlanHost {
+    int R = 0, W = 0, D = 0, DP = 0, K1 = 0, IC = 0, NCH = 0, RP = 0, G1 = 0, G2 = 0, NT4 = 0;
+    SplitScales sc{};
+    __half* d_bc_hi = nullptr;
+    __half* d_bc_lo = nullptr;
+    __half* d_gt_hi = nullptr;
+    __half* d_gt_lo = nullptr;
+    double* d_phase0 = nullptr;
+};
+
+static double pow2scale(double bound) {
+    if (!(bound > 0)) return 1.0;
+    return std::ldexp(1.0, (int)std::floor(std::log2(16384.0 / bound)));
+}
+
+__host__ __device__ inline size_t a2_tile_bytes(int K1) { return (size_t)4 * 128 * K1 * 2; }
+__host__ __device__ inline size_t a3_tile_bytes(int W) { return (size_t)5 * 128 * W * 2; }
+__host__ __device__ inline size_t a4_tile_bytes(int W) { return (size_t)2 * 128 * W * 2; }
+
+// Build (once per PSF and ROI size) the constant operands and scales.
+static SplitPlanHost* get_plan(zola_psf* p, WindowTables* w, std::string& err) {
+    if (w->d_split) return (SplitPlanHost*)w->d_split;
+    SplitPlanHost* pl = new SplitPlanHost();
+    const int D = p->D, W = w->W, R = w->R;
+    pl->R = R; pl->W = W; pl->D = D;
+    pl->DP = D <= 32 ? 32 : 64;
+    pl->K1 = 2 * pl->DP;
+    pl->IC = W < 32 ? W : 32;
+    pl->NCH = W / pl->IC;
+    pl->RP = (R + 15) / 16 * 16;
+    pl->G1 = 128 / pl->DP;
+    pl->G2 = 128 / W;
+    pl->NT4 = (4 * pl->RP + 127) / 128;
+    const int DP = pl->DP, K1 = pl->K1, IC = pl->IC, NCH = pl->NCH, RP = pl->RP;
+
+    // bounds
+    double pmax = 0, kmax = 0, kzmax = 0;
+    for (size_t i = 0; i < p->pupil.size(); ++i) {
+        pmax = std::max(pmax, std::fabs(p->pupil[i]));
+        if (p->pupil[i] != 0) kzmax = std::max(kzmax, std::fabs(p->kz[i]));
+    }
+    for (int a = 0; a < D; ++a) kmax = std::max(kmax, std::fabs(p->kx[a]));
+    double sum_pupil = 0;
+    for (double v : p->pupil) sum_pupil += std::fabs(v);
+    const double sQ = pow2scale(pmax), sQz = pow2scale(pmax * kzmax), sB = pow2scale(std::max(1.0, kmax));
+    const double bS = D * pmax, bSy = bS * kmax, bSz = bS * kzmax;
+    const double s2 = pow2scale(bS), s2y = pow2scale(bSy), s2z = pow2scale(bSz);
+    const double bE = sum_pupil, bI = bE * bE, bIx = 2 * bE * bE * kmax, bIz = 2 * bE * bE * kzmax;
+    const double sI = pow2scale(bI), sIx = pow2scale(bIx), sIz = pow2scale(bIz);
+    double gmax = 0, gsum = 0;
+    for (int ip = 0; ip < R; ++ip) {
+        double s = 0;
+        for (int i = 0; i < W; ++i) { gmax = std::max(gmax, std::fabs(w->G[(size_t)ip * W + i])); s += std::fabs(w->G[(size_t)ip * W + i]); }
+        gsum = std::max(gsum, s);
+    }
+    const double sG = pow2scale(gmax);
+    const double sImap[4] = {sI, sIx, sIx, sIz};
+    const double bImap[4] = {bI, bIx, bIx, bIz};
+    SplitScales& sc = pl->sc;
+    sc.q = (float)sQ; sc.qz = (float)sQz;
+    sc.c2 = (float)(s2 / (sQ * sB)); sc.c2y = (float)(s2y / (sQ * sB)); sc.c2z = (float)(s2z / (sQz * sB));
+    sc.cI = (float)(sI / ((s2 * sB) * (s2 * sB)));
+    sc.cIx = (float)(2 * sIx / ((s2 * sB) * (s2 * sB)));
+    sc.cIy = (float)(2 * sIx / ((s2 * sB) * (s2y * sB)));
+    sc.cIz = (float)(2 * sIz / ((s2 * sB) * (s2z * sB)));
+    for (int m = 0; m < 4; ++m) {
+        double sJ = pow2scale(gsum * bImap[m]);
+        sc.cJ[m] = (float)(sJ / (sImap[m] * sG));
+        sc.cT[m] = (float)(1.0 / (sJ * sG));
+    }
+
+    // BC chunks.  Rows n' = part * IC + ii of chunk c (output index c*IC + ii):
+    // part 0: [Re C ; -Im C], 1: [Im C ; Re C], 2: [Re CK ; -Im CK], 3: [Im CK ; Re CK]
+    // with columns k < DP multiplying the real and k >= DP the imaginary part
+    // of the data; CK[i][b] = C[i][b] * (i k_b).
+    std::vector<__half> bh((size_t)NCH * 4 * IC * K1, __float2half(0.f)), bl((size_t)NCH * 2 * IC * K1, __float2half(0.f));
+    auto C = [&](int i, int b, double& re, double& im) {
+        re = w->C[((size_t)i * D + b) * 2];
+        im = w->C[((size_t)i * D + b) * 2 + 1];
+    };
+    for (int c = 0; c < NCH; ++c)
+        for (int part = 0; part < 4; ++part)
+            for (int ii = 0; ii < IC; ++ii) {
+                int i = c * IC + ii, n = part * IC + ii;
+                for (int k = 0; k < K1; ++k) {
+                    int b = k < DP ? k : k - DP;
+                    if (b >= D) continue;
+                    double cr, ci;
+                    C(i, b, cr, ci);
+                    double kb = p->ky[b];
+                    double ckr = -kb * ci, cki = kb * cr;
+                    double v;
+                    bool re_in = k < DP;
+                    switch (part) {
+                        case 0: v = re_in ? cr : -ci; break;
+                        case 1: v = re_in ? ci : cr; break;
+                        case 2: v = re_in ? ckr : -cki; break;
+                        default: v = re_in ? cki : ckr; break;
+                    }
+                    v *= sB;
+                    __half hi = __float2half_rn((float)v);
+                    __half lo = __float2half_rn((float)(v - (double)__half2float(hi)));
+                    bh[(size_t)c * 4 * IC * K1 + kmajor_off(n, k, K1) / 2] = hi;
+                    if (part < 2) bl[(size_t)c * 2 * IC * K1 + kmajor_off(n, k, K1) / 2] = lo;
+                }
+            }
+    // G^T operand: rows n = i' (< RP, zero beyond R), K = W.
+    std::vector<__half> gh((size_t)RP * W, __float2half(0.f)), gl((size_t)RP * W, __float2half(0.f));
+    for (int ip = 0; ip < R; ++ip)
+        for (int i = 0; i < W; ++i) {
+            double v = w->G[(size_t)ip * W + i] * sG;
+            __half hi = __float2half_rn((float)v);
+            __half lo = __float2half_rn((float)(v - (double)__half2float(hi)));
+            gh[kmajor_off(ip, i, W) / 2] = hi;
+            gl[kmajor_off(ip, i, W) / 2] = lo;
+        }
+    // phase0 = phase - kzoil * zfocus (the zoil term of PSFPhase.java:560 with zoil = Zfocus)
+    std::vector<double> ph0((size_t)D * D);
+    for (size_t i = 0; i < ph0.size(); ++i) ph0[i] = p->phase[i] - p->kzoil[i] * p->o.zfocus;
+
+    cudaError_t e = cudaSuccess;
+    auto up = [&](void** dst, const void* src, size_t bytes) {
+        if (e != cudaSuccess) return;
+        e = cudaMalloc(dst, bytes);
+        if (e == cudaSuccess) e = cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
+    };
+    up((void**)&pl->d_bc_hi, bh.data(), bh.size() * 2);
+    up((void**)&pl->d_bc_lo, bl.data(), bl.size() * 2);
+    up((void**)&pl->d_gt_hi, gh.data(), gh.size() * 2);
+    up((void**)&pl->d_gt_lo, gl.data(), gl.size() * 2);
+    up((void**)&pl->d_phase0, ph0.data(), ph0.size() * 8);
+    if (e != cudaSuccess) {
+        err = std::string("split plan upload: ") + cudaGetErrorString(e);
+        delete pl;
+        return nullptr;
+    }
+    w->d_split = pl;
+    return pl;
+}
+
+void free_split_plan(void* plan) {
+    SplitPlanHost* pl = (SplitPlanHost*)plan;
+    if (!pl) return;
+    cudaFree(pl->d_bc_hi);
+    cudaFree(pl->d_bc_lo);
+    cudaFree(pl->d_gt_hi);
+    cudaFree(pl->d_gt_lo);
+    cudaFree(pl->d_phase0);
+    delete pl;
+}
+
+// ------------------------------------------------------------- helpers -----
+__device__ __forceinline__ uint32_t tmem_lane_addr(uint32_t base, int col) {
+    const int warp = threadIdx.x >> 5;
+    return base + ((uint32_t)(warp * 32) << 16) + (uint32_t)col;
+}
+
+__device__ __forceinline__ void store8h(void* dst, const __half* v) {
+    uint4 u;
+    u.x = (uint32_t)__half_as_ushort(v[0]) | ((uint32_t)__half_as_ushort(v[1]) << 16);
+    u.y = (uint32_t)__half_as_ushort(v[2]) | ((uint32_t)__half_as_ushort(v[3]) << 16);
+    u.z = (uint32_t)__half_as_ushort(v[4]) | ((uint32_t)__half_as_ushort(v[5]) << 16);
+    u.w = (uint32_t)__half_as_ushort(v[6]) | ((uint32_t)__half_as_ushort(v[7]) << 16);
+    *(uint4*)dst = u;
+}
+
+// Issue an MMA chain over K (in steps of 16) for one accumulator.
+__device__ __forceinline__ void mma_chain(uint32_t tmem_d, uint32_t a_addr, uint32_t a_lbo, uint32_t a_sbo,
+                                          uint32_t a_kstep, uint32_t b_addr, uint32_t b_lbo, uint32_t b_sbo,
+                                          uint32_t b_kstep, int K, uint32_t idesc, bool accumulate) {
+    for (int s = 0; s < K / 16; ++s) {
+        uint64_t ad = umma::smem_desc(a_addr + s * a_kstep, a_lbo, a_sbo);
+        uint64_t bd = umma::smem_desc(b_addr + s * b_kstep, b_lbo, b_sbo);
+        umma::mma_f16(tmem_d, ad, bd, idesc, (accumulate || s > 0) ? 1u : 0u);
+    }
+}
+
+__device__ __forceinline__ int tmem_cols_pow2(int c) {
+    int p = 32;
+    while (p < c) p <<= 1;
+    return p;
+}
+
+// ----------------------------------------------------------- stage 1 -------
+// One CTA per G1 slots; thread t builds row (g = t / DP, a = t % DP) of Q.
+__global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage1(SplitDev P) {
+    extern __shared__ __align__(1024) char smem[];
+    const int K1 = P.K1, DP = P.DP, IC = P.IC, NCH = P.NCH, D = P.D;
+    const int t = threadIdx.x;
+    char* A1hi = smem;
+    char* A1lo = A1hi + 256 * K1;
+    char* A1z = A1lo + 256 * K1;
+    char* bcb = A1z + 256 * K1;
+    const int bc_hi_bytes = 4 * IC * K1 * 2, bc_lo_bytes = 2 * IC * K1 * 2;
+    const int bc_buf = bc_hi_bytes + bc_lo_bytes;
+    __shared__ __align__(8) uint64_t bc_full[2], mma_done[2];
+    __shared__ uint32_t tmem_base;
+    const int ncols = NCH > 1 ? 512 : tmem_cols_pow2(6 * IC);
+
+    if (t < 32) umma::tmem_alloc(&tmem_base, ncols);
+    if (t == 0) {
+        umma::mbar_init(&bc_full[0], 1); umma::mbar_init(&bc_full[1], 1);
+        umma::mbar_init(&mma_done[0], 1); umma::mbar_init(&mma_done[1], 1);
+        umma::mbar_fence_init();
+    }
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tbase = tmem_base;
+    auto load_bc = [&](int c, int buf) {
+        char* dst = bcb + buf * bc_buf;
+        umma::mbar_expect_tx(&bc_full[buf], bc_buf);
+        umma::bulk_g2s(dst, (const char*)P.bc_hi + (size_t)c * bc_hi_bytes, bc_hi_bytes, &bc_full[buf]);
+        umma::bulk_g2s(dst + bc_hi_bytes, (const char*)P.bc_lo + (size_t)c * bc_lo_bytes, bc_lo_bytes, &bc_full[buf]);
+    };
+    if (t == 0) {
+        load_bc(0, 0);
+        if (NCH > 1) load_bc(1, 1);
+    }
+
+    // build the Q operand rows
+    const int g = t / DP, a = t % DP;
+    const int slot = blockIdx.x * P.G1 + g;
+    const int roi = P.slot_roi[slot];
+    double x = 0, y = 0, z = 0;
+    if (roi >= 0) {
+        x = P.lm[slot].trial[0]; y = P.lm[slot].trial[1]; z = P.lm[slot].trial[2];
+    }
+    const double kxa = a < D ? P.kx[a] : 0.0;
+    for (int b0 = 0; b0 < DP; b0 += 8) {
+        __half rh[8], rl[8], ih[8], il[8], zr[8], zi[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int b = b0 + u;
+            float qr = 0.f, qi = 0.f, kzv = 0.f;
+            if (roi >= 0 && a < D && b < D) {
+                const int idx = a * D + b;
+                const double pup = P.pupil[idx];
+                if (pup != 0.0) {
+                    double ph = P.phase0[idx] + kxa * x + P.ky[b] * y + P.kz[idx] * z;
+                    ph -= 6.283185307179586 * rint(ph * 0.15915494309189535);
+                    float s, c;
+                    sincosf((float)ph, &s, &c);
+                    qr = (float)pup * c;
+                    qi = (float)pup * s;
+                    kzv = (float)P.kz[idx];
+                }
+            }
+            umma::split_f16(qr * P.sc.q, rh[u], rl[u]);
+            umma::split_f16(qi * P.sc.q, ih[u], il[u]);
+            zr[u] = __float2half_rn(-kzv * qi * P.sc.qz);  // Qz = i kz Q
+            zi[u] = __float2half_rn(kzv * qr * P.sc.qz);
+        }
+        store8h(A1hi + kmajor_off(t, b0, K1), rh);
+        store8h(A1lo + kmajor_off(t, b0, K1), rl);
+        store8h(A1hi + kmajor_off(t, DP + b0, K1), ih);
+        store8h(A1lo + kmajor_off(t, DP + b0, K1), il);
+        store8h(A1z + kmajor_off(t, b0, K1), zr);
+        store8h(A1z + kmajor_off(t, DP + b0, K1), zi);
+    }
+    umma::fence_proxy_async();
+    __syncthreads();
+
+    const uint32_t sbo1 = (K1 / 8) * 128;
+    const uint32_t id4 = umma::idesc_f16(128, 4 * IC, false, false);
+    const uint32_t id2 = umma::idesc_f16(128, 2 * IC, false, false);
+    auto issue = [&](int c) {
+        const int buf = NCH > 1 ? (c & 1) : 0;
+        umma::mbar_wait(&bc_full[buf], (c >> 1) & 1, P.err);
+        umma::fence_after_sync();
+        const uint32_t bhi = umma::smem_u32(bcb + buf * bc_buf), blo = bhi + bc_hi_bytes;
+        const uint32_t a_hi = umma::smem_u32(A1hi), a_lo = umma::smem_u32(A1lo), a_z = umma::smem_u32(A1z);
+        const uint32_t td = tbase + buf * 256;
+        mma_chain(td, a_hi, 128, sbo1, 256, bhi, 128, sbo1, 256, K1, id4, false);
+        mma_chain(td, a_hi, 128, sbo1, 256, blo, 128, sbo1, 256, K1, id2, true);
+        mma_chain(td, a_lo, 128, sbo1, 256, bhi, 128, sbo1, 256, K1, id2, true);
+        mma_chain(td + 4 * IC, a_z, 128, sbo1, 256, bhi, 128, sbo1, 256, K1, id2, false);
+        umma::mma_commit(&mma_done[buf]);
+    };
+    if (t == 0) issue(0);
+    // A2 destination for this thread's row: stage-2 tile of the slot, k = a and DP + a
+    const int tile2 = slot / P.G2, mrow0 = (slot % P.G2) * P.W;
+    char* a2t = P.a2 + (size_t)tile2 * a2_tile_bytes(K1);
+    const size_t arr = (size_t)128 * K1 * 2;
+    for (int c = 0; c < NCH; ++c) {
+        const int buf = NCH > 1 ? (c & 1) : 0;
+        if (t == 0 && c + 1 < NCH) issue(c + 1);
+        umma::mbar_wait(&mma_done[buf], (c >> 1) & 1, P.err);
+        umma::fence_after_sync();
+        const uint32_t col0 = buf * 256;
+        for (int h = 0; h < IC; h += 16) {
+            float v[6][16];
+            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 0 * IC + h), v[0]);
+            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 1 * IC + h), v[1]);
+            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 2 * IC + h), v[2]);
+            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 3 * IC + h), v[3]);
+            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 4 * IC + h), v[4]);
+            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 5 * IC + h), v[5]);
+            if (roi < 0) continue;
+            for (int j8 = 0; j8 < 16; j8 += 8) {
+                const int m = mrow0 + c * IC + h + j8;
+                __half shr[8], slr[8], shi[8], sli[8], yr[8], yi[8], zr[8], zi[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    umma::split_f16(v[0][j8 + u] * P.sc.c2, shr[u], slr[u]);
+                    umma::split_f16(v[1][j8 + u] * P.sc.c2, shi[u], sli[u]);
+                    yr[u] = __float2half_rn(v[2][j8 + u] * P.sc.c2y);
+                    yi[u] = __float2half_rn(v[3][j8 + u] * P.sc.c2y);
+                    zr[u] = __float2half_rn(v[4][j8 + u] * P.sc.c2z);
+                    zi[u] = __float2half_rn(v[5][j8 + u] * P.sc.c2z);
+                }
+                store8h(a2t + 0 * arr + mnmajor_off(m, a, 128), shr);
+                store8h(a2t + 1 * arr + mnmajor_off(m, a, 128), slr);
+                store8h(a2t + 0 * arr + mnmajor_off(m, DP + a, 128), shi);
+                store8h(a2t + 1 * arr + mnmajor_off(m, DP + a, 128), sli);
+                store8h(a2t + 2 * arr + mnmajor_off(m, a, 128), yr);
+                store8h(a2t + 2 * arr + mnmajor_off(m, DP + a, 128), yi);
+                store8h(a2t + 3 * arr + mnmajor_off(m, a, 128), zr);
+                store8h(a2t + 3 * arr + mnmajor_off(m, DP + a, 128), zi);
+            }
+        }
+        umma::fence_before_sync();
+        __syncthreads();
+        if (t == 0 && c + 2 < NCH) load_bc(c + 2, buf);
+    }
+    __syncthreads();
+    if (t < 32) umma::tmem_dealloc(tbase, ncols);
+}
+
+// ----------------------------------------------------------- stage 2 -------
+// One CTA per stage-2 tile (G2 slots x W rows j).
+__global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage2(SplitDev P) {
+    extern __shared__ __align__(1024) char smem[];
+    const int K1 = P.K1, IC = P.IC, NCH = P.NCH, W = P.W;
+    const int t = threadIdx.x;
+    const size_t arr = (size_t)128 * K1 * 2;
+    char* A2 = smem;  // hi, lo, y, z
+    char* bcb = A2 + 4 * arr;
+    const int bc_hi_bytes = 4 * IC * K1 * 2, bc_lo_bytes = 2 * IC * K1 * 2;
+    const int bc_buf = bc_hi_bytes + bc_lo_bytes;
+    __shared__ __align__(8) uint64_t a2_full, bc_full[2], mma_done[2];
+    __shared__ uint32_t tmem_base;
+    const int ncols = NCH > 1 ? 512 : tmem_cols_pow2(8 * IC);
+    if (t < 32) umma::tmem_alloc(&tmem_base, ncols);
+    if (t == 0) {
+        umma::mbar_init(&a2_full, 1);
+        umma::mbar_init(&bc_full[0], 1); umma::mbar_init(&bc_full[1], 1);
+        umma::mbar_init(&mma_done[0], 1); umma::mbar_init(&mma_done[1], 1);
+        umma::mbar_fence_init();
+    }
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tbase = tmem_base;
+    auto load_bc = [&](int c, int buf) {
+        char* dst = bcb + buf * bc_buf;
+        umma::mbar_expect_tx(&bc_full[buf], bc_buf);
+        umma::bulk_g2s(dst, (const char*)P.bc_hi + (size_t)c * bc_hi_bytes, bc_hi_bytes, &bc_full[buf]);
+        umma::bulk_g2s(dst + bc_hi_bytes, (const char*)P.bc_lo + (size_t)c * bc_lo_bytes, bc_lo_bytes, &bc_full[buf]);
+    };
+    const char* src = P.a2 + (size_t)blockIdx.x * a2_tile_bytes(K1);
+    if (t == 0) {
+        umma::mbar_expect_tx(&a2_full, (uint32_t)(4 * arr));
+        for (int q = 0; q < 4; ++q) umma::bulk_g2s(A2 + q * arr, src + q * arr, (uint32_t)arr, &a2_full);
+        load_bc(0, 0);
+        if (NCH > 1) load_bc(1, 1);
+    }
+    const uint32_t lbo_mn = (128 / 8) * 128, kstep_mn = 2 * lbo_mn, sbo_k = (K1 / 8) * 128;
+    const uint32_t id4 = umma::idesc_f16(128, 4 * IC, true, false);
+    const uint32_t id2 = umma::idesc_f16(128, 2 * IC, true, false);
+    auto issue = [&](int c) {
+        const int buf = NCH > 1 ? (c & 1) : 0;
+        if (c == 0) umma::mbar_wait(&a2_full, 0, P.err);
+        umma::mbar_wait(&bc_full[buf], (c >> 1) & 1, P.err);
+        umma::fence_after_sync();
+        const uint32_t bhi = umma::smem_u32(bcb + buf * bc_buf), blo = bhi + bc_hi_bytes;
+        const uint32_t ahi = umma::smem_u32(A2), alo = ahi + arr, ay = ahi + 2 * arr, az = ahi + 3 * arr;
+        const uint32_t td = tbase + buf * 256;
+        mma_chain(td, ahi, lbo_mn, 128, kstep_mn, bhi, 128, sbo_k, 256, K1, id4, false);
+        mma_chain(td, ahi, lbo_mn, 128, kstep_mn, blo, 128, sbo_k, 256, K1, id2, true);
+        mma_chain(td, alo, lbo_mn, 128, kstep_mn, bhi, 128, sbo_k, 256, K1, id2, true);
+        mma_chain(td + 4 * IC, ay, lbo_mn, 128, kstep_mn, bhi, 128, sbo_k, 256, K1, id2, false);
+        mma_chain(td + 6 * IC, az, lbo_mn, 128, kstep_mn, bhi, 128, sbo_k, 256, K1, id2, false);
+        umma::mma_commit(&mma_done[buf]);
+    };
+    if (t == 0) issue(0);
+    char* a3t = P.a3 + (size_t)blockIdx.x * a3_tile_bytes(W);
+    const size_t arr3 = (size_t)128 * W * 2;
+    for (int c = 0; c < NCH; ++c) {
+        const int buf = NCH > 1 ? (c & 1) : 0;
+        if (t == 0 && c + 1 < NCH) issue(c + 1);
+        umma::mbar_wait(&mma_done[buf], (c >> 1) & 1, P.err);
+        umma::fence_after_sync();
+        const uint32_t col0 = buf * 256;
+        for (int h = 0; h < IC; h += 16) {
+            float er[16], ei[16], xr[16], xi[16];
+            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 0 * IC + h), er);
+            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 1 * IC + h), ei);
+            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 2 * IC + h), xr);
+            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 3 * IC + h), xi);
+            float I0[16], I1[16];
+#pragma unroll
+            for (int u = 0; u < 16; ++u) {
+                I0[u] = (er[u] * er[u] + ei[u] * ei[u]) * P.sc.cI;
+                I1[u] = (er[u] * xr[u] + ei[u] * xi[u]) * P.sc.cIx;
+            }
+            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 4 * IC + h), xr);
+            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 5 * IC + h), xi);
+            float I2[16];
+#pragma unroll
+            for (int u = 0; u < 16; ++u) I2[u] = (er[u] * xr[u] + ei[u] * xi[u]) * P.sc.cIy;
+            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 6 * IC + h), xr);
+            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 7 * IC + h), xi);
+            float I3[16];
+#pragma unroll
+            for (int u = 0; u < 16; ++u) I3[u] = (er[u] * xr[u] + ei[u] * xi[u]) * P.sc.cIz;
+            for (int i8 = 0; i8 < 16; i8 += 8) {
+                const int i = c * IC + h + i8;
+                __half hh[8], ll[8], dx[8], dy[8], dz[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    umma::split_f16(I0[i8 + u], hh[u], ll[u]);
+                    dx[u] = __float2half_rn(I1[i8 + u]);
+                    dy[u] = __float2half_rn(I2[i8 + u]);
+                    dz[u] = __float2half_rn(I3[i8 + u]);
+                }
+                const uint32_t off = kmajor_off(t, i, W);
+                store8h(a3t + 0 * arr3 + off, hh);
+                store8h(a3t + 1 * arr3 + off, ll);
+                store8h(a3t + 2 * arr3 + off, dx);
+                store8h(a3t + 3 * arr3 + off, dy);
+                store8h(a3t + 4 * arr3 + off, dz);
+            }
+        }
+        umma::fence_before_sync();
+        __syncthreads();
+        if (t == 0 && c + 2 < NCH) load_bc(c + 2, buf);
+    }
+    __syncthreads();
+    if (t < 32) umma::tmem_dealloc(tbase, ncols);
+}
+
+// ----------------------------------------------------------- stage 3 -------
+// Blur along the first image index: J^T[(g2, j)][i'] = sum_i I[j][i] G[i'][i].
+__global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage3(SplitDev P) {
+    extern __shared__ __align__(1024) char smem[];
+    const int W = P.W, RP = P.RP, t = threadIdx.x;
+    const size_t arr3 = (size_t)128 * W * 2, gbytes = (size_t)RP * W * 2;
+    char* A3 = smem;
+    char* GT = A3 + 5 * arr3;  // hi, lo
+    __shared__ __align__(8) uint64_t full, done;
+    __shared__ uint32_t tmem_base;
+    const int ncols = tmem_cols_pow2(4 * RP);
+    if (t < 32) umma::tmem_alloc(&tmem_base, ncols);
+    if (t == 0) {
+        umma::mbar_init(&full, 1);
+        umma::mbar_init(&done, 1);
+        umma::mbar_fence_init();
+    }
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tbase = tmem_base;
+    if (t == 0) {
+        umma::mbar_expect_tx(&full, (uint32_t)(5 * arr3 + 2 * gbytes));
+        const char* src = P.a3 + (size_t)blockIdx.x * a3_tile_bytes(W);
+        for (int q = 0; q < 5; ++q) umma::bulk_g2s(A3 + q * arr3, src + q * arr3, (uint32_t)arr3, &full);
+        umma::bulk_g2s(GT, P.gt_hi, (uint32_t)gbytes, &full);
+        umma::bulk_g2s(GT + gbytes, P.gt_lo, (uint32_t)gbytes, &full);
+        umma::mbar_wait(&full, 0, P.err);
+        umma::fence_after_sync();
+        const uint32_t sbo = (W / 8) * 128;
+        const uint32_t id = umma::idesc_f16(128, RP, false, false);
+        const uint32_t a0 = umma::smem_u32(A3), ghi = umma::smem_u32(GT), glo = ghi + (uint32_t)gbytes;
+        mma_chain(tbase, a0, 128, sbo, 256, ghi, 128, sbo, 256, W, id, false);
+        mma_chain(tbase, a0, 128, sbo, 256, glo, 128, sbo, 256, W, id, true);
+        mma_chain(tbase, a0 + (uint32_t)arr3, 128, sbo, 256, ghi, 128, sbo, 256, W, id, true);
+        for (int m = 1; m < 4; ++m)
+            mma_chain(tbase + m * RP, a0 + (uint32_t)((m + 1) * arr3), 128, sbo, 256, ghi, 128, sbo, 256, W, id, false);
+        umma::mma_commit(&done);
+    }
+    umma::mbar_wait(&done, 0, P.err);
+    umma::fence_after_sync();
+    // epilogue: thread row m = (g2, j) -> A4 column k = j of the slot's (map, i') rows
+    const int g2 = t / W, j = t % W;
+    const int slot = blockIdx.x * P.G2 + g2;
+    char* a4s = P.a4 + (size_t)slot * P.NT4 * a4_tile_bytes(W);
+    const size_t arr4 = (size_t)128 * W * 2;
+    for (int m = 0; m < 4; ++m)
+        for (int h = 0; h < RP; h += 16) {
+            float v[16];
+            umma::tmem_ld16(tmem_lane_addr(tbase, m * RP + h), v);
+            for (int i8 = 0; i8 < 16; i8 += 8) {
+                const int r = m * RP + h + i8;
+                char* tile = a4s + (size_t)(r / 128) * a4_tile_bytes(W);
+                __half hh[8], ll[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) umma::split_f16(v[i8 + u] * P.sc.cJ[m], hh[u], ll[u]);
+                const uint32_t off = mnmajor_off(r % 128, j, 128);
+                store8h(tile + off, hh);
+                store8h(tile + arr4 + off, ll);
+            }
+        }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (t < 32) umma::tmem_dealloc(tbase, ncols);
+}
+
+// ----------------------------------------------------------- stage 4 -------
+// Blur along the second index: T[(map, i')][j'] = sum_j J[i'][j] G[j'][j].
+__global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage4(SplitDev P) {
+    extern __shared__ __align__(1024) char smem[];
+    const int W = P.W, RP = P.RP, R = P.R, t = threadIdx.x;
+    const size_t arr4 = (size_t)128 * W * 2, gbytes = (size_t)RP * W * 2;
+    char* A4 = smem;  // hi, lo
+    char* GT = A4 + 2 * arr4;
+    __shared__ __align__(8) uint64_t full, done;
+    __shared__ uint32_t tmem_base;
+    const int ncols = tmem_cols_pow2(RP);
+    if (t < 32) umma::tmem_alloc(&tmem_base, ncols);
+    if (t == 0) {
+        umma::mbar_init(&full, 1);
+        umma::mbar_init(&done, 1);
+        umma::mbar_fence_init();
+    }
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tbase = tmem_base;
+    const int slot = blockIdx.x / P.NT4, tile = blockIdx.x % P.NT4;
+    if (t == 0) {
+        umma::mbar_expect_tx(&full, (uint32_t)(2 * arr4 + 2 * gbytes));
+        const char* src = P.a4 + (size_t)blockIdx.x * a4_tile_bytes(W);
+        umma::bulk_g2s(A4, src, (uint32_t)(2 * arr4), &full);
+        umma::bulk_g2s(GT, P.gt_hi, (uint32_t)gbytes, &full);
+        umma::bulk_g2s(GT + gbytes, P.gt_lo, (uint32_t)gbytes, &full);
+        umma::mbar_wait(&full, 0, P.err);
+        umma::fence_after_sync();
+        const uint32_t lbo_mn = (128 / 8) * 128, kstep_mn = 2 * lbo_mn, sbo_k = (W / 8) * 128;
+        const uint32_t id = umma::idesc_f16(128, RP, true, false);
+        const uint32_t ahi = umma::smem_u32(A4), alo = ahi + (uint32_t)arr4;
+        const uint32_t ghi = umma::smem_u32(GT), glo = ghi + (uint32_t)gbytes;
+        mma_chain(tbase, ahi, lbo_mn, 128, kstep_mn, ghi, 128, sbo_k, 256, W, id, false);
+        mma_chain(tbase, ahi, lbo_mn, 128, kstep_mn, glo, 128, sbo_k, 256, W, id, true);
+        mma_chain(tbase, alo, lbo_mn, 128, kstep_mn, ghi, 128, sbo_k, 256, W, id, true);
+        umma::mma_commit(&done);
+    }
+    umma::mbar_wait(&done, 0, P.err);
+    umma::fence_after_sync();
+    const int r = tile * 128 + t, map = r / RP, ip = r % RP;
+    for (int h = 0; h < RP; h += 16) {
+        float v[16];
+        umma::tmem_ld16(tmem_lane_addr(tbase, h), v);
+        if (map < 4 && ip < R) {
+            float* dst = P.tmaps + (((size_t)slot * 4 + map) * R + ip) * R;
+            for (int u = 0; u < 16 && h + u < R; ++u) dst[h + u] = v[u] * P.sc.cT[map];
+        }
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (t < 32) umma::tmem_dealloc(tbase, ncols);
+}
+
+// ----------------------------------------------------------- stage 5 -------
+constexpr int NRED = 1 + 5 + 15 + 15;
+
+__device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
+    float y = v - c;
+    float t2 = s + y;
+    c = (t2 - s) - y;
+    s = t2;
+}
+
+template <int NV>
+__device__ inline void block_sum_pairs(float (&s)[NV], float (&c)[NV], double* red, double* out) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double x = (double)s[k] - (double)c[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) red[warp * NV + k] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < NV) {
+        double v = 0;
+        for (int w = 0; w < SPLIT_THREADS / 32; ++w) v += red[w * NV + threadIdx.x];
+        out[threadIdx.x] = v;
+    }
+    __syncthreads();
+}
+
+// One CTA per slot: likelihood sums at the trial point, then the FP64 LM step.
+__global__ void __launch_bounds__(SPLIT_THREADS) k_stage5(SplitDev P, const float* rois, const double* init, int n,
+                                                          FitParamsDev prm, double* out5, double* crlb5,
+                                                          double* nll_out, int* st_out, int* it_out) {
+    __shared__ double red[4 * NRED];
+    __shared__ double tot[NRED];
+    const int slot = blockIdx.x, R = P.R, RR = R * R, t = threadIdx.x;
+    const int roi = P.slot_roi[slot];
+    if (roi < 0) return;
+    const float* T0 = P.tmaps + (size_t)slot * 4 * RR;
+    const float* d = rois + (size_t)roi * RR;
+    // normalisation sums
+    float ns[4] = {0, 0, 0, 0}, nc[4] = {0, 0, 0, 0};
+    for (int k = t; k < RR; k += SPLIT_THREADS) {
+        const float v = T0[k];
+        const float sg = v < 0 ? -1.f : 1.f;
+        kahan_add(ns[0], nc[0], fabsf(v));
+        kahan_add(ns[1], nc[1], sg * T0[RR + k]);
+        kahan_add(ns[2], nc[2], sg * T0[2 * RR + k]);
+        kahan_add(ns[3], nc[3], sg * T0[3 * RR + k]);
+    }
+    block_sum_pairs<4>(ns, nc, red, tot);
+    const float S = (float)tot[0], Dx = (float)tot[1], Dy = (float)tot[2], Dz = (float)tot[3];
+    const float invS = 1.f / S;
+    const double* th = P.lm[slot].trial;
+    const float A = (float)th[3], B = (float)th[4];
+    float s[NRED], c[NRED];
+#pragma unroll
+    for (int k = 0; k < NRED; ++k) { s[k] = 0.f; c[k] = 0.f; }
+    bool bad = false;
+    for (int k = t; k < RR; k += SPLIT_THREADS) {
+        const float v = T0[k];
+        const float sg = v < 0 ? -1.f : 1.f;
+        const float psi = fabsf(v) * invS;
+        float j[5];
+        j[0] = A * (sg * T0[RR + k] - psi * Dx) * invS;
+        j[1] = A * (sg * T0[2 * RR + k] - psi * Dy) * invS;
+        j[2] = A * (sg * T0[3 * RR + k] - psi * Dz) * invS;
+        j[3] = psi;
+        j[4] = 1.f;
+        const float mu = A * psi + B;
+        if (!(mu > 0.f)) { bad = true; continue; }
+        const float dk = d[k];
+        kahan_add(s[0], c[0], dk > 0.f ? mu - dk - dk * logf(mu / dk) : mu);
+        const float wg = 1.f - dk / mu, wf = 1.f / mu, wh = dk * wf * wf;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) kahan_add(s[1 + q], c[1 + q], wg * j[q]);
+        int o = 6;
+#pragma unroll
+        for (int q = 0; q < 5; ++q)
+#pragma unroll
+            for (int r2 = 0; r2 <= q; ++r2) {
+                kahan_add(s[o], c[o], wh * j[q] * j[r2]);
+                kahan_add(s[o + 15], c[o + 15], wf * j[q] * j[r2]);
+                ++o;
+            }
+    }
+    if (bad) s[0] = INFINITY;
+    block_sum_pairs<NRED>(s, c, red, tot);
+    if (t != 0) return;
+    double nll = tot[0], g[5], H[25], F[25];
+    for (int q = 0; q < 5; ++q) g[q] = tot[1 + q];
+    int o = 6;
+    for (int q = 0; q < 5; ++q)
+        for (int r2 = 0; r2 <= q; ++r2) {
+            H[q * 5 + r2] = H[r2 * 5 + q] = tot[o];
+            F[q * 5 + r2] = F[r2 * 5 + q] = tot[o + 15];
+            ++o;
+        }
+    LMState& st = P.lm[slot];
+    if (P.slot_phase[slot] == 0) {
+        for (int q = 0; q < 5; ++q) st.th[q] = st.trial[q];
+        lm_start(st, nll, g, H, F);
+        P.slot_phase[slot] = 1;
+    } else {
+        lm_update(st, nll, g, H, F, prm);
+    }
+    if (lm_propose(st, prm)) return;
+    // retire
+    for (int q = 0; q < 5; ++q) out5[5 * roi + q] = st.th[q];
+    if (nll_out) nll_out[roi] = st.nll;
+    if (st_out) st_out[roi] = st.status;
+    if (it_out) it_out[roi] = st.evals;
+    if (crlb5) lm_crlb(st.F, crlb5 + 5 * roi);
+    // refill from the queue
+    const int next = atomicAdd(P.queue, 1);
+    if (next < n) {
+        P.slot_roi[slot] = next;
+        P.slot_phase[slot] = 0;
+        for (int q = 0; q < 5; ++q) st.trial[q] = init[5 * next + q];
+        lm_clamp(st.trial, prm);
+    } else {
+        P.slot_roi[slot] = -1;
+        atomicSub(P.active, 1);
+    }
+}
+
+// Fill the pool from the queue.
+__global__ void k_init_slots(SplitDev P, const double* init, int n, FitParamsDev prm) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= P.P) return;
+    if (slot < n) {
+        P.slot_roi[slot] = slot;
+        P.slot_phase[slot] = 0;
+        for (int q = 0; q < 5; ++q) P.lm[slot].trial[q] = init[5 * slot + q];
+        lm_clamp(P.lm[slot].trial, prm);
+    } else {
+        P.slot_roi[slot] = -1;
+    }
+    if (slot == 0) {
+        *P.queue = P.P < n ? P.P : n;
+        *P.active = P.P < n ? P.P : n;
+        *P.err = 0;
+    }
+}
+
+// ---------------------------------------------------------------- host -----
+static size_t smem_stage1(const SplitPlanHost& pl) { return (size_t)768 * pl.K1 + 2 * (size_t)12 * pl.IC * pl.K1; }
+static size_t smem_stage2(const SplitPlanHost& pl) { return (size_t)1024 * pl.K1 + 2 * (size_t)12 * pl.IC * pl.K1; }
+static size_t smem_stage3(const SplitPlanHost& pl) { return (size_t)5 * 128 * pl.W * 2 + (size_t)4 * pl.RP * pl.W; }
+static size_t smem_stage4(const SplitPlanHost& pl) { return (size_t)2 * 128 * pl.W * 2 + (size_t)4 * pl.RP * pl.W; }
+
+// psi and d psi / d{x,y,z} of every occupied slot from its blurred maps
+// (model-only evaluation through the tensor-core stages).
+__global__ void k_model_out(SplitDev P, int n, double* out, double* dout) {
+    const int slot = blockIdx.x, R = P.R, RR = R * R;
+    if (slot >= n) return;
+    __shared__ float red[4][4];
+    const float* T0 = P.tmaps + (size_t)slot * 4 * RR;
+    float v[4] = {0, 0, 0, 0};
+    for (int k = threadIdx.x; k < RR; k += blockDim.x) {
+        float t0 = T0[k], sg = t0 < 0 ? -1.f : 1.f;
+        v[0] += fabsf(t0);
+        v[1] += sg * T0[RR + k];
+        v[2] += sg * T0[2 * RR + k];
+        v[3] += sg * T0[3 * RR + k];
+    }
+    for (int q = 0; q < 4; ++q)
+        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+    if ((threadIdx.x & 31) == 0)
+        for (int q = 0; q < 4; ++q) red[threadIdx.x >> 5][q] = v[q];
+    __syncthreads();
+    float S = 0, D3[3] = {0, 0, 0};
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+        S += red[w][0];
+        for (int q = 0; q < 3; ++q) D3[q] += red[w][q + 1];
+    }
+    for (int k = threadIdx.x; k < RR; k += blockDim.x) {
+        float t0 = T0[k], sg = t0 < 0 ? -1.f : 1.f, psi = fabsf(t0) / S;
+        out[(size_t)slot * RR + k] = psi;
+        if (dout)
+            for (int q = 0; q < 3; ++q)
+                dout[((size_t)slot * 3 + q) * RR + k] = (sg * T0[(q + 1) * RR + k] - psi * D3[q]) / S;
+    }
+}
+
+// Slots evaluate the given (x, y, z) points (model-only use of the pool).
+__global__ void k_init_points(SplitDev P, const double* xyz, int n) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= P.P) return;
+    if (slot < n) {
+        P.slot_roi[slot] = slot;
+        for (int q = 0; q < 3; ++q) P.lm[slot].trial[q] = xyz[3 * slot + q];
+        P.lm[slot].trial[3] = 1.0;
+        P.lm[slot].trial[4] = 0.0;
+    } else {
+        P.slot_roi[slot] = -1;
+    }
+    if (slot == 0) *P.err = 0;
+}
+
+struct SplitPool {
+    SplitPlanHost* pl = nullptr;
+    SplitDev D{};
+    size_t s1 = 0, s2 = 0, s3 = 0, s4 = 0;
+};
+
+static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pmax_override, SplitPool& sp,
+                      cudaStream_t st) {
+    if (p->D > 64) {
+        ctx->err = "split path: pupil disk wider than 64 rows (grid too large for this optics)";
+        return ZOLA_E_UNSUPPORTED;
+    }
+    if (w->W < 32 || w->R > 64) {
+        ctx->err = "split path supports windows W >= 32 and ROI sides up to 64";
+        return ZOLA_E_UNSUPPORTED;
+    }
+    SplitPlanHost* pl = get_plan(p, w, ctx->err);
+    if (!pl) return ZOLA_E_CUDA;
+    sp.pl = pl;
+    sp.s1 = smem_stage1(*pl); sp.s2 = smem_stage2(*pl); sp.s3 = smem_stage3(*pl); sp.s4 = smem_stage4(*pl);
+    if (sp.s1 > 227 * 1024 || sp.s2 > 227 * 1024 || sp.s3 > 227 * 1024 || sp.s4 > 227 * 1024) {
+        ctx->err = "split path: shared-memory plan exceeds 227 KB";
+        return ZOLA_E_UNSUPPORTED;
+    }
+    const size_t per_slot = a2_tile_bytes(pl->K1) / pl->G2 + a3_tile_bytes(pl->W) / pl->G2 +
+                            (size_t)pl->NT4 * a4_tile_bytes(pl->W) + (size_t)4 * pl->R * pl->R * 4 + sizeof(LMState) + 16;
+    int Pmax = (int)std::min<size_t>(32768, ((size_t)3 << 30) / per_slot);
+    if (pmax_override > 0) Pmax = std::min(Pmax, pmax_override);
+    Pmax = std::max(4, Pmax / 4 * 4);
+    const int P = std::min(Pmax, (n + 3) / 4 * 4);
+    auto al = [](size_t v) { return (v + 1023) / 1024 * 1024; };
+    const size_t b_a2 = al((size_t)(P / pl->G2) * a2_tile_bytes(pl->K1));
+    const size_t b_a3 = al((size_t)(P / pl->G2) * a3_tile_bytes(pl->W));
+    const size_t b_a4 = al((size_t)P * pl->NT4 * a4_tile_bytes(pl->W));
+    const size_t b_t = al((size_t)P * 4 * pl->R * pl->R * 4);
+    const size_t b_lm = al((size_t)P * sizeof(LMState));
+    const size_t b_int = al((size_t)P * 8 + 64);
+    if (ensure_scratch(ctx, b_a2 + b_a3 + b_a4 + b_t + b_lm + b_int, ctx->err)) return ZOLA_E_CUDA;
+    char* base = (char*)ctx->scratch;
+    SplitDev& D = sp.D;
+    D = SplitDev{};
+    D.R = pl->R; D.W = pl->W; D.D = pl->D; D.DP = pl->DP; D.K1 = pl->K1; D.IC = pl->IC; D.NCH = pl->NCH;
+    D.RP = pl->RP; D.G1 = pl->G1; D.G2 = pl->G2; D.NT4 = pl->NT4; D.P = P; D.a0 = p->a0; D.N = p->N;
+    D.zfocus = p->o.zfocus;
+    D.bc_hi = pl->d_bc_hi; D.bc_lo = pl->d_bc_lo; D.gt_hi = pl->d_gt_hi; D.gt_lo = pl->d_gt_lo;
+    D.pupil = p->view.pupil; D.phase0 = pl->d_phase0; D.kz = p->view.kz; D.kx = p->view.kx; D.ky = p->view.ky;
+    D.a2 = base; base += b_a2;
+    D.a3 = base; base += b_a3;
+    D.a4 = base; base += b_a4;
+    D.tmaps = (float*)base; base += b_t;
+    D.lm = (LMState*)base; base += b_lm;
+    D.slot_roi = (int*)base;
+    D.slot_phase = D.slot_roi + P;
+    D.queue = D.slot_phase + P;
+    D.active = D.queue + 1;
+    D.err = D.queue + 2;
+    D.sc = pl->sc;
+    ZOLA_CUDA_CHECK(cudaMemsetAsync(D.a4, 0, b_a4, st), ctx);
+    ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_stage1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.s1), ctx);
+    ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_stage2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.s2), ctx);
+    ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_stage3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.s3), ctx);
+    ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_stage4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.s4), ctx);
+    return ZOLA_OK;
+}
+
+static void launch_model_stages(zola_ctx* ctx, const SplitPool& sp, cudaStream_t st) {
+    const SplitPlanHost& pl = *sp.pl;
+    const int P = sp.D.P;
+    k_stage1<<<P / pl.G1, SPLIT_THREADS, sp.s1, st>>>(sp.D);
+    k_stage2<<<P / pl.G2, SPLIT_THREADS, sp.s2, st>>>(sp.D);
+    k_stage3<<<P / pl.G2, SPLIT_THREADS, sp.s3, st>>>(sp.D);
+    k_stage4<<<P * pl.NT4, SPLIT_THREADS, sp.s4, st>>>(sp.D);
+    ctx->launches += 4;
+}
+
+static int read_flags(zola_ctx* ctx, const SplitDev& D, cudaStream_t st, int* active, int* err) {
+    if (!ctx->h_flags) ZOLA_CUDA_CHECK(cudaMallocHost(&ctx->h_flags, 4 * sizeof(int)), ctx);
+    ZOLA_CUDA_CHECK(cudaMemcpyAsync(ctx->h_flags, D.active, 2 * sizeof(int), cudaMemcpyDeviceToHost, st), ctx);
+    ZOLA_CUDA_CHECK(cudaStreamSynchronize(st), ctx);
+    *active = ctx->h_flags[0];
+    *err = ctx->h_flags[1];
+    return ZOLA_OK;
+}
+
+int launch_model_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const double* d_xyz, int n, double* d_out,
+                       double* d_dout, cudaStream_t st) {
+    for (int done = 0; done < n;) {
+        SplitPool sp;
+        int rc = setup_pool(ctx, p, w, n - done, 0, sp, st);
+        if (rc) return rc;
+        const int m = std::min(sp.D.P, n - done);
+        k_init_points<<<(sp.D.P + 127) / 128, 128, 0, st>>>(sp.D, d_xyz + 3 * (size_t)done, m);
+        launch_model_stages(ctx, sp, st);
+        const size_t RR = (size_t)w->R * w->R;
+        k_model_out<<<m, 128, 0, st>>>(sp.D, m, d_out + RR * done, d_dout ? d_dout + 3 * RR * done : nullptr);
+        ctx->launches += 2;
+        ZOLA_CUDA_CHECK(cudaGetLastError(), ctx);
+        int active, err;
+        rc = read_flags(ctx, sp.D, st, &active, &err);
+        if (rc) return rc;
+        if (err) { ctx->err = "split model: a bounded device wait timed out"; return ZOLA_E_TIMEOUT; }
+        done += m;
+    }
+    return ZOLA_OK;
+}
+
+int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_rois, const double* d_init, int n,
+                     const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll, int* d_status,
+                     int* d_iters, cudaStream_t st) {
+    SplitPool sp;
+    int rc = setup_pool(ctx, p, w, n, ctx->split_pool_max, sp, st);
+    if (rc) return rc;
+    const SplitDev& D = sp.D;
+    const int P = D.P;
+    FitParamsDev fp{prm->zmin, prm->zmax, prm->xymax, prm->tol_xyz, prm->step_xy, prm->step_z, prm->max_iter};
+    k_init_slots<<<(P + 127) / 128, 128, 0, st>>>(D, d_init, n, fp);
+    ctx->launches++;
+    ZOLA_CUDA_CHECK(cudaGetLastError(), ctx);
+    const int max_rounds = (prm->max_iter + 2) * ((n + P - 1) / P + 1) + 8;
+    int rounds = 0;
+    while (true) {
+        for (int k = 0; k < 4; ++k) {
+            launch_model_stages(ctx, sp, st);
+            k_stage5<<<P, SPLIT_THREADS, 0, st>>>(D, d_rois, d_init, n, fp, d_out5, d_crlb5, d_nll, d_status, d_iters);
+            ctx->launches++;
+        }
+        rounds += 4;
+        ZOLA_CUDA_CHECK(cudaGetLastError(), ctx);
+        int active, err;
+        rc = read_flags(ctx, D, st, &active, &err);
+        if (rc) return rc;
+        if (err) { ctx->err = "split fit: a bounded device wait timed out"; return ZOLA_E_TIMEOUT; }
+        if (active <= 0) break;
+        if (rounds > max_rounds) { ctx->err = "split fit: did not drain the ROI queue"; return ZOLA_E_TIMEOUT; }
+    }
+    return ZOLA_OK;
 }
 
 }  // namespace zola

@@ -1,0 +1,151 @@
+// Thin inline-PTX layer for the sm_100a tensor-core path: UMMA (tcgen05.mma)
+// shared-memory descriptors, instruction descriptors, TMEM allocation and
+// loads, mbarriers and 1-D bulk (TMA) copies.  Descriptor bit layouts follow
+// the public PTX ISA for tcgen05 (the same fields CUTLASS's
+// cute/arch/mma_sm100_desc.hpp names).
+//
+// Operand tiles are stored in the canonical no-swizzle ("interleaved") layout
+// made of 8 x 16-byte core matrices (8 rows of 8 f16 values, 128 contiguous
+// bytes):
+//   K-major  (rows = M or N, K contiguous inside a core matrix):
+//     byte(r, k) = ((r/8) * (K/8) + k/8) * 128 + (r%8) * 16 + (k%8) * 2
+//     LBO (K-direction core stride) = 128, SBO (row-direction core stride) = (K/8)*128
+//   MN-major (8 consecutive rows contiguous inside a 16-byte unit):
+//     byte(r, k) = ((k/8) * (MN/8) + r/8) * 128 + (k%8) * 16 + (r%8) * 2
+//     LBO (K-direction core stride) = (MN/8)*128, SBO (row-direction core stride) = 128
+// One kind::f16 MMA consumes K = 16, i.e. two core matrices along K.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cstdint>
+
+namespace zola {
+namespace umma {
+
+__host__ __device__ constexpr uint32_t kmajor_off(uint32_t r, uint32_t k, uint32_t K) {
+    return ((r >> 3) * (K >> 3) + (k >> 3)) * 128u + (r & 7u) * 16u + (k & 7u) * 2u;
+}
+__host__ __device__ constexpr uint32_t mnmajor_off(uint32_t r, uint32_t k, uint32_t MN) {
+    return ((k >> 3) * (MN >> 3) + (r >> 3)) * 128u + (k & 7u) * 16u + (r & 7u) * 2u;
+}
+
+// Shared-memory matrix descriptor, SWIZZLE_NONE, version 1 (sm_100).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1u << 46;  // descriptor version for tcgen05
+    return d;                 // base offset 0, legacy LBO mode, layout type 0 (no swizzle)
+}
+
+// Instruction descriptor for kind::f16 with f16 A/B and f32 accumulation.
+__host__ __device__ constexpr uint32_t idesc_f16(int M, int N, bool a_mn_major, bool b_mn_major) {
+    return (1u << 4)                              // D format: f32
+           | (0u << 7) | (0u << 10)               // A, B format: f16
+           | ((a_mn_major ? 1u : 0u) << 15)
+           | ((b_mn_major ? 1u : 0u) << 16)
+           | ((uint32_t)(N >> 3) << 17)
+           | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                        uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+        :
+        : "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 :
+                 : "r"(smem_u32(mbar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// TMEM allocation by one full warp; the allocated base address lands in *dst.
+__device__ __forceinline__ void tmem_alloc(uint32_t* dst, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :
+                 : "r"(smem_u32(dst)), "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+// 32 lanes x 32 bit, 16 consecutive columns per thread.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* mbar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* mbar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)), "r"(bytes)
+                 : "memory");
+}
+
+// Bounded wait on an mbarrier phase: gives up after ~2^31 clocks (about a
+// second) and raises *err so the host can report ZOLA_E_TIMEOUT.
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, int* err) {
+    uint32_t addr = smem_u32(mbar);
+    long long t0 = clock64();
+    while (true) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}\n"
+            : "=r"(done)
+            : "r"(addr), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > (1ll << 31)) {
+            if (err) atomicExch(err, 1);
+            return false;
+        }
+    }
+}
+
+// 1-D bulk copy global -> shared, completion tracked on mbar (no multicast).
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* mbar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        :
+        : "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(mbar))
+        : "memory");
+}
+
+// Split x into hi + lo halves (x ~= hi + lo to about 2^-22 relative).
+__device__ __forceinline__ void split_f16(float x, __half& hi, __half& lo) {
+    hi = __float2half_rn(x);
+    lo = __float2half_rn(x - __half2float(hi));
+}
+
+}  // namespace umma
+}  // namespace zola

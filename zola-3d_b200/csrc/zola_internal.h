@@ -69,6 +69,8 @@ struct zola_ctx {
     size_t scratch_bytes = 0;
     int* d_counter = nullptr;
     int* d_status_word = nullptr;
+    int* h_flags = nullptr;      // pinned host words read back by the split fit loop
+    int split_pool_max = 0;      // 0: size the split slot pool automatically
 };
 
 struct zola_psf {
@@ -98,6 +100,9 @@ int launch_fit_f64(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_r
                    int* d_status, int* d_iters, cudaStream_t st);
 
 // fit_split.cu
+int launch_model_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const double* d_xyz, int n, double* d_out,
+                       double* d_dout, cudaStream_t st);
+void free_split_plan(void* plan);
 int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_rois, const double* d_init,
                      int n, const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll,
                      int* d_status, int* d_iters, cudaStream_t st);
