@@ -1,0 +1,476 @@
+"""Benchmark: batched mixed-size Poisson MLE fits (split precision vs plain FP64 GPU).
+
+Workload (one step): 1,000,000 synthetic ROIs, 50% 16x16 (astigmatic PSF, pupil
+64^2), 30% 24x24 (saddle PSF Z(3,3) = 0.3 lambda, pupil 96^2 rounded to 128^2 as
+the CPU path does), 20% 48x48 (45-mode tetrapod, pupil 128^2); photons
+LogNormal(ln 3000, 0.6), Poisson noise, seed 2 (+ rank).  Every ROI is fitted
+with the 5-parameter Levenberg-Marquardt MLE (max 50 model evaluations) through
+the library's split-precision tcgen05 path; the plain FP64 GPU form of the same
+fit runs on a sample of the same job for the speed-up and the accuracy check.
+
+Usage: python bench.py [--gpus N --steps K --warmup W --impl b200|reference]
+Prints one JSON line (rank 0).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MLE ROI fits/sec at ≤0.5 nm vs FP64 oracle (batched split-prec vs plain GPU)"
+UNIT = "ROI fits/s"
+TWO_PI = 2 * np.pi
+DX = 0.11
+
+
+def zern_astig(rng):
+    z = np.zeros(15)
+    z[5] = 0.08 * TWO_PI
+    for k in (7, 8, 12):
+        z[k] = rng.normal(0, 0.02) * TWO_PI
+    return z
+
+
+def zern_saddle(rng):
+    z = np.zeros(28)
+    z[9] = 0.3 * TWO_PI
+    return z
+
+
+def zern_tetrapod(rng):
+    z = rng.normal(0, 0.02, 45) * TWO_PI
+    z[:3] = 0
+    z[5] = 0.6 * TWO_PI
+    z[13] = 0.3 * TWO_PI
+    z[25] = 0.15 * TWO_PI
+    return z
+
+
+CLASSES = [
+    dict(name="astig16", frac=0.5, R=16, N=64, zern=zern_astig, zr=0.6, bg=20.0, zsym=False),
+    dict(name="saddle24", frac=0.3, R=24, N=128, zern=zern_saddle, zr=1.0, bg=20.0, zsym=True),
+    dict(name="tetra48", frac=0.2, R=48, N=128, zern=zern_tetrapod, zr=2.0, bg=30.0, zsym=False),
+]
+
+
+def class_counts(n):
+    c = [int(round(n * k["frac"])) for k in CLASSES]
+    c[0] += n - sum(c)
+    return c
+
+
+def disk_rows(N):
+    # disk bounding rows for NA 1.4, lambda 0.66 um, pixel 0.11 um (30 at N=64, 60 at N=128)
+    c = N / 2 - 0.5
+    ring = (1.4 / 0.66) ** 2
+    rows = [i for i in range(N) if ((i - c) / (N * DX)) ** 2 <= ring]
+    return len(rows)
+
+
+def window(R, N):
+    w = min(2 * R, N)
+    p = 1
+    while p < w:
+        p <<= 1
+    return p
+
+
+# ----------------------------------------------------------------- data ----
+def make_job(z, ctx, torch, n, seed, device, only=None):
+    """Synthetic ROIs on the device (FP64 library model + Poisson noise)."""
+    rng = np.random.default_rng(seed)
+    job = []
+    for cls, cnt in zip(CLASSES, class_counts(n)):
+        if only and cls["name"] not in only:
+            continue
+        R, N = cls["R"], cls["N"]
+        zern = cls["zern"](np.random.default_rng(seed * 100 + R))
+        psf = z.PSF(ctx, z.optics(size_fft=N, xystep=DX, na=1.4, wavelength=0.66, n_oil=1.518, sigma=0.9), zern)
+        truth = np.zeros((cnt, 5))
+        truth[:, :2] = rng.uniform(-DX, DX, (cnt, 2))
+        truth[:, 2] = rng.uniform(-cls["zr"], cls["zr"], cnt)
+        truth[:, 3] = rng.lognormal(np.log(3000.0), 0.6, cnt)
+        truth[:, 4] = cls["bg"]
+        rois = torch.empty((cnt, R, R), dtype=torch.float32, device=device)
+        chunk = 1 << 16
+        gen = torch.Generator(device=device)
+        gen.manual_seed(seed * 1000 + R)
+        for s in range(0, cnt, chunk):
+            e = min(cnt, s + chunk)
+            xyz = torch.tensor(truth[s:e, :3], dtype=torch.float64, device=device)
+            psi = torch.empty((e - s, R, R), dtype=torch.float64, device=device)
+            psf.model_dev(R, xyz, psi, stream=torch.cuda.current_stream().cuda_stream)
+            torch.cuda.synchronize()
+            a = torch.tensor(truth[s:e, 3], dtype=torch.float64, device=device)[:, None, None]
+            mu = a * psi + cls["bg"]
+            rois[s:e] = torch.poisson(mu, generator=gen).float()
+        # initial values: x = y = 0 (ROI centre), z on the 100 nm library grid,
+        # B from the ROI border, A from the background-subtracted sum
+        init = np.zeros((cnt, 5))
+        init[:, 2] = np.round(truth[:, 2] / 0.1) * 0.1
+        border = torch.cat([rois[:, 0, :], rois[:, -1, :], rois[:, 1:-1, 0], rois[:, 1:-1, -1]], dim=1)
+        b = border.mean(dim=1).double()
+        a = (rois.double().sum(dim=(1, 2)) - b * R * R).clamp(min=100.0)
+        init[:, 3] = a.cpu().numpy()
+        init[:, 4] = b.cpu().numpy()
+        # tol 1e-4 um: the reference's stopping distance (Localization.java:31), here on the Newton step
+        prm_kw = dict(zmin=-cls["zr"] - 0.3, zmax=cls["zr"] + 0.3, xymax=R * DX / 2, max_iter=50, tol_xyz=1e-4)
+        job.append(dict(cls=cls, psf=psf, zern=zern, truth=truth, rois=rois,
+                        init=torch.tensor(init, dtype=torch.float64, device=device), init_np=init, prm_kw=prm_kw,
+                        out=torch.empty((cnt, 5), dtype=torch.float64, device=device),
+                        crlb=torch.empty((cnt, 5), dtype=torch.float64, device=device),
+                        nll=torch.empty(cnt, dtype=torch.float64, device=device),
+                        status=torch.empty(cnt, dtype=torch.int32, device=device),
+                        iters=torch.empty(cnt, dtype=torch.int32, device=device)))
+    return job
+
+
+def run_step(z, job, precision, stream_ptr, sl=None):
+    for j in job:
+        p = z.PSF.fit_params(precision=precision, **j["prm_kw"])
+        s = sl if sl is not None else slice(None)
+        j["psf"].fit_dev(j["rois"][s], j["init"][s], p, j["out"][s], j["crlb"][s], j["nll"][s], j["status"][s],
+                         j["iters"][s], stream=stream_ptr)
+
+
+# --------------------------------------------------------------- clocks ----
+class ClockSampler:
+    def __init__(self, device):
+        self.p = None
+        self.device = device
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(device), "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                text=True)
+        except (OSError, ValueError):
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+            out, _ = self.p.communicate()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx.append(float(f[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------ baselines ----
+def cpu_baseline(budget_s=15.0, seed=2):
+    """The oracle port of the reference's CPU localisation (coordinate descent,
+    FFT model, Localization.java) on a bounded sample of the workload, all host
+    threads.  Returns fits/s for the job's class mix."""
+    import oracle as O
+    threads = os.cpu_count() or 1
+    per_fit = []
+    counts = []
+    for cls in CLASSES:
+        R, N = cls["R"], cls["N"]
+        zern = cls["zern"](np.random.default_rng(seed * 100 + R))
+        p = O.OraclePSF(N, DX, 1.4, 0.66, 1.518, 1.518, 0.9, zern)
+        rng = np.random.default_rng(seed + 7 * R)
+        n1 = max(threads, 2)
+        truth = np.c_[rng.uniform(-DX, DX, (n1, 2)), rng.uniform(-cls["zr"], cls["zr"], n1),
+                      rng.lognormal(np.log(3000.0), 0.6, n1), np.full(n1, cls["bg"])]
+        rois = rng.poisson(truth[:, 3, None, None] * p.model(R, truth[:, :3]) + cls["bg"]).astype(float)
+        init = np.c_[truth[:, 3] * 0.9, truth[:, 4], np.zeros((n1, 2)), np.round(truth[:, 2] / 0.1) * 0.1]
+        t0 = time.perf_counter()
+        p.localize_cd(rois, init, -cls["zr"] - 0.3, cls["zr"] + 0.3, 20, 0.0, threads=threads)
+        dt = time.perf_counter() - t0
+        per_fit.append(dt / n1)
+        counts.append(n1)
+        if sum(per_fit) * threads > budget_s:
+            break
+    t_job = sum(c["frac"] * t for c, t in zip(CLASSES, per_fit)) / sum(c["frac"] for c in CLASSES[:len(per_fit)])
+    sample = ", ".join(f"{n} {c['name']}" for c, n in zip(CLASSES, counts))
+    return 1.0 / t_job, threads, sample
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    vals = []
+    for i in range(args.warmup + args.steps):
+        v, cores, sample = cpu_baseline(budget_s=args.cpu_seconds, seed=2 + i)
+        if i >= args.warmup:
+            vals.append(v)
+    v = float(np.median(vals))
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": config_block(args.rois),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"per step: {sample} ROIs fitted by the oracle's restatement of the "
+                                       "reference coordinate-descent localisation (Localization.java), "
+                                       "throughput weighted by the job's class mix"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def config_block(n):
+    return {"workload": "batched mixed-size 5-parameter Poisson MLE ROI fits, split-precision tcgen05 vs plain "
+                        "FP64 GPU", "rois_per_step": n,
+            "mix": "50% 16x16 astigmatic (pupil 64^2), 30% 24x24 saddle Z(3,3)=0.3 lambda (pupil 96^2 -> 128^2 as "
+                   "the CPU path rounds), 20% 48x48 45-mode tetrapod (pupil 128^2)",
+            "photons": "LogNormal(ln 3000, 0.6)", "max_evaluations": 50, "seed": 2,
+            "l2": "inputs larger than L2 (float32 ROIs ~3 GB per step)"}
+
+
+# ----------------------------------------------------------------- main ----
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--rois", type=int, default=1_000_000)
+    ap.add_argument("--fp64-sample", type=int, default=20_000)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--classes", default="", help="comma list of ROI classes to run (profiling); default all")
+    ap.add_argument("--pool", type=int, default=4096, help="max ROIs in flight per fit call (0: library default)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+    import __graft_entry__ as ge
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=device)
+    z = ge.load_package()
+    ctx = z.Context(local)
+    if args.pool:
+        ctx.set_pool(args.pool)
+    ext = torch.cuda.ExternalStream(ctx.stream, device=device)
+    only = [c for c in args.classes.split(",") if c]
+    job = make_job(z, ctx, torch, args.rois, seed=2 + rank, device=device, only=only)
+    n_total = sum(j["rois"].shape[0] for j in job)
+    torch.cuda.synchronize()
+
+    # warm-up (split path), also primes tables and the slot pool
+    for _ in range(args.warmup):
+        run_step(z, job, z.ZOLA_PREC_SPLIT, ctx.stream)
+    ext.synchronize()
+
+    # timed steps (device time on the library stream; max over ranks)
+    ctx.profile(True)
+    ctx.stage_stats(reset=True)
+    l0 = ctx.launches
+    clocks = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(ext)
+    for _ in range(args.steps):
+        run_step(z, job, z.ZOLA_PREC_SPLIT, ctx.stream)
+    ev1.record(ext)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    launches = ctx.launches - l0
+    stats = ctx.stage_stats(reset=True)
+    ctx.profile(False)
+    if world > 1:
+        t = torch.tensor([ms], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    ms_step = ms / args.steps
+    value = n_total * world / (ms_step / 1000.0)
+
+    # per-class split timing (one extra pass outside the timed region)
+    per_class = {}
+    for j in job:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        p = z.PSF.fit_params(precision=z.ZOLA_PREC_SPLIT, **j["prm_kw"])
+        j["psf"].fit_dev(j["rois"], j["init"], p, j["out"], j["crlb"], j["nll"], j["status"], j["iters"],
+                         stream=ctx.stream)
+        e1.record(ext)
+        e1.synchronize()
+        t = e0.elapsed_time(e1) / 1000.0
+        per_class[j["cls"]["name"]] = {"rois": int(j["rois"].shape[0]), "seconds": t,
+                                       "fits_per_s": j["rois"].shape[0] / t,
+                                       "mean_evals": float(j["iters"].double().mean().item())}
+
+    # per-class useful evaluations for the roofline
+    iters = {j["cls"]["name"]: int(j["iters"].sum().item()) for j in job}
+    split_res = {j["cls"]["name"]: (j["out"].cpu().numpy(), j["status"].cpu().numpy()) for j in job}
+
+    # plain FP64 GPU form on a sample of the same job (and the accuracy check)
+    fp64 = {}
+    acc = {"max_dxy_nm": 0.0, "max_dz_nm": 0.0, "max_dA_rel": 0.0, "compared": 0, "converged_frac": 0.0}
+    t_job64 = 0.0
+    conv = []
+    for j in job:
+        cnt = j["rois"].shape[0]
+        m = max(64, int(args.fp64_sample * j["cls"]["frac"]))
+        m = min(m, cnt)
+        sl = slice(0, m)
+        p64 = z.PSF.fit_params(precision=z.ZOLA_PREC_FP64, **j["prm_kw"])
+        out64 = torch.empty((m, 5), dtype=torch.float64, device=device)
+        st64 = torch.empty(m, dtype=torch.int32, device=device)
+        it64 = torch.empty(m, dtype=torch.int32, device=device)
+        # warm-up then timed pass on the library stream
+        j["psf"].fit_dev(j["rois"][:64], j["init"][:64], p64, out64[:64], None, None, st64[:64], it64[:64],
+                         stream=ctx.stream)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        j["psf"].fit_dev(j["rois"][sl], j["init"][sl], p64, out64, None, None, st64, it64, stream=ctx.stream)
+        e1.record(ext)
+        e1.synchronize()
+        t = e0.elapsed_time(e1) / 1000.0
+        t_job64 += t / m * cnt
+        fp64[j["cls"]["name"]] = {"sample": m, "seconds": t, "fits_per_s": m / t}
+        a = out64.cpu().numpy()
+        sa = st64.cpu().numpy()
+        b, sb = split_res[j["cls"]["name"]]
+        b, sb = b[:m], sb[:m]
+        ok = (sa == 1) & (sb == 1)
+        conv.append(ok.mean())
+        d = np.abs(a[ok] - b[ok])
+        if j["cls"]["zsym"]:
+            d[:, 2] = np.abs(np.abs(a[ok, 2]) - np.abs(b[ok, 2]))
+        acc["max_dxy_nm"] = max(acc["max_dxy_nm"], float(d[:, :2].max() * 1000) if ok.any() else 0.0)
+        acc["max_dz_nm"] = max(acc["max_dz_nm"], float(d[:, 2].max() * 1000) if ok.any() else 0.0)
+        acc["max_dA_rel"] = max(acc["max_dA_rel"], float((d[:, 3] / a[ok, 3]).max()) if ok.any() else 0.0)
+        acc["compared"] += int(ok.sum())
+        if ok.any():
+            within = (d[:, :2].max(1) <= 0.5e-3) & (d[:, 2] <= 1e-3) & (d[:, 3] / a[ok, 3] <= 1e-3)
+            acc.setdefault("per_class", {})[j["cls"]["name"]] = {
+                "compared": int(ok.sum()), "within_tolerance": float(within.mean()),
+                "p99_dxy_nm": float(np.percentile(d[:, :2].max(1), 99) * 1000),
+                "p99_dz_nm": float(np.percentile(d[:, 2], 99) * 1000),
+                "p99_dA_rel": float(np.percentile(d[:, 3] / a[ok, 3], 99))}
+    acc["converged_frac"] = float(np.mean(conv))
+    fp64_value = n_total / t_job64
+
+    # roofline of the dominant tensor kernel (algorithmic flops: complex MAC = 8 flops)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    peak_tf = peaks.get("bf16_tflops_sustained", 1400.0)
+    peak_src = "of measured (sustained)" if "bf16_tflops_sustained" in peaks else "of fallback"
+    fl = {"split_stage1_pupil_dft": 0.0, "split_stage2_window_dft": 0.0, "split_stage3_blur_rows": 0.0,
+          "split_stage4_blur_cols": 0.0}
+    for j in job:
+        R, N = j["cls"]["R"], j["cls"]["N"]
+        W, D = window(R, N), disk_rows(N)
+        ev = iters[j["cls"]["name"]] * args.steps
+        fl["split_stage1_pupil_dft"] += ev * 3 * 8 * W * D * D
+        fl["split_stage2_window_dft"] += ev * 4 * 8 * W * W * D
+        fl["split_stage3_blur_rows"] += ev * 4 * 2 * R * W * W
+        fl["split_stage4_blur_cols"] += ev * 4 * 2 * R * R * W
+    dom = max(fl, key=lambda k: stats[k][0])
+    t_dom = stats[dom][0] / 1000.0
+    achieved = fl[dom] / t_dom / 1e12 if t_dom > 0 else 0.0
+    stage_table = {k: {"ms": round(v[0], 3), "launches": v[1]} for k, v in stats.items() if v[1]}
+    roofline = {"bound": "tensor", "kernel": dom, "achieved": round(achieved, 2), "peak": peak_tf,
+                "unit": "TFLOP/s", "frac": round(achieved / peak_tf, 4), "peak_source": peak_src,
+                "traffic": None, "stages": stage_table,
+                "note": "achieved = algorithmic flops of the useful model evaluations (complex MAC = 8 flops) / "
+                        "summed CUDA-event duration of that kernel's launches in the timed steps"}
+
+    # end to end through the host C-ABI (pinned host buffers, H2D + D2H inside the call)
+    e2e = None
+    if rank == 0 or True:
+        host = []
+        h2d = d2h = 0
+        for j in job:
+            r = torch.empty(j["rois"].shape, dtype=torch.float32, pin_memory=True)
+            r.copy_(j["rois"])
+            i0 = torch.empty(j["init"].shape, dtype=torch.float64, pin_memory=True)
+            i0.copy_(j["init"])
+            host.append((r.numpy(), i0.numpy()))
+            h2d += r.numel() * 4 + i0.numel() * 8
+            d2h += j["rois"].shape[0] * (5 * 8 + 5 * 8 + 8 + 4 + 4)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for j, (r, i0) in zip(job, host):
+            j["psf"].fit(r, i0, z.PSF.fit_params(precision=z.ZOLA_PREC_SPLIT, **j["prm_kw"]))
+        t_e2e = time.perf_counter() - t0
+        if world > 1:
+            t = torch.tensor([t_e2e], device=device)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            t_e2e = float(t.item())
+        e2e = {"value": n_total * world / t_e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, cores, sample = cpu_baseline(budget_s=args.cpu_seconds)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"{sample} ROIs fitted by the oracle's restatement of the reference coordinate-descent "
+                         "localisation (Localization.java), throughput weighted by the job's class mix"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f16x3 (split) / f32 sums / f64 solve", "data": "synthetic",
+                "config": dict(config_block(args.rois), parallelism=f"replicas x{world}"),
+                "e2e": e2e, "gpu_launches": int(launches), "clocks": clk, "roofline": roofline,
+                "cpu_baseline": cpu,
+                "split_per_class": per_class,
+                "fp64_plain_gpu": {"value": fp64_value, "unit": UNIT, "per_class": fp64},
+                "speedup_vs_fp64_plain": value / world / fp64_value,
+                "accuracy_vs_fp64": acc}
+        print(json.dumps(line), flush=True)
+    for j in job:
+        j["psf"].close()
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -135,6 +135,15 @@ ZOLA_API int zola_fit_batch_dev(zola_ctx* ctx, zola_psf* psf, int R, const float
  * Smaller pools keep the stage intermediates resident in L2. */
 ZOLA_API int zola_ctx_set_pool(zola_ctx* ctx, int max_slots);
 
+/* Per-kernel timing.  With profiling on, every kernel launch of a fit or model
+ * call is bracketed by CUDA events on its stream and the elapsed device time is
+ * accumulated per kernel kind: 0..4 the split stages 1..5, 5 the FP64 fit,
+ * 6 the FP64 model, 7 other.  zola_ctx_stage_stats copies ZOLA_NSTAGES
+ * millisecond totals and launch counts (either pointer may be null). */
+#define ZOLA_NSTAGES 8
+ZOLA_API int zola_ctx_profile(zola_ctx* ctx, int enable);
+ZOLA_API int zola_ctx_stage_stats(zola_ctx* ctx, double* ms, long long* launches, int reset);
+
 /* Number of kernel launches the library issued since the context was created
  * (bench bookkeeping). */
 ZOLA_API long long zola_ctx_launches(const zola_ctx* ctx);

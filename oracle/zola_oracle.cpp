@@ -475,12 +475,15 @@ double model_eval(const Psf* p, int R, const double* d, const double* th, double
     return nll;
 }
 
-// Cholesky solve of (H + lambda diag H) delta = -g; false if not positive definite.
+// Cholesky solve of (H + lambda max(diag H, floor)) delta = -g; false if not
+// positive definite.  The floors (1 um^-2 for x, y, z; 1e-10 and 1e-6 for A
+// and B) keep the damping positive where a derivative vanishes by symmetry.
 bool damped_solve(const double H[5][5], const double* g, double lambda, double* delta) {
+    static const double floor_[5] = {1.0, 1.0, 1.0, 1e-10, 1e-6};
     double L[5][5] = {};
     for (int i = 0; i < 5; ++i)
         for (int j = 0; j <= i; ++j) {
-            double s = H[i][j] + (i == j ? lambda * H[i][i] : 0.0);
+            double s = H[i][j] + (i == j ? lambda * std::max(H[i][i], floor_[i]) : 0.0);
             for (int k = 0; k < j; ++k) s -= L[i][k] * L[j][k];
             if (i == j) {
                 if (!(s > 0)) return false;
@@ -521,7 +524,17 @@ int lm_fit(const Psf* p, int R, const double* d, const double* init, const LMPar
     int evals = 1;
     double lambda = 1e-3;
     int status = 2;
+    // converged when the undamped Gauss-Newton step from the accepted point
+    // moves x, y, z by less than tol and A, B by less than 1e-5 of their values
+    // (distance to the local optimum)
+    auto at_optimum = [&]() {
+        double d0[5];
+        if (!damped_solve(H, g, 0.0, d0)) return false;
+        return std::max(std::fabs(d0[0]), std::max(std::fabs(d0[1]), std::fabs(d0[2]))) < P.tol_xyz &&
+               std::fabs(d0[3]) < 1e-5 * th[3] && std::fabs(d0[4]) < 1e-5 * std::max(th[4], 1.0);
+    };
     if (!std::isfinite(nll)) status = -1;
+    else if (at_optimum()) status = 1;
     while (status == 2 && evals < P.max_iter) {
         double delta[5];
         if (!damped_solve(H, g, lambda, delta)) {
@@ -536,18 +549,16 @@ int lm_fit(const Psf* p, int R, const double* d, const double* init, const LMPar
         double t2[5], g2[5], H2[5][5];
         for (int q = 0; q < 5; ++q) t2[q] = th[q] + scale * delta[q];
         clamp_theta(t2, P);
-        double step = std::max(std::fabs(t2[0] - th[0]), std::max(std::fabs(t2[1] - th[1]), std::fabs(t2[2] - th[2])));
         double nll2 = model_eval(p, R, d, t2, g2, H2, psi2, dpsi2);
         ++evals;
         if (nll2 <= nll) {
             for (int q = 0; q < 5; ++q) { th[q] = t2[q]; g[q] = g2[q]; for (int r = 0; r < 5; ++r) H[q][r] = H2[q][r]; }
             nll = nll2;
             lambda = std::max(lambda * 0.1, 1e-7);
-            if (step < P.tol_xyz) status = 1;
+            if (at_optimum()) status = 1;
         } else {
             lambda *= 10;
-            if (step < P.tol_xyz) status = 1;
-            else if (lambda > 1e7) status = 3;
+            if (lambda > 1e7) status = 3;
         }
     }
     for (int q = 0; q < 5; ++q) out[q] = th[q];

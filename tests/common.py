@@ -43,3 +43,25 @@ def synth_rois(model_fn, R, n, seed, zrange=0.6, photons=2000.0, sigma_ln=0.4, b
     psi = model_fn(R, truth[:, :3])
     rois = rng.poisson(truth[:, 3, None, None] * psi + bg).astype(np.float32)
     return rois, truth
+
+
+def z_symmetric(zern):
+    """True when only odd Zernike terms (m odd <=> n odd) are non-zero: then
+    I(r, -z) = I(r, z) exactly and z is identified up to its sign."""
+    idx = 0
+    n = 0
+    while idx < len(zern):
+        for m in range(-n, n + 1, 2):
+            if idx < len(zern) and zern[idx] != 0 and n % 2 == 0 and idx > 2:
+                return False
+            idx += 1
+        n += 1
+    return True
+
+
+def theta_diff(a, b, zsym):
+    """|a - b| per parameter, comparing |z| when the PSF is z-symmetric."""
+    d = np.abs(a - b)
+    if zsym:
+        d[:, 2] = np.abs(np.abs(a[:, 2]) - np.abs(b[:, 2]))
+    return d

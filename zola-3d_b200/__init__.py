@@ -48,7 +48,9 @@ class FitParams(ctypes.Structure):
 EXPORTS = ["zola_ctx_create", "zola_ctx_destroy", "zola_last_error", "zola_ctx_stream", "zola_ctx_launches",
            "zola_ctx_set_pool", "zola_psf_load", "zola_psf_free", "zola_psf_info", "zola_psf_model",
            "zola_psf_model_dev", "zola_psf_model_prec", "zola_psf_model_prec_dev", "zola_fit_batch",
-           "zola_fit_batch_dev"]
+           "zola_fit_batch_dev", "zola_ctx_profile", "zola_ctx_stage_stats"]
+STAGES = ["split_stage1_pupil_dft", "split_stage2_window_dft", "split_stage3_blur_rows", "split_stage4_blur_cols",
+          "split_stage5_likelihood_lm", "fp64_fit", "fp64_model", "other"]
 
 _lib = None
 
@@ -77,6 +79,8 @@ def lib():
         L.zola_psf_model_prec.argtypes = [vp, i, vp, i, vp, vp, i]
         L.zola_psf_model_prec_dev.argtypes = [vp, i, vp, i, vp, vp, i, vp]
         L.zola_ctx_set_pool.argtypes = [vp, i]
+        L.zola_ctx_profile.argtypes = [vp, i]
+        L.zola_ctx_stage_stats.argtypes = [vp, vp, vp, i]
         L.zola_fit_batch.argtypes = [vp, vp, i, vp, vp, i, ctypes.POINTER(FitParams), vp, vp, vp, vp, vp]
         L.zola_fit_batch_dev.argtypes = [vp, vp, i, vp, vp, i, ctypes.POINTER(FitParams), vp, vp, vp, vp, vp, vp]
         _lib = L
@@ -115,6 +119,17 @@ class Context:
     def set_pool(self, max_slots):
         """Bound the split fit's slot pool (ROIs in flight); 0 = automatic."""
         self.check(lib().zola_ctx_set_pool(self.h, int(max_slots)), "zola_ctx_set_pool")
+
+    def profile(self, enable=True):
+        """Time every library kernel launch with CUDA events on its stream."""
+        self.check(lib().zola_ctx_profile(self.h, int(bool(enable))), "zola_ctx_profile")
+
+    def stage_stats(self, reset=False):
+        """{stage: (total device ms, launches)} accumulated while profiling."""
+        ms = np.zeros(len(STAGES))
+        n = np.zeros(len(STAGES), np.int64)
+        self.check(lib().zola_ctx_stage_stats(self.h, _ptr(ms), _ptr(n), int(bool(reset))), "zola_ctx_stage_stats")
+        return {s: (float(ms[k]), int(n[k])) for k, s in enumerate(STAGES)}
 
     @property
     def launches(self):

@@ -29,6 +29,38 @@ int ensure_scratch(zola_ctx* ctx, size_t bytes, std::string& err) {
     return 0;
 }
 
+void prof_begin(zola_ctx* ctx, int stage, cudaStream_t st) {
+    if (!ctx->profile) return;
+    if ((size_t)ctx->ev_used + 2 > ctx->ev_pool.size()) {
+        for (int k = 0; k < 64; ++k) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            ctx->ev_pool.push_back(e);
+        }
+        ctx->ev_stage.resize(ctx->ev_pool.size() / 2);
+    }
+    ctx->ev_stage[ctx->ev_used / 2] = stage;
+    cudaEventRecord(ctx->ev_pool[ctx->ev_used++], st);
+}
+
+void prof_end(zola_ctx* ctx, cudaStream_t st) {
+    if (!ctx->profile) return;
+    cudaEventRecord(ctx->ev_pool[ctx->ev_used++], st);
+}
+
+void prof_collect(zola_ctx* ctx) {
+    if (!ctx->profile) return;
+    for (int k = 0; k + 1 < ctx->ev_used; k += 2) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, ctx->ev_pool[k], ctx->ev_pool[k + 1]) == cudaSuccess) {
+            int sidx = ctx->ev_stage[k / 2];
+            ctx->stage_ms[sidx] += ms;
+            ctx->stage_launches[sidx] += 1;
+        }
+    }
+    ctx->ev_used = 0;
+}
+
 }  // namespace zola
 
 namespace {
@@ -95,6 +127,7 @@ int zola_ctx_destroy(zola_ctx* ctx) {
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->d_counter) cudaFree(ctx->d_counter);
     if (ctx->h_flags) cudaFreeHost(ctx->h_flags);
+    for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return ZOLA_OK;
@@ -105,6 +138,26 @@ const char* zola_last_error(const zola_ctx* ctx) { return ctx ? ctx->err.c_str()
 void* zola_ctx_stream(zola_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
 long long zola_ctx_launches(const zola_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+int zola_ctx_profile(zola_ctx* ctx, int enable) {
+    if (!ctx) return ZOLA_E_ARG;
+    cudaStreamSynchronize(ctx->stream);
+    prof_collect(ctx);
+    ctx->profile = enable ? 1 : 0;
+    return ZOLA_OK;
+}
+
+int zola_ctx_stage_stats(zola_ctx* ctx, double* ms, long long* launches, int reset) {
+    if (!ctx) return ZOLA_E_ARG;
+    cudaStreamSynchronize(ctx->stream);
+    prof_collect(ctx);
+    for (int k = 0; k < ZOLA_NSTAGES; ++k) {
+        if (ms) ms[k] = ctx->stage_ms[k];
+        if (launches) launches[k] = ctx->stage_launches[k];
+        if (reset) { ctx->stage_ms[k] = 0; ctx->stage_launches[k] = 0; }
+    }
+    return ZOLA_OK;
+}
 
 int zola_psf_load(zola_ctx* ctx, const zola_optics* optics, const double* zernike, int nz, zola_psf** out) {
     if (!ctx || !optics || !out) return set_err(ctx, ZOLA_E_ARG, "zola_psf_load: null argument");

@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(F64_THREADS) fit_f64_kernel(PsfView P, WinView
         for (int q = 0; q < 5; ++q) th[q] = st.th[q];
         eval_lik_f64(P, Wn, w, d, th, red, nll, g, H, F);
         if (threadIdx.x == 0) {
-            lm_start(st, nll, g, H, F);
+            lm_start(st, nll, g, H, F, prm);
             go = lm_propose(st, prm) ? 1 : 0;
         }
         __syncthreads();
@@ -355,8 +355,10 @@ int launch_model_f64(zola_ctx* ctx, zola_psf* p, WindowTables* w, const double* 
     if (f64_layout(ctx, p, w, nblocks, per_cta, use_smem, smem, ctx->err)) return ZOLA_E_CUDA;
     ZOLA_CUDA_CHECK(cudaFuncSetAttribute(model_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), ctx);
     WinView wv{w->R, w->W, w->d_C, w->d_G};
+    prof_begin(ctx, 6, st);
     model_f64_kernel<<<nblocks, F64_THREADS, smem, st>>>(p->view, wv, d_xyz, n, d_out, d_dout, (char*)ctx->scratch,
                                                          per_cta, use_smem);
+    prof_end(ctx, st);
     ctx->launches++;
     ZOLA_CUDA_CHECK(cudaGetLastError(), ctx);
     return ZOLA_OK;
@@ -375,9 +377,11 @@ int launch_fit_f64(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_r
     FitParamsDev fp{prm->zmin, prm->zmax, prm->xymax, prm->tol_xyz, prm->step_xy, prm->step_z, prm->max_iter};
     WinView wv{w->R, w->W, w->d_C, w->d_G};
     ZOLA_CUDA_CHECK(cudaMemsetAsync(ctx->d_counter, 0, sizeof(int), st), ctx);
+    prof_begin(ctx, 5, st);
     fit_f64_kernel<<<nblocks, F64_THREADS, smem, st>>>(p->view, wv, d_rois, d_init, n, fp, d_out5, d_crlb5, d_nll,
                                                        d_status, d_iters, (char*)ctx->scratch, per_cta, use_smem,
                                                        ctx->d_counter);
+    prof_end(ctx, st);
     ctx->launches++;
     ZOLA_CUDA_CHECK(cudaGetLastError(), ctx);
     return ZOLA_OK;

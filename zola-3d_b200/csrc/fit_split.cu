@@ -45,7 +45,11 @@ namespace zola {
 using umma::kmajor_off;
 using umma::mnmajor_off;
 
-constexpr int SPLIT_THREADS = 128;
+// Stages 1-4 run 512 threads: four warpgroups share the 128 TMEM lanes (lane
+// quadrant = warp % 4, so thread t owns tile row t % 128) and split the column
+// work of every epilogue and of the Q build; stage 5 runs 128 threads per slot.
+constexpr int SPLIT_THREADS = 512;
+constexpr int LIK_THREADS = 128;
 
 // ---------------------------------------------------------------- plan ------
 struct SplitScales {
@@ -240,8 +244,8 @@ void free_split_plan(void* plan) {
 
 // ------------------------------------------------------------- helpers -----
 __device__ __forceinline__ uint32_t tmem_lane_addr(uint32_t base, int col) {
-    const int warp = threadIdx.x >> 5;
-    return base + ((uint32_t)(warp * 32) << 16) + (uint32_t)col;
+    const int quad = (threadIdx.x >> 5) & 3;
+    return base + ((uint32_t)(quad * 32) << 16) + (uint32_t)col;
 }
 
 __device__ __forceinline__ void store8h(void* dst, const __half* v) {
@@ -306,8 +310,9 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage1(SplitDev P) {
         if (NCH > 1) load_bc(1, 1);
     }
 
-    // build the Q operand rows
-    const int g = t / DP, a = t % DP;
+    // build the Q operand rows: thread -> row (g, a) = t % 128, columns b of its warpgroup
+    const int row = t & 127, wg = t >> 7;
+    const int g = row / DP, a = row % DP;
     const int slot = blockIdx.x * P.G1 + g;
     const int roi = P.slot_roi[slot];
     double x = 0, y = 0, z = 0;
@@ -315,7 +320,8 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage1(SplitDev P) {
         x = P.lm[slot].trial[0]; y = P.lm[slot].trial[1]; z = P.lm[slot].trial[2];
     }
     const double kxa = a < D ? P.kx[a] : 0.0;
-    for (int b0 = 0; b0 < DP; b0 += 8) {
+    const int bq = DP / 4;
+    for (int b0 = wg * bq; b0 < (wg + 1) * bq; b0 += 8) {
         __half rh[8], rl[8], ih[8], il[8], zr[8], zi[8];
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
@@ -327,10 +333,10 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage1(SplitDev P) {
                 if (pup != 0.0) {
                     double ph = P.phase0[idx] + kxa * x + P.ky[b] * y + P.kz[idx] * z;
                     ph -= 6.283185307179586 * rint(ph * 0.15915494309189535);
-                    float s, c;
-                    sincosf((float)ph, &s, &c);
-                    qr = (float)pup * c;
-                    qi = (float)pup * s;
+                    float sn, cs;
+                    sincosf((float)ph, &sn, &cs);
+                    qr = (float)pup * cs;
+                    qi = (float)pup * sn;
                     kzv = (float)P.kz[idx];
                 }
             }
@@ -339,12 +345,12 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage1(SplitDev P) {
             zr[u] = __float2half_rn(-kzv * qi * P.sc.qz);  // Qz = i kz Q
             zi[u] = __float2half_rn(kzv * qr * P.sc.qz);
         }
-        store8h(A1hi + kmajor_off(t, b0, K1), rh);
-        store8h(A1lo + kmajor_off(t, b0, K1), rl);
-        store8h(A1hi + kmajor_off(t, DP + b0, K1), ih);
-        store8h(A1lo + kmajor_off(t, DP + b0, K1), il);
-        store8h(A1z + kmajor_off(t, b0, K1), zr);
-        store8h(A1z + kmajor_off(t, DP + b0, K1), zi);
+        store8h(A1hi + kmajor_off(row, b0, K1), rh);
+        store8h(A1lo + kmajor_off(row, b0, K1), rl);
+        store8h(A1hi + kmajor_off(row, DP + b0, K1), ih);
+        store8h(A1lo + kmajor_off(row, DP + b0, K1), il);
+        store8h(A1z + kmajor_off(row, b0, K1), zr);
+        store8h(A1z + kmajor_off(row, DP + b0, K1), zi);
     }
     umma::fence_proxy_async();
     __syncthreads();
@@ -376,36 +382,30 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage1(SplitDev P) {
         umma::mbar_wait(&mma_done[buf], (c >> 1) & 1, P.err);
         umma::fence_after_sync();
         const uint32_t col0 = buf * 256;
-        for (int h = 0; h < IC; h += 16) {
-            float v[6][16];
-            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 0 * IC + h), v[0]);
-            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 1 * IC + h), v[1]);
-            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 2 * IC + h), v[2]);
-            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 3 * IC + h), v[3]);
-            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 4 * IC + h), v[4]);
-            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 5 * IC + h), v[5]);
-            if (roi < 0) continue;
-            for (int j8 = 0; j8 < 16; j8 += 8) {
-                const int m = mrow0 + c * IC + h + j8;
-                __half shr[8], slr[8], shi[8], sli[8], yr[8], yi[8], zr[8], zi[8];
+        for (int h = wg * 8; h < IC; h += 32) {
+            float v[6][8];
 #pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    umma::split_f16(v[0][j8 + u] * P.sc.c2, shr[u], slr[u]);
-                    umma::split_f16(v[1][j8 + u] * P.sc.c2, shi[u], sli[u]);
-                    yr[u] = __float2half_rn(v[2][j8 + u] * P.sc.c2y);
-                    yi[u] = __float2half_rn(v[3][j8 + u] * P.sc.c2y);
-                    zr[u] = __float2half_rn(v[4][j8 + u] * P.sc.c2z);
-                    zi[u] = __float2half_rn(v[5][j8 + u] * P.sc.c2z);
-                }
-                store8h(a2t + 0 * arr + mnmajor_off(m, a, 128), shr);
-                store8h(a2t + 1 * arr + mnmajor_off(m, a, 128), slr);
-                store8h(a2t + 0 * arr + mnmajor_off(m, DP + a, 128), shi);
-                store8h(a2t + 1 * arr + mnmajor_off(m, DP + a, 128), sli);
-                store8h(a2t + 2 * arr + mnmajor_off(m, a, 128), yr);
-                store8h(a2t + 2 * arr + mnmajor_off(m, DP + a, 128), yi);
-                store8h(a2t + 3 * arr + mnmajor_off(m, a, 128), zr);
-                store8h(a2t + 3 * arr + mnmajor_off(m, DP + a, 128), zi);
+            for (int part = 0; part < 6; ++part) umma::tmem_ld8(tmem_lane_addr(tbase, col0 + part * IC + h), v[part]);
+            if (roi < 0) continue;
+            const int m = mrow0 + c * IC + h;
+            __half shr[8], slr[8], shi[8], sli[8], yr[8], yi[8], zr[8], zi[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                umma::split_f16(v[0][u] * P.sc.c2, shr[u], slr[u]);
+                umma::split_f16(v[1][u] * P.sc.c2, shi[u], sli[u]);
+                yr[u] = __float2half_rn(v[2][u] * P.sc.c2y);
+                yi[u] = __float2half_rn(v[3][u] * P.sc.c2y);
+                zr[u] = __float2half_rn(v[4][u] * P.sc.c2z);
+                zi[u] = __float2half_rn(v[5][u] * P.sc.c2z);
             }
+            store8h(a2t + 0 * arr + mnmajor_off(m, a, 128), shr);
+            store8h(a2t + 1 * arr + mnmajor_off(m, a, 128), slr);
+            store8h(a2t + 0 * arr + mnmajor_off(m, DP + a, 128), shi);
+            store8h(a2t + 1 * arr + mnmajor_off(m, DP + a, 128), sli);
+            store8h(a2t + 2 * arr + mnmajor_off(m, a, 128), yr);
+            store8h(a2t + 2 * arr + mnmajor_off(m, DP + a, 128), yi);
+            store8h(a2t + 3 * arr + mnmajor_off(m, a, 128), zr);
+            store8h(a2t + 3 * arr + mnmajor_off(m, DP + a, 128), zi);
         }
         umma::fence_before_sync();
         __syncthreads();
@@ -473,51 +473,39 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage2(SplitDev P) {
     if (t == 0) issue(0);
     char* a3t = P.a3 + (size_t)blockIdx.x * a3_tile_bytes(W);
     const size_t arr3 = (size_t)128 * W * 2;
+    const int row = t & 127, wg = t >> 7;
     for (int c = 0; c < NCH; ++c) {
         const int buf = NCH > 1 ? (c & 1) : 0;
         if (t == 0 && c + 1 < NCH) issue(c + 1);
         umma::mbar_wait(&mma_done[buf], (c >> 1) & 1, P.err);
         umma::fence_after_sync();
         const uint32_t col0 = buf * 256;
-        for (int h = 0; h < IC; h += 16) {
-            float er[16], ei[16], xr[16], xi[16];
-            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 0 * IC + h), er);
-            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 1 * IC + h), ei);
-            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 2 * IC + h), xr);
-            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 3 * IC + h), xi);
-            float I0[16], I1[16];
+        for (int h = wg * 8; h < IC; h += 32) {
+            float er[8], ei[8], xr[8], xi[8];
+            umma::tmem_ld8(tmem_lane_addr(tbase, col0 + 0 * IC + h), er);
+            umma::tmem_ld8(tmem_lane_addr(tbase, col0 + 1 * IC + h), ei);
+            umma::tmem_ld8(tmem_lane_addr(tbase, col0 + 2 * IC + h), xr);
+            umma::tmem_ld8(tmem_lane_addr(tbase, col0 + 3 * IC + h), xi);
+            __half hh[8], ll[8], dx[8], dy[8], dz[8];
 #pragma unroll
-            for (int u = 0; u < 16; ++u) {
-                I0[u] = (er[u] * er[u] + ei[u] * ei[u]) * P.sc.cI;
-                I1[u] = (er[u] * xr[u] + ei[u] * xi[u]) * P.sc.cIx;
+            for (int u = 0; u < 8; ++u) {
+                umma::split_f16((er[u] * er[u] + ei[u] * ei[u]) * P.sc.cI, hh[u], ll[u]);
+                dx[u] = __float2half_rn((er[u] * xr[u] + ei[u] * xi[u]) * P.sc.cIx);
             }
-            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 4 * IC + h), xr);
-            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 5 * IC + h), xi);
-            float I2[16];
+            umma::tmem_ld8(tmem_lane_addr(tbase, col0 + 4 * IC + h), xr);
+            umma::tmem_ld8(tmem_lane_addr(tbase, col0 + 5 * IC + h), xi);
 #pragma unroll
-            for (int u = 0; u < 16; ++u) I2[u] = (er[u] * xr[u] + ei[u] * xi[u]) * P.sc.cIy;
-            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 6 * IC + h), xr);
-            umma::tmem_ld16(tmem_lane_addr(tbase, col0 + 7 * IC + h), xi);
-            float I3[16];
+            for (int u = 0; u < 8; ++u) dy[u] = __float2half_rn((er[u] * xr[u] + ei[u] * xi[u]) * P.sc.cIy);
+            umma::tmem_ld8(tmem_lane_addr(tbase, col0 + 6 * IC + h), xr);
+            umma::tmem_ld8(tmem_lane_addr(tbase, col0 + 7 * IC + h), xi);
 #pragma unroll
-            for (int u = 0; u < 16; ++u) I3[u] = (er[u] * xr[u] + ei[u] * xi[u]) * P.sc.cIz;
-            for (int i8 = 0; i8 < 16; i8 += 8) {
-                const int i = c * IC + h + i8;
-                __half hh[8], ll[8], dx[8], dy[8], dz[8];
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    umma::split_f16(I0[i8 + u], hh[u], ll[u]);
-                    dx[u] = __float2half_rn(I1[i8 + u]);
-                    dy[u] = __float2half_rn(I2[i8 + u]);
-                    dz[u] = __float2half_rn(I3[i8 + u]);
-                }
-                const uint32_t off = kmajor_off(t, i, W);
-                store8h(a3t + 0 * arr3 + off, hh);
-                store8h(a3t + 1 * arr3 + off, ll);
-                store8h(a3t + 2 * arr3 + off, dx);
-                store8h(a3t + 3 * arr3 + off, dy);
-                store8h(a3t + 4 * arr3 + off, dz);
-            }
+            for (int u = 0; u < 8; ++u) dz[u] = __float2half_rn((er[u] * xr[u] + ei[u] * xi[u]) * P.sc.cIz);
+            const uint32_t off = kmajor_off(row, c * IC + h, W);
+            store8h(a3t + 0 * arr3 + off, hh);
+            store8h(a3t + 1 * arr3 + off, ll);
+            store8h(a3t + 2 * arr3 + off, dx);
+            store8h(a3t + 3 * arr3 + off, dy);
+            store8h(a3t + 4 * arr3 + off, dz);
         }
         umma::fence_before_sync();
         __syncthreads();
@@ -567,26 +555,27 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage3(SplitDev P) {
     }
     umma::mbar_wait(&done, 0, P.err);
     umma::fence_after_sync();
-    // epilogue: thread row m = (g2, j) -> A4 column k = j of the slot's (map, i') rows
-    const int g2 = t / W, j = t % W;
+    // epilogue: thread row (g2, j) = t % 128 -> A4 column k = j of the slot's
+    // (map, i') rows; warpgroup = map
+    const int row = t & 127, m = t >> 7;
+    const int g2 = row / W, j = row % W;
     const int slot = blockIdx.x * P.G2 + g2;
     char* a4s = P.a4 + (size_t)slot * P.NT4 * a4_tile_bytes(W);
     const size_t arr4 = (size_t)128 * W * 2;
-    for (int m = 0; m < 4; ++m)
-        for (int h = 0; h < RP; h += 16) {
-            float v[16];
-            umma::tmem_ld16(tmem_lane_addr(tbase, m * RP + h), v);
-            for (int i8 = 0; i8 < 16; i8 += 8) {
-                const int r = m * RP + h + i8;
-                char* tile = a4s + (size_t)(r / 128) * a4_tile_bytes(W);
-                __half hh[8], ll[8];
+    for (int h = 0; h < RP; h += 16) {
+        float v[16];
+        umma::tmem_ld16(tmem_lane_addr(tbase, m * RP + h), v);
+        for (int i8 = 0; i8 < 16; i8 += 8) {
+            const int r = m * RP + h + i8;
+            char* tile = a4s + (size_t)(r / 128) * a4_tile_bytes(W);
+            __half hh[8], ll[8];
 #pragma unroll
-                for (int u = 0; u < 8; ++u) umma::split_f16(v[i8 + u] * P.sc.cJ[m], hh[u], ll[u]);
-                const uint32_t off = mnmajor_off(r % 128, j, 128);
-                store8h(tile + off, hh);
-                store8h(tile + arr4 + off, ll);
-            }
+            for (int u = 0; u < 8; ++u) umma::split_f16(v[i8 + u] * P.sc.cJ[m], hh[u], ll[u]);
+            const uint32_t off = mnmajor_off(r % 128, j, 128);
+            store8h(tile + off, hh);
+            store8h(tile + arr4 + off, ll);
         }
+    }
     umma::fence_before_sync();
     __syncthreads();
     if (t < 32) umma::tmem_dealloc(tbase, ncols);
@@ -632,13 +621,15 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage4(SplitDev P) {
     }
     umma::mbar_wait(&done, 0, P.err);
     umma::fence_after_sync();
-    const int r = tile * 128 + t, map = r / RP, ip = r % RP;
-    for (int h = 0; h < RP; h += 16) {
-        float v[16];
-        umma::tmem_ld16(tmem_lane_addr(tbase, h), v);
+    const int row = t & 127, wg = t >> 7;
+    const int r = tile * 128 + row, map = r / RP, ip = r % RP;
+    const int cq = RP / 4;
+    for (int h = wg * cq; h < (wg + 1) * cq; h += 4) {
+        float v[4];
+        umma::tmem_ld4(tmem_lane_addr(tbase, h), v);
         if (map < 4 && ip < R) {
             float* dst = P.tmaps + (((size_t)slot * 4 + map) * R + ip) * R;
-            for (int u = 0; u < 16 && h + u < R; ++u) dst[h + u] = v[u] * P.sc.cT[map];
+            for (int u = 0; u < 4 && h + u < R; ++u) dst[h + u] = v[u] * P.sc.cT[map];
         }
     }
     umma::fence_before_sync();
@@ -669,14 +660,14 @@ __device__ inline void block_sum_pairs(float (&s)[NV], float (&c)[NV], double* r
     __syncthreads();
     if (threadIdx.x < NV) {
         double v = 0;
-        for (int w = 0; w < SPLIT_THREADS / 32; ++w) v += red[w * NV + threadIdx.x];
+        for (int w = 0; w < LIK_THREADS / 32; ++w) v += red[w * NV + threadIdx.x];
         out[threadIdx.x] = v;
     }
     __syncthreads();
 }
 
 // One CTA per slot: likelihood sums at the trial point, then the FP64 LM step.
-__global__ void __launch_bounds__(SPLIT_THREADS) k_stage5(SplitDev P, const float* rois, const double* init, int n,
+__global__ void __launch_bounds__(LIK_THREADS) k_stage5(SplitDev P, const float* rois, const double* init, int n,
                                                           FitParamsDev prm, double* out5, double* crlb5,
                                                           double* nll_out, int* st_out, int* it_out) {
     __shared__ double red[4 * NRED];
@@ -688,7 +679,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS) k_stage5(SplitDev P, const floa
     const float* d = rois + (size_t)roi * RR;
     // normalisation sums
     float ns[4] = {0, 0, 0, 0}, nc[4] = {0, 0, 0, 0};
-    for (int k = t; k < RR; k += SPLIT_THREADS) {
+    for (int k = t; k < RR; k += LIK_THREADS) {
         const float v = T0[k];
         const float sg = v < 0 ? -1.f : 1.f;
         kahan_add(ns[0], nc[0], fabsf(v));
@@ -705,7 +696,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS) k_stage5(SplitDev P, const floa
 #pragma unroll
     for (int k = 0; k < NRED; ++k) { s[k] = 0.f; c[k] = 0.f; }
     bool bad = false;
-    for (int k = t; k < RR; k += SPLIT_THREADS) {
+    for (int k = t; k < RR; k += LIK_THREADS) {
         const float v = T0[k];
         const float sg = v < 0 ? -1.f : 1.f;
         const float psi = fabsf(v) * invS;
@@ -747,7 +738,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS) k_stage5(SplitDev P, const floa
     LMState& st = P.lm[slot];
     if (P.slot_phase[slot] == 0) {
         for (int q = 0; q < 5; ++q) st.th[q] = st.trial[q];
-        lm_start(st, nll, g, H, F);
+        lm_start(st, nll, g, H, F, prm);
         P.slot_phase[slot] = 1;
     } else {
         lm_update(st, nll, g, H, F, prm);
@@ -914,10 +905,18 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
 static void launch_model_stages(zola_ctx* ctx, const SplitPool& sp, cudaStream_t st) {
     const SplitPlanHost& pl = *sp.pl;
     const int P = sp.D.P;
+    prof_begin(ctx, 0, st);
     k_stage1<<<P / pl.G1, SPLIT_THREADS, sp.s1, st>>>(sp.D);
+    prof_end(ctx, st);
+    prof_begin(ctx, 1, st);
     k_stage2<<<P / pl.G2, SPLIT_THREADS, sp.s2, st>>>(sp.D);
+    prof_end(ctx, st);
+    prof_begin(ctx, 2, st);
     k_stage3<<<P / pl.G2, SPLIT_THREADS, sp.s3, st>>>(sp.D);
+    prof_end(ctx, st);
+    prof_begin(ctx, 3, st);
     k_stage4<<<P * pl.NT4, SPLIT_THREADS, sp.s4, st>>>(sp.D);
+    prof_end(ctx, st);
     ctx->launches += 4;
 }
 
@@ -925,6 +924,7 @@ static int read_flags(zola_ctx* ctx, const SplitDev& D, cudaStream_t st, int* ac
     if (!ctx->h_flags) ZOLA_CUDA_CHECK(cudaMallocHost(&ctx->h_flags, 4 * sizeof(int)), ctx);
     ZOLA_CUDA_CHECK(cudaMemcpyAsync(ctx->h_flags, D.active, 2 * sizeof(int), cudaMemcpyDeviceToHost, st), ctx);
     ZOLA_CUDA_CHECK(cudaStreamSynchronize(st), ctx);
+    prof_collect(ctx);
     *active = ctx->h_flags[0];
     *err = ctx->h_flags[1];
     return ZOLA_OK;
@@ -969,7 +969,9 @@ int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d
     while (true) {
         for (int k = 0; k < 4; ++k) {
             launch_model_stages(ctx, sp, st);
-            k_stage5<<<P, SPLIT_THREADS, 0, st>>>(D, d_rois, d_init, n, fp, d_out5, d_crlb5, d_nll, d_status, d_iters);
+            prof_begin(ctx, 4, st);
+            k_stage5<<<P, LIK_THREADS, 0, st>>>(D, d_rois, d_init, n, fp, d_out5, d_crlb5, d_nll, d_status, d_iters);
+            prof_end(ctx, st);
             ctx->launches++;
         }
         rounds += 4;

@@ -39,14 +39,22 @@ __host__ __device__ inline void lm_clamp(double* t, const FitParamsDev& P) {
     t[4] = fmax(t[4], 0.01);
 }
 
-// Cholesky solve of (H + lambda diag H) delta = -g.
+// Damping floors (units 1/um^2 for x, y, z; 1/photon^2 for A and B): the
+// Marquardt term lambda * max(H_ii, floor_i) stays positive where a
+// derivative vanishes by symmetry (e.g. d mu / dz at x = y = z = 0 for an
+// odd aberration), so the damped system can always be solved.
+__host__ __device__ inline double lm_floor(int i) {
+    return i < 3 ? 1.0 : (i == 3 ? 1e-10 : 1e-6);
+}
+
+// Cholesky solve of (H + lambda max(diag H, floor)) delta = -g.
 __host__ __device__ inline bool lm_solve(const double* H, const double* g, double lambda, double* delta) {
     double L[5][5];
     for (int i = 0; i < 5; ++i)
         for (int j = 0; j < 5; ++j) L[i][j] = 0.0;
     for (int i = 0; i < 5; ++i)
         for (int j = 0; j <= i; ++j) {
-            double s = H[i * 5 + j] + (i == j ? lambda * H[i * 5 + i] : 0.0);
+            double s = H[i * 5 + j] + (i == j ? lambda * fmax(H[i * 5 + i], lm_floor(i)) : 0.0);
             for (int k = 0; k < j; ++k) s -= L[i][k] * L[j][k];
             if (i == j) {
                 if (!(s > 0.0)) return false;
@@ -69,14 +77,28 @@ __host__ __device__ inline bool lm_solve(const double* H, const double* g, doubl
     return true;
 }
 
+// Convergence test at an accepted point: the undamped Gauss-Newton step
+// -H^-1 g (the distance to the optimum of the local quadratic model) moves
+// x, y and z by less than tol and A, B by less than 1e-5 of their values.
+// Damped steps shrink with lambda on flat likelihoods, so their size alone is
+// not a distance to the optimum.
+__host__ __device__ inline bool lm_at_optimum(const LMState& s, const FitParamsDev& P) {
+    double d[5];
+    if (!lm_solve(s.H, s.g, 0.0, d)) return false;
+    return fmax(fabs(d[0]), fmax(fabs(d[1]), fabs(d[2]))) < P.tol_xyz && fabs(d[3]) < 1e-5 * s.th[3] &&
+           fabs(d[4]) < 1e-5 * fmax(s.th[4], 1.0);
+}
+
 // First evaluation result at the (clamped) initial point.
-__host__ __device__ inline void lm_start(LMState& s, double nll, const double* g, const double* H, const double* F) {
+__host__ __device__ inline void lm_start(LMState& s, double nll, const double* g, const double* H, const double* F,
+                                         const FitParamsDev& P) {
     s.nll = nll;
     for (int q = 0; q < 5; ++q) s.g[q] = g[q];
     for (int q = 0; q < 25; ++q) { s.H[q] = H[q]; s.F[q] = F[q]; }
     s.evals = 1;
     s.lambda = 1e-3;
     s.status = isfinite(nll) ? 2 : -1;
+    if (s.status == 2 && lm_at_optimum(s, P)) s.status = 1;
 }
 
 // Propose the next trial point.  Returns false when the fit is finished.
@@ -110,11 +132,10 @@ __host__ __device__ inline void lm_update(LMState& s, double nll, const double* 
         for (int q = 0; q < 25; ++q) { s.H[q] = H[q]; s.F[q] = F[q]; }
         s.nll = nll;
         s.lambda = fmax(s.lambda * 0.1, 1e-7);
-        if (s.step < P.tol_xyz) s.status = 1;
+        if (lm_at_optimum(s, P)) s.status = 1;
     } else {
         s.lambda *= 10.0;
-        if (s.step < P.tol_xyz) s.status = 1;
-        else if (s.lambda > 1e7) s.status = 3;
+        if (s.lambda > 1e7) s.status = 3;
     }
 }
 

@@ -71,7 +71,21 @@ struct zola_ctx {
     int* d_status_word = nullptr;
     int* h_flags = nullptr;      // pinned host words read back by the split fit loop
     int split_pool_max = 0;      // 0: size the split slot pool automatically
+    // optional per-kernel timing with CUDA events on the launch stream
+    int profile = 0;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<int> ev_stage;   // stage id of each recorded (start, stop) pair
+    int ev_used = 0;
+    double stage_ms[ZOLA_NSTAGES] = {};
+    long long stage_launches[ZOLA_NSTAGES] = {};
 };
+
+namespace zola {
+// Kernel-timing helpers (capi.cu): bracket a launch when profiling is on.
+void prof_begin(zola_ctx* ctx, int stage, cudaStream_t st);
+void prof_end(zola_ctx* ctx, cudaStream_t st);
+void prof_collect(zola_ctx* ctx);  // call after the stream was synchronised
+}  // namespace zola
 
 struct zola_psf {
     zola_ctx* ctx = nullptr;
