@@ -525,13 +525,13 @@ int lm_fit(const Psf* p, int R, const double* d, const double* init, const LMPar
     double lambda = 1e-3;
     int status = 2;
     // converged when the undamped Gauss-Newton step from the accepted point
-    // moves x, y, z by less than tol and A, B by less than 1e-5 of their values
+    // moves x, y, z by less than tol and A, B by less than 1e-4 of their values
     // (distance to the local optimum)
     auto at_optimum = [&]() {
         double d0[5];
         if (!damped_solve(H, g, 0.0, d0)) return false;
         return std::max(std::fabs(d0[0]), std::max(std::fabs(d0[1]), std::fabs(d0[2]))) < P.tol_xyz &&
-               std::fabs(d0[3]) < 1e-5 * th[3] && std::fabs(d0[4]) < 1e-5 * std::max(th[4], 1.0);
+               std::fabs(d0[3]) < 1e-4 * th[3] && std::fabs(d0[4]) < 1e-4 * std::max(th[4], 1.0);
     };
     if (!std::isfinite(nll)) status = -1;
     else if (at_optimum()) status = 1;

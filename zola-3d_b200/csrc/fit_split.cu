@@ -639,6 +639,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage4(SplitDev P) {
 
 // ----------------------------------------------------------- stage 5 -------
 constexpr int NRED = 1 + 5 + 15 + 15;
+constexpr int LIK_SLOTS = LIK_THREADS / 32;  // one warp per slot
 
 __device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
     float y = v - c;
@@ -647,86 +648,83 @@ __device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
     s = t2;
 }
 
-template <int NV>
-__device__ inline void block_sum_pairs(float (&s)[NV], float (&c)[NV], double* red, double* out) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+__device__ __forceinline__ double warp_sum(double x) {
 #pragma unroll
-    for (int k = 0; k < NV; ++k) {
-        double x = (double)s[k] - (double)c[k];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-        if (lane == 0) red[warp * NV + k] = x;
-    }
-    __syncthreads();
-    if (threadIdx.x < NV) {
-        double v = 0;
-        for (int w = 0; w < LIK_THREADS / 32; ++w) v += red[w * NV + threadIdx.x];
-        out[threadIdx.x] = v;
-    }
-    __syncthreads();
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
 }
 
-// One CTA per slot: likelihood sums at the trial point, then the FP64 LM step.
+// One warp per slot: likelihood sums at the trial point (per-pixel terms in
+// FP32; the likelihood and gradient with Kahan compensation, the Hessian and
+// Fisher terms plain; lane partials combined in FP64), then the FP64 LM step on
+// lane 0.
 __global__ void __launch_bounds__(LIK_THREADS) k_stage5(SplitDev P, const float* rois, const double* init, int n,
-                                                          FitParamsDev prm, double* out5, double* crlb5,
-                                                          double* nll_out, int* st_out, int* it_out) {
-    __shared__ double red[4 * NRED];
-    __shared__ double tot[NRED];
-    const int slot = blockIdx.x, R = P.R, RR = R * R, t = threadIdx.x;
+                                                        FitParamsDev prm, double* out5, double* crlb5,
+                                                        double* nll_out, int* st_out, int* it_out) {
+    const int lane = threadIdx.x & 31;
+    const int slot = blockIdx.x * LIK_SLOTS + (threadIdx.x >> 5);
+    if (slot >= P.P) return;
     const int roi = P.slot_roi[slot];
     if (roi < 0) return;
+    const int R = P.R, RR = R * R;
     const float* T0 = P.tmaps + (size_t)slot * 4 * RR;
     const float* d = rois + (size_t)roi * RR;
     // normalisation sums
-    float ns[4] = {0, 0, 0, 0}, nc[4] = {0, 0, 0, 0};
-    for (int k = t; k < RR; k += LIK_THREADS) {
+    float ns[4] = {0, 0, 0, 0}, nc = 0.f;
+    for (int k = lane; k < RR; k += 32) {
         const float v = T0[k];
         const float sg = v < 0 ? -1.f : 1.f;
-        kahan_add(ns[0], nc[0], fabsf(v));
-        kahan_add(ns[1], nc[1], sg * T0[RR + k]);
-        kahan_add(ns[2], nc[2], sg * T0[2 * RR + k]);
-        kahan_add(ns[3], nc[3], sg * T0[3 * RR + k]);
+        kahan_add(ns[0], nc, fabsf(v));
+        ns[1] += sg * T0[RR + k];
+        ns[2] += sg * T0[2 * RR + k];
+        ns[3] += sg * T0[3 * RR + k];
     }
-    block_sum_pairs<4>(ns, nc, red, tot);
-    const float S = (float)tot[0], Dx = (float)tot[1], Dy = (float)tot[2], Dz = (float)tot[3];
+    const float S = (float)warp_sum((double)ns[0] - (double)nc);
+    const float Dx = (float)warp_sum(ns[1]), Dy = (float)warp_sum(ns[2]), Dz = (float)warp_sum(ns[3]);
     const float invS = 1.f / S;
     const double* th = P.lm[slot].trial;
     const float A = (float)th[3], B = (float)th[4];
-    float s[NRED], c[NRED];
+    float sg6[6], cg6[6], sh[30];
 #pragma unroll
-    for (int k = 0; k < NRED; ++k) { s[k] = 0.f; c[k] = 0.f; }
+    for (int k = 0; k < 6; ++k) { sg6[k] = 0.f; cg6[k] = 0.f; }
+#pragma unroll
+    for (int k = 0; k < 30; ++k) sh[k] = 0.f;
     bool bad = false;
-    for (int k = t; k < RR; k += LIK_THREADS) {
+    for (int k = lane; k < RR; k += 32) {
         const float v = T0[k];
-        const float sg = v < 0 ? -1.f : 1.f;
+        const float sgn = v < 0 ? -1.f : 1.f;
         const float psi = fabsf(v) * invS;
         float j[5];
-        j[0] = A * (sg * T0[RR + k] - psi * Dx) * invS;
-        j[1] = A * (sg * T0[2 * RR + k] - psi * Dy) * invS;
-        j[2] = A * (sg * T0[3 * RR + k] - psi * Dz) * invS;
+        j[0] = A * (sgn * T0[RR + k] - psi * Dx) * invS;
+        j[1] = A * (sgn * T0[2 * RR + k] - psi * Dy) * invS;
+        j[2] = A * (sgn * T0[3 * RR + k] - psi * Dz) * invS;
         j[3] = psi;
         j[4] = 1.f;
         const float mu = A * psi + B;
         if (!(mu > 0.f)) { bad = true; continue; }
         const float dk = d[k];
-        kahan_add(s[0], c[0], dk > 0.f ? mu - dk - dk * logf(mu / dk) : mu);
+        kahan_add(sg6[0], cg6[0], dk > 0.f ? mu - dk - dk * logf(mu / dk) : mu);
         const float wg = 1.f - dk / mu, wf = 1.f / mu, wh = dk * wf * wf;
 #pragma unroll
-        for (int q = 0; q < 5; ++q) kahan_add(s[1 + q], c[1 + q], wg * j[q]);
-        int o = 6;
+        for (int q = 0; q < 5; ++q) kahan_add(sg6[1 + q], cg6[1 + q], wg * j[q]);
+        int o = 0;
 #pragma unroll
         for (int q = 0; q < 5; ++q)
 #pragma unroll
             for (int r2 = 0; r2 <= q; ++r2) {
-                kahan_add(s[o], c[o], wh * j[q] * j[r2]);
-                kahan_add(s[o + 15], c[o + 15], wf * j[q] * j[r2]);
+                sh[o] += wh * j[q] * j[r2];
+                sh[o + 15] += wf * j[q] * j[r2];
                 ++o;
             }
     }
-    if (bad) s[0] = INFINITY;
-    block_sum_pairs<NRED>(s, c, red, tot);
-    if (t != 0) return;
-    double nll = tot[0], g[5], H[25], F[25];
+    double tot[NRED];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) tot[k] = warp_sum((double)sg6[k] - (double)cg6[k]);
+#pragma unroll
+    for (int k = 0; k < 30; ++k) tot[6 + k] = warp_sum((double)sh[k]);
+    const bool anybad = __any_sync(0xffffffffu, bad);
+    if (lane != 0) return;
+    double nll = anybad ? INFINITY : tot[0], g[5], H[25], F[25];
     for (int q = 0; q < 5; ++q) g[q] = tot[1 + q];
     int o = 6;
     for (int q = 0; q < 5; ++q)
@@ -970,7 +968,8 @@ int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d
         for (int k = 0; k < 4; ++k) {
             launch_model_stages(ctx, sp, st);
             prof_begin(ctx, 4, st);
-            k_stage5<<<P, LIK_THREADS, 0, st>>>(D, d_rois, d_init, n, fp, d_out5, d_crlb5, d_nll, d_status, d_iters);
+            k_stage5<<<(P + LIK_SLOTS - 1) / LIK_SLOTS, LIK_THREADS, 0, st>>>(D, d_rois, d_init, n, fp, d_out5, d_crlb5,
+                                                                             d_nll, d_status, d_iters);
             prof_end(ctx, st);
             ctx->launches++;
         }

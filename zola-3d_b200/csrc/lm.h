@@ -79,14 +79,14 @@ __host__ __device__ inline bool lm_solve(const double* H, const double* g, doubl
 
 // Convergence test at an accepted point: the undamped Gauss-Newton step
 // -H^-1 g (the distance to the optimum of the local quadratic model) moves
-// x, y and z by less than tol and A, B by less than 1e-5 of their values.
+// x, y and z by less than tol and A, B by less than 1e-4 of their values.
 // Damped steps shrink with lambda on flat likelihoods, so their size alone is
 // not a distance to the optimum.
 __host__ __device__ inline bool lm_at_optimum(const LMState& s, const FitParamsDev& P) {
     double d[5];
     if (!lm_solve(s.H, s.g, 0.0, d)) return false;
-    return fmax(fabs(d[0]), fmax(fabs(d[1]), fabs(d[2]))) < P.tol_xyz && fabs(d[3]) < 1e-5 * s.th[3] &&
-           fabs(d[4]) < 1e-5 * fmax(s.th[4], 1.0);
+    return fmax(fabs(d[0]), fmax(fabs(d[1]), fabs(d[2]))) < P.tol_xyz && fabs(d[3]) < 1e-4 * s.th[3] &&
+           fabs(d[4]) < 1e-4 * fmax(s.th[4], 1.0);
 }
 
 // First evaluation result at the (clamped) initial point.
