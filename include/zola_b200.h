@@ -131,6 +131,25 @@ ZOLA_API int zola_fit_batch_dev(zola_ctx* ctx, zola_psf* psf, int R, const float
                        int n, const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll,
                        int* d_status, int* d_iters, void* stream);
 
+/* Allocation-free FP64 fit (this entry point has no counterpart in the
+ * reference).  For callers that must not allocate device memory while they fit
+ * (a host application that owns all device memory and lends plugins only its
+ * own buffers; an acquisition thread that cannot stall on cudaMalloc/cudaFree,
+ * which may synchronise the device): the plain FP64 fit of zola_fit_batch_dev
+ * with its work areas and ROI counter in a 64 MiB array inside the library
+ * image, held on every GPU that loads the library until the process exits.
+ * Device buffers and stream as in zola_fit_batch_dev; prm->precision must be
+ * ZOLA_PREC_FP64.  The PSF's tables for this ROI size must exist (any model or
+ * fit call with this R, e.g. zola_psf_model_dev(psf, R, NULL, 0, NULL, NULL, s),
+ * prepares them); the call itself allocates nothing.  Its first call on a
+ * device looks up the array's device address; make that first call before any
+ * stream capture.  ROI sizes whose per-block work area exceeds the array are
+ * rejected with ZOLA_E_ARG; large windows run on fewer blocks.  All calls share
+ * the array: calls that overlap on the GPU race, so serialise them. */
+ZOLA_API int zola_fit_batch_noalloc(zola_psf* psf, int R, const float* d_rois, const double* d_init5, int n,
+                                    const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll,
+                                    int* d_status, int* d_iters, void* stream);
+
 /* Upper bound on the split fit's slot pool (ROIs in flight); 0 = automatic.
  * Smaller pools keep the stage intermediates resident in L2. */
 ZOLA_API int zola_ctx_set_pool(zola_ctx* ctx, int max_slots);

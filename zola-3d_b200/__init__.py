@@ -48,7 +48,7 @@ class FitParams(ctypes.Structure):
 EXPORTS = ["zola_ctx_create", "zola_ctx_destroy", "zola_last_error", "zola_ctx_stream", "zola_ctx_launches",
            "zola_ctx_set_pool", "zola_psf_load", "zola_psf_free", "zola_psf_info", "zola_psf_model",
            "zola_psf_model_dev", "zola_psf_model_prec", "zola_psf_model_prec_dev", "zola_fit_batch",
-           "zola_fit_batch_dev", "zola_ctx_profile", "zola_ctx_stage_stats"]
+           "zola_fit_batch_dev", "zola_ctx_profile", "zola_ctx_stage_stats", "zola_fit_batch_noalloc"]
 STAGES = ["split_stage1_pupil_dft", "split_stage2_window_dft", "split_stage3_blur_rows", "split_stage4_blur_cols",
           "split_stage5_likelihood_lm", "fp64_fit", "fp64_model", "other"]
 
@@ -80,6 +80,7 @@ def lib():
         L.zola_psf_model_prec_dev.argtypes = [vp, i, vp, i, vp, vp, i, vp]
         L.zola_ctx_set_pool.argtypes = [vp, i]
         L.zola_ctx_profile.argtypes = [vp, i]
+        L.zola_fit_batch_noalloc.argtypes = [vp, i, vp, vp, i, ctypes.POINTER(FitParams), vp, vp, vp, vp, vp, vp]
         L.zola_ctx_stage_stats.argtypes = [vp, vp, vp, i]
         L.zola_fit_batch.argtypes = [vp, vp, i, vp, vp, i, ctypes.POINTER(FitParams), vp, vp, vp, vp, vp]
         L.zola_fit_batch_dev.argtypes = [vp, vp, i, vp, vp, i, ctypes.POINTER(FitParams), vp, vp, vp, vp, vp, vp]
@@ -228,6 +229,19 @@ class PSF:
         self.ctx.check(lib().zola_fit_batch_dev(self.ctx.h, self.h, R, _ptr(rois), _ptr(init), n, ctypes.byref(prm),
                                                 _ptr(out), _ptr(crlb), _ptr(nll), _ptr(status), _ptr(iters), stream),
                        "zola_fit_batch_dev")
+
+
+def fit_noalloc_dev(psf, rois, init, prm, out, crlb=None, nll=None, status=None, iters=None, stream=None):
+    """Allocation-free FP64 fit (zola_fit_batch_noalloc) over torch CUDA tensors.
+
+    For callers that must not allocate device memory while fitting: the work
+    areas live in a fixed 64 MiB array inside the library on each GPU.  The
+    PSF's tables for this ROI size must have been prepared by an earlier model
+    or fit call with the same R; calls that overlap on the GPU race."""
+    n, R = rois.shape[0], rois.shape[1]
+    psf.ctx.check(lib().zola_fit_batch_noalloc(psf.h, R, _ptr(rois), _ptr(init), n, ctypes.byref(prm), _ptr(out),
+                                               _ptr(crlb), _ptr(nll), _ptr(status), _ptr(iters), stream),
+                  "zola_fit_batch_noalloc")
 
 
 def load_calibration_json(path, size_fft=128, n_wat=None, zfocus=0.0, kz_reset=False):

@@ -18,6 +18,8 @@
 // q == r, which holds for the fit tables (kz = 0 where evanescent).
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "lm.h"
 #include "zola_internal.h"
 
@@ -388,3 +390,121 @@ int launch_fit_f64(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_r
 }
 
 }  // namespace zola
+
+// ------------------------------------------------------------------------
+// Allocation-free FP64 fit.
+//
+// Some callers cannot allocate device memory at the time they fit: a host
+// application that reserves all device memory for itself at start-up and hands
+// plugins only the buffers it owns, or an acquisition thread that must not
+// stall on cudaMalloc / cudaFree (both can synchronise the whole device).  For
+// them zola_fit_batch_noalloc runs the plain FP64 fit with its per-block work
+// areas and its ROI-queue counter in the file-scope array below instead of the
+// context's scratch.  The array is part of the library image: every GPU on
+// which the library is loaded holds its NOALLOC_SCRATCH_BYTES until the
+// process exits.  All calls share it, and it keeps the previous call's
+// contents (the counter is cleared at the start of every call), so calls whose
+// work overlaps on the GPU (other streams, other host threads) race; serialise
+// them.
+namespace zola {
+constexpr size_t NOALLOC_SCRATCH_BYTES = (size_t)64 << 20;  // 64 MiB
+}  // namespace zola
+
+static __device__ __align__(256) unsigned char g_fit_noalloc_scratch[zola::NOALLOC_SCRATCH_BYTES];
+
+namespace {
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[64] = {};
+
+// Device address of the scratch array on the current device, looked up once
+// per device (host code must not use the array's name as a device pointer).
+void* noalloc_scratch(int device, std::string& err) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (device < 0 || device >= 64) {
+        err = "zola_fit_batch_noalloc: device index out of range";
+        return nullptr;
+    }
+    if (!g_noalloc_ptr[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_fit_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            err = std::string("zola_fit_batch_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+            return nullptr;
+        }
+        g_noalloc_ptr[device] = p;
+    }
+    return g_noalloc_ptr[device];
+}
+}  // namespace
+
+extern "C" int zola_fit_batch_noalloc(zola_psf* psf, int R, const float* d_rois, const double* d_init5, int n,
+                                      const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll,
+                                      int* d_status, int* d_iters, void* stream) {
+    using namespace zola;
+    if (!psf) return ZOLA_E_ARG;
+    zola_ctx* ctx = psf->ctx;
+    if (!prm || prm->precision != ZOLA_PREC_FP64 || prm->max_iter < 1 || prm->max_iter > 1000 ||
+        !(prm->zmax >= prm->zmin) || !(prm->xymax > 0) || !(prm->step_xy > 0) || !(prm->step_z > 0) ||
+        !(prm->tol_xyz >= 0)) {
+        ctx->err = "zola_fit_batch_noalloc: needs valid FP64 fit params (precision = ZOLA_PREC_FP64)";
+        return ZOLA_E_ARG;
+    }
+    if (n < 0 || (n > 0 && (!d_rois || !d_init5 || !d_out5))) {
+        ctx->err = "zola_fit_batch_noalloc: bad n or null buffer";
+        return ZOLA_E_ARG;
+    }
+    if (psf->o.kz_reset) {
+        ctx->err = "zola_fit_batch_noalloc: fit needs a PSF built with kz_reset = 0";
+        return ZOLA_E_ARG;
+    }
+    // Only look the window tables up: building them would allocate.
+    auto it = psf->win.find(R);
+    if (it == psf->win.end()) {
+        ctx->err = "zola_fit_batch_noalloc: tables for this ROI size are not prepared; call "
+                   "zola_psf_model_dev(psf, R, NULL, 0, NULL, NULL, stream) once beforehand";
+        return ZOLA_E_ARG;
+    }
+    WindowTables* w = &it->second;
+    if (n == 0) return ZOLA_OK;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev != ctx->device) {
+        ctx->err = "zola_fit_batch_noalloc: make the PSF's device current first";
+        return ZOLA_E_ARG;
+    }
+    char* base = (char*)noalloc_scratch(dev, ctx->err);
+    if (!base) return ZOLA_E_CUDA;
+    const size_t per_cta = f64_work_bytes(psf->D, w->W, w->R);
+    const int use_smem = per_cta + 8192 <= 200 * 1024;
+    const size_t smem = 8192 + (use_smem ? per_cta : 0);
+    int* counter = (int*)base;
+    char* work = base + 256;
+    const size_t room = NOALLOC_SCRATCH_BYTES - 256;
+    int nblocks = std::min(n, ctx->num_sms * 2);
+    if (use_smem && smem > 110 * 1024) nblocks = std::min(n, ctx->num_sms);
+    if (!use_smem) {
+        if (per_cta > room) {
+            ctx->err = "zola_fit_batch_noalloc: one block's work area (" + std::to_string(per_cta) +
+                       " bytes for this ROI size) exceeds the 64 MiB static scratch";
+            return ZOLA_E_ARG;
+        }
+        nblocks = std::min<long long>(nblocks, (long long)(room / per_cta));
+    }
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    cudaError_t e = cudaFuncSetAttribute(fit_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) e = cudaMemsetAsync(counter, 0, sizeof(int), st);
+    if (e != cudaSuccess) {
+        ctx->err = std::string("zola_fit_batch_noalloc: ") + cudaGetErrorString(e);
+        return ZOLA_E_CUDA;
+    }
+    FitParamsDev fp{prm->zmin, prm->zmax, prm->xymax, prm->tol_xyz, prm->step_xy, prm->step_z, prm->max_iter};
+    WinView wv{w->R, w->W, w->d_C, w->d_G};
+    fit_f64_kernel<<<nblocks, F64_THREADS, smem, st>>>(psf->view, wv, d_rois, d_init5, n, fp, d_out5, d_crlb5, d_nll,
+                                                       d_status, d_iters, work, per_cta, use_smem, counter);
+    ctx->launches++;
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        ctx->err = std::string("zola_fit_batch_noalloc: ") + cudaGetErrorString(e);
+        return ZOLA_E_CUDA;
+    }
+    return ZOLA_OK;
+}
