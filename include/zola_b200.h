@@ -88,7 +88,8 @@ typedef struct {
 #define ZOLA_FIT_STALLED 3
 #define ZOLA_FIT_NAN -1
 
-/* --- context (replaces MyCudaStream.init / destroy, cuda/MyCudaStream.java:36-132) */
+/* --- context (replaces MyCudaStream.init / destroy, cuda/MyCudaStream.java:36-132).
+ * Free every PSF of a context (zola_psf_free) before destroying the context. */
 ZOLA_API int zola_ctx_create(int device, zola_ctx** out);
 ZOLA_API int zola_ctx_destroy(zola_ctx* ctx);
 ZOLA_API const char* zola_last_error(const zola_ctx* ctx);
