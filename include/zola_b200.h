@@ -132,6 +132,69 @@ ZOLA_API int zola_fit_batch_dev(zola_ctx* ctx, zola_psf* psf, int R, const float
                        int n, const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll,
                        int* d_status, int* d_iters, void* stream);
 
+/* --- detection (replaces Predetection / Predetection_cross_: library build,
+ * setImage and convolveNormalizedInFourierDomain; process/cpu/Predetection.java:63-593,
+ * process/gpu/Predetection_cross_.java:104-785).  psf must be built with
+ * kz_reset = 1 (the reference builds its library from DataPhase.psf after
+ * setNwat).  Library: ceil((maxZ-minZ)/step) slices at z = minZ + k*step
+ * (accumulated), R x R each; thr is the NCC threshold (reference: 0.1). */
+typedef struct zola_detector zola_detector;
+ZOLA_API int zola_detector_create(zola_psf* psf, int SX, int SY, int R, double minZ, double maxZ, double step,
+                                  double thr, zola_detector** out);
+ZOLA_API int zola_detector_free(zola_detector* det);
+/* Number of slices; optionally their z (um) and the normalised library PSFs
+ * (nslices x R x R, sum 1), as Predetection.getRange / getPSFNonNormalized. */
+ZOLA_API int zola_detector_info(const zola_detector* det, int* nslices, double* range, double* psfs);
+/* frames: nframes x SX x SY photons (double, first index x).  out: nframes x
+ * cap rows of 7 doubles (score, slice r, i, j, dz, dx, dy), sorted by
+ * descending score with ties in the reference's order; counts[f] = number of
+ * candidates of frame f (if it exceeds cap the list is truncated: retry with
+ * a larger cap). */
+ZOLA_API int zola_detect(zola_detector* det, const double* frames, int nframes, int cap, double* out, int* counts);
+ZOLA_API int zola_detect_dev(zola_detector* det, const double* d_frames, int nframes, int cap, double* d_out,
+                             int* d_counts, void* stream);
+
+/* --- frame localization pipeline (replaces LocalizationPipeline_ / the
+ * detect -> localize -> filter loop; process/cpu/LocalizationPipeline.java:145-1250).
+ * One row per accepted localization, in the ThunderStorm CSV units. */
+typedef struct {
+    int id, frame;
+    double x_nm, y_nm, z_nm;        /* 1000 * (pixel * dx - x) as the reference writes them */
+    double intensity, background;   /* photons, photons / px */
+    double chi2;                    /* scoreCompute: mean (patch - model)^2 / model */
+    double crlb_x_nm, crlb_y_nm, crlb_z_nm;
+} zola_localization;
+
+typedef struct {
+    int patch;                /* ROI side R; must equal the detector's R */
+    double minZ, maxZ;        /* accepted z range (ZfocusCenter -/+ axialRange/2); the fit box is 0.3 um wider */
+    double photon_threshold;  /* photonThreshold */
+    double max_snr;           /* maxSNR (reference: 1) */
+    int max_iter;             /* LM evaluations per ROI */
+    double tol_xyz;           /* LM stopping distance, um */
+    int precision;            /* ZOLA_PREC_FP64 or ZOLA_PREC_SPLIT for the fits */
+    int cand_cap;             /* max candidates per frame (0: 1024) */
+    int frames_per_batch;     /* frames per device batch (0: 1024) */
+} zola_loc_params;
+
+/* frames: nframes x SX x SY photons (double, first index x, already converted
+ * with the camera ADU / gain / offset and clamped at 0 as the reference does).
+ * det: a detector on a kz_reset = 1 PSF; fit_psf: the same calibration with
+ * kz_reset = 0.  Rows are ordered by frame, then by processing order; ids are
+ * 0..n-1; frames are numbered from frame0.  Returns ZOLA_E_ARG with *nout set
+ * to the needed size if out_cap is too small. */
+ZOLA_API int zola_localize_frames(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const double* frames,
+                                  int nframes, int frame0, const zola_loc_params* prm, zola_localization* out,
+                                  int out_cap, int* nout);
+
+/* ThunderStorm-style CSV writer (data/PLocalization.java:224-306,
+ * data/StackLocalization.java:1332-1360): header id,frame,x [nm],...,
+ * occurrenceMerging; values floored to 1e-3 and printed as Java's
+ * Double.toString; drift columns 0.0, occurrence 1.  append = 1 skips the header. */
+ZOLA_API int zola_write_csv(const char* path, const zola_localization* locs, int n, int append);
+/* Java Double.toString formatting of one value (the CSV number format). */
+ZOLA_API int zola_format_double_java(double v, char* buf, int len);
+
 /* Allocation-free FP64 fit (this entry point has no counterpart in the
  * reference).  For callers that must not allocate device memory while they fit
  * (a host application that owns all device memory and lends plugins only its

@@ -56,6 +56,8 @@ def lib():
         L.orc_det_nslices.argtypes = [vp]
         L.orc_det_library.argtypes = [vp, vp, vp]
         L.orc_detect.argtypes = [vp, i, vp, i, vp, vp, i]
+        L.orc_localize_frames.restype = i
+        L.orc_localize_frames.argtypes = [vp, vp, i, vp, d, d, d, d, i, vp, i]
         L.orc_calib_nll.restype = d
         L.orc_calib_nll.argtypes = [vp, i, i, vp, vp, d, d, d, d, d]
         _lib = L
@@ -173,6 +175,15 @@ class OracleDetector:
         psfs = np.zeros((self.nz, self.R, self.R))
         lib().orc_det_library(self.h, _p(rng), _p(psfs))
         return rng, psfs
+
+    def localize_frames(self, fit_psf, frames, minZ, maxZ, photon_thr=500.0, max_snr=1.0, threads=1, cap=100000):
+        """LocalizationPipeline frame loop with the reference coordinate descent.
+        Rows: frame, x_nm, y_nm, z_nm, A, B, chi2, crlbx, crlby, crlbz."""
+        frames = _f64(frames)
+        rows = np.zeros((cap, 10))
+        n = lib().orc_localize_frames(self.h, fit_psf.h, frames.shape[0], _p(frames), minZ, maxZ, photon_thr, max_snr,
+                                      cap, _p(rows), threads)
+        return rows[:min(n, cap)]
 
     def detect(self, frames, cap=4096, threads=1):
         frames = _f64(frames)

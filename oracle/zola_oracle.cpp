@@ -882,6 +882,100 @@ void orc_detect(void* d, int nframes, const double* frames, int cap, double* out
     });
 }
 
+// Frame pipeline (LocalizationThread.run, LocalizationPipeline.java:720-990)
+// with the reference coordinate-descent fit (iterMax 20, z clamp minZ-0.3 ..
+// maxZ+0.3) and finite-difference CRLB.  det uses the resetKz library PSF,
+// psf the fit PSF.  Rows: frame, x_nm, y_nm, z_nm, A, B, chi2, crlbx, crlby,
+// crlbz (nm), in processing order per frame.
+int orc_localize_frames(void* dh, void* ph, int nframes, const double* frames, double minZ, double maxZ,
+                        double photonThr, double maxSNR, int rows_cap, double* rows, int threads) {
+    Detector* D = (Detector*)dh;
+    const Psf* p = (const Psf*)ph;
+    const int SX = D->SX, SY = D->SY, R = D->R, h = R / 2;
+    std::vector<std::vector<std::array<double, 10>>> per(nframes);
+    parallel_for(nframes, threads, [&](int f) {
+        const double* img = frames + (size_t)f * SX * SY;
+        std::vector<std::array<double, 7>> v;
+        det_frame(D, img, v);
+        std::vector<char> mask((size_t)SX * SY, 0);
+        std::vector<double> patch((size_t)R * R), psi((size_t)R * R);
+        int pointer = 0;
+        while (true) {
+            int sel = -1;
+            for (int i = pointer; i < (int)v.size(); ++i) {
+                int ci = (int)std::lround(v[i][2]), cj = (int)std::lround(v[i][3]);
+                if (mask[(size_t)ci * SY + cj]) continue;
+                if (ci > R / 2 + 1 && cj > R / 2 + 1 && ci < SX - R / 2 - 1 && cj < SY - R / 2 - 1) { sel = i; pointer = i + 1; break; }
+            }
+            if (sel < 0) break;
+            int r = (int)std::lround(v[sel][1]), ci = (int)std::lround(v[sel][2]), cj = (int)std::lround(v[sel][3]);
+            bool treated = false;
+            for (int a = 0; a < R && !treated; ++a)
+                for (int b = 0; b < R; ++b) {
+                    if (mask[(size_t)(ci - h + a) * SY + (cj - h + b)]) { treated = true; break; }
+                    patch[(size_t)a * R + b] = img[(size_t)(ci - h + a) * SY + (cj - h + b)];
+                }
+            if (treated) continue;
+            const std::vector<double>& lp = D->libpsf[r];  // getAandB (LocalizationPipeline.java:1119-1162)
+            double maxp = -INFINITY, maxi = -INFINITY;
+            for (int k = 0; k < R * R; ++k) { maxi = std::max(maxi, lp[k]); maxp = std::max(maxp, patch[k]); }
+            double thr = maxi * 0.1, A = 0, B = 0, ca = 0, cb = 0;
+            for (int k = 0; k < R * R; ++k) {
+                if (lp[k] < thr) { B += patch[k]; cb++; } else { A += patch[k]; ca++; }
+            }
+            B = cb != 0 ? B / cb : 0;
+            A -= ca * B;
+            bool part = false;
+            if (maxp / B > maxSNR && B > 0) {
+                CD cd;
+                cd.p = p; cd.R = R; cd.d = patch.data();
+                cd.minZ = minZ - .3; cd.maxZ = maxZ + .3; cd.iterMax = 20; cd.photonThreshold = photonThr;
+                cd.maxShift = p->dx / 2.;
+                cd.psi.resize(R * R); cd.mu.resize(R * R);
+                cd.ta = A; cd.tb = B; cd.tx = -v[sel][5]; cd.ty = -v[sel][6]; cd.tz = D->range[r] + v[sel][4];
+                int st = cd.run();
+                if (st == 1) {
+                    psf_model(p, R, cd.tx, cd.ty, p->zfocus, cd.tz, psi.data(), nullptr);
+                    double mthr = 0;
+                    for (int k = 0; k < R * R; ++k) mthr = std::max(mthr, psi[k] * cd.ta + cd.tb - cd.tb);
+                    mthr *= .2;
+                    if (cd.ta > photonThr && std::fabs(cd.tx) < 10 * p->dx && std::fabs(cd.ty) < 10 * p->dx) {
+                        int px = (int)(ci - (cd.tx / p->dx)), py = (int)(cj - (cd.ty / p->dx));
+                        if (px >= 0 && px < SX && py >= 0 && py < SY && !mask[(size_t)px * SY + py] && cd.tz > minZ && cd.tz < maxZ) {
+                            double chi = 0;
+                            for (int k = 0; k < R * R; ++k) {
+                                double mu = psi[k] * cd.ta + cd.tb;
+                                chi += (patch[k] - mu) * (patch[k] - mu) / mu;
+                            }
+                            chi /= (double)(R * R);
+                            double cr[3];
+                            fisher_crlb_fd(p, R, cd.tx, cd.ty, cd.tz, cd.ta, cd.tb, cr);
+                            per[f].push_back({(double)f, 1000 * (ci * p->dx - cd.tx), 1000 * (cj * p->dx - cd.ty), 1000 * cd.tz,
+                                              cd.ta, cd.tb, chi, 1000 * cr[0], 1000 * cr[1], 1000 * cr[2]});
+                            for (int a = 0; a < R; ++a)
+                                for (int b = 0; b < R; ++b)
+                                    if (psi[(size_t)a * R + b] * cd.ta + cd.tb - cd.tb > mthr) mask[(size_t)(ci - h + a) * SY + (cj - h + b)] = 1;
+                            part = true;
+                        }
+                    }
+                }
+            }
+            if (!part)
+                for (int a = 0; a < R; ++a)
+                    for (int b = 0; b < R; ++b)
+                        if (patch[(size_t)a * R + b] > maxp * .5) mask[(size_t)(ci - h + a) * SY + (cj - h + b)] = 1;
+        }
+    });
+    int n = 0;
+    for (int f = 0; f < nframes; ++f)
+        for (auto& row : per[f]) {
+            if (n < rows_cap)
+                for (int c = 0; c < 10; ++c) rows[(size_t)n * 10 + c] = row[c];
+            ++n;
+        }
+    return n;
+}
+
 // Calibration stack NLL (ZernikePhaseRetrieval.java:1843-1874) for one bead:
 // slices s at zoil = dz[s] + bz, zwat = 0; mu = A*psi + B clamped at 1e-8;
 // NLL = sum mu - d ln mu.  Registration x/y/z enter as the kx, ky, kz_oil

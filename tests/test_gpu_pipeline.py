@@ -1,0 +1,59 @@
+"""GPU frame pipeline (detect -> fit -> filters/mask) against the oracle's
+restatement of LocalizationPipeline with the reference coordinate descent."""
+import numpy as np
+import pytest
+
+import oracle as O
+from common import OPTICS, astig_zernike
+from test_gpu_detect import make_frames
+
+pytestmark = pytest.mark.gpu
+
+
+def match(got, want, tol_nm=20.0):
+    pairs = []
+    used = set()
+    for w in want:
+        best, bk = None, None
+        for k, g in enumerate(got):
+            if k in used or g["frame"] != int(w[0]):
+                continue
+            d = np.hypot(g["x_nm"] - w[1], g["y_nm"] - w[2])
+            if d < tol_nm and (best is None or d < best):
+                best, bk = d, k
+        if bk is not None:
+            used.add(bk)
+            pairs.append((got[bk], w))
+    return pairs
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_pipeline_matches_reference_pipeline(zpkg, ctx, precision):
+    zern = astig_zernike()
+    S, R = 96, 16
+    psf_det = zpkg.PSF(ctx, zpkg.optics(size_fft=64, kz_reset=True, **OPTICS), zern)
+    psf_fit = zpkg.PSF(ctx, zpkg.optics(size_fft=64, **OPTICS), zern)
+    ref_det = O.OraclePSF(64, 0.11, 1.4, 0.66, 1.518, 1.518, 0.9, zern, kz_reset=True)
+    ref_fit = O.OraclePSF(64, 0.11, 1.4, 0.66, 1.518, 1.518, 0.9, zern)
+    frames = make_frames(ref_fit.model, S, 8, seed=77, emitters=4, R=32)
+    minZ, maxZ = -0.6, 0.6
+    det = zpkg.Detector(psf_det, S, S, R, minZ, maxZ, 0.11, 0.1)
+    odet = O.OracleDetector(ref_det, S, S, R, minZ, maxZ, 0.11, 0.1)
+    got = zpkg.localize_frames(ctx, det, psf_fit, frames, minZ, maxZ, photon_threshold=500.0, precision=precision,
+                               max_iter=40)
+    want = odet.localize_frames(ref_fit, frames, minZ, maxZ, photon_thr=500.0, threads=4)
+    assert len(want) > 10
+    assert abs(len(got) - len(want)) <= max(2, 0.1 * len(want))
+    pairs = match(got, want)
+    assert len(pairs) >= 0.9 * len(want)
+    dxy = np.array([max(abs(g["x_nm"] - w[1]), abs(g["y_nm"] - w[2])) for g, w in pairs])
+    dz = np.array([abs(g["z_nm"] - w[3]) for g, w in pairs])
+    dA = np.array([abs(g["intensity"] - w[4]) / w[4] for g, w in pairs])
+    # reference coordinate descent vs LM: same optimum, loose stopping of the former
+    assert np.median(dxy) < 0.5 and np.median(dz) < 1.0 and np.median(dA) < 1e-3
+    assert (dxy < 2.0).mean() > 0.9
+    crx = np.array([abs(g["crlb_x_nm"] - w[7]) / w[7] for g, w in pairs])
+    assert np.median(crx) < 1e-2
+    assert (got["frame"][1:] >= got["frame"][:-1]).all()
+    assert list(got["id"]) == list(range(len(got)))
+    det.close()

@@ -39,6 +39,20 @@ class Optics(ctypes.Structure):
                 ("kz_reset", ctypes.c_int)]
 
 
+class Localization(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_int), ("frame", ctypes.c_int), ("x_nm", ctypes.c_double), ("y_nm", ctypes.c_double),
+                ("z_nm", ctypes.c_double), ("intensity", ctypes.c_double), ("background", ctypes.c_double),
+                ("chi2", ctypes.c_double), ("crlb_x_nm", ctypes.c_double), ("crlb_y_nm", ctypes.c_double),
+                ("crlb_z_nm", ctypes.c_double)]
+
+
+class LocParams(ctypes.Structure):
+    _fields_ = [("patch", ctypes.c_int), ("minZ", ctypes.c_double), ("maxZ", ctypes.c_double),
+                ("photon_threshold", ctypes.c_double), ("max_snr", ctypes.c_double), ("max_iter", ctypes.c_int),
+                ("tol_xyz", ctypes.c_double), ("precision", ctypes.c_int), ("cand_cap", ctypes.c_int),
+                ("frames_per_batch", ctypes.c_int)]
+
+
 class FitParams(ctypes.Structure):
     _fields_ = [("zmin", ctypes.c_double), ("zmax", ctypes.c_double), ("xymax", ctypes.c_double),
                 ("max_iter", ctypes.c_int), ("tol_xyz", ctypes.c_double), ("step_xy", ctypes.c_double),
@@ -48,7 +62,9 @@ class FitParams(ctypes.Structure):
 EXPORTS = ["zola_ctx_create", "zola_ctx_destroy", "zola_last_error", "zola_ctx_stream", "zola_ctx_launches",
            "zola_ctx_set_pool", "zola_psf_load", "zola_psf_free", "zola_psf_info", "zola_psf_model",
            "zola_psf_model_dev", "zola_psf_model_prec", "zola_psf_model_prec_dev", "zola_fit_batch",
-           "zola_fit_batch_dev", "zola_ctx_profile", "zola_ctx_stage_stats", "zola_fit_batch_noalloc"]
+           "zola_fit_batch_dev", "zola_ctx_profile", "zola_ctx_stage_stats", "zola_fit_batch_noalloc",
+           "zola_detector_create", "zola_detector_free", "zola_detector_info", "zola_detect", "zola_detect_dev",
+           "zola_localize_frames", "zola_write_csv", "zola_format_double_java"]
 STAGES = ["split_stage1_pupil_dft", "split_stage2_window_dft", "split_stage3_blur_rows", "split_stage4_blur_cols",
           "split_stage5_likelihood_lm", "fp64_fit", "fp64_model", "other"]
 
@@ -80,6 +96,14 @@ def lib():
         L.zola_psf_model_prec_dev.argtypes = [vp, i, vp, i, vp, vp, i, vp]
         L.zola_ctx_set_pool.argtypes = [vp, i]
         L.zola_ctx_profile.argtypes = [vp, i]
+        L.zola_detector_create.argtypes = [vp, i, i, i, d, d, d, d, ctypes.POINTER(vp)]
+        L.zola_localize_frames.argtypes = [vp, vp, vp, vp, i, i, ctypes.POINTER(LocParams), vp, i, ctypes.POINTER(i)]
+        L.zola_write_csv.argtypes = [ctypes.c_char_p, vp, i, i]
+        L.zola_format_double_java.argtypes = [d, ctypes.c_char_p, i]
+        L.zola_detector_free.argtypes = [vp]
+        L.zola_detector_info.argtypes = [vp, ctypes.POINTER(i), vp, vp]
+        L.zola_detect.argtypes = [vp, vp, i, i, vp, vp]
+        L.zola_detect_dev.argtypes = [vp, vp, i, i, vp, vp, vp]
         L.zola_fit_batch_noalloc.argtypes = [vp, i, vp, vp, i, ctypes.POINTER(FitParams), vp, vp, vp, vp, vp, vp]
         L.zola_ctx_stage_stats.argtypes = [vp, vp, vp, i]
         L.zola_fit_batch.argtypes = [vp, vp, i, vp, vp, i, ctypes.POINTER(FitParams), vp, vp, vp, vp, vp]
@@ -229,6 +253,91 @@ class PSF:
         self.ctx.check(lib().zola_fit_batch_dev(self.ctx.h, self.h, R, _ptr(rois), _ptr(init), n, ctypes.byref(prm),
                                                 _ptr(out), _ptr(crlb), _ptr(nll), _ptr(status), _ptr(iters), stream),
                        "zola_fit_batch_dev")
+
+
+class Detector:
+    """PSF-library NCC detection (Predetection / Predetection_cross_).
+
+    psf must be built with kz_reset=True (the reference builds the library from
+    its resetKz tables).  Frames are (n, SX, SY) photons, first index x."""
+
+    def __init__(self, psf, SX, SY, R, minZ, maxZ, step, thr=0.1):
+        self.psf, self.SX, self.SY, self.R = psf, SX, SY, R
+        h = ctypes.c_void_p()
+        psf.ctx.check(lib().zola_detector_create(psf.h, SX, SY, R, minZ, maxZ, step, thr, ctypes.byref(h)),
+                      "zola_detector_create")
+        self.h = h
+        nz = ctypes.c_int()
+        lib().zola_detector_info(h, ctypes.byref(nz), None, None)
+        self.nz = nz.value
+
+    def library(self):
+        rng = np.zeros(self.nz)
+        psfs = np.zeros((self.nz, self.R, self.R))
+        lib().zola_detector_info(self.h, ctypes.byref(ctypes.c_int()), _ptr(rng), _ptr(psfs))
+        return rng, psfs
+
+    def detect(self, frames, cap=2048):
+        frames = np.ascontiguousarray(frames, dtype=np.float64)
+        nf = frames.shape[0]
+        out = np.zeros((nf, cap, 7))
+        counts = np.zeros(nf, np.int32)
+        self.psf.ctx.check(lib().zola_detect(self.h, _ptr(frames), nf, cap, _ptr(out), _ptr(counts)), "zola_detect")
+        return [out[f, :min(cap, counts[f])] for f in range(nf)], counts
+
+    def detect_dev(self, frames, cap, out, counts, stream=None):
+        self.psf.ctx.check(lib().zola_detect_dev(self.h, _ptr(frames), frames.shape[0], cap, _ptr(out), _ptr(counts),
+                                                 stream), "zola_detect_dev")
+
+    def close(self):
+        if getattr(self, "h", None) and getattr(self.psf, "h", None):
+            lib().zola_detector_free(self.h)
+        self.h = None
+
+
+LOC_COLUMNS = ["id", "frame", "x_nm", "y_nm", "z_nm", "intensity", "background", "chi2", "crlb_x_nm", "crlb_y_nm",
+               "crlb_z_nm"]
+
+
+def localize_frames(ctx, det, fit_psf, frames, minZ, maxZ, photon_threshold=500.0, max_snr=1.0, max_iter=30,
+                    tol_xyz=1e-4, precision=ZOLA_PREC_FP64, frame0=0, cand_cap=1024, frames_per_batch=1024):
+    """Detect and localize every frame (LocalizationPipeline): returns a
+    structured numpy array with LOC_COLUMNS, one row per localization."""
+    frames = np.ascontiguousarray(frames, dtype=np.float64)
+    nf = frames.shape[0]
+    prm = LocParams(det.R, float(minZ), float(maxZ), float(photon_threshold), float(max_snr), int(max_iter),
+                    float(tol_xyz), int(precision), int(cand_cap), int(frames_per_batch))
+    cap = max(64, nf * 64)
+    out = (Localization * cap)()
+    n = ctypes.c_int()
+    ctx.check(lib().zola_localize_frames(ctx.h, det.h, fit_psf.h, _ptr(frames), nf, int(frame0), ctypes.byref(prm),
+                                         ctypes.cast(out, ctypes.c_void_p), cap, ctypes.byref(n)),
+              "zola_localize_frames")
+    dt = np.dtype([(c, np.int32 if c in ("id", "frame") else np.float64) for c in LOC_COLUMNS])
+    arr = np.zeros(n.value, dtype=dt)
+    for k in range(n.value):
+        arr[k] = tuple(getattr(out[k], c) for c in LOC_COLUMNS)
+    return arr
+
+
+def write_csv(path, locs, append=False):
+    """ThunderStorm-style CSV exactly as ZOLA writes it (zola_write_csv)."""
+    n = len(locs)
+    buf = (Localization * max(1, n))()
+    for k in range(n):
+        for c in LOC_COLUMNS:
+            setattr(buf[k], c, locs[k][c].item() if hasattr(locs[k][c], "item") else locs[k][c])
+    rc = lib().zola_write_csv(path.encode(), ctypes.cast(buf, ctypes.c_void_p), n, int(bool(append)))
+    if rc != 0:
+        raise ZolaError(f"zola_write_csv failed ({rc}) for {path}")
+
+
+def java_double(v):
+    """Java Double.toString of v (the CSV number format)."""
+    b = ctypes.create_string_buffer(64)
+    if lib().zola_format_double_java(float(v), b, 64) != 0:
+        raise ZolaError("zola_format_double_java failed")
+    return b.value.decode()
 
 
 def fit_noalloc_dev(psf, rois, init, prm, out, crlb=None, nll=None, status=None, iters=None, stream=None):

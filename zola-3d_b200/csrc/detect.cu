@@ -1,0 +1,404 @@
+// PSF-library cross-correlation detection (process/cpu/Predetection.java:63-593).
+//
+// Per frame (S_x x S_y photons, first index x):
+//   k_det_var    local mean / variance over the R-wide box by the reference's
+//                running sums (Predetection.java:337-405), operation for
+//                operation (no FMA contraction), on the float-rounded image
+//   k_det_corr   normalised cross-correlation with the zero-mean library PSFs.
+//                The reference multiplies unitary FFTs on a zero-padded M x M
+//                grid (M = pow2(2S)); with that padding the product is the
+//                linear correlation corr(i,j) = sum_uv img[i+u-R/2][j+v-R/2]
+//                psf0[u][v], scaled by 1/sqrt(Mx My).  It is computed directly
+//                in FP64 here: score = corr / sqrt(varPSF * varImage)
+//                (-1 / -2 where a variance is not positive, :459-471).
+//   k_det_nms    per slice r in order: tmp = max over j +- 3 where score > 0
+//                (tmp keeps the previous slice's value elsewhere, as the
+//                reference reuses it), then peaks with score > thr equal to
+//                tmp and to the max of tmp over i +- 3, with parabolic x/y/z
+//                refinement (:480-560).  Rows: score, r, i, j, topZ, topX, topY.
+//   k_det_sort   stable sort by descending score (Arrays.sort of the rows in
+//                insertion order r, j, i; :447-454).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+#include "zola_internal.h"
+
+namespace zola {
+
+
+
+// ---------------------------------------------------------------------------
+// Running sums exactly as Predetection.setImage: first along y for every x,
+// then along x for every y.  Double arithmetic with explicit rounding
+// intrinsics so the compiler cannot fuse multiply-adds.
+__global__ void k_det_var(DetView V, const double* frames, double* rowsum, double* rowsq, double* var) {
+    const int f = blockIdx.x, SX = V.SX, SY = V.SY, h = V.R / 2;
+    const double* img = frames + (size_t)f * SX * SY;
+    double* s1 = rowsum + (size_t)f * SX * SY;
+    double* s2 = rowsq + (size_t)f * SX * SY;
+    double* vr = var + (size_t)f * SX * SY;
+    auto F = [&](int i, int j) { return (double)(float)img[(size_t)i * SY + j]; };
+    for (int i = threadIdx.x; i < SX; i += blockDim.x) {
+        double a = 0.0, b = 0.0;
+        for (int t = 0; t < h + 1; ++t)
+            if (t < SY) { a = __dadd_rn(a, F(i, t)); b = __dadd_rn(b, __dmul_rn(F(i, t), F(i, t))); }
+        s1[(size_t)i * SY] = a;
+        s2[(size_t)i * SY] = b;
+        for (int ii = 1; ii < SY; ++ii) {
+            double v = a, w = b;
+            if (ii - h >= 0) { v = __dsub_rn(v, F(i, ii - h)); w = __dsub_rn(w, __dmul_rn(F(i, ii - h), F(i, ii - h))); }
+            if (ii + h < SY) { v = __dadd_rn(v, F(i, ii + h)); w = __dadd_rn(w, __dmul_rn(F(i, ii + h), F(i, ii + h))); }
+            s1[(size_t)i * SY + ii] = v;
+            s2[(size_t)i * SY + ii] = w;
+            a = v;
+            b = w;
+        }
+    }
+    __syncthreads();
+    for (int ii = threadIdx.x; ii < SY; ii += blockDim.x) {
+        double a = 0.0, b = 0.0;
+        for (int t = 0; t < h + 1; ++t)
+            if (t < SX) { a = __dadd_rn(a, s1[(size_t)t * SY + ii]); b = __dadd_rn(b, s2[(size_t)t * SY + ii]); }
+        for (int i = 0; i < SX; ++i) {
+            if (i > 0) {
+                double v = a, w = b;
+                if (i - h >= 0) { v = __dsub_rn(v, s1[(size_t)(i - h) * SY + ii]); w = __dsub_rn(w, s2[(size_t)(i - h) * SY + ii]); }
+                if (i + h < SX) { v = __dadd_rn(v, s1[(size_t)(i + h) * SY + ii]); w = __dadd_rn(w, s2[(size_t)(i + h) * SY + ii]); }
+                a = v;
+                b = w;
+            }
+            const double n = V.norm[(size_t)i * SY + ii];
+            const double mean = __ddiv_rn(a, n);
+            vr[(size_t)i * SY + ii] = __dsub_rn(__ddiv_rn(b, n), __dmul_rn(mean, mean));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Direct FP64 correlation of a 16 x 16 output tile against ZC slices.
+constexpr int DT = 16;
+constexpr int ZC = 8;
+
+__global__ void __launch_bounds__(256) k_det_corr(DetView V, int zc, const double* frames, const double* var,
+                                                  double* score) {
+    extern __shared__ double sm[];
+    const int SX = V.SX, SY = V.SY, R = V.R, Z = V.Z, h = R / 2, TW = DT + R;
+    const int f = blockIdx.z;
+    const int z0 = blockIdx.y * zc;
+    const int tiles_y = (SY + DT - 1) / DT;
+    const int i0 = (blockIdx.x / tiles_y) * DT, j0 = (blockIdx.x % tiles_y) * DT;
+    double* tile = sm;               // TW x TW image with halo
+    double* ps = tile + TW * TW;     // ZC x R x R
+    const double* img = frames + (size_t)f * SX * SY;
+    for (int k = threadIdx.x; k < TW * TW; k += blockDim.x) {
+        const int a = k / TW, b = k % TW;
+        const int i = i0 - h + a, j = j0 - h + b;
+        tile[k] = (i >= 0 && i < SX && j >= 0 && j < SY) ? img[(size_t)i * SY + j] : 0.0;
+    }
+    const int nz = min(zc, Z - z0);
+    for (int k = threadIdx.x; k < nz * R * R; k += blockDim.x) ps[k] = V.psf0[(size_t)z0 * R * R + k];
+    __syncthreads();
+    const int ti = threadIdx.x / DT, tj = threadIdx.x % DT;
+    const int i = i0 + ti, j = j0 + tj;
+    double acc[ZC];
+#pragma unroll
+    for (int q = 0; q < ZC; ++q) acc[q] = 0.0;
+    for (int u = 0; u < R; ++u) {
+        const double* trow = tile + (ti + u) * TW + tj;
+        for (int v = 0; v < R; ++v) {
+            const double x = trow[v];
+#pragma unroll
+            for (int q = 0; q < ZC; ++q)
+                if (q < nz) acc[q] = fma(x, ps[(q * R + u) * R + v], acc[q]);
+        }
+    }
+    if (i >= SX || j >= SY) return;
+    const double vi = var[(size_t)f * SX * SY + (size_t)i * SY + j];
+    for (int q = 0; q < nz; ++q) {
+        const int r = z0 + q;
+        const double vp = V.varpsf[r];
+        const double s = sqrt(vp * vi);
+        double o;
+        if (s > 0) o = (acc[q] * V.inv_m) / s;
+        else if (vp <= 0) o = -1.0;
+        else o = -2.0;
+        score[(((size_t)f * Z + r) * SX + i) * SY + j] = o;
+    }
+}
+
+// ---------------------------------------------------------------------------
+__device__ inline double parabola_top(double xa, double ya, double xb, double yb, double xc, double yc) {
+    const double a = (yc - ya) / ((xc - xa) * (xc - xb)) - (yb - ya) / ((xb - xa) * (xc - xb));
+    const double b = ((yb - ya) / (xb - xa)) - a * (xb + xa);
+    return -b / (2 * a);
+}
+
+// One CTA per frame; slices in order because tmp carries over between them.
+__global__ void __launch_bounds__(1024) k_det_nms(DetView V, const double* score, double* tmp, double* cand,
+                                                  long long* keys, int* counts) {
+    const int f = blockIdx.x, SX = V.SX, SY = V.SY, Z = V.Z, dec = 3;
+    const int lo = max(dec, V.R / 2);
+    const double* sc = score + (size_t)f * Z * SX * SY;
+    double* tm = tmp + (size_t)f * SX * SY;
+    double* out = cand + (size_t)f * V.cap * 7;
+    long long* key = keys + (size_t)f * V.cap;
+    __shared__ int cnt;
+    if (threadIdx.x == 0) cnt = 0;
+    for (int k = threadIdx.x; k < SX * SY; k += blockDim.x) tm[k] = 0.0;
+    __syncthreads();
+    auto S = [&](int r, int i, int j) { return sc[((size_t)r * SX + i) * SY + j]; };
+    for (int r = 0; r < Z; ++r) {
+        for (int k = threadIdx.x; k < SX * SY; k += blockDim.x) {
+            const int i = k / SY, j = k % SY;
+            if (i < lo || i >= SX - lo || j < lo || j >= SY - lo) continue;
+            if (S(r, i, j) > 0) {
+                double t = -INFINITY;
+                for (int a = -dec; a <= dec; ++a) t = fmax(S(r, i, j + a), t);
+                tm[k] = t;
+            }
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < SX * SY; k += blockDim.x) {
+            const int i = k / SY, j = k % SY;
+            if (i < lo || i >= SX - lo || j < lo || j >= SY - lo) continue;
+            const double v = S(r, i, j);
+            if (!(v > V.thr) || v != tm[k]) continue;
+            double mx = -INFINITY;
+            for (int a = -dec; a <= dec; ++a) mx = fmax(tm[(size_t)(i + a) * SY + j], mx);
+            if (mx != v) continue;
+            double tz = 0, tx = 0, ty = 0;
+            if (r > 1 && r < Z - 1) tz = parabola_top(-V.zstep, S(r - 1, i, j), 0, v, V.zstep, S(r + 1, i, j));
+            if (i > 1 && i < SX - 1) tx = parabola_top(-V.dx, S(r, i - 1, j), 0, v, V.dx, S(r, i + 1, j));
+            if (j > 1 && j < SY - 1) ty = parabola_top(-V.dx, S(r, i, j - 1), 0, v, V.dx, S(r, i, j + 1));
+            const int slot = atomicAdd(&cnt, 1);
+            if (slot < V.cap) {
+                double* row = out + (size_t)slot * 7;
+                row[0] = v; row[1] = r; row[2] = i; row[3] = j; row[4] = tz; row[5] = tx; row[6] = ty;
+                key[slot] = ((long long)r * SY + j) * SX + i;  // the reference's insertion order
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) counts[f] = cnt;
+}
+
+// Sort one frame's candidates by (score descending, insertion order ascending).
+__global__ void __launch_bounds__(1024) k_det_sort(DetView V, double* cand, long long* keys, const int* counts,
+                                                   double* out) {
+    extern __shared__ char smraw[];
+    const int f = blockIdx.x, n = min(counts[f], V.cap);
+    int P2 = 1;
+    while (P2 < n) P2 <<= 1;
+    double* s = (double*)smraw;
+    long long* k = (long long*)(s + P2);
+    int* id = (int*)(k + P2);
+    const double* c = cand + (size_t)f * V.cap * 7;
+    const long long* kk = keys + (size_t)f * V.cap;
+    for (int t = threadIdx.x; t < P2; t += blockDim.x) {
+        if (t < n) { s[t] = c[(size_t)t * 7]; k[t] = kk[t]; id[t] = t; }
+        else { s[t] = -INFINITY; k[t] = 0x7fffffffffffffffll; id[t] = -1; }
+    }
+    __syncthreads();
+    // bitonic sort: "before" = higher score, then smaller key
+    for (int size = 2; size <= P2; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int t = threadIdx.x; t < P2; t += blockDim.x) {
+                const int o = t ^ stride;
+                if (o > t) {
+                    const bool up = (t & size) == 0;
+                    const bool t_before = s[t] > s[o] || (s[t] == s[o] && k[t] < k[o]);
+                    if (up != t_before) {
+                        double ts = s[t]; s[t] = s[o]; s[o] = ts;
+                        long long tk = k[t]; k[t] = k[o]; k[o] = tk;
+                        int ti = id[t]; id[t] = id[o]; id[o] = ti;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    double* dst = out + (size_t)f * V.cap * 7;
+    for (int t = threadIdx.x; t < n * 7; t += blockDim.x) {
+        const int row = t / 7, col = t % 7;
+        dst[t] = c[(size_t)id[row] * 7 + col];
+    }
+}
+
+}  // namespace zola
+
+// ------------------------------------------------------------------ host ----
+
+using namespace zola;
+
+extern "C" {
+
+int zola_detector_create(zola_psf* psf, int SX, int SY, int R, double minZ, double maxZ, double step, double thr,
+                         zola_detector** out) {
+    if (!psf || !out) return ZOLA_E_ARG;
+    zola_ctx* ctx = psf->ctx;
+    *out = nullptr;
+    if (SX < 8 || SY < 8 || SX > 4096 || SY > 4096 || R < 4 || R % 2 || R > SX || R > SY || R > 96 || !(step > 0) ||
+        !(maxZ > minZ)) {
+        ctx->err = "zola_detector_create: need 8 <= S <= 4096, even R <= min(S, 96), step > 0, maxZ > minZ";
+        return ZOLA_E_ARG;
+    }
+    int number = (int)std::ceil((maxZ - minZ) / step);  // Predetection.java:120-127
+    if (number < 1 || number > 4096) { ctx->err = "zola_detector_create: bad number of library slices"; return ZOLA_E_ARG; }
+    zola_detector* d = new zola_detector();
+    d->psf = psf;
+    double z = minZ;
+    for (int i = 0; i < number; ++i) { d->range.push_back(z); z += step; }
+    // library PSFs with the FP64 model: x = y = 0, zoil = Zfocus, zwat = range[i]
+    std::vector<double> xyz(3 * (size_t)number);
+    for (int i = 0; i < number; ++i) { xyz[3 * i] = 0; xyz[3 * i + 1] = 0; xyz[3 * i + 2] = d->range[i]; }
+    d->h_psf.resize((size_t)number * R * R);
+    int rc = zola_psf_model(psf, R, xyz.data(), number, d->h_psf.data(), nullptr);
+    if (rc) { delete d; return rc; }
+    std::vector<double> psf0((size_t)number * R * R), varpsf(number), norm((size_t)SX * SY);
+    for (int i = 0; i < number; ++i) {  // Predetection.java:178-204
+        const double* p = d->h_psf.data() + (size_t)i * R * R;
+        double mean = 0;
+        for (int k = 0; k < R * R; ++k) mean += p[k];
+        mean /= (double)R * R;
+        double v = 0;
+        for (int k = 0; k < R * R; ++k) {
+            double q = p[k] - mean;
+            psf0[(size_t)i * R * R + k] = q;
+            v += q * q;
+        }
+        varpsf[i] = v / (double)(R * R);
+    }
+    for (int i = 0; i < SX; ++i)  // Predetection.java:95-116 (index rules kept)
+        for (int ii = 0; ii < SY; ++ii) {
+            int vx1 = R / 2, vx2 = R / 2, vy1 = R / 2, vy2 = R / 2;
+            if (i < R / 2 - 1) vx1 = i + 1;
+            if (i > SX - R / 2 - 2) vx2 = SY - i - 1;
+            if (ii < R / 2 - 1) vy1 = ii + 1;
+            if (ii > SX - R / 2 - 2) vy2 = SY - ii - 2;
+            norm[(size_t)i * SY + ii] = (double)((vx1 + vx2) * (vy1 + vy2));
+        }
+    size_t total = psf0.size() + varpsf.size() + norm.size();
+    cudaError_t e = cudaMalloc(&d->d_lib, total * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemcpy(d->d_lib, psf0.data(), psf0.size() * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d->d_lib + psf0.size(), varpsf.data(), varpsf.size() * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(d->d_lib + psf0.size() + varpsf.size(), norm.data(), norm.size() * 8, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        ctx->err = std::string("zola_detector_create: ") + cudaGetErrorString(e);
+        if (d->d_lib) cudaFree(d->d_lib);
+        delete d;
+        return ZOLA_E_CUDA;
+    }
+    int MX = 1, MY = 1;
+    while (MX < 2 * SX) MX <<= 1;
+    while (MY < 2 * SY) MY <<= 1;
+    DetView& v = d->v;
+    v.SX = SX; v.SY = SY; v.R = R; v.Z = number; v.cap = 0;
+    v.inv_m = 1.0 / std::sqrt((double)MX * (double)MY);
+    v.thr = thr; v.zstep = step; v.dx = psf->o.xystep;
+    v.psf0 = d->d_lib; v.varpsf = d->d_lib + psf0.size(); v.norm = d->d_lib + psf0.size() + varpsf.size();
+    *out = d;
+    return ZOLA_OK;
+}
+
+int zola_detector_free(zola_detector* d) {
+    if (!d) return ZOLA_E_ARG;
+    cudaStreamSynchronize(d->psf->ctx->stream);
+    cudaFree(d->d_lib);
+    delete d;
+    return ZOLA_OK;
+}
+
+int zola_detector_info(const zola_detector* d, int* nslices, double* range, double* psfs) {
+    if (!d || !nslices) return ZOLA_E_ARG;
+    *nslices = d->v.Z;
+    if (range)
+        for (int i = 0; i < d->v.Z; ++i) range[i] = d->range[i];
+    if (psfs)
+        for (size_t k = 0; k < d->h_psf.size(); ++k) psfs[k] = d->h_psf[k];
+    return ZOLA_OK;
+}
+
+int zola_detect_dev(zola_detector* d, const double* d_frames, int nframes, int cap, double* d_out, int* d_counts,
+                    void* stream) {
+    if (!d) return ZOLA_E_ARG;
+    zola_ctx* ctx = d->psf->ctx;
+    if (nframes < 0 || cap < 1 || cap > 8192 || (nframes > 0 && (!d_frames || !d_out || !d_counts))) {
+        ctx->err = "zola_detect: bad nframes / cap (1..8192) or null buffer";
+        return ZOLA_E_ARG;
+    }
+    if (nframes == 0) return ZOLA_OK;
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    DetView v = d->v;
+    v.cap = cap;
+    const size_t SS = (size_t)v.SX * v.SY;
+    // scratch: rowsum, rowsq, var, tmp (4 x SS per frame), scores (Z x SS), candidates, keys
+    const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)nframes, ((size_t)1 << 31) / ((4 + v.Z) * SS * 8 + (size_t)cap * 64)));
+    const size_t per = (4 + v.Z) * SS * 8 + (size_t)cap * 7 * 8 + (size_t)cap * 8;
+    if (ensure_scratch(ctx, per * chunk + 1024, ctx->err)) return ZOLA_E_CUDA;
+    for (int f0 = 0; f0 < nframes; f0 += chunk) {
+        const int nf = std::min(chunk, nframes - f0);
+        char* b = (char*)ctx->scratch;
+        double* rowsum = (double*)b; b += nf * SS * 8;
+        double* rowsq = (double*)b; b += nf * SS * 8;
+        double* var = (double*)b; b += nf * SS * 8;
+        double* tmp = (double*)b; b += nf * SS * 8;
+        double* score = (double*)b; b += nf * v.Z * SS * 8;
+        double* cand = (double*)b; b += (size_t)nf * cap * 7 * 8;
+        long long* keys = (long long*)b;
+        const double* fr = d_frames + (size_t)f0 * SS;
+        prof_begin(ctx, 7, st);
+        k_det_var<<<nf, 256, 0, st>>>(v, fr, rowsum, rowsq, var);
+        const int tiles = ((v.SX + DT - 1) / DT) * ((v.SY + DT - 1) / DT);
+        const size_t tile_b = (size_t)(DT + v.R) * (DT + v.R) * 8, slice_b = (size_t)v.R * v.R * 8;
+        const int zc = (int)std::max<size_t>(1, std::min<size_t>(ZC, (200 * 1024 - tile_b) / slice_b));
+        const size_t smem = tile_b + (size_t)zc * slice_b;
+        cudaFuncSetAttribute(k_det_corr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        dim3 grid(tiles, (v.Z + zc - 1) / zc, nf);
+        k_det_corr<<<grid, 256, smem, st>>>(v, zc, fr, var, score);
+        k_det_nms<<<nf, 1024, 0, st>>>(v, score, tmp, cand, keys, d_counts + f0);
+        int p2 = 1;
+        while (p2 < cap) p2 <<= 1;
+        const size_t ssort = (size_t)p2 * (8 + 8 + 4);
+        cudaFuncSetAttribute(k_det_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssort);
+        k_det_sort<<<nf, 1024, ssort, st>>>(v, cand, keys, d_counts + f0, d_out + (size_t)f0 * cap * 7);
+        prof_end(ctx, st);
+        ctx->launches += 4;
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) { ctx->err = std::string("zola_detect: ") + cudaGetErrorString(e); return ZOLA_E_CUDA; }
+    }
+    return ZOLA_OK;
+}
+
+int zola_detect(zola_detector* d, const double* frames, int nframes, int cap, double* out, int* counts) {
+    if (!d) return ZOLA_E_ARG;
+    zola_ctx* ctx = d->psf->ctx;
+    if (nframes < 0 || cap < 1 || cap > 8192 || (nframes > 0 && (!frames || !out || !counts))) {
+        ctx->err = "zola_detect: bad nframes / cap (1..8192) or null buffer";
+        return ZOLA_E_ARG;
+    }
+    if (nframes == 0) return ZOLA_OK;
+    const size_t SS = (size_t)d->v.SX * d->v.SY;
+    double* df = nullptr;
+    double* dout = nullptr;
+    int* dc = nullptr;
+    cudaError_t e = cudaMalloc(&df, SS * nframes * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&dout, (size_t)nframes * cap * 7 * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&dc, (size_t)nframes * 4);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(df, frames, SS * nframes * 8, cudaMemcpyHostToDevice, ctx->stream);
+    int rc = ZOLA_OK;
+    if (e == cudaSuccess) rc = zola_detect_dev(d, df, nframes, cap, dout, dc, ctx->stream);
+    if (e == cudaSuccess && rc == ZOLA_OK) {
+        e = cudaMemcpyAsync(counts, dc, (size_t)nframes * 4, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, (size_t)nframes * cap * 7 * 8, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    }
+    if (df) cudaFree(df);
+    if (dout) cudaFree(dout);
+    if (dc) cudaFree(dc);
+    if (e != cudaSuccess) { ctx->err = std::string("zola_detect: ") + cudaGetErrorString(e); return ZOLA_E_CUDA; }
+    return rc;
+}
+
+}  // extern "C"

@@ -81,6 +81,25 @@ struct zola_ctx {
 };
 
 namespace zola {
+struct DetView {
+    int SX, SY, R, Z, cap;
+    double inv_m;        // 1 / sqrt(Mx My)
+    double thr, zstep, dx;
+    const double* psf0;  // Z x R x R zero-mean library PSFs
+    const double* varpsf;
+    const double* norm;  // SX x SY box counts (normImage)
+};
+}  // namespace zola
+
+struct zola_detector {
+    zola_psf* psf = nullptr;
+    zola::DetView v{};
+    std::vector<double> range;
+    double* d_lib = nullptr;    // psf0 | varpsf | norm
+    std::vector<double> h_psf;  // Z x R x R normalised library PSFs (pipeline initialisation)
+};
+
+namespace zola {
 // Kernel-timing helpers (capi.cu): bracket a launch when profiling is on.
 void prof_begin(zola_ctx* ctx, int stage, cudaStream_t st);
 void prof_end(zola_ctx* ctx, cudaStream_t st);
