@@ -195,6 +195,28 @@ ZOLA_API int zola_write_csv(const char* path, const zola_localization* locs, int
 /* Java Double.toString formatting of one value (the CSV number format). */
 ZOLA_API int zola_format_double_java(double v, char* buf, int len);
 
+/* --- Zernike calibration from bead z-stacks (replaces ZernikePhaseRetrieval's
+ * stack NLL and its coordinate-wise finite-difference updates;
+ * process/cpu/ZernikePhaseRetrieval.java:1081-1198, 1843-1874).
+ * Bead b, slice s: PSF at (x_b, y_b, zoil = dz[s] + z_b, zwat = 0) with phase
+ * sum_{i>=3} zernike[i] Z_i (modes 0-2, the reference's per-bead registration,
+ * are carried as x_b, y_b, z_b and ignored in zernike); mu = A_b psi + B_b
+ * (floored at 1e-8 as the reference); NLL = sum mu - d ln mu, FP64 on the GPU.
+ * bead: nbead x (x, y, z, A, B); stacks: nbead x nslice x R x R photons. */
+ZOLA_API int zola_calib_forward(zola_psf* psf, int R, int nz, const double* zernike, int nbead, int nslice,
+                                const double* dz, const double* bead, const double* stacks, double* nll,
+                                double* model /* nullable: nbead x nslice x R x R */);
+/* NLL and its exact gradient by the hand-written adjoint: grad_zernike[nz]
+ * (0 for modes 0-2) and grad_bead[nbead x 5]. */
+ZOLA_API int zola_calib_backward(zola_psf* psf, int R, int nz, const double* zernike, int nbead, int nslice,
+                                 const double* dz, const double* bead, const double* stacks, double* nll,
+                                 double* grad_zernike, double* grad_bead);
+/* Levenberg-Marquardt fit of zernike[3..nz) and every bead's x, y, z, A, B
+ * (updated in place): adjoint gradient, Gauss-Newton matrix from forward
+ * tangents, FP64 damped solve. */
+ZOLA_API int zola_calib_fit(zola_psf* psf, int R, int nz, double* zernike, int nbead, int nslice, const double* dz,
+                            double* bead, const double* stacks, int max_iter, double* nll, int* iters);
+
 /* Allocation-free FP64 fit (this entry point has no counterpart in the
  * reference).  For callers that must not allocate device memory while they fit
  * (a host application that owns all device memory and lends plugins only its

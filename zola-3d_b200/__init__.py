@@ -64,7 +64,8 @@ EXPORTS = ["zola_ctx_create", "zola_ctx_destroy", "zola_last_error", "zola_ctx_s
            "zola_psf_model_dev", "zola_psf_model_prec", "zola_psf_model_prec_dev", "zola_fit_batch",
            "zola_fit_batch_dev", "zola_ctx_profile", "zola_ctx_stage_stats", "zola_fit_batch_noalloc",
            "zola_detector_create", "zola_detector_free", "zola_detector_info", "zola_detect", "zola_detect_dev",
-           "zola_localize_frames", "zola_write_csv", "zola_format_double_java"]
+           "zola_localize_frames", "zola_write_csv", "zola_format_double_java", "zola_calib_forward",
+           "zola_calib_backward", "zola_calib_fit"]
 STAGES = ["split_stage1_pupil_dft", "split_stage2_window_dft", "split_stage3_blur_rows", "split_stage4_blur_cols",
           "split_stage5_likelihood_lm", "fp64_fit", "fp64_model", "other"]
 
@@ -99,6 +100,9 @@ def lib():
         L.zola_detector_create.argtypes = [vp, i, i, i, d, d, d, d, ctypes.POINTER(vp)]
         L.zola_localize_frames.argtypes = [vp, vp, vp, vp, i, i, ctypes.POINTER(LocParams), vp, i, ctypes.POINTER(i)]
         L.zola_write_csv.argtypes = [ctypes.c_char_p, vp, i, i]
+        L.zola_calib_forward.argtypes = [vp, i, i, vp, i, i, vp, vp, vp, vp, vp]
+        L.zola_calib_backward.argtypes = [vp, i, i, vp, i, i, vp, vp, vp, vp, vp, vp]
+        L.zola_calib_fit.argtypes = [vp, i, i, vp, i, i, vp, vp, vp, i, vp, vp]
         L.zola_format_double_java.argtypes = [d, ctypes.c_char_p, i]
         L.zola_detector_free.argtypes = [vp]
         L.zola_detector_info.argtypes = [vp, ctypes.POINTER(i), vp, vp]
@@ -293,6 +297,50 @@ class Detector:
         if getattr(self, "h", None) and getattr(self.psf, "h", None):
             lib().zola_detector_free(self.h)
         self.h = None
+
+
+class Calibration:
+    """Bead z-stack calibration (ZernikePhaseRetrieval) on a kz_reset=False PSF.
+
+    stacks: (nbead, nslice, R, R) photons; dz: (nslice,) slice positions (um);
+    bead: (nbead, 5) = x, y, z, A, B; zernike: (nz,) radians (modes 0-2 unused)."""
+
+    def __init__(self, psf, stacks, dz):
+        self.psf = psf
+        self.stacks = np.ascontiguousarray(stacks, dtype=np.float64)
+        self.dz = np.ascontiguousarray(dz, dtype=np.float64)
+        self.nb, self.ns, self.R = self.stacks.shape[0], self.stacks.shape[1], self.stacks.shape[2]
+
+    def forward(self, zernike, bead, model=False):
+        z = np.ascontiguousarray(zernike, dtype=np.float64)
+        b = np.ascontiguousarray(bead, dtype=np.float64)
+        nll = np.zeros(1)
+        m = np.zeros_like(self.stacks) if model else None
+        self.psf.ctx.check(lib().zola_calib_forward(self.psf.h, self.R, len(z), _ptr(z), self.nb, self.ns, _ptr(self.dz),
+                                                    _ptr(b), _ptr(self.stacks), _ptr(nll), _ptr(m)),
+                           "zola_calib_forward")
+        return (nll[0], m) if model else nll[0]
+
+    def backward(self, zernike, bead):
+        z = np.ascontiguousarray(zernike, dtype=np.float64)
+        b = np.ascontiguousarray(bead, dtype=np.float64)
+        nll = np.zeros(1)
+        gz = np.zeros(len(z))
+        gb = np.zeros((self.nb, 5))
+        self.psf.ctx.check(lib().zola_calib_backward(self.psf.h, self.R, len(z), _ptr(z), self.nb, self.ns,
+                                                     _ptr(self.dz), _ptr(b), _ptr(self.stacks), _ptr(nll), _ptr(gz),
+                                                     _ptr(gb)), "zola_calib_backward")
+        return nll[0], gz, gb
+
+    def fit(self, zernike, bead, max_iter=30):
+        z = np.array(zernike, dtype=np.float64)
+        b = np.array(bead, dtype=np.float64)
+        nll = np.zeros(1)
+        it = ctypes.c_int()
+        self.psf.ctx.check(lib().zola_calib_fit(self.psf.h, self.R, len(z), _ptr(z), self.nb, self.ns, _ptr(self.dz),
+                                                _ptr(b), _ptr(self.stacks), int(max_iter), _ptr(nll), ctypes.byref(it)),
+                           "zola_calib_fit")
+        return z, b, nll[0], it.value
 
 
 LOC_COLUMNS = ["id", "frame", "x_nm", "y_nm", "z_nm", "intensity", "background", "chi2", "crlb_x_nm", "crlb_y_nm",
