@@ -239,6 +239,37 @@ ZOLA_API int zola_fit_batch_noalloc(zola_psf* psf, int R, const float* d_rois, c
 /* Upper bound on the split fit's slot pool (ROIs in flight); 0 = automatic.
  * Smaller pools keep the stage intermediates resident in L2. */
 ZOLA_API int zola_ctx_set_pool(zola_ctx* ctx, int max_slots);
+/* Split fit kernel layout: ZOLA_SPLIT_STAGED (default) runs the five stages
+ * as separate kernels through global memory; ZOLA_SPLIT_FUSED runs stage 1
+ * plus one kernel for stages 2-5 per LM round (same arithmetic, FP32 sums in
+ * another order).  Windows whose fused plan does not fit in shared memory
+ * always run staged. */
+#define ZOLA_SPLIT_STAGED 0
+#define ZOLA_SPLIT_FUSED 1
+ZOLA_API int zola_ctx_set_split_mode(zola_ctx* ctx, int mode);
+
+/* ---- CRLB curves and the z-centre search ------------------------------- */
+/* Cramer-Rao bounds (x, y, z, A, B) of an emitter at (0, 0, z[i]) (um), zoil =
+ * optics.zfocus, for n depths, from the finite-difference Fisher matrix of
+ * process/cpu/CRLB.java:255-340 (computeFisher): central steps h (um) in x, y,
+ * z; mu = photons psi + background; the A row steps the formed mean by +-a_step
+ * photons (dmu/dA = mu a_step / h, as the reference) and the B row by +-h.
+ * R is the model side (the reference uses the FFT grid size).  Replaces the
+ * per-depth Java loops of CRLB.run (:73-160).  crlb5 is n x 5 (host). */
+ZOLA_API int zola_crlb_curve(zola_psf* psf, int R, const double* z, int n, double photons, double background,
+                             double h, double a_step, double* crlb5);
+/* SearchPSFcenter.getPosition (process/cpu/SearchPSFcenter.java:37-84): the
+ * depth z (um) that the localization pipeline stores as ZfocusCenter and
+ * centres its [minZ, maxZ] = ZfocusCenter -+ axialRange / 2 on
+ * (process/cpu/LocalizationPipeline.java:157-172).  Variant ZOLA_CENTER_CPU
+ * follows process/cpu/SearchPSFcenter.java (h = 5 nm, A step 100 h);
+ * ZOLA_CENTER_GPU follows process/gpu/SearchPSFcenter_.java (h = 0.5 nm, A step
+ * h, and zfocus at once when n_oil == n_wat).  3000 photons, background 50, as
+ * the reference.  axial_range <= 0 returns optics.zfocus.  R as above (the
+ * reference builds its model at the FFT size, SearchPSFcenter.java:31). */
+#define ZOLA_CENTER_CPU 0
+#define ZOLA_CENTER_GPU 1
+ZOLA_API int zola_psf_center_search(zola_psf* psf, int R, double axial_range, int variant, double* z_center);
 
 /* Per-kernel timing.  With profiling on, every kernel launch of a fit or model
  * call is bracketed by CUDA events on its stream and the elapsed device time is

@@ -50,6 +50,9 @@ def lib():
         L.orc_nll_grad.restype = d
         L.orc_nll_grad.argtypes = [vp, i, vp, vp, vp, vp]
         L.orc_crlb_fd.argtypes = [vp, i, vp, vp]
+        L.orc_center_search.restype = d
+        L.orc_center_search.argtypes = [vp, i, d, i, vp]
+        L.orc_crlb_curve.argtypes = [vp, i, i, vp, d, d, d, d, vp]
         L.orc_det_create.restype = vp
         L.orc_det_create.argtypes = [vp, i, i, i, d, d, d, d]
         L.orc_det_destroy.argtypes = [vp]
@@ -148,6 +151,21 @@ class OraclePSF:
         th = _f64(theta)
         out = np.zeros(3)
         lib().orc_crlb_fd(self.h, R, _p(th), _p(out))
+        return out
+
+    def center_search(self, R, axial_range, variant=0):
+        """SearchPSFcenter.getPosition (variant 0: process/cpu, 1: process/gpu form)."""
+        st = ctypes.c_int()
+        z = lib().orc_center_search(self.h, int(R), float(axial_range), int(variant), ctypes.byref(st))
+        if st.value:
+            raise IndexError("center search: range window ran past the CRLB table")
+        return z
+
+    def crlb_curve(self, R, z, photons=3000.0, bg=50.0, h=0.005, a_step=0.5):
+        """CRLB (x, y, z, A, B) at (0, 0, z) from the finite-difference Fisher matrix."""
+        z = _f64(z)
+        out = np.zeros((len(z), 5))
+        lib().orc_crlb_curve(self.h, int(R), len(z), _p(z), photons, bg, h, a_step, _p(out))
         return out
 
     def calib_nll(self, R, dz, stack, x, y, z, A, B):

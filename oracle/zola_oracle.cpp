@@ -23,6 +23,8 @@
 //   likelihood        process/cpu/Localization.java:1125-1143
 //   coordinate descent process/cpu/Localization.java:491-1058
 //   Fisher / CRLB     process/cpu/Localization.java:317-451
+//   z-centre search   process/cpu/SearchPSFcenter.java:37-330 (and the GPU
+//                     form process/gpu/SearchPSFcenter_.java)
 //   detection         process/cpu/Predetection.java:63-593
 //   calibration NLL   process/cpu/ZernikePhaseRetrieval.java:1843-1874
 // plus the FP64 Levenberg-Marquardt fit of the same Poisson NLL with analytic
@@ -388,10 +390,13 @@ struct CD {
 
 // Finite-difference Fisher matrix and CRLB, Localization.java:317-451,
 // including its A-derivative, which differentiates mu*(a+-h)+b (mu, not psi).
-void fisher_crlb_fd(const Psf* p, int R, double x, double y, double z, double a, double b,
-                    double* crlb3) {
+// Finite-difference Fisher matrix of Localization.java:317-451 (also
+// process/cpu/CRLB.java:255-340 and SearchPSFcenter.java:210-330): central
+// differences of step h in x, y, z; the A and B rows perturb the already
+// formed mean f1 = a psi + b, so dmu/dA = f1 * ha / h and dmu/dB = 1.
+void fisher_fd(const Psf* p, int R, double x, double y, double z, double a, double b, double h, double ha,
+               double F[5][5]) {
     int n = R * R;
-    double h = .0005;
     std::vector<double> f(n), f1(n), f0[5], f2[5], tmp(n);
     for (int q = 0; q < 5; ++q) { f0[q].resize(n); f2[q].resize(n); }
     psf_model(p, R, x, y, p->zfocus, z, f.data(), nullptr);
@@ -404,10 +409,9 @@ void fisher_crlb_fd(const Psf* p, int R, double x, double y, double z, double a,
         for (int k = 0; k < n; ++k) f0[q][k] = tmp[k] * a + b;
     }
     for (int k = 0; k < n; ++k) {
-        f0[3][k] = f1[k] * (a - h) + b; f2[3][k] = f1[k] * (a + h) + b;
+        f0[3][k] = f1[k] * (a - ha) + b; f2[3][k] = f1[k] * (a + ha) + b;
         f0[4][k] = f1[k] * a + (b - h); f2[4][k] = f1[k] * a + (b + h);
     }
-    double F[5][5];
     for (int q = 0; q < 5; ++q)
         for (int qq = 0; qq < 5; ++qq) {
             double s = 0;
@@ -418,7 +422,11 @@ void fisher_crlb_fd(const Psf* p, int R, double x, double y, double z, double a,
             }
             F[q][qq] = s;
         }
-    // Gauss-Jordan inverse with partial pivoting; on failure fall back to 1/F_ii.
+}
+
+// sqrt(diag(F^-1)) (Gauss-Jordan with partial pivoting); when F is singular,
+// sqrt(1 / F_ii) as the reference's fallback.
+void crlb_from_fisher(const double F[5][5], double* crlb, int nout) {
     double M[5][10];
     for (int i = 0; i < 5; ++i)
         for (int j = 0; j < 10; ++j) M[i][j] = j < 5 ? F[i][j] : (j - 5 == i ? 1 : 0);
@@ -435,10 +443,89 @@ void fisher_crlb_fd(const Psf* p, int R, double x, double y, double z, double a,
             for (int j = 0; j < 10; ++j) M[r][j] -= fct * M[c][j];
         }
     }
-    for (int i = 0; i < 3; ++i) {
-        if (ok) crlb3[i] = std::sqrt(M[i][5 + i]);
-        else crlb3[i] = F[i][i] != 0 ? std::sqrt(1 / F[i][i]) : 1.79769313486231570e308;
+    for (int i = 0; i < nout; ++i) {
+        if (ok) crlb[i] = std::sqrt(M[i][5 + i]);
+        else crlb[i] = F[i][i] != 0 ? std::sqrt(1 / F[i][i]) : 1.79769313486231570e308;
     }
+}
+
+void fisher_crlb_fd(const Psf* p, int R, double x, double y, double z, double a, double b,
+                    double* crlb3) {
+    double F[5][5];
+    fisher_fd(p, R, x, y, z, a, b, .0005, .0005, F);
+    crlb_from_fisher(F, crlb3, 3);
+}
+
+// ------------------------------------------------------ z-centre search ----
+// process/cpu/SearchPSFcenter.java:37-203 (variant 0: h = 5 nm, A step 100 h)
+// and process/gpu/SearchPSFcenter_.java (variant 1: h = 0.5 nm, A step h,
+// returns zfocus at once when n_oil == n_wat).  Emitter at (0, 0, zwat = u),
+// zoil = zfocus, 3000 photons, background 50; the model is the R x R field
+// with R the grid size the caller loaded (SearchPSFcenter.java:31 builds it
+// at the FFT size).  Loops keep the reference's floating-point accumulation.
+struct CenterSearch {
+    const Psf* p;
+    int R;
+    double h, ha;
+    double crlb_xy(double z) const {
+        double F[5][5], c[5];
+        fisher_fd(p, R, 0, 0, z, 3000, 50, h, ha, F);
+        crlb_from_fisher(F, c, 5);
+        return std::sqrt(c[0] * c[0] + c[1] * c[1]);
+    }
+    double min_position(double minZ, double maxZ, double stepZ) const {  // :173-203
+        double best = INFINITY, pos = 0;
+        for (double u = minZ; u < maxZ; u += stepZ) {
+            double c = crlb_xy(u);
+            if (best > c) { best = c; pos = u; }
+        }
+        return pos;
+    }
+    bool min_range(double minZ, double maxZ, double stepZ, double axialRange, double* out) const {  // :88-170
+        double ar = axialRange / 2;
+        std::vector<double> crlb;
+        for (double u = minZ - ar / 2; u <= maxZ + ar / 2; u += stepZ) crlb.push_back(crlb_xy(u));
+        double best = INFINITY, pos = 0;
+        int nb = (int)(ar / (2 * stepZ));
+        for (double u = minZ; u < maxZ; u += stepZ) {
+            double s = 0;
+            int nb2 = -(int)(ar / (2 * stepZ));
+            for (double i = -ar / 2; i <= ar / 2; i += stepZ) {
+                int k = nb + nb2;
+                if (k < 0 || k >= (int)crlb.size()) return false;
+                s += crlb[k];
+                nb2++;
+            }
+            if (best > s) { best = s; pos = u; }
+            nb++;
+        }
+        *out = pos;
+        return true;
+    }
+};
+
+double center_search(const Psf* p, int R, double axialRange, int variant, int* status) {  // :37-84
+    *status = 0;
+    double zfocus = p->zfocus;
+    if (axialRange <= 0) return zfocus;
+    if (variant == 1 && p->n_oil == p->n_wat) return zfocus;
+    CenterSearch cs{p, R, variant == 1 ? .0005 : .005, variant == 1 ? .0005 : .005 * 100};
+    double stepZ = p->dx * 5;
+    double minZ = zfocus - 2 * axialRange - std::fabs(zfocus);
+    double maxZ = zfocus + std::fabs(zfocus) + 2 * axialRange;
+    double position = cs.min_position(minZ, maxZ, stepZ);
+    double old = INFINITY;
+    for (int i = 0; i < 10; i++) {
+        minZ = position - stepZ * 5;
+        maxZ = position + stepZ * 5;
+        stepZ = stepZ / 2;
+        position = cs.min_position(minZ, maxZ, stepZ);
+        if (std::fabs(old - position) < 0.00001) break;
+        old = position;
+    }
+    double out = position;
+    if (!cs.min_range(position - axialRange * 2, position + axialRange * 2, p->dx, axialRange, &out)) *status = -1;
+    return out;
 }
 
 // ------------------------------------------------------------ LM fit -------
@@ -852,6 +939,17 @@ double orc_nll_grad(void* h, int R, const double* patch, const double* th, doubl
     return v;
 }
 
+double orc_center_search(void* h, int R, double axial_range, int variant, int* status) {
+    return center_search((Psf*)h, R, axial_range, variant, status);
+}
+void orc_crlb_curve(void* h, int R, int n, const double* z, double photons, double bg, double step, double a_step,
+                    double* crlb5) {
+    for (int i = 0; i < n; ++i) {
+        double F[5][5];
+        fisher_fd((Psf*)h, R, 0, 0, z[i], photons, bg, step, a_step, F);
+        crlb_from_fisher(F, crlb5 + 5 * i, 5);
+    }
+}
 void orc_crlb_fd(void* h, int R, const double* th, double* crlb3) {
     const Psf* p = (const Psf*)h;
     fisher_crlb_fd(p, R, th[0], th[1], th[2], th[3], th[4], crlb3);

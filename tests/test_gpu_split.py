@@ -72,3 +72,29 @@ def test_split_fit_small_pool_refills(zpkg, ctx):
     assert (small["iters"] > 0).all()
     assert np.array_equal(full["status"], small["status"])
     assert np.allclose(full["theta"], small["theta"], rtol=0, atol=1e-9)
+
+
+@pytest.mark.parametrize("N,R,zern", CASES)
+def test_fused_and_staged_split_kernels_agree(zpkg, ctx, N, R, zern):
+    """The five separate stage kernels (default) and stage 1 + fused stages 2-5
+    compute the same fits: only the FP32 accumulation order differs, so the
+    results agree to well inside the fit tolerance (0.1 nm)."""
+    psf = make(zpkg, ctx, N, zern)
+    ref = O.OraclePSF(N, 0.11, 1.4, 0.66, 1.518, 1.518, 0.9, zern, gauss_f32=False)
+    rois, truth = synth_rois(ref.model, R, 40, seed=9 + R, zrange=0.6, photons=3000)
+    init = truth.copy()
+    init[:, :2] = 0
+    init[:, 2] = np.round(truth[:, 2] / 0.1) * 0.1
+    prm = zpkg.PSF.fit_params(-1.0, 1.0, R * 0.11 / 2, max_iter=40, tol_xyz=1e-4, precision=zpkg.ZOLA_PREC_SPLIT)
+    staged = psf.fit(rois, init, prm)
+    ctx.set_split_mode("fused")
+    try:
+        fused = psf.fit(rois, init, prm)
+    finally:
+        ctx.set_split_mode("staged")
+    ok = (fused["status"] == 1) & (staged["status"] == 1)
+    assert ok.mean() > 0.8
+    d = theta_diff(fused["theta"][ok], staged["theta"][ok], z_symmetric(zern))
+    assert d[:, :3].max() * 1000 < 0.25
+    assert np.median(d[:, :3]) * 1000 < 0.02
+    assert (d[:, 3] / staged["theta"][ok, 3]).max() < 5e-4

@@ -102,3 +102,82 @@ def test_detection_finds_isolated_emitter():
     c = det.detect(img[None])[0]
     assert len(c) >= 1
     assert (int(c[0, 2]), int(c[0, 3])) in [(32, 38), (31, 38), (32, 37), (33, 38), (32, 39)]
+
+
+def _center_psf(N=64, zfocus=0.4, n_wat=1.33):
+    o = OPTICS
+    return O.OraclePSF(N, o["xystep"], o["na"], o["wavelength"], o["n_oil"], n_wat, o["sigma"], astig_zernike(),
+                       zfocus=zfocus, gauss_f32=False)
+
+
+def test_fd_fisher_crlb_matches_the_analytic_fisher_with_the_reference_A_row():
+    """CRLB.computeFisher: central differences in x, y, z; the A row perturbs the
+    formed mean (dmu/dA = mu a_step / h), the B row has dmu/dB = 1."""
+    p = _center_psf()
+    z = np.array([-0.3, 0.1, 0.45])
+    ph, bg, h, ha = 3000.0, 50.0, 5e-4, 5e-4
+    c = p.crlb_curve(32, z, ph, bg, h, ha)
+    for k, zz in enumerate(z):
+        psi, d = p.model(32, [0.0, 0.0, zz], derivs=True)
+        mu = ph * psi[0] + bg
+        J = [ph * d[0, 0], ph * d[0, 1], ph * d[0, 2], mu * (ha / h), np.ones_like(mu)]
+        F = np.array([[np.sum(a * b / mu) for b in J] for a in J])
+        assert np.allclose(c[k], np.sqrt(np.diag(np.linalg.inv(F))), rtol=1e-4)
+
+
+def _center_search_py(p, R, axial, dx, zfocus):
+    """SearchPSFcenter.getPosition restated in Python over the oracle's CRLB curve."""
+    lat = lambda zs: np.hypot(*p.crlb_curve(R, zs, 3000.0, 50.0, 0.005, 0.5)[:, :2].T)
+
+    def frange(a, b, s, incl=False):
+        out, u = [], a
+        while (u <= b) if incl else (u < b):
+            out.append(u)
+            u += s
+        return out
+
+    def min_pos(a, b, s):
+        zs = frange(a, b, s)
+        c = lat(zs)
+        best, pos = np.inf, 0.0
+        for u, v in zip(zs, c):
+            if best > v:
+                best, pos = v, u
+        return pos
+
+    step = dx * 5
+    pos = min_pos(zfocus - 2 * axial - abs(zfocus), zfocus + abs(zfocus) + 2 * axial, step)
+    old = np.inf
+    for _ in range(10):
+        a, b = pos - step * 5, pos + step * 5
+        step = step / 2
+        pos = min_pos(a, b, step)
+        if abs(old - pos) < 1e-5:
+            break
+        old = pos
+    ar = axial / 2
+    a, b = pos - 2 * axial, pos + 2 * axial
+    crlb = lat(frange(a - ar / 2, b + ar / 2, dx, incl=True))
+    best, out = np.inf, 0.0
+    nb = int(ar / (2 * dx))
+    for u in frange(a, b, dx):
+        s, nb2 = 0.0, -int(ar / (2 * dx))
+        for _ in frange(-ar / 2, ar / 2, dx, incl=True):
+            s += crlb[nb + nb2]
+            nb2 += 1
+        if best > s:
+            best, out = s, u
+        nb += 1
+    return out
+
+
+def test_center_search_restatement_agrees():
+    p = _center_psf(zfocus=0.4)
+    zc = p.center_search(32, 1.0, 0)
+    assert zc == _center_search_py(p, 32, 1.0, 0.11, 0.4)
+
+
+def test_center_search_gpu_form_returns_zfocus_when_index_matched():
+    p = _center_psf(zfocus=0.3, n_wat=1.518)
+    assert p.center_search(32, 1.0, 1) == 0.3
+    assert p.center_search(32, -1.0, 0) == 0.3

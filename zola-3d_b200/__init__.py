@@ -25,6 +25,10 @@ LIB_PATH = os.path.join(_HERE, "libzola_b200.so")
 
 ZOLA_PREC_FP64 = 0
 ZOLA_PREC_SPLIT = 1
+ZOLA_SPLIT_STAGED = 0
+ZOLA_SPLIT_FUSED = 1
+ZOLA_CENTER_CPU = 0
+ZOLA_CENTER_GPU = 1
 FIT_STATUS = {1: "converged", 2: "max_iter", 3: "stalled", -1: "nan"}
 
 
@@ -65,7 +69,8 @@ EXPORTS = ["zola_ctx_create", "zola_ctx_destroy", "zola_last_error", "zola_ctx_s
            "zola_fit_batch_dev", "zola_ctx_profile", "zola_ctx_stage_stats", "zola_fit_batch_noalloc",
            "zola_detector_create", "zola_detector_free", "zola_detector_info", "zola_detect", "zola_detect_dev",
            "zola_localize_frames", "zola_write_csv", "zola_format_double_java", "zola_calib_forward",
-           "zola_calib_backward", "zola_calib_fit"]
+           "zola_calib_backward", "zola_calib_fit", "zola_ctx_set_split_mode", "zola_crlb_curve",
+           "zola_psf_center_search"]
 STAGES = ["split_stage1_pupil_dft", "split_stage2_window_dft", "split_stage3_blur_rows", "split_stage4_blur_cols",
           "split_stage5_likelihood_lm", "fp64_fit", "fp64_model", "other"]
 
@@ -96,6 +101,9 @@ def lib():
         L.zola_psf_model_prec.argtypes = [vp, i, vp, i, vp, vp, i]
         L.zola_psf_model_prec_dev.argtypes = [vp, i, vp, i, vp, vp, i, vp]
         L.zola_ctx_set_pool.argtypes = [vp, i]
+        L.zola_ctx_set_split_mode.argtypes = [vp, i]
+        L.zola_crlb_curve.argtypes = [vp, i, vp, i, d, d, d, d, vp]
+        L.zola_psf_center_search.argtypes = [vp, i, d, i, ctypes.POINTER(d)]
         L.zola_ctx_profile.argtypes = [vp, i]
         L.zola_detector_create.argtypes = [vp, i, i, i, d, d, d, d, ctypes.POINTER(vp)]
         L.zola_localize_frames.argtypes = [vp, vp, vp, vp, i, i, ctypes.POINTER(LocParams), vp, i, ctypes.POINTER(i)]
@@ -148,6 +156,11 @@ class Context:
     def set_pool(self, max_slots):
         """Bound the split fit's slot pool (ROIs in flight); 0 = automatic."""
         self.check(lib().zola_ctx_set_pool(self.h, int(max_slots)), "zola_ctx_set_pool")
+
+    def set_split_mode(self, mode):
+        """"staged" (default): five stage kernels per LM round; "fused": stage 1 + one kernel for stages 2-5."""
+        code = {"staged": ZOLA_SPLIT_STAGED, "fused": ZOLA_SPLIT_FUSED}[mode]
+        self.check(lib().zola_ctx_set_split_mode(self.h, code), "zola_ctx_set_split_mode")
 
     def profile(self, enable=True):
         """Time every library kernel launch with CUDA events on its stream."""
@@ -257,6 +270,22 @@ class PSF:
         self.ctx.check(lib().zola_fit_batch_dev(self.ctx.h, self.h, R, _ptr(rois), _ptr(init), n, ctypes.byref(prm),
                                                 _ptr(out), _ptr(crlb), _ptr(nll), _ptr(status), _ptr(iters), stream),
                        "zola_fit_batch_dev")
+
+    def crlb_curve(self, R, z, photons=3000.0, background=50.0, h=0.0005, a_step=0.0005):
+        """CRLB (x, y, z, A, B) at (0, 0, z) for each depth, finite-difference
+        Fisher matrix (CRLB.computeFisher; defaults are CRLB.run's h = 0.5 nm)."""
+        z = np.ascontiguousarray(np.atleast_1d(z), dtype=np.float64)
+        out = np.zeros((len(z), 5))
+        self.ctx.check(lib().zola_crlb_curve(self.h, int(R), _ptr(z), len(z), float(photons), float(background),
+                                             float(h), float(a_step), _ptr(out)), "zola_crlb_curve")
+        return out
+
+    def center_search(self, axial_range, R=None, variant=ZOLA_CENTER_CPU):
+        """SearchPSFcenter.getPosition: the ZfocusCenter depth (um) for an axial range (um)."""
+        zc = ctypes.c_double()
+        self.ctx.check(lib().zola_psf_center_search(self.h, int(R or self.N), float(axial_range), int(variant),
+                                                    ctypes.byref(zc)), "zola_psf_center_search")
+        return zc.value
 
 
 class Detector:

@@ -29,6 +29,27 @@ int ensure_scratch(zola_ctx* ctx, size_t bytes, std::string& err) {
     return 0;
 }
 
+// Staging area of the host-buffer calls: grows in 64 MiB steps, never shrinks,
+// so repeated calls of similar size allocate nothing.
+int ensure_io(zola_ctx* ctx, size_t bytes) {
+    if (bytes <= ctx->io_bytes) return 0;
+    const size_t step = (size_t)64 << 20;
+    bytes = (bytes + step - 1) / step * step;
+    if (ctx->io) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(ctx->io);
+        ctx->io = nullptr;
+        ctx->io_bytes = 0;
+    }
+    cudaError_t e = cudaMalloc(&ctx->io, bytes);
+    if (e != cudaSuccess) {
+        ctx->err = std::string("staging cudaMalloc: ") + cudaGetErrorString(e);
+        return ZOLA_E_CUDA;
+    }
+    ctx->io_bytes = bytes;
+    return 0;
+}
+
 void prof_begin(zola_ctx* ctx, int stage, cudaStream_t st) {
     if (!ctx->profile) return;
     if ((size_t)ctx->ev_used + 2 > ctx->ev_pool.size()) {
@@ -85,13 +106,6 @@ bool check_fit_params(zola_ctx* ctx, const zola_fit_params* prm) {
     return true;
 }
 
-template <class T>
-struct DevBuf {
-    T* p = nullptr;
-    ~DevBuf() { if (p) cudaFree(p); }
-    cudaError_t alloc(size_t n) { return cudaMalloc(&p, n * sizeof(T)); }
-};
-
 }  // namespace
 
 extern "C" {
@@ -125,6 +139,7 @@ int zola_ctx_destroy(zola_ctx* ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     if (ctx->scratch) cudaFree(ctx->scratch);
+    if (ctx->io) cudaFree(ctx->io);
     if (ctx->d_counter) cudaFree(ctx->d_counter);
     if (ctx->h_flags) cudaFreeHost(ctx->h_flags);
     for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
@@ -257,6 +272,12 @@ int zola_ctx_set_pool(zola_ctx* ctx, int max_slots) {
     return ZOLA_OK;
 }
 
+int zola_ctx_set_split_mode(zola_ctx* ctx, int mode) {
+    if (!ctx || (mode != ZOLA_SPLIT_STAGED && mode != ZOLA_SPLIT_FUSED)) return ZOLA_E_ARG;
+    ctx->split_fused = mode == ZOLA_SPLIT_FUSED;
+    return ZOLA_OK;
+}
+
 int zola_fit_batch_dev(zola_ctx* ctx, zola_psf* psf, int R, const float* d_rois, const double* d_init5, int n,
                        const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll, int* d_status,
                        int* d_iters, void* stream) {
@@ -280,27 +301,31 @@ int zola_fit_batch(zola_ctx* ctx, zola_psf* psf, int R, const float* rois, const
     if (n < 0 || (n > 0 && (!rois || !init5 || !out5))) return set_err(ctx, ZOLA_E_ARG, "zola_fit_batch: bad n or null buffer");
     if (n == 0) return ZOLA_OK;
     cudaSetDevice(ctx->device);
-    size_t rr = (size_t)R * R;
-    DevBuf<float> dr;
-    DevBuf<double> di, dout, dcr, dnll;
-    DevBuf<int> dst, dit;
-    ZOLA_CUDA_CHECK(dr.alloc(rr * n), ctx);
-    ZOLA_CUDA_CHECK(di.alloc(5 * (size_t)n), ctx);
-    ZOLA_CUDA_CHECK(dout.alloc(5 * (size_t)n), ctx);
-    if (crlb5) ZOLA_CUDA_CHECK(dcr.alloc(5 * (size_t)n), ctx);
-    if (nll) ZOLA_CUDA_CHECK(dnll.alloc((size_t)n), ctx);
-    if (status) ZOLA_CUDA_CHECK(dst.alloc((size_t)n), ctx);
-    if (iters) ZOLA_CUDA_CHECK(dit.alloc((size_t)n), ctx);
-    ZOLA_CUDA_CHECK(cudaMemcpyAsync(dr.p, rois, rr * n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream), ctx);
-    ZOLA_CUDA_CHECK(cudaMemcpyAsync(di.p, init5, 5 * n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream), ctx);
-    int rc = zola_fit_batch_dev(ctx, psf, R, dr.p, di.p, n, prm, dout.p, crlb5 ? dcr.p : nullptr, nll ? dnll.p : nullptr,
-                                status ? dst.p : nullptr, iters ? dit.p : nullptr, ctx->stream);
+    const size_t rr = (size_t)R * R, nn = (size_t)n;
+    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    // staging layout: rois | init | out | crlb | nll | status | iters
+    const size_t off_i = al(rr * nn * sizeof(float)), off_o = off_i + al(5 * nn * sizeof(double));
+    const size_t off_c = off_o + al(5 * nn * sizeof(double)), off_n = off_c + al(5 * nn * sizeof(double));
+    const size_t off_s = off_n + al(nn * sizeof(double)), off_t = off_s + al(nn * sizeof(int));
+    const size_t total = off_t + al(nn * sizeof(int));
+    if (ensure_io(ctx, total)) return ZOLA_E_CUDA;
+    char* base = (char*)ctx->io;
+    float* dr = (float*)base;
+    double* di = (double*)(base + off_i);
+    double* dout = (double*)(base + off_o);
+    double* dcr = crlb5 ? (double*)(base + off_c) : nullptr;
+    double* dnll = nll ? (double*)(base + off_n) : nullptr;
+    int* dst = status ? (int*)(base + off_s) : nullptr;
+    int* dit = iters ? (int*)(base + off_t) : nullptr;
+    ZOLA_CUDA_CHECK(cudaMemcpyAsync(dr, rois, rr * nn * sizeof(float), cudaMemcpyHostToDevice, ctx->stream), ctx);
+    ZOLA_CUDA_CHECK(cudaMemcpyAsync(di, init5, 5 * nn * sizeof(double), cudaMemcpyHostToDevice, ctx->stream), ctx);
+    int rc = zola_fit_batch_dev(ctx, psf, R, dr, di, n, prm, dout, dcr, dnll, dst, dit, ctx->stream);
     if (rc) return rc;
-    ZOLA_CUDA_CHECK(cudaMemcpyAsync(out5, dout.p, 5 * n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), ctx);
-    if (crlb5) ZOLA_CUDA_CHECK(cudaMemcpyAsync(crlb5, dcr.p, 5 * n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), ctx);
-    if (nll) ZOLA_CUDA_CHECK(cudaMemcpyAsync(nll, dnll.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), ctx);
-    if (status) ZOLA_CUDA_CHECK(cudaMemcpyAsync(status, dst.p, n * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), ctx);
-    if (iters) ZOLA_CUDA_CHECK(cudaMemcpyAsync(iters, dit.p, n * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), ctx);
+    ZOLA_CUDA_CHECK(cudaMemcpyAsync(out5, dout, 5 * nn * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), ctx);
+    if (crlb5) ZOLA_CUDA_CHECK(cudaMemcpyAsync(crlb5, dcr, 5 * nn * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), ctx);
+    if (nll) ZOLA_CUDA_CHECK(cudaMemcpyAsync(nll, dnll, nn * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), ctx);
+    if (status) ZOLA_CUDA_CHECK(cudaMemcpyAsync(status, dst, nn * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), ctx);
+    if (iters) ZOLA_CUDA_CHECK(cudaMemcpyAsync(iters, dit, nn * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), ctx);
     ZOLA_CUDA_CHECK(cudaStreamSynchronize(ctx->stream), ctx);
     return ZOLA_OK;
 }

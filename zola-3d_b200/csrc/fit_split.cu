@@ -68,6 +68,9 @@ struct SplitDev {
     // constant operands
     const __half* bc_hi;  // NCH chunks of 4IC x K1 (K-major)
     const __half* bc_lo;  // NCH chunks of 2IC x K1
+    const __half* bc2_hi; // NCH2 chunks of 4*16 x K1 (fused kernel)
+    const __half* bc2_lo; // NCH2 chunks of 2*16 x K1
+    int NCH2;
     const __half* gt_hi;  // RP x W (K-major)
     const __half* gt_lo;
     // pupil tables (D x D, row a <-> kx, column b <-> ky), FP64
@@ -93,9 +96,12 @@ struct SplitDev {
 
 struct SplitPlanHost {
     int R = 0, W = 0, D = 0, DP = 0, K1 = 0, IC = 0, NCH = 0, RP = 0, G1 = 0, G2 = 0, NT4 = 0;
+    int IC2 = 16, NCH2 = 0;  // fused stage 2-5 kernel: 16-wide i-chunks
     SplitScales sc{};
     __half* d_bc_hi = nullptr;
     __half* d_bc_lo = nullptr;
+    __half* d_bc2_hi = nullptr;
+    __half* d_bc2_lo = nullptr;
     __half* d_gt_hi = nullptr;
     __half* d_gt_lo = nullptr;
     double* d_phase0 = nullptr;
@@ -109,6 +115,13 @@ static double pow2scale(double bound) {
 __host__ __device__ inline size_t a2_tile_bytes(int K1) { return (size_t)4 * 128 * K1 * 2; }
 __host__ __device__ inline size_t a3_tile_bytes(int W) { return (size_t)5 * 128 * W * 2; }
 __host__ __device__ inline size_t a4_tile_bytes(int W) { return (size_t)2 * 128 * W * 2; }
+// Row stride (floats) of the fused kernel's shared-memory maps: a multiple of 4
+// congruent to 4 mod 32, so that 32 lanes storing float4 at consecutive rows
+// cover all banks once per 8 lanes.
+__host__ __device__ inline int tm_stride(int R) {
+    const int s = (R + 3) & ~3;
+    return s + (4 - s % 32 + 32) % 32;
+}
 
 // Build (once per PSF and ROI size) the constant operands and scales.
 static SplitPlanHost* get_plan(zola_psf* p, WindowTables* w, std::string& err) {
@@ -166,37 +179,46 @@ static SplitPlanHost* get_plan(zola_psf* p, WindowTables* w, std::string& err) {
     // part 0: [Re C ; -Im C], 1: [Im C ; Re C], 2: [Re CK ; -Im CK], 3: [Im CK ; Re CK]
     // with columns k < DP multiplying the real and k >= DP the imaginary part
     // of the data; CK[i][b] = C[i][b] * (i k_b).
-    std::vector<__half> bh((size_t)NCH * 4 * IC * K1, __float2half(0.f)), bl((size_t)NCH * 2 * IC * K1, __float2half(0.f));
     auto C = [&](int i, int b, double& re, double& im) {
         re = w->C[((size_t)i * D + b) * 2];
         im = w->C[((size_t)i * D + b) * 2 + 1];
     };
-    for (int c = 0; c < NCH; ++c)
-        for (int part = 0; part < 4; ++part)
-            for (int ii = 0; ii < IC; ++ii) {
-                int i = c * IC + ii, n = part * IC + ii;
-                for (int k = 0; k < K1; ++k) {
-                    int b = k < DP ? k : k - DP;
-                    if (b >= D) continue;
-                    double cr, ci;
-                    C(i, b, cr, ci);
-                    double kb = p->ky[b];
-                    double ckr = -kb * ci, cki = kb * cr;
-                    double v;
-                    bool re_in = k < DP;
-                    switch (part) {
-                        case 0: v = re_in ? cr : -ci; break;
-                        case 1: v = re_in ? ci : cr; break;
-                        case 2: v = re_in ? ckr : -cki; break;
-                        default: v = re_in ? cki : ckr; break;
+    auto pack_bc = [&](int icw, std::vector<__half>& bh, std::vector<__half>& bl) {
+        const int nch = W / icw;
+        bh.assign((size_t)nch * 4 * icw * K1, __float2half(0.f));
+        bl.assign((size_t)nch * 2 * icw * K1, __float2half(0.f));
+        for (int c = 0; c < nch; ++c)
+            for (int part = 0; part < 4; ++part)
+                for (int ii = 0; ii < icw; ++ii) {
+                    int i = c * icw + ii, n = part * icw + ii;
+                    for (int k = 0; k < K1; ++k) {
+                        int b = k < DP ? k : k - DP;
+                        if (b >= D) continue;
+                        double cr, ci;
+                        C(i, b, cr, ci);
+                        double kb = p->ky[b];
+                        double ckr = -kb * ci, cki = kb * cr;
+                        double v;
+                        bool re_in = k < DP;
+                        switch (part) {
+                            case 0: v = re_in ? cr : -ci; break;
+                            case 1: v = re_in ? ci : cr; break;
+                            case 2: v = re_in ? ckr : -cki; break;
+                            default: v = re_in ? cki : ckr; break;
+                        }
+                        v *= sB;
+                        __half hi = __float2half_rn((float)v);
+                        __half lo = __float2half_rn((float)(v - (double)__half2float(hi)));
+                        bh[(size_t)c * 4 * icw * K1 + kmajor_off(n, k, K1) / 2] = hi;
+                        if (part < 2) bl[(size_t)c * 2 * icw * K1 + kmajor_off(n, k, K1) / 2] = lo;
                     }
-                    v *= sB;
-                    __half hi = __float2half_rn((float)v);
-                    __half lo = __float2half_rn((float)(v - (double)__half2float(hi)));
-                    bh[(size_t)c * 4 * IC * K1 + kmajor_off(n, k, K1) / 2] = hi;
-                    if (part < 2) bl[(size_t)c * 2 * IC * K1 + kmajor_off(n, k, K1) / 2] = lo;
                 }
-            }
+    };
+    std::vector<__half> bh, bl, bh2, bl2;
+    pack_bc(IC, bh, bl);
+    pl->IC2 = W < 16 ? W : 16;
+    pl->NCH2 = W / pl->IC2;
+    pack_bc(pl->IC2, bh2, bl2);
     // G^T operand: rows n = i' (< RP, zero beyond R), K = W.
     std::vector<__half> gh((size_t)RP * W, __float2half(0.f)), gl((size_t)RP * W, __float2half(0.f));
     for (int ip = 0; ip < R; ++ip)
@@ -219,6 +241,8 @@ static SplitPlanHost* get_plan(zola_psf* p, WindowTables* w, std::string& err) {
     };
     up((void**)&pl->d_bc_hi, bh.data(), bh.size() * 2);
     up((void**)&pl->d_bc_lo, bl.data(), bl.size() * 2);
+    up((void**)&pl->d_bc2_hi, bh2.data(), bh2.size() * 2);
+    up((void**)&pl->d_bc2_lo, bl2.data(), bl2.size() * 2);
     up((void**)&pl->d_gt_hi, gh.data(), gh.size() * 2);
     up((void**)&pl->d_gt_lo, gl.data(), gl.size() * 2);
     up((void**)&pl->d_phase0, ph0.data(), ph0.size() * 8);
@@ -236,6 +260,8 @@ void free_split_plan(void* plan) {
     if (!pl) return;
     cudaFree(pl->d_bc_hi);
     cudaFree(pl->d_bc_lo);
+    cudaFree(pl->d_bc2_hi);
+    cudaFree(pl->d_bc2_lo);
     cudaFree(pl->d_gt_hi);
     cudaFree(pl->d_gt_lo);
     cudaFree(pl->d_phase0);
@@ -274,6 +300,15 @@ __device__ __forceinline__ int tmem_cols_pow2(int c) {
     return p;
 }
 
+// True when any of the g slots from s0 holds a ROI.  Every thread evaluates it
+// before the first barrier, so CTAs whose slots have all retired (the pool
+// drains at the end of a batch) exit at once.
+__device__ __forceinline__ bool tile_live(const SplitDev& P, int s0, int g) {
+    bool live = false;
+    for (int k = 0; k < g; ++k) live |= P.slot_roi[s0 + k] >= 0;
+    return live;
+}
+
 // ----------------------------------------------------------- stage 1 -------
 // One CTA per G1 slots; thread t builds row (g = t / DP, a = t % DP) of Q.
 __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage1(SplitDev P) {
@@ -289,6 +324,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage1(SplitDev P) {
     __shared__ __align__(8) uint64_t bc_full[2], mma_done[2];
     __shared__ uint32_t tmem_base;
     const int ncols = NCH > 1 ? 512 : tmem_cols_pow2(6 * IC);
+    if (!tile_live(P, blockIdx.x * P.G1, P.G1)) return;
 
     if (t < 32) umma::tmem_alloc(&tmem_base, ncols);
     if (t == 0) {
@@ -429,6 +465,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage2(SplitDev P) {
     __shared__ __align__(8) uint64_t a2_full, bc_full[2], mma_done[2];
     __shared__ uint32_t tmem_base;
     const int ncols = NCH > 1 ? 512 : tmem_cols_pow2(8 * IC);
+    if (!tile_live(P, blockIdx.x * P.G2, P.G2)) return;
     if (t < 32) umma::tmem_alloc(&tmem_base, ncols);
     if (t == 0) {
         umma::mbar_init(&a2_full, 1);
@@ -526,6 +563,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage3(SplitDev P) {
     __shared__ __align__(8) uint64_t full, done;
     __shared__ uint32_t tmem_base;
     const int ncols = tmem_cols_pow2(4 * RP);
+    if (!tile_live(P, blockIdx.x * P.G2, P.G2)) return;
     if (t < 32) umma::tmem_alloc(&tmem_base, ncols);
     if (t == 0) {
         umma::mbar_init(&full, 1);
@@ -592,6 +630,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage4(SplitDev P) {
     __shared__ __align__(8) uint64_t full, done;
     __shared__ uint32_t tmem_base;
     const int ncols = tmem_cols_pow2(RP);
+    if (!tile_live(P, blockIdx.x / P.NT4, 1)) return;
     if (t < 32) umma::tmem_alloc(&tmem_base, ncols);
     if (t == 0) {
         umma::mbar_init(&full, 1);
@@ -761,6 +800,338 @@ __global__ void __launch_bounds__(LIK_THREADS) k_stage5(SplitDev P, const float*
     }
 }
 
+// ------------------------------------------------- fused stages 2 to 5 ------
+// One CTA per stage-2 tile (G2 slots x W rows j).  The window DFT runs over
+// 16-wide i-chunks; each chunk's intensity products go straight into the
+// row-blur accumulators (stage 3, chunked over K = i) in TMEM; the finished
+// row-blurred maps are rebuilt as stage-4 operands in the (now free) A2
+// region; the column blur lands in shared memory as FP32 maps; and the
+// likelihood sums and the FP64 LM step (stage 5) run on them in place.  Only
+// the A2 tile crosses global memory.
+//
+// Shared memory: [A2: 4 x 128 x K1 f16 | later A4 tiles] [BC chunk buffers]
+// [A3 chunk: 5 x 128 x 16 f16] [G^T hi, lo]; once the column blur is done the
+// whole block holds the FP32 maps (row stride tm_stride(R)).
+// TMEM: stage-2 chunk buffers at 0 (and 128), row-blur accumulators at JB,
+// column-blur outputs at 0 once stage 2 is done.
+__global__ void __launch_bounds__(SPLIT_THREADS, 1) k_fused25(SplitDev P, const float* rois, const double* init, int n,
+                                                              FitParamsDev prm, double* out5, double* crlb5,
+                                                              double* nll_out, int* st_out, int* it_out) {
+    extern __shared__ __align__(1024) char smem[];
+    constexpr int IC2 = 16;
+    const int K1 = P.K1, W = P.W, RP = P.RP, R = P.R, G2 = P.G2, NT4 = P.NT4, NCH2 = P.NCH2;
+    const int t = threadIdx.x, row = t & 127, wg = t >> 7, warp = t >> 5, lane = t & 31;
+    const bool dbl = W >= 64;
+    const int nbuf = dbl ? 2 : 1;
+    const size_t arr2 = (size_t)128 * K1 * 2;
+    const int bc_hi_b = 4 * IC2 * K1 * 2, bc_lo_b = 2 * IC2 * K1 * 2, bcb = bc_hi_b + bc_lo_b;
+    const int arr3 = 128 * IC2 * 2;
+    const int gtb = RP * W * 2;
+    char* A2 = smem;
+    char* BCB = A2 + 4 * arr2;
+    char* A3 = BCB + nbuf * bcb;
+    char* GT = A3 + 5 * arr3;
+    float* Tm = (float*)smem;  // FP32 maps after stage 4
+    const int RS = tm_stride(R), MS = R * RS;
+    __shared__ __align__(8) uint64_t full_a2, bc_full[2], mma2[2], mma3, mma4;
+    __shared__ uint32_t tmem_base;
+    __shared__ double red[SPLIT_THREADS / 32][NRED];
+    __shared__ int bad_slot[4];
+    const int ncols = dbl ? 512 : 256;
+    const int JB = dbl ? 256 : 128;
+    if (!tile_live(P, blockIdx.x * G2, G2)) return;
+    if (t < 4) bad_slot[t] = 0;
+    if (t < 32) umma::tmem_alloc(&tmem_base, ncols);
+    if (t == 0) {
+        umma::mbar_init(&full_a2, 1);
+        umma::mbar_init(&bc_full[0], 1); umma::mbar_init(&bc_full[1], 1);
+        umma::mbar_init(&mma2[0], 1); umma::mbar_init(&mma2[1], 1);
+        umma::mbar_init(&mma3, 1); umma::mbar_init(&mma4, 1);
+        umma::mbar_fence_init();
+    }
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tbase = tmem_base;
+    auto load_bc = [&](int c, int buf) {
+        char* dst = BCB + buf * bcb;
+        umma::mbar_expect_tx(&bc_full[buf], bcb);
+        umma::bulk_g2s(dst, (const char*)P.bc2_hi + (size_t)c * bc_hi_b, bc_hi_b, &bc_full[buf]);
+        umma::bulk_g2s(dst + bc_hi_b, (const char*)P.bc2_lo + (size_t)c * bc_lo_b, bc_lo_b, &bc_full[buf]);
+    };
+    if (t == 0) {
+        umma::mbar_expect_tx(&full_a2, (uint32_t)(4 * arr2 + 2 * gtb));
+        const char* src = P.a2 + (size_t)blockIdx.x * a2_tile_bytes(K1);
+        for (int q = 0; q < 4; ++q) umma::bulk_g2s(A2 + q * arr2, src + q * arr2, (uint32_t)arr2, &full_a2);
+        umma::bulk_g2s(GT, P.gt_hi, (uint32_t)gtb, &full_a2);
+        umma::bulk_g2s(GT + gtb, P.gt_lo, (uint32_t)gtb, &full_a2);
+        load_bc(0, 0);
+        if (dbl && NCH2 > 1) load_bc(1, 1);
+    }
+    const uint32_t lbo_mn = (128 / 8) * 128, kstep_mn = 2 * lbo_mn, sbo_k1 = (K1 / 8) * 128, sbo_w = (W / 8) * 128;
+    const uint32_t id64 = umma::idesc_f16(128, 4 * IC2, true, false);
+    const uint32_t id32 = umma::idesc_f16(128, 2 * IC2, true, false);
+    const uint32_t idJ = umma::idesc_f16(128, RP, false, false);
+    const uint32_t id4 = umma::idesc_f16(128, RP, true, false);
+    auto bc_parity = [&](int c) { return dbl ? (uint32_t)((c >> 1) & 1) : (uint32_t)(c & 1); };
+    auto issue2 = [&](int c) {
+        const int buf = dbl ? (c & 1) : 0;
+        if (c == 0) umma::mbar_wait(&full_a2, 0, P.err);
+        umma::mbar_wait(&bc_full[buf], bc_parity(c), P.err);
+        umma::fence_after_sync();
+        const uint32_t bhi = umma::smem_u32(BCB + buf * bcb), blo = bhi + bc_hi_b;
+        const uint32_t ahi = umma::smem_u32(A2), alo = ahi + (uint32_t)arr2, ay = ahi + 2 * (uint32_t)arr2,
+                       az = ahi + 3 * (uint32_t)arr2;
+        const uint32_t td = tbase + buf * 128;
+        mma_chain(td, ahi, lbo_mn, 128, kstep_mn, bhi, 128, sbo_k1, 256, K1, id64, false);
+        mma_chain(td, ahi, lbo_mn, 128, kstep_mn, blo, 128, sbo_k1, 256, K1, id32, true);
+        mma_chain(td, alo, lbo_mn, 128, kstep_mn, bhi, 128, sbo_k1, 256, K1, id32, true);
+        mma_chain(td + 64, ay, lbo_mn, 128, kstep_mn, bhi, 128, sbo_k1, 256, K1, id32, false);
+        mma_chain(td + 96, az, lbo_mn, 128, kstep_mn, bhi, 128, sbo_k1, 256, K1, id32, false);
+        umma::mma_commit(&mma2[buf]);
+    };
+    if (t == 0) issue2(0);
+    for (int c = 0; c < NCH2; ++c) {
+        const int buf = dbl ? (c & 1) : 0;
+        if (t == 0 && dbl && c + 1 < NCH2) issue2(c + 1);
+        umma::mbar_wait(&mma2[buf], bc_parity(c), P.err);
+        if (c > 0) umma::mbar_wait(&mma3, (uint32_t)((c - 1) & 1), P.err);  // A3 chunk buffer free
+        umma::fence_after_sync();
+        {
+            const uint32_t b0 = buf * 128;
+            const int u0 = wg * 4;
+            float er[4], ei[4], xr[4], xi[4];
+            umma::tmem_ld4(tmem_lane_addr(tbase, b0 + 0 * IC2 + u0), er);
+            umma::tmem_ld4(tmem_lane_addr(tbase, b0 + 1 * IC2 + u0), ei);
+            umma::tmem_ld4(tmem_lane_addr(tbase, b0 + 2 * IC2 + u0), xr);
+            umma::tmem_ld4(tmem_lane_addr(tbase, b0 + 3 * IC2 + u0), xi);
+            __half hh[4], ll[4], dx[4], dy[4], dz[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                umma::split_f16((er[u] * er[u] + ei[u] * ei[u]) * P.sc.cI, hh[u], ll[u]);
+                dx[u] = __float2half_rn((er[u] * xr[u] + ei[u] * xi[u]) * P.sc.cIx);
+            }
+            umma::tmem_ld4(tmem_lane_addr(tbase, b0 + 64 + u0), xr);
+            umma::tmem_ld4(tmem_lane_addr(tbase, b0 + 80 + u0), xi);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) dy[u] = __float2half_rn((er[u] * xr[u] + ei[u] * xi[u]) * P.sc.cIy);
+            umma::tmem_ld4(tmem_lane_addr(tbase, b0 + 96 + u0), xr);
+            umma::tmem_ld4(tmem_lane_addr(tbase, b0 + 112 + u0), xi);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) dz[u] = __float2half_rn((er[u] * xr[u] + ei[u] * xi[u]) * P.sc.cIz);
+            const uint32_t off = kmajor_off(row, u0, IC2);
+            const __half* arrs[5] = {hh, ll, dx, dy, dz};
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                uint2 v;
+                v.x = (uint32_t)__half_as_ushort(arrs[q][0]) | ((uint32_t)__half_as_ushort(arrs[q][1]) << 16);
+                v.y = (uint32_t)__half_as_ushort(arrs[q][2]) | ((uint32_t)__half_as_ushort(arrs[q][3]) << 16);
+                *(uint2*)(A3 + q * arr3 + off) = v;
+            }
+        }
+        umma::fence_before_sync();
+        umma::fence_proxy_async();
+        __syncthreads();
+        if (t == 0) {
+            umma::fence_after_sync();
+            const uint32_t a3 = umma::smem_u32(A3), ghi = umma::smem_u32(GT) + (uint32_t)c * 256,
+                           glo = umma::smem_u32(GT) + (uint32_t)gtb + (uint32_t)c * 256;
+            const uint32_t sbo3 = (IC2 / 8) * 128;
+            // one K = 16 step per chunk: J_m += A3_m G^T[:, chunk]
+            umma::mma_f16(tbase + JB, umma::smem_desc(a3, 128, sbo3), umma::smem_desc(ghi, 128, sbo_w), idJ, c > 0);
+            umma::mma_f16(tbase + JB, umma::smem_desc(a3, 128, sbo3), umma::smem_desc(glo, 128, sbo_w), idJ, 1);
+            umma::mma_f16(tbase + JB, umma::smem_desc(a3 + arr3, 128, sbo3), umma::smem_desc(ghi, 128, sbo_w), idJ, 1);
+            for (int m = 1; m < 4; ++m)
+                umma::mma_f16(tbase + JB + m * RP, umma::smem_desc(a3 + (m + 1) * arr3, 128, sbo3),
+                              umma::smem_desc(ghi, 128, sbo_w), idJ, c > 0);
+            umma::mma_commit(&mma3);
+            if (c + nbuf < NCH2) load_bc(c + nbuf, buf);
+            if (!dbl && c + 1 < NCH2) issue2(c + 1);
+        }
+    }
+    umma::mbar_wait(&mma3, (uint32_t)((NCH2 - 1) & 1), P.err);
+    umma::fence_after_sync();
+    // stage 3 epilogue: row-blurred maps -> stage-4 operands in the A2 region
+    {
+        const int g2 = row / W, j = row % W, m = wg;
+        const size_t t4 = (size_t)2 * 128 * W * 2, arr4 = (size_t)128 * W * 2;
+        for (int h = 0; h < RP; h += 16) {
+            float v[16];
+            umma::tmem_ld16(tmem_lane_addr(tbase, JB + m * RP + h), v);
+            for (int i8 = 0; i8 < 16; i8 += 8) {
+                const int r = m * RP + h + i8;
+                char* tile = A2 + (size_t)(g2 * NT4 + r / 128) * t4;
+                __half hh[8], ll[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) umma::split_f16(v[i8 + u] * P.sc.cJ[m], hh[u], ll[u]);
+                const uint32_t off = mnmajor_off(r % 128, j, 128);
+                store8h(tile + off, hh);
+                store8h(tile + arr4 + off, ll);
+            }
+        }
+    }
+    umma::fence_before_sync();
+    umma::fence_proxy_async();
+    __syncthreads();
+    if (t == 0) {
+        umma::fence_after_sync();
+        const size_t t4 = (size_t)2 * 128 * W * 2, arr4 = (size_t)128 * W * 2;
+        const uint32_t ghi = umma::smem_u32(GT), glo = ghi + (uint32_t)gtb;
+        for (int tt = 0; tt < G2 * NT4; ++tt) {
+            const uint32_t ahi = umma::smem_u32(A2 + (size_t)tt * t4), alo = ahi + (uint32_t)arr4;
+            const uint32_t td = tbase + tt * RP;
+            mma_chain(td, ahi, lbo_mn, 128, kstep_mn, ghi, 128, sbo_w, 256, W, id4, false);
+            mma_chain(td, ahi, lbo_mn, 128, kstep_mn, glo, 128, sbo_w, 256, W, id4, true);
+            mma_chain(td, alo, lbo_mn, 128, kstep_mn, ghi, 128, sbo_w, 256, W, id4, true);
+        }
+        umma::mma_commit(&mma4);
+    }
+    umma::mbar_wait(&mma4, 0, P.err);
+    umma::fence_after_sync();
+    // stage 4 epilogue: FP32 maps into shared memory
+    {
+        const int cq = RP / 4;
+        for (int tt = 0; tt < G2 * NT4; ++tt) {
+            const int g2 = tt / NT4, r = (tt % NT4) * 128 + row, map = r / RP, ip = r % RP;
+            for (int h = wg * cq; h < (wg + 1) * cq; h += 4) {
+                float v[4];
+                umma::tmem_ld4(tmem_lane_addr(tbase, tt * RP + h), v);
+                if (map < 4 && ip < R && h < R) {
+                    const float c = P.sc.cT[map];
+                    float* dst = Tm + (size_t)(g2 * 4 + map) * MS + ip * RS + h;
+                    if (h + 4 <= R)
+                        *(float4*)dst = make_float4(v[0] * c, v[1] * c, v[2] * c, v[3] * c);
+                    else
+                        for (int u = 0; h + u < R; ++u) dst[u] = v[u] * c;
+                }
+            }
+        }
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    // stage 5: per slot, 16 / G2 warps
+    const int wps = (SPLIT_THREADS / 32) / G2, g2 = warp / wps, tid_s = t - g2 * wps * 32, nts = wps * 32;
+    const int slot = blockIdx.x * G2 + g2;
+    const int roi = P.slot_roi[slot];
+    const int RR = R * R;
+    const float* T0 = Tm + (size_t)g2 * 4 * MS;
+    float ns[4] = {0, 0, 0, 0}, nc = 0.f;
+    if (roi >= 0)
+        for (int k = tid_s; k < RR; k += nts) {
+            const int ip = k / R, o = ip * RS + (k - ip * R);
+            const float v = T0[o], sg = v < 0 ? -1.f : 1.f;
+            kahan_add(ns[0], nc, fabsf(v));
+            ns[1] += sg * T0[MS + o];
+            ns[2] += sg * T0[2 * MS + o];
+            ns[3] += sg * T0[3 * MS + o];
+        }
+    {
+        double v0 = warp_sum((double)ns[0] - (double)nc), v1 = warp_sum(ns[1]), v2 = warp_sum(ns[2]), v3 = warp_sum(ns[3]);
+        if (lane == 0) { red[warp][0] = v0; red[warp][1] = v1; red[warp][2] = v2; red[warp][3] = v3; }
+    }
+    __syncthreads();
+    double sum4[4] = {0, 0, 0, 0};
+    for (int w = g2 * wps; w < (g2 + 1) * wps; ++w)
+        for (int q = 0; q < 4; ++q) sum4[q] += red[w][q];
+    __syncthreads();
+    const float S = (float)sum4[0], Dx = (float)sum4[1], Dy = (float)sum4[2], Dz = (float)sum4[3];
+    const float invS = 1.f / S;
+    float sg6[6], cg6[6], sh[30];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) { sg6[k] = 0.f; cg6[k] = 0.f; }
+#pragma unroll
+    for (int k = 0; k < 30; ++k) sh[k] = 0.f;
+    bool bad = false;
+    if (roi >= 0) {
+        const double* th = P.lm[slot].trial;
+        const float A = (float)th[3], B = (float)th[4];
+        const float* d = rois + (size_t)roi * RR;
+        for (int k = tid_s; k < RR; k += nts) {
+            const int ip = k / R, to = ip * RS + (k - ip * R);
+            const float v = T0[to], sgn = v < 0 ? -1.f : 1.f, psi = fabsf(v) * invS;
+            float jv[5];
+            jv[0] = A * (sgn * T0[MS + to] - psi * Dx) * invS;
+            jv[1] = A * (sgn * T0[2 * MS + to] - psi * Dy) * invS;
+            jv[2] = A * (sgn * T0[3 * MS + to] - psi * Dz) * invS;
+            jv[3] = psi;
+            jv[4] = 1.f;
+            const float mu = A * psi + B;
+            if (!(mu > 0.f)) { bad = true; continue; }
+            const float dk = d[k];
+            kahan_add(sg6[0], cg6[0], dk > 0.f ? mu - dk - dk * logf(mu / dk) : mu);
+            const float wgt = 1.f - dk / mu, wf = 1.f / mu, wh = dk * wf * wf;
+#pragma unroll
+            for (int q = 0; q < 5; ++q) kahan_add(sg6[1 + q], cg6[1 + q], wgt * jv[q]);
+            int o = 0;
+#pragma unroll
+            for (int q = 0; q < 5; ++q)
+#pragma unroll
+                for (int r2 = 0; r2 <= q; ++r2) {
+                    sh[o] += wh * jv[q] * jv[r2];
+                    sh[o + 15] += wf * jv[q] * jv[r2];
+                    ++o;
+                }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const double v = warp_sum((double)sg6[k] - (double)cg6[k]);
+        if (lane == 0) red[warp][k] = v;
+    }
+#pragma unroll
+    for (int k = 0; k < 30; ++k) {
+        const double v = warp_sum((double)sh[k]);
+        if (lane == 0) red[warp][6 + k] = v;
+    }
+    if (bad) bad_slot[g2] = 1;
+    __syncthreads();
+    if (tid_s == 0 && roi >= 0) {
+        double tot[NRED];
+        for (int q = 0; q < NRED; ++q) {
+            double v = 0;
+            for (int w = g2 * wps; w < (g2 + 1) * wps; ++w) v += red[w][q];
+            tot[q] = v;
+        }
+        double nll = bad_slot[g2] ? INFINITY : tot[0], g[5], H[25], F[25];
+        for (int q = 0; q < 5; ++q) g[q] = tot[1 + q];
+        int o = 6;
+        for (int q = 0; q < 5; ++q)
+            for (int r2 = 0; r2 <= q; ++r2) {
+                H[q * 5 + r2] = H[r2 * 5 + q] = tot[o];
+                F[q * 5 + r2] = F[r2 * 5 + q] = tot[o + 15];
+                ++o;
+            }
+        LMState& st = P.lm[slot];
+        bool next_trial = false;
+        if (P.slot_phase[slot] == 0) {
+            for (int q = 0; q < 5; ++q) st.th[q] = st.trial[q];
+            lm_start(st, nll, g, H, F, prm);
+            P.slot_phase[slot] = 1;
+        } else {
+            lm_update(st, nll, g, H, F, prm);
+        }
+        next_trial = lm_propose(st, prm);
+        if (!next_trial) {
+            for (int q = 0; q < 5; ++q) out5[5 * roi + q] = st.th[q];
+            if (nll_out) nll_out[roi] = st.nll;
+            if (st_out) st_out[roi] = st.status;
+            if (it_out) it_out[roi] = st.evals;
+            if (crlb5) lm_crlb(st.F, crlb5 + 5 * roi);
+            const int nx = atomicAdd(P.queue, 1);
+            if (nx < n) {
+                P.slot_roi[slot] = nx;
+                P.slot_phase[slot] = 0;
+                for (int q = 0; q < 5; ++q) st.trial[q] = init[5 * nx + q];
+                lm_clamp(st.trial, prm);
+            } else {
+                P.slot_roi[slot] = -1;
+                atomicSub(P.active, 1);
+            }
+        }
+    }
+    __syncthreads();
+    if (t < 32) umma::tmem_dealloc(tbase, ncols);
+}
+
 // Fill the pool from the queue.
 __global__ void k_init_slots(SplitDev P, const double* init, int n, FitParamsDev prm) {
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
@@ -785,6 +1156,17 @@ static size_t smem_stage1(const SplitPlanHost& pl) { return (size_t)768 * pl.K1 
 static size_t smem_stage2(const SplitPlanHost& pl) { return (size_t)1024 * pl.K1 + 2 * (size_t)12 * pl.IC * pl.K1; }
 static size_t smem_stage3(const SplitPlanHost& pl) { return (size_t)5 * 128 * pl.W * 2 + (size_t)4 * pl.RP * pl.W; }
 static size_t smem_stage4(const SplitPlanHost& pl) { return (size_t)2 * 128 * pl.W * 2 + (size_t)4 * pl.RP * pl.W; }
+static size_t smem_fused(const SplitPlanHost& pl) {
+    const int nbuf = pl.W >= 64 ? 2 : 1;
+    return (size_t)4 * 128 * pl.K1 * 2 + (size_t)nbuf * 12 * 16 * pl.K1 + (size_t)5 * 128 * 16 * 2 +
+           (size_t)2 * pl.RP * pl.W * 2;
+}
+static bool fused_fits(const SplitPlanHost& pl) {
+    const size_t maps = (size_t)pl.G2 * 4 * pl.R * tm_stride(pl.R) * 4;
+    const size_t a4 = (size_t)pl.G2 * pl.NT4 * 2 * 128 * pl.W * 2;
+    return smem_fused(pl) <= 225 * 1024 && maps <= smem_fused(pl) &&
+           a4 <= (size_t)4 * 128 * pl.K1 * 2 && pl.G2 <= 4 && 4 * pl.RP + (pl.W >= 64 ? 256 : 128) <= (pl.W >= 64 ? 512 : 256);
+}
 
 // psi and d psi / d{x,y,z} of every occupied slot from its blurred maps
 // (model-only evaluation through the tensor-core stages).
@@ -838,7 +1220,7 @@ __global__ void k_init_points(SplitDev P, const double* xyz, int n) {
 struct SplitPool {
     SplitPlanHost* pl = nullptr;
     SplitDev D{};
-    size_t s1 = 0, s2 = 0, s3 = 0, s4 = 0;
+    size_t s1 = 0, s2 = 0, s3 = 0, s4 = 0, sf = 0;
 };
 
 static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pmax_override, SplitPool& sp,
@@ -880,6 +1262,7 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
     D.RP = pl->RP; D.G1 = pl->G1; D.G2 = pl->G2; D.NT4 = pl->NT4; D.P = P; D.a0 = p->a0; D.N = p->N;
     D.zfocus = p->o.zfocus;
     D.bc_hi = pl->d_bc_hi; D.bc_lo = pl->d_bc_lo; D.gt_hi = pl->d_gt_hi; D.gt_lo = pl->d_gt_lo;
+    D.bc2_hi = pl->d_bc2_hi; D.bc2_lo = pl->d_bc2_lo; D.NCH2 = pl->NCH2;
     D.pupil = p->view.pupil; D.phase0 = pl->d_phase0; D.kz = p->view.kz; D.kx = p->view.kx; D.ky = p->view.ky;
     D.a2 = base; base += b_a2;
     D.a3 = base; base += b_a3;
@@ -897,6 +1280,9 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
     ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_stage2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.s2), ctx);
     ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_stage3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.s3), ctx);
     ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_stage4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.s4), ctx);
+    sp.sf = smem_fused(*pl);
+    if (fused_fits(*pl))
+        ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_fused25, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.sf), ctx);
     return ZOLA_OK;
 }
 
@@ -964,8 +1350,20 @@ int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d
     ZOLA_CUDA_CHECK(cudaGetLastError(), ctx);
     const int max_rounds = (prm->max_iter + 2) * ((n + P - 1) / P + 1) + 8;
     int rounds = 0;
+    const bool fused = ctx->split_fused && fused_fits(*sp.pl);
     while (true) {
         for (int k = 0; k < 4; ++k) {
+            if (fused) {
+                prof_begin(ctx, 0, st);
+                k_stage1<<<P / sp.pl->G1, SPLIT_THREADS, sp.s1, st>>>(D);
+                prof_end(ctx, st);
+                prof_begin(ctx, 1, st);
+                k_fused25<<<P / sp.pl->G2, SPLIT_THREADS, sp.sf, st>>>(D, d_rois, d_init, n, fp, d_out5, d_crlb5, d_nll,
+                                                                      d_status, d_iters);
+                prof_end(ctx, st);
+                ctx->launches += 2;
+                continue;
+            }
             launch_model_stages(ctx, sp, st);
             prof_begin(ctx, 4, st);
             k_stage5<<<(P + LIK_SLOTS - 1) / LIK_SLOTS, LIK_THREADS, 0, st>>>(D, d_rois, d_init, n, fp, d_out5, d_crlb5,

@@ -67,10 +67,15 @@ struct zola_ctx {
     // reusable device scratch (FP64 fit work areas, counters)
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
+    // grow-only device staging for the host-buffer entry points (inputs and
+    // results of one call; never overlaps scratch)
+    void* io = nullptr;
+    size_t io_bytes = 0;
     int* d_counter = nullptr;
     int* d_status_word = nullptr;
     int* h_flags = nullptr;      // pinned host words read back by the split fit loop
     int split_pool_max = 0;      // 0: size the split slot pool automatically
+    int split_fused = 0;         // 1: stage 1 + one fused kernel for stages 2-5 per LM round
     // optional per-kernel timing with CUDA events on the launch stream
     int profile = 0;
     std::vector<cudaEvent_t> ev_pool;
@@ -141,6 +146,18 @@ int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d
                      int* d_status, int* d_iters, cudaStream_t st);
 
 int ensure_scratch(zola_ctx* ctx, size_t bytes, std::string& err);
+int ensure_io(zola_ctx* ctx, size_t bytes);
+
+// Owned device allocation released on scope exit (one-time host paths).
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { if (p) cudaFree(p); }
+    cudaError_t alloc(size_t n) { return cudaMalloc(&p, n * sizeof(T)); }
+};
 
 }  // namespace zola
 
