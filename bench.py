@@ -23,13 +23,13 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# DRAM bytes per slot of one launch (ncu dram__bytes_read.sum + dram__bytes_write.sum,
-# 48x48 tetrapod class, 4000 slots per launch, staged kernels).
-NCU_TRAFFIC = {("tetra48", "split_stage1_pupil_dft"): 97.727488e6 / 4000,
-               ("tetra48", "split_stage2_window_dft"): 1128.219648e6 / 4000,
-               ("tetra48", "split_stage3_blur_rows"): 1013.042688e6 / 4000,
-               ("tetra48", "split_stage4_blur_cols"): 653.105152e6 / 4000,
-               ("tetra48", "split_stage5_likelihood_lm"): 55.940352e6 / 4000}
+# DRAM bytes per slot of one launch (ncu dram__bytes_read.sum + dram__bytes_write.sum
+# of one launch per kernel, 48x48 tetrapod class, full pool of 4096 slots).
+NCU_TRAFFIC = {("tetra48", "split_stage1_pupil_dft"): (0.960000e6 + 478.294016e6) / 4096,
+               ("tetra48", "split_stage2_window_dft"): (537.137152e6 + 618.686720e6) / 4096,
+               ("tetra48", "split_stage3_blur_rows"): (671.153920e6 + 366.961152e6) / 4096,
+               ("tetra48", "split_stage4_blur_cols"): (536.933120e6 + 131.593728e6) / 4096,
+               ("tetra48", "split_stage5_likelihood_lm"): (233.258752e6 + 4.537088e6) / 4096}
 
 METRIC = "MLE ROI fits/sec at ≤0.5 nm vs FP64 oracle (batched split-prec vs plain GPU)"
 UNIT = "ROI fits/s"
@@ -286,8 +286,9 @@ def main():
     device = torch.device("cuda", local)
     if world > 1:
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=device)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=device)
     z = ge.load_package()
+    import zola3d_b200.replicas as rp
     ctx = z.Context(local)
     if args.pool:
         ctx.set_pool(args.pool)
@@ -304,12 +305,9 @@ def main():
     ext.synchronize()
 
     # timed steps (device time on the library stream; max over ranks)
-    ctx.profile(True)
-    ctx.stage_stats(reset=True)
     l0 = ctx.launches
     clocks = ClockSampler(local)
-    if world > 1:
-        dist.barrier()
+    rp.barrier()
     torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
@@ -322,22 +320,16 @@ def main():
     ms = ev0.elapsed_time(ev1)
     clk = clocks.stop()
     launches = ctx.launches - l0
-    stats = ctx.stage_stats(reset=True)
-    ctx.profile(False)
-    if world > 1:
-        t = torch.tensor([ms], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
+    ms = rp.max_over_ranks(ms, device)
+    rp.barrier()
     ms_step = ms / args.steps
     value = n_total * world / (ms_step / 1000.0)
 
-    # per-class split timing and per-class kernel times (one extra pass outside the timed region)
+    # per-class split timing (one extra pass outside the timed region), then a
+    # pass with every launch bracketed by CUDA events for the per-kernel times
     per_class = {}
     class_stats = {}
     for j in job:
-        ctx.profile(True)
-        ctx.stage_stats(reset=True)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(ext)
@@ -346,12 +338,20 @@ def main():
                          stream=ctx.stream)
         e1.record(ext)
         e1.synchronize()
-        class_stats[j["cls"]["name"]] = ctx.stage_stats(reset=True)
-        ctx.profile(False)
         t = e0.elapsed_time(e1) / 1000.0
         per_class[j["cls"]["name"]] = {"rois": int(j["rois"].shape[0]), "seconds": t,
                                        "fits_per_s": j["rois"].shape[0] / t,
                                        "mean_evals": float(j["iters"].double().mean().item())}
+    stats = None
+    for j in job:
+        ctx.profile(True)
+        ctx.stage_stats(reset=True)
+        p = z.PSF.fit_params(precision=z.ZOLA_PREC_SPLIT, **j["prm_kw"])
+        j["psf"].fit_dev(j["rois"], j["init"], p, j["out"], j["crlb"], j["nll"], j["status"], j["iters"],
+                         stream=ctx.stream)
+        class_stats[j["cls"]["name"]] = st = ctx.stage_stats(reset=True)
+        ctx.profile(False)
+        stats = st if stats is None else {k: (stats[k][0] + v[0], stats[k][1] + v[1]) for k, v in st.items()}
 
     # per-class useful evaluations for the roofline
     iters = {j["cls"]["name"]: int(j["iters"].sum().item()) for j in job}
@@ -450,39 +450,33 @@ def main():
                 "traffic": None if traffic is None else int(traffic * min(args.pool or 4096, 32768)),
                 "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu launch of this kernel on "
                                 "this class (4000 slots), scaled to a full pool launch by slots",
-                "stages_timed_region": stage_table, "per_class": by_class,
+                "stages_all_classes": stage_table, "per_class": by_class,
                 "note": "achieved = algorithmic flops of the useful model evaluations (complex MAC = 8 flops) / "
                         "summed CUDA-event duration of that kernel's launches for that class"}
 
     # end to end through the host C-ABI (pinned host buffers, H2D + D2H inside the call)
     e2e = None
-    if rank == 0 or True:
-        host = []
-        h2d = d2h = 0
-        for j in job:
-            r = torch.empty(j["rois"].shape, dtype=torch.float32, pin_memory=True)
-            r.copy_(j["rois"])
-            i0 = torch.empty(j["init"].shape, dtype=torch.float64, pin_memory=True)
-            i0.copy_(j["init"])
-            host.append((r.numpy(), i0.numpy()))
-            h2d += r.numel() * 4 + i0.numel() * 8
-            d2h += j["rois"].shape[0] * (5 * 8 + 5 * 8 + 8 + 4 + 4)
-        # one untimed pass sizes the library's staging area, then the timed pass
-        for j, (r, i0) in zip(job, host):
-            j["psf"].fit(r, i0, z.PSF.fit_params(precision=z.ZOLA_PREC_SPLIT, **j["prm_kw"]))
-        torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
-        t0 = time.perf_counter()
-        for j, (r, i0) in zip(job, host):
-            j["psf"].fit(r, i0, z.PSF.fit_params(precision=z.ZOLA_PREC_SPLIT, **j["prm_kw"]))
-        t_e2e = time.perf_counter() - t0
-        if world > 1:
-            t = torch.tensor([t_e2e], device=device)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            t_e2e = float(t.item())
-        e2e = {"value": n_total * world / t_e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(d2h)}
+    host = []
+    h2d = d2h = 0
+    for j in job:
+        r = torch.empty(j["rois"].shape, dtype=torch.float32, pin_memory=True)
+        r.copy_(j["rois"])
+        i0 = torch.empty(j["init"].shape, dtype=torch.float64, pin_memory=True)
+        i0.copy_(j["init"])
+        host.append((r.numpy(), i0.numpy()))
+        h2d += r.numel() * 4 + i0.numel() * 8
+        d2h += j["rois"].shape[0] * (5 * 8 + 5 * 8 + 8 + 4 + 4)
+    # one untimed pass sizes the library's staging area, then the timed pass
+    for j, (r, i0) in zip(job, host):
+        j["psf"].fit(r, i0, z.PSF.fit_params(precision=z.ZOLA_PREC_SPLIT, **j["prm_kw"]))
+    torch.cuda.synchronize()
+    rp.barrier()
+    t0 = time.perf_counter()
+    for j, (r, i0) in zip(job, host):
+        j["psf"].fit(r, i0, z.PSF.fit_params(precision=z.ZOLA_PREC_SPLIT, **j["prm_kw"]))
+    t_e2e = rp.max_over_ranks(time.perf_counter() - t0, device)
+    e2e = {"value": n_total * world / t_e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(d2h)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
