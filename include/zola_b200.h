@@ -197,25 +197,52 @@ ZOLA_API int zola_format_double_java(double v, char* buf, int len);
 
 /* --- Zernike calibration from bead z-stacks (replaces ZernikePhaseRetrieval's
  * stack NLL and its coordinate-wise finite-difference updates;
- * process/cpu/ZernikePhaseRetrieval.java:1081-1198, 1843-1874).
- * Bead b, slice s: PSF at (x_b, y_b, zoil = dz[s] + z_b, zwat = 0) with phase
- * sum_{i>=3} zernike[i] Z_i (modes 0-2, the reference's per-bead registration,
- * are carried as x_b, y_b, z_b and ignored in zernike); mu = A_b psi + B_b
- * (floored at 1e-8 as the reference); NLL = sum mu - d ln mu, FP64 on the GPU.
- * bead: nbead x (x, y, z, A, B); stacks: nbead x nslice x R x R photons. */
-ZOLA_API int zola_calib_forward(zola_psf* psf, int R, int nz, const double* zernike, int nbead, int nslice,
-                                const double* dz, const double* bead, const double* stacks, double* nll,
+ * process/cpu/ZernikePhaseRetrieval.java:225-300, 860-1198, 1519-1530,
+ * 1843-1874).  Bead b, slice s: PSF at (x_b, y_b, zoil = dz[s] + z_b,
+ * zwat = 0) with phase sum_{i>=3} zernike[i] Z_i (modes 0-2, the reference's
+ * per-bead registration, are carried as x_b, y_b, z_b and ignored in zernike)
+ * and blur width sigma (px);
+ *   mu = psi (photons[b][s] + a_bs) + sum_k c_bk m_k(i, ii),
+ *   m = 1, i, i^2, ii, i ii, ii^2 (patch pixel (i, ii), first index x),
+ * floored at 1e-8 as the reference; NLL = sum mu - d ln mu, FP64 on the GPU.
+ * a_bs is the reference's fit_a + fit_a_each; c_bk its PolynomialBackground. */
+typedef struct {
+    int R;                 /* patch side (even) */
+    int nz;                /* Zernike modes (4..231) */
+    int nbead, nslice;
+    const double* dz;      /* nslice slice offsets, um */
+    const double* stacks;  /* nbead x nslice x R x R photons */
+    const double* photons; /* nbead x nslice photon curve (zola_calib_init); NULL = 0 */
+} zola_calib_data;
+/* bead parameters per bead: x, y, z (um), a[nslice], c[6] */
+#define ZOLA_CALIB_BEAD_STRIDE(nslice) (3 + (nslice) + 6)
+ZOLA_API int zola_calib_forward(zola_psf* psf, const zola_calib_data* data, const double* zernike, double sigma,
+                                const double* bead, double* nll,
                                 double* model /* nullable: nbead x nslice x R x R */);
 /* NLL and its exact gradient by the hand-written adjoint: grad_zernike[nz]
- * (0 for modes 0-2) and grad_bead[nbead x 5]. */
-ZOLA_API int zola_calib_backward(zola_psf* psf, int R, int nz, const double* zernike, int nbead, int nslice,
-                                 const double* dz, const double* bead, const double* stacks, double* nll,
-                                 double* grad_zernike, double* grad_bead);
-/* Levenberg-Marquardt fit of zernike[3..nz) and every bead's x, y, z, A, B
- * (updated in place): adjoint gradient, Gauss-Newton matrix from forward
- * tangents, FP64 damped solve. */
-ZOLA_API int zola_calib_fit(zola_psf* psf, int R, int nz, double* zernike, int nbead, int nslice, const double* dz,
-                            double* bead, const double* stacks, int max_iter, double* nll, int* iters);
+ * (0 for modes 0-2), grad_sigma (nullable), grad_bead (bead layout). */
+ZOLA_API int zola_calib_backward(zola_psf* psf, const zola_calib_data* data, const double* zernike, double sigma,
+                                 const double* bead, double* nll, double* grad_zernike, double* grad_sigma,
+                                 double* grad_bead);
+/* Levenberg-Marquardt fit of zernike[3..nz), sigma (with ZOLA_CALIB_FIT_SIGMA)
+ * and every bead's parameters, updated in place: adjoint gradient,
+ * Gauss-Newton matrix from device tangents, FP64 damped solve. */
+#define ZOLA_CALIB_FIT_SIGMA 1
+ZOLA_API int zola_calib_fit(zola_psf* psf, const zola_calib_data* data, double* zernike, double* sigma, double* bead,
+                            int max_iter, int flags, double* nll, int* iters);
+/* InitBackgroundAndPhotonNumber (process/InitBackgroundAndPhotonNumber.java:
+ * 50-72, 110-420, 587-900): converts the raw stack (nslice x W x H, first
+ * index x, ADU) to photons + 1 with slope adu/gain and offset, refines the
+ * bead seeds (xpoints/ypoints, pixels, in place), fits the order-2 background
+ * surface of the stack's low voxels, and returns per bead the background
+ * background[nbead], the photon curve photons[nbead x nslice] (box-filtered
+ * over +-max((int)(0.5/zstep)/2, 1) slices) and the patches
+ * patches[nbead x nslice x size_patch^2] (outside the image: background).
+ * poly_background (nullable) receives the W x H surface. */
+ZOLA_API int zola_calib_init(zola_ctx* ctx, const float* raw, int nslice, int W, int H, float* xpoints,
+                             float* ypoints, int nbead, int size_patch, double adu, double gain, double offset,
+                             double zstep, double* photons, double* background, double* patches,
+                             double* poly_background);
 
 /* Allocation-free FP64 fit (this entry point has no counterpart in the
  * reference).  For callers that must not allocate device memory while they fit

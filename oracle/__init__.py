@@ -63,6 +63,10 @@ def lib():
         L.orc_localize_frames.argtypes = [vp, vp, i, vp, d, d, d, d, i, vp, i]
         L.orc_calib_nll.restype = d
         L.orc_calib_nll.argtypes = [vp, i, i, vp, vp, d, d, d, d, d]
+        L.orc_calib_nll_full.restype = d
+        L.orc_calib_nll_full.argtypes = [vp, i, i, vp, vp, vp, d, d, d, d, vp, vp]
+        L.orc_calib_init.restype = i
+        L.orc_calib_init.argtypes = [vp, i, i, i, vp, vp, i, i, d, d, d, d, vp, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -168,6 +172,13 @@ class OraclePSF:
         lib().orc_crlb_curve(self.h, int(R), len(z), _p(z), photons, bg, h, a_step, _p(out))
         return out
 
+    def calib_nll_full(self, R, dz, stack, photons, sigma, xyz, a, c):
+        """Stack NLL of one bead with per-slice photons + a, order-2 background c[6], blur sigma."""
+        dz, stack, a, c = _f64(dz), _f64(stack), _f64(a), _f64(c)
+        ph = None if photons is None else _f64(photons)
+        return lib().orc_calib_nll_full(self.h, R, len(dz), _p(dz), _p(stack), _p(ph) if ph is not None else None,
+                                        sigma, xyz[0], xyz[1], xyz[2], _p(a), _p(c))
+
     def calib_nll(self, R, dz, stack, x, y, z, A, B):
         dz = _f64(dz)
         stack = _f64(stack)
@@ -210,3 +221,21 @@ class OracleDetector:
         counts = np.zeros(nf, np.int32)
         lib().orc_detect(self.h, nf, _p(frames), cap, _p(out), _p(counts), threads)
         return [out[f, :min(cap, counts[f])] for f in range(nf)]
+
+
+def calib_init(raw, xpoints, ypoints, size_patch, adu=1.0, gain=1.0, offset=0.0, zstep=0.05):
+    """InitBackgroundAndPhotonNumber restated (raw: (nslice, W, H) ADU)."""
+    raw = _f64(raw)
+    ns, W, H = raw.shape
+    xp = np.array(xpoints, dtype=np.float32)
+    yp = np.array(ypoints, dtype=np.float32)
+    nb = len(xp)
+    ph = np.zeros((nb, ns))
+    bg = np.zeros(nb)
+    pt = np.zeros((nb, ns, size_patch, size_patch))
+    poly = np.zeros((W, H))
+    rc = lib().orc_calib_init(_p(raw), ns, W, H, _p(xp), _p(yp), nb, size_patch, adu, gain, offset, zstep, _p(ph),
+                              _p(bg), _p(pt), _p(poly))
+    if rc:
+        raise ValueError("singular background fit")
+    return dict(x=xp, y=yp, background=bg, photons=ph, patches=pt, surface=poly)

@@ -26,7 +26,8 @@
 //   z-centre search   process/cpu/SearchPSFcenter.java:37-330 (and the GPU
 //                     form process/gpu/SearchPSFcenter_.java)
 //   detection         process/cpu/Predetection.java:63-593
-//   calibration NLL   process/cpu/ZernikePhaseRetrieval.java:1843-1874
+//   calibration NLL   process/cpu/ZernikePhaseRetrieval.java:1519-1530, 1843-1874
+//   calibration init  process/InitBackgroundAndPhotonNumber.java (+ utils/PolynomialFit.java)
 // plus the FP64 Levenberg-Marquardt fit of the same Poisson NLL with analytic
 // x/y/z derivatives (no reference counterpart: the "FP64 oracle of the same
 // fit" that the GPU fits are compared against).
@@ -1092,6 +1093,215 @@ double orc_calib_nll(void* h, int R, int nslice, const double* dz, const double*
         }
     }
     return nll;
+}
+
+
+// Calibration stack NLL of one bead with the reference's full photometry
+// (ZernikePhaseRetrieval.java:1843-1874, background :1519-1530):
+//   mu = psi (A0_s + a_s) + sum_k c_k m_k(i, ii),  m = 1, i, i^2, ii, i ii, ii^2
+// (PolynomialBackground, order 2, exponent digits of 0..8 in base 3), mu <= 0
+// -> 1e-8; psi at (x, y, zoil = dz_s + z, zwat = 0) with blur width sigma.
+double orc_calib_nll_full(void* h, int R, int nslice, const double* dz, const double* stack, const double* A0,
+                          double sigma, double x, double y, double z, const double* a, const double* c) {
+    Psf q = *(const Psf*)h;
+    q.sigma = sigma;
+    std::vector<double> psi(R * R);
+    double nll = 0;
+    for (int s = 0; s < nslice; ++s) {
+        psf_model(&q, R, x, y, dz[s] + z, 0.0, psi.data(), nullptr);
+        const double At = (A0 ? A0[s] : 0.0) + a[s];
+        for (int i = 0; i < R; ++i)
+            for (int ii = 0; ii < R; ++ii) {
+                const double bg = c[0] + c[1] * i + c[2] * (double)i * i + c[3] * ii + c[4] * (double)i * ii +
+                                  c[5] * (double)ii * ii;
+                double mu = psi[i * R + ii] * At + bg;
+                if (mu <= 0) mu = 0.00000001;
+                nll += mu - stack[((size_t)s * R + i) * R + ii] * std::log(mu);
+            }
+    }
+    return nll;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Least squares of values v at (x, y) on the order-2 basis 1, x, x^2, y, xy, y^2
+// by normal equations and Gaussian elimination (utils/PolynomialFit.java:80-140,
+// 544-600); returns false when singular.
+bool poly2_fit(const std::vector<double>& xs, const std::vector<double>& ys, const std::vector<double>& v,
+               double coef[6]) {
+    const int ex[6] = {0, 1, 2, 0, 1, 0}, ey[6] = {0, 0, 0, 1, 1, 2};
+    double M[6][7] = {};
+    for (size_t k = 0; k < v.size(); ++k) {
+        double m[6];
+        for (int t = 0; t < 6; ++t) m[t] = std::pow(xs[k], ex[t]) * std::pow(ys[k], ey[t]);
+        for (int i = 0; i < 6; ++i) {
+            for (int j = 0; j < 6; ++j) M[i][j] += m[i] * m[j];
+            M[i][6] += m[i] * v[k];
+        }
+    }
+    for (int c = 0; c < 6; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < 6; ++r) if (std::fabs(M[r][c]) > std::fabs(M[piv][c])) piv = r;
+        if (M[piv][c] == 0) return false;
+        for (int j = 0; j < 7; ++j) std::swap(M[c][j], M[piv][j]);
+        for (int r = c + 1; r < 6; ++r) {
+            const double f = M[r][c] / M[c][c];
+            for (int j = c; j < 7; ++j) M[r][j] -= f * M[c][j];
+        }
+    }
+    for (int i = 5; i >= 0; --i) {
+        double s = M[i][6];
+        for (int j = i + 1; j < 6; ++j) s -= M[i][j] * coef[j];
+        coef[i] = s / M[i][i];
+    }
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+// InitBackgroundAndPhotonNumber (process/InitBackgroundAndPhotonNumber.java):
+// ADU -> photons + 1 (:50-72), seed refinement (:587-640), the stack's
+// polynomial background from low, dilated voxels around the dimmest slices
+// (:642-900), per-bead background B, per-slice photons A (box-filtered over
+// +-sizeFilt slices) and the bead patches (:110-420).  Image [slice][x][y].
+int orc_calib_init(const double* raw, int ns, int W, int H, float* xp, float* yp, int nb, int sp, double adu,
+                   double gain, double offset, double zstep, double* A, double* B, double* patches, double* poly) {
+    const size_t N = (size_t)ns * W * H;
+    std::vector<double> im(N);
+    const double slope = adu / gain, intercept = -offset * adu / gain;
+    for (size_t k = 0; k < N; ++k) {
+        double v = (raw[k] * slope + intercept) + 1;
+        im[k] = v < 0 ? 0 : v;
+    }
+    auto at = [&](int z, int i, int ii) { return im[((size_t)z * W + i) * H + ii]; };
+    const int sizeFilt = std::max((int)(0.5 / zstep) / 2, 1);
+    // refinePoints
+    for (int p = 0; p < nb; ++p) {
+        const int x0 = (int)(xp[p]) - sp / 2, y0 = (int)(yp[p]) - sp / 2;
+        std::vector<double> sub((size_t)sp * sp, 0.0);
+        for (int z = 0; z < ns; ++z)
+            for (int u = 0; u < sp; ++u)
+                for (int uu = 0; uu < sp; ++uu)
+                    if (x0 + u >= 0 && x0 + u < W && y0 + uu >= 0 && y0 + uu < H) sub[u * sp + uu] += at(z, x0 + u, y0 + uu);
+        std::vector<double> v(sub);
+        std::sort(v.begin(), v.end());
+        const double thr = v[(int)((v.size() - 1) * .9)];
+        double mx = 0, my = 0, sum = 0;
+        int count = 0;
+        for (int u = sp / 4; u < 3 * sp / 4; ++u)
+            for (int uu = sp / 4; uu < 3 * sp / 4; ++uu)
+                if (sub[u * sp + uu] > thr) {
+                    mx += (x0 + u) * sub[u * sp + uu];
+                    my += (y0 + uu) * sub[u * sp + uu];
+                    sum += sub[u * sp + uu];
+                    count++;
+                }
+        if (count >= 1) {
+            const float fx = (float)(mx / sum), fy = (float)(my / sum);
+            const float dxf = xp[p] - fx, dyf = yp[p] - fy;
+            if (std::sqrt((double)(dxf * dxf)) < sp / 4) xp[p] = fx;
+            if (std::sqrt((double)(dyf * dyf)) < sp / 4) yp[p] = fy;
+        }
+    }
+    // computeBackground
+    double mean0 = 0, std0 = 0;
+    for (size_t k = 0; k < N; ++k) mean0 += im[k];
+    mean0 /= (double)(int)N;
+    for (size_t k = 0; k < N; ++k) std0 += (im[k] - mean0) * (im[k] - mean0);
+    std0 /= (double)(int)N;
+    std0 = std::sqrt(std0);
+    double mean = 0, sd = 0;
+    int cnt0 = 0;
+    for (size_t k = 0; k < N; ++k)
+        if (im[k] <= mean0 + 2 * std0) { mean += im[k]; cnt0++; }
+    if (cnt0 > 0) mean /= cnt0;
+    for (size_t k = 0; k < N; ++k)
+        if (im[k] <= mean0 + 3 * std0) sd += (im[k] - mean) * (im[k] - mean);
+    if (cnt0 > 0) { sd /= cnt0; sd = std::sqrt(sd); }
+    std::vector<char> is2(N);
+    for (size_t k = 0; k < N; ++k) is2[k] = im[k] > mean + 3 * sd ? 0 : 1;
+    std::vector<double> mstack(ns, 0.0), filt(ns, 0.0);
+    for (int z = 0; z < ns; ++z) {
+        int c = 0;
+        for (int i = 0; i < W; ++i)
+            for (int ii = 0; ii < H; ++ii)
+                if (is2[((size_t)z * W + i) * H + ii]) { mstack[z] += at(z, i, ii); c++; }
+        if (c != 0) mstack[z] /= c;
+    }
+    int mp = 0;
+    for (int z = 0; z < ns; ++z) {
+        int c = 0;
+        for (int u = -sizeFilt; u <= sizeFilt; ++u)
+            if (z + u >= 0 && z + u < ns) { filt[z] += mstack[z + u]; c++; }
+        if (c != 0) filt[z] /= c;
+        if (filt[z] < filt[mp]) mp = z;
+    }
+    const int nn = sizeFilt;
+    if (mp < nn) mp = nn;
+    if (mp >= ns - nn) mp = ns - nn - 1;
+    std::vector<double> px, py, pv;
+    for (int i = 0; i < W; ++i)
+        for (int ii = 0; ii < H; ++ii) {
+            int count = 0;
+            double m = 0;
+            for (int z = 0; z < ns; ++z) {
+                bool ok = !(z < mp - nn) && !(z > mp + nn);
+                if (ok) {
+                    for (int u = -2; u <= 2 && ok; ++u)
+                        for (int uu = -2; uu <= 2 && ok; ++uu)
+                            for (int uuu = -2; uuu <= 2 && ok; ++uuu)
+                                if (z + u >= 0 && z + u < ns && i + uu >= 0 && i + uu < W && ii + uuu >= 0 &&
+                                    ii + uuu < H && !is2[((size_t)(z + u) * W + i + uu) * H + ii + uuu])
+                                    ok = false;
+                }
+                if (ok) { count++; m += at(z, i, ii); }
+            }
+            if (count >= 1) {
+                px.push_back(i);
+                py.push_back(ii);
+                pv.push_back(m / count);
+            }
+        }
+    double cf[6];
+    if (!poly2_fit(px, py, pv, cf)) return -1;
+    std::vector<double> pb((size_t)W * H);
+    for (int i = 0; i < W; ++i)
+        for (int ii = 0; ii < H; ++ii)
+            pb[(size_t)i * H + ii] = cf[0] + cf[1] * i + cf[2] * std::pow((double)i, 2) + cf[3] * ii +
+                                     cf[4] * i * (double)ii + cf[5] * std::pow((double)ii, 2);
+    if (poly) std::memcpy(poly, pb.data(), pb.size() * 8);
+    // B per bead, A per slice (box filtered), patches
+    for (int p = 0; p < nb; ++p) {
+        const int x0 = (int)(xp[p]) - sp / 2, y0 = (int)(yp[p]) - sp / 2;
+        double b = 0, cb = 0;
+        for (int u = 0; u < sp; ++u)
+            for (int uu = 0; uu < sp; ++uu)
+                if (x0 + u >= 0 && x0 + u < W && y0 + uu >= 0 && y0 + uu < H) { b += pb[(size_t)(x0 + u) * H + y0 + uu]; cb++; }
+        if (cb >= 1) b /= cb;
+        B[p] = b;
+        std::vector<double> a(ns, 0.0);
+        for (int z = 0; z < ns; ++z)
+            for (int u = 0; u < sp; ++u)
+                for (int uu = 0; uu < sp; ++uu)
+                    if (x0 + u >= 0 && x0 + u < W && y0 + uu >= 0 && y0 + uu < H) a[z] += at(z, x0 + u, y0 + uu) - b;
+        for (int z = 0; z < ns; ++z) {
+            double m = 0, c = 0;
+            for (int f = -sizeFilt; f <= sizeFilt; ++f)
+                if (z + f >= 0 && z + f < ns) { m += a[z + f]; c++; }
+            if (c >= 1) m /= c;
+            A[(size_t)p * ns + z] = m;
+        }
+        for (int z = 0; z < ns; ++z)
+            for (int u = 0; u < sp; ++u)
+                for (int uu = 0; uu < sp; ++uu)
+                    patches[(((size_t)p * ns + z) * sp + u) * sp + uu] =
+                        (x0 + u >= 0 && x0 + u < W && y0 + uu >= 0 && y0 + uu < H) ? at(z, x0 + u, y0 + uu) : b;
+    }
+    return 0;
 }
 
 }  // extern "C"

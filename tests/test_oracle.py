@@ -181,3 +181,41 @@ def test_center_search_gpu_form_returns_zfocus_when_index_matched():
     p = _center_psf(zfocus=0.3, n_wat=1.518)
     assert p.center_search(32, 1.0, 1) == 0.3
     assert p.center_search(32, -1.0, 0) == 0.3
+
+
+def _bead_stack(seed=4, ns=21, W=72, H=64, nb=3, R=24):
+    """Synthetic raw stack: tilted-plane background + beads with a z-dependent photon curve."""
+    rng = np.random.default_rng(seed)
+    o = OPTICS
+    p = O.OraclePSF(64, o["xystep"], o["na"], o["wavelength"], o["n_oil"], o["n_oil"], o["sigma"], astig_zernike(),
+                    gauss_f32=False)
+    ii, jj = np.meshgrid(np.arange(W), np.arange(H), indexing="ij")
+    plane = 40.0 + 0.05 * ii - 0.03 * jj
+    dz = (np.arange(ns) - ns // 2) * 0.1
+    pts = np.array([[18.3, 20.6], [50.2, 21.4], [33.7, 45.1]])[:nb]
+    A = 8000.0 * np.exp(-0.5 * (dz / 1.2) ** 2)
+    img = np.repeat(plane[None], ns, 0)
+    for (px, py) in pts:
+        ix, iy = int(px), int(py)
+        for s in range(ns):
+            # a positive model x moves the PSF towards lower pixel indices
+            m = p.model_oil(R, (ix - px) * o["xystep"], (iy - py) * o["xystep"], dz[s], 0.0)
+            img[s, ix - R // 2:ix + R // 2, iy - R // 2:iy + R // 2] += A[s] * m
+    raw = rng.poisson(img).astype(np.float64)
+    return raw, pts, A, plane, dz
+
+
+def test_calib_init_recovers_background_photons_and_seeds():
+    raw, pts, A, plane, dz = _bead_stack()
+    seeds = np.round(pts) + np.array([1.0, -1.0])
+    out = O.calib_init(raw, seeds[:, 0], seeds[:, 1], 24, zstep=0.1)
+    # refined seeds: intensity centroid of the brightest pixels, within a pixel of the bead
+    assert np.abs(out["x"] - pts[:, 0]).max() < 1.0 and np.abs(out["y"] - pts[:, 1]).max() < 1.0
+    # background surface: the plane + 1 (photon conversion adds 1)
+    assert np.abs(out["surface"] - (plane + 1)).max() < 1.5
+    for k in range(3):
+        x0, y0 = int(out["x"][k]) - 12, int(out["y"][k]) - 12
+        assert abs(out["background"][k] - (plane[x0:x0 + 24, y0:y0 + 24].mean() + 1)) < 1.0
+    # photon curve: the patch holds most of the bead's photons; the box filter smooths the Gaussian profile
+    assert np.all(np.abs(out["photons"][:, len(dz) // 2] / A[len(dz) // 2] - 0.95) < 0.08)
+    assert out["patches"].shape == (3, len(dz), 24, 24)

@@ -70,7 +70,7 @@ EXPORTS = ["zola_ctx_create", "zola_ctx_destroy", "zola_last_error", "zola_ctx_s
            "zola_detector_create", "zola_detector_free", "zola_detector_info", "zola_detect", "zola_detect_dev",
            "zola_localize_frames", "zola_write_csv", "zola_format_double_java", "zola_calib_forward",
            "zola_calib_backward", "zola_calib_fit", "zola_ctx_set_split_mode", "zola_crlb_curve",
-           "zola_psf_center_search"]
+           "zola_psf_center_search", "zola_calib_init"]
 STAGES = ["split_stage1_pupil_dft", "split_stage2_window_dft", "split_stage3_blur_rows", "split_stage4_blur_cols",
           "split_stage5_likelihood_lm", "fp64_fit", "fp64_model", "other"]
 
@@ -108,9 +108,10 @@ def lib():
         L.zola_detector_create.argtypes = [vp, i, i, i, d, d, d, d, ctypes.POINTER(vp)]
         L.zola_localize_frames.argtypes = [vp, vp, vp, vp, i, i, ctypes.POINTER(LocParams), vp, i, ctypes.POINTER(i)]
         L.zola_write_csv.argtypes = [ctypes.c_char_p, vp, i, i]
-        L.zola_calib_forward.argtypes = [vp, i, i, vp, i, i, vp, vp, vp, vp, vp]
-        L.zola_calib_backward.argtypes = [vp, i, i, vp, i, i, vp, vp, vp, vp, vp, vp]
-        L.zola_calib_fit.argtypes = [vp, i, i, vp, i, i, vp, vp, vp, i, vp, vp]
+        L.zola_calib_forward.argtypes = [vp, ctypes.POINTER(CalibData), vp, d, vp, vp, vp]
+        L.zola_calib_backward.argtypes = [vp, ctypes.POINTER(CalibData), vp, d, vp, vp, vp, vp, vp]
+        L.zola_calib_fit.argtypes = [vp, ctypes.POINTER(CalibData), vp, vp, vp, i, i, vp, vp]
+        L.zola_calib_init.argtypes = [vp, vp, i, i, i, vp, vp, i, i, d, d, d, d, vp, vp, vp, vp]
         L.zola_format_double_java.argtypes = [d, ctypes.c_char_p, i]
         L.zola_detector_free.argtypes = [vp]
         L.zola_detector_info.argtypes = [vp, ctypes.POINTER(i), vp, vp]
@@ -328,48 +329,99 @@ class Detector:
         self.h = None
 
 
+class CalibData(ctypes.Structure):
+    _fields_ = [("R", ctypes.c_int), ("nz", ctypes.c_int), ("nbead", ctypes.c_int), ("nslice", ctypes.c_int),
+                ("dz", ctypes.c_void_p), ("stacks", ctypes.c_void_p), ("photons", ctypes.c_void_p)]
+
+
+ZOLA_CALIB_FIT_SIGMA = 1
+NPOLY = 6
+
+
+def calib_init(ctx, raw, xpoints, ypoints, size_patch, adu=1.0, gain=1.0, offset=0.0, zstep=0.05):
+    """InitBackgroundAndPhotonNumber: raw stack (nslice, W, H) ADU -> dict with
+    refined seeds x/y (pixels), background (nbead,), photons (nbead, nslice),
+    patches (nbead, nslice, size_patch, size_patch) and the (W, H) surface."""
+    raw = np.ascontiguousarray(raw, dtype=np.float32)
+    ns, W, H = raw.shape
+    xp = np.array(xpoints, dtype=np.float32)
+    yp = np.array(ypoints, dtype=np.float32)
+    nb = len(xp)
+    ph = np.zeros((nb, ns))
+    bg = np.zeros(nb)
+    pt = np.zeros((nb, ns, size_patch, size_patch))
+    poly = np.zeros((W, H))
+    ctx.check(lib().zola_calib_init(ctx.h, _ptr(raw), ns, W, H, _ptr(xp), _ptr(yp), nb, int(size_patch), float(adu),
+                                    float(gain), float(offset), float(zstep), _ptr(ph), _ptr(bg), _ptr(pt),
+                                    _ptr(poly)), "zola_calib_init")
+    return dict(x=xp, y=yp, background=bg, photons=ph, patches=pt, surface=poly)
+
+
 class Calibration:
     """Bead z-stack calibration (ZernikePhaseRetrieval) on a kz_reset=False PSF.
 
     stacks: (nbead, nslice, R, R) photons; dz: (nslice,) slice positions (um);
-    bead: (nbead, 5) = x, y, z, A, B; zernike: (nz,) radians (modes 0-2 unused)."""
+    photons: (nbead, nslice) photon curve from calib_init (or None);
+    zernike: (nz,) radians (modes 0-2 unused); sigma: blur width (px);
+    bead: (nbead, 3 + nslice + 6) = x, y, z, a[nslice], c[6] (see bead_params)."""
 
-    def __init__(self, psf, stacks, dz):
+    def __init__(self, psf, stacks, dz, photons=None, nz=None):
         self.psf = psf
         self.stacks = np.ascontiguousarray(stacks, dtype=np.float64)
         self.dz = np.ascontiguousarray(dz, dtype=np.float64)
         self.nb, self.ns, self.R = self.stacks.shape[0], self.stacks.shape[1], self.stacks.shape[2]
+        self.photons = None if photons is None else np.ascontiguousarray(photons, dtype=np.float64)
+        self.nz = nz
 
-    def forward(self, zernike, bead, model=False):
+    def _data(self, nz):
+        return CalibData(self.R, int(nz), self.nb, self.ns, self.dz.ctypes.data, self.stacks.ctypes.data,
+                         None if self.photons is None else self.photons.ctypes.data)
+
+    def bead_params(self, xyz=None, a=None, background=None):
+        """Bead parameter array: xyz (nbead, 3), a (nbead, nslice) photon offsets,
+        background (nbead,) constant term of the polynomial."""
+        b = np.zeros((self.nb, 3 + self.ns + NPOLY))
+        if xyz is not None:
+            b[:, :3] = xyz
+        if a is not None:
+            b[:, 3:3 + self.ns] = a
+        if background is not None:
+            b[:, 3 + self.ns] = background
+        return b
+
+    def forward(self, zernike, sigma, bead, model=False):
         z = np.ascontiguousarray(zernike, dtype=np.float64)
         b = np.ascontiguousarray(bead, dtype=np.float64)
         nll = np.zeros(1)
         m = np.zeros_like(self.stacks) if model else None
-        self.psf.ctx.check(lib().zola_calib_forward(self.psf.h, self.R, len(z), _ptr(z), self.nb, self.ns, _ptr(self.dz),
-                                                    _ptr(b), _ptr(self.stacks), _ptr(nll), _ptr(m)),
-                           "zola_calib_forward")
+        data = self._data(len(z))
+        self.psf.ctx.check(lib().zola_calib_forward(self.psf.h, ctypes.byref(data), _ptr(z), float(sigma), _ptr(b),
+                                                    _ptr(nll), _ptr(m)), "zola_calib_forward")
         return (nll[0], m) if model else nll[0]
 
-    def backward(self, zernike, bead):
+    def backward(self, zernike, sigma, bead):
         z = np.ascontiguousarray(zernike, dtype=np.float64)
         b = np.ascontiguousarray(bead, dtype=np.float64)
         nll = np.zeros(1)
         gz = np.zeros(len(z))
-        gb = np.zeros((self.nb, 5))
-        self.psf.ctx.check(lib().zola_calib_backward(self.psf.h, self.R, len(z), _ptr(z), self.nb, self.ns,
-                                                     _ptr(self.dz), _ptr(b), _ptr(self.stacks), _ptr(nll), _ptr(gz),
-                                                     _ptr(gb)), "zola_calib_backward")
-        return nll[0], gz, gb
+        gs = np.zeros(1)
+        gb = np.zeros_like(b)
+        data = self._data(len(z))
+        self.psf.ctx.check(lib().zola_calib_backward(self.psf.h, ctypes.byref(data), _ptr(z), float(sigma), _ptr(b),
+                                                     _ptr(nll), _ptr(gz), _ptr(gs), _ptr(gb)), "zola_calib_backward")
+        return nll[0], gz, gs[0], gb
 
-    def fit(self, zernike, bead, max_iter=30):
+    def fit(self, zernike, sigma, bead, max_iter=30, fit_sigma=True):
         z = np.array(zernike, dtype=np.float64)
+        sg = np.array([sigma], dtype=np.float64)
         b = np.array(bead, dtype=np.float64)
         nll = np.zeros(1)
         it = ctypes.c_int()
-        self.psf.ctx.check(lib().zola_calib_fit(self.psf.h, self.R, len(z), _ptr(z), self.nb, self.ns, _ptr(self.dz),
-                                                _ptr(b), _ptr(self.stacks), int(max_iter), _ptr(nll), ctypes.byref(it)),
-                           "zola_calib_fit")
-        return z, b, nll[0], it.value
+        data = self._data(len(z))
+        self.psf.ctx.check(lib().zola_calib_fit(self.psf.h, ctypes.byref(data), _ptr(z), _ptr(sg), _ptr(b),
+                                                int(max_iter), ZOLA_CALIB_FIT_SIGMA if fit_sigma else 0, _ptr(nll),
+                                                ctypes.byref(it)), "zola_calib_fit")
+        return z, sg[0], b, nll[0], it.value
 
 
 LOC_COLUMNS = ["id", "frame", "x_nm", "y_nm", "z_nm", "intensity", "background", "chi2", "crlb_x_nm", "crlb_y_nm",

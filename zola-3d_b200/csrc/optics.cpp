@@ -149,6 +149,38 @@ int build_psf_tables(zola_psf* p, const zola_optics* o, const double* zern, int 
 //   h(d) = (1/W) sum_f g(f) cos(2 pi f d / W),
 // which is separable.  The final R x R crop reads window rows (i'-R/2) mod W,
 // so G[i'][i] = h(((i'-R/2) - (i-W/2)) mod W) and blurred = G I G^T.
+// R x W blur-and-crop matrix of the window: row ip is the circulant kernel
+// h(d) = (1/W) sum_f g(f) cos(2 pi f d / W) of the spectral Gaussian
+// g(f) = exp(-f^2 / (2 s^2)), s = W / (2 pi sigma), shifted so that output
+// pixel ip sits at window pixel ip - R/2 + W/2.  With dG, also d G / d sigma
+// (dg/dsigma = -g f^2 / (s^2 sigma)).
+void blur_matrix(int R, int W, double sigma, std::vector<double>& G, std::vector<double>* dG) {
+    std::vector<double> h(W), dh(W);
+    const double s = W / (2 * M_PI * sigma);
+    for (int d = 0; d < W; ++d) {
+        double acc = 0.0, dacc = 0.0;
+        for (int f = 0; f < W; ++f) {
+            int fs = f < W / 2 ? f : f - W;
+            double g = std::exp(-0.5 * (double)fs * fs / (s * s));
+            long long m = ((long long)f * d) % W;
+            const double cs = std::cos(2 * M_PI * (double)m / W);
+            acc += g * cs;
+            dacc += -g * (double)fs * fs / (s * s * sigma) * cs;
+        }
+        h[d] = acc / W;
+        dh[d] = dacc / W;
+    }
+    G.resize((size_t)R * W);
+    if (dG) dG->resize((size_t)R * W);
+    for (int ip = 0; ip < R; ++ip)
+        for (int i = 0; i < W; ++i) {
+            int d = ((ip - R / 2) - (i - W / 2)) % W;
+            if (d < 0) d += W;
+            G[(size_t)ip * W + i] = h[d];
+            if (dG) (*dG)[(size_t)ip * W + i] = dh[d];
+        }
+}
+
 WindowTables* get_window(zola_psf* p, int R, std::string& err) {
     auto it = p->win.find(R);
     if (it != p->win.end()) return &it->second;
@@ -170,25 +202,7 @@ WindowTables* get_window(zola_psf* p, int R, std::string& err) {
             t.C[((size_t)w * D + a) * 2] = std::cos(ang);
             t.C[((size_t)w * D + a) * 2 + 1] = std::sin(ang);
         }
-    std::vector<double> h(W);
-    const double s = W / (2 * M_PI * p->o.sigma);
-    for (int d = 0; d < W; ++d) {
-        double acc = 0.0;
-        for (int f = 0; f < W; ++f) {
-            int fs = f < W / 2 ? f : f - W;
-            double g = std::exp(-0.5 * (double)fs * fs / (s * s));
-            long long m = ((long long)f * d) % W;
-            acc += g * std::cos(2 * M_PI * (double)m / W);
-        }
-        h[d] = acc / W;
-    }
-    t.G.resize((size_t)R * W);
-    for (int ip = 0; ip < R; ++ip)
-        for (int i = 0; i < W; ++i) {
-            int d = ((ip - R / 2) - (i - W / 2)) % W;
-            if (d < 0) d += W;
-            t.G[(size_t)ip * W + i] = h[d];
-        }
+    blur_matrix(R, W, p->o.sigma, t.G, nullptr);
     cudaError_t e = cudaMalloc(&t.d_C, t.C.size() * sizeof(double));
     if (e == cudaSuccess) e = cudaMemcpy(t.d_C, t.C.data(), t.C.size() * sizeof(double), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMalloc(&t.d_G, t.G.size() * sizeof(double));

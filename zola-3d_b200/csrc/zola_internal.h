@@ -129,6 +129,7 @@ namespace zola {
 int build_psf_tables(zola_psf* p, const zola_optics* o, const double* zern, int nz, std::string& err);
 int window_size(int R, int N);
 WindowTables* get_window(zola_psf* p, int R, std::string& err);
+void blur_matrix(int R, int W, double sigma, std::vector<double>& G, std::vector<double>* dG);
 
 // fit_f64.cu
 int launch_model_f64(zola_ctx* ctx, zola_psf* p, WindowTables* w, const double* d_xyz, int n,
