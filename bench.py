@@ -139,6 +139,51 @@ def make_job(z, ctx, torch, n, seed, device, only=None):
     return job
 
 
+def detect_fit_config(z, ctx, nframes, seed=1, precision=None):
+    """Frames of 256^2 px with Poisson(5) tetrapod emitters (45 modes, pupil 128^2,
+    z in +-2 um, A ~ LogNormal(ln 4000, 0.5), B = 30), detected against a 41-slice
+    library (0.1 um) with 40 x 40 ROIs and fitted through the frame pipeline.
+    Returns the frames/s of zola_localize_frames (host frames in, rows out)."""
+    S, R, N = 256, 40, 128
+    rng = np.random.default_rng(seed)
+    zern = zern_tetrapod(np.random.default_rng(seed * 100 + 7))
+    base = dict(size_fft=N, xystep=DX, na=1.4, wavelength=0.66, n_oil=1.518, sigma=0.9)
+    psf_det = z.PSF(ctx, z.optics(kz_reset=True, **base), zern)
+    psf_fit = z.PSF(ctx, z.optics(**base), zern)
+    P = 64  # rendering patch
+    emit = []
+    for f in range(nframes):
+        for _ in range(rng.poisson(5)):
+            cx, cy = rng.uniform(P / 2, S - P / 2, 2)
+            emit.append((f, cx, cy, rng.uniform(-2.0, 2.0), rng.lognormal(np.log(4000.0), 0.5)))
+    emit = np.array(emit)
+    ix, iy = emit[:, 1].astype(int), emit[:, 2].astype(int)
+    # a positive model x moves the PSF towards lower pixel indices
+    xyz = np.c_[(ix - emit[:, 1]) * DX, (iy - emit[:, 2]) * DX, emit[:, 3]]
+    psi = psf_fit.model(P, xyz)
+    img = np.full((nframes, S, S), 30.0)
+    for k in range(len(emit)):
+        f = int(emit[k, 0])
+        img[f, ix[k] - P // 2:ix[k] + P // 2, iy[k] - P // 2:iy[k] + P // 2] += emit[k, 4] * psi[k]
+    frames = rng.poisson(img).astype(np.float64)
+    det = z.Detector(psf_det, S, S, R, -2.0, 2.0, 0.1, 0.1)
+    prec = z.ZOLA_PREC_SPLIT if precision is None else precision
+    kw = dict(photon_threshold=500.0, precision=prec, max_iter=50, tol_xyz=1e-4)
+    z.localize_frames(ctx, det, psf_fit, frames[:min(4, nframes)], -2.0, 2.0, **kw)  # warm-up: tables, plans
+    t0 = time.perf_counter()
+    rows = z.localize_frames(ctx, det, psf_fit, frames, -2.0, 2.0, **kw)
+    dt = time.perf_counter() - t0
+    nz = det.nz
+    det.close()
+    psf_det.close()
+    psf_fit.close()
+    return {"frames": nframes, "seconds": dt, "frames_per_s": nframes / dt, "emitters": int(len(emit)),
+            "localizations": int(len(rows)), "library_slices": nz,
+            "detect_fp64_flops_per_frame": 2.0 * S * S * R * R * nz,
+            "workload": "256x256 frames, Poisson(5) tetrapod emitters, R = 40, 0.1 um library over +-2 um, "
+                        "split-precision fits, host frames in and localization rows out"}
+
+
 def run_step(z, job, precision, stream_ptr, sl=None):
     for j in job:
         p = z.PSF.fit_params(precision=precision, **j["prm_kw"])
@@ -266,6 +311,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--classes", default="", help="comma list of ROI classes to run (profiling); default all")
     ap.add_argument("--pool", type=int, default=4096, help="max ROIs in flight per fit call (0: library default)")
+    ap.add_argument("--detect-frames", type=int, default=200,
+                    help="frames of the detect -> fit pipeline measurement (0: skip)")
     ap.add_argument("--split-mode", default="staged", choices=["staged", "fused"],
                     help="split fit kernels: five stage kernels, or stage 1 + fused stages 2-5")
     args = ap.parse_args()
@@ -478,6 +525,8 @@ def main():
     e2e = {"value": n_total * world / t_e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h)}
 
+    detect = detect_fit_config(z, ctx, args.detect_frames, seed=1 + rank) if args.detect_frames > 0 else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, cores, sample = cpu_baseline(budget_s=args.cpu_seconds)
@@ -495,7 +544,8 @@ def main():
                 "split_per_class": per_class,
                 "fp64_plain_gpu": {"value": fp64_value, "unit": UNIT, "per_class": fp64},
                 "speedup_vs_fp64_plain": value / world / fp64_value,
-                "accuracy_vs_fp64": acc}
+                "accuracy_vs_fp64": acc,
+                "detect_fit_pipeline": detect}
         print(json.dumps(line), flush=True)
     for j in job:
         j["psf"].close()

@@ -175,6 +175,8 @@ typedef struct {
     int precision;            /* ZOLA_PREC_FP64 or ZOLA_PREC_SPLIT for the fits */
     int cand_cap;             /* max candidates per frame (0: 1024) */
     int frames_per_batch;     /* frames per device batch (0: 1024) */
+    int wave_fits;            /* candidates fitted ahead per frame and wave (0: 16); any value gives the
+                                 same rows as the reference's one-at-a-time walk */
 } zola_loc_params;
 
 /* frames: nframes x SX x SY photons (double, first index x, already converted

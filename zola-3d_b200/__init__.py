@@ -54,7 +54,7 @@ class LocParams(ctypes.Structure):
     _fields_ = [("patch", ctypes.c_int), ("minZ", ctypes.c_double), ("maxZ", ctypes.c_double),
                 ("photon_threshold", ctypes.c_double), ("max_snr", ctypes.c_double), ("max_iter", ctypes.c_int),
                 ("tol_xyz", ctypes.c_double), ("precision", ctypes.c_int), ("cand_cap", ctypes.c_int),
-                ("frames_per_batch", ctypes.c_int)]
+                ("frames_per_batch", ctypes.c_int), ("wave_fits", ctypes.c_int)]
 
 
 class FitParams(ctypes.Structure):
@@ -429,13 +429,13 @@ LOC_COLUMNS = ["id", "frame", "x_nm", "y_nm", "z_nm", "intensity", "background",
 
 
 def localize_frames(ctx, det, fit_psf, frames, minZ, maxZ, photon_threshold=500.0, max_snr=1.0, max_iter=30,
-                    tol_xyz=1e-4, precision=ZOLA_PREC_FP64, frame0=0, cand_cap=1024, frames_per_batch=1024):
+                    tol_xyz=1e-4, precision=ZOLA_PREC_FP64, frame0=0, cand_cap=1024, frames_per_batch=1024, wave_fits=0):
     """Detect and localize every frame (LocalizationPipeline): returns a
     structured numpy array with LOC_COLUMNS, one row per localization."""
     frames = np.ascontiguousarray(frames, dtype=np.float64)
     nf = frames.shape[0]
     prm = LocParams(det.R, float(minZ), float(maxZ), float(photon_threshold), float(max_snr), int(max_iter),
-                    float(tol_xyz), int(precision), int(cand_cap), int(frames_per_batch))
+                    float(tol_xyz), int(precision), int(cand_cap), int(frames_per_batch), int(wave_fits))
     cap = max(64, nf * 64)
     out = (Localization * cap)()
     n = ctypes.c_int()

@@ -7,18 +7,26 @@
 //     (myGetMaxPositions, :1218-1250);
 //   - skip it if any pixel of its R x R patch is masked;
 //   - getAandB init from the library PSF of its slice (:1119-1162); fit only
-//     if maxPatch / B > maxSNR (1) and B > 0;
+//     if maxPatch / B > maxSNR (1) and B > 0, else mask the patch pixels above
+//     half the patch maximum;
 //   - accept if A > photonThreshold, |x|,|y| < 10 px, the rounded position is
 //     inside the frame and unmasked, and minZ < z < maxZ (:859-945); then mask
 //     the pixels where model - B > 0.2 max(model - B);
 //   - otherwise mask the patch pixels above half the patch maximum (:967-977).
-// The mask makes each frame sequential, so frames are processed in waves:
-// every wave advances each frame to its next candidate that needs a fit (one
-// per frame) and fits all of them in one batched call (FP64 or split), then
-// applies the filters and masks.  Rows come out in frame order and, within a
-// frame, in processing order; x/y/z in nm as 1000*(i*dx - x) (:905-907), chi2
-// as scoreCompute (:1099-1115), CRLB from the Fisher matrix the reference
-// forms (Localization.java:317-451: dmu/dA taken as mu, h -> 0 limit).
+// A candidate's fit reads only the raw patch and its getAandB start, never
+// the mask, so the fits do not depend on the order.  Frames advance in waves:
+// each wave takes, per frame, the next K candidates that need a fit under the
+// current mask (one CTA per frame tests candidates in parallel chunks: border,
+// centre and patch masks, getAandB, SNR), fits all of them in one batched call
+// (FP64 or split), evaluates the model at every fitted position, and then one
+// CTA per frame replays the reference's sequential walk over the candidates
+// the wave covered: mask tests, acceptance, mask updates.  A candidate masked
+// by an earlier one in the same wave was fitted for nothing; masks only grow,
+// so a candidate the wave found masked stays skipped.  Accepted localizations
+// get chi2 as scoreCompute (:1099-1115) and the CRLB from the Fisher matrix the
+// reference forms (Localization.java:317-451: dmu/dA taken as mu, h -> 0
+// limit).  Rows come out in frame order and, within a frame, in candidate
+// order; x/y/z in nm as 1000*(i*dx - x) (:905-907).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -41,89 +49,199 @@ struct PipeView {
     unsigned char* mask;      // nframes x SX x SY
     const double* cand;       // nframes x cap x 7
     const int* counts;        // nframes
-    int* pointer;             // nframes
-    int* done;                // nframes
     const double* libpsf;     // Z x R x R (normalised library PSFs)
     const double* range;      // Z
-    // wave outputs
-    int* slot_frame;          // n_slots: frame of each fit slot
-    int* nslots;
+    int* cand_slot;           // nframes x cap: fit slot; -1 not fitted (SNR), -2 outside the border,
+                              // -3 masked when the wave looked at it
+    double* cand_maxp;        // nframes x cap: patch maximum
+    int* pointer;             // nframes: first candidate not yet walked
+    int* limit;               // nframes: end of the candidates the current wave covers
+    int* done;                // nframes
+    int* nslots;              // slots of the current wave
+    int slot_cap;
     float* rois;              // slots x R x R
     double* init;             // slots x 5
-    double* meta;             // slots x 4: ci, cj, maxPatch, candidate index
+    int* slot_frame;          // slots
+    int* slot_cand;           // slots
 };
 
-// Advance every frame to its next candidate that needs a fit.
-__global__ void k_pipe_select(PipeView V) {
-    const int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= V.nframes || V.done[f]) return;
-    const int SX = V.SX, SY = V.SY, R = V.R, h = R / 2;
+__device__ inline bool pipe_inside(const PipeView& V, int ci, int cj) {
+    const int h = V.R / 2;
+    return ci > h + 1 && cj > h + 1 && ci < V.SX - h - 1 && cj < V.SY - h - 1;
+}
+
+// getAandB with the library PSF of slice r, threshold 10% of its max; returns
+// whether the candidate is fitted (maxPatch / B > maxSNR and B > 0).
+__device__ bool pipe_a_and_b(const PipeView& V, const double* img, int r, int ci, int cj, double* A_, double* B_,
+                             double* maxp_) {
+    const int R = V.R, h = R / 2, SY = V.SY;
+    const double* psf = V.libpsf + (size_t)r * R * R;
+    double maxp = -INFINITY, maxi = -INFINITY;
+    for (int a = 0; a < R; ++a)
+        for (int b = 0; b < R; ++b) {
+            maxi = fmax(maxi, psf[a * R + b]);
+            maxp = fmax(maxp, img[(size_t)(ci - h + a) * SY + (cj - h + b)]);
+        }
+    const double thr = maxi * 0.1;
+    double B = 0, A = 0, cb = 0, ca = 0;
+    for (int a = 0; a < R; ++a)
+        for (int b = 0; b < R; ++b) {
+            const double v = img[(size_t)(ci - h + a) * SY + (cj - h + b)];
+            if (psf[a * R + b] < thr) { B += v; cb += 1; } else { A += v; ca += 1; }
+        }
+    B = cb != 0 ? B / cb : 0.0;
+    A -= ca * B;
+    *A_ = A;
+    *B_ = B;
+    *maxp_ = maxp;
+    return maxp / B > V.max_snr && B > 0;
+}
+
+// One wave's selection for one frame (one CTA): walking the candidates from
+// the frame's pointer in chunks of blockDim, each thread tests one candidate
+// under the current mask; the first K that need a fit (in candidate order) get
+// slots and their ROI and start.  limit = just past the K-th (or the end).
+__global__ void __launch_bounds__(128) k_pipe_wave(PipeView V, int K) {
+    const int f = blockIdx.x, SX = V.SX, SY = V.SY, R = V.R, h = R / 2, RR = R * R;
+    if (V.done[f]) return;
     const double* img = V.images + (size_t)f * SX * SY;
-    unsigned char* mk = V.mask + (size_t)f * SX * SY;
+    const unsigned char* mk = V.mask + (size_t)f * SX * SY;
     const double* cand = V.cand + (size_t)f * V.cap * 7;
     const int n = min(V.counts[f], V.cap);
-    int p = V.pointer[f];
-    while (true) {
-        int sel = -1;
-        for (int i = p; i < n; ++i) {  // myGetMaxPositions
-            const int ci = (int)llrint(cand[(size_t)i * 7 + 2]), cj = (int)llrint(cand[(size_t)i * 7 + 3]);
-            if (mk[(size_t)ci * SY + cj]) continue;
-            if (ci > h + 1 && cj > h + 1 && ci < SX - h - 1 && cj < SY - h - 1) {
-                sel = i;
-                p = i + 1;
-                break;
+    __shared__ unsigned char sel[128];
+    __shared__ int s_got, s_lim, s_base;
+    int taken = 0, limit = n;
+    for (int c0 = V.pointer[f]; c0 < n && taken < K; c0 += blockDim.x) {
+        const int i = c0 + threadIdx.x;
+        int code = -4;
+        double A = 0, B = 0, maxp = 0;
+        if (i < n) {
+            const double* row = cand + (size_t)i * 7;
+            const int r = (int)llrint(row[1]), ci = (int)llrint(row[2]), cj = (int)llrint(row[3]);
+            if (!pipe_inside(V, ci, cj)) {
+                code = -2;
+            } else {
+                bool masked = mk[(size_t)ci * SY + cj] != 0;
+                for (int k = 0; k < RR && !masked; ++k) masked = mk[(size_t)(ci - h + k / R) * SY + (cj - h + k % R)] != 0;
+                code = masked ? -3 : (pipe_a_and_b(V, img, r, ci, cj, &A, &B, &maxp) ? 0 : -1);
+            }
+            V.cand_slot[(size_t)f * V.cap + i] = code;
+            V.cand_maxp[(size_t)f * V.cap + i] = maxp;
+        }
+        sel[threadIdx.x] = code == 0;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int got = 0, lim = -1;
+            for (int t = 0; t < (int)blockDim.x && c0 + t < n; ++t) {
+                if (!sel[t]) continue;
+                if (got == K - taken) { sel[t] = 0; continue; }
+                ++got;
+                if (got == K - taken) lim = c0 + t + 1;
+            }
+            if (lim >= 0)
+                for (int t = lim - c0; t < (int)blockDim.x; ++t) sel[t] = 0;
+            s_got = got;
+            s_lim = lim;
+            s_base = got ? atomicAdd(V.nslots, got) : 0;
+            int k = 0;
+            for (int t = 0; t < (int)blockDim.x && c0 + t < n; ++t)
+                if (sel[t]) {
+                    const int s = s_base + k++;
+                    V.cand_slot[(size_t)f * V.cap + c0 + t] = s < V.slot_cap ? s : -5;
+                }
+        }
+        __syncthreads();
+        if (sel[threadIdx.x]) {
+            const int s = V.cand_slot[(size_t)f * V.cap + i];
+            if (s >= 0) {
+                const double* row = cand + (size_t)i * 7;
+                const int r = (int)llrint(row[1]), ci = (int)llrint(row[2]), cj = (int)llrint(row[3]);
+                float* roi = V.rois + (size_t)s * RR;
+                for (int a = 0; a < R; ++a)
+                    for (int b = 0; b < R; ++b) roi[a * R + b] = (float)img[(size_t)(ci - h + a) * SY + (cj - h + b)];
+                double* in = V.init + (size_t)s * 5;  // loc.init(A, B, -dx, -dy, range[r] + dz)
+                in[0] = -row[5];
+                in[1] = -row[6];
+                in[2] = V.range[r] + row[4];
+                in[3] = A;
+                in[4] = B;
+                V.slot_frame[s] = f;
+                V.slot_cand[s] = i;
             }
         }
-        if (sel < 0) {
-            V.done[f] = 1;
-            V.pointer[f] = p;
-            return;
-        }
-        const double* row = cand + (size_t)sel * 7;
-        const int r = (int)llrint(row[1]), ci = (int)llrint(row[2]), cj = (int)llrint(row[3]);
-        bool treated = false;
-        for (int a = 0; a < R && !treated; ++a)
-            for (int b = 0; b < R; ++b)
-                if (mk[(size_t)(ci - h + a) * SY + (cj - h + b)]) { treated = true; break; }
-        if (treated) continue;  // alreadyTreated
-        // getAandB with the library PSF of slice r, threshold 10% of its max
-        const double* psf = V.libpsf + (size_t)r * R * R;
-        double maxp = -INFINITY, maxi = -INFINITY;
-        for (int a = 0; a < R; ++a)
-            for (int b = 0; b < R; ++b) {
-                maxi = fmax(maxi, psf[a * R + b]);
-                maxp = fmax(maxp, img[(size_t)(ci - h + a) * SY + (cj - h + b)]);
+        taken += s_got;
+        if (s_lim >= 0) limit = s_lim;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) V.limit[f] = limit;
+}
+
+// Model threshold of each fitted slot: 0.2 max(0, max(psi A + B - B))
+// (maxModelThreshold, LocalizationPipeline.java:872-880).
+__global__ void k_pipe_mthr(int n, int RR, const double* theta, const double* psi, double* mthr) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const double A = theta[5 * s + 3], B = theta[5 * s + 4];
+    const double* ps = psi + (size_t)s * RR;
+    double m = 0.0;
+    for (int k = 0; k < RR; ++k) m = fmax(m, ps[k] * A + B - B);
+    mthr[s] = m * 0.2;
+}
+
+// The reference's sequential walk over one frame's candidates (one CTA per
+// frame), with the speculative fits.  Accepted slots are listed with their
+// candidate index as the in-frame order.
+__global__ void __launch_bounds__(256) k_pipe_replay(PipeView V, const double* theta, const int* status,
+                                                     const double* psi, const double* mthr, int* acc_slot,
+                                                     int* acc_seq, int* nacc) {
+    const int f = blockIdx.x, SX = V.SX, SY = V.SY, R = V.R, h = R / 2, RR = R * R;
+    unsigned char* mk = V.mask + (size_t)f * SX * SY;
+    const double* img = V.images + (size_t)f * SX * SY;
+    const double* cand = V.cand + (size_t)f * V.cap * 7;
+    if (V.done[f]) return;
+    const int n = min(V.counts[f], V.cap), lim = V.limit[f];
+    for (int i = V.pointer[f]; i < lim; ++i) {
+        const int slot = V.cand_slot[(size_t)f * V.cap + i];
+        if (slot == -2 || slot == -3) continue;  // outside the border, or masked (masks only grow)
+        const int ci = (int)llrint(cand[(size_t)i * 7 + 2]), cj = (int)llrint(cand[(size_t)i * 7 + 3]);
+        if (mk[(size_t)ci * SY + cj]) continue;  // uniform read of the (synchronised) mask
+        bool mine = false;
+        for (int k = threadIdx.x; k < RR; k += blockDim.x)
+            mine |= mk[(size_t)(ci - h + k / R) * SY + (cj - h + k % R)] != 0;
+        if (__syncthreads_or(mine)) continue;  // alreadyTreated
+        const double maxp = V.cand_maxp[(size_t)f * V.cap + i];
+        bool accepted = false;
+        if (slot >= 0 && status[slot] != ZOLA_FIT_NAN) {
+            const double* th = theta + (size_t)slot * 5;
+            const double x = th[0], y = th[1], z = th[2], A = th[3];
+            if (A > V.photon_thr && fabs(x) < 10 * V.dx && fabs(y) < 10 * V.dx) {
+                const int px = (int)(ci - x / V.dx), py = (int)(cj - y / V.dx);
+                accepted = px >= 0 && px < SX && py >= 0 && py < SY && !mk[(size_t)px * SY + py] && z > V.minZ &&
+                           z < V.maxZ;
             }
-        const double thr = maxi * 0.1;
-        double B = 0, A = 0, cb = 0, ca = 0;
-        for (int a = 0; a < R; ++a)
-            for (int b = 0; b < R; ++b) {
-                const double v = img[(size_t)(ci - h + a) * SY + (cj - h + b)];
-                if (psf[a * R + b] < thr) { B += v; cb += 1; } else { A += v; ca += 1; }
-            }
-        B = cb != 0 ? B / cb : 0.0;
-        A -= ca * B;
-        if (maxp / B > V.max_snr && B > 0) {
-            const int s = atomicAdd(V.nslots, 1);
-            V.slot_frame[s] = f;
-            float* roi = V.rois + (size_t)s * R * R;
-            for (int a = 0; a < R; ++a)
-                for (int b = 0; b < R; ++b) roi[a * R + b] = (float)img[(size_t)(ci - h + a) * SY + (cj - h + b)];
-            double* in = V.init + (size_t)s * 5;  // loc.init(A, B, -dx, -dy, range[r] + dz)
-            in[0] = -row[5];
-            in[1] = -row[6];
-            in[2] = V.range[r] + row[4];
-            in[3] = A;
-            in[4] = B;
-            double* m = V.meta + (size_t)s * 4;
-            m[0] = ci; m[1] = cj; m[2] = maxp; m[3] = sel;
-            V.pointer[f] = p;
-            return;
         }
-        // not fitted: mask the patch pixels above half the patch maximum
-        for (int a = 0; a < R; ++a)
-            for (int b = 0; b < R; ++b)
-                if (img[(size_t)(ci - h + a) * SY + (cj - h + b)] > maxp * 0.5) mk[(size_t)(ci - h + a) * SY + (cj - h + b)] = 1;
+        __syncthreads();  // every thread has read the mask before it changes
+        if (accepted) {
+            if (threadIdx.x == 0) {
+                const int o = atomicAdd(nacc, 1);
+                acc_slot[o] = slot;
+                acc_seq[o] = i;
+            }
+            const double A = theta[(size_t)slot * 5 + 3], B = theta[(size_t)slot * 5 + 4], thr = mthr[slot];
+            const double* ps = psi + (size_t)slot * RR;
+            for (int k = threadIdx.x; k < RR; k += blockDim.x)
+                if (ps[k] * A + B - B > thr) mk[(size_t)(ci - h + k / R) * SY + (cj - h + k % R)] = 1;
+        } else {
+            for (int k = threadIdx.x; k < RR; k += blockDim.x) {
+                const size_t px = (size_t)(ci - h + k / R) * SY + (cj - h + k % R);
+                if (img[px] > maxp * 0.5) mk[px] = 1;
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        V.pointer[f] = lim;
+        V.done[f] = lim >= n;
     }
 }
 
@@ -132,74 +250,57 @@ struct LocRow {
     double x, y, z, A, B, chi2, cx, cy, cz;
 };
 
-// Filters, mask update and output rows for the fitted slots of one wave.
-__global__ void k_pipe_finish(PipeView V, int n, const double* theta, const int* status, const double* psi,
-                              const double* dpsi, int wave, LocRow* rows, int* nrows, int rows_cap) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
-    const int f = V.slot_frame[s], SX = V.SX, SY = V.SY, R = V.R, h = R / 2, RR = R * R;
-    unsigned char* mk = V.mask + (size_t)f * SX * SY;
-    const double* m = V.meta + (size_t)s * 4;
-    const int ci = (int)m[0], cj = (int)m[1];
-    const double maxp = m[2];
-    const double* th = theta + (size_t)s * 5;
-    const double x = th[0], y = th[1], z = th[2], A = th[3], B = th[4];
-    const double* ps = psi + (size_t)s * RR;
-    const float* roi = V.rois + (size_t)s * RR;
-    bool accepted = false;
-    if (status[s] != ZOLA_FIT_NAN) {
-        double mmax = 0.0;  // maxModelThreshold starts at 0 (LocalizationPipeline.java:872-880)
-        for (int k = 0; k < RR; ++k) mmax = fmax(mmax, ps[k] * A + B - B);
-        const double mthr = mmax * 0.2;
-        if (A > V.photon_thr && fabs(x) < 10 * V.dx && fabs(y) < 10 * V.dx) {
-            const int px = (int)(ci - x / V.dx), py = (int)(cj - y / V.dx);
-            if (px >= 0 && px < SX && py >= 0 && py < SY && !mk[(size_t)px * SY + py] && z > V.minZ && z < V.maxZ) {
-                accepted = true;
-                double chi = 0;
-                for (int k = 0; k < RR; ++k) {
-                    const double mu = ps[k] * A + B;
-                    const double dd = roi[k] - mu;
-                    chi += dd * dd / mu;
-                }
-                chi /= RR;
-                // Fisher matrix as the reference forms it: d mu / dA taken as mu
-                double F[25];
-                for (int q = 0; q < 25; ++q) F[q] = 0;
-                for (int k = 0; k < RR; ++k) {
-                    const double mu = ps[k] * A + B;
-                    const double d[5] = {A * dpsi[((size_t)s * 3 + 0) * RR + k], A * dpsi[((size_t)s * 3 + 1) * RR + k],
-                                         A * dpsi[((size_t)s * 3 + 2) * RR + k], mu, 1.0};
-                    for (int q = 0; q < 5; ++q)
-                        for (int r2 = 0; r2 < 5; ++r2) F[q * 5 + r2] += d[q] * d[r2] / mu;
-                }
-                double cr[5];
-                lm_crlb(F, cr);
-                for (int q = 0; q < 3; ++q)
-                    if (!(cr[q] == cr[q])) cr[q] = F[q * 5 + q] != 0 ? sqrt(1.0 / F[q * 5 + q]) : 1.79769313486231570e308;
-                const int o = atomicAdd(nrows, 1);
-                if (o < rows_cap) {
-                    LocRow& L = rows[o];
-                    L.frame = f; L.seq = wave;
-                    L.x = 1000 * (ci * V.dx - x); L.y = 1000 * (cj * V.dx - y); L.z = 1000 * z;
-                    L.A = A; L.B = B; L.chi2 = chi;
-                    L.cx = 1000 * cr[0]; L.cy = 1000 * cr[1]; L.cz = 1000 * cr[2];
-                }
-                for (int a = 0; a < R; ++a)
-                    for (int b = 0; b < R; ++b)
-                        if (ps[a * R + b] * A + B - B > mthr) mk[(size_t)(ci - h + a) * SY + (cj - h + b)] = 1;
-            }
-        }
-    }
-    if (!accepted)
-        for (int a = 0; a < R; ++a)
-            for (int b = 0; b < R; ++b)
-                if (roi[a * R + b] > maxp * 0.5) mk[(size_t)(ci - h + a) * SY + (cj - h + b)] = 1;
-}
-
 __global__ void k_take_xyz(int n, const double* theta, double* xyz) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s < n)
-        for (int q = 0; q < 3; ++q) xyz[3 * s + q] = theta[5 * s + q];
+        for (int q = 0; q < 3; ++q) xyz[3 * s + q] = theta[5 * (size_t)s + q];
+}
+
+__global__ void k_take_acc(int n, const int* acc_slot, const double* theta, double* xyz) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n)
+        for (int q = 0; q < 3; ++q) xyz[3 * k + q] = theta[5 * (size_t)acc_slot[k] + q];
+}
+
+// chi2 and CRLB of the accepted localizations (psi, dpsi evaluated at their
+// fitted positions, in acceptance-list order).
+__global__ void k_pipe_rows(PipeView V, int n, const int* acc_slot, const int* acc_seq, const double* theta,
+                            const double* psi, const double* dpsi, LocRow* rows) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int s = acc_slot[k], R = V.R, RR = R * R;
+    const int f = V.slot_frame[s], i = V.slot_cand[s];
+    const double* row = V.cand + ((size_t)f * V.cap + i) * 7;
+    const int ci = (int)llrint(row[2]), cj = (int)llrint(row[3]);
+    const double* th = theta + (size_t)s * 5;
+    const double x = th[0], y = th[1], z = th[2], A = th[3], B = th[4];
+    const double* ps = psi + (size_t)k * RR;
+    const float* roi = V.rois + (size_t)s * RR;
+    double chi = 0;
+    for (int q = 0; q < RR; ++q) {
+        const double mu = ps[q] * A + B;
+        const double dd = roi[q] - mu;
+        chi += dd * dd / mu;
+    }
+    chi /= RR;
+    double F[25];
+    for (int q = 0; q < 25; ++q) F[q] = 0;
+    for (int p = 0; p < RR; ++p) {
+        const double mu = ps[p] * A + B;
+        const double d[5] = {A * dpsi[((size_t)k * 3 + 0) * RR + p], A * dpsi[((size_t)k * 3 + 1) * RR + p],
+                             A * dpsi[((size_t)k * 3 + 2) * RR + p], mu, 1.0};
+        for (int q = 0; q < 5; ++q)
+            for (int r2 = 0; r2 < 5; ++r2) F[q * 5 + r2] += d[q] * d[r2] / mu;
+    }
+    double cr[5];
+    lm_crlb(F, cr);
+    for (int q = 0; q < 3; ++q)
+        if (!(cr[q] == cr[q])) cr[q] = F[q * 5 + q] != 0 ? sqrt(1.0 / F[q * 5 + q]) : 1.79769313486231570e308;
+    LocRow& L = rows[k];
+    L.frame = f; L.seq = acc_seq[k];
+    L.x = 1000 * (ci * V.dx - x); L.y = 1000 * (cj * V.dx - y); L.z = 1000 * z;
+    L.A = A; L.B = B; L.chi2 = chi;
+    L.cx = 1000 * cr[0]; L.cy = 1000 * cr[1]; L.cz = 1000 * cr[2];
 }
 
 }  // namespace zola
@@ -210,9 +311,23 @@ namespace {
 
 struct Buf {
     void* p = nullptr;
+    size_t bytes = 0;
+    Buf() = default;
+    Buf(const Buf&) = delete;
+    Buf& operator=(const Buf&) = delete;
     ~Buf() { if (p) cudaFree(p); }
-    cudaError_t alloc(size_t b) { return cudaMalloc(&p, b ? b : 1); }
+    cudaError_t alloc(size_t b) {
+        if (b <= bytes && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, b ? b : 1);
+        if (e == cudaSuccess) bytes = b ? b : 1;
+        return e;
+    }
 };
+
+constexpr int PIPE_WAVE_FITS = 16;  // speculative fits per frame and wave
 
 }  // namespace
 
@@ -222,7 +337,7 @@ extern "C" int zola_localize_frames(zola_ctx* ctx, zola_detector* det, zola_psf*
     if (!ctx || !det || !fit_psf || !prm || !nout || (nframes > 0 && (!frames || !out))) return ZOLA_E_ARG;
     *nout = 0;
     if (nframes <= 0) return ZOLA_OK;
-    const int Z = det->v.Z, SX = det->v.SX, SY = det->v.SY, R = det->v.R;
+    const int SX = det->v.SX, SY = det->v.SY, R = det->v.R;
     if (det->psf->ctx != ctx || fit_psf->ctx != ctx) { ctx->err = "zola_localize_frames: objects of another context"; return ZOLA_E_ARG; }
     if (prm->patch != R) { ctx->err = "zola_localize_frames: params.patch must equal the detector's R"; return ZOLA_E_ARG; }
     if (fit_psf->o.kz_reset) { ctx->err = "zola_localize_frames: the fit PSF needs kz_reset = 0"; return ZOLA_E_ARG; }
@@ -232,17 +347,20 @@ extern "C" int zola_localize_frames(zola_ctx* ctx, zola_detector* det, zola_psf*
     const int FB = std::max(1, std::min(nframes, prm->frames_per_batch > 0 ? prm->frames_per_batch : 1024));
     const size_t SS = (size_t)SX * SY, RR = (size_t)R * R;
     cudaStream_t st = ctx->stream;
-    Buf b_img, b_mask, b_cand, b_cnt, b_ptr, b_done, b_lib, b_rng, b_sf, b_ns, b_rois, b_init, b_meta, b_out5, b_st,
-        b_xyz, b_psi, b_dpsi, b_rows, b_nrows;
+    const int K = prm->wave_fits > 0 ? prm->wave_fits : PIPE_WAVE_FITS;
+    const int slot_cap = FB * K;
+    Buf b_img, b_mask, b_cand, b_cnt, b_lib, b_rng, b_cslot, b_cmax, b_ptr, b_lim, b_done, b_ns, b_rois, b_init, b_sf,
+        b_sc, b_out5, b_st, b_xyz, b_psi, b_mthr, b_acc, b_seq, b_nacc, b_dpsi, b_rows;
     cudaError_t e = cudaSuccess;
     auto A = [&](Buf& b, size_t bytes) { if (e == cudaSuccess) e = b.alloc(bytes); };
     A(b_img, SS * FB * 8); A(b_mask, SS * FB); A(b_cand, (size_t)FB * cap * 7 * 8); A(b_cnt, (size_t)FB * 4);
-    A(b_ptr, (size_t)FB * 4); A(b_done, (size_t)FB * 4); A(b_lib, lib.size() * 8); A(b_rng, range.size() * 8);
-    A(b_sf, (size_t)FB * 4); A(b_ns, 64); A(b_rois, RR * FB * 4); A(b_init, (size_t)FB * 40); A(b_meta, (size_t)FB * 32);
-    A(b_out5, (size_t)FB * 40); A(b_st, (size_t)FB * 4); A(b_xyz, (size_t)FB * 24); A(b_psi, RR * FB * 8);
-    A(b_dpsi, 3 * RR * FB * 8);
-    const int rows_cap = FB * 64;
-    A(b_rows, (size_t)rows_cap * sizeof(LocRow)); A(b_nrows, 64);
+    A(b_lib, lib.size() * 8); A(b_rng, range.size() * 8); A(b_cslot, (size_t)FB * cap * 4);
+    A(b_cmax, (size_t)FB * cap * 8); A(b_ptr, (size_t)FB * 4); A(b_lim, (size_t)FB * 4); A(b_done, (size_t)FB * 4);
+    A(b_ns, 64); A(b_nacc, 64);
+    A(b_rois, RR * slot_cap * 4); A(b_init, (size_t)slot_cap * 40); A(b_sf, (size_t)slot_cap * 4);
+    A(b_sc, (size_t)slot_cap * 4); A(b_out5, (size_t)slot_cap * 40); A(b_st, (size_t)slot_cap * 4);
+    A(b_xyz, (size_t)slot_cap * 24); A(b_psi, RR * slot_cap * 8); A(b_mthr, (size_t)slot_cap * 8);
+    A(b_acc, (size_t)slot_cap * 4); A(b_seq, (size_t)slot_cap * 4);
     if (e == cudaSuccess) e = cudaMemcpyAsync(b_lib.p, lib.data(), lib.size() * 8, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(b_rng.p, range.data(), range.size() * 8, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) { ctx->err = std::string("zola_localize_frames: ") + cudaGetErrorString(e); return ZOLA_E_CUDA; }
@@ -253,12 +371,16 @@ extern "C" int zola_localize_frames(zola_ctx* ctx, zola_detector* det, zola_psf*
     V.dx = fit_psf->o.xystep; V.minZ = prm->minZ; V.maxZ = prm->maxZ; V.photon_thr = prm->photon_threshold;
     V.max_snr = prm->max_snr;
     V.images = (double*)b_img.p; V.mask = (unsigned char*)b_mask.p; V.cand = (double*)b_cand.p;
-    V.counts = (int*)b_cnt.p; V.pointer = (int*)b_ptr.p; V.done = (int*)b_done.p;
-    V.libpsf = (double*)b_lib.p; V.range = (double*)b_rng.p;
-    V.slot_frame = (int*)b_sf.p; V.nslots = (int*)b_ns.p; V.rois = (float*)b_rois.p; V.init = (double*)b_init.p;
-    V.meta = (double*)b_meta.p;
+    V.counts = (int*)b_cnt.p; V.libpsf = (double*)b_lib.p; V.range = (double*)b_rng.p;
+    V.cand_slot = (int*)b_cslot.p; V.cand_maxp = (double*)b_cmax.p; V.pointer = (int*)b_ptr.p;
+    V.limit = (int*)b_lim.p; V.done = (int*)b_done.p; V.nslots = (int*)b_ns.p; V.slot_cap = slot_cap;
+    V.rois = (float*)b_rois.p; V.init = (double*)b_init.p; V.slot_frame = (int*)b_sf.p; V.slot_cand = (int*)b_sc.p;
     std::vector<LocRow> all;
-    int h_ns = 0, h_nrows = 0;
+    std::vector<int> done;
+    auto fail = [&](cudaError_t err) {
+        ctx->err = std::string("zola_localize_frames: ") + cudaGetErrorString(err);
+        return ZOLA_E_CUDA;
+    };
     for (int f0 = 0; f0 < nframes; f0 += FB) {
         const int nf = std::min(FB, nframes - f0);
         V.nframes = nf;
@@ -266,44 +388,65 @@ extern "C" int zola_localize_frames(zola_ctx* ctx, zola_detector* det, zola_psf*
         if (e == cudaSuccess) e = cudaMemsetAsync(b_mask.p, 0, SS * nf, st);
         if (e == cudaSuccess) e = cudaMemsetAsync(b_ptr.p, 0, (size_t)nf * 4, st);
         if (e == cudaSuccess) e = cudaMemsetAsync(b_done.p, 0, (size_t)nf * 4, st);
-        if (e == cudaSuccess) e = cudaMemsetAsync(b_nrows.p, 0, 4, st);
-        if (e != cudaSuccess) { ctx->err = std::string("zola_localize_frames: ") + cudaGetErrorString(e); return ZOLA_E_CUDA; }
+        if (e != cudaSuccess) return fail(e);
         int rc = zola_detect_dev(det, (double*)b_img.p, nf, cap, (double*)b_cand.p, (int*)b_cnt.p, st);
         if (rc) return rc;
         for (int wave = 0;; ++wave) {
-            if (cudaMemsetAsync(b_ns.p, 0, 4, st) != cudaSuccess) return ZOLA_E_CUDA;
-            k_pipe_select<<<(nf + 127) / 128, 128, 0, st>>>(V);
+            e = cudaMemsetAsync(b_ns.p, 0, 4, st);
+            if (e == cudaSuccess) e = cudaMemsetAsync(b_nacc.p, 0, 4, st);
+            if (e != cudaSuccess) return fail(e);
+            k_pipe_wave<<<nf, 128, 0, st>>>(V, K);
             ctx->launches++;
-            e = cudaMemcpyAsync(&h_ns, b_ns.p, 4, cudaMemcpyDeviceToHost, st);
+            int nslot = 0;
+            e = cudaMemcpyAsync(&nslot, b_ns.p, 4, cudaMemcpyDeviceToHost, st);
             if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-            if (e != cudaSuccess) { ctx->err = std::string("zola_localize_frames: ") + cudaGetErrorString(e); return ZOLA_E_CUDA; }
-            if (h_ns == 0) break;
-            rc = zola_fit_batch_dev(ctx, fit_psf, R, (float*)b_rois.p, (double*)b_init.p, h_ns, &fp, (double*)b_out5.p,
-                                    nullptr, nullptr, (int*)b_st.p, nullptr, st);
-            if (rc) return rc;
-            k_take_xyz<<<(h_ns + 127) / 128, 128, 0, st>>>(h_ns, (double*)b_out5.p, (double*)b_xyz.p);
+            if (e != cudaSuccess) return fail(e);
+            if (nslot > 0) {
+                rc = zola_fit_batch_dev(ctx, fit_psf, R, (float*)b_rois.p, (double*)b_init.p, nslot, &fp,
+                                        (double*)b_out5.p, nullptr, nullptr, (int*)b_st.p, nullptr, st);
+                if (rc) return rc;
+                // psi at every fitted position (mask updates of the walk)
+                k_take_xyz<<<(nslot + 127) / 128, 128, 0, st>>>(nslot, (double*)b_out5.p, (double*)b_xyz.p);
+                ctx->launches++;
+                rc = zola_psf_model_dev(fit_psf, R, (double*)b_xyz.p, nslot, (double*)b_psi.p, nullptr, st);
+                if (rc) return rc;
+                k_pipe_mthr<<<(nslot + 127) / 128, 128, 0, st>>>(nslot, (int)RR, (double*)b_out5.p,
+                                                                 (double*)b_psi.p, (double*)b_mthr.p);
+                ctx->launches++;
+            }
+            k_pipe_replay<<<nf, 256, 0, st>>>(V, (double*)b_out5.p, (int*)b_st.p, (double*)b_psi.p,
+                                             (double*)b_mthr.p, (int*)b_acc.p, (int*)b_seq.p, (int*)b_nacc.p);
             ctx->launches++;
-            rc = zola_psf_model_dev(fit_psf, R, (double*)b_xyz.p, h_ns, (double*)b_psi.p, (double*)b_dpsi.p, st);
-            if (rc) return rc;
-            k_pipe_finish<<<(h_ns + 127) / 128, 128, 0, st>>>(V, h_ns, (double*)b_out5.p, (int*)b_st.p,
-                                                              (double*)b_psi.p, (double*)b_dpsi.p, wave,
-                                                              (LocRow*)b_rows.p, (int*)b_nrows.p, rows_cap);
-            ctx->launches++;
-            if (cudaGetLastError() != cudaSuccess) { ctx->err = "zola_localize_frames: kernel launch failed"; return ZOLA_E_CUDA; }
+            int nacc = 0;
+            done.assign(nf, 0);
+            e = cudaMemcpyAsync(&nacc, b_nacc.p, 4, cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(done.data(), b_done.p, (size_t)nf * 4, cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) return fail(e);
+            if (nacc > 0) {
+                A(b_dpsi, 3 * RR * (size_t)nacc * 8); A(b_rows, (size_t)nacc * sizeof(LocRow));
+                if (e != cudaSuccess) return fail(e);
+                k_take_acc<<<(nacc + 127) / 128, 128, 0, st>>>(nacc, (int*)b_acc.p, (double*)b_out5.p,
+                                                               (double*)b_xyz.p);
+                ctx->launches++;
+                // the walk has used psi; its buffer now takes the accepted positions' models
+                rc = zola_psf_model_dev(fit_psf, R, (double*)b_xyz.p, nacc, (double*)b_psi.p, (double*)b_dpsi.p, st);
+                if (rc) return rc;
+                k_pipe_rows<<<(nacc + 127) / 128, 128, 0, st>>>(V, nacc, (int*)b_acc.p, (int*)b_seq.p,
+                                                                (double*)b_out5.p, (double*)b_psi.p,
+                                                                (double*)b_dpsi.p, (LocRow*)b_rows.p);
+                ctx->launches++;
+                std::vector<LocRow> rows(nacc);
+                e = cudaMemcpyAsync(rows.data(), b_rows.p, (size_t)nacc * sizeof(LocRow), cudaMemcpyDeviceToHost, st);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+                if (e != cudaSuccess) return fail(e);
+                for (auto& r : rows) r.frame += f0;
+                all.insert(all.end(), rows.begin(), rows.end());
+            }
+            if (std::all_of(done.begin(), done.end(), [](int d) { return d != 0; })) break;
         }
-        e = cudaMemcpyAsync(&h_nrows, b_nrows.p, 4, cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) { ctx->err = std::string("zola_localize_frames: ") + cudaGetErrorString(e); return ZOLA_E_CUDA; }
-        if (h_nrows > rows_cap) { ctx->err = "zola_localize_frames: more than 64 localizations per frame"; return ZOLA_E_ARG; }
-        std::vector<LocRow> rows(h_nrows);
-        if (h_nrows) {
-            e = cudaMemcpy(rows.data(), b_rows.p, (size_t)h_nrows * sizeof(LocRow), cudaMemcpyDeviceToHost);
-            if (e != cudaSuccess) { ctx->err = std::string("zola_localize_frames: ") + cudaGetErrorString(e); return ZOLA_E_CUDA; }
-        }
-        for (auto& r : rows) r.frame += f0;
-        all.insert(all.end(), rows.begin(), rows.end());
     }
-    std::stable_sort(all.begin(), all.end(), [](const LocRow& a, const LocRow& b) {
+    std::sort(all.begin(), all.end(), [](const LocRow& a, const LocRow& b) {
         return a.frame != b.frame ? a.frame < b.frame : a.seq < b.seq;
     });
     if ((int)all.size() > out_cap) { ctx->err = "zola_localize_frames: out_cap too small"; *nout = (int)all.size(); return ZOLA_E_ARG; }
