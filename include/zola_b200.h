@@ -246,6 +246,25 @@ ZOLA_API int zola_calib_init(zola_ctx* ctx, const float* raw, int nslice, int W,
                              double zstep, double* photons, double* background, double* patches,
                              double* poly_background);
 
+/* --- 3-D drift correction (replaces DriftCorrection / DriftCorrection_:
+ * process/cpu/DriftCorrection.java:125-990, utils/SplineFit.java).
+ * Localizations (x, y, z nm, frame; crlb nm, -1 or NULL = unknown) are binned
+ * in time; all pairs of bins are cross-correlated as 3-D histograms in
+ * half-overlapping windows of sizeFFT voxels (sizeFFT = the power of two
+ * covering max_drift_um, the voxel grown by 1% steps until sizeFFT <= 128);
+ * bin drifts relative to bin 0 come from the least squares over all pairs
+ * (two passes of outlier rejection at the mean CRLB), and each localization's
+ * drift from the spline of the bin drifts at its frame.
+ * bin_drift: bins x (frame index, dx, dy, dz nm); loc_drift (nullable): n x 3
+ * nm; pixel_nm_used (nullable): the voxel size after the growth. */
+typedef struct {
+    double pixel_nm;      /* histogram voxel (reference: pixelsizeNM) */
+    int bins;             /* time bins */
+    double max_drift_um;  /* subImageSizeUm: the window covers this drift */
+} zola_drift_params;
+ZOLA_API int zola_drift(zola_ctx* ctx, const double* xyz_nm, const double* crlb_nm, const int* frame, int n,
+                        const zola_drift_params* prm, double* bin_drift, double* loc_drift, double* pixel_nm_used);
+
 /* Allocation-free FP64 fit (this entry point has no counterpart in the
  * reference).  For callers that must not allocate device memory while they fit
  * (a host application that owns all device memory and lends plugins only its

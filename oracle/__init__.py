@@ -66,6 +66,8 @@ def lib():
         L.orc_calib_nll_full.restype = d
         L.orc_calib_nll_full.argtypes = [vp, i, i, vp, vp, vp, d, d, d, d, vp, vp]
         L.orc_calib_init.restype = i
+        L.orc_drift.restype = i
+        L.orc_drift.argtypes = [vp, vp, vp, i, d, i, d, vp, vp, vp]
         L.orc_calib_init.argtypes = [vp, i, i, i, vp, vp, i, i, d, d, d, d, vp, vp, vp, vp]
         _lib = L
     return _lib
@@ -239,3 +241,19 @@ def calib_init(raw, xpoints, ypoints, size_patch, adu=1.0, gain=1.0, offset=0.0,
     if rc:
         raise ValueError("singular background fit")
     return dict(x=xp, y=yp, background=bg, photons=ph, patches=pt, surface=poly)
+
+
+def drift(xyz_nm, frame, crlb_nm=None, pixel_nm=10.0, bins=20, max_drift_um=0.5):
+    """DriftCorrection restated: (bin_drift (bins, 4), per-localization drift (n, 3), voxel size used)."""
+    xyz = _f64(xyz_nm)
+    fr = np.ascontiguousarray(frame, dtype=np.int32)
+    cr = None if crlb_nm is None else _f64(crlb_nm)
+    n = len(fr)
+    out_b = np.zeros((bins, 4))
+    out_l = np.zeros((n, 3))
+    px = np.zeros(1)
+    rc = lib().orc_drift(_p(xyz), _p(cr) if cr is not None else None, _p(fr), n, pixel_nm, bins, max_drift_um,
+                         _p(out_b), _p(out_l), _p(px))
+    if rc:
+        raise ValueError("bad drift arguments")
+    return out_b, out_l, px[0]

@@ -28,6 +28,8 @@
 //   detection         process/cpu/Predetection.java:63-593
 //   calibration NLL   process/cpu/ZernikePhaseRetrieval.java:1519-1530, 1843-1874
 //   calibration init  process/InitBackgroundAndPhotonNumber.java (+ utils/PolynomialFit.java)
+//   drift correction  process/cpu/DriftCorrection.java, utils/SplineFit.java,
+//                     utils/GaussianElimination.java
 // plus the FP64 Levenberg-Marquardt fit of the same Poisson NLL with analytic
 // x/y/z derivatives (no reference counterpart: the "FP64 oracle of the same
 // fit" that the GPU fits are compared against).
@@ -1300,6 +1302,344 @@ int orc_calib_init(const double* raw, int ns, int W, int H, float* xp, float* yp
                 for (int uu = 0; uu < sp; ++uu)
                     patches[(((size_t)p * ns + z) * sp + u) * sp + uu] =
                         (x0 + u >= 0 && x0 + u < W && y0 + uu >= 0 && y0 + uu < H) ? at(z, x0 + u, y0 + uu) : b;
+    }
+    return 0;
+}
+
+
+}  // extern "C"
+
+namespace {
+
+// In-place 3D FFT of a P0 x P1 x P2 complex cube (index [a][b][c]), 1-D passes
+// along each axis (sign -1 forward, +1 inverse; unitary per pass).
+void fft3d(std::vector<cplx>& v, int P0, int P1, int P2, int sign) {
+    std::vector<cplx> line(std::max(P0, std::max(P1, P2)));
+    for (int a = 0; a < P0; ++a)
+        for (int b = 0; b < P1; ++b) fft1d(&v[((size_t)a * P1 + b) * P2], P2, sign);
+    for (int a = 0; a < P0; ++a)
+        for (int c = 0; c < P2; ++c) {
+            for (int b = 0; b < P1; ++b) line[b] = v[((size_t)a * P1 + b) * P2 + c];
+            fft1d(line.data(), P1, sign);
+            for (int b = 0; b < P1; ++b) v[((size_t)a * P1 + b) * P2 + c] = line[b];
+        }
+    for (int b = 0; b < P1; ++b)
+        for (int c = 0; c < P2; ++c) {
+            for (int a = 0; a < P0; ++a) line[a] = v[((size_t)a * P1 + b) * P2 + c];
+            fft1d(line.data(), P0, sign);
+            for (int a = 0; a < P0; ++a) v[((size_t)a * P1 + b) * P2 + c] = line[a];
+        }
+}
+
+// utils/GaussianElimination.java:107-140 (partial pivoting; exact-zero pivot = singular).
+bool gauss_solve(std::vector<std::vector<double>> A, std::vector<double> b, std::vector<double>& x) {
+    const int N = (int)b.size();
+    for (int p = 0; p < N; ++p) {
+        int mx = p;
+        for (int i = p + 1; i < N; ++i) if (std::fabs(A[i][p]) > std::fabs(A[mx][p])) mx = i;
+        std::swap(A[p], A[mx]);
+        std::swap(b[p], b[mx]);
+        if (std::fabs(A[p][p]) <= 0) return false;
+        for (int i = p + 1; i < N; ++i) {
+            const double alpha = A[i][p] / A[p][p];
+            b[i] -= alpha * b[p];
+            for (int j = p; j < N; ++j) A[i][j] -= alpha * A[p][j];
+        }
+    }
+    x.assign(N, 0.0);
+    for (int i = N - 1; i >= 0; --i) {
+        double sum = 0.0;
+        for (int j = i + 1; j < N; ++j) sum += A[i][j] * x[j];
+        x[i] = (b[i] - sum) / A[i][i];
+    }
+    return true;
+}
+
+// Interpolating polynomial through up to 4 points (utils/SplineFit.java's
+// PolynomialFit windows), value and first derivative by Newton divided
+// differences.
+struct Cubic {
+    int n = 0;
+    double x[4], c[4];
+    void fit(const double* xs, const double* ys, int m) {
+        n = m;
+        for (int i = 0; i < m; ++i) { x[i] = xs[i]; c[i] = ys[i]; }
+        for (int j = 1; j < m; ++j)
+            for (int i = m - 1; i >= j; --i) c[i] = (c[i] - c[i - 1]) / (x[i] - x[i - j]);
+    }
+    double value(double t) const {
+        double v = c[n - 1];
+        for (int i = n - 2; i >= 0; --i) v = v * (t - x[i]) + c[i];
+        return v;
+    }
+    double slope(double t) const {
+        double v = c[n - 1], d = 0;
+        for (int i = n - 2; i >= 0; --i) { d = d * (t - x[i]) + v; v = v * (t - x[i]) + c[i]; }
+        return d;
+    }
+};
+
+// SplineFit (utils/SplineFit.java:24-75, 88-150, 195-250): cubic windows of 4
+// consecutive knots, linear extrapolation with the end windows' slopes.
+struct Spline {
+    std::vector<double> x, y;
+    std::vector<Cubic> pf;
+    void fit(const std::vector<double>& xs, const std::vector<double>& ys) {
+        x = xs; y = ys;
+        for (size_t i = 0; i < x.size(); ++i)  // bubble sort as the reference
+            for (size_t ii = 1; ii < x.size() - i; ++ii)
+                if (x[ii] < x[ii - 1]) { std::swap(x[ii], x[ii - 1]); std::swap(y[ii], y[ii - 1]); }
+        const int L = (int)x.size();
+        pf.assign(std::max(1, L + 1 - 4), Cubic());
+        if (L < 2) return;
+        if (L < 4) { pf[0].fit(x.data(), y.data(), L); return; }
+        for (int id = 0; id < L - 3; ++id) pf[id].fit(&x[id], &y[id], 4);
+    }
+    double eval(double X) const {
+        const int L = (int)x.size();
+        if (L < 2) return -1;
+        if (L < 4) return pf[0].value(X);
+        int id = 0;
+        for (int i = 0; i < L; ++i) { id = i; if (X < x[i]) break; }
+        if (X > x[L - 1]) id = L;
+        if (id == 1) id = 2;
+        if (id == L - 1) id = L - 2;
+        if (id == 0) return pf[0].slope(x[0]) * (X - x[0]) + y[0];
+        if (id == L) return pf[L - 4].slope(x[L - 1]) * (X - x[L - 1]) + y[L - 1];
+        return pf[id - 2].value(X);
+    }
+};
+
+// LocalMaxima.run(threshold) (process/cpu/DriftCorrection.java:1084-1200) on a
+// W0 x W1 x W2 float volume: centroid of the values above the threshold
+// quantile in the 11^3 patch around the first maximum; returns the drift
+// (-(c - size/2)) along the three indices.
+void local_maxima(const std::vector<float>& im, int W0, int W1, int W2, double thr, double d[3]) {
+    int s0 = std::min(11, W0 - 1), s1 = std::min(11, W1 - 1), s2 = std::min(11, W2 - 1);
+    if (s0 % 2 == 0) s0--;
+    if (s1 % 2 == 0) s1--;
+    if (s2 % 2 == 0) s2--;
+    s0 = std::max(s0, 1); s1 = std::max(s1, 1); s2 = std::max(s2, 1);  // one-voxel axes (the reference throws)
+    double mx = 4.9e-324;  // Double.MIN_VALUE
+    int a0 = 0, b0 = 0, c0 = 0;
+    for (int i = 0; i < W0; ++i)
+        for (int ii = 0; ii < W1; ++ii)
+            for (int iii = 0; iii < W2; ++iii)
+                if (mx < im[((size_t)i * W1 + ii) * W2 + iii]) { mx = im[((size_t)i * W1 + ii) * W2 + iii]; a0 = i; b0 = ii; c0 = iii; }
+    std::vector<float> v;
+    auto inb = [&](int i, int ii, int iii) {
+        return i + a0 - s0 / 2 >= 0 && ii + b0 - s1 / 2 >= 0 && iii + c0 - s2 / 2 >= 0 && i + a0 - s0 / 2 < W0 &&
+               ii + b0 - s1 / 2 < W1 && iii + c0 - s2 / 2 < W2;
+    };
+    auto val = [&](int i, int ii, int iii) {
+        return im[((size_t)(i + a0 - s0 / 2) * W1 + (ii + b0 - s1 / 2)) * W2 + (iii + c0 - s2 / 2)];
+    };
+    for (int i = 0; i < s0; ++i)
+        for (int ii = 0; ii < s1; ++ii)
+            for (int iii = 0; iii < s2; ++iii)
+                if (inb(i, ii, iii)) v.push_back(val(i, ii, iii));
+    std::sort(v.begin(), v.end());
+    const float t = v[(int)((v.size() - 1) * thr)];
+    double x = 0, y = 0, z = 0, sum = 0;
+    for (int i = 0; i < s0; ++i)
+        for (int ii = 0; ii < s1; ++ii)
+            for (int iii = 0; iii < s2; ++iii)
+                if (inb(i, ii, iii) && val(i, ii, iii) > t) {
+                    const double w = val(i, ii, iii);
+                    sum += w;
+                    x += (i + a0 - s0 / 2) * w;
+                    y += (ii + b0 - s1 / 2) * w;
+                    z += (iii + c0 - s2 / 2) * w;
+                }
+    x /= sum; y /= sum; z /= sum;
+    d[0] = -(x - W0 / 2);
+    d[1] = -(y - W1 / 2);
+    d[2] = -(z - W2 / 2);
+}
+
+}  // namespace
+
+extern "C" {
+
+// DriftCorrection (process/cpu/DriftCorrection.java:125-410, 418-990): 3-D
+// histograms of the localizations per time bin in half-overlapping windows of
+// sizeFFT voxels (zero-padded to twice that), Gaussian-filtered in Fourier
+// space, all-pairs cross-correlations summed over the windows, sub-voxel peak
+// centroids, least-squares drift per bin relative to bin 0 with two passes of
+// outlier rejection at the mean CRLB, and the SplineFit of the bin drifts at
+// every localization's frame.  xyz / crlb in nm (crlb -1: unknown).
+// bin_out: bins x 4 (frame index, dx, dy, dz nm); loc_out: n x 3.
+int orc_drift(const double* xyz, const double* crlb, const int* frame, int n, double pixel_nm, int bin,
+              double sub_um, double* bin_out, double* loc_out, double* px_used) {
+    if (n < 1 || bin < 1) return -1;
+    int sizeFFT = (int)std::pow(2, (int)std::ceil(std::log(sub_um / (pixel_nm / 1000.)) / std::log(2)));
+    while (sizeFFT > 128) {
+        pixel_nm *= 1.01;
+        sizeFFT = (int)std::pow(2, (int)std::ceil(std::log(sub_um / (std::floor(pixel_nm + 0.5) / 1000.)) / std::log(2)));
+    }
+    pixel_nm = std::floor(pixel_nm + 0.5);
+    if (px_used) *px_used = pixel_nm;
+    const double DMIN = 4.9e-324, DMAX = 1.7976931348623157e308;
+    double minX = DMAX, maxX = DMIN, minY = DMAX, maxY = DMIN, minZ = DMAX, maxZ = DMIN;
+    int minF = 2147483647, maxF = -2147483647 - 1;
+    double px = 0, py = 0, pz = 0;
+    int cx = 0, cy = 0, cz = 0;
+    for (int k = 0; k < n; ++k) {
+        const double x = xyz[3 * k], y = xyz[3 * k + 1], z = xyz[3 * k + 2];
+        const int f = frame[k];
+        if (x < minX) minX = x;
+        if (y < minY) minY = y;
+        if (x > maxX) maxX = x;
+        if (y > maxY) maxY = y;
+        if (z < minZ) minZ = z;
+        if (z > maxZ) maxZ = z;
+        if (f < minF) minF = f;
+        if (f > maxF) maxF = f;
+        if (crlb) {
+            if (crlb[3 * k] != -1) { px += crlb[3 * k]; cx++; }
+            if (crlb[3 * k + 1] != -1) { py += crlb[3 * k + 1]; cy++; }
+            if (crlb[3 * k + 2] != -1) { pz += crlb[3 * k + 2]; cz++; }
+        }
+    }
+    px = cx == 0 ? 50 : px / cx;
+    py = cy == 0 ? 50 : py / cy;
+    pz = cz == 0 ? 50 : pz / cz;
+    int width = std::max((int)std::ceil((maxX - minX) / pixel_nm), 1);
+    int height = std::max((int)std::ceil((maxY - minY) / pixel_nm), 1);
+    int depth = std::max((int)std::ceil((maxZ - minZ) / pixel_nm), 1);
+    int sF[3] = {std::min(sizeFFT, width), std::min(sizeFFT, height), std::min(sizeFFT, depth)};
+    for (int d = 0; d < 3; ++d) sF[d] = std::max(sF[d], (int)std::pow(2, std::ceil(std::log(sF[d]) / std::log(2))));
+    const int ext[3] = {width, height, depth};
+    int nb[3];
+    for (int d = 0; d < 3; ++d)  // a one-voxel extent gives one window (the reference divides by zero there)
+        nb[d] = sF[d] < 2 ? 1 : (int)std::ceil((double)(ext[d] - sF[d] / 2) / (double)(sF[d] / 2));
+    const int P[3] = {2 * sF[0], 2 * sF[1], 2 * sF[2]};  // x, y, z
+    const size_t PV = (size_t)P[0] * P[1] * P[2];
+    // Fourier Gaussian, cube index [z][y][x], float-rounded (:290-320)
+    const double sigma = 3 * std::max(std::max(px, py), pz) / pixel_nm;
+    double sf2[3];
+    for (int d = 0; d < 3; ++d) { const double v = (1. / sigma) * (double)P[d] / (M_PI * 2.); sf2[d] = v * v; }
+    std::vector<float> gauss(PV);
+    for (int xx = 0; xx < P[0]; ++xx)
+        for (int yy = 0; yy < P[1]; ++yy)
+            for (int zz = 0; zz < P[2]; ++zz) {
+                const int xs = (xx + P[0] / 2) % P[0], ys = (yy + P[1] / 2) % P[1], zs = (zz + P[2] / 2) % P[2];
+                const double dx = (xx - P[0] / 2.) * (xx - P[0] / 2.), dy = (yy - P[1] / 2.) * (yy - P[1] / 2.),
+                             dz = (zz - P[2] / 2.) * (zz - P[2] / 2.);
+                gauss[((size_t)zs * P[1] + ys) * P[0] + xs] = (float)std::exp(-.5 * (dx / sf2[0] + dy / sf2[1] + dz / sf2[2]));
+            }
+    std::vector<int> pos1, pos2;
+    for (int t = 0; t < bin - 1; ++t)
+        for (int s = t + 1; s < bin; ++s) { pos1.push_back(t); pos2.push_back(s); }
+    const int tot = (int)pos1.size();
+    const size_t RV = (size_t)sF[0] * sF[1] * sF[2];
+    std::vector<float> result((size_t)tot * RV, 0.0f);
+    std::vector<std::vector<cplx>> spec(bin, std::vector<cplx>(PV));
+    std::vector<cplx> prod(PV), tmp(PV);
+    for (int u = 0; u < nb[0]; ++u)
+        for (int uu = 0; uu < nb[1]; ++uu)
+            for (int uuu = 0; uuu < nb[2]; ++uuu) {
+                const int uv[3] = {u, uu, uuu};
+                double g0[3], g1[3];
+                for (int d = 0; d < 3; ++d) {
+                    g0[d] = (uv[d] / 2) * sF[d] * pixel_nm + (uv[d] % 2) * (sF[d] / 2) * pixel_nm;
+                    g1[d] = (uv[d] / 2 + 1) * sF[d] * pixel_nm + (uv[d] % 2) * (sF[d] / 2) * pixel_nm;
+                }
+                std::vector<std::vector<double>> img(bin, std::vector<double>(PV, 0.0));
+                for (int k = 0; k < n; ++k) {
+                    const double x = xyz[3 * k] - minX, y = xyz[3 * k + 1] - minY, z = xyz[3 * k + 2] - minZ;
+                    if (!(x >= g0[0] && x < g1[0] && y >= g0[1] && y < g1[1] && z >= g0[2] && z < g1[2])) continue;
+                    const int idBin = bin * (frame[k] - minF) / (1 + maxF - minF);
+                    const int xi = sF[0] / 2 + std::min(std::max((int)(std::fmod(x, sF[0] * pixel_nm) / pixel_nm), 0), sF[0] - 1);
+                    const int yi = sF[1] / 2 + std::min(std::max((int)(std::fmod(y, sF[1] * pixel_nm) / pixel_nm), 0), sF[1] - 1);
+                    const int zi = sF[2] / 2 + std::min(std::max((int)(std::fmod(z, sF[2] * pixel_nm) / pixel_nm), 0), sF[2] - 1);
+                    img[idBin][((size_t)zi * P[1] + yi) * P[0] + xi] += 1;
+                }
+                for (int b = 0; b < bin; ++b) {  // Init: shift3D, FFT, Gaussian
+                    for (int a = 0; a < P[2]; ++a)
+                        for (int bb = 0; bb < P[1]; ++bb)
+                            for (int c = 0; c < P[0]; ++c)
+                                spec[b][((size_t)a * P[1] + bb) * P[0] + c] =
+                                    cplx(img[b][((size_t)((a + P[2] / 2) % P[2]) * P[1] + (bb + P[1] / 2) % P[1]) * P[0] +
+                                                (c + P[0] / 2) % P[0]], 0.0);
+                    fft3d(spec[b], P[2], P[1], P[0], -1);
+                    for (size_t k = 0; k < PV; ++k) spec[b][k] *= (double)gauss[k];
+                }
+                for (int id = 0; id < tot; ++id) {  // Process: F1 conj(F2), IFFT, shift3D, crop
+                    const auto& F1 = spec[pos1[id]];
+                    const auto& F2 = spec[pos2[id]];
+                    for (size_t k = 0; k < PV; ++k) prod[k] = F1[k] * std::conj(F2[k]);
+                    fft3d(prod, P[2], P[1], P[0], +1);
+                    for (int a = 0; a < sF[2]; ++a)
+                        for (int bb = 0; bb < sF[1]; ++bb)
+                            for (int c = 0; c < sF[0]; ++c) {
+                                const int as = (a + sF[2] / 2 + P[2] / 2) % P[2], bs = (bb + sF[1] / 2 + P[1] / 2) % P[1],
+                                          cs = (c + sF[0] / 2 + P[0] / 2) % P[0];
+                                result[(size_t)id * RV + ((size_t)a * sF[1] + bb) * sF[0] + c] +=
+                                    (float)prod[((size_t)as * P[1] + bs) * P[0] + cs].real();
+                            }
+                }
+            }
+    const double fpb = ((double)(maxF - minF)) / ((double)bin);
+    std::vector<double> di(bin, 0.0), dr[3];
+    for (int d = 0; d < 3; ++d) dr[d].assign(bin, 0.0);
+    di[0] = (double)minF + fpb / 2.;
+    std::vector<std::vector<double>> Am(tot, std::vector<double>(std::max(bin - 1, 0), 0.0));
+    std::vector<double> Rm[3];
+    for (int d = 0; d < 3; ++d) Rm[d].assign(tot, 0.0);
+    for (int id = 0; id < tot; ++id) {
+        std::vector<float> vol(result.begin() + (size_t)id * RV, result.begin() + (size_t)(id + 1) * RV);
+        double lm[3];  // along z, y, x indices
+        local_maxima(vol, sF[2], sF[1], sF[0], .95, lm);
+        const double drift[3] = {lm[2] * pixel_nm, lm[1] * pixel_nm, lm[0] * pixel_nm};
+        const int t = pos1[id], s = pos2[id];
+        if (t == 0) {
+            di[s] = (((double)s) / ((double)bin)) * ((double)(1. + maxF - minF)) + ((double)minF) + (fpb / 2.);
+            for (int d = 0; d < 3; ++d) dr[d][s] = drift[d];
+        }
+        for (int d = 0; d < 3; ++d) Rm[d][id] = drift[d];
+        if (t != 0) Am[id][t - 1] = -1;
+        Am[id][s - 1] = 1;
+    }
+    const double thr[3] = {px, py, pz};
+    if (bin > 2 && tot > bin) {
+        std::vector<int> del[3];
+        for (int check = 0; check < 2; ++check)
+            for (int d = 0; d < 3; ++d) {
+                std::vector<std::vector<double>> An;
+                std::vector<double> Rn;
+                for (int i = 0; i < tot; ++i) {
+                    if (std::find(del[d].begin(), del[d].end(), i) != del[d].end()) continue;
+                    An.push_back(Am[i]);
+                    Rn.push_back(Rm[d][i]);
+                }
+                if ((int)An.size() < bin - 1) continue;
+                const int m = bin - 1;
+                std::vector<std::vector<double>> N(m, std::vector<double>(m, 0.0));
+                std::vector<double> r(m, 0.0), sol;
+                for (int a = 0; a < m; ++a) {
+                    for (int b = 0; b < m; ++b)
+                        for (size_t i = 0; i < An.size(); ++i) N[a][b] += An[i][a] * An[i][b];
+                    for (size_t i = 0; i < An.size(); ++i) r[a] += An[i][a] * Rn[i];
+                }
+                if (!gauss_solve(N, r, sol)) continue;
+                for (size_t i = 0; i < An.size(); ++i) {
+                    double fit = 0;
+                    for (int a = 0; a < m; ++a) fit += An[i][a] * sol[a];
+                    if (std::fabs(fit - Rn[i]) > thr[d]) del[d].push_back((int)i);
+                }
+                for (int a = 0; a < m; ++a) dr[d][a + 1] = sol[a];
+            }
+    }
+    for (int b = 0; b < bin; ++b) {
+        bin_out[4 * b] = di[b];
+        for (int d = 0; d < 3; ++d) bin_out[4 * b + 1 + d] = dr[d][b];
+    }
+    if (loc_out) {
+        Spline sp[3];
+        for (int d = 0; d < 3; ++d) sp[d].fit(di, dr[d]);
+        for (int k = 0; k < n; ++k)
+            for (int d = 0; d < 3; ++d) loc_out[3 * k + d] = sp[d].eval((double)frame[k]);
     }
     return 0;
 }

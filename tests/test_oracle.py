@@ -219,3 +219,35 @@ def test_calib_init_recovers_background_photons_and_seeds():
     # photon curve: the patch holds most of the bead's photons; the box filter smooths the Gaussian profile
     assert np.all(np.abs(out["photons"][:, len(dz) // 2] / A[len(dz) // 2] - 0.95) < 0.08)
     assert out["patches"].shape == (3, len(dz), 24, 24)
+
+
+def drift_data(seed=0, nf=1000, nbead=40, n_per=30, L=600.0, Lz=200.0, vel=(0.03, -0.02, 0.01), noise=4.0):
+    """Static 3-D structure localized repeatedly while the stage drifts linearly (nm / frame)."""
+    rng = np.random.default_rng(seed)
+    pts = np.c_[rng.uniform(0, L, (nbead, 2)), rng.uniform(0, Lz, nbead)]
+    frames = rng.integers(0, nf, nbead * n_per)
+    src = np.repeat(np.arange(nbead), n_per)
+    dt = np.outer(frames, vel)
+    xyz = pts[src] + dt + rng.normal(0, noise, (len(src), 3))
+    return xyz, frames.astype(np.int32), np.full((len(src), 3), noise), dt, np.array(vel)
+
+
+def test_drift_restatement_recovers_a_linear_drift():
+    xyz, fr, cr, dt, vel = drift_data()
+    b, l, px = O.drift(xyz, fr, cr, pixel_nm=20.0, bins=6, max_drift_um=0.16)
+    assert px == 20.0
+    # bin centres: minF + (s / bins)(1 + maxF - minF) + (maxF - minF) / (2 bins)
+    fpb = (fr.max() - fr.min()) / 6
+    assert np.allclose(b[:, 0], fr.min() + np.arange(6) / 6 * (1 + fr.max() - fr.min()) + fpb / 2)
+    want = np.outer(b[:, 0] - b[0, 0], vel)
+    assert np.abs(b[:, 1:] - want).max() < 6.0
+    # per localization: the spline of the bin drifts at its frame, relative to bin 0's centre
+    assert np.abs(l - (dt - np.outer(np.full(len(fr), b[0, 0]), vel))).max() < 7.0
+
+
+def test_drift_restatement_handles_flat_z():
+    xyz, fr, cr, dt, vel = drift_data(seed=1, vel=(0.02, 0.01, 0.0))
+    xyz[:, 2] = 0.0
+    b, l, px = O.drift(xyz, fr, cr, pixel_nm=20.0, bins=4, max_drift_um=0.16)
+    assert np.all(b[:, 3] == 0.0)
+    assert np.abs(b[:, 1:3] - np.outer(b[:, 0] - b[0, 0], vel[:2])).max() < 6.0

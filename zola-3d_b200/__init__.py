@@ -70,7 +70,7 @@ EXPORTS = ["zola_ctx_create", "zola_ctx_destroy", "zola_last_error", "zola_ctx_s
            "zola_detector_create", "zola_detector_free", "zola_detector_info", "zola_detect", "zola_detect_dev",
            "zola_localize_frames", "zola_write_csv", "zola_format_double_java", "zola_calib_forward",
            "zola_calib_backward", "zola_calib_fit", "zola_ctx_set_split_mode", "zola_crlb_curve",
-           "zola_psf_center_search", "zola_calib_init"]
+           "zola_psf_center_search", "zola_calib_init", "zola_drift"]
 STAGES = ["split_stage1_pupil_dft", "split_stage2_window_dft", "split_stage3_blur_rows", "split_stage4_blur_cols",
           "split_stage5_likelihood_lm", "fp64_fit", "fp64_model", "other"]
 
@@ -112,6 +112,7 @@ def lib():
         L.zola_calib_backward.argtypes = [vp, ctypes.POINTER(CalibData), vp, d, vp, vp, vp, vp, vp]
         L.zola_calib_fit.argtypes = [vp, ctypes.POINTER(CalibData), vp, vp, vp, i, i, vp, vp]
         L.zola_calib_init.argtypes = [vp, vp, i, i, i, vp, vp, i, i, d, d, d, d, vp, vp, vp, vp]
+        L.zola_drift.argtypes = [vp, vp, vp, vp, i, ctypes.POINTER(DriftParams), vp, vp, ctypes.POINTER(d)]
         L.zola_format_double_java.argtypes = [d, ctypes.c_char_p, i]
         L.zola_detector_free.argtypes = [vp]
         L.zola_detector_info.argtypes = [vp, ctypes.POINTER(i), vp, vp]
@@ -327,6 +328,26 @@ class Detector:
         if getattr(self, "h", None) and getattr(self.psf, "h", None):
             lib().zola_detector_free(self.h)
         self.h = None
+
+
+class DriftParams(ctypes.Structure):
+    _fields_ = [("pixel_nm", ctypes.c_double), ("bins", ctypes.c_int), ("max_drift_um", ctypes.c_double)]
+
+
+def drift(ctx, xyz_nm, frame, crlb_nm=None, pixel_nm=10.0, bins=20, max_drift_um=0.5):
+    """DriftCorrection: returns (bin_drift (bins, 4) = frame index, dx, dy, dz nm,
+    per-localization drift (n, 3) nm, voxel size used)."""
+    xyz = np.ascontiguousarray(xyz_nm, dtype=np.float64)
+    fr = np.ascontiguousarray(frame, dtype=np.int32)
+    cr = None if crlb_nm is None else np.ascontiguousarray(crlb_nm, dtype=np.float64)
+    n = len(fr)
+    out_b = np.zeros((int(bins), 4))
+    out_l = np.zeros((n, 3))
+    px = ctypes.c_double()
+    prm = DriftParams(float(pixel_nm), int(bins), float(max_drift_um))
+    ctx.check(lib().zola_drift(ctx.h, _ptr(xyz), _ptr(cr), _ptr(fr), n, ctypes.byref(prm), _ptr(out_b), _ptr(out_l),
+                               ctypes.byref(px)), "zola_drift")
+    return out_b, out_l, px.value
 
 
 class CalibData(ctypes.Structure):
