@@ -132,6 +132,17 @@ ZOLA_API int zola_fit_batch_dev(zola_ctx* ctx, zola_psf* psf, int R, const float
                        int n, const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll,
                        int* d_status, int* d_iters, void* stream);
 
+/* sCMOS form (process/cpu/Localization.java:1132, utils/SCMOScamera.java):
+ * scmos holds, per ROI pixel, var/gain^2 of the camera pixel; it is added to
+ * the model mean (mu = A psi + B + scmos), and rois are then
+ * (ADU - offset)/gain + var/gain^2 as the reference converts them. */
+ZOLA_API int zola_fit_batch_scmos(zola_ctx* ctx, zola_psf* psf, int R, const float* rois, const float* scmos,
+                                  const double* init5, int n, const zola_fit_params* prm, double* out5, double* crlb5,
+                                  double* nll, int* status, int* iters);
+ZOLA_API int zola_fit_batch_scmos_dev(zola_ctx* ctx, zola_psf* psf, int R, const float* d_rois, const float* d_scmos,
+                                      const double* d_init5, int n, const zola_fit_params* prm, double* d_out5,
+                                      double* d_crlb5, double* d_nll, int* d_status, int* d_iters, void* stream);
+
 /* --- detection (replaces Predetection / Predetection_cross_: library build,
  * setImage and convolveNormalizedInFourierDomain; process/cpu/Predetection.java:63-593,
  * process/gpu/Predetection_cross_.java:104-785).  psf must be built with
@@ -188,6 +199,17 @@ typedef struct {
 ZOLA_API int zola_localize_frames(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const double* frames,
                                   int nframes, int frame0, const zola_loc_params* prm, zola_localization* out,
                                   int out_cap, int* nout);
+
+/* sCMOS form of the pipeline (LocalizationPipeline.java:588-640, 799-820,
+ * utils/SCMOScamera.java): adu frames (float, nframes x SX x SY) and per-pixel
+ * offset, gain and variance maps (SX x SY).  Detection runs on
+ * (adu - offset)/gain + vargain[0] clamped at 0, fits on (adu - offset)/gain +
+ * vargain with vargain = variance / gain^2 added to the model mean; getAandB
+ * works on patch - vargain. */
+ZOLA_API int zola_localize_frames_scmos(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const float* adu,
+                                        int nframes, int frame0, const zola_loc_params* prm, const double* offset,
+                                        const double* gain, const double* variance, zola_localization* out,
+                                        int out_cap, int* nout);
 
 /* ThunderStorm-style CSV writer (data/PLocalization.java:224-306,
  * data/StackLocalization.java:1332-1360): header id,frame,x [nm],...,

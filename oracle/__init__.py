@@ -47,6 +47,7 @@ def lib():
         L.orc_psf_model_oil.argtypes = [vp, i, d, d, d, d, vp]
         L.orc_localize_cd.argtypes = [vp, i, i, vp, vp, d, d, i, d, vp, vp, vp, vp, i]
         L.orc_fit_lm.argtypes = [vp, i, i, vp, vp, vp, i, vp, vp, vp, vp, vp, i]
+        L.orc_fit_lm_scmos.argtypes = [vp, i, i, vp, vp, vp, vp, i, vp, vp, vp, vp, vp, i]
         L.orc_nll_grad.restype = d
         L.orc_nll_grad.argtypes = [vp, i, vp, vp, vp, vp]
         L.orc_crlb_fd.argtypes = [vp, i, vp, vp]
@@ -61,6 +62,8 @@ def lib():
         L.orc_detect.argtypes = [vp, i, vp, i, vp, vp, i]
         L.orc_localize_frames.restype = i
         L.orc_localize_frames.argtypes = [vp, vp, i, vp, d, d, d, d, i, vp, i]
+        L.orc_localize_frames_scmos.restype = i
+        L.orc_localize_frames_scmos.argtypes = [vp, vp, i, vp, vp, vp, vp, d, d, d, d, i, vp, i]
         L.orc_calib_nll.restype = d
         L.orc_calib_nll.argtypes = [vp, i, i, vp, vp, d, d, d, d, d]
         L.orc_calib_nll_full.restype = d
@@ -145,6 +148,20 @@ class OraclePSF:
                          _p(ev), _p(cr) if crlb else None, threads)
         return (out, nll, st, ev, cr) if crlb else (out, nll, st, ev)
 
+    def fit_lm_scmos(self, patches, scmos, init_xyzab, zmin, zmax, xymax, tol_xyz=1e-5, step_xy=0.11, step_z=0.22,
+                     max_iter=30, threads=1):
+        """lm_fit with the sCMOS term var/gain^2 (n, R, R) added to the model mean."""
+        patches, scmos, init = _f64(patches), _f64(scmos), _f64(init_xyzab)
+        n, R = patches.shape[0], patches.shape[1]
+        prm = _f64([zmin, zmax, xymax, tol_xyz, step_xy, step_z])
+        out = np.zeros((n, 5))
+        nll = np.zeros(n)
+        st = np.zeros(n, np.int32)
+        ev = np.zeros(n, np.int32)
+        lib().orc_fit_lm_scmos(self.h, R, n, _p(patches), _p(scmos), _p(init), _p(prm), max_iter, _p(out), _p(nll),
+                               _p(st), _p(ev), None, threads)
+        return out, nll, st, ev
+
     def nll_grad(self, patch, theta):
         patch = _f64(patch)
         th = _f64(theta)
@@ -214,6 +231,15 @@ class OracleDetector:
         rows = np.zeros((cap, 10))
         n = lib().orc_localize_frames(self.h, fit_psf.h, frames.shape[0], _p(frames), minZ, maxZ, photon_thr, max_snr,
                                       cap, _p(rows), threads)
+        return rows[:min(n, cap)]
+
+    def localize_frames_scmos(self, fit_psf, adu, offset, gain, variance, minZ, maxZ, photon_thr=500.0, max_snr=1.0,
+                              threads=1, cap=100000):
+        """sCMOS pipeline: ADU frames and per-pixel offset / gain / variance maps."""
+        adu, off, gn, var = _f64(adu), _f64(offset), _f64(gain), _f64(variance)
+        rows = np.zeros((cap, 10))
+        n = lib().orc_localize_frames_scmos(self.h, fit_psf.h, adu.shape[0], _p(adu), _p(off), _p(gn), _p(var), minZ,
+                                            maxZ, photon_thr, max_snr, cap, _p(rows), threads)
         return rows[:min(n, cap)]
 
     def detect(self, frames, cap=4096, threads=1):

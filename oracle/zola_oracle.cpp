@@ -298,6 +298,7 @@ struct CD {
     const Psf* p;
     int R;
     const double* d;   // patch R*R (photons), [x][y]
+    const double* v = nullptr;  // sCMOS var/gain^2 patch (Localization.java:1132), or none
     double minZ, maxZ;
     int iterMax;
     double photonThreshold;
@@ -311,7 +312,7 @@ struct CD {
         ++nevals;
         double l = 0;
         for (int k = 0; k < R * R; ++k) {
-            double m = psi[k] * a + b;
+            double m = psi[k] * a + b + (v ? v[k] : 0.0);
             mu[k] = m;
             l += m - d[k] * std::log(m);
         }
@@ -543,14 +544,16 @@ struct LMParams {
 
 // Deviance-form Poisson NLL: sum mu - d - d ln(mu/d) (mu - d ln mu + const).
 // Returns +inf if any mu <= 0.
+// v (nullable): the sCMOS term var/gain^2 added to the model mean
+// (process/cpu/Localization.java:1132).
 double model_eval(const Psf* p, int R, const double* d, const double* th, double* g, double H[5][5],
-                  std::vector<double>& psi, std::vector<double>& dpsi) {
+                  std::vector<double>& psi, std::vector<double>& dpsi, const double* v = nullptr) {
     int n = R * R;
     psf_model(p, R, th[0], th[1], p->zfocus, th[2], psi.data(), dpsi.data());
     double nll = 0;
     for (int q = 0; q < 5; ++q) { g[q] = 0; for (int r = 0; r < 5; ++r) H[q][r] = 0; }
     for (int k = 0; k < n; ++k) {
-        double mu = th[3] * psi[k] + th[4];
+        double mu = th[3] * psi[k] + th[4] + (v ? v[k] : 0.0);
         if (!(mu > 0)) return INFINITY;
         double dk = d[k];
         nll += dk > 0 ? mu - dk - dk * std::log(mu / dk) : mu;
@@ -604,13 +607,13 @@ void clamp_theta(double* th, const LMParams& P) {
 
 // status: 1 converged, 2 max evaluations, 3 stalled (lambda at bound), -1 NaN.
 int lm_fit(const Psf* p, int R, const double* d, const double* init, const LMParams& P,
-           double* out, double* nll_out, int* evals_out, double* crlb5) {
+           double* out, double* nll_out, int* evals_out, double* crlb5, const double* v = nullptr) {
     int n = R * R;
     std::vector<double> psi(n), dpsi(3 * n), psi2(n), dpsi2(3 * n);
     double th[5], g[5], H[5][5];
     for (int q = 0; q < 5; ++q) th[q] = init[q];
     clamp_theta(th, P);
-    double nll = model_eval(p, R, d, th, g, H, psi, dpsi);
+    double nll = model_eval(p, R, d, th, g, H, psi, dpsi, v);
     int evals = 1;
     double lambda = 1e-3;
     int status = 2;
@@ -639,7 +642,7 @@ int lm_fit(const Psf* p, int R, const double* d, const double* init, const LMPar
         double t2[5], g2[5], H2[5][5];
         for (int q = 0; q < 5; ++q) t2[q] = th[q] + scale * delta[q];
         clamp_theta(t2, P);
-        double nll2 = model_eval(p, R, d, t2, g2, H2, psi2, dpsi2);
+        double nll2 = model_eval(p, R, d, t2, g2, H2, psi2, dpsi2, v);
         ++evals;
         if (nll2 <= nll) {
             for (int q = 0; q < 5; ++q) { th[q] = t2[q]; g[q] = g2[q]; for (int r = 0; r < 5; ++r) H[q][r] = H2[q][r]; }
@@ -655,10 +658,10 @@ int lm_fit(const Psf* p, int R, const double* d, const double* init, const LMPar
     *nll_out = nll;
     *evals_out = evals;
     if (crlb5) {  // sqrt(diag(F^-1)) from the analytic Fisher matrix at the optimum
-        model_eval(p, R, d, th, g, H, psi, dpsi);
+        model_eval(p, R, d, th, g, H, psi, dpsi, v);
         double F[5][5] = {};
         for (int k = 0; k < n; ++k) {
-            double mu = th[3] * psi[k] + th[4];
+            double mu = th[3] * psi[k] + th[4] + (v ? v[k] : 0.0);
             double j[5] = {th[3] * dpsi[k], th[3] * dpsi[n + k], th[3] * dpsi[2 * n + k], psi[k], 1.0};
             for (int q = 0; q < 5; ++q) for (int r = 0; r < 5; ++r) F[q][r] += j[q] * j[r] / mu;
         }
@@ -932,6 +935,18 @@ void orc_fit_lm(void* h, int R, int n, const double* patches, const double* init
     });
 }
 
+// The same fits with a per-ROI sCMOS term (n x R x R, added to the mean).
+void orc_fit_lm_scmos(void* h, int R, int n, const double* patches, const double* scmos, const double* init,
+                      const double* params, int max_iter, double* out, double* nll, int* status, int* evals,
+                      double* crlb5, int threads) {
+    const Psf* p = (const Psf*)h;
+    LMParams P{params[0], params[1], params[2], max_iter, params[3], params[4], params[5]};
+    parallel_for(n, threads, [&](int i) {
+        status[i] = lm_fit(p, R, patches + (size_t)i * R * R, init + 5 * i, P, out + 5 * i, nll + i, evals + i,
+                           crlb5 ? crlb5 + 5 * i : nullptr, scmos + (size_t)i * R * R);
+    });
+}
+
 // Deviance-form NLL and its analytic gradient / Gauss-Newton Hessian at theta.
 double orc_nll_grad(void* h, int R, const double* patch, const double* th, double* g, double* H25) {
     const Psf* p = (const Psf*)h;
@@ -988,18 +1003,25 @@ void orc_detect(void* d, int nframes, const double* frames, int cap, double* out
 // maxZ+0.3) and finite-difference CRLB.  det uses the resetKz library PSF,
 // psf the fit PSF.  Rows: frame, x_nm, y_nm, z_nm, A, B, chi2, crlbx, crlby,
 // crlbz (nm), in processing order per frame.
-int orc_localize_frames(void* dh, void* ph, int nframes, const double* frames, double minZ, double maxZ,
-                        double photonThr, double maxSNR, int rows_cap, double* rows, int threads) {
-    Detector* D = (Detector*)dh;
-    const Psf* p = (const Psf*)ph;
+}  // extern "C"
+
+namespace {
+
+// LocalizationPipeline frame loop.  det_frames feed the detection, fit_frames
+// the patches; vmap (SX x SY, nullable) is the sCMOS var/gain^2 map: getAandB
+// then uses patch - v (:1168-1211), the fit and the model add v, and the
+// Fisher matrix leaves it out (Localization.java:317-451).
+int localize_frames_impl(Detector* D, const Psf* p, int nframes, const double* det_frames, const double* fit_frames,
+                         const double* vmap, double minZ, double maxZ, double photonThr, double maxSNR, int rows_cap,
+                         double* rows, int threads) {
     const int SX = D->SX, SY = D->SY, R = D->R, h = R / 2;
     std::vector<std::vector<std::array<double, 10>>> per(nframes);
     parallel_for(nframes, threads, [&](int f) {
-        const double* img = frames + (size_t)f * SX * SY;
+        const double* img = fit_frames + (size_t)f * SX * SY;
         std::vector<std::array<double, 7>> v;
-        det_frame(D, img, v);
+        det_frame(D, det_frames + (size_t)f * SX * SY, v);
         std::vector<char> mask((size_t)SX * SY, 0);
-        std::vector<double> patch((size_t)R * R), psi((size_t)R * R);
+        std::vector<double> patch((size_t)R * R), psi((size_t)R * R), sv((size_t)R * R, 0.0);
         int pointer = 0;
         while (true) {
             int sel = -1;
@@ -1015,21 +1037,22 @@ int orc_localize_frames(void* dh, void* ph, int nframes, const double* frames, d
                 for (int b = 0; b < R; ++b) {
                     if (mask[(size_t)(ci - h + a) * SY + (cj - h + b)]) { treated = true; break; }
                     patch[(size_t)a * R + b] = img[(size_t)(ci - h + a) * SY + (cj - h + b)];
+                    if (vmap) sv[(size_t)a * R + b] = vmap[(size_t)(ci - h + a) * SY + (cj - h + b)];
                 }
             if (treated) continue;
             const std::vector<double>& lp = D->libpsf[r];  // getAandB (LocalizationPipeline.java:1119-1162)
             double maxp = -INFINITY, maxi = -INFINITY;
-            for (int k = 0; k < R * R; ++k) { maxi = std::max(maxi, lp[k]); maxp = std::max(maxp, patch[k]); }
+            for (int k = 0; k < R * R; ++k) { maxi = std::max(maxi, lp[k]); maxp = std::max(maxp, patch[k] - sv[k]); }
             double thr = maxi * 0.1, A = 0, B = 0, ca = 0, cb = 0;
             for (int k = 0; k < R * R; ++k) {
-                if (lp[k] < thr) { B += patch[k]; cb++; } else { A += patch[k]; ca++; }
+                if (lp[k] < thr) { B += patch[k] - sv[k]; cb++; } else { A += patch[k] - sv[k]; ca++; }
             }
             B = cb != 0 ? B / cb : 0;
             A -= ca * B;
             bool part = false;
             if (maxp / B > maxSNR && B > 0) {
                 CD cd;
-                cd.p = p; cd.R = R; cd.d = patch.data();
+                cd.p = p; cd.R = R; cd.d = patch.data(); cd.v = vmap ? sv.data() : nullptr;
                 cd.minZ = minZ - .3; cd.maxZ = maxZ + .3; cd.iterMax = 20; cd.photonThreshold = photonThr;
                 cd.maxShift = p->dx / 2.;
                 cd.psi.resize(R * R); cd.mu.resize(R * R);
@@ -1038,14 +1061,14 @@ int orc_localize_frames(void* dh, void* ph, int nframes, const double* frames, d
                 if (st == 1) {
                     psf_model(p, R, cd.tx, cd.ty, p->zfocus, cd.tz, psi.data(), nullptr);
                     double mthr = 0;
-                    for (int k = 0; k < R * R; ++k) mthr = std::max(mthr, psi[k] * cd.ta + cd.tb - cd.tb);
+                    for (int k = 0; k < R * R; ++k) mthr = std::max(mthr, psi[k] * cd.ta + cd.tb + sv[k] - cd.tb);
                     mthr *= .2;
                     if (cd.ta > photonThr && std::fabs(cd.tx) < 10 * p->dx && std::fabs(cd.ty) < 10 * p->dx) {
                         int px = (int)(ci - (cd.tx / p->dx)), py = (int)(cj - (cd.ty / p->dx));
                         if (px >= 0 && px < SX && py >= 0 && py < SY && !mask[(size_t)px * SY + py] && cd.tz > minZ && cd.tz < maxZ) {
                             double chi = 0;
                             for (int k = 0; k < R * R; ++k) {
-                                double mu = psi[k] * cd.ta + cd.tb;
+                                double mu = psi[k] * cd.ta + cd.tb + sv[k];
                                 chi += (patch[k] - mu) * (patch[k] - mu) / mu;
                             }
                             chi /= (double)(R * R);
@@ -1055,7 +1078,8 @@ int orc_localize_frames(void* dh, void* ph, int nframes, const double* frames, d
                                               cd.ta, cd.tb, chi, 1000 * cr[0], 1000 * cr[1], 1000 * cr[2]});
                             for (int a = 0; a < R; ++a)
                                 for (int b = 0; b < R; ++b)
-                                    if (psi[(size_t)a * R + b] * cd.ta + cd.tb - cd.tb > mthr) mask[(size_t)(ci - h + a) * SY + (cj - h + b)] = 1;
+                                    if (psi[(size_t)a * R + b] * cd.ta + cd.tb + sv[(size_t)a * R + b] - cd.tb > mthr)
+                                        mask[(size_t)(ci - h + a) * SY + (cj - h + b)] = 1;
                             part = true;
                         }
                     }
@@ -1075,6 +1099,37 @@ int orc_localize_frames(void* dh, void* ph, int nframes, const double* frames, d
             ++n;
         }
     return n;
+}
+
+}  // namespace
+
+extern "C" {
+
+int orc_localize_frames(void* dh, void* ph, int nframes, const double* frames, double minZ, double maxZ,
+                        double photonThr, double maxSNR, int rows_cap, double* rows, int threads) {
+    return localize_frames_impl((Detector*)dh, (const Psf*)ph, nframes, frames, frames, nullptr, minZ, maxZ,
+                                photonThr, maxSNR, rows_cap, rows, threads);
+}
+
+// sCMOS form (LocalizationPipeline.java:588-640): detection on
+// (ADU - offset)/gain + vargain[0][0] clamped at 0, fits on
+// (ADU - offset)/gain + vargain, vargain = variance / gain^2.
+int orc_localize_frames_scmos(void* dh, void* ph, int nframes, const double* adu, const double* offset,
+                              const double* gain, const double* variance, double minZ, double maxZ, double photonThr,
+                              double maxSNR, int rows_cap, double* rows, int threads) {
+    Detector* D = (Detector*)dh;
+    const size_t SS = (size_t)D->SX * D->SY;
+    std::vector<double> vg(SS), det(SS * nframes), fit(SS * nframes);
+    for (size_t k = 0; k < SS; ++k) vg[k] = variance[k] / (gain[k] * gain[k]);
+    for (int f = 0; f < nframes; ++f)
+        for (size_t k = 0; k < SS; ++k) {
+            const double c = (adu[(size_t)f * SS + k] - offset[k]) / gain[k];
+            double dv = c + vg[0];
+            det[(size_t)f * SS + k] = dv < 0 ? 0 : dv;
+            fit[(size_t)f * SS + k] = c + vg[k];
+        }
+    return localize_frames_impl(D, (const Psf*)ph, nframes, det.data(), fit.data(), vg.data(), minZ, maxZ, photonThr,
+                                maxSNR, rows_cap, rows, threads);
 }
 
 // Calibration stack NLL (ZernikePhaseRetrieval.java:1843-1874) for one bead:

@@ -70,7 +70,8 @@ EXPORTS = ["zola_ctx_create", "zola_ctx_destroy", "zola_last_error", "zola_ctx_s
            "zola_detector_create", "zola_detector_free", "zola_detector_info", "zola_detect", "zola_detect_dev",
            "zola_localize_frames", "zola_write_csv", "zola_format_double_java", "zola_calib_forward",
            "zola_calib_backward", "zola_calib_fit", "zola_ctx_set_split_mode", "zola_crlb_curve",
-           "zola_psf_center_search", "zola_calib_init", "zola_drift"]
+           "zola_psf_center_search", "zola_calib_init", "zola_drift", "zola_fit_batch_scmos",
+           "zola_fit_batch_scmos_dev", "zola_localize_frames_scmos"]
 STAGES = ["split_stage1_pupil_dft", "split_stage2_window_dft", "split_stage3_blur_rows", "split_stage4_blur_cols",
           "split_stage5_likelihood_lm", "fp64_fit", "fp64_model", "other"]
 
@@ -112,6 +113,11 @@ def lib():
         L.zola_calib_backward.argtypes = [vp, ctypes.POINTER(CalibData), vp, d, vp, vp, vp, vp, vp]
         L.zola_calib_fit.argtypes = [vp, ctypes.POINTER(CalibData), vp, vp, vp, i, i, vp, vp]
         L.zola_calib_init.argtypes = [vp, vp, i, i, i, vp, vp, i, i, d, d, d, d, vp, vp, vp, vp]
+        L.zola_fit_batch_scmos.argtypes = [vp, vp, i, vp, vp, vp, i, ctypes.POINTER(FitParams), vp, vp, vp, vp, vp]
+        L.zola_fit_batch_scmos_dev.argtypes = [vp, vp, i, vp, vp, vp, i, ctypes.POINTER(FitParams), vp, vp, vp, vp,
+                                               vp, vp]
+        L.zola_localize_frames_scmos.argtypes = [vp, vp, vp, vp, i, i, ctypes.POINTER(LocParams), vp, vp, vp, vp, i,
+                                                 ctypes.POINTER(i)]
         L.zola_drift.argtypes = [vp, vp, vp, vp, i, ctypes.POINTER(DriftParams), vp, vp, ctypes.POINTER(d)]
         L.zola_format_double_java.argtypes = [d, ctypes.c_char_p, i]
         L.zola_detector_free.argtypes = [vp]
@@ -252,8 +258,9 @@ class PSF:
         return FitParams(float(zmin), float(zmax), float(xymax), int(max_iter), float(tol_xyz), float(step_xy),
                          float(step_z), int(precision))
 
-    def fit(self, rois, init, prm, crlb=True):
-        """Batched MLE fit of host ROIs (n, R, R) photons from init (n, 5) = x, y, z, A, B."""
+    def fit(self, rois, init, prm, crlb=True, scmos=None):
+        """Batched MLE fit of host ROIs (n, R, R) photons from init (n, 5) = x, y, z, A, B.
+        scmos (n, R, R), optional: var/gain^2 of each ROI pixel, added to the model mean."""
         rois = np.ascontiguousarray(rois, dtype=np.float32)
         init = np.ascontiguousarray(init, dtype=np.float64)
         n, R = rois.shape[0], rois.shape[1]
@@ -262,8 +269,14 @@ class PSF:
         nll = np.zeros(n)
         st = np.zeros(n, np.int32)
         it = np.zeros(n, np.int32)
-        self.ctx.check(lib().zola_fit_batch(self.ctx.h, self.h, R, _ptr(rois), _ptr(init), n, ctypes.byref(prm),
-                                            _ptr(out), _ptr(cr), _ptr(nll), _ptr(st), _ptr(it)), "zola_fit_batch")
+        if scmos is None:
+            self.ctx.check(lib().zola_fit_batch(self.ctx.h, self.h, R, _ptr(rois), _ptr(init), n, ctypes.byref(prm),
+                                                _ptr(out), _ptr(cr), _ptr(nll), _ptr(st), _ptr(it)), "zola_fit_batch")
+        else:
+            v = np.ascontiguousarray(scmos, dtype=np.float32)
+            self.ctx.check(lib().zola_fit_batch_scmos(self.ctx.h, self.h, R, _ptr(rois), _ptr(v), _ptr(init), n,
+                                                      ctypes.byref(prm), _ptr(out), _ptr(cr), _ptr(nll), _ptr(st),
+                                                      _ptr(it)), "zola_fit_batch_scmos")
         return dict(theta=out, crlb=cr, nll=nll, status=st, iters=it)
 
     def fit_dev(self, rois, init, prm, out, crlb=None, nll=None, status=None, iters=None, stream=None):
@@ -463,6 +476,28 @@ def localize_frames(ctx, det, fit_psf, frames, minZ, maxZ, photon_threshold=500.
     ctx.check(lib().zola_localize_frames(ctx.h, det.h, fit_psf.h, _ptr(frames), nf, int(frame0), ctypes.byref(prm),
                                          ctypes.cast(out, ctypes.c_void_p), cap, ctypes.byref(n)),
               "zola_localize_frames")
+    dt = np.dtype([(c, np.int32 if c in ("id", "frame") else np.float64) for c in LOC_COLUMNS])
+    arr = np.zeros(n.value, dtype=dt)
+    for k in range(n.value):
+        arr[k] = tuple(getattr(out[k], c) for c in LOC_COLUMNS)
+    return arr
+
+def localize_frames_scmos(ctx, det, fit_psf, adu, offset, gain, variance, minZ, maxZ, photon_threshold=500.0,
+                          max_snr=1.0, max_iter=30, tol_xyz=1e-4, precision=ZOLA_PREC_FP64, frame0=0, cand_cap=1024,
+                          frames_per_batch=1024, wave_fits=0):
+    """sCMOS pipeline: ADU frames (n, SX, SY) and offset / gain / variance maps (SX, SY)."""
+    adu = np.ascontiguousarray(adu, dtype=np.float32)
+    maps = [np.ascontiguousarray(m, dtype=np.float64) for m in (offset, gain, variance)]
+    nf = adu.shape[0]
+    prm = LocParams(det.R, float(minZ), float(maxZ), float(photon_threshold), float(max_snr), int(max_iter),
+                    float(tol_xyz), int(precision), int(cand_cap), int(frames_per_batch), int(wave_fits))
+    cap = max(64, nf * 64)
+    out = (Localization * cap)()
+    n = ctypes.c_int()
+    ctx.check(lib().zola_localize_frames_scmos(ctx.h, det.h, fit_psf.h, _ptr(adu), nf, int(frame0), ctypes.byref(prm),
+                                               _ptr(maps[0]), _ptr(maps[1]), _ptr(maps[2]),
+                                               ctypes.cast(out, ctypes.c_void_p), cap, ctypes.byref(n)),
+              "zola_localize_frames_scmos")
     dt = np.dtype([(c, np.int32 if c in ("id", "frame") else np.float64) for c in LOC_COLUMNS])
     arr = np.zeros(n.value, dtype=dt)
     for k in range(n.value):

@@ -278,9 +278,13 @@ int zola_ctx_set_split_mode(zola_ctx* ctx, int mode) {
     return ZOLA_OK;
 }
 
-int zola_fit_batch_dev(zola_ctx* ctx, zola_psf* psf, int R, const float* d_rois, const double* d_init5, int n,
-                       const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll, int* d_status,
-                       int* d_iters, void* stream) {
+}  // extern "C"
+
+namespace {
+
+int fit_dev_impl(zola_ctx* ctx, zola_psf* psf, int R, const float* d_rois, const float* d_scmos,
+                 const double* d_init5, int n, const zola_fit_params* prm, double* d_out5, double* d_crlb5,
+                 double* d_nll, int* d_status, int* d_iters, void* stream) {
     if (!ctx || !psf) return ZOLA_E_ARG;
     if (psf->ctx != ctx) return set_err(ctx, ZOLA_E_ARG, "psf belongs to another context");
     if (!check_fit_params(ctx, prm)) return ZOLA_E_ARG;
@@ -291,23 +295,26 @@ int zola_fit_batch_dev(zola_ctx* ctx, zola_psf* psf, int R, const float* d_rois,
     if (n == 0) return ZOLA_OK;
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
     if (prm->precision == ZOLA_PREC_SPLIT)
-        return launch_fit_split(ctx, psf, w, d_rois, d_init5, n, prm, d_out5, d_crlb5, d_nll, d_status, d_iters, st);
-    return launch_fit_f64(ctx, psf, w, d_rois, d_init5, n, prm, d_out5, d_crlb5, d_nll, d_status, d_iters, st);
+        return launch_fit_split(ctx, psf, w, d_rois, d_scmos, d_init5, n, prm, d_out5, d_crlb5, d_nll, d_status, d_iters,
+                                st);
+    return launch_fit_f64(ctx, psf, w, d_rois, d_scmos, d_init5, n, prm, d_out5, d_crlb5, d_nll, d_status, d_iters, st);
 }
 
-int zola_fit_batch(zola_ctx* ctx, zola_psf* psf, int R, const float* rois, const double* init5, int n,
-                   const zola_fit_params* prm, double* out5, double* crlb5, double* nll, int* status, int* iters) {
+int fit_host_impl(zola_ctx* ctx, zola_psf* psf, int R, const float* rois, const float* scmos, const double* init5,
+                  int n, const zola_fit_params* prm, double* out5, double* crlb5, double* nll, int* status,
+                  int* iters) {
     if (!ctx || !psf) return ZOLA_E_ARG;
     if (n < 0 || (n > 0 && (!rois || !init5 || !out5))) return set_err(ctx, ZOLA_E_ARG, "zola_fit_batch: bad n or null buffer");
     if (n == 0) return ZOLA_OK;
     cudaSetDevice(ctx->device);
     const size_t rr = (size_t)R * R, nn = (size_t)n;
     auto al = [](size_t b) { return (b + 255) / 256 * 256; };
-    // staging layout: rois | init | out | crlb | nll | status | iters
+    // staging layout: rois | init | out | crlb | nll | status | iters | scmos
     const size_t off_i = al(rr * nn * sizeof(float)), off_o = off_i + al(5 * nn * sizeof(double));
     const size_t off_c = off_o + al(5 * nn * sizeof(double)), off_n = off_c + al(5 * nn * sizeof(double));
     const size_t off_s = off_n + al(nn * sizeof(double)), off_t = off_s + al(nn * sizeof(int));
-    const size_t total = off_t + al(nn * sizeof(int));
+    const size_t off_v = off_t + al(nn * sizeof(int));
+    const size_t total = off_v + (scmos ? al(rr * nn * sizeof(float)) : 0);
     if (ensure_io(ctx, total)) return ZOLA_E_CUDA;
     char* base = (char*)ctx->io;
     float* dr = (float*)base;
@@ -317,9 +324,11 @@ int zola_fit_batch(zola_ctx* ctx, zola_psf* psf, int R, const float* rois, const
     double* dnll = nll ? (double*)(base + off_n) : nullptr;
     int* dst = status ? (int*)(base + off_s) : nullptr;
     int* dit = iters ? (int*)(base + off_t) : nullptr;
+    float* dv = scmos ? (float*)(base + off_v) : nullptr;
     ZOLA_CUDA_CHECK(cudaMemcpyAsync(dr, rois, rr * nn * sizeof(float), cudaMemcpyHostToDevice, ctx->stream), ctx);
     ZOLA_CUDA_CHECK(cudaMemcpyAsync(di, init5, 5 * nn * sizeof(double), cudaMemcpyHostToDevice, ctx->stream), ctx);
-    int rc = zola_fit_batch_dev(ctx, psf, R, dr, di, n, prm, dout, dcr, dnll, dst, dit, ctx->stream);
+    if (scmos) ZOLA_CUDA_CHECK(cudaMemcpyAsync(dv, scmos, rr * nn * sizeof(float), cudaMemcpyHostToDevice, ctx->stream), ctx);
+    int rc = fit_dev_impl(ctx, psf, R, dr, dv, di, n, prm, dout, dcr, dnll, dst, dit, ctx->stream);
     if (rc) return rc;
     ZOLA_CUDA_CHECK(cudaMemcpyAsync(out5, dout, 5 * nn * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), ctx);
     if (crlb5) ZOLA_CUDA_CHECK(cudaMemcpyAsync(crlb5, dcr, 5 * nn * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), ctx);
@@ -328,6 +337,36 @@ int zola_fit_batch(zola_ctx* ctx, zola_psf* psf, int R, const float* rois, const
     if (iters) ZOLA_CUDA_CHECK(cudaMemcpyAsync(iters, dit, nn * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), ctx);
     ZOLA_CUDA_CHECK(cudaStreamSynchronize(ctx->stream), ctx);
     return ZOLA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int zola_fit_batch_dev(zola_ctx* ctx, zola_psf* psf, int R, const float* d_rois, const double* d_init5, int n,
+                       const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll, int* d_status,
+                       int* d_iters, void* stream) {
+    return fit_dev_impl(ctx, psf, R, d_rois, nullptr, d_init5, n, prm, d_out5, d_crlb5, d_nll, d_status, d_iters, stream);
+}
+
+int zola_fit_batch(zola_ctx* ctx, zola_psf* psf, int R, const float* rois, const double* init5, int n,
+                   const zola_fit_params* prm, double* out5, double* crlb5, double* nll, int* status, int* iters) {
+    return fit_host_impl(ctx, psf, R, rois, nullptr, init5, n, prm, out5, crlb5, nll, status, iters);
+}
+
+int zola_fit_batch_scmos_dev(zola_ctx* ctx, zola_psf* psf, int R, const float* d_rois, const float* d_scmos,
+                             const double* d_init5, int n, const zola_fit_params* prm, double* d_out5, double* d_crlb5,
+                             double* d_nll, int* d_status, int* d_iters, void* stream) {
+    if (ctx && n > 0 && !d_scmos) return set_err(ctx, ZOLA_E_ARG, "zola_fit_batch_scmos: null sCMOS map");
+    return fit_dev_impl(ctx, psf, R, d_rois, d_scmos, d_init5, n, prm, d_out5, d_crlb5, d_nll, d_status, d_iters,
+                        stream);
+}
+
+int zola_fit_batch_scmos(zola_ctx* ctx, zola_psf* psf, int R, const float* rois, const float* scmos,
+                         const double* init5, int n, const zola_fit_params* prm, double* out5, double* crlb5,
+                         double* nll, int* status, int* iters) {
+    if (ctx && n > 0 && !scmos) return set_err(ctx, ZOLA_E_ARG, "zola_fit_batch_scmos: null sCMOS map");
+    return fit_host_impl(ctx, psf, R, rois, scmos, init5, n, prm, out5, crlb5, nll, status, iters);
 }
 
 }  // extern "C"

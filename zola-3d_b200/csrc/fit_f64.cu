@@ -235,7 +235,9 @@ __global__ void __launch_bounds__(F64_THREADS) model_f64_kernel(PsfView P, WinVi
 }
 
 // Likelihood, gradient, Gauss-Newton Hessian and Fisher matrix at theta.
-__device__ void eval_lik_f64(const PsfView& P, const WinView& Wn, const F64Work& w, const float* d,
+// sv (nullable): the ROI's sCMOS term var/gain^2, added to the mean
+// (process/cpu/Localization.java:1132).
+__device__ void eval_lik_f64(const PsfView& P, const WinView& Wn, const F64Work& w, const float* d, const float* sv,
                              const double* th, double* red, double& nll, double* g, double* H, double* F) {
     const int R = Wn.R;
     eval_maps_f64(P, Wn, w, th[0], th[1], P.zfocus, th[2], true);
@@ -254,7 +256,7 @@ __device__ void eval_lik_f64(const PsfView& P, const WinView& Wn, const F64Work&
         for (int q = 0; q < 3; ++q) j[q] = A * (sg * w.T[(q + 1) * R * R + k] - psi * s[q + 1]) / s[0];
         j[3] = psi;
         j[4] = 1.0;
-        double mu = A * psi + B;
+        double mu = A * psi + B + (sv ? (double)sv[k] : 0.0);
         if (!(mu > 0.0)) { bad = true; continue; }
         double dk = (double)d[k];
         v[0] += dk > 0 ? mu - dk - dk * log(mu / dk) : mu;
@@ -286,7 +288,8 @@ __device__ void eval_lik_f64(const PsfView& P, const WinView& Wn, const F64Work&
 }
 
 __global__ void __launch_bounds__(F64_THREADS) fit_f64_kernel(PsfView P, WinView Wn, const float* rois,
-                                                              const double* init, int n, FitParamsDev prm,
+                                                              const float* scmos, const double* init, int n,
+                                                              FitParamsDev prm,
                                                               double* out5, double* crlb5, double* nll_out,
                                                               int* st_out, int* it_out, char* gscratch,
                                                               size_t per_cta, int use_smem, int* counter) {
@@ -304,6 +307,7 @@ __global__ void __launch_bounds__(F64_THREADS) fit_f64_kernel(PsfView P, WinView
         const int r = roi;
         if (r >= n) break;
         const float* d = rois + (size_t)r * R * R;
+        const float* sv = scmos ? scmos + (size_t)r * R * R : nullptr;
         if (threadIdx.x == 0) {
             for (int q = 0; q < 5; ++q) st.th[q] = init[5 * r + q];
             lm_clamp(st.th, prm);
@@ -311,7 +315,7 @@ __global__ void __launch_bounds__(F64_THREADS) fit_f64_kernel(PsfView P, WinView
         __syncthreads();
         double th[5], nll, g[5], H[25], F[25];
         for (int q = 0; q < 5; ++q) th[q] = st.th[q];
-        eval_lik_f64(P, Wn, w, d, th, red, nll, g, H, F);
+        eval_lik_f64(P, Wn, w, d, sv, th, red, nll, g, H, F);
         if (threadIdx.x == 0) {
             lm_start(st, nll, g, H, F, prm);
             go = lm_propose(st, prm) ? 1 : 0;
@@ -319,7 +323,7 @@ __global__ void __launch_bounds__(F64_THREADS) fit_f64_kernel(PsfView P, WinView
         __syncthreads();
         while (go) {
             for (int q = 0; q < 5; ++q) th[q] = st.trial[q];
-            eval_lik_f64(P, Wn, w, d, th, red, nll, g, H, F);
+            eval_lik_f64(P, Wn, w, d, sv, th, red, nll, g, H, F);
             if (threadIdx.x == 0) {
                 lm_update(st, nll, g, H, F, prm);
                 go = lm_propose(st, prm) ? 1 : 0;
@@ -366,9 +370,9 @@ int launch_model_f64(zola_ctx* ctx, zola_psf* p, WindowTables* w, const double* 
     return ZOLA_OK;
 }
 
-int launch_fit_f64(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_rois, const double* d_init, int n,
-                   const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll, int* d_status,
-                   int* d_iters, cudaStream_t st) {
+int launch_fit_f64(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_rois, const float* d_scmos,
+                   const double* d_init, int n, const zola_fit_params* prm, double* d_out5, double* d_crlb5,
+                   double* d_nll, int* d_status, int* d_iters, cudaStream_t st) {
     if (n <= 0) return ZOLA_OK;
     int nblocks = std::min(n, ctx->num_sms * 2);
     size_t per_cta, smem;
@@ -380,7 +384,8 @@ int launch_fit_f64(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_r
     WinView wv{w->R, w->W, w->d_C, w->d_G};
     ZOLA_CUDA_CHECK(cudaMemsetAsync(ctx->d_counter, 0, sizeof(int), st), ctx);
     prof_begin(ctx, 5, st);
-    fit_f64_kernel<<<nblocks, F64_THREADS, smem, st>>>(p->view, wv, d_rois, d_init, n, fp, d_out5, d_crlb5, d_nll,
+    fit_f64_kernel<<<nblocks, F64_THREADS, smem, st>>>(p->view, wv, d_rois, d_scmos, d_init, n, fp, d_out5, d_crlb5,
+                                                       d_nll,
                                                        d_status, d_iters, (char*)ctx->scratch, per_cta, use_smem,
                                                        ctx->d_counter);
     prof_end(ctx, st);
@@ -498,7 +503,8 @@ extern "C" int zola_fit_batch_noalloc(zola_psf* psf, int R, const float* d_rois,
     }
     FitParamsDev fp{prm->zmin, prm->zmax, prm->xymax, prm->tol_xyz, prm->step_xy, prm->step_z, prm->max_iter};
     WinView wv{w->R, w->W, w->d_C, w->d_G};
-    fit_f64_kernel<<<nblocks, F64_THREADS, smem, st>>>(psf->view, wv, d_rois, d_init5, n, fp, d_out5, d_crlb5, d_nll,
+    fit_f64_kernel<<<nblocks, F64_THREADS, smem, st>>>(psf->view, wv, d_rois, nullptr, d_init5, n, fp, d_out5,
+                                                       d_crlb5, d_nll,
                                                        d_status, d_iters, work, per_cta, use_smem, counter);
     ctx->launches++;
     e = cudaGetLastError();

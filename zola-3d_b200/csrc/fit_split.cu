@@ -697,7 +697,8 @@ __device__ __forceinline__ double warp_sum(double x) {
 // FP32; the likelihood and gradient with Kahan compensation, the Hessian and
 // Fisher terms plain; lane partials combined in FP64), then the FP64 LM step on
 // lane 0.
-__global__ void __launch_bounds__(LIK_THREADS) k_stage5(SplitDev P, const float* rois, const double* init, int n,
+__global__ void __launch_bounds__(LIK_THREADS) k_stage5(SplitDev P, const float* rois, const float* scmos,
+                                                        const double* init, int n,
                                                         FitParamsDev prm, double* out5, double* crlb5,
                                                         double* nll_out, int* st_out, int* it_out) {
     const int lane = threadIdx.x & 31;
@@ -708,6 +709,7 @@ __global__ void __launch_bounds__(LIK_THREADS) k_stage5(SplitDev P, const float*
     const int R = P.R, RR = R * R;
     const float* T0 = P.tmaps + (size_t)slot * 4 * RR;
     const float* d = rois + (size_t)roi * RR;
+    const float* sv = scmos ? scmos + (size_t)roi * RR : nullptr;  // sCMOS var/gain^2 (Localization.java:1132)
     // normalisation sums
     float ns[4] = {0, 0, 0, 0}, nc = 0.f;
     for (int k = lane; k < RR; k += 32) {
@@ -739,7 +741,7 @@ __global__ void __launch_bounds__(LIK_THREADS) k_stage5(SplitDev P, const float*
         j[2] = A * (sgn * T0[3 * RR + k] - psi * Dz) * invS;
         j[3] = psi;
         j[4] = 1.f;
-        const float mu = A * psi + B;
+        const float mu = A * psi + B + (sv ? sv[k] : 0.f);
         if (!(mu > 0.f)) { bad = true; continue; }
         const float dk = d[k];
         kahan_add(sg6[0], cg6[0], dk > 0.f ? mu - dk - dk * logf(mu / dk) : mu);
@@ -814,7 +816,8 @@ __global__ void __launch_bounds__(LIK_THREADS) k_stage5(SplitDev P, const float*
 // whole block holds the FP32 maps (row stride tm_stride(R)).
 // TMEM: stage-2 chunk buffers at 0 (and 128), row-blur accumulators at JB,
 // column-blur outputs at 0 once stage 2 is done.
-__global__ void __launch_bounds__(SPLIT_THREADS, 1) k_fused25(SplitDev P, const float* rois, const double* init, int n,
+__global__ void __launch_bounds__(SPLIT_THREADS, 1) k_fused25(SplitDev P, const float* rois, const float* scmos,
+                                                              const double* init, int n,
                                                               FitParamsDev prm, double* out5, double* crlb5,
                                                               double* nll_out, int* st_out, int* it_out) {
     extern __shared__ __align__(1024) char smem[];
@@ -1045,6 +1048,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_fused25(SplitDev P, const 
         const double* th = P.lm[slot].trial;
         const float A = (float)th[3], B = (float)th[4];
         const float* d = rois + (size_t)roi * RR;
+        const float* sv = scmos ? scmos + (size_t)roi * RR : nullptr;
         for (int k = tid_s; k < RR; k += nts) {
             const int ip = k / R, to = ip * RS + (k - ip * R);
             const float v = T0[to], sgn = v < 0 ? -1.f : 1.f, psi = fabsf(v) * invS;
@@ -1054,7 +1058,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_fused25(SplitDev P, const 
             jv[2] = A * (sgn * T0[3 * MS + to] - psi * Dz) * invS;
             jv[3] = psi;
             jv[4] = 1.f;
-            const float mu = A * psi + B;
+            const float mu = A * psi + B + (sv ? sv[k] : 0.f);
             if (!(mu > 0.f)) { bad = true; continue; }
             const float dk = d[k];
             kahan_add(sg6[0], cg6[0], dk > 0.f ? mu - dk - dk * logf(mu / dk) : mu);
@@ -1336,7 +1340,8 @@ int launch_model_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const double
     return ZOLA_OK;
 }
 
-int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_rois, const double* d_init, int n,
+int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_rois, const float* d_scmos,
+                     const double* d_init, int n,
                      const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll, int* d_status,
                      int* d_iters, cudaStream_t st) {
     SplitPool sp;
@@ -1358,7 +1363,7 @@ int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d
                 k_stage1<<<P / sp.pl->G1, SPLIT_THREADS, sp.s1, st>>>(D);
                 prof_end(ctx, st);
                 prof_begin(ctx, 1, st);
-                k_fused25<<<P / sp.pl->G2, SPLIT_THREADS, sp.sf, st>>>(D, d_rois, d_init, n, fp, d_out5, d_crlb5, d_nll,
+                k_fused25<<<P / sp.pl->G2, SPLIT_THREADS, sp.sf, st>>>(D, d_rois, d_scmos, d_init, n, fp, d_out5, d_crlb5, d_nll,
                                                                       d_status, d_iters);
                 prof_end(ctx, st);
                 ctx->launches += 2;
@@ -1366,7 +1371,7 @@ int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d
             }
             launch_model_stages(ctx, sp, st);
             prof_begin(ctx, 4, st);
-            k_stage5<<<(P + LIK_SLOTS - 1) / LIK_SLOTS, LIK_THREADS, 0, st>>>(D, d_rois, d_init, n, fp, d_out5, d_crlb5,
+            k_stage5<<<(P + LIK_SLOTS - 1) / LIK_SLOTS, LIK_THREADS, 0, st>>>(D, d_rois, d_scmos, d_init, n, fp, d_out5, d_crlb5,
                                                                              d_nll, d_status, d_iters);
             prof_end(ctx, st);
             ctx->launches++;

@@ -45,7 +45,10 @@ namespace zola {
 struct PipeView {
     int SX, SY, R, cap, nframes;
     double dx, minZ, maxZ, photon_thr, max_snr;
-    const double* images;     // nframes x SX x SY
+    const double* images;     // nframes x SX x SY: detection images
+    const double* fimg;       // nframes x SX x SY: fit images (= images without sCMOS)
+    const double* vmap;       // SX x SY sCMOS var/gain^2, or nullptr
+    float* slot_v;            // slots x R x R sCMOS patches (with vmap)
     unsigned char* mask;      // nframes x SX x SY
     const double* cand;       // nframes x cap x 7
     const int* counts;        // nframes
@@ -70,23 +73,27 @@ __device__ inline bool pipe_inside(const PipeView& V, int ci, int cj) {
     return ci > h + 1 && cj > h + 1 && ci < V.SX - h - 1 && cj < V.SY - h - 1;
 }
 
-// getAandB with the library PSF of slice r, threshold 10% of its max; returns
-// whether the candidate is fitted (maxPatch / B > maxSNR and B > 0).
+// getAandB with the library PSF of slice r, threshold 10% of its max, on the
+// patch minus the sCMOS term when there is one (:1119-1211); returns whether
+// the candidate is fitted (maxPatch / B > maxSNR and B > 0).
 __device__ bool pipe_a_and_b(const PipeView& V, const double* img, int r, int ci, int cj, double* A_, double* B_,
                              double* maxp_) {
+    const double* vm = V.vmap;
     const int R = V.R, h = R / 2, SY = V.SY;
     const double* psf = V.libpsf + (size_t)r * R * R;
     double maxp = -INFINITY, maxi = -INFINITY;
     for (int a = 0; a < R; ++a)
         for (int b = 0; b < R; ++b) {
+            const size_t px = (size_t)(ci - h + a) * SY + (cj - h + b);
             maxi = fmax(maxi, psf[a * R + b]);
-            maxp = fmax(maxp, img[(size_t)(ci - h + a) * SY + (cj - h + b)]);
+            maxp = fmax(maxp, img[px] - (vm ? vm[px] : 0.0));
         }
     const double thr = maxi * 0.1;
     double B = 0, A = 0, cb = 0, ca = 0;
     for (int a = 0; a < R; ++a)
         for (int b = 0; b < R; ++b) {
-            const double v = img[(size_t)(ci - h + a) * SY + (cj - h + b)];
+            const size_t px = (size_t)(ci - h + a) * SY + (cj - h + b);
+            const double v = img[px] - (vm ? vm[px] : 0.0);
             if (psf[a * R + b] < thr) { B += v; cb += 1; } else { A += v; ca += 1; }
         }
     B = cb != 0 ? B / cb : 0.0;
@@ -104,7 +111,7 @@ __device__ bool pipe_a_and_b(const PipeView& V, const double* img, int r, int ci
 __global__ void __launch_bounds__(128) k_pipe_wave(PipeView V, int K) {
     const int f = blockIdx.x, SX = V.SX, SY = V.SY, R = V.R, h = R / 2, RR = R * R;
     if (V.done[f]) return;
-    const double* img = V.images + (size_t)f * SX * SY;
+    const double* img = V.fimg + (size_t)f * SX * SY;
     const unsigned char* mk = V.mask + (size_t)f * SX * SY;
     const double* cand = V.cand + (size_t)f * V.cap * 7;
     const int n = min(V.counts[f], V.cap);
@@ -159,6 +166,11 @@ __global__ void __launch_bounds__(128) k_pipe_wave(PipeView V, int K) {
                 float* roi = V.rois + (size_t)s * RR;
                 for (int a = 0; a < R; ++a)
                     for (int b = 0; b < R; ++b) roi[a * R + b] = (float)img[(size_t)(ci - h + a) * SY + (cj - h + b)];
+                if (V.vmap) {
+                    float* sv = V.slot_v + (size_t)s * RR;
+                    for (int a = 0; a < R; ++a)
+                        for (int b = 0; b < R; ++b) sv[a * R + b] = (float)V.vmap[(size_t)(ci - h + a) * SY + (cj - h + b)];
+                }
                 double* in = V.init + (size_t)s * 5;  // loc.init(A, B, -dx, -dy, range[r] + dz)
                 in[0] = -row[5];
                 in[1] = -row[6];
@@ -176,15 +188,16 @@ __global__ void __launch_bounds__(128) k_pipe_wave(PipeView V, int K) {
     if (threadIdx.x == 0) V.limit[f] = limit;
 }
 
-// Model threshold of each fitted slot: 0.2 max(0, max(psi A + B - B))
-// (maxModelThreshold, LocalizationPipeline.java:872-880).
-__global__ void k_pipe_mthr(int n, int RR, const double* theta, const double* psi, double* mthr) {
+// Model threshold of each fitted slot: 0.2 max(0, max(model - B)), model =
+// psi A + B (+ sCMOS v) (maxModelThreshold, LocalizationPipeline.java:860-880).
+__global__ void k_pipe_mthr(int n, int RR, const double* theta, const double* psi, const float* slot_v, double* mthr) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
     const double A = theta[5 * s + 3], B = theta[5 * s + 4];
     const double* ps = psi + (size_t)s * RR;
+    const float* sv = slot_v ? slot_v + (size_t)s * RR : nullptr;
     double m = 0.0;
-    for (int k = 0; k < RR; ++k) m = fmax(m, ps[k] * A + B - B);
+    for (int k = 0; k < RR; ++k) m = fmax(m, ps[k] * A + B + (sv ? (double)sv[k] : 0.0) - B);
     mthr[s] = m * 0.2;
 }
 
@@ -196,7 +209,7 @@ __global__ void __launch_bounds__(256) k_pipe_replay(PipeView V, const double* t
                                                      int* acc_seq, int* nacc) {
     const int f = blockIdx.x, SX = V.SX, SY = V.SY, R = V.R, h = R / 2, RR = R * R;
     unsigned char* mk = V.mask + (size_t)f * SX * SY;
-    const double* img = V.images + (size_t)f * SX * SY;
+    const double* img = V.fimg + (size_t)f * SX * SY;
     const double* cand = V.cand + (size_t)f * V.cap * 7;
     if (V.done[f]) return;
     const int n = min(V.counts[f], V.cap), lim = V.limit[f];
@@ -229,8 +242,10 @@ __global__ void __launch_bounds__(256) k_pipe_replay(PipeView V, const double* t
             }
             const double A = theta[(size_t)slot * 5 + 3], B = theta[(size_t)slot * 5 + 4], thr = mthr[slot];
             const double* ps = psi + (size_t)slot * RR;
+            const float* sv = V.vmap ? V.slot_v + (size_t)slot * RR : nullptr;
             for (int k = threadIdx.x; k < RR; k += blockDim.x)
-                if (ps[k] * A + B - B > thr) mk[(size_t)(ci - h + k / R) * SY + (cj - h + k % R)] = 1;
+                if (ps[k] * A + B + (sv ? (double)sv[k] : 0.0) - B > thr)
+                    mk[(size_t)(ci - h + k / R) * SY + (cj - h + k % R)] = 1;
         } else {
             for (int k = threadIdx.x; k < RR; k += blockDim.x) {
                 const size_t px = (size_t)(ci - h + k / R) * SY + (cj - h + k % R);
@@ -276,9 +291,10 @@ __global__ void k_pipe_rows(PipeView V, int n, const int* acc_slot, const int* a
     const double x = th[0], y = th[1], z = th[2], A = th[3], B = th[4];
     const double* ps = psi + (size_t)k * RR;
     const float* roi = V.rois + (size_t)s * RR;
+    const float* sv = V.vmap ? V.slot_v + (size_t)s * RR : nullptr;
     double chi = 0;
-    for (int q = 0; q < RR; ++q) {
-        const double mu = ps[q] * A + B;
+    for (int q = 0; q < RR; ++q) {  // scoreCompute against the model (with the sCMOS term)
+        const double mu = ps[q] * A + B + (sv ? (double)sv[q] : 0.0);
         const double dd = roi[q] - mu;
         chi += dd * dd / mu;
     }
@@ -331,10 +347,30 @@ constexpr int PIPE_WAVE_FITS = 16;  // speculative fits per frame and wave
 
 }  // namespace
 
-extern "C" int zola_localize_frames(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const double* frames,
-                                    int nframes, int frame0, const zola_loc_params* prm, zola_localization* out,
-                                    int out_cap, int* nout) {
-    if (!ctx || !det || !fit_psf || !prm || !nout || (nframes > 0 && (!frames || !out))) return ZOLA_E_ARG;
+namespace zola {
+
+// sCMOS frames (LocalizationPipeline.java:588-640): c = (ADU - offset)/gain;
+// detection image c + vargain[0] clamped at 0, fit image c + vargain.
+__global__ void k_pipe_scmos(const float* adu, const double* offset, const double* gain, const double* vg, size_t SS,
+                             int nf, double* det_img, double* fit_img) {
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < SS * nf; k += (size_t)gridDim.x * blockDim.x) {
+        const size_t px = k % SS;
+        const double c = ((double)adu[k] - offset[px]) / gain[px];
+        const double d = c + vg[0];
+        det_img[k] = d < 0 ? 0 : d;
+        fit_img[k] = c + vg[px];
+    }
+}
+
+}  // namespace zola
+
+namespace {
+
+// frames: photon frames (no sCMOS); or adu + offset/gain/variance maps (sCMOS).
+int localize_impl(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const double* frames, const float* adu,
+                  const double* offset, const double* gain, const double* variance, int nframes, int frame0,
+                  const zola_loc_params* prm, zola_localization* out, int out_cap, int* nout) {
+    const bool scmos = adu != nullptr;
     *nout = 0;
     if (nframes <= 0) return ZOLA_OK;
     const int SX = det->v.SX, SY = det->v.SY, R = det->v.R;
@@ -350,7 +386,8 @@ extern "C" int zola_localize_frames(zola_ctx* ctx, zola_detector* det, zola_psf*
     const int K = prm->wave_fits > 0 ? prm->wave_fits : PIPE_WAVE_FITS;
     const int slot_cap = FB * K;
     Buf b_img, b_mask, b_cand, b_cnt, b_lib, b_rng, b_cslot, b_cmax, b_ptr, b_lim, b_done, b_ns, b_rois, b_init, b_sf,
-        b_sc, b_out5, b_st, b_xyz, b_psi, b_mthr, b_acc, b_seq, b_nacc, b_dpsi, b_rows;
+        b_sc, b_out5, b_st, b_xyz, b_psi, b_mthr, b_acc, b_seq, b_nacc, b_dpsi, b_rows, b_fimg, b_adu, b_off, b_gain,
+        b_vg, b_sv;
     cudaError_t e = cudaSuccess;
     auto A = [&](Buf& b, size_t bytes) { if (e == cudaSuccess) e = b.alloc(bytes); };
     A(b_img, SS * FB * 8); A(b_mask, SS * FB); A(b_cand, (size_t)FB * cap * 7 * 8); A(b_cnt, (size_t)FB * 4);
@@ -361,6 +398,15 @@ extern "C" int zola_localize_frames(zola_ctx* ctx, zola_detector* det, zola_psf*
     A(b_sc, (size_t)slot_cap * 4); A(b_out5, (size_t)slot_cap * 40); A(b_st, (size_t)slot_cap * 4);
     A(b_xyz, (size_t)slot_cap * 24); A(b_psi, RR * slot_cap * 8); A(b_mthr, (size_t)slot_cap * 8);
     A(b_acc, (size_t)slot_cap * 4); A(b_seq, (size_t)slot_cap * 4);
+    if (scmos) {
+        A(b_fimg, SS * FB * 8); A(b_adu, SS * FB * 4); A(b_off, SS * 8); A(b_gain, SS * 8); A(b_vg, SS * 8);
+        A(b_sv, RR * slot_cap * 4);
+        std::vector<double> vg(SS);
+        for (size_t k = 0; k < SS; ++k) vg[k] = variance[k] / (gain[k] * gain[k]);  // SCMOScamera.java:95
+        if (e == cudaSuccess) e = cudaMemcpy(b_vg.p, vg.data(), SS * 8, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(b_off.p, offset, SS * 8, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(b_gain.p, gain, SS * 8, cudaMemcpyHostToDevice);
+    }
     if (e == cudaSuccess) e = cudaMemcpyAsync(b_lib.p, lib.data(), lib.size() * 8, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(b_rng.p, range.data(), range.size() * 8, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) { ctx->err = std::string("zola_localize_frames: ") + cudaGetErrorString(e); return ZOLA_E_CUDA; }
@@ -371,6 +417,9 @@ extern "C" int zola_localize_frames(zola_ctx* ctx, zola_detector* det, zola_psf*
     V.dx = fit_psf->o.xystep; V.minZ = prm->minZ; V.maxZ = prm->maxZ; V.photon_thr = prm->photon_threshold;
     V.max_snr = prm->max_snr;
     V.images = (double*)b_img.p; V.mask = (unsigned char*)b_mask.p; V.cand = (double*)b_cand.p;
+    V.fimg = scmos ? (double*)b_fimg.p : (double*)b_img.p;
+    V.vmap = scmos ? (double*)b_vg.p : nullptr;
+    V.slot_v = scmos ? (float*)b_sv.p : nullptr;
     V.counts = (int*)b_cnt.p; V.libpsf = (double*)b_lib.p; V.range = (double*)b_rng.p;
     V.cand_slot = (int*)b_cslot.p; V.cand_maxp = (double*)b_cmax.p; V.pointer = (int*)b_ptr.p;
     V.limit = (int*)b_lim.p; V.done = (int*)b_done.p; V.nslots = (int*)b_ns.p; V.slot_cap = slot_cap;
@@ -384,7 +433,17 @@ extern "C" int zola_localize_frames(zola_ctx* ctx, zola_detector* det, zola_psf*
     for (int f0 = 0; f0 < nframes; f0 += FB) {
         const int nf = std::min(FB, nframes - f0);
         V.nframes = nf;
-        e = cudaMemcpyAsync(b_img.p, frames + (size_t)f0 * SS, SS * nf * 8, cudaMemcpyHostToDevice, st);
+        if (scmos) {
+            e = cudaMemcpyAsync(b_adu.p, adu + (size_t)f0 * SS, SS * nf * 4, cudaMemcpyHostToDevice, st);
+            if (e == cudaSuccess) {
+                k_pipe_scmos<<<ctx->num_sms * 8, 256, 0, st>>>((float*)b_adu.p, (double*)b_off.p, (double*)b_gain.p,
+                                                              (double*)b_vg.p, SS, nf, (double*)b_img.p,
+                                                              (double*)b_fimg.p);
+                ctx->launches++;
+            }
+        } else {
+            e = cudaMemcpyAsync(b_img.p, frames + (size_t)f0 * SS, SS * nf * 8, cudaMemcpyHostToDevice, st);
+        }
         if (e == cudaSuccess) e = cudaMemsetAsync(b_mask.p, 0, SS * nf, st);
         if (e == cudaSuccess) e = cudaMemsetAsync(b_ptr.p, 0, (size_t)nf * 4, st);
         if (e == cudaSuccess) e = cudaMemsetAsync(b_done.p, 0, (size_t)nf * 4, st);
@@ -402,8 +461,11 @@ extern "C" int zola_localize_frames(zola_ctx* ctx, zola_detector* det, zola_psf*
             if (e == cudaSuccess) e = cudaStreamSynchronize(st);
             if (e != cudaSuccess) return fail(e);
             if (nslot > 0) {
-                rc = zola_fit_batch_dev(ctx, fit_psf, R, (float*)b_rois.p, (double*)b_init.p, nslot, &fp,
-                                        (double*)b_out5.p, nullptr, nullptr, (int*)b_st.p, nullptr, st);
+                rc = scmos ? zola_fit_batch_scmos_dev(ctx, fit_psf, R, (float*)b_rois.p, (float*)b_sv.p,
+                                                      (double*)b_init.p, nslot, &fp, (double*)b_out5.p, nullptr,
+                                                      nullptr, (int*)b_st.p, nullptr, st)
+                           : zola_fit_batch_dev(ctx, fit_psf, R, (float*)b_rois.p, (double*)b_init.p, nslot, &fp,
+                                                (double*)b_out5.p, nullptr, nullptr, (int*)b_st.p, nullptr, st);
                 if (rc) return rc;
                 // psi at every fitted position (mask updates of the walk)
                 k_take_xyz<<<(nslot + 127) / 128, 128, 0, st>>>(nslot, (double*)b_out5.p, (double*)b_xyz.p);
@@ -411,7 +473,7 @@ extern "C" int zola_localize_frames(zola_ctx* ctx, zola_detector* det, zola_psf*
                 rc = zola_psf_model_dev(fit_psf, R, (double*)b_xyz.p, nslot, (double*)b_psi.p, nullptr, st);
                 if (rc) return rc;
                 k_pipe_mthr<<<(nslot + 127) / 128, 128, 0, st>>>(nslot, (int)RR, (double*)b_out5.p,
-                                                                 (double*)b_psi.p, (double*)b_mthr.p);
+                                                                 (double*)b_psi.p, V.slot_v, (double*)b_mthr.p);
                 ctx->launches++;
             }
             k_pipe_replay<<<nf, 256, 0, st>>>(V, (double*)b_out5.p, (int*)b_st.p, (double*)b_psi.p,
@@ -460,6 +522,26 @@ extern "C" int zola_localize_frames(zola_ctx* ctx, zola_detector* det, zola_psf*
     }
     *nout = (int)all.size();
     return ZOLA_OK;
+}
+
+}  // namespace
+
+extern "C" int zola_localize_frames(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const double* frames,
+                                    int nframes, int frame0, const zola_loc_params* prm, zola_localization* out,
+                                    int out_cap, int* nout) {
+    if (!ctx || !det || !fit_psf || !prm || !nout || (nframes > 0 && (!frames || !out))) return ZOLA_E_ARG;
+    return localize_impl(ctx, det, fit_psf, frames, nullptr, nullptr, nullptr, nullptr, nframes, frame0, prm, out,
+                         out_cap, nout);
+}
+
+extern "C" int zola_localize_frames_scmos(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const float* adu,
+                                          int nframes, int frame0, const zola_loc_params* prm, const double* offset,
+                                          const double* gain, const double* variance, zola_localization* out,
+                                          int out_cap, int* nout) {
+    if (!ctx || !det || !fit_psf || !prm || !nout || (nframes > 0 && (!adu || !out)) || !offset || !gain || !variance)
+        return ZOLA_E_ARG;
+    return localize_impl(ctx, det, fit_psf, nullptr, adu, offset, gain, variance, nframes, frame0, prm, out, out_cap,
+                         nout);
 }
 
 // ThunderStorm-style CSV (data/PLocalization.java:224-306): values floored to

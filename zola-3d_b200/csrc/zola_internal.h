@@ -134,17 +134,17 @@ void blur_matrix(int R, int W, double sigma, std::vector<double>& G, std::vector
 // fit_f64.cu
 int launch_model_f64(zola_ctx* ctx, zola_psf* p, WindowTables* w, const double* d_xyz, int n,
                      double* d_out, double* d_dout, cudaStream_t st);
-int launch_fit_f64(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_rois, const double* d_init,
-                   int n, const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll,
-                   int* d_status, int* d_iters, cudaStream_t st);
+int launch_fit_f64(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_rois, const float* d_scmos,
+                   const double* d_init, int n, const zola_fit_params* prm, double* d_out5, double* d_crlb5,
+                   double* d_nll, int* d_status, int* d_iters, cudaStream_t st);
 
 // fit_split.cu
 int launch_model_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const double* d_xyz, int n, double* d_out,
                        double* d_dout, cudaStream_t st);
 void free_split_plan(void* plan);
-int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_rois, const double* d_init,
-                     int n, const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll,
-                     int* d_status, int* d_iters, cudaStream_t st);
+int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_rois, const float* d_scmos,
+                     const double* d_init, int n, const zola_fit_params* prm, double* d_out5, double* d_crlb5,
+                     double* d_nll, int* d_status, int* d_iters, cudaStream_t st);
 
 int ensure_scratch(zola_ctx* ctx, size_t bytes, std::string& err);
 int ensure_io(zola_ctx* ctx, size_t bytes);
