@@ -73,12 +73,13 @@ struct SplitDev {
     int NCH2;
     const __half* gt_hi;  // RP x W (K-major)
     const __half* gt_lo;
-    // pupil tables (D x D, row a <-> kx, column b <-> ky), FP64
-    const double* pupil;
+    // pupil tables padded to DP x DP (row a <-> kx, column b <-> ky; zero
+    // beyond the D disk rows and columns), in the warp-load order of stage 1
+    const float* pupf;     // pupil (the model uses it in FP32)
     const double* phase0;  // phase - kzoil * zfocus
     const double* kz;
-    const double* kx;
-    const double* ky;
+    const double* kx;      // DP
+    const double* ky;      // DP
     // pool slabs
     char* a2;      // P/G2 tiles x 4 arrays x 128 x K1 f16
     char* a3;      // P/G2 tiles x 5 arrays x 128 x W f16
@@ -104,7 +105,11 @@ struct SplitPlanHost {
     __half* d_bc2_lo = nullptr;
     __half* d_gt_hi = nullptr;
     __half* d_gt_lo = nullptr;
-    double* d_phase0 = nullptr;
+    double* d_phase0 = nullptr;  // DP x DP
+    double* d_kz = nullptr;      // DP x DP
+    float* d_pupf = nullptr;     // DP x DP
+    double* d_kx = nullptr;      // DP
+    double* d_ky = nullptr;      // DP
 };
 
 static double pow2scale(double bound) {
@@ -137,7 +142,7 @@ static SplitPlanHost* get_plan(zola_psf* p, WindowTables* w, std::string& err) {
     pl->G1 = 128 / pl->DP;
     pl->G2 = 128 / W;
     pl->NT4 = (4 * pl->RP + 127) / 128;
-    const int DP = pl->DP, K1 = pl->K1, IC = pl->IC, NCH = pl->NCH, RP = pl->RP;
+    const int DP = pl->DP, K1 = pl->K1, IC = pl->IC, RP = pl->RP;
 
     // bounds
     double pmax = 0, kmax = 0, kzmax = 0;
@@ -229,9 +234,25 @@ static SplitPlanHost* get_plan(zola_psf* p, WindowTables* w, std::string& err) {
             gh[kmajor_off(ip, i, W) / 2] = hi;
             gl[kmajor_off(ip, i, W) / 2] = lo;
         }
-    // phase0 = phase - kzoil * zfocus (the zoil term of PSFPhase.java:560 with zoil = Zfocus)
-    std::vector<double> ph0((size_t)D * D);
-    for (size_t i = 0; i < ph0.size(); ++i) ph0[i] = p->phase[i] - p->kzoil[i] * p->o.zfocus;
+    // phase0 = phase - kzoil * zfocus (the zoil term of PSFPhase.java:560 with zoil = Zfocus),
+    // padded to DP x DP with the other pupil tables
+    std::vector<double> ph0((size_t)DP * DP, 0.0), kzp((size_t)DP * DP, 0.0), kxp(DP, 0.0), kyp(DP, 0.0);
+    std::vector<float> pupf((size_t)DP * DP, 0.f);
+    // Order of the DP x DP tables: [b / 8][(b % 8) / 2][a][b % 2] for phase0 and kz
+    // (double pairs), [b / 8][(b % 8) / 4][a][b % 4] for the pupil (float quads), so
+    // that 32 consecutive rows a of one column group are one contiguous warp load.
+    for (int a = 0; a < D; ++a) {
+        kxp[a] = p->kx[a];
+        kyp[a] = p->ky[a];
+        for (int b = 0; b < D; ++b) {
+            const size_t i = (size_t)a * D + b;
+            const size_t o2 = (((size_t)(b / 8) * 4 + (b % 8) / 2) * DP + a) * 2 + b % 2;
+            const size_t o4 = (((size_t)(b / 8) * 2 + (b % 8) / 4) * DP + a) * 4 + b % 4;
+            ph0[o2] = p->phase[i] - p->kzoil[i] * p->o.zfocus;
+            kzp[o2] = p->kz[i];
+            pupf[o4] = (float)p->pupil[i];
+        }
+    }
 
     cudaError_t e = cudaSuccess;
     auto up = [&](void** dst, const void* src, size_t bytes) {
@@ -246,6 +267,10 @@ static SplitPlanHost* get_plan(zola_psf* p, WindowTables* w, std::string& err) {
     up((void**)&pl->d_gt_hi, gh.data(), gh.size() * 2);
     up((void**)&pl->d_gt_lo, gl.data(), gl.size() * 2);
     up((void**)&pl->d_phase0, ph0.data(), ph0.size() * 8);
+    up((void**)&pl->d_kz, kzp.data(), kzp.size() * 8);
+    up((void**)&pl->d_pupf, pupf.data(), pupf.size() * 4);
+    up((void**)&pl->d_kx, kxp.data(), kxp.size() * 8);
+    up((void**)&pl->d_ky, kyp.data(), kyp.size() * 8);
     if (e != cudaSuccess) {
         err = std::string("split plan upload: ") + cudaGetErrorString(e);
         delete pl;
@@ -265,6 +290,10 @@ void free_split_plan(void* plan) {
     cudaFree(pl->d_gt_hi);
     cudaFree(pl->d_gt_lo);
     cudaFree(pl->d_phase0);
+    cudaFree(pl->d_kz);
+    cudaFree(pl->d_pupf);
+    cudaFree(pl->d_kx);
+    cudaFree(pl->d_ky);
     delete pl;
 }
 
@@ -281,6 +310,45 @@ __device__ __forceinline__ void store8h(void* dst, const __half* v) {
     u.z = (uint32_t)__half_as_ushort(v[4]) | ((uint32_t)__half_as_ushort(v[5]) << 16);
     u.w = (uint32_t)__half_as_ushort(v[6]) | ((uint32_t)__half_as_ushort(v[7]) << 16);
     *(uint4*)dst = u;
+}
+
+// Two floats rounded to a packed f16 pair (a in the low half).
+__device__ __forceinline__ uint32_t pack_h2(float a, float b) {
+    union { __half2 h; uint32_t u; } cv;
+    cv.h = __floats2half2_rn(a, b);
+    return cv.u;
+}
+
+// hi + lo f16 split of two floats, as packed pairs (the same values as
+// umma::split_f16 on each, with one conversion instruction per pair).
+__device__ __forceinline__ void split2(float a, float b, uint32_t& hi, uint32_t& lo) {
+    union { __half2 h; uint32_t u; } h, l;
+    h.h = __floats2half2_rn(a, b);
+    const float2 f = __half22float2(h.h);
+    l.h = __floats2half2_rn(a - f.x, b - f.y);
+    hi = h.u;
+    lo = l.u;
+}
+
+__device__ __forceinline__ void store4w(void* dst, const uint32_t* w) { *(uint4*)dst = make_uint4(w[0], w[1], w[2], w[3]); }
+
+// sin and cos of an FP64 phase.  The phase is reduced in FP64 by the nearest
+// multiple q of pi/2 (pi/2 as a two-double sum, so r = ph - q pi/2 keeps FP64
+// accuracy for any phase the model produces); r in [-pi/4, pi/4] is rounded
+// to FP32 and sin r, cos r come from their Taylor polynomials of degree 9 and
+// 10 (truncation below 2e-9 on that interval, under the FP32 rounding of the
+// result), rotated by the quadrant q mod 4.
+__device__ __forceinline__ void sincos_phase(double ph, float& s, float& c) {
+    const double q = rint(ph * 0.6366197723675814);
+    double r = fma(-q, 1.5707963267948966, ph);
+    r = fma(-q, 6.123233995736766e-17, r);
+    const float x = (float)r, x2 = x * x;
+    const float sp = fmaf(x * x2, -1.f / 6 + x2 * (1.f / 120 + x2 * (-1.f / 5040 + x2 * (1.f / 362880))), x);
+    const float cp = 1.f + x2 * (-0.5f + x2 * (1.f / 24 + x2 * (-1.f / 720 + x2 * (1.f / 40320 + x2 * (-1.f / 3628800)))));
+    const int k = (int)q & 3;
+    const float ss = (k & 1) ? cp : sp, cc = (k & 1) ? sp : cp;
+    s = (k & 2) ? -ss : ss;
+    c = ((k + 1) & 2) ? -cc : cc;
 }
 
 // Issue an MMA chain over K (in steps of 16) for one accumulator.
@@ -313,7 +381,7 @@ __device__ __forceinline__ bool tile_live(const SplitDev& P, int s0, int g) {
 // One CTA per G1 slots; thread t builds row (g = t / DP, a = t % DP) of Q.
 __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage1(SplitDev P) {
     extern __shared__ __align__(1024) char smem[];
-    const int K1 = P.K1, DP = P.DP, IC = P.IC, NCH = P.NCH, D = P.D;
+    const int K1 = P.K1, DP = P.DP, IC = P.IC, NCH = P.NCH;
     const int t = threadIdx.x;
     char* A1hi = smem;
     char* A1lo = A1hi + 256 * K1;
@@ -346,47 +414,70 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage1(SplitDev P) {
         if (NCH > 1) load_bc(1, 1);
     }
 
-    // build the Q operand rows: thread -> row (g, a) = t % 128, columns b of its warpgroup
+    // epilogue mapping: thread -> tile row (g, a) = t % 128 (its TMEM lane), column share of its warpgroup
     const int row = t & 127, wg = t >> 7;
     const int g = row / DP, a = row % DP;
     const int slot = blockIdx.x * P.G1 + g;
     const int roi = P.slot_roi[slot];
-    double x = 0, y = 0, z = 0;
-    if (roi >= 0) {
-        x = P.lm[slot].trial[0]; y = P.lm[slot].trial[1]; z = P.lm[slot].trial[2];
-    }
-    const double kxa = a < D ? P.kx[a] : 0.0;
-    const int bq = DP / 4;
-    for (int b0 = wg * bq; b0 < (wg + 1) * bq; b0 += 8) {
-        __half rh[8], rl[8], ih[8], il[8], zr[8], zi[8];
+
+    // Q build: thread -> pupil row qa and 8 columns qb0.. of every slot it covers.  The
+    // DP x DP / 8 threads of one slot read each table entry once, as 512-byte warp loads
+    // (the tables are stored in that order), and apply it to each of the CTA's slots.
+    {
+        const int nps = DP * DP / 8;  // threads per slot: 512 (DP = 64) or 128 (DP = 32)
+        const int qi0 = t % nps, qa = qi0 % DP, qbg = qi0 / DP, qb0 = qbg * 8;
+        double ph0[8], kzr[8], kyr[8];
+        float pu[8];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const int b = b0 + u;
-            float qr = 0.f, qi = 0.f, kzv = 0.f;
-            if (roi >= 0 && a < D && b < D) {
-                const int idx = a * D + b;
-                const double pup = P.pupil[idx];
-                if (pup != 0.0) {
-                    double ph = P.phase0[idx] + kxa * x + P.ky[b] * y + P.kz[idx] * z;
-                    ph -= 6.283185307179586 * rint(ph * 0.15915494309189535);
-                    float sn, cs;
-                    sincosf((float)ph, &sn, &cs);
-                    qr = (float)pup * cs;
-                    qi = (float)pup * sn;
-                    kzv = (float)P.kz[idx];
-                }
-            }
-            umma::split_f16(qr * P.sc.q, rh[u], rl[u]);
-            umma::split_f16(qi * P.sc.q, ih[u], il[u]);
-            zr[u] = __float2half_rn(-kzv * qi * P.sc.qz);  // Qz = i kz Q
-            zi[u] = __float2half_rn(kzv * qr * P.sc.qz);
+        for (int u = 0; u < 8; u += 2) {
+            const double2 v0 = *(const double2*)(P.phase0 + (((size_t)qbg * 4 + u / 2) * DP + qa) * 2);
+            const double2 v1 = *(const double2*)(P.kz + (((size_t)qbg * 4 + u / 2) * DP + qa) * 2);
+            const double2 v2 = *(const double2*)(P.ky + qb0 + u);
+            ph0[u] = v0.x; ph0[u + 1] = v0.y;
+            kzr[u] = v1.x; kzr[u + 1] = v1.y;
+            kyr[u] = v2.x; kyr[u + 1] = v2.y;
         }
-        store8h(A1hi + kmajor_off(row, b0, K1), rh);
-        store8h(A1lo + kmajor_off(row, b0, K1), rl);
-        store8h(A1hi + kmajor_off(row, DP + b0, K1), ih);
-        store8h(A1lo + kmajor_off(row, DP + b0, K1), il);
-        store8h(A1z + kmajor_off(row, b0, K1), zr);
-        store8h(A1z + kmajor_off(row, DP + b0, K1), zi);
+#pragma unroll
+        for (int u = 0; u < 8; u += 4) {
+            const float4 v = *(const float4*)(P.pupf + (((size_t)qbg * 2 + u / 4) * DP + qa) * 4);
+            pu[u] = v.x; pu[u + 1] = v.y; pu[u + 2] = v.z; pu[u + 3] = v.w;
+        }
+        const double kxa = P.kx[qa];
+        for (int qg = t / nps; qg < P.G1; qg += SPLIT_THREADS / nps) {
+            const int qslot = blockIdx.x * P.G1 + qg;
+            const bool live = P.slot_roi[qslot] >= 0;
+            double x = 0, y = 0, z = 0;
+            if (live) {
+                x = P.lm[qslot].trial[0]; y = P.lm[qslot].trial[1]; z = P.lm[qslot].trial[2];
+            }
+            const int qrow = qg * DP + qa;
+            uint32_t rh[4], rl[4], ih[4], il[4], zr[4], zi[4];
+#pragma unroll
+            for (int u = 0; u < 8; u += 2) {
+                float qr[2], qi[2], kzv[2];
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    qr[e] = 0.f; qi[e] = 0.f; kzv[e] = 0.f;
+                    if (live && pu[u + e] != 0.f) {
+                        float sn, cs;
+                        sincos_phase(ph0[u + e] + kxa * x + kyr[u + e] * y + kzr[u + e] * z, sn, cs);
+                        qr[e] = pu[u + e] * cs;
+                        qi[e] = pu[u + e] * sn;
+                        kzv[e] = (float)kzr[u + e];
+                    }
+                }
+                split2(qr[0] * P.sc.q, qr[1] * P.sc.q, rh[u / 2], rl[u / 2]);
+                split2(qi[0] * P.sc.q, qi[1] * P.sc.q, ih[u / 2], il[u / 2]);
+                zr[u / 2] = pack_h2(-kzv[0] * qi[0] * P.sc.qz, -kzv[1] * qi[1] * P.sc.qz);  // Qz = i kz Q
+                zi[u / 2] = pack_h2(kzv[0] * qr[0] * P.sc.qz, kzv[1] * qr[1] * P.sc.qz);
+            }
+            store4w(A1hi + kmajor_off(qrow, qb0, K1), rh);
+            store4w(A1lo + kmajor_off(qrow, qb0, K1), rl);
+            store4w(A1hi + kmajor_off(qrow, DP + qb0, K1), ih);
+            store4w(A1lo + kmajor_off(qrow, DP + qb0, K1), il);
+            store4w(A1z + kmajor_off(qrow, qb0, K1), zr);
+            store4w(A1z + kmajor_off(qrow, DP + qb0, K1), zi);
+        }
     }
     umma::fence_proxy_async();
     __syncthreads();
@@ -424,24 +515,24 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage1(SplitDev P) {
             for (int part = 0; part < 6; ++part) umma::tmem_ld8(tmem_lane_addr(tbase, col0 + part * IC + h), v[part]);
             if (roi < 0) continue;
             const int m = mrow0 + c * IC + h;
-            __half shr[8], slr[8], shi[8], sli[8], yr[8], yi[8], zr[8], zi[8];
+            uint32_t shr[4], slr[4], shi[4], sli[4], yr[4], yi[4], zr[4], zi[4];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                umma::split_f16(v[0][u] * P.sc.c2, shr[u], slr[u]);
-                umma::split_f16(v[1][u] * P.sc.c2, shi[u], sli[u]);
-                yr[u] = __float2half_rn(v[2][u] * P.sc.c2y);
-                yi[u] = __float2half_rn(v[3][u] * P.sc.c2y);
-                zr[u] = __float2half_rn(v[4][u] * P.sc.c2z);
-                zi[u] = __float2half_rn(v[5][u] * P.sc.c2z);
+            for (int u = 0; u < 8; u += 2) {
+                split2(v[0][u] * P.sc.c2, v[0][u + 1] * P.sc.c2, shr[u / 2], slr[u / 2]);
+                split2(v[1][u] * P.sc.c2, v[1][u + 1] * P.sc.c2, shi[u / 2], sli[u / 2]);
+                yr[u / 2] = pack_h2(v[2][u] * P.sc.c2y, v[2][u + 1] * P.sc.c2y);
+                yi[u / 2] = pack_h2(v[3][u] * P.sc.c2y, v[3][u + 1] * P.sc.c2y);
+                zr[u / 2] = pack_h2(v[4][u] * P.sc.c2z, v[4][u + 1] * P.sc.c2z);
+                zi[u / 2] = pack_h2(v[5][u] * P.sc.c2z, v[5][u + 1] * P.sc.c2z);
             }
-            store8h(a2t + 0 * arr + mnmajor_off(m, a, 128), shr);
-            store8h(a2t + 1 * arr + mnmajor_off(m, a, 128), slr);
-            store8h(a2t + 0 * arr + mnmajor_off(m, DP + a, 128), shi);
-            store8h(a2t + 1 * arr + mnmajor_off(m, DP + a, 128), sli);
-            store8h(a2t + 2 * arr + mnmajor_off(m, a, 128), yr);
-            store8h(a2t + 2 * arr + mnmajor_off(m, DP + a, 128), yi);
-            store8h(a2t + 3 * arr + mnmajor_off(m, a, 128), zr);
-            store8h(a2t + 3 * arr + mnmajor_off(m, DP + a, 128), zi);
+            store4w(a2t + 0 * arr + mnmajor_off(m, a, 128), shr);
+            store4w(a2t + 1 * arr + mnmajor_off(m, a, 128), slr);
+            store4w(a2t + 0 * arr + mnmajor_off(m, DP + a, 128), shi);
+            store4w(a2t + 1 * arr + mnmajor_off(m, DP + a, 128), sli);
+            store4w(a2t + 2 * arr + mnmajor_off(m, a, 128), yr);
+            store4w(a2t + 2 * arr + mnmajor_off(m, DP + a, 128), yi);
+            store4w(a2t + 3 * arr + mnmajor_off(m, a, 128), zr);
+            store4w(a2t + 3 * arr + mnmajor_off(m, DP + a, 128), zi);
         }
         umma::fence_before_sync();
         __syncthreads();
@@ -523,26 +614,28 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage2(SplitDev P) {
             umma::tmem_ld8(tmem_lane_addr(tbase, col0 + 1 * IC + h), ei);
             umma::tmem_ld8(tmem_lane_addr(tbase, col0 + 2 * IC + h), xr);
             umma::tmem_ld8(tmem_lane_addr(tbase, col0 + 3 * IC + h), xi);
-            __half hh[8], ll[8], dx[8], dy[8], dz[8];
+            uint32_t hh[4], ll[4], dx[4], dy[4], dz[4];
+            auto ipx = [&](int u, float cf) { return (er[u] * xr[u] + ei[u] * xi[u]) * cf; };
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                umma::split_f16((er[u] * er[u] + ei[u] * ei[u]) * P.sc.cI, hh[u], ll[u]);
-                dx[u] = __float2half_rn((er[u] * xr[u] + ei[u] * xi[u]) * P.sc.cIx);
+            for (int u = 0; u < 8; u += 2) {
+                split2((er[u] * er[u] + ei[u] * ei[u]) * P.sc.cI, (er[u + 1] * er[u + 1] + ei[u + 1] * ei[u + 1]) * P.sc.cI,
+                       hh[u / 2], ll[u / 2]);
+                dx[u / 2] = pack_h2(ipx(u, P.sc.cIx), ipx(u + 1, P.sc.cIx));
             }
             umma::tmem_ld8(tmem_lane_addr(tbase, col0 + 4 * IC + h), xr);
             umma::tmem_ld8(tmem_lane_addr(tbase, col0 + 5 * IC + h), xi);
 #pragma unroll
-            for (int u = 0; u < 8; ++u) dy[u] = __float2half_rn((er[u] * xr[u] + ei[u] * xi[u]) * P.sc.cIy);
+            for (int u = 0; u < 8; u += 2) dy[u / 2] = pack_h2(ipx(u, P.sc.cIy), ipx(u + 1, P.sc.cIy));
             umma::tmem_ld8(tmem_lane_addr(tbase, col0 + 6 * IC + h), xr);
             umma::tmem_ld8(tmem_lane_addr(tbase, col0 + 7 * IC + h), xi);
 #pragma unroll
-            for (int u = 0; u < 8; ++u) dz[u] = __float2half_rn((er[u] * xr[u] + ei[u] * xi[u]) * P.sc.cIz);
+            for (int u = 0; u < 8; u += 2) dz[u / 2] = pack_h2(ipx(u, P.sc.cIz), ipx(u + 1, P.sc.cIz));
             const uint32_t off = kmajor_off(row, c * IC + h, W);
-            store8h(a3t + 0 * arr3 + off, hh);
-            store8h(a3t + 1 * arr3 + off, ll);
-            store8h(a3t + 2 * arr3 + off, dx);
-            store8h(a3t + 3 * arr3 + off, dy);
-            store8h(a3t + 4 * arr3 + off, dz);
+            store4w(a3t + 0 * arr3 + off, hh);
+            store4w(a3t + 1 * arr3 + off, ll);
+            store4w(a3t + 2 * arr3 + off, dx);
+            store4w(a3t + 3 * arr3 + off, dy);
+            store4w(a3t + 4 * arr3 + off, dz);
         }
         umma::fence_before_sync();
         __syncthreads();
@@ -606,12 +699,12 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage3(SplitDev P) {
         for (int i8 = 0; i8 < 16; i8 += 8) {
             const int r = m * RP + h + i8;
             char* tile = a4s + (size_t)(r / 128) * a4_tile_bytes(W);
-            __half hh[8], ll[8];
+            uint32_t hh[4], ll[4];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) umma::split_f16(v[i8 + u] * P.sc.cJ[m], hh[u], ll[u]);
+            for (int u = 0; u < 8; u += 2) split2(v[i8 + u] * P.sc.cJ[m], v[i8 + u + 1] * P.sc.cJ[m], hh[u / 2], ll[u / 2]);
             const uint32_t off = mnmajor_off(r % 128, j, 128);
-            store8h(tile + off, hh);
-            store8h(tile + arr4 + off, ll);
+            store4w(tile + off, hh);
+            store4w(tile + arr4 + off, ll);
         }
     }
     umma::fence_before_sync();
@@ -679,6 +772,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage4(SplitDev P) {
 // ----------------------------------------------------------- stage 5 -------
 constexpr int NRED = 1 + 5 + 15 + 15;
 constexpr int LIK_SLOTS = LIK_THREADS / 32;  // one warp per slot
+constexpr int S5_UNROLL = 4;                  // pixels per lane whose loads are in flight together
 
 __device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
     float y = v - c;
@@ -710,15 +804,28 @@ __global__ void __launch_bounds__(LIK_THREADS) k_stage5(SplitDev P, const float*
     const float* T0 = P.tmaps + (size_t)slot * 4 * RR;
     const float* d = rois + (size_t)roi * RR;
     const float* sv = scmos ? scmos + (size_t)roi * RR : nullptr;  // sCMOS var/gain^2 (Localization.java:1132)
-    // normalisation sums
+    // normalisation sums.  Each lane walks its pixels k = lane, lane + 32, ...
+    // in order; the loads of S5_UNROLL consecutive pixels are issued together
+    // so that several memory round trips overlap.
     float ns[4] = {0, 0, 0, 0}, nc = 0.f;
-    for (int k = lane; k < RR; k += 32) {
-        const float v = T0[k];
-        const float sg = v < 0 ? -1.f : 1.f;
-        kahan_add(ns[0], nc, fabsf(v));
-        ns[1] += sg * T0[RR + k];
-        ns[2] += sg * T0[2 * RR + k];
-        ns[3] += sg * T0[3 * RR + k];
+    for (int k0 = lane; k0 < RR; k0 += 32 * S5_UNROLL) {
+        float tv[S5_UNROLL][4];
+#pragma unroll
+        for (int j = 0; j < S5_UNROLL; ++j) {
+            const int k = k0 + 32 * j;
+            if (k < RR)
+                for (int m = 0; m < 4; ++m) tv[j][m] = T0[m * RR + k];
+        }
+#pragma unroll
+        for (int j = 0; j < S5_UNROLL; ++j) {
+            if (k0 + 32 * j >= RR) continue;
+            const float v = tv[j][0];
+            const float sg = v < 0 ? -1.f : 1.f;
+            kahan_add(ns[0], nc, fabsf(v));
+            ns[1] += sg * tv[j][1];
+            ns[2] += sg * tv[j][2];
+            ns[3] += sg * tv[j][3];
+        }
     }
     const float S = (float)warp_sum((double)ns[0] - (double)nc);
     const float Dx = (float)warp_sum(ns[1]), Dy = (float)warp_sum(ns[2]), Dz = (float)warp_sum(ns[3]);
@@ -731,32 +838,46 @@ __global__ void __launch_bounds__(LIK_THREADS) k_stage5(SplitDev P, const float*
 #pragma unroll
     for (int k = 0; k < 30; ++k) sh[k] = 0.f;
     bool bad = false;
-    for (int k = lane; k < RR; k += 32) {
-        const float v = T0[k];
-        const float sgn = v < 0 ? -1.f : 1.f;
-        const float psi = fabsf(v) * invS;
-        float j[5];
-        j[0] = A * (sgn * T0[RR + k] - psi * Dx) * invS;
-        j[1] = A * (sgn * T0[2 * RR + k] - psi * Dy) * invS;
-        j[2] = A * (sgn * T0[3 * RR + k] - psi * Dz) * invS;
-        j[3] = psi;
-        j[4] = 1.f;
-        const float mu = A * psi + B + (sv ? sv[k] : 0.f);
-        if (!(mu > 0.f)) { bad = true; continue; }
-        const float dk = d[k];
-        kahan_add(sg6[0], cg6[0], dk > 0.f ? mu - dk - dk * logf(mu / dk) : mu);
-        const float wg = 1.f - dk / mu, wf = 1.f / mu, wh = dk * wf * wf;
+    for (int k0 = lane; k0 < RR; k0 += 32 * S5_UNROLL) {
+        float tv[S5_UNROLL][4], dv[S5_UNROLL], vv[S5_UNROLL];
 #pragma unroll
-        for (int q = 0; q < 5; ++q) kahan_add(sg6[1 + q], cg6[1 + q], wg * j[q]);
-        int o = 0;
-#pragma unroll
-        for (int q = 0; q < 5; ++q)
-#pragma unroll
-            for (int r2 = 0; r2 <= q; ++r2) {
-                sh[o] += wh * j[q] * j[r2];
-                sh[o + 15] += wf * j[q] * j[r2];
-                ++o;
+        for (int jj = 0; jj < S5_UNROLL; ++jj) {
+            const int k = k0 + 32 * jj;
+            if (k < RR) {
+                for (int m = 0; m < 4; ++m) tv[jj][m] = T0[m * RR + k];
+                dv[jj] = d[k];
+                vv[jj] = sv ? sv[k] : 0.f;
             }
+        }
+#pragma unroll
+        for (int jj = 0; jj < S5_UNROLL; ++jj) {
+            if (k0 + 32 * jj >= RR) continue;
+            const float v = tv[jj][0];
+            const float sgn = v < 0 ? -1.f : 1.f;
+            const float psi = fabsf(v) * invS;
+            float j[5];
+            j[0] = A * (sgn * tv[jj][1] - psi * Dx) * invS;
+            j[1] = A * (sgn * tv[jj][2] - psi * Dy) * invS;
+            j[2] = A * (sgn * tv[jj][3] - psi * Dz) * invS;
+            j[3] = psi;
+            j[4] = 1.f;
+            const float mu = A * psi + B + vv[jj];
+            if (!(mu > 0.f)) { bad = true; continue; }
+            const float dk = dv[jj];
+            kahan_add(sg6[0], cg6[0], dk > 0.f ? mu - dk - dk * logf(mu / dk) : mu);
+            const float wg = 1.f - dk / mu, wf = 1.f / mu, wh = dk * wf * wf;
+#pragma unroll
+            for (int q = 0; q < 5; ++q) kahan_add(sg6[1 + q], cg6[1 + q], wg * j[q]);
+            int o = 0;
+#pragma unroll
+            for (int q = 0; q < 5; ++q)
+#pragma unroll
+                for (int r2 = 0; r2 <= q; ++r2) {
+                    sh[o] += wh * j[q] * j[r2];
+                    sh[o + 15] += wf * j[q] * j[r2];
+                    ++o;
+                }
+        }
     }
     double tot[NRED];
 #pragma unroll
@@ -1267,7 +1388,7 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
     D.zfocus = p->o.zfocus;
     D.bc_hi = pl->d_bc_hi; D.bc_lo = pl->d_bc_lo; D.gt_hi = pl->d_gt_hi; D.gt_lo = pl->d_gt_lo;
     D.bc2_hi = pl->d_bc2_hi; D.bc2_lo = pl->d_bc2_lo; D.NCH2 = pl->NCH2;
-    D.pupil = p->view.pupil; D.phase0 = pl->d_phase0; D.kz = p->view.kz; D.kx = p->view.kx; D.ky = p->view.ky;
+    D.pupf = pl->d_pupf; D.phase0 = pl->d_phase0; D.kz = pl->d_kz; D.kx = pl->d_kx; D.ky = pl->d_ky;
     D.a2 = base; base += b_a2;
     D.a3 = base; base += b_a3;
     D.a4 = base; base += b_a4;
