@@ -71,6 +71,7 @@ struct SplitDev {
     const __half* bc2_hi; // NCH2 chunks of 4*16 x K1 (fused kernel)
     const __half* bc2_lo; // NCH2 chunks of 2*16 x K1
     int NCH2;
+    const __half* bcs;    // K1/16 K-slabs of 6W x 16 (wide stage kernels)
     const __half* gt_hi;  // RP x W (K-major)
     const __half* gt_lo;
     // pupil tables padded to DP x DP (row a <-> kx, column b <-> ky; zero
@@ -103,6 +104,7 @@ struct SplitPlanHost {
     __half* d_bc_lo = nullptr;
     __half* d_bc2_hi = nullptr;
     __half* d_bc2_lo = nullptr;
+    __half* d_bcs = nullptr;
     __half* d_gt_hi = nullptr;
     __half* d_gt_lo = nullptr;
     double* d_phase0 = nullptr;  // DP x DP
@@ -188,6 +190,28 @@ static SplitPlanHost* get_plan(zola_psf* p, WindowTables* w, std::string& err) {
         re = w->C[((size_t)i * D + b) * 2];
         im = w->C[((size_t)i * D + b) * 2 + 1];
     };
+    // scaled constant of part `part` at output index i and data column k (0 beyond the disk)
+    auto bc_value = [&](int part, int i, int k) {
+        const int b = k < DP ? k : k - DP;
+        if (b >= D) return 0.0;
+        double cr, ci;
+        C(i, b, cr, ci);
+        const double kb = p->ky[b];
+        const double ckr = -kb * ci, cki = kb * cr;
+        const bool re_in = k < DP;
+        double v;
+        switch (part) {
+            case 0: v = re_in ? cr : -ci; break;
+            case 1: v = re_in ? ci : cr; break;
+            case 2: v = re_in ? ckr : -cki; break;
+            default: v = re_in ? cki : ckr; break;
+        }
+        return v * sB;
+    };
+    auto split_h = [](double v, __half& hi, __half& lo) {
+        hi = __float2half_rn((float)v);
+        lo = __float2half_rn((float)(v - (double)__half2float(hi)));
+    };
     auto pack_bc = [&](int icw, std::vector<__half>& bh, std::vector<__half>& bl) {
         const int nch = W / icw;
         bh.assign((size_t)nch * 4 * icw * K1, __float2half(0.f));
@@ -197,28 +221,25 @@ static SplitPlanHost* get_plan(zola_psf* p, WindowTables* w, std::string& err) {
                 for (int ii = 0; ii < icw; ++ii) {
                     int i = c * icw + ii, n = part * icw + ii;
                     for (int k = 0; k < K1; ++k) {
-                        int b = k < DP ? k : k - DP;
-                        if (b >= D) continue;
-                        double cr, ci;
-                        C(i, b, cr, ci);
-                        double kb = p->ky[b];
-                        double ckr = -kb * ci, cki = kb * cr;
-                        double v;
-                        bool re_in = k < DP;
-                        switch (part) {
-                            case 0: v = re_in ? cr : -ci; break;
-                            case 1: v = re_in ? ci : cr; break;
-                            case 2: v = re_in ? ckr : -cki; break;
-                            default: v = re_in ? cki : ckr; break;
-                        }
-                        v *= sB;
-                        __half hi = __float2half_rn((float)v);
-                        __half lo = __float2half_rn((float)(v - (double)__half2float(hi)));
+                        __half hi, lo;
+                        split_h(bc_value(part, i, k), hi, lo);
                         bh[(size_t)c * 4 * icw * K1 + kmajor_off(n, k, K1) / 2] = hi;
                         if (part < 2) bl[(size_t)c * 2 * icw * K1 + kmajor_off(n, k, K1) / 2] = lo;
                     }
                 }
     };
+    // K-slabs of the wide stage kernels: for K step s (columns 16s .. 16s + 15),
+    // rows n = q * W + i with q = 0..3 the hi values of parts 0..3 and q = 4, 5
+    // the lo values of parts 0, 1; K-major with K = 16 (6W x 32 bytes a slab).
+    std::vector<__half> bs((size_t)(K1 / 16) * 6 * W * 16, __float2half(0.f));
+    for (int st = 0; st < K1 / 16; ++st)
+        for (int q = 0; q < 6; ++q)
+            for (int i = 0; i < W; ++i)
+                for (int kk = 0; kk < 16; ++kk) {
+                    __half hi, lo;
+                    split_h(bc_value(q < 4 ? q : q - 4, i, 16 * st + kk), hi, lo);
+                    bs[(size_t)st * 6 * W * 16 + kmajor_off(q * W + i, kk, 16) / 2] = q < 4 ? hi : lo;
+                }
     std::vector<__half> bh, bl, bh2, bl2;
     pack_bc(IC, bh, bl);
     pl->IC2 = W < 16 ? W : 16;
@@ -264,6 +285,7 @@ static SplitPlanHost* get_plan(zola_psf* p, WindowTables* w, std::string& err) {
     up((void**)&pl->d_bc_lo, bl.data(), bl.size() * 2);
     up((void**)&pl->d_bc2_hi, bh2.data(), bh2.size() * 2);
     up((void**)&pl->d_bc2_lo, bl2.data(), bl2.size() * 2);
+    up((void**)&pl->d_bcs, bs.data(), bs.size() * 2);
     up((void**)&pl->d_gt_hi, gh.data(), gh.size() * 2);
     up((void**)&pl->d_gt_lo, gl.data(), gl.size() * 2);
     up((void**)&pl->d_phase0, ph0.data(), ph0.size() * 8);
@@ -287,6 +309,7 @@ void free_split_plan(void* plan) {
     cudaFree(pl->d_bc_lo);
     cudaFree(pl->d_bc2_hi);
     cudaFree(pl->d_bc2_lo);
+    cudaFree(pl->d_bcs);
     cudaFree(pl->d_gt_hi);
     cudaFree(pl->d_gt_lo);
     cudaFree(pl->d_phase0);
@@ -542,107 +565,235 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage1(SplitDev P) {
     if (t < 32) umma::tmem_dealloc(tbase, ncols);
 }
 
-// ----------------------------------------------------------- stage 2 -------
-// One CTA per stage-2 tile (G2 slots x W rows j).
-__global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage2(SplitDev P) {
+// ------------------------------------------------- stage 2 (persistent) -----
+// One CTA per SM walks the stage-2 tiles (G2 slots x W rows j) with the
+// constants resident in shared memory: the K-slabs (16 columns of K1, all 6W
+// rows: hi of parts 0-3, lo of parts 0-1) are loaded once per CTA, so the
+// per-tile traffic is the A2 operand only, streamed in 4 KB K-slabs per array
+// through an NBUF-deep ring by a producer warp.  Per K step, hi x [parts 0-3]
+// produces E and Ex (N up to 256 per instruction), hi x [lo parts 0-1] and
+// lo x [parts 0-1] accumulate onto E, y x [parts 0-1] and z x [parts 0-1]
+// produce Ey and Ez.  The 8W accumulator columns fit TMEM for W <= 64 (one
+// phase); for W = 128 phase A computes E and Ex, its epilogue stores I, lo(I)
+// and I_x and keeps E in registers, and phase B reuses the columns for Ey and
+// Ez.  Warps 0-15 run the epilogues (thread 0 also issues the MMAs), warp 16
+// is the producer.
+constexpr int S2_THREADS = SPLIT_THREADS + 32;
+constexpr int S2_NBUF = 4;
+
+__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, %0;" ::"n"(SPLIT_THREADS) : "memory"); }
+// The same barrier, returning the OR of p over its threads (the same value in every thread).
+__device__ __forceinline__ bool epi_bar_or(bool p) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred P, Q;\n\tsetp.ne.u32 P, %1, 0;\n\t"
+        "bar.red.or.pred Q, 1, %2, P;\n\tselp.u32 %0, 1, 0, Q;\n\t}\n"
+        : "=r"(r)
+        : "r"((uint32_t)p), "n"(SPLIT_THREADS)
+        : "memory");
+    return r != 0;
+}
+
+__host__ __device__ constexpr int s2_ring_bytes(int W) { return (W > 64 ? 2 : 4) * 4096; }
+__host__ __device__ constexpr int s2_slab_bytes(int W) { return 6 * W * 32; }
+
+template <int W>
+__global__ void __launch_bounds__(S2_THREADS, 1) k_stage2p(SplitDev P, int ntiles) {
     extern __shared__ __align__(1024) char smem[];
-    const int K1 = P.K1, IC = P.IC, NCH = P.NCH, W = P.W;
-    const int t = threadIdx.x;
-    const size_t arr = (size_t)128 * K1 * 2;
-    char* A2 = smem;  // hi, lo, y, z
-    char* bcb = A2 + 4 * arr;
-    const int bc_hi_bytes = 4 * IC * K1 * 2, bc_lo_bytes = 2 * IC * K1 * 2;
-    const int bc_buf = bc_hi_bytes + bc_lo_bytes;
-    __shared__ __align__(8) uint64_t a2_full, bc_full[2], mma_done[2];
+    constexpr bool TWO = W > 64;
+    constexpr int SLAB = s2_slab_bytes(W), RING = s2_ring_bytes(W), NBUF = S2_NBUF;
+    constexpr int NCOLS = W >= 64 ? 512 : 256;
+    constexpr int NARR = TWO ? 2 : 4;  // A2 arrays per ring step
+    const int K1 = P.K1, G2 = P.G2, t = threadIdx.x;
+    const int NS = K1 / 16, NSTEP = TWO ? 2 * NS : NS;
+    const uint32_t arr = 128u * K1 * 2;
+    char* CS = smem;                 // NS constant K-slabs
+    char* RB = smem + NS * SLAB;     // ring of A2 K-slabs
+    __shared__ __align__(8) uint64_t cfull, full[NBUF], freed[NBUF], accA, accB;
     __shared__ uint32_t tmem_base;
-    const int ncols = NCH > 1 ? 512 : tmem_cols_pow2(8 * IC);
-    if (!tile_live(P, blockIdx.x * P.G2, P.G2)) return;
-    if (t < 32) umma::tmem_alloc(&tmem_base, ncols);
+    if (t < 32) umma::tmem_alloc(&tmem_base, NCOLS);
     if (t == 0) {
-        umma::mbar_init(&a2_full, 1);
-        umma::mbar_init(&bc_full[0], 1); umma::mbar_init(&bc_full[1], 1);
-        umma::mbar_init(&mma_done[0], 1); umma::mbar_init(&mma_done[1], 1);
+        umma::mbar_init(&cfull, 1);
+        for (int b = 0; b < NBUF; ++b) { umma::mbar_init(&full[b], 1); umma::mbar_init(&freed[b], 1); }
+        umma::mbar_init(&accA, 1);
+        umma::mbar_init(&accB, 1);
         umma::mbar_fence_init();
     }
     __syncthreads();
     umma::fence_after_sync();
     const uint32_t tbase = tmem_base;
-    auto load_bc = [&](int c, int buf) {
-        char* dst = bcb + buf * bc_buf;
-        umma::mbar_expect_tx(&bc_full[buf], bc_buf);
-        umma::bulk_g2s(dst, (const char*)P.bc_hi + (size_t)c * bc_hi_bytes, bc_hi_bytes, &bc_full[buf]);
-        umma::bulk_g2s(dst + bc_hi_bytes, (const char*)P.bc_lo + (size_t)c * bc_lo_bytes, bc_lo_bytes, &bc_full[buf]);
-    };
-    const char* src = P.a2 + (size_t)blockIdx.x * a2_tile_bytes(K1);
-    if (t == 0) {
-        umma::mbar_expect_tx(&a2_full, (uint32_t)(4 * arr));
-        for (int q = 0; q < 4; ++q) umma::bulk_g2s(A2 + q * arr, src + q * arr, (uint32_t)arr, &a2_full);
-        load_bc(0, 0);
-        if (NCH > 1) load_bc(1, 1);
-    }
-    const uint32_t lbo_mn = (128 / 8) * 128, kstep_mn = 2 * lbo_mn, sbo_k = (K1 / 8) * 128;
-    const uint32_t id4 = umma::idesc_f16(128, 4 * IC, true, false);
-    const uint32_t id2 = umma::idesc_f16(128, 2 * IC, true, false);
-    auto issue = [&](int c) {
-        const int buf = NCH > 1 ? (c & 1) : 0;
-        if (c == 0) umma::mbar_wait(&a2_full, 0, P.err);
-        umma::mbar_wait(&bc_full[buf], (c >> 1) & 1, P.err);
-        umma::fence_after_sync();
-        const uint32_t bhi = umma::smem_u32(bcb + buf * bc_buf), blo = bhi + bc_hi_bytes;
-        const uint32_t ahi = umma::smem_u32(A2), alo = ahi + arr, ay = ahi + 2 * arr, az = ahi + 3 * arr;
-        const uint32_t td = tbase + buf * 256;
-        mma_chain(td, ahi, lbo_mn, 128, kstep_mn, bhi, 128, sbo_k, 256, K1, id4, false);
-        mma_chain(td, ahi, lbo_mn, 128, kstep_mn, blo, 128, sbo_k, 256, K1, id2, true);
-        mma_chain(td, alo, lbo_mn, 128, kstep_mn, bhi, 128, sbo_k, 256, K1, id2, true);
-        mma_chain(td + 4 * IC, ay, lbo_mn, 128, kstep_mn, bhi, 128, sbo_k, 256, K1, id2, false);
-        mma_chain(td + 6 * IC, az, lbo_mn, 128, kstep_mn, bhi, 128, sbo_k, 256, K1, id2, false);
-        umma::mma_commit(&mma_done[buf]);
-    };
-    if (t == 0) issue(0);
-    char* a3t = P.a3 + (size_t)blockIdx.x * a3_tile_bytes(W);
-    const size_t arr3 = (size_t)128 * W * 2;
-    const int row = t & 127, wg = t >> 7;
-    for (int c = 0; c < NCH; ++c) {
-        const int buf = NCH > 1 ? (c & 1) : 0;
-        if (t == 0 && c + 1 < NCH) issue(c + 1);
-        umma::mbar_wait(&mma_done[buf], (c >> 1) & 1, P.err);
-        umma::fence_after_sync();
-        const uint32_t col0 = buf * 256;
-        for (int h = wg * 8; h < IC; h += 32) {
-            float er[8], ei[8], xr[8], xi[8];
-            umma::tmem_ld8(tmem_lane_addr(tbase, col0 + 0 * IC + h), er);
-            umma::tmem_ld8(tmem_lane_addr(tbase, col0 + 1 * IC + h), ei);
-            umma::tmem_ld8(tmem_lane_addr(tbase, col0 + 2 * IC + h), xr);
-            umma::tmem_ld8(tmem_lane_addr(tbase, col0 + 3 * IC + h), xi);
-            uint32_t hh[4], ll[4], dx[4], dy[4], dz[4];
-            auto ipx = [&](int u, float cf) { return (er[u] * xr[u] + ei[u] * xi[u]) * cf; };
-#pragma unroll
-            for (int u = 0; u < 8; u += 2) {
-                split2((er[u] * er[u] + ei[u] * ei[u]) * P.sc.cI, (er[u + 1] * er[u + 1] + ei[u + 1] * ei[u + 1]) * P.sc.cI,
-                       hh[u / 2], ll[u / 2]);
-                dx[u / 2] = pack_h2(ipx(u, P.sc.cIx), ipx(u + 1, P.sc.cIx));
+
+    if (t >= SPLIT_THREADS) {  // ---------------- producer warp
+        if (t != SPLIT_THREADS) return;
+        umma::mbar_expect_tx(&cfull, (uint32_t)(NS * SLAB));
+        for (int s = 0; s < NS; ++s)
+            umma::bulk_g2s(CS + s * SLAB, (const char*)P.bcs + (size_t)s * SLAB, SLAB, &cfull);
+        int q = 0;
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+            if (!tile_live(P, tile * G2, G2)) continue;
+            const char* src = P.a2 + (size_t)tile * a2_tile_bytes(K1);
+            for (int n = 0; n < NSTEP; ++n, ++q) {
+                const int buf = q % NBUF;
+                if (q >= NBUF && !umma::mbar_wait(&freed[buf], (uint32_t)((q / NBUF - 1) & 1), P.err)) return;
+                const bool pb = TWO && n >= NS;
+                const int s = pb ? n - NS : n;
+                const int a0 = pb ? 2 : 0;  // phase B streams the y and z arrays
+                umma::mbar_expect_tx(&full[buf], RING);
+                for (int j = 0; j < NARR; ++j)
+                    umma::bulk_g2s(RB + buf * RING + j * 4096, src + (size_t)(a0 + j) * arr + (size_t)s * 4096, 4096,
+                                   &full[buf]);
             }
-            umma::tmem_ld8(tmem_lane_addr(tbase, col0 + 4 * IC + h), xr);
-            umma::tmem_ld8(tmem_lane_addr(tbase, col0 + 5 * IC + h), xi);
-#pragma unroll
-            for (int u = 0; u < 8; u += 2) dy[u / 2] = pack_h2(ipx(u, P.sc.cIy), ipx(u + 1, P.sc.cIy));
-            umma::tmem_ld8(tmem_lane_addr(tbase, col0 + 6 * IC + h), xr);
-            umma::tmem_ld8(tmem_lane_addr(tbase, col0 + 7 * IC + h), xi);
-#pragma unroll
-            for (int u = 0; u < 8; u += 2) dz[u / 2] = pack_h2(ipx(u, P.sc.cIz), ipx(u + 1, P.sc.cIz));
-            const uint32_t off = kmajor_off(row, c * IC + h, W);
-            store4w(a3t + 0 * arr3 + off, hh);
-            store4w(a3t + 1 * arr3 + off, ll);
-            store4w(a3t + 2 * arr3 + off, dx);
-            store4w(a3t + 3 * arr3 + off, dy);
-            store4w(a3t + 4 * arr3 + off, dz);
         }
-        umma::fence_before_sync();
-        __syncthreads();
-        if (t == 0 && c + 2 < NCH) load_bc(c + 2, buf);
+        return;
     }
-    __syncthreads();
-    if (t < 32) umma::tmem_dealloc(tbase, ncols);
+
+    // ---------------- epilogue warps; thread 0 issues the MMAs
+    const int row = t & 127, wg = t >> 7;
+    constexpr int CW = W / 4;  // indices i per warpgroup
+    const size_t arr3 = (size_t)128 * W * 2;
+    const uint32_t lbo_mn = (128 / 8) * 128;
+    int q = 0, ph = 0;
+    auto issue_steps = [&](int n0, int n1) {
+        for (int n = n0; n < n1; ++n, ++q) {
+            const int buf = q % NBUF;
+            if (!umma::mbar_wait(&full[buf], (uint32_t)((q / NBUF) & 1), P.err)) return;
+            umma::fence_after_sync();
+            const uint32_t rb = umma::smem_u32(RB + buf * RING);
+            const bool pb = TWO && n >= NS;
+            const uint32_t cb = umma::smem_u32(CS + (pb ? n - NS : n) * SLAB);
+            const bool first = (pb ? n - NS : n) == 0;
+            auto mma = [&](uint32_t a, int row0, int N, int col, bool acc) {
+                const uint64_t ad = umma::smem_desc(a, lbo_mn, 128);
+                const uint64_t bd = umma::smem_desc(cb + (uint32_t)(row0 / 8) * 256, 128, 256);
+                umma::mma_f16(tbase + col, ad, bd, umma::idesc_f16(128, N, true, false), acc ? 1u : 0u);
+            };
+            if (!pb) {
+#pragma unroll
+                for (int r = 0; r < 4 * W; r += 256) mma(rb, r, 4 * W < 256 ? 4 * W : 256, r, !first);  // E, Ex
+                mma(rb, 4 * W, 2 * W, 0, true);         // + hi x lo(C)
+                mma(rb + 4096, 0, 2 * W, 0, true);      // + lo x hi(C)
+                if (!TWO) {
+                    mma(rb + 8192, 0, 2 * W, 4 * W, !first);   // Ey
+                    mma(rb + 12288, 0, 2 * W, 6 * W, !first);  // Ez
+                }
+            } else {
+                mma(rb, 0, 2 * W, 0, !first);          // Ey
+                mma(rb + 4096, 0, 2 * W, 2 * W, !first);  // Ez
+            }
+            umma::mma_commit(&freed[buf]);
+        }
+    };
+    auto ipx = [](const float* er, const float* ei, const float* xr, const float* xi, int u, float cf) {
+        return (er[u] * xr[u] + ei[u] * xi[u]) * cf;
+    };
+    if (t == 0) umma::mbar_wait(&cfull, 0, P.err);
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        if (!tile_live(P, tile * G2, G2)) continue;
+        char* a3t = P.a3 + (size_t)tile * a3_tile_bytes(W);
+        if (t == 0) {
+            issue_steps(0, NS);
+            umma::mma_commit(&accA);
+        }
+        umma::mbar_wait(&accA, (uint32_t)ph, P.err);
+        umma::fence_after_sync();
+        if constexpr (TWO) {
+            float er[CW], ei[CW];
+#pragma unroll
+            for (int h = 0; h < CW; h += 8) {
+                const int i0 = wg * CW + h;
+                float xr[8], xi[8];
+                umma::tmem_ld8(tmem_lane_addr(tbase, i0), er + h);
+                umma::tmem_ld8(tmem_lane_addr(tbase, W + i0), ei + h);
+                umma::tmem_ld8(tmem_lane_addr(tbase, 2 * W + i0), xr);
+                umma::tmem_ld8(tmem_lane_addr(tbase, 3 * W + i0), xi);
+                uint32_t hh[4], ll[4], dx[4];
+#pragma unroll
+                for (int u = 0; u < 8; u += 2) {
+                    split2((er[h + u] * er[h + u] + ei[h + u] * ei[h + u]) * P.sc.cI,
+                           (er[h + u + 1] * er[h + u + 1] + ei[h + u + 1] * ei[h + u + 1]) * P.sc.cI, hh[u / 2],
+                           ll[u / 2]);
+                    dx[u / 2] = pack_h2(ipx(er + h, ei + h, xr, xi, u, P.sc.cIx),
+                                        ipx(er + h, ei + h, xr, xi, u + 1, P.sc.cIx));
+                }
+                const uint32_t off = kmajor_off(row, i0, W);
+                store4w(a3t + 0 * arr3 + off, hh);
+                store4w(a3t + 1 * arr3 + off, ll);
+                store4w(a3t + 2 * arr3 + off, dx);
+            }
+            umma::fence_before_sync();
+            epi_bar();
+            if (t == 0) {
+                umma::fence_after_sync();
+                issue_steps(NS, NSTEP);
+                umma::mma_commit(&accB);
+            }
+            umma::mbar_wait(&accB, (uint32_t)ph, P.err);
+            umma::fence_after_sync();
+#pragma unroll
+            for (int h = 0; h < CW; h += 8) {
+                const int i0 = wg * CW + h;
+                float xr[8], xi[8];
+                uint32_t dy[4], dz[4];
+                umma::tmem_ld8(tmem_lane_addr(tbase, i0), xr);
+                umma::tmem_ld8(tmem_lane_addr(tbase, W + i0), xi);
+#pragma unroll
+                for (int u = 0; u < 8; u += 2)
+                    dy[u / 2] = pack_h2(ipx(er + h, ei + h, xr, xi, u, P.sc.cIy),
+                                        ipx(er + h, ei + h, xr, xi, u + 1, P.sc.cIy));
+                umma::tmem_ld8(tmem_lane_addr(tbase, 2 * W + i0), xr);
+                umma::tmem_ld8(tmem_lane_addr(tbase, 3 * W + i0), xi);
+#pragma unroll
+                for (int u = 0; u < 8; u += 2)
+                    dz[u / 2] = pack_h2(ipx(er + h, ei + h, xr, xi, u, P.sc.cIz),
+                                        ipx(er + h, ei + h, xr, xi, u + 1, P.sc.cIz));
+                const uint32_t off = kmajor_off(row, i0, W);
+                store4w(a3t + 3 * arr3 + off, dy);
+                store4w(a3t + 4 * arr3 + off, dz);
+            }
+        } else {
+#pragma unroll
+            for (int h = 0; h < CW; h += 8) {
+                const int i0 = wg * CW + h;
+                float er[8], ei[8], xr[8], xi[8];
+                umma::tmem_ld8(tmem_lane_addr(tbase, i0), er);
+                umma::tmem_ld8(tmem_lane_addr(tbase, W + i0), ei);
+                umma::tmem_ld8(tmem_lane_addr(tbase, 2 * W + i0), xr);
+                umma::tmem_ld8(tmem_lane_addr(tbase, 3 * W + i0), xi);
+                uint32_t hh[4], ll[4], dx[4], dy[4], dz[4];
+#pragma unroll
+                for (int u = 0; u < 8; u += 2) {
+                    split2((er[u] * er[u] + ei[u] * ei[u]) * P.sc.cI,
+                           (er[u + 1] * er[u + 1] + ei[u + 1] * ei[u + 1]) * P.sc.cI, hh[u / 2], ll[u / 2]);
+                    dx[u / 2] = pack_h2(ipx(er, ei, xr, xi, u, P.sc.cIx), ipx(er, ei, xr, xi, u + 1, P.sc.cIx));
+                }
+                umma::tmem_ld8(tmem_lane_addr(tbase, 4 * W + i0), xr);
+                umma::tmem_ld8(tmem_lane_addr(tbase, 5 * W + i0), xi);
+#pragma unroll
+                for (int u = 0; u < 8; u += 2)
+                    dy[u / 2] = pack_h2(ipx(er, ei, xr, xi, u, P.sc.cIy), ipx(er, ei, xr, xi, u + 1, P.sc.cIy));
+                umma::tmem_ld8(tmem_lane_addr(tbase, 6 * W + i0), xr);
+                umma::tmem_ld8(tmem_lane_addr(tbase, 7 * W + i0), xi);
+#pragma unroll
+                for (int u = 0; u < 8; u += 2)
+                    dz[u / 2] = pack_h2(ipx(er, ei, xr, xi, u, P.sc.cIz), ipx(er, ei, xr, xi, u + 1, P.sc.cIz));
+                const uint32_t off = kmajor_off(row, i0, W);
+                store4w(a3t + 0 * arr3 + off, hh);
+                store4w(a3t + 1 * arr3 + off, ll);
+                store4w(a3t + 2 * arr3 + off, dx);
+                store4w(a3t + 3 * arr3 + off, dy);
+                store4w(a3t + 4 * arr3 + off, dz);
+            }
+        }
+        // all TMEM reads of this tile done before the next tile's MMAs
+        // (a bounded wait that gave up makes every epilogue thread leave the loop together)
+        umma::fence_before_sync();
+        const bool abort = epi_bar_or(t == 0 && *(volatile int*)P.err != 0);
+        if (t == 0) umma::fence_after_sync();
+        ph ^= 1;
+        if (abort) break;
+    }
+    epi_bar();
+    if (t < 32) umma::tmem_dealloc(tbase, NCOLS);
 }
 
 // ----------------------------------------------------------- stage 3 -------
@@ -1278,7 +1429,9 @@ __global__ void k_init_slots(SplitDev P, const double* init, int n, FitParamsDev
 
 // ---------------------------------------------------------------- host -----
 static size_t smem_stage1(const SplitPlanHost& pl) { return (size_t)768 * pl.K1 + 2 * (size_t)12 * pl.IC * pl.K1; }
-static size_t smem_stage2(const SplitPlanHost& pl) { return (size_t)1024 * pl.K1 + 2 * (size_t)12 * pl.IC * pl.K1; }
+static size_t smem_stage2p(const SplitPlanHost& pl) {
+    return (size_t)(pl.K1 / 16) * s2_slab_bytes(pl.W) + (size_t)S2_NBUF * s2_ring_bytes(pl.W);
+}
 static size_t smem_stage3(const SplitPlanHost& pl) { return (size_t)5 * 128 * pl.W * 2 + (size_t)4 * pl.RP * pl.W; }
 static size_t smem_stage4(const SplitPlanHost& pl) { return (size_t)2 * 128 * pl.W * 2 + (size_t)4 * pl.RP * pl.W; }
 static size_t smem_fused(const SplitPlanHost& pl) {
@@ -1348,6 +1501,23 @@ struct SplitPool {
     size_t s1 = 0, s2 = 0, s3 = 0, s4 = 0, sf = 0;
 };
 
+static cudaError_t stage2_attr(int W, size_t smem) {
+    const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    if (W == 32) return cudaFuncSetAttribute(k_stage2p<32>, a, (int)smem);
+    if (W == 64) return cudaFuncSetAttribute(k_stage2p<64>, a, (int)smem);
+    return cudaFuncSetAttribute(k_stage2p<128>, a, (int)smem);
+}
+
+static void launch_stage2(zola_ctx* ctx, const SplitPool& sp, int ntiles, cudaStream_t st) {
+    const int grid = std::min(ntiles, ctx->num_sms);
+    if (sp.D.W == 32)
+        k_stage2p<32><<<grid, S2_THREADS, sp.s2, st>>>(sp.D, ntiles);
+    else if (sp.D.W == 64)
+        k_stage2p<64><<<grid, S2_THREADS, sp.s2, st>>>(sp.D, ntiles);
+    else
+        k_stage2p<128><<<grid, S2_THREADS, sp.s2, st>>>(sp.D, ntiles);
+}
+
 static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pmax_override, SplitPool& sp,
                       cudaStream_t st) {
     if (p->D > 64) {
@@ -1361,7 +1531,11 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
     SplitPlanHost* pl = get_plan(p, w, ctx->err);
     if (!pl) return ZOLA_E_CUDA;
     sp.pl = pl;
-    sp.s1 = smem_stage1(*pl); sp.s2 = smem_stage2(*pl); sp.s3 = smem_stage3(*pl); sp.s4 = smem_stage4(*pl);
+    if (w->W != 32 && w->W != 64 && w->W != 128) {
+        ctx->err = "split path: window sizes 32, 64 and 128 only";
+        return ZOLA_E_UNSUPPORTED;
+    }
+    sp.s1 = smem_stage1(*pl); sp.s2 = smem_stage2p(*pl); sp.s3 = smem_stage3(*pl); sp.s4 = smem_stage4(*pl);
     if (sp.s1 > 227 * 1024 || sp.s2 > 227 * 1024 || sp.s3 > 227 * 1024 || sp.s4 > 227 * 1024) {
         ctx->err = "split path: shared-memory plan exceeds 227 KB";
         return ZOLA_E_UNSUPPORTED;
@@ -1387,7 +1561,7 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
     D.RP = pl->RP; D.G1 = pl->G1; D.G2 = pl->G2; D.NT4 = pl->NT4; D.P = P; D.a0 = p->a0; D.N = p->N;
     D.zfocus = p->o.zfocus;
     D.bc_hi = pl->d_bc_hi; D.bc_lo = pl->d_bc_lo; D.gt_hi = pl->d_gt_hi; D.gt_lo = pl->d_gt_lo;
-    D.bc2_hi = pl->d_bc2_hi; D.bc2_lo = pl->d_bc2_lo; D.NCH2 = pl->NCH2;
+    D.bc2_hi = pl->d_bc2_hi; D.bc2_lo = pl->d_bc2_lo; D.NCH2 = pl->NCH2; D.bcs = pl->d_bcs;
     D.pupf = pl->d_pupf; D.phase0 = pl->d_phase0; D.kz = pl->d_kz; D.kx = pl->d_kx; D.ky = pl->d_ky;
     D.a2 = base; base += b_a2;
     D.a3 = base; base += b_a3;
@@ -1402,7 +1576,7 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
     D.sc = pl->sc;
     ZOLA_CUDA_CHECK(cudaMemsetAsync(D.a4, 0, b_a4, st), ctx);
     ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_stage1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.s1), ctx);
-    ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_stage2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.s2), ctx);
+    ZOLA_CUDA_CHECK(stage2_attr(pl->W, sp.s2), ctx);
     ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_stage3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.s3), ctx);
     ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_stage4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.s4), ctx);
     sp.sf = smem_fused(*pl);
@@ -1418,7 +1592,7 @@ static void launch_model_stages(zola_ctx* ctx, const SplitPool& sp, cudaStream_t
     k_stage1<<<P / pl.G1, SPLIT_THREADS, sp.s1, st>>>(sp.D);
     prof_end(ctx, st);
     prof_begin(ctx, 1, st);
-    k_stage2<<<P / pl.G2, SPLIT_THREADS, sp.s2, st>>>(sp.D);
+    launch_stage2(ctx, sp, P / pl.G2, st);
     prof_end(ctx, st);
     prof_begin(ctx, 2, st);
     k_stage3<<<P / pl.G2, SPLIT_THREADS, sp.s3, st>>>(sp.D);
