@@ -47,9 +47,9 @@ using umma::mnmajor_off;
 
 // Stages 1-4 run 512 threads: four warpgroups share the 128 TMEM lanes (lane
 // quadrant = warp % 4, so thread t owns tile row t % 128) and split the column
-// work of every epilogue and of the Q build; stage 5 runs 128 threads per slot.
+// work of every epilogue and of the Q build; the LM step runs one thread per slot.
 constexpr int SPLIT_THREADS = 512;
-constexpr int LIK_THREADS = 128;
+constexpr int LM_THREADS = 128;
 
 // ---------------------------------------------------------------- plan ------
 struct SplitScales {
@@ -74,6 +74,8 @@ struct SplitDev {
     const __half* bcs;    // K1/16 K-slabs of 6W x 16 (wide stage kernels)
     const __half* gt_hi;  // RP x W (K-major)
     const __half* gt_lo;
+    const __half* g128_hi;  // 128 x W (K-major, rows >= R zero): the column-blur A operand
+    const __half* g128_lo;
     // pupil tables padded to DP x DP (row a <-> kx, column b <-> ky; zero
     // beyond the D disk rows and columns), in the warp-load order of stage 1
     const float* pupf;     // pupil (the model uses it in FP32)
@@ -85,7 +87,8 @@ struct SplitDev {
     char* a2;      // P/G2 tiles x 4 arrays x 128 x K1 f16
     char* a3;      // P/G2 tiles x 5 arrays x 128 x W f16
     char* a4;      // P x NT4 tiles x 2 arrays x 128 x W f16
-    float* tmaps;  // P x 4 x R x R
+    float* tmaps;  // P x 4 x R x R (model-only evaluation)
+    double* sums;  // P x NSUM likelihood sums (fit)
     // slot state
     int* slot_roi;
     int* slot_phase;
@@ -107,6 +110,8 @@ struct SplitPlanHost {
     __half* d_bcs = nullptr;
     __half* d_gt_hi = nullptr;
     __half* d_gt_lo = nullptr;
+    __half* d_g128_hi = nullptr;
+    __half* d_g128_lo = nullptr;
     double* d_phase0 = nullptr;  // DP x DP
     double* d_kz = nullptr;      // DP x DP
     float* d_pupf = nullptr;     // DP x DP
@@ -122,6 +127,9 @@ static double pow2scale(double bound) {
 __host__ __device__ inline size_t a2_tile_bytes(int K1) { return (size_t)4 * 128 * K1 * 2; }
 __host__ __device__ inline size_t a3_tile_bytes(int W) { return (size_t)5 * 128 * W * 2; }
 __host__ __device__ inline size_t a4_tile_bytes(int W) { return (size_t)2 * 128 * W * 2; }
+// Row-blurred maps J of one slot as the column-blur B operand: hi then lo, each
+// MN-major with N = 4 RP rows n = (map, i') and K = W columns j.
+__host__ __device__ inline size_t a4_slot_bytes(int W, int RP) { return (size_t)2 * 4 * RP * W * 2; }
 // Row stride (floats) of the fused kernel's shared-memory maps: a multiple of 4
 // congruent to 4 mod 32, so that 32 lanes storing float4 at consecutive rows
 // cover all banks once per 8 lanes.
@@ -255,6 +263,12 @@ static SplitPlanHost* get_plan(zola_psf* p, WindowTables* w, std::string& err) {
             gh[kmajor_off(ip, i, W) / 2] = hi;
             gl[kmajor_off(ip, i, W) / 2] = lo;
         }
+    std::vector<__half> g1h((size_t)128 * W, __float2half(0.f)), g1l((size_t)128 * W, __float2half(0.f));
+    for (int ip = 0; ip < R; ++ip)
+        for (int i = 0; i < W; ++i) {
+            g1h[kmajor_off(ip, i, W) / 2] = gh[kmajor_off(ip, i, W) / 2];
+            g1l[kmajor_off(ip, i, W) / 2] = gl[kmajor_off(ip, i, W) / 2];
+        }
     // phase0 = phase - kzoil * zfocus (the zoil term of PSFPhase.java:560 with zoil = Zfocus),
     // padded to DP x DP with the other pupil tables
     std::vector<double> ph0((size_t)DP * DP, 0.0), kzp((size_t)DP * DP, 0.0), kxp(DP, 0.0), kyp(DP, 0.0);
@@ -288,6 +302,8 @@ static SplitPlanHost* get_plan(zola_psf* p, WindowTables* w, std::string& err) {
     up((void**)&pl->d_bcs, bs.data(), bs.size() * 2);
     up((void**)&pl->d_gt_hi, gh.data(), gh.size() * 2);
     up((void**)&pl->d_gt_lo, gl.data(), gl.size() * 2);
+    up((void**)&pl->d_g128_hi, g1h.data(), g1h.size() * 2);
+    up((void**)&pl->d_g128_lo, g1l.data(), g1l.size() * 2);
     up((void**)&pl->d_phase0, ph0.data(), ph0.size() * 8);
     up((void**)&pl->d_kz, kzp.data(), kzp.size() * 8);
     up((void**)&pl->d_pupf, pupf.data(), pupf.size() * 4);
@@ -312,6 +328,8 @@ void free_split_plan(void* plan) {
     cudaFree(pl->d_bcs);
     cudaFree(pl->d_gt_hi);
     cudaFree(pl->d_gt_lo);
+    cudaFree(pl->d_g128_hi);
+    cudaFree(pl->d_g128_lo);
     cudaFree(pl->d_phase0);
     cudaFree(pl->d_kz);
     cudaFree(pl->d_pupf);
@@ -581,15 +599,18 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage1(SplitDev P) {
 constexpr int S2_THREADS = SPLIT_THREADS + 32;
 constexpr int S2_NBUF = 4;
 
-__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, %0;" ::"n"(SPLIT_THREADS) : "memory"); }
+// Named barrier 1 over the first N threads of the CTA (the epilogue warps).
+template <int N = SPLIT_THREADS>
+__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, %0;" ::"n"(N) : "memory"); }
 // The same barrier, returning the OR of p over its threads (the same value in every thread).
+template <int N = SPLIT_THREADS>
 __device__ __forceinline__ bool epi_bar_or(bool p) {
     uint32_t r;
     asm volatile(
         "{\n\t.reg .pred P, Q;\n\tsetp.ne.u32 P, %1, 0;\n\t"
         "bar.red.or.pred Q, 1, %2, P;\n\tselp.u32 %0, 1, 0, Q;\n\t}\n"
         : "=r"(r)
-        : "r"((uint32_t)p), "n"(SPLIT_THREADS)
+        : "r"((uint32_t)p), "n"(N)
         : "memory");
     return r != 0;
 }
@@ -842,20 +863,20 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage3(SplitDev P) {
     const int row = t & 127, m = t >> 7;
     const int g2 = row / W, j = row % W;
     const int slot = blockIdx.x * P.G2 + g2;
-    char* a4s = P.a4 + (size_t)slot * P.NT4 * a4_tile_bytes(W);
-    const size_t arr4 = (size_t)128 * W * 2;
+    const int NT = 4 * RP;
+    char* a4s = P.a4 + (size_t)slot * a4_slot_bytes(W, RP);
+    const size_t arrJ = (size_t)NT * W * 2;
     for (int h = 0; h < RP; h += 16) {
         float v[16];
         umma::tmem_ld16(tmem_lane_addr(tbase, m * RP + h), v);
         for (int i8 = 0; i8 < 16; i8 += 8) {
-            const int r = m * RP + h + i8;
-            char* tile = a4s + (size_t)(r / 128) * a4_tile_bytes(W);
+            const int r = m * RP + h + i8;  // n = (map, i')
             uint32_t hh[4], ll[4];
 #pragma unroll
             for (int u = 0; u < 8; u += 2) split2(v[i8 + u] * P.sc.cJ[m], v[i8 + u + 1] * P.sc.cJ[m], hh[u / 2], ll[u / 2]);
-            const uint32_t off = mnmajor_off(r % 128, j, 128);
-            store4w(tile + off, hh);
-            store4w(tile + arr4 + off, ll);
+            const uint32_t off = mnmajor_off(r, j, NT);
+            store4w(a4s + off, hh);
+            store4w(a4s + arrJ + off, ll);
         }
     }
     umma::fence_before_sync();
@@ -864,17 +885,21 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage3(SplitDev P) {
 }
 
 // ----------------------------------------------------------- stage 4 -------
-// Blur along the second index: T[(map, i')][j'] = sum_j J[i'][j] G[j'][j].
+// Blur along the second index, transposed so that one pixel column lands in
+// one TMEM lane: T^T[j'][(map, i')] = sum_j G[j'][j] J[(map, i')][j]
+// (A = G padded to 128 rows, B = the slot's J with N = 4 RP).  Model-only
+// evaluation: one CTA per slot writes the FP32 maps.
 __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage4(SplitDev P) {
     extern __shared__ __align__(1024) char smem[];
-    const int W = P.W, RP = P.RP, R = P.R, t = threadIdx.x;
-    const size_t arr4 = (size_t)128 * W * 2, gbytes = (size_t)RP * W * 2;
-    char* A4 = smem;  // hi, lo
-    char* GT = A4 + 2 * arr4;
+    const int W = P.W, RP = P.RP, R = P.R, NT = 4 * RP, t = threadIdx.x;
+    const uint32_t jarr = (uint32_t)NT * W * 2, garr = 128u * W * 2;
+    char* J = smem;  // hi, lo
+    char* G = J + 2 * jarr;
     __shared__ __align__(8) uint64_t full, done;
     __shared__ uint32_t tmem_base;
-    const int ncols = tmem_cols_pow2(RP);
-    if (!tile_live(P, blockIdx.x / P.NT4, 1)) return;
+    const int slot = blockIdx.x;
+    if (P.slot_roi[slot] < 0) return;
+    const int ncols = tmem_cols_pow2(NT);
     if (t < 32) umma::tmem_alloc(&tmem_base, ncols);
     if (t == 0) {
         umma::mbar_init(&full, 1);
@@ -884,36 +909,32 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage4(SplitDev P) {
     __syncthreads();
     umma::fence_after_sync();
     const uint32_t tbase = tmem_base;
-    const int slot = blockIdx.x / P.NT4, tile = blockIdx.x % P.NT4;
     if (t == 0) {
-        umma::mbar_expect_tx(&full, (uint32_t)(2 * arr4 + 2 * gbytes));
-        const char* src = P.a4 + (size_t)blockIdx.x * a4_tile_bytes(W);
-        umma::bulk_g2s(A4, src, (uint32_t)(2 * arr4), &full);
-        umma::bulk_g2s(GT, P.gt_hi, (uint32_t)gbytes, &full);
-        umma::bulk_g2s(GT + gbytes, P.gt_lo, (uint32_t)gbytes, &full);
-        umma::mbar_wait(&full, 0, P.err);
-        umma::fence_after_sync();
-        const uint32_t lbo_mn = (128 / 8) * 128, kstep_mn = 2 * lbo_mn, sbo_k = (W / 8) * 128;
-        const uint32_t id = umma::idesc_f16(128, RP, true, false);
-        const uint32_t ahi = umma::smem_u32(A4), alo = ahi + (uint32_t)arr4;
-        const uint32_t ghi = umma::smem_u32(GT), glo = ghi + (uint32_t)gbytes;
-        mma_chain(tbase, ahi, lbo_mn, 128, kstep_mn, ghi, 128, sbo_k, 256, W, id, false);
-        mma_chain(tbase, ahi, lbo_mn, 128, kstep_mn, glo, 128, sbo_k, 256, W, id, true);
-        mma_chain(tbase, alo, lbo_mn, 128, kstep_mn, ghi, 128, sbo_k, 256, W, id, true);
+        umma::mbar_expect_tx(&full, 2 * jarr + 2 * garr);
+        umma::bulk_g2s(J, P.a4 + (size_t)slot * a4_slot_bytes(W, RP), 2 * jarr, &full);
+        umma::bulk_g2s(G, P.g128_hi, garr, &full);
+        umma::bulk_g2s(G + garr, P.g128_lo, garr, &full);
+        if (umma::mbar_wait(&full, 0, P.err)) {
+            umma::fence_after_sync();
+            const uint32_t id = umma::idesc_f16(128, NT, false, true);
+            const uint32_t ghi = umma::smem_u32(G), glo = ghi + garr, jhi = umma::smem_u32(J), jlo = jhi + jarr;
+            const uint32_t sbo_g = (W / 8) * 128, lbo_j = (NT / 8) * 128, kstep_j = 2 * lbo_j;
+            mma_chain(tbase, ghi, 128, sbo_g, 256, jhi, lbo_j, 128, kstep_j, W, id, false);
+            mma_chain(tbase, glo, 128, sbo_g, 256, jhi, lbo_j, 128, kstep_j, W, id, true);
+            mma_chain(tbase, ghi, 128, sbo_g, 256, jlo, lbo_j, 128, kstep_j, W, id, true);
+        }
         umma::mma_commit(&done);
     }
     umma::mbar_wait(&done, 0, P.err);
     umma::fence_after_sync();
-    const int row = t & 127, wg = t >> 7;
-    const int r = tile * 128 + row, map = r / RP, ip = r % RP;
-    const int cq = RP / 4;
-    for (int h = wg * cq; h < (wg + 1) * cq; h += 4) {
+    // thread: pixel column j' = its TMEM lane, map = its warpgroup, rows i' = 0..RP-1
+    const int jp = t & 127, map = t >> 7;
+    float* dst = P.tmaps + ((size_t)slot * 4 + map) * R * R;
+    for (int h = 0; h < RP; h += 4) {
         float v[4];
-        umma::tmem_ld4(tmem_lane_addr(tbase, h), v);
-        if (map < 4 && ip < R) {
-            float* dst = P.tmaps + (((size_t)slot * 4 + map) * R + ip) * R;
-            for (int u = 0; u < 4 && h + u < R; ++u) dst[h + u] = v[u] * P.sc.cT[map];
-        }
+        umma::tmem_ld4(tmem_lane_addr(tbase, map * RP + h), v);
+        if (jp < R)
+            for (int u = 0; u < 4 && h + u < R; ++u) dst[(size_t)(h + u) * R + jp] = v[u] * P.sc.cT[map];
     }
     umma::fence_before_sync();
     __syncthreads();
@@ -922,8 +943,6 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage4(SplitDev P) {
 
 // ----------------------------------------------------------- stage 5 -------
 constexpr int NRED = 1 + 5 + 15 + 15;
-constexpr int LIK_SLOTS = LIK_THREADS / 32;  // one warp per slot
-constexpr int S5_UNROLL = 4;                  // pixels per lane whose loads are in flight together
 
 __device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
     float y = v - c;
@@ -938,16 +957,20 @@ __device__ __forceinline__ double warp_sum(double x) {
     return x;
 }
 
+constexpr int S5_THREADS = 128;
+constexpr int S5_SLOTS = S5_THREADS / 32;  // one warp per slot
+constexpr int S5_UNROLL = 4;               // pixels per lane whose loads are in flight together
+
 // One warp per slot: likelihood sums at the trial point (per-pixel terms in
 // FP32; the likelihood and gradient with Kahan compensation, the Hessian and
 // Fisher terms plain; lane partials combined in FP64), then the FP64 LM step on
 // lane 0.
-__global__ void __launch_bounds__(LIK_THREADS) k_stage5(SplitDev P, const float* rois, const float* scmos,
+__global__ void __launch_bounds__(S5_THREADS) k_stage5(SplitDev P, const float* rois, const float* scmos,
                                                         const double* init, int n,
                                                         FitParamsDev prm, double* out5, double* crlb5,
                                                         double* nll_out, int* st_out, int* it_out) {
     const int lane = threadIdx.x & 31;
-    const int slot = blockIdx.x * LIK_SLOTS + (threadIdx.x >> 5);
+    const int slot = blockIdx.x * S5_SLOTS + (threadIdx.x >> 5);
     if (slot >= P.P) return;
     const int roi = P.slot_roi[slot];
     if (roi < 0) return;
@@ -1038,6 +1061,316 @@ __global__ void __launch_bounds__(LIK_THREADS) k_stage5(SplitDev P, const float*
     const bool anybad = __any_sync(0xffffffffu, bad);
     if (lane != 0) return;
     double nll = anybad ? INFINITY : tot[0], g[5], H[25], F[25];
+    for (int q = 0; q < 5; ++q) g[q] = tot[1 + q];
+    int o = 6;
+    for (int q = 0; q < 5; ++q)
+        for (int r2 = 0; r2 <= q; ++r2) {
+            H[q * 5 + r2] = H[r2 * 5 + q] = tot[o];
+            F[q * 5 + r2] = F[r2 * 5 + q] = tot[o + 15];
+            ++o;
+        }
+    LMState& st = P.lm[slot];
+    if (P.slot_phase[slot] == 0) {
+        for (int q = 0; q < 5; ++q) st.th[q] = st.trial[q];
+        lm_start(st, nll, g, H, F, prm);
+        P.slot_phase[slot] = 1;
+    } else {
+        lm_update(st, nll, g, H, F, prm);
+    }
+    if (lm_propose(st, prm)) return;
+    // retire
+    for (int q = 0; q < 5; ++q) out5[5 * roi + q] = st.th[q];
+    if (nll_out) nll_out[roi] = st.nll;
+    if (st_out) st_out[roi] = st.status;
+    if (it_out) it_out[roi] = st.evals;
+    if (crlb5) lm_crlb(st.F, crlb5 + 5 * roi);
+    // refill from the queue
+    const int next = atomicAdd(P.queue, 1);
+    if (next < n) {
+        P.slot_roi[slot] = next;
+        P.slot_phase[slot] = 0;
+        for (int q = 0; q < 5; ++q) st.trial[q] = init[5 * next + q];
+        lm_clamp(st.trial, prm);
+    } else {
+        P.slot_roi[slot] = -1;
+        atomicSub(P.active, 1);
+    }
+}
+
+// ---------------------------------- stages 4 + 5 sums (persistent) -----
+// One CTA per SM walks the occupied slots.  The column blur is computed
+// transposed, T^T[j'][(map, i')] = sum_j G[j'][j] J[(map, i')][j] (A = G
+// padded to 128 rows, resident in shared memory; B = the slot's J, N = 4 RP,
+// streamed in K-slabs by a producer warp; three FP16 products per K step
+// issued by an MMA warp into one of two TMEM buffers), so TMEM lane j' holds
+// all four maps of pixel column j'.  The epilogue warps read them straight
+// from TMEM and form the normalisation, likelihood, gradient, Gauss-Newton
+// Hessian and Fisher sums (process/cpu/Localization.java:1125-1143 with the
+// Jacobian of psi = |T|/sum|T| of PSFPhase.java:602-629): per-pixel terms in
+// FP32, likelihood and gradient with Kahan compensation, thread partials
+// combined in FP64.  The next slot's MMAs run in the other TMEM buffer
+// meanwhile.  The sums and a non-positive-model flag go to P.sums; k_lm
+// applies the FP64 LM step.
+constexpr int NSUM = NRED + 1;
+constexpr int E45_THREADS = 384;                 // 12 epilogue warps: three per TMEM lane quadrant
+constexpr int S45_THREADS = E45_THREADS + 64;    // + producer warp + MMA warp
+constexpr int S45_NBUF = 4;
+constexpr int S45_MIN_R = 40;  // ROI side from which the fused form is faster
+
+__host__ __device__ inline size_t s45_roi_bytes(int R) { return ((size_t)R * R * 4 + 127) / 128 * 128; }
+
+__device__ __forceinline__ void warp_arrive(uint64_t* mbar) {
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) umma::mbar_arrive(mbar);
+}
+
+__global__ void __launch_bounds__(S45_THREADS, 1) k_stage45p(SplitDev P, const float* rois, const float* scmos) {
+    extern __shared__ __align__(1024) char smem[];
+    const int W = P.W, RP = P.RP, R = P.R, NT = 4 * RP, RR = R * R, t = threadIdx.x;
+    const int warp = t >> 5, lane = t & 31, NS4 = W / 16;
+    const uint32_t garr = 128u * W * 2, kslab = 32u * NT, ringb = 2 * kslab, roib = (uint32_t)s45_roi_bytes(R);
+    char* G = smem;                      // G hi, lo
+    char* RG = G + 2 * garr;             // ring of J K-slabs (hi, lo)
+    char* RO = RG + S45_NBUF * ringb;    // two buffers of (ROI, sCMOS variance)
+    float* Tm = (float*)(RO + 4 * roib); // the slot's four FP32 maps, row stride RS
+    const int RS = tm_stride(R), MS = R * RS;
+    const bool vec = (R % 2) == 0;       // whole 16-byte units: ROI copies by TMA
+    __shared__ __align__(8) uint64_t gfull, full[S45_NBUF], freed[S45_NBUF], acc[2], tfree[2], rfull[2], rfree[2], fin;
+    __shared__ uint32_t tmem_base;
+    __shared__ double red[E45_THREADS / 32][NRED];
+    __shared__ int bad_w[E45_THREADS / 32];
+    const int ncols = tmem_cols_pow2(2 * NT);
+    if (t < 32) umma::tmem_alloc(&tmem_base, ncols);
+    if (t == 0) {
+        umma::mbar_init(&gfull, 1);
+        for (int b = 0; b < S45_NBUF; ++b) { umma::mbar_init(&full[b], 1); umma::mbar_init(&freed[b], 1); }
+        for (int b = 0; b < 2; ++b) {
+            umma::mbar_init(&acc[b], 1);
+            umma::mbar_init(&tfree[b], E45_THREADS / 32);
+            umma::mbar_init(&rfull[b], 1);
+            umma::mbar_init(&rfree[b], E45_THREADS / 32);
+        }
+        umma::mbar_init(&fin, 1);
+        umma::mbar_fence_init();
+    }
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tbase = tmem_base;
+
+    if (warp == E45_THREADS / 32) {  // ---------------- producer
+        if (lane != 0) return;
+        umma::mbar_expect_tx(&gfull, 2 * garr);
+        umma::bulk_g2s(G, P.g128_hi, garr, &gfull);
+        umma::bulk_g2s(G + garr, P.g128_lo, garr, &gfull);
+        int q = 0, n = 0;
+        bool ok = true;
+        for (int slot = blockIdx.x; slot < P.P && ok; slot += gridDim.x) {
+            const int roi = P.slot_roi[slot];
+            if (roi < 0) continue;
+            const int b = n & 1;
+            if (vec) {
+                if (n >= 2 && !umma::mbar_wait(&rfree[b], (uint32_t)(((n >> 1) - 1) & 1), P.err)) break;
+                char* dst = RO + b * 2 * roib;
+                umma::mbar_expect_tx(&rfull[b], (scmos ? 2u : 1u) * RR * 4);
+                umma::bulk_g2s(dst, rois + (size_t)roi * RR, RR * 4, &rfull[b]);
+                if (scmos) umma::bulk_g2s(dst + roib, scmos + (size_t)roi * RR, RR * 4, &rfull[b]);
+            }
+            ++n;
+            const char* src = P.a4 + (size_t)slot * a4_slot_bytes(W, RP);
+            for (int s = 0; s < NS4; ++s, ++q) {
+                const int buf = q % S45_NBUF;
+                if (q >= S45_NBUF && !umma::mbar_wait(&freed[buf], (uint32_t)((q / S45_NBUF - 1) & 1), P.err)) {
+                    ok = false;
+                    break;
+                }
+                umma::mbar_expect_tx(&full[buf], ringb);
+                umma::bulk_g2s(RG + buf * ringb, src + (size_t)s * kslab, kslab, &full[buf]);
+                umma::bulk_g2s(RG + buf * ringb + kslab, src + (size_t)NT * W * 2 + (size_t)s * kslab, kslab, &full[buf]);
+            }
+        }
+        // copies still in flight land before the CTA can exit
+        umma::mbar_wait(&gfull, 0, P.err);
+        for (int j = q > S45_NBUF ? q - S45_NBUF : 0; j < q; ++j)
+            umma::mbar_wait(&full[j % S45_NBUF], (uint32_t)((j / S45_NBUF) & 1), P.err);
+        if (vec)
+            for (int m = n > 2 ? n - 2 : 0; m < n; ++m) umma::mbar_wait(&rfull[m & 1], (uint32_t)((m >> 1) & 1), P.err);
+        return;
+    }
+    if (warp == E45_THREADS / 32 + 1) {  // ---------------- MMA issuer
+        if (lane != 0) return;
+        const uint32_t id = umma::idesc_f16(128, NT, false, true);
+        const uint32_t sbo_g = (W / 8) * 128, lbo_j = (NT / 8) * 128;
+        const uint32_t ghi = umma::smem_u32(G), glo = ghi + garr;
+        bool ok = umma::mbar_wait(&gfull, 0, P.err);
+        int q = 0, n = 0;
+        for (int slot = blockIdx.x; slot < P.P && ok; slot += gridDim.x) {
+            if (P.slot_roi[slot] < 0) continue;
+            const int b = n & 1;
+            if (n >= 2 && !umma::mbar_wait(&tfree[b], (uint32_t)(((n >> 1) - 1) & 1), P.err)) break;
+            umma::fence_after_sync();
+            const uint32_t td = tbase + b * NT;
+            for (int s = 0; s < NS4; ++s, ++q) {
+                const int buf = q % S45_NBUF;
+                if (!umma::mbar_wait(&full[buf], (uint32_t)((q / S45_NBUF) & 1), P.err)) { ok = false; break; }
+                umma::fence_after_sync();
+                const uint32_t jhi = umma::smem_u32(RG + buf * ringb), jlo = jhi + kslab;
+                const uint64_t gh = umma::smem_desc(ghi + s * 256, 128, sbo_g), gl = umma::smem_desc(glo + s * 256, 128, sbo_g);
+                const uint64_t bh = umma::smem_desc(jhi, lbo_j, 128), bl = umma::smem_desc(jlo, lbo_j, 128);
+                umma::mma_f16(td, gh, bh, id, s > 0 ? 1u : 0u);
+                umma::mma_f16(td, gl, bh, id, 1u);
+                umma::mma_f16(td, gh, bl, id, 1u);
+                umma::mma_commit(&freed[buf]);
+            }
+            umma::mma_commit(&acc[b]);
+            ++n;
+        }
+        umma::mma_commit(&fin);
+        return;
+    }
+
+    // ---------------- epilogue warps.  The maps go from TMEM (lane = pixel column j') to
+    // shared memory, which frees the TMEM buffer for the slot after next; the pixel sums
+    // then run over all epilogue threads.
+    const int jp = (warp & 3) * 32 + lane, wg = warp >> 2;
+    constexpr int NWG = E45_THREADS / 128, NW = E45_THREADS / 32;
+    int n = 0;
+    for (int slot = blockIdx.x; slot < P.P; slot += gridDim.x) {
+        const int roi = P.slot_roi[slot];
+        if (roi < 0) continue;
+        const int b = n & 1;
+        const uint32_t ph = (uint32_t)((n >> 1) & 1);
+        ++n;
+        umma::mbar_wait(&acc[b], ph, P.err);
+        umma::fence_after_sync();
+        const uint32_t tb = tbase + b * NT;
+        for (int c0 = 4 * wg; c0 < RP; c0 += 4 * NWG) {
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                float v[4];
+                umma::tmem_ld4(tmem_lane_addr(tb, m * RP + c0), v);
+                if (jp < R)
+                    for (int u = 0; u < 4 && c0 + u < R; ++u) Tm[m * MS + (c0 + u) * RS + jp] = v[u] * P.sc.cT[m];
+            }
+        }
+        umma::fence_before_sync();
+        warp_arrive(&tfree[b]);
+        if (vec) umma::mbar_wait(&rfull[b], ph, P.err);
+        epi_bar<E45_THREADS>();
+        // normalisation sums
+        float ns[4] = {0, 0, 0, 0}, nc = 0.f;
+        for (int k = t; k < RR; k += E45_THREADS) {
+            const int ip = k / R, o = ip * RS + (k - ip * R);
+            const float v = Tm[o], sg = v < 0 ? -1.f : 1.f;
+            kahan_add(ns[0], nc, fabsf(v));
+            ns[1] += sg * Tm[MS + o];
+            ns[2] += sg * Tm[2 * MS + o];
+            ns[3] += sg * Tm[3 * MS + o];
+        }
+        {
+            const double v0 = warp_sum((double)ns[0] - (double)nc), v1 = warp_sum(ns[1]), v2 = warp_sum(ns[2]),
+                         v3 = warp_sum(ns[3]);
+            if (lane == 0) { red[warp][0] = v0; red[warp][1] = v1; red[warp][2] = v2; red[warp][3] = v3; }
+        }
+        epi_bar<E45_THREADS>();
+        double sum4[4] = {0, 0, 0, 0};
+        for (int w = 0; w < NW; ++w)
+            for (int q = 0; q < 4; ++q) sum4[q] += red[w][q];
+        epi_bar<E45_THREADS>();
+        const float S = (float)sum4[0], Dx = (float)sum4[1], Dy = (float)sum4[2], Dz = (float)sum4[3];
+        const float invS = 1.f / S;
+        const double* th = P.lm[slot].trial;
+        const float A = (float)th[3], B = (float)th[4];
+        const float* d = vec ? (const float*)(RO + b * 2 * roib) : rois + (size_t)roi * RR;
+        const float* sv = !scmos ? nullptr : vec ? (const float*)(RO + b * 2 * roib + roib) : scmos + (size_t)roi * RR;
+        float sg6[6], cg6[6], sh[30];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) { sg6[k] = 0.f; cg6[k] = 0.f; }
+#pragma unroll
+        for (int k = 0; k < 30; ++k) sh[k] = 0.f;
+        bool bad = false;
+        for (int k = t; k < RR; k += E45_THREADS) {
+            const int ip = k / R, to = ip * RS + (k - ip * R);
+            const float v = Tm[to], sgn = v < 0 ? -1.f : 1.f, psi = fabsf(v) * invS;
+            float jv[5];
+            jv[0] = A * (sgn * Tm[MS + to] - psi * Dx) * invS;
+            jv[1] = A * (sgn * Tm[2 * MS + to] - psi * Dy) * invS;
+            jv[2] = A * (sgn * Tm[3 * MS + to] - psi * Dz) * invS;
+            jv[3] = psi;
+            jv[4] = 1.f;
+            const float mu = A * psi + B + (sv ? sv[k] : 0.f);
+            if (!(mu > 0.f)) { bad = true; continue; }
+            const float dk = d[k];
+            kahan_add(sg6[0], cg6[0], dk > 0.f ? mu - dk - dk * logf(mu / dk) : mu);
+            const float wgt = 1.f - dk / mu, wf = 1.f / mu, wh = dk * wf * wf;
+#pragma unroll
+            for (int q = 0; q < 5; ++q) kahan_add(sg6[1 + q], cg6[1 + q], wgt * jv[q]);
+            int o = 0;
+#pragma unroll
+            for (int q = 0; q < 5; ++q)
+#pragma unroll
+                for (int r2 = 0; r2 <= q; ++r2) {
+                    sh[o] += wh * jv[q] * jv[r2];
+                    sh[o + 15] += wf * jv[q] * jv[r2];
+                    ++o;
+                }
+        }
+        if (vec) warp_arrive(&rfree[b]);  // this slot's ROI buffer is free for the slot after next
+        // 36 sums per thread -> per warp: a butterfly reduce-scatter leaves sum k on lane k
+        // (k < 32); the last four reduce plainly
+        {
+            double v[32];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) v[k] = (double)sg6[k] - (double)cg6[k];
+#pragma unroll
+            for (int k = 0; k < 26; ++k) v[6 + k] = sh[k];
+#pragma unroll
+            for (int h = 16; h >= 1; h >>= 1) {
+                const bool up = (lane & h) != 0;
+#pragma unroll
+                for (int i = 0; i < h; ++i) {
+                    const double send = up ? v[i] : v[i + h], keep = up ? v[i + h] : v[i];
+                    v[i] = keep + __shfl_xor_sync(0xffffffffu, send, h);
+                }
+            }
+            red[warp][lane] = v[0];
+#pragma unroll
+            for (int k = 26; k < 30; ++k) {
+                const double x = warp_sum((double)sh[k]);
+                if (lane == 0) red[warp][6 + k] = x;
+            }
+        }
+        const bool wbad = __any_sync(0xffffffffu, bad);
+        if (lane == 0) bad_w[warp] = wbad;
+        epi_bar<E45_THREADS>();
+        if (t < NRED) {
+            double v = 0;
+            for (int w = 0; w < NW; ++w) v += red[w][t];
+            P.sums[(size_t)slot * NSUM + t] = v;
+        }
+        if (t == NRED) {
+            int any = 0;
+            for (int w = 0; w < NW; ++w) any |= bad_w[w];
+            P.sums[(size_t)slot * NSUM + NRED] = any ? 1.0 : 0.0;
+        }
+        // (a bounded wait that gave up makes every epilogue thread leave the loop together)
+        if (epi_bar_or<E45_THREADS>(t == 0 && *(volatile int*)P.err != 0)) break;
+    }
+    if (t == 0) umma::mbar_wait(&fin, 0, P.err);  // every MMA of this CTA has completed
+    epi_bar<E45_THREADS>();
+    if (t < 32) umma::tmem_dealloc(tbase, ncols);
+}
+
+// The FP64 LM step of every occupied slot from its sums (one thread per slot):
+// start or update the damped Gauss-Newton iteration, propose the next trial
+// point, or retire the ROI and refill the slot from the queue.
+__global__ void k_lm(SplitDev P, const double* init, int n, FitParamsDev prm, double* out5, double* crlb5,
+                     double* nll_out, int* st_out, int* it_out) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= P.P) return;
+    const int roi = P.slot_roi[slot];
+    if (roi < 0) return;
+    const double* tot = P.sums + (size_t)slot * NSUM;
+    double nll = tot[NRED] != 0.0 ? INFINITY : tot[0], g[5], H[25], F[25];
     for (int q = 0; q < 5; ++q) g[q] = tot[1 + q];
     int o = 6;
     for (int q = 0; q < 5; ++q)
@@ -1433,7 +1766,7 @@ static size_t smem_stage2p(const SplitPlanHost& pl) {
     return (size_t)(pl.K1 / 16) * s2_slab_bytes(pl.W) + (size_t)S2_NBUF * s2_ring_bytes(pl.W);
 }
 static size_t smem_stage3(const SplitPlanHost& pl) { return (size_t)5 * 128 * pl.W * 2 + (size_t)4 * pl.RP * pl.W; }
-static size_t smem_stage4(const SplitPlanHost& pl) { return (size_t)2 * 128 * pl.W * 2 + (size_t)4 * pl.RP * pl.W; }
+static size_t smem_stage4(const SplitPlanHost& pl) { return a4_slot_bytes(pl.W, pl.RP) + (size_t)2 * 128 * pl.W * 2; }
 static size_t smem_fused(const SplitPlanHost& pl) {
     const int nbuf = pl.W >= 64 ? 2 : 1;
     return (size_t)4 * 128 * pl.K1 * 2 + (size_t)nbuf * 12 * 16 * pl.K1 + (size_t)5 * 128 * 16 * 2 +
@@ -1498,7 +1831,7 @@ __global__ void k_init_points(SplitDev P, const double* xyz, int n) {
 struct SplitPool {
     SplitPlanHost* pl = nullptr;
     SplitDev D{};
-    size_t s1 = 0, s2 = 0, s3 = 0, s4 = 0, sf = 0;
+    size_t s1 = 0, s2 = 0, s3 = 0, s4 = 0, s45 = 0, sf = 0;
 };
 
 static cudaError_t stage2_attr(int W, size_t smem) {
@@ -1536,12 +1869,15 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
         return ZOLA_E_UNSUPPORTED;
     }
     sp.s1 = smem_stage1(*pl); sp.s2 = smem_stage2p(*pl); sp.s3 = smem_stage3(*pl); sp.s4 = smem_stage4(*pl);
-    if (sp.s1 > 227 * 1024 || sp.s2 > 227 * 1024 || sp.s3 > 227 * 1024 || sp.s4 > 227 * 1024) {
+    sp.s45 = (size_t)2 * 128 * pl->W * 2 + (size_t)S45_NBUF * 2 * 32 * 4 * pl->RP + 4 * s45_roi_bytes(pl->R) +
+             (size_t)4 * pl->R * tm_stride(pl->R) * 4;
+    if (sp.s1 > 227 * 1024 || sp.s2 > 227 * 1024 || sp.s3 > 227 * 1024 || sp.s4 > 227 * 1024 ||
+        sp.s45 > 227 * 1024) {
         ctx->err = "split path: shared-memory plan exceeds 227 KB";
         return ZOLA_E_UNSUPPORTED;
     }
     const size_t per_slot = a2_tile_bytes(pl->K1) / pl->G2 + a3_tile_bytes(pl->W) / pl->G2 +
-                            (size_t)pl->NT4 * a4_tile_bytes(pl->W) + (size_t)4 * pl->R * pl->R * 4 + sizeof(LMState) + 16;
+                            (size_t)pl->NT4 * a4_tile_bytes(pl->W) + (size_t)4 * pl->R * pl->R * 4 + sizeof(LMState) + NSUM * 8 + 16;
     int Pmax = (int)std::min<size_t>(32768, ((size_t)3 << 30) / per_slot);
     if (pmax_override > 0) Pmax = std::min(Pmax, pmax_override);
     Pmax = std::max(4, Pmax / 4 * 4);
@@ -1552,8 +1888,9 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
     const size_t b_a4 = al((size_t)P * pl->NT4 * a4_tile_bytes(pl->W));
     const size_t b_t = al((size_t)P * 4 * pl->R * pl->R * 4);
     const size_t b_lm = al((size_t)P * sizeof(LMState));
+    const size_t b_sums = al((size_t)P * NSUM * 8);
     const size_t b_int = al((size_t)P * 8 + 64);
-    if (ensure_scratch(ctx, b_a2 + b_a3 + b_a4 + b_t + b_lm + b_int, ctx->err)) return ZOLA_E_CUDA;
+    if (ensure_scratch(ctx, b_a2 + b_a3 + b_a4 + b_t + b_lm + b_sums + b_int, ctx->err)) return ZOLA_E_CUDA;
     char* base = (char*)ctx->scratch;
     SplitDev& D = sp.D;
     D = SplitDev{};
@@ -1561,6 +1898,7 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
     D.RP = pl->RP; D.G1 = pl->G1; D.G2 = pl->G2; D.NT4 = pl->NT4; D.P = P; D.a0 = p->a0; D.N = p->N;
     D.zfocus = p->o.zfocus;
     D.bc_hi = pl->d_bc_hi; D.bc_lo = pl->d_bc_lo; D.gt_hi = pl->d_gt_hi; D.gt_lo = pl->d_gt_lo;
+    D.g128_hi = pl->d_g128_hi; D.g128_lo = pl->d_g128_lo;
     D.bc2_hi = pl->d_bc2_hi; D.bc2_lo = pl->d_bc2_lo; D.NCH2 = pl->NCH2; D.bcs = pl->d_bcs;
     D.pupf = pl->d_pupf; D.phase0 = pl->d_phase0; D.kz = pl->d_kz; D.kx = pl->d_kx; D.ky = pl->d_ky;
     D.a2 = base; base += b_a2;
@@ -1568,6 +1906,7 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
     D.a4 = base; base += b_a4;
     D.tmaps = (float*)base; base += b_t;
     D.lm = (LMState*)base; base += b_lm;
+    D.sums = (double*)base; base += b_sums;
     D.slot_roi = (int*)base;
     D.slot_phase = D.slot_roi + P;
     D.queue = D.slot_phase + P;
@@ -1579,13 +1918,15 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
     ZOLA_CUDA_CHECK(stage2_attr(pl->W, sp.s2), ctx);
     ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_stage3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.s3), ctx);
     ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_stage4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.s4), ctx);
+    ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_stage45p, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.s45), ctx);
     sp.sf = smem_fused(*pl);
     if (fused_fits(*pl))
         ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_fused25, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.sf), ctx);
     return ZOLA_OK;
 }
 
-static void launch_model_stages(zola_ctx* ctx, const SplitPool& sp, cudaStream_t st) {
+// Stages 1-3 (pupil DFT, window DFT, row blur) of every occupied slot.
+static void launch_stages123(zola_ctx* ctx, const SplitPool& sp, cudaStream_t st) {
     const SplitPlanHost& pl = *sp.pl;
     const int P = sp.D.P;
     prof_begin(ctx, 0, st);
@@ -1597,10 +1938,16 @@ static void launch_model_stages(zola_ctx* ctx, const SplitPool& sp, cudaStream_t
     prof_begin(ctx, 2, st);
     k_stage3<<<P / pl.G2, SPLIT_THREADS, sp.s3, st>>>(sp.D);
     prof_end(ctx, st);
+    ctx->launches += 3;
+}
+
+// Model-only evaluation: stages 1-3 and the column blur into FP32 maps.
+static void launch_model_stages(zola_ctx* ctx, const SplitPool& sp, cudaStream_t st) {
+    launch_stages123(ctx, sp, st);
     prof_begin(ctx, 3, st);
-    k_stage4<<<P * pl.NT4, SPLIT_THREADS, sp.s4, st>>>(sp.D);
+    k_stage4<<<sp.D.P, SPLIT_THREADS, sp.s4, st>>>(sp.D);
     prof_end(ctx, st);
-    ctx->launches += 4;
+    ctx->launches += 1;
 }
 
 static int read_flags(zola_ctx* ctx, const SplitDev& D, cudaStream_t st, int* active, int* err) {
@@ -1651,6 +1998,11 @@ int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d
     const int max_rounds = (prm->max_iter + 2) * ((n + P - 1) / P + 1) + 8;
     int rounds = 0;
     const bool fused = ctx->split_fused && fused_fits(*sp.pl);
+    // Large ROIs: column blur and likelihood sums in one persistent kernel (the
+    // maps never leave the SM).  Small ROIs: the column-blur maps go through
+    // memory to the warp-per-slot likelihood kernel, which keeps many slots in
+    // flight per SM.
+    const bool fused45 = sp.pl->R >= S45_MIN_R;
     while (true) {
         for (int k = 0; k < 4; ++k) {
             if (fused) {
@@ -1664,12 +2016,24 @@ int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d
                 ctx->launches += 2;
                 continue;
             }
-            launch_model_stages(ctx, sp, st);
-            prof_begin(ctx, 4, st);
-            k_stage5<<<(P + LIK_SLOTS - 1) / LIK_SLOTS, LIK_THREADS, 0, st>>>(D, d_rois, d_scmos, d_init, n, fp, d_out5, d_crlb5,
-                                                                             d_nll, d_status, d_iters);
-            prof_end(ctx, st);
-            ctx->launches++;
+            if (fused45) {
+                launch_stages123(ctx, sp, st);
+                prof_begin(ctx, 3, st);
+                k_stage45p<<<std::min(P, ctx->num_sms), S45_THREADS, sp.s45, st>>>(D, d_rois, d_scmos);
+                prof_end(ctx, st);
+                prof_begin(ctx, 4, st);
+                k_lm<<<(P + LM_THREADS - 1) / LM_THREADS, LM_THREADS, 0, st>>>(D, d_init, n, fp, d_out5, d_crlb5,
+                                                                            d_nll, d_status, d_iters);
+                prof_end(ctx, st);
+                ctx->launches += 2;
+            } else {
+                launch_model_stages(ctx, sp, st);
+                prof_begin(ctx, 4, st);
+                k_stage5<<<(P + S5_SLOTS - 1) / S5_SLOTS, S5_THREADS, 0, st>>>(D, d_rois, d_scmos, d_init, n, fp, d_out5,
+                                                                              d_crlb5, d_nll, d_status, d_iters);
+                prof_end(ctx, st);
+                ctx->launches++;
+            }
         }
         rounds += 4;
         ZOLA_CUDA_CHECK(cudaGetLastError(), ctx);

@@ -111,6 +111,15 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v) {
     for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// 32 lanes x 32 bit, 2 consecutive columns per thread.
+__device__ __forceinline__ void tmem_ld2(uint32_t taddr, float* v) {
+    uint32_t r[2];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];" : "=r"(r[0]), "=r"(r[1]) : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    v[0] = __uint_as_float(r[0]);
+    v[1] = __uint_as_float(r[1]);
+}
+
 // 32 lanes x 32 bit, 4 consecutive columns per thread.
 __device__ __forceinline__ void tmem_ld4(uint32_t taddr, float* v) {
     uint32_t r[4];
@@ -152,6 +161,11 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, int* 
             return false;
         }
     }
+}
+
+// Plain arrive (count 1) on an mbarrier.
+__device__ __forceinline__ void mbar_arrive(uint64_t* mbar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(mbar)) : "memory");
 }
 
 // 1-D bulk copy global -> shared, completion tracked on mbar (no multicast).
