@@ -169,7 +169,7 @@ def detect_fit_config(z, ctx, nframes, seed=1, precision=None):
     det = z.Detector(psf_det, S, S, R, -2.0, 2.0, 0.1, 0.1)
     prec = z.ZOLA_PREC_SPLIT if precision is None else precision
     kw = dict(photon_threshold=500.0, precision=prec, max_iter=50, tol_xyz=1e-4)
-    z.localize_frames(ctx, det, psf_fit, frames[:min(4, nframes)], -2.0, 2.0, **kw)  # warm-up: tables, plans
+    z.localize_frames(ctx, det, psf_fit, frames, -2.0, 2.0, **kw)  # warm-up: tables, plans, scratch sizes
     t0 = time.perf_counter()
     rows = z.localize_frames(ctx, det, psf_fit, frames, -2.0, 2.0, **kw)
     dt = time.perf_counter() - t0

@@ -1115,7 +1115,8 @@ constexpr int NSUM = NRED + 1;
 constexpr int E45_THREADS = 384;                 // 12 epilogue warps: three per TMEM lane quadrant
 constexpr int S45_THREADS = E45_THREADS + 64;    // + producer warp + MMA warp
 constexpr int S45_NBUF = 4;
-constexpr int S45_MIN_R = 40;  // ROI side from which the fused form is faster
+constexpr int S45_MIN_R = 40;       // ROI side from which the fused form is faster
+constexpr int S45_MIN_POOL = 1024;  // and the pool size (small batches favour many short kernels)
 
 __host__ __device__ inline size_t s45_roi_bytes(int R) { return ((size_t)R * R * 4 + 127) / 128 * 128; }
 
@@ -1998,11 +1999,11 @@ int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d
     const int max_rounds = (prm->max_iter + 2) * ((n + P - 1) / P + 1) + 8;
     int rounds = 0;
     const bool fused = ctx->split_fused && fused_fits(*sp.pl);
-    // Large ROIs: column blur and likelihood sums in one persistent kernel (the
-    // maps never leave the SM).  Small ROIs: the column-blur maps go through
-    // memory to the warp-per-slot likelihood kernel, which keeps many slots in
-    // flight per SM.
-    const bool fused45 = sp.pl->R >= S45_MIN_R;
+    // Large ROIs in large pools: column blur and likelihood sums in one
+    // persistent kernel (the maps never leave the SM).  Otherwise the
+    // column-blur maps go through memory to the warp-per-slot likelihood
+    // kernel, which keeps many slots in flight per SM.
+    const bool fused45 = sp.pl->R >= S45_MIN_R && P >= S45_MIN_POOL;
     while (true) {
         for (int k = 0; k < 4; ++k) {
             if (fused) {
