@@ -62,12 +62,10 @@ struct SplitScales {
 
 struct SplitDev {
     // geometry
-    int R, W, D, DP, K1, IC, NCH, RP, G1, G2, NT4, P;
+    int R, W, D, DP, K1, RP, G1, G2, NT4, P;
     int a0, N;
     double zfocus;
     // constant operands
-    const __half* bc_hi;  // NCH chunks of 4IC x K1 (K-major)
-    const __half* bc_lo;  // NCH chunks of 2IC x K1
     const __half* bc2_hi; // NCH2 chunks of 4*16 x K1 (fused kernel)
     const __half* bc2_lo; // NCH2 chunks of 2*16 x K1
     int NCH2;
@@ -100,11 +98,9 @@ struct SplitDev {
 };
 
 struct SplitPlanHost {
-    int R = 0, W = 0, D = 0, DP = 0, K1 = 0, IC = 0, NCH = 0, RP = 0, G1 = 0, G2 = 0, NT4 = 0;
+    int R = 0, W = 0, D = 0, DP = 0, K1 = 0, RP = 0, G1 = 0, G2 = 0, NT4 = 0;
     int IC2 = 16, NCH2 = 0;  // fused stage 2-5 kernel: 16-wide i-chunks
     SplitScales sc{};
-    __half* d_bc_hi = nullptr;
-    __half* d_bc_lo = nullptr;
     __half* d_bc2_hi = nullptr;
     __half* d_bc2_lo = nullptr;
     __half* d_bcs = nullptr;
@@ -130,6 +126,12 @@ __host__ __device__ inline size_t a4_tile_bytes(int W) { return (size_t)2 * 128 
 // Row-blurred maps J of one slot as the column-blur B operand: hi then lo, each
 // MN-major with N = 4 RP rows n = (map, i') and K = W columns j.
 __host__ __device__ inline size_t a4_slot_bytes(int W, int RP) { return (size_t)2 * 4 * RP * W * 2; }
+// K order of every operand along a pupil DFT (stage 1: column b, stage 2: row
+// a, each with its real and imaginary part): k = 16 (b / 8) + 8 [imaginary] +
+// b % 8, so that one 16-wide K step holds both parts of 8 consecutive indices.
+__host__ __device__ inline int kperm(int b, bool im) { return 16 * (b >> 3) + (im ? 8 : 0) + (b & 7); }
+// the natural K index (real parts 0..DP-1, then imaginary parts) of position kp
+__host__ __device__ inline int knat(int kp, int DP) { return ((kp & 8) ? DP : 0) + 8 * (kp >> 4) + (kp & 7); }
 // Row stride (floats) of the fused kernel's shared-memory maps: a multiple of 4
 // congruent to 4 mod 32, so that 32 lanes storing float4 at consecutive rows
 // cover all banks once per 8 lanes.
@@ -146,13 +148,11 @@ static SplitPlanHost* get_plan(zola_psf* p, WindowTables* w, std::string& err) {
     pl->R = R; pl->W = W; pl->D = D;
     pl->DP = D <= 32 ? 32 : 64;
     pl->K1 = 2 * pl->DP;
-    pl->IC = W < 32 ? W : 32;
-    pl->NCH = W / pl->IC;
     pl->RP = (R + 15) / 16 * 16;
     pl->G1 = 128 / pl->DP;
     pl->G2 = 128 / W;
     pl->NT4 = (4 * pl->RP + 127) / 128;
-    const int DP = pl->DP, K1 = pl->K1, IC = pl->IC, RP = pl->RP;
+    const int DP = pl->DP, K1 = pl->K1, RP = pl->RP;
 
     // bounds
     double pmax = 0, kmax = 0, kzmax = 0;
@@ -231,12 +231,13 @@ static SplitPlanHost* get_plan(zola_psf* p, WindowTables* w, std::string& err) {
                     for (int k = 0; k < K1; ++k) {
                         __half hi, lo;
                         split_h(bc_value(part, i, k), hi, lo);
-                        bh[(size_t)c * 4 * icw * K1 + kmajor_off(n, k, K1) / 2] = hi;
-                        if (part < 2) bl[(size_t)c * 2 * icw * K1 + kmajor_off(n, k, K1) / 2] = lo;
+                        const int kp = kperm(k < DP ? k : k - DP, k >= DP);
+                        bh[(size_t)c * 4 * icw * K1 + kmajor_off(n, kp, K1) / 2] = hi;
+                        if (part < 2) bl[(size_t)c * 2 * icw * K1 + kmajor_off(n, kp, K1) / 2] = lo;
                     }
                 }
     };
-    // K-slabs of the wide stage kernels: for K step s (columns 16s .. 16s + 15),
+    // K-slabs of the wide stage kernels: for K step s (positions 16s .. 16s + 15 of the K order above),
     // rows n = q * W + i with q = 0..3 the hi values of parts 0..3 and q = 4, 5
     // the lo values of parts 0, 1; K-major with K = 16 (6W x 32 bytes a slab).
     std::vector<__half> bs((size_t)(K1 / 16) * 6 * W * 16, __float2half(0.f));
@@ -245,11 +246,10 @@ static SplitPlanHost* get_plan(zola_psf* p, WindowTables* w, std::string& err) {
             for (int i = 0; i < W; ++i)
                 for (int kk = 0; kk < 16; ++kk) {
                     __half hi, lo;
-                    split_h(bc_value(q < 4 ? q : q - 4, i, 16 * st + kk), hi, lo);
+                    split_h(bc_value(q < 4 ? q : q - 4, i, knat(16 * st + kk, DP)), hi, lo);
                     bs[(size_t)st * 6 * W * 16 + kmajor_off(q * W + i, kk, 16) / 2] = q < 4 ? hi : lo;
                 }
-    std::vector<__half> bh, bl, bh2, bl2;
-    pack_bc(IC, bh, bl);
+    std::vector<__half> bh2, bl2;
     pl->IC2 = W < 16 ? W : 16;
     pl->NCH2 = W / pl->IC2;
     pack_bc(pl->IC2, bh2, bl2);
@@ -295,8 +295,6 @@ static SplitPlanHost* get_plan(zola_psf* p, WindowTables* w, std::string& err) {
         e = cudaMalloc(dst, bytes);
         if (e == cudaSuccess) e = cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
     };
-    up((void**)&pl->d_bc_hi, bh.data(), bh.size() * 2);
-    up((void**)&pl->d_bc_lo, bl.data(), bl.size() * 2);
     up((void**)&pl->d_bc2_hi, bh2.data(), bh2.size() * 2);
     up((void**)&pl->d_bc2_lo, bl2.data(), bl2.size() * 2);
     up((void**)&pl->d_bcs, bs.data(), bs.size() * 2);
@@ -321,8 +319,6 @@ static SplitPlanHost* get_plan(zola_psf* p, WindowTables* w, std::string& err) {
 void free_split_plan(void* plan) {
     SplitPlanHost* pl = (SplitPlanHost*)plan;
     if (!pl) return;
-    cudaFree(pl->d_bc_hi);
-    cudaFree(pl->d_bc_lo);
     cudaFree(pl->d_bc2_hi);
     cudaFree(pl->d_bc2_lo);
     cudaFree(pl->d_bcs);
@@ -342,6 +338,24 @@ void free_split_plan(void* plan) {
 __device__ __forceinline__ uint32_t tmem_lane_addr(uint32_t base, int col) {
     const int quad = (threadIdx.x >> 5) & 3;
     return base + ((uint32_t)(quad * 32) << 16) + (uint32_t)col;
+}
+
+// N groups of 8 TMEM columns of this thread's lane, all loads in flight before
+// one wait; the empty asm after the wait keeps every use of a loaded register
+// behind it.
+template <int N>
+__device__ __forceinline__ void tmem_ld8_multi(const uint32_t (&addr)[N], float (&v)[N][8]) {
+    uint32_t r[N][8];
+#pragma unroll
+    for (int i = 0; i < N; ++i) umma::tmem_ld8_nw(addr[i], r[i]);
+    umma::tmem_wait_ld();
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            asm volatile("" : "+r"(r[i][j]));
+            v[i][j] = __uint_as_float(r[i][j]);
+        }
 }
 
 __device__ __forceinline__ void store8h(void* dst, const __half* v) {
@@ -418,169 +432,303 @@ __device__ __forceinline__ bool tile_live(const SplitDev& P, int s0, int g) {
     return live;
 }
 
-// ----------------------------------------------------------- stage 1 -------
-// One CTA per G1 slots; thread t builds row (g = t / DP, a = t % DP) of Q.
-__global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage1(SplitDev P) {
-    extern __shared__ __align__(1024) char smem[];
-    const int K1 = P.K1, DP = P.DP, IC = P.IC, NCH = P.NCH;
-    const int t = threadIdx.x;
-    char* A1hi = smem;
-    char* A1lo = A1hi + 256 * K1;
-    char* A1z = A1lo + 256 * K1;
-    char* bcb = A1z + 256 * K1;
-    const int bc_hi_bytes = 4 * IC * K1 * 2, bc_lo_bytes = 2 * IC * K1 * 2;
-    const int bc_buf = bc_hi_bytes + bc_lo_bytes;
-    __shared__ __align__(8) uint64_t bc_full[2], mma_done[2];
-    __shared__ uint32_t tmem_base;
-    const int ncols = NCH > 1 ? 512 : tmem_cols_pow2(6 * IC);
-    if (!tile_live(P, blockIdx.x * P.G1, P.G1)) return;
+// ----------------------------------------------- persistent-kernel helpers ----
+// Named barrier 1 over the first N threads of the CTA (the epilogue warps).
+template <int N = SPLIT_THREADS>
+__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, %0;" ::"n"(N) : "memory"); }
+// The same barrier, returning the OR of p over its threads (the same value in every thread).
+template <int N = SPLIT_THREADS>
+__device__ __forceinline__ bool epi_bar_or(bool p) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred P, Q;\n\tsetp.ne.u32 P, %1, 0;\n\t"
+        "bar.red.or.pred Q, 1, %2, P;\n\tselp.u32 %0, 1, 0, Q;\n\t}\n"
+        : "=r"(r)
+        : "r"((uint32_t)p), "n"(N)
+        : "memory");
+    return r != 0;
+}
 
-    if (t < 32) umma::tmem_alloc(&tmem_base, ncols);
+__host__ __device__ constexpr int s2_slab_bytes(int W) { return 6 * W * 32; }
+
+__host__ __device__ constexpr int s2_ring_bytes(int W) { return (W > 64 ? 2 : 4) * 4096; }
+
+__device__ __forceinline__ void warp_arrive(uint64_t* mbar) {
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) umma::mbar_arrive(mbar);
+}
+
+// ------------------------------------------------- stage 1 (persistent) -----
+// One CTA per SM walks the stage-1 tiles (G1 slots x DP pupil rows a) with the
+// DFT constants resident in shared memory (the K-slabs the window stage uses).
+// The 512 builder threads compute the pupil field Q one K step at a time (8
+// pupil columns b with their real and imaginary parts, in the K order of
+// kperm) into a 4-deep ring; the MMA warp multiplies each step against the
+// resident constants: hi x [parts 0-3] gives S and S_y, hi x [lo parts 0-1]
+// and lo x [parts 0-1] accumulate onto S, and Q_z = i kz Q x [parts 0-1] gives
+// S_z.  S, S_y and S_z need 6W columns: for W = 128 that exceeds TMEM, so a
+// second pass over K rebuilds only Q_z.  The builders then move the
+// accumulators to the stage-2 operand A2 (rows (slot, i), K = a).
+constexpr int S1_THREADS = SPLIT_THREADS + 32;
+constexpr int S1_NBQ = 4;
+constexpr int S1_QB = 128 * 32;  // one Q array for one K step: 128 rows x 16 k, f16
+
+__host__ __device__ constexpr int s1_qring_bytes(int W) { return (W > 64 ? 2 : 3) * S1_QB; }
+
+template <int W>
+__global__ void __launch_bounds__(S1_THREADS, 1) k_stage1p(SplitDev P, int ntiles) {
+    extern __shared__ __align__(1024) char smem[];
+    constexpr bool TWO = W > 64;
+    constexpr int SLAB = s2_slab_bytes(W), QRING = s1_qring_bytes(W), NBQ = S1_NBQ, QB = S1_QB;
+    constexpr int NCOLS = W >= 64 ? 512 : 256;
+    const int K1 = P.K1, DP = P.DP, G1 = P.G1, t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    // W = 128 comes with K1 = 128 (64 pupil rows): 8 K steps, known here so that the
+    // Q_z values of pass A stay in registers for pass B
+    const int NS = TWO ? 8 : K1 / 16;
+    char* CS = smem;               // NS constant K-slabs
+    char* QR = smem + NS * SLAB;   // ring of Q K-slabs
+    __shared__ __align__(8) uint64_t cfull, qfull[NBQ], qfree[NBQ], accA, accB, tfree, fin;
+    __shared__ uint32_t tmem_base;
+    if (t < 32) umma::tmem_alloc(&tmem_base, NCOLS);
     if (t == 0) {
-        umma::mbar_init(&bc_full[0], 1); umma::mbar_init(&bc_full[1], 1);
-        umma::mbar_init(&mma_done[0], 1); umma::mbar_init(&mma_done[1], 1);
+        umma::mbar_init(&cfull, 1);
+        for (int b = 0; b < NBQ; ++b) { umma::mbar_init(&qfull[b], SPLIT_THREADS); umma::mbar_init(&qfree[b], 1); }
+        umma::mbar_init(&accA, 1);
+        umma::mbar_init(&accB, 1);
+        umma::mbar_init(&tfree, SPLIT_THREADS / 32);
+        umma::mbar_init(&fin, 1);
         umma::mbar_fence_init();
     }
     __syncthreads();
     umma::fence_after_sync();
     const uint32_t tbase = tmem_base;
-    auto load_bc = [&](int c, int buf) {
-        char* dst = bcb + buf * bc_buf;
-        umma::mbar_expect_tx(&bc_full[buf], bc_buf);
-        umma::bulk_g2s(dst, (const char*)P.bc_hi + (size_t)c * bc_hi_bytes, bc_hi_bytes, &bc_full[buf]);
-        umma::bulk_g2s(dst + bc_hi_bytes, (const char*)P.bc_lo + (size_t)c * bc_lo_bytes, bc_lo_bytes, &bc_full[buf]);
-    };
     if (t == 0) {
-        load_bc(0, 0);
-        if (NCH > 1) load_bc(1, 1);
+        umma::mbar_expect_tx(&cfull, (uint32_t)(NS * SLAB));
+        for (int s = 0; s < NS; ++s)
+            umma::bulk_g2s(CS + s * SLAB, (const char*)P.bcs + (size_t)s * SLAB, SLAB, &cfull);
     }
 
-    // epilogue mapping: thread -> tile row (g, a) = t % 128 (its TMEM lane), column share of its warpgroup
+    if (warp == SPLIT_THREADS / 32) {  // ---------------- MMA issuer
+        if (lane != 0) return;
+        bool ok = umma::mbar_wait(&cfull, 0, P.err);
+        int q = 0, nwait = 0, nphase = 0;
+        auto tmem_ready = [&]() {  // every MMA phase after the first waits for the epilogue before it
+            if (nphase++ == 0) return true;
+            const bool r = umma::mbar_wait(&tfree, (uint32_t)(nwait & 1), P.err);
+            ++nwait;
+            umma::fence_after_sync();
+            return r;
+        };
+        auto steps = [&](bool pb) {
+            for (int s = 0; s < NS; ++s, ++q) {
+                const int buf = q % NBQ;
+                if (!umma::mbar_wait(&qfull[buf], (uint32_t)((q / NBQ) & 1), P.err)) return false;
+                umma::fence_after_sync();
+                const uint32_t qs = umma::smem_u32(QR + buf * QRING), cb = umma::smem_u32(CS + s * SLAB);
+                auto mma = [&](uint32_t a, int row0, int N, int col, bool acc) {
+                    const uint64_t ad = umma::smem_desc(a, 128, 256);
+                    const uint64_t bd = umma::smem_desc(cb + (uint32_t)(row0 / 8) * 256, 128, 256);
+                    umma::mma_f16(tbase + col, ad, bd, umma::idesc_f16(128, N, false, false), acc ? 1u : 0u);
+                };
+                if (!pb) {
+#pragma unroll
+                    for (int r = 0; r < 4 * W; r += 256) mma(qs, r, 4 * W < 256 ? 4 * W : 256, r, s > 0);  // S, S_y
+                    mma(qs, 4 * W, 2 * W, 0, true);    // + hi x lo(C)
+                    mma(qs + QB, 0, 2 * W, 0, true);   // + lo x hi(C)
+                    if (!TWO) mma(qs + 2 * QB, 0, 2 * W, 4 * W, s > 0);  // S_z
+                } else {
+                    mma(qs, 0, 2 * W, 0, s > 0);       // S_z
+                }
+                umma::mma_commit(&qfree[buf]);
+            }
+            return true;
+        };
+        for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+            if (!tile_live(P, tile * G1, G1)) continue;
+            ok = tmem_ready() && steps(false);
+            umma::mma_commit(&accA);
+            if (TWO && ok) {
+                ok = tmem_ready() && steps(true);
+                umma::mma_commit(&accB);
+            }
+        }
+        umma::mma_commit(&fin);
+        return;
+    }
+
+    // ---------------- builders / epilogue
+    // build mapping: slab row brow (8 per warp, conflict-free 4-byte stores), column pair bp
+    const int brow = 8 * warp + (lane & 7), bp = lane >> 3;
+    const int bg = brow / DP, ba = brow % DP;
+    // epilogue mapping: TMEM row (g, a) = t % 128, its warpgroup's share of the output index i
     const int row = t & 127, wg = t >> 7;
     const int g = row / DP, a = row % DP;
-    const int slot = blockIdx.x * P.G1 + g;
-    const int roi = P.slot_roi[slot];
-
-    // Q build: thread -> pupil row qa and 8 columns qb0.. of every slot it covers.  The
-    // DP x DP / 8 threads of one slot read each table entry once, as 512-byte warp loads
-    // (the tables are stored in that order), and apply it to each of the CTA's slots.
-    {
-        const int nps = DP * DP / 8;  // threads per slot: 512 (DP = 64) or 128 (DP = 32)
-        const int qi0 = t % nps, qa = qi0 % DP, qbg = qi0 / DP, qb0 = qbg * 8;
-        double ph0[8], kzr[8], kyr[8];
-        float pu[8];
-#pragma unroll
-        for (int u = 0; u < 8; u += 2) {
-            const double2 v0 = *(const double2*)(P.phase0 + (((size_t)qbg * 4 + u / 2) * DP + qa) * 2);
-            const double2 v1 = *(const double2*)(P.kz + (((size_t)qbg * 4 + u / 2) * DP + qa) * 2);
-            const double2 v2 = *(const double2*)(P.ky + qb0 + u);
-            ph0[u] = v0.x; ph0[u + 1] = v0.y;
-            kzr[u] = v1.x; kzr[u + 1] = v1.y;
-            kyr[u] = v2.x; kyr[u + 1] = v2.y;
+    const int kre = kperm(a, false), kim = kperm(a, true);
+    const size_t arr = (size_t)128 * K1 * 2;
+    constexpr int CW = W / 4;
+    int q = 0, ntile = 0;
+    bool abort = false;
+    for (int tile = blockIdx.x; tile < ntiles && !abort; tile += gridDim.x) {
+        if (!tile_live(P, tile * G1, G1)) continue;
+        const uint32_t ph = (uint32_t)(ntile & 1);
+        ++ntile;
+        const int bslot = tile * G1 + bg;
+        const bool blive = P.slot_roi[bslot] >= 0;
+        double x = 0, y = 0, z = 0;
+        if (blive) {
+            x = P.lm[bslot].trial[0]; y = P.lm[bslot].trial[1]; z = P.lm[bslot].trial[2];
         }
+        const double kxa = P.kx[ba];
+        // one K step of Q (columns b = 8 s + 2 bp + {0, 1} of row brow); the table loads of
+        // the next step are issued before this step's arithmetic
+        struct QTab { double2 p0, kz, ky; float2 pu; };
+        auto qtab = [&](int s) {
+            QTab q2;
+            q2.p0 = *(const double2*)(P.phase0 + (((size_t)s * 4 + bp) * DP + ba) * 2);
+            q2.kz = *(const double2*)(P.kz + (((size_t)s * 4 + bp) * DP + ba) * 2);
+            q2.ky = *(const double2*)(P.ky + 8 * s + 2 * bp);
+            q2.pu = *(const float2*)(P.pupf + (((size_t)s * 2 + (bp >> 1)) * DP + ba) * 4 + (bp & 1) * 2);
+            return q2;
+        };
+        const uint32_t ore = kmajor_off(brow, 2 * bp, 16), oim = kmajor_off(brow, 8 + 2 * bp, 16);
+        auto slot_wait = [&]() {  // ring slot for the next K step
+            const int buf = q % NBQ;
+            if (q >= NBQ) umma::mbar_wait(&qfree[buf], (uint32_t)((q / NBQ - 1) & 1), P.err);
+            ++q;
+            return QR + buf * QRING;
+        };
+        auto slot_done = [&](char* qs) {
+            umma::fence_proxy_async();
+            umma::mbar_arrive(&qfull[(qs - QR) / QRING]);
+        };
+        uint32_t zkeep[TWO ? 8 : 1][2] = {};  // pass A's Q_z of each K step (W = 128)
+        auto build = [&](int s, const QTab& tb, uint32_t& zr, uint32_t& zi) {
+            const double ph0[2] = {tb.p0.x, tb.p0.y}, kzr[2] = {tb.kz.x, tb.kz.y}, kyr[2] = {tb.ky.x, tb.ky.y};
+            const float pu[2] = {tb.pu.x, tb.pu.y};
+            float qr[2], qi[2], kzv[2];
 #pragma unroll
-        for (int u = 0; u < 8; u += 4) {
-            const float4 v = *(const float4*)(P.pupf + (((size_t)qbg * 2 + u / 4) * DP + qa) * 4);
-            pu[u] = v.x; pu[u + 1] = v.y; pu[u + 2] = v.z; pu[u + 3] = v.w;
-        }
-        const double kxa = P.kx[qa];
-        for (int qg = t / nps; qg < P.G1; qg += SPLIT_THREADS / nps) {
-            const int qslot = blockIdx.x * P.G1 + qg;
-            const bool live = P.slot_roi[qslot] >= 0;
-            double x = 0, y = 0, z = 0;
-            if (live) {
-                x = P.lm[qslot].trial[0]; y = P.lm[qslot].trial[1]; z = P.lm[qslot].trial[2];
+            for (int e = 0; e < 2; ++e) {
+                qr[e] = 0.f; qi[e] = 0.f; kzv[e] = 0.f;
+                if (blive && pu[e] != 0.f) {
+                    float sn, cs;
+                    sincos_phase(ph0[e] + kxa * x + kyr[e] * y + kzr[e] * z, sn, cs);
+                    qr[e] = pu[e] * cs;
+                    qi[e] = pu[e] * sn;
+                    kzv[e] = (float)kzr[e];
+                }
             }
-            const int qrow = qg * DP + qa;
-            uint32_t rh[4], rl[4], ih[4], il[4], zr[4], zi[4];
+            zr = pack_h2(-kzv[0] * qi[0] * P.sc.qz, -kzv[1] * qi[1] * P.sc.qz);  // Q_z = i kz Q
+            zi = pack_h2(kzv[0] * qr[0] * P.sc.qz, kzv[1] * qr[1] * P.sc.qz);
+            uint32_t rh, rl, ih, il;
+            split2(qr[0] * P.sc.q, qr[1] * P.sc.q, rh, rl);
+            split2(qi[0] * P.sc.q, qi[1] * P.sc.q, ih, il);
+            char* qs = slot_wait();
+            *(uint32_t*)(qs + ore) = rh;
+            *(uint32_t*)(qs + oim) = ih;
+            *(uint32_t*)(qs + QB + ore) = rl;
+            *(uint32_t*)(qs + QB + oim) = il;
+            if (!TWO) {
+                *(uint32_t*)(qs + 2 * QB + ore) = zr;
+                *(uint32_t*)(qs + 2 * QB + oim) = zi;
+            }
+            slot_done(qs);
+        };
+        auto build_z = [&](int s) {  // pass B (W = 128): the kept Q_z of step s
+            char* qs = slot_wait();
+            *(uint32_t*)(qs + ore) = zkeep[TWO ? s : 0][0];
+            *(uint32_t*)(qs + oim) = zkeep[TWO ? s : 0][1];
+            slot_done(qs);
+        };
+        // A2 destination of this thread's TMEM row: stage-2 tile of the slot, K positions of a
+        const int slot = tile * G1 + g;
+        const bool live = P.slot_roi[slot] >= 0;
+        const int tile2 = slot / P.G2, mrow0 = (slot % P.G2) * W;
+        char* a2t = P.a2 + (size_t)tile2 * a2_tile_bytes(K1);
+        // epilogue of one pass: maps at TMEM columns c0 (S), c0 + 2W (S_y), zc (S_z; < 0: none)
+        auto epilogue = [&](bool sy, int zc, uint32_t phase, uint64_t* accb) {
+            umma::mbar_wait(accb, phase, P.err);
+            umma::fence_after_sync();
+#pragma unroll 1
+            for (int h = wg * CW; h < (wg + 1) * CW; h += 8) {
+                const int m = mrow0 + h;
+                if (sy) {
+                    float v4[4][8];
+                    const uint32_t ad[4] = {tmem_lane_addr(tbase, h), tmem_lane_addr(tbase, W + h),
+                                            tmem_lane_addr(tbase, 2 * W + h), tmem_lane_addr(tbase, 3 * W + h)};
+                    tmem_ld8_multi<4>(ad, v4);
+                    const float *sr = v4[0], *si = v4[1], *yr = v4[2], *yi = v4[3];
+                    if (live) {
+                        uint32_t shr[4], slr[4], shi[4], sli[4], wyr[4], wyi[4];
 #pragma unroll
-            for (int u = 0; u < 8; u += 2) {
-                float qr[2], qi[2], kzv[2];
-#pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    qr[e] = 0.f; qi[e] = 0.f; kzv[e] = 0.f;
-                    if (live && pu[u + e] != 0.f) {
-                        float sn, cs;
-                        sincos_phase(ph0[u + e] + kxa * x + kyr[u + e] * y + kzr[u + e] * z, sn, cs);
-                        qr[e] = pu[u + e] * cs;
-                        qi[e] = pu[u + e] * sn;
-                        kzv[e] = (float)kzr[u + e];
+                        for (int u = 0; u < 8; u += 2) {
+                            split2(sr[u] * P.sc.c2, sr[u + 1] * P.sc.c2, shr[u / 2], slr[u / 2]);
+                            split2(si[u] * P.sc.c2, si[u + 1] * P.sc.c2, shi[u / 2], sli[u / 2]);
+                            wyr[u / 2] = pack_h2(yr[u] * P.sc.c2y, yr[u + 1] * P.sc.c2y);
+                            wyi[u / 2] = pack_h2(yi[u] * P.sc.c2y, yi[u + 1] * P.sc.c2y);
+                        }
+                        store4w(a2t + 0 * arr + mnmajor_off(m, kre, 128), shr);
+                        store4w(a2t + 1 * arr + mnmajor_off(m, kre, 128), slr);
+                        store4w(a2t + 0 * arr + mnmajor_off(m, kim, 128), shi);
+                        store4w(a2t + 1 * arr + mnmajor_off(m, kim, 128), sli);
+                        store4w(a2t + 2 * arr + mnmajor_off(m, kre, 128), wyr);
+                        store4w(a2t + 2 * arr + mnmajor_off(m, kim, 128), wyi);
                     }
                 }
-                split2(qr[0] * P.sc.q, qr[1] * P.sc.q, rh[u / 2], rl[u / 2]);
-                split2(qi[0] * P.sc.q, qi[1] * P.sc.q, ih[u / 2], il[u / 2]);
-                zr[u / 2] = pack_h2(-kzv[0] * qi[0] * P.sc.qz, -kzv[1] * qi[1] * P.sc.qz);  // Qz = i kz Q
-                zi[u / 2] = pack_h2(kzv[0] * qr[0] * P.sc.qz, kzv[1] * qr[1] * P.sc.qz);
-            }
-            store4w(A1hi + kmajor_off(qrow, qb0, K1), rh);
-            store4w(A1lo + kmajor_off(qrow, qb0, K1), rl);
-            store4w(A1hi + kmajor_off(qrow, DP + qb0, K1), ih);
-            store4w(A1lo + kmajor_off(qrow, DP + qb0, K1), il);
-            store4w(A1z + kmajor_off(qrow, qb0, K1), zr);
-            store4w(A1z + kmajor_off(qrow, DP + qb0, K1), zi);
-        }
-    }
-    umma::fence_proxy_async();
-    __syncthreads();
-
-    const uint32_t sbo1 = (K1 / 8) * 128;
-    const uint32_t id4 = umma::idesc_f16(128, 4 * IC, false, false);
-    const uint32_t id2 = umma::idesc_f16(128, 2 * IC, false, false);
-    auto issue = [&](int c) {
-        const int buf = NCH > 1 ? (c & 1) : 0;
-        umma::mbar_wait(&bc_full[buf], (c >> 1) & 1, P.err);
-        umma::fence_after_sync();
-        const uint32_t bhi = umma::smem_u32(bcb + buf * bc_buf), blo = bhi + bc_hi_bytes;
-        const uint32_t a_hi = umma::smem_u32(A1hi), a_lo = umma::smem_u32(A1lo), a_z = umma::smem_u32(A1z);
-        const uint32_t td = tbase + buf * 256;
-        mma_chain(td, a_hi, 128, sbo1, 256, bhi, 128, sbo1, 256, K1, id4, false);
-        mma_chain(td, a_hi, 128, sbo1, 256, blo, 128, sbo1, 256, K1, id2, true);
-        mma_chain(td, a_lo, 128, sbo1, 256, bhi, 128, sbo1, 256, K1, id2, true);
-        mma_chain(td + 4 * IC, a_z, 128, sbo1, 256, bhi, 128, sbo1, 256, K1, id2, false);
-        umma::mma_commit(&mma_done[buf]);
-    };
-    if (t == 0) issue(0);
-    // A2 destination for this thread's row: stage-2 tile of the slot, k = a and DP + a
-    const int tile2 = slot / P.G2, mrow0 = (slot % P.G2) * P.W;
-    char* a2t = P.a2 + (size_t)tile2 * a2_tile_bytes(K1);
-    const size_t arr = (size_t)128 * K1 * 2;
-    for (int c = 0; c < NCH; ++c) {
-        const int buf = NCH > 1 ? (c & 1) : 0;
-        if (t == 0 && c + 1 < NCH) issue(c + 1);
-        umma::mbar_wait(&mma_done[buf], (c >> 1) & 1, P.err);
-        umma::fence_after_sync();
-        const uint32_t col0 = buf * 256;
-        for (int h = wg * 8; h < IC; h += 32) {
-            float v[6][8];
+                if (zc >= 0) {
+                    float v2[2][8];
+                    const uint32_t ad[2] = {tmem_lane_addr(tbase, zc + h), tmem_lane_addr(tbase, zc + W + h)};
+                    tmem_ld8_multi<2>(ad, v2);
+                    const float *zr8 = v2[0], *zi8 = v2[1];
+                    if (live) {
+                        uint32_t wzr[4], wzi[4];
 #pragma unroll
-            for (int part = 0; part < 6; ++part) umma::tmem_ld8(tmem_lane_addr(tbase, col0 + part * IC + h), v[part]);
-            if (roi < 0) continue;
-            const int m = mrow0 + c * IC + h;
-            uint32_t shr[4], slr[4], shi[4], sli[4], yr[4], yi[4], zr[4], zi[4];
-#pragma unroll
-            for (int u = 0; u < 8; u += 2) {
-                split2(v[0][u] * P.sc.c2, v[0][u + 1] * P.sc.c2, shr[u / 2], slr[u / 2]);
-                split2(v[1][u] * P.sc.c2, v[1][u + 1] * P.sc.c2, shi[u / 2], sli[u / 2]);
-                yr[u / 2] = pack_h2(v[2][u] * P.sc.c2y, v[2][u + 1] * P.sc.c2y);
-                yi[u / 2] = pack_h2(v[3][u] * P.sc.c2y, v[3][u + 1] * P.sc.c2y);
-                zr[u / 2] = pack_h2(v[4][u] * P.sc.c2z, v[4][u + 1] * P.sc.c2z);
-                zi[u / 2] = pack_h2(v[5][u] * P.sc.c2z, v[5][u + 1] * P.sc.c2z);
+                        for (int u = 0; u < 8; u += 2) {
+                            wzr[u / 2] = pack_h2(zr8[u] * P.sc.c2z, zr8[u + 1] * P.sc.c2z);
+                            wzi[u / 2] = pack_h2(zi8[u] * P.sc.c2z, zi8[u + 1] * P.sc.c2z);
+                        }
+                        store4w(a2t + 3 * arr + mnmajor_off(m, kre, 128), wzr);
+                        store4w(a2t + 3 * arr + mnmajor_off(m, kim, 128), wzi);
+                    }
+                }
             }
-            store4w(a2t + 0 * arr + mnmajor_off(m, a, 128), shr);
-            store4w(a2t + 1 * arr + mnmajor_off(m, a, 128), slr);
-            store4w(a2t + 0 * arr + mnmajor_off(m, DP + a, 128), shi);
-            store4w(a2t + 1 * arr + mnmajor_off(m, DP + a, 128), sli);
-            store4w(a2t + 2 * arr + mnmajor_off(m, a, 128), yr);
-            store4w(a2t + 2 * arr + mnmajor_off(m, DP + a, 128), yi);
-            store4w(a2t + 3 * arr + mnmajor_off(m, a, 128), zr);
-            store4w(a2t + 3 * arr + mnmajor_off(m, DP + a, 128), zi);
+            umma::fence_before_sync();
+            warp_arrive(&tfree);
+        };
+        if constexpr (TWO) {
+            QTab cur = qtab(0);
+#pragma unroll
+            for (int s = 0; s < 8; ++s) {
+                QTab nxt;
+                if (s + 1 < 8) nxt = qtab(s + 1);
+                build(s, cur, zkeep[s][0], zkeep[s][1]);
+                if (s + 1 < 8) cur = nxt;
+            }
+#pragma unroll
+            for (int s = 0; s < NBQ; ++s) build_z(s);
+            epilogue(true, -1, ph, &accA);
+#pragma unroll
+            for (int s = NBQ; s < 8; ++s) build_z(s);
+            epilogue(false, 0, ph, &accB);
+        } else {
+            QTab cur = qtab(0);
+            for (int s = 0; s < NS; ++s) {
+                QTab nxt;
+                if (s + 1 < NS) nxt = qtab(s + 1);
+                uint32_t zr, zi;
+                build(s, cur, zr, zi);
+                if (s + 1 < NS) cur = nxt;
+            }
+            epilogue(true, 4 * W, ph, &accA);
         }
-        umma::fence_before_sync();
-        __syncthreads();
-        if (t == 0 && c + 2 < NCH) load_bc(c + 2, buf);
+        // (a bounded wait that gave up makes every builder leave the loop together)
+        abort = epi_bar_or(t == 0 && *(volatile int*)P.err != 0);
     }
-    __syncthreads();
-    if (t < 32) umma::tmem_dealloc(tbase, ncols);
+    if (t == 0) {
+        umma::mbar_wait(&fin, 0, P.err);    // every MMA of this CTA has completed
+        umma::mbar_wait(&cfull, 0, P.err);  // and the constant copies have landed
+    }
+    epi_bar();
+    if (t < 32) umma::tmem_dealloc(tbase, NCOLS);
 }
 
 // ------------------------------------------------- stage 2 (persistent) -----
@@ -598,25 +746,6 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage1(SplitDev P) {
 // is the producer.
 constexpr int S2_THREADS = SPLIT_THREADS + 32;
 constexpr int S2_NBUF = 4;
-
-// Named barrier 1 over the first N threads of the CTA (the epilogue warps).
-template <int N = SPLIT_THREADS>
-__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, %0;" ::"n"(N) : "memory"); }
-// The same barrier, returning the OR of p over its threads (the same value in every thread).
-template <int N = SPLIT_THREADS>
-__device__ __forceinline__ bool epi_bar_or(bool p) {
-    uint32_t r;
-    asm volatile(
-        "{\n\t.reg .pred P, Q;\n\tsetp.ne.u32 P, %1, 0;\n\t"
-        "bar.red.or.pred Q, 1, %2, P;\n\tselp.u32 %0, 1, 0, Q;\n\t}\n"
-        : "=r"(r)
-        : "r"((uint32_t)p), "n"(N)
-        : "memory");
-    return r != 0;
-}
-
-__host__ __device__ constexpr int s2_ring_bytes(int W) { return (W > 64 ? 2 : 4) * 4096; }
-__host__ __device__ constexpr int s2_slab_bytes(int W) { return 6 * W * 32; }
 
 template <int W>
 __global__ void __launch_bounds__(S2_THREADS, 1) k_stage2p(SplitDev P, int ntiles) {
@@ -722,11 +851,13 @@ __global__ void __launch_bounds__(S2_THREADS, 1) k_stage2p(SplitDev P, int ntile
 #pragma unroll
             for (int h = 0; h < CW; h += 8) {
                 const int i0 = wg * CW + h;
-                float xr[8], xi[8];
-                umma::tmem_ld8(tmem_lane_addr(tbase, i0), er + h);
-                umma::tmem_ld8(tmem_lane_addr(tbase, W + i0), ei + h);
-                umma::tmem_ld8(tmem_lane_addr(tbase, 2 * W + i0), xr);
-                umma::tmem_ld8(tmem_lane_addr(tbase, 3 * W + i0), xi);
+                float v4[4][8];
+                const uint32_t ad[4] = {tmem_lane_addr(tbase, i0), tmem_lane_addr(tbase, W + i0),
+                                        tmem_lane_addr(tbase, 2 * W + i0), tmem_lane_addr(tbase, 3 * W + i0)};
+                tmem_ld8_multi<4>(ad, v4);
+#pragma unroll
+                for (int u = 0; u < 8; ++u) { er[h + u] = v4[0][u]; ei[h + u] = v4[1][u]; }
+                const float *xr = v4[2], *xi = v4[3];
                 uint32_t hh[4], ll[4], dx[4];
 #pragma unroll
                 for (int u = 0; u < 8; u += 2) {
@@ -753,20 +884,18 @@ __global__ void __launch_bounds__(S2_THREADS, 1) k_stage2p(SplitDev P, int ntile
 #pragma unroll
             for (int h = 0; h < CW; h += 8) {
                 const int i0 = wg * CW + h;
-                float xr[8], xi[8];
+                float v4[4][8];
+                const uint32_t ad[4] = {tmem_lane_addr(tbase, i0), tmem_lane_addr(tbase, W + i0),
+                                        tmem_lane_addr(tbase, 2 * W + i0), tmem_lane_addr(tbase, 3 * W + i0)};
+                tmem_ld8_multi<4>(ad, v4);
                 uint32_t dy[4], dz[4];
-                umma::tmem_ld8(tmem_lane_addr(tbase, i0), xr);
-                umma::tmem_ld8(tmem_lane_addr(tbase, W + i0), xi);
 #pragma unroll
-                for (int u = 0; u < 8; u += 2)
-                    dy[u / 2] = pack_h2(ipx(er + h, ei + h, xr, xi, u, P.sc.cIy),
-                                        ipx(er + h, ei + h, xr, xi, u + 1, P.sc.cIy));
-                umma::tmem_ld8(tmem_lane_addr(tbase, 2 * W + i0), xr);
-                umma::tmem_ld8(tmem_lane_addr(tbase, 3 * W + i0), xi);
-#pragma unroll
-                for (int u = 0; u < 8; u += 2)
-                    dz[u / 2] = pack_h2(ipx(er + h, ei + h, xr, xi, u, P.sc.cIz),
-                                        ipx(er + h, ei + h, xr, xi, u + 1, P.sc.cIz));
+                for (int u = 0; u < 8; u += 2) {
+                    dy[u / 2] = pack_h2(ipx(er + h, ei + h, v4[0], v4[1], u, P.sc.cIy),
+                                        ipx(er + h, ei + h, v4[0], v4[1], u + 1, P.sc.cIy));
+                    dz[u / 2] = pack_h2(ipx(er + h, ei + h, v4[2], v4[3], u, P.sc.cIz),
+                                        ipx(er + h, ei + h, v4[2], v4[3], u + 1, P.sc.cIz));
+                }
                 const uint32_t off = kmajor_off(row, i0, W);
                 store4w(a3t + 3 * arr3 + off, dy);
                 store4w(a3t + 4 * arr3 + off, dz);
@@ -775,11 +904,11 @@ __global__ void __launch_bounds__(S2_THREADS, 1) k_stage2p(SplitDev P, int ntile
 #pragma unroll
             for (int h = 0; h < CW; h += 8) {
                 const int i0 = wg * CW + h;
-                float er[8], ei[8], xr[8], xi[8];
-                umma::tmem_ld8(tmem_lane_addr(tbase, i0), er);
-                umma::tmem_ld8(tmem_lane_addr(tbase, W + i0), ei);
-                umma::tmem_ld8(tmem_lane_addr(tbase, 2 * W + i0), xr);
-                umma::tmem_ld8(tmem_lane_addr(tbase, 3 * W + i0), xi);
+                float v4[4][8];
+                const uint32_t ad[4] = {tmem_lane_addr(tbase, i0), tmem_lane_addr(tbase, W + i0),
+                                        tmem_lane_addr(tbase, 2 * W + i0), tmem_lane_addr(tbase, 3 * W + i0)};
+                tmem_ld8_multi<4>(ad, v4);
+                const float *er = v4[0], *ei = v4[1], *xr = v4[2], *xi = v4[3];
                 uint32_t hh[4], ll[4], dx[4], dy[4], dz[4];
 #pragma unroll
                 for (int u = 0; u < 8; u += 2) {
@@ -787,16 +916,15 @@ __global__ void __launch_bounds__(S2_THREADS, 1) k_stage2p(SplitDev P, int ntile
                            (er[u + 1] * er[u + 1] + ei[u + 1] * ei[u + 1]) * P.sc.cI, hh[u / 2], ll[u / 2]);
                     dx[u / 2] = pack_h2(ipx(er, ei, xr, xi, u, P.sc.cIx), ipx(er, ei, xr, xi, u + 1, P.sc.cIx));
                 }
-                umma::tmem_ld8(tmem_lane_addr(tbase, 4 * W + i0), xr);
-                umma::tmem_ld8(tmem_lane_addr(tbase, 5 * W + i0), xi);
+                float w4[4][8];
+                const uint32_t bd[4] = {tmem_lane_addr(tbase, 4 * W + i0), tmem_lane_addr(tbase, 5 * W + i0),
+                                        tmem_lane_addr(tbase, 6 * W + i0), tmem_lane_addr(tbase, 7 * W + i0)};
+                tmem_ld8_multi<4>(bd, w4);
 #pragma unroll
-                for (int u = 0; u < 8; u += 2)
-                    dy[u / 2] = pack_h2(ipx(er, ei, xr, xi, u, P.sc.cIy), ipx(er, ei, xr, xi, u + 1, P.sc.cIy));
-                umma::tmem_ld8(tmem_lane_addr(tbase, 6 * W + i0), xr);
-                umma::tmem_ld8(tmem_lane_addr(tbase, 7 * W + i0), xi);
-#pragma unroll
-                for (int u = 0; u < 8; u += 2)
-                    dz[u / 2] = pack_h2(ipx(er, ei, xr, xi, u, P.sc.cIz), ipx(er, ei, xr, xi, u + 1, P.sc.cIz));
+                for (int u = 0; u < 8; u += 2) {
+                    dy[u / 2] = pack_h2(ipx(er, ei, w4[0], w4[1], u, P.sc.cIy), ipx(er, ei, w4[0], w4[1], u + 1, P.sc.cIy));
+                    dz[u / 2] = pack_h2(ipx(er, ei, w4[2], w4[3], u, P.sc.cIz), ipx(er, ei, w4[2], w4[3], u + 1, P.sc.cIz));
+                }
                 const uint32_t off = kmajor_off(row, i0, W);
                 store4w(a3t + 0 * arr3 + off, hh);
                 store4w(a3t + 1 * arr3 + off, ll);
@@ -1120,10 +1248,6 @@ constexpr int S45_MIN_POOL = 1024;  // and the pool size (small batches favour m
 
 __host__ __device__ inline size_t s45_roi_bytes(int R) { return ((size_t)R * R * 4 + 127) / 128 * 128; }
 
-__device__ __forceinline__ void warp_arrive(uint64_t* mbar) {
-    __syncwarp();
-    if ((threadIdx.x & 31) == 0) umma::mbar_arrive(mbar);
-}
 
 __global__ void __launch_bounds__(S45_THREADS, 1) k_stage45p(SplitDev P, const float* rois, const float* scmos) {
     extern __shared__ __align__(1024) char smem[];
@@ -1245,13 +1369,17 @@ __global__ void __launch_bounds__(S45_THREADS, 1) k_stage45p(SplitDev P, const f
         umma::fence_after_sync();
         const uint32_t tb = tbase + b * NT;
         for (int c0 = 4 * wg; c0 < RP; c0 += 4 * NWG) {
+            uint32_t r[4][4];
 #pragma unroll
-            for (int m = 0; m < 4; ++m) {
-                float v[4];
-                umma::tmem_ld4(tmem_lane_addr(tb, m * RP + c0), v);
-                if (jp < R)
-                    for (int u = 0; u < 4 && c0 + u < R; ++u) Tm[m * MS + (c0 + u) * RS + jp] = v[u] * P.sc.cT[m];
-            }
+            for (int m = 0; m < 4; ++m) umma::tmem_ld4_nw(tmem_lane_addr(tb, m * RP + c0), r[m]);
+            umma::tmem_wait_ld();
+#pragma unroll
+            for (int m = 0; m < 4; ++m)
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    asm volatile("" : "+r"(r[m][u]));
+                    if (jp < R && c0 + u < R) Tm[m * MS + (c0 + u) * RS + jp] = __uint_as_float(r[m][u]) * P.sc.cT[m];
+                }
         }
         umma::fence_before_sync();
         warp_arrive(&tfree[b]);
@@ -1289,6 +1417,7 @@ __global__ void __launch_bounds__(S45_THREADS, 1) k_stage45p(SplitDev P, const f
 #pragma unroll
         for (int k = 0; k < 30; ++k) sh[k] = 0.f;
         bool bad = false;
+#pragma unroll 2
         for (int k = t; k < RR; k += E45_THREADS) {
             const int ip = k / R, to = ip * RS + (k - ip * R);
             const float v = Tm[to], sgn = v < 0 ? -1.f : 1.f, psi = fabsf(v) * invS;
@@ -1762,7 +1891,9 @@ __global__ void k_init_slots(SplitDev P, const double* init, int n, FitParamsDev
 }
 
 // ---------------------------------------------------------------- host -----
-static size_t smem_stage1(const SplitPlanHost& pl) { return (size_t)768 * pl.K1 + 2 * (size_t)12 * pl.IC * pl.K1; }
+static size_t smem_stage1p(const SplitPlanHost& pl) {
+    return (size_t)(pl.K1 / 16) * s2_slab_bytes(pl.W) + (size_t)S1_NBQ * s1_qring_bytes(pl.W);
+}
 static size_t smem_stage2p(const SplitPlanHost& pl) {
     return (size_t)(pl.K1 / 16) * s2_slab_bytes(pl.W) + (size_t)S2_NBUF * s2_ring_bytes(pl.W);
 }
@@ -1835,6 +1966,23 @@ struct SplitPool {
     size_t s1 = 0, s2 = 0, s3 = 0, s4 = 0, s45 = 0, sf = 0;
 };
 
+static cudaError_t stage1_attr(int W, size_t smem) {
+    const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    if (W == 32) return cudaFuncSetAttribute(k_stage1p<32>, a, (int)smem);
+    if (W == 64) return cudaFuncSetAttribute(k_stage1p<64>, a, (int)smem);
+    return cudaFuncSetAttribute(k_stage1p<128>, a, (int)smem);
+}
+
+static void launch_stage1(zola_ctx* ctx, const SplitPool& sp, int ntiles, cudaStream_t st) {
+    const int grid = std::min(ntiles, ctx->num_sms);
+    if (sp.D.W == 32)
+        k_stage1p<32><<<grid, S1_THREADS, sp.s1, st>>>(sp.D, ntiles);
+    else if (sp.D.W == 64)
+        k_stage1p<64><<<grid, S1_THREADS, sp.s1, st>>>(sp.D, ntiles);
+    else
+        k_stage1p<128><<<grid, S1_THREADS, sp.s1, st>>>(sp.D, ntiles);
+}
+
 static cudaError_t stage2_attr(int W, size_t smem) {
     const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
     if (W == 32) return cudaFuncSetAttribute(k_stage2p<32>, a, (int)smem);
@@ -1865,11 +2013,15 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
     SplitPlanHost* pl = get_plan(p, w, ctx->err);
     if (!pl) return ZOLA_E_CUDA;
     sp.pl = pl;
+    if (w->W == 128 && 2 * (p->D <= 32 ? 32 : 64) != 128) {
+        ctx->err = "split path: a 128 window needs a pupil disk of more than 32 rows";
+        return ZOLA_E_UNSUPPORTED;
+    }
     if (w->W != 32 && w->W != 64 && w->W != 128) {
         ctx->err = "split path: window sizes 32, 64 and 128 only";
         return ZOLA_E_UNSUPPORTED;
     }
-    sp.s1 = smem_stage1(*pl); sp.s2 = smem_stage2p(*pl); sp.s3 = smem_stage3(*pl); sp.s4 = smem_stage4(*pl);
+    sp.s1 = smem_stage1p(*pl); sp.s2 = smem_stage2p(*pl); sp.s3 = smem_stage3(*pl); sp.s4 = smem_stage4(*pl);
     sp.s45 = (size_t)2 * 128 * pl->W * 2 + (size_t)S45_NBUF * 2 * 32 * 4 * pl->RP + 4 * s45_roi_bytes(pl->R) +
              (size_t)4 * pl->R * tm_stride(pl->R) * 4;
     if (sp.s1 > 227 * 1024 || sp.s2 > 227 * 1024 || sp.s3 > 227 * 1024 || sp.s4 > 227 * 1024 ||
@@ -1895,10 +2047,10 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
     char* base = (char*)ctx->scratch;
     SplitDev& D = sp.D;
     D = SplitDev{};
-    D.R = pl->R; D.W = pl->W; D.D = pl->D; D.DP = pl->DP; D.K1 = pl->K1; D.IC = pl->IC; D.NCH = pl->NCH;
+    D.R = pl->R; D.W = pl->W; D.D = pl->D; D.DP = pl->DP; D.K1 = pl->K1;
     D.RP = pl->RP; D.G1 = pl->G1; D.G2 = pl->G2; D.NT4 = pl->NT4; D.P = P; D.a0 = p->a0; D.N = p->N;
     D.zfocus = p->o.zfocus;
-    D.bc_hi = pl->d_bc_hi; D.bc_lo = pl->d_bc_lo; D.gt_hi = pl->d_gt_hi; D.gt_lo = pl->d_gt_lo;
+    D.gt_hi = pl->d_gt_hi; D.gt_lo = pl->d_gt_lo;
     D.g128_hi = pl->d_g128_hi; D.g128_lo = pl->d_g128_lo;
     D.bc2_hi = pl->d_bc2_hi; D.bc2_lo = pl->d_bc2_lo; D.NCH2 = pl->NCH2; D.bcs = pl->d_bcs;
     D.pupf = pl->d_pupf; D.phase0 = pl->d_phase0; D.kz = pl->d_kz; D.kx = pl->d_kx; D.ky = pl->d_ky;
@@ -1915,7 +2067,7 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
     D.err = D.queue + 2;
     D.sc = pl->sc;
     ZOLA_CUDA_CHECK(cudaMemsetAsync(D.a4, 0, b_a4, st), ctx);
-    ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_stage1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.s1), ctx);
+    ZOLA_CUDA_CHECK(stage1_attr(pl->W, sp.s1), ctx);
     ZOLA_CUDA_CHECK(stage2_attr(pl->W, sp.s2), ctx);
     ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_stage3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.s3), ctx);
     ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_stage4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.s4), ctx);
@@ -1931,7 +2083,7 @@ static void launch_stages123(zola_ctx* ctx, const SplitPool& sp, cudaStream_t st
     const SplitPlanHost& pl = *sp.pl;
     const int P = sp.D.P;
     prof_begin(ctx, 0, st);
-    k_stage1<<<P / pl.G1, SPLIT_THREADS, sp.s1, st>>>(sp.D);
+    launch_stage1(ctx, sp, P / pl.G1, st);
     prof_end(ctx, st);
     prof_begin(ctx, 1, st);
     launch_stage2(ctx, sp, P / pl.G2, st);
@@ -2008,7 +2160,7 @@ int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d
         for (int k = 0; k < 4; ++k) {
             if (fused) {
                 prof_begin(ctx, 0, st);
-                k_stage1<<<P / sp.pl->G1, SPLIT_THREADS, sp.s1, st>>>(D);
+                launch_stage1(ctx, sp, P / sp.pl->G1, st);
                 prof_end(ctx, st);
                 prof_begin(ctx, 1, st);
                 k_fused25<<<P / sp.pl->G2, SPLIT_THREADS, sp.sf, st>>>(D, d_rois, d_scmos, d_init, n, fp, d_out5, d_crlb5, d_nll,
