@@ -24,12 +24,13 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 # DRAM bytes per slot of one launch (ncu dram__bytes_read.sum + dram__bytes_write.sum
-# of one launch per kernel, 48x48 tetrapod class, full pool of 4096 slots).
-NCU_TRAFFIC = {("tetra48", "split_stage1_pupil_dft"): (0.960000e6 + 478.294016e6) / 4096,
-               ("tetra48", "split_stage2_window_dft"): (537.137152e6 + 618.686720e6) / 4096,
-               ("tetra48", "split_stage3_blur_rows"): (671.153920e6 + 366.961152e6) / 4096,
-               ("tetra48", "split_stage4_blur_cols"): (536.933120e6 + 131.593728e6) / 4096,
-               ("tetra48", "split_stage5_likelihood_lm"): (233.258752e6 + 4.537088e6) / 4096}
+# of one launch per kernel, 48x48 tetrapod class, full pool of 4096 slots; stage 4 is
+# the fused column-blur/likelihood kernel and stage 5 the LM step for this class).
+NCU_TRAFFIC = {("tetra48", "split_stage1_pupil_dft"): (1.070080e6 + 476.936448e6) / 4096,
+               ("tetra48", "split_stage2_window_dft"): (537.341952e6 + 624.652288e6) / 4096,
+               ("tetra48", "split_stage3_blur_rows"): (671.155456e6 + 363.580928e6) / 4096,
+               ("tetra48", "split_stage4_blur_cols"): (441.092608e6 + 1.092864e6) / 4096,
+               ("tetra48", "split_stage5_likelihood_lm"): (2.430720e6 + 0.0) / 4096}
 
 METRIC = "MLE ROI fits/sec at ≤0.5 nm vs FP64 oracle (batched split-prec vs plain GPU)"
 UNIT = "ROI fits/s"
@@ -496,7 +497,7 @@ def main():
                 "unit": "TFLOP/s", "frac": round(achieved / peak_tf, 4), "peak_source": peak_src,
                 "traffic": None if traffic is None else int(traffic * min(args.pool or 4096, 32768)),
                 "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu launch of this kernel on "
-                                "this class (4000 slots), scaled to a full pool launch by slots",
+                                "this class (4096 slots), scaled to the pool by slots",
                 "stages_all_classes": stage_table, "per_class": by_class,
                 "note": "achieved = algorithmic flops of the useful model evaluations (complex MAC = 8 flops) / "
                         "summed CUDA-event duration of that kernel's launches for that class"}
