@@ -8,28 +8,31 @@
 //   stage 2  E^T = S^T C^T (+ Ex, Ey, Ez)                rows (roi, j)   K = 2DP
 //            epilogue: I = |E|^2, I_t = 2 Re(conj(E) E_t)
 //   stage 3  J^T = I G^T  (blur along the first image index)  rows (roi, j)  K = W
-//   stage 4  T  = J G^T   (blur along the second index)       rows (map, i') K = W
+//   stage 4  T^T = G J^T  (blur along the second index, transposed so that a
+//            TMEM lane holds one pixel column of all four maps)    K = W
 //   stage 5  likelihood, gradient, Gauss-Newton Hessian and Fisher sums in
 //            FP32 with Kahan compensation, then the FP64 5x5 LM solve, damping
 //            and convergence test; converged slots are retired and refilled
 //            from the ROI queue (a device counter).
 //
 // C is the W x D partial-DFT matrix, CK = C diag(i k) its x/y derivative, Q the
-// pupil field (built in registers from the pupil tables and the slot's trial
-// x, y, z), G the R x W circular-blur matrix (see optics.cpp).  Complex
-// products are real GEMMs on [re | im] operands.  Every operand that sets the
-// likelihood value (Q, S, E, I, J of the model itself, and the constants C, G)
-// is an FP16 hi + lo pair and multiplied with three products
-// (hi*hi + hi*lo + lo*hi, FP32 accumulation): about 2^-22 relative.  The
-// derivative maps only enter the gradient and the Hessian; their operands are
-// single FP16 products, whose rounding moves the optimum by about
-// 2^-11 x CRLB (~0.01 nm), far below the 0.5 nm budget.
+// pupil field (built from the pupil tables and the slot's trial x, y, z), G
+// the R x W circular-blur matrix (see optics.cpp).  Complex products are real
+// GEMMs on [re | im] operands.  Every operand that sets the likelihood value
+// (Q, S, E, I, J of the model itself, and the constants C, G) is an FP16 hi +
+// lo pair and multiplied with three products (hi*hi + hi*lo + lo*hi, FP32
+// accumulation): about 2^-22 relative.  The derivative maps only enter the
+// gradient and the Hessian; their operands are single FP16 products, whose
+// rounding moves the optimum by about 2^-11 x CRLB (~0.01 nm), far below the
+// 0.5 nm budget.
 //
-// All operands use the canonical no-swizzle layouts of umma.h.  Intermediate
-// operands travel through a global (L2-resident for moderate pools) slab laid
-// out exactly as the shared-memory tiles, so each stage fetches a tile with
-// 1-D bulk (TMA) copies.  Scales are powers of two chosen from host-side bounds
-// so no FP16 value overflows; they are exact and undone in FP32.
+// Stages 1 and 2 are persistent kernels that keep the DFT constants in shared
+// memory and issue N = 256 MMAs; for large ROIs stages 4 and 5 run as one
+// persistent kernel plus an LM kernel.  All operands use the canonical
+// no-swizzle layouts of umma.h.  Intermediate operands travel through global
+// slabs laid out as the shared-memory tiles (or K-slabs of them), fetched with
+// 1-D bulk (TMA) copies.  Scales are powers of two chosen from host-side
+// bounds so no FP16 value overflows; they are exact and undone in FP32.
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
