@@ -454,7 +454,10 @@ def main():
     acc["converged_frac"] = float(np.mean(conv))
     fp64_value = n_total / t_job64
 
-    # roofline of the dominant tensor kernel (algorithmic flops: complex MAC = 8 flops)
+    # roofline of the dominant kernel.  Each split stage has an algorithmic flop
+    # count (a complex MAC = 8 flops) and an algorithmic DRAM byte count (the
+    # operands it must read and write per evaluation); its bound is the larger
+    # of the two time floors at the measured peaks.
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -462,20 +465,26 @@ def main():
     except OSError:
         pass
     peak_tf = peaks.get("bf16_tflops_sustained", 1400.0)
-    peak_src = "of measured (sustained)" if "bf16_tflops_sustained" in peaks else "of fallback"
-    # Per class and tensor stage: algorithmic flops of the useful evaluations
-    # (a complex MAC = 8 flops) / that kernel's summed CUDA-event time in the
-    # per-class pass.  The headline entry is the (class, kernel) pair with the
-    # largest device time; its DRAM traffic per launch is the ncu figure below.
-    flops = {}
+    peak_gbs = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "of measured" if "bf16_tflops_sustained" in peaks and "hbm_gbs" in peaks else "of fallback"
+    flops, nbytes = {}, {}
+    fused45 = lambda R: R >= 40 and (args.pool or 4096) >= 1024  # noqa: E731  (the library's path choice)
     for j in job:
         R, N = j["cls"]["R"], j["cls"]["N"]
         W, D = window(R, N), disk_rows(N)
+        DP = 32 if D <= 32 else 64
+        K1, RP = 2 * DP, (R + 15) // 16 * 16
         ev = iters[j["cls"]["name"]]
+        a2, a3, jb, roi, maps = 8 * W * K1, 10 * W * W, 16 * RP * W, 4 * R * R, 16 * R * R
         flops[j["cls"]["name"]] = {"split_stage1_pupil_dft": ev * 3 * 8 * W * D * D,
                                    "split_stage2_window_dft": ev * 4 * 8 * W * W * D,
                                    "split_stage3_blur_rows": ev * 4 * 2 * R * W * W,
                                    "split_stage4_blur_cols": ev * 4 * 2 * R * R * W}
+        nbytes[j["cls"]["name"]] = {"split_stage1_pupil_dft": ev * a2,
+                                    "split_stage2_window_dft": ev * (a2 + a3),
+                                    "split_stage3_blur_rows": ev * (a3 + jb),
+                                    "split_stage4_blur_cols": ev * (jb + (roi if fused45(R) else maps)),
+                                    "split_stage5_likelihood_lm": ev * (0 if fused45(R) else maps + roi)}
     by_class = {}
     best = None
     for name, st in class_stats.items():
@@ -484,23 +493,40 @@ def main():
             if not n_k:
                 continue
             e = {"ms": round(ms_k, 3), "launches": n_k}
-            if k in flops[name] and ms_k > 0:
-                tf = flops[name][k] / (ms_k / 1000.0) / 1e12
-                e.update(tflops=round(tf, 2), frac=round(tf / peak_tf, 4))
-                if best is None or ms_k > best[2]:
-                    best = (name, k, ms_k, tf, n_k)
+            sec = ms_k / 1000.0
+            if ms_k > 0 and k in flops[name]:
+                tf = flops[name][k] / sec / 1e12
+                e.update(tflops=round(tf, 2), tensor_frac=round(tf / peak_tf, 4))
+            if ms_k > 0 and k in nbytes[name]:
+                gbs = nbytes[name][k] / sec / 1e9
+                e.update(gbs=round(gbs, 1), hbm_frac=round(gbs / peak_gbs, 4))
+            if ms_k > 0 and k in nbytes[name] and (best is None or ms_k > best[2]):
+                best = (name, k, ms_k)
             by_class[name][k] = e
     stage_table = {k: {"ms": round(v[0], 3), "launches": v[1]} for k, v in stats.items() if v[1]}
-    name, dom, _, achieved, _ = best
+    name, dom, _ = best
+    ent = by_class[name][dom]
+    hbm_floor = nbytes[name].get(dom, 0) / (peak_gbs * 1e9)
+    tensor_floor = flops[name].get(dom, 0) / (peak_tf * 1e12)
     traffic = NCU_TRAFFIC.get((name, dom))
-    roofline = {"bound": "tensor", "kernel": dom, "class": name, "achieved": round(achieved, 2), "peak": peak_tf,
-                "unit": "TFLOP/s", "frac": round(achieved / peak_tf, 4), "peak_source": peak_src,
-                "traffic": None if traffic is None else int(traffic * min(args.pool or 4096, 32768)),
-                "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu launch of this kernel on "
-                                "this class (4096 slots), scaled to the pool by slots",
-                "stages_all_classes": stage_table, "per_class": by_class,
-                "note": "achieved = algorithmic flops of the useful model evaluations (complex MAC = 8 flops) / "
-                        "summed CUDA-event duration of that kernel's launches for that class"}
+    if hbm_floor >= tensor_floor:
+        roofline = {"bound": "hbm", "achieved": ent["gbs"], "peak": peak_gbs, "unit": "GB/s", "frac": ent["hbm_frac"],
+                    "tensor_achieved_tflops": ent.get("tflops"), "tensor_frac": ent.get("tensor_frac")}
+    else:
+        roofline = {"bound": "tensor", "achieved": ent["tflops"], "peak": peak_tf, "unit": "TFLOP/s",
+                    "frac": ent["tensor_frac"], "hbm_achieved_gbs": ent.get("gbs"), "hbm_frac": ent.get("hbm_frac")}
+    roofline.update({
+        "kernel": dom, "class": name, "peak_source": peak_src,
+        "traffic": None if traffic is None else int(traffic * min(args.pool or 4096, 32768)),
+        "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu launch of this kernel on "
+                        "this class (4096 slots), scaled to the pool by slots",
+        "algorithmic_bytes_per_launch": None if dom not in nbytes[name] else
+        int(nbytes[name][dom] / max(1, iters[name]) * min(args.pool or 4096, 32768)),
+        "stages_all_classes": stage_table, "per_class": by_class,
+        "note": "achieved = algorithmic bytes (operands each evaluation must read and write: A2 8*W*K1, A3 "
+                "10*W^2, J 16*RP*W, ROI 4*R^2, maps 16*R^2 bytes) or algorithmic flops (complex MAC = 8 flops) of "
+                "the useful model evaluations / summed CUDA-event duration of that kernel's launches for that "
+                "class; the bound is the larger floor at the measured peaks (copy GB/s, sustained bf16 TFLOP/s)"})
 
     # end to end through the host C-ABI (pinned host buffers, H2D + D2H inside the call)
     e2e = None
