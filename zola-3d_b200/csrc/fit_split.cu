@@ -52,7 +52,7 @@ using umma::mnmajor_off;
 // quadrant = warp % 4, so thread t owns tile row t % 128) and split the column
 // work of every epilogue and of the Q build; the LM step runs one thread per slot.
 constexpr int SPLIT_THREADS = 512;
-constexpr int LM_THREADS = 128;
+constexpr int LM_THREADS = 32;  // one warp per block: the FP64 LM step of 4096 slots spreads over 128 SMs
 
 // ---------------------------------------------------------------- plan ------
 struct SplitScales {
@@ -1088,18 +1088,16 @@ __device__ __forceinline__ double warp_sum(double x) {
     return x;
 }
 
+constexpr int NSUM = NRED + 1;  // sums per slot: NRED + the non-positive-model flag
 constexpr int S5_THREADS = 128;
 constexpr int S5_SLOTS = S5_THREADS / 32;  // one warp per slot
 constexpr int S5_UNROLL = 4;               // pixels per lane whose loads are in flight together
 
 // One warp per slot: likelihood sums at the trial point (per-pixel terms in
 // FP32; the likelihood and gradient with Kahan compensation, the Hessian and
-// Fisher terms plain; lane partials combined in FP64), then the FP64 LM step on
-// lane 0.
-__global__ void __launch_bounds__(S5_THREADS) k_stage5(SplitDev P, const float* rois, const float* scmos,
-                                                        const double* init, int n,
-                                                        FitParamsDev prm, double* out5, double* crlb5,
-                                                        double* nll_out, int* st_out, int* it_out) {
+// Fisher terms plain; lane partials combined in FP64), written to P.sums for
+// the LM step (k_lm).
+__global__ void __launch_bounds__(S5_THREADS) k_stage5(SplitDev P, const float* rois, const float* scmos) {
     const int lane = threadIdx.x & 31;
     const int slot = blockIdx.x * S5_SLOTS + (threadIdx.x >> 5);
     if (slot >= P.P) return;
@@ -1191,41 +1189,9 @@ __global__ void __launch_bounds__(S5_THREADS) k_stage5(SplitDev P, const float* 
     for (int k = 0; k < 30; ++k) tot[6 + k] = warp_sum((double)sh[k]);
     const bool anybad = __any_sync(0xffffffffu, bad);
     if (lane != 0) return;
-    double nll = anybad ? INFINITY : tot[0], g[5], H[25], F[25];
-    for (int q = 0; q < 5; ++q) g[q] = tot[1 + q];
-    int o = 6;
-    for (int q = 0; q < 5; ++q)
-        for (int r2 = 0; r2 <= q; ++r2) {
-            H[q * 5 + r2] = H[r2 * 5 + q] = tot[o];
-            F[q * 5 + r2] = F[r2 * 5 + q] = tot[o + 15];
-            ++o;
-        }
-    LMState& st = P.lm[slot];
-    if (P.slot_phase[slot] == 0) {
-        for (int q = 0; q < 5; ++q) st.th[q] = st.trial[q];
-        lm_start(st, nll, g, H, F, prm);
-        P.slot_phase[slot] = 1;
-    } else {
-        lm_update(st, nll, g, H, F, prm);
-    }
-    if (lm_propose(st, prm)) return;
-    // retire
-    for (int q = 0; q < 5; ++q) out5[5 * roi + q] = st.th[q];
-    if (nll_out) nll_out[roi] = st.nll;
-    if (st_out) st_out[roi] = st.status;
-    if (it_out) it_out[roi] = st.evals;
-    if (crlb5) lm_crlb(st.F, crlb5 + 5 * roi);
-    // refill from the queue
-    const int next = atomicAdd(P.queue, 1);
-    if (next < n) {
-        P.slot_roi[slot] = next;
-        P.slot_phase[slot] = 0;
-        for (int q = 0; q < 5; ++q) st.trial[q] = init[5 * next + q];
-        lm_clamp(st.trial, prm);
-    } else {
-        P.slot_roi[slot] = -1;
-        atomicSub(P.active, 1);
-    }
+    double* out = P.sums + (size_t)slot * NSUM;
+    for (int q = 0; q < NRED; ++q) out[q] = tot[q];
+    out[NRED] = anybad ? 1.0 : 0.0;
 }
 
 // ---------------------------------- stages 4 + 5 sums (persistent) -----
@@ -1242,7 +1208,6 @@ __global__ void __launch_bounds__(S5_THREADS) k_stage5(SplitDev P, const float* 
 // combined in FP64.  The next slot's MMAs run in the other TMEM buffer
 // meanwhile.  The sums and a non-positive-model flag go to P.sums; k_lm
 // applies the FP64 LM step.
-constexpr int NSUM = NRED + 1;
 constexpr int E45_THREADS = 384;                 // 12 epilogue warps: three per TMEM lane quadrant
 constexpr int S45_THREADS = E45_THREADS + 64;    // + producer warp + MMA warp
 constexpr int S45_NBUF = 4;
@@ -1512,7 +1477,8 @@ __global__ void k_lm(SplitDev P, const double* init, int n, FitParamsDev prm, do
             F[q * 5 + r2] = F[r2 * 5 + q] = tot[o + 15];
             ++o;
         }
-    LMState& st = P.lm[slot];
+    // the step works on a local copy of the slot state (written back once)
+    LMState st = P.lm[slot];
     if (P.slot_phase[slot] == 0) {
         for (int q = 0; q < 5; ++q) st.th[q] = st.trial[q];
         lm_start(st, nll, g, H, F, prm);
@@ -1520,7 +1486,9 @@ __global__ void k_lm(SplitDev P, const double* init, int n, FitParamsDev prm, do
     } else {
         lm_update(st, nll, g, H, F, prm);
     }
-    if (lm_propose(st, prm)) return;
+    const bool more = lm_propose(st, prm);
+    P.lm[slot] = st;
+    if (more) return;
     // retire
     for (int q = 0; q < 5; ++q) out5[5 * roi + q] = st.th[q];
     if (nll_out) nll_out[roi] = st.nll;
@@ -1532,8 +1500,9 @@ __global__ void k_lm(SplitDev P, const double* init, int n, FitParamsDev prm, do
     if (next < n) {
         P.slot_roi[slot] = next;
         P.slot_phase[slot] = 0;
-        for (int q = 0; q < 5; ++q) st.trial[q] = init[5 * next + q];
-        lm_clamp(st.trial, prm);
+        double* tr = P.lm[slot].trial;
+        for (int q = 0; q < 5; ++q) tr[q] = init[5 * next + q];
+        lm_clamp(tr, prm);
     } else {
         P.slot_roi[slot] = -1;
         atomicSub(P.active, 1);
@@ -2185,10 +2154,11 @@ int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d
             } else {
                 launch_model_stages(ctx, sp, st);
                 prof_begin(ctx, 4, st);
-                k_stage5<<<(P + S5_SLOTS - 1) / S5_SLOTS, S5_THREADS, 0, st>>>(D, d_rois, d_scmos, d_init, n, fp, d_out5,
-                                                                              d_crlb5, d_nll, d_status, d_iters);
+                k_stage5<<<(P + S5_SLOTS - 1) / S5_SLOTS, S5_THREADS, 0, st>>>(D, d_rois, d_scmos);
+                k_lm<<<(P + LM_THREADS - 1) / LM_THREADS, LM_THREADS, 0, st>>>(D, d_init, n, fp, d_out5, d_crlb5,
+                                                                            d_nll, d_status, d_iters);
                 prof_end(ctx, st);
-                ctx->launches++;
+                ctx->launches += 2;
             }
         }
         rounds += 4;
