@@ -1204,9 +1204,8 @@ __global__ void __launch_bounds__(S5_THREADS) k_stage5(SplitDev P, const float* 
 // from TMEM and form the normalisation, likelihood, gradient, Gauss-Newton
 // Hessian and Fisher sums (process/cpu/Localization.java:1125-1143 with the
 // Jacobian of psi = |T|/sum|T| of PSFPhase.java:602-629): per-pixel terms in
-// FP32, likelihood and gradient with Kahan compensation, thread partials
-// combined in FP64.  The next slot's MMAs run in the other TMEM buffer
-// meanwhile.  The sums and a non-positive-model flag go to P.sums; k_lm
+// FP32 (a thread sums a few pixels), thread partials combined in FP64.  The
+// next slot's MMAs run in the other TMEM buffer meanwhile.  The sums and a non-positive-model flag go to P.sums; k_lm
 // applies the FP64 LM step.
 constexpr int E45_THREADS = 384;                 // 12 epilogue warps: three per TMEM lane quadrant
 constexpr int S45_THREADS = E45_THREADS + 64;    // + producer warp + MMA warp
@@ -1336,6 +1335,8 @@ __global__ void __launch_bounds__(S45_THREADS, 1) k_stage45p(SplitDev P, const f
         umma::mbar_wait(&acc[b], ph, P.err);
         umma::fence_after_sync();
         const uint32_t tb = tbase + b * NT;
+        // the normalisation sums accumulate over the values this thread copies
+        float ns[4] = {0, 0, 0, 0};
         for (int c0 = 4 * wg; c0 < RP; c0 += 4 * NWG) {
             uint32_t r[4][4];
 #pragma unroll
@@ -1344,28 +1345,28 @@ __global__ void __launch_bounds__(S45_THREADS, 1) k_stage45p(SplitDev P, const f
 #pragma unroll
             for (int m = 0; m < 4; ++m)
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    asm volatile("" : "+r"(r[m][u]));
-                    if (jp < R && c0 + u < R) Tm[m * MS + (c0 + u) * RS + jp] = __uint_as_float(r[m][u]) * P.sc.cT[m];
+                for (int u = 0; u < 4; ++u) asm volatile("" : "+r"(r[m][u]));
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (jp >= R || c0 + u >= R) continue;
+                float v[4];
+#pragma unroll
+                for (int m = 0; m < 4; ++m) {
+                    v[m] = __uint_as_float(r[m][u]) * P.sc.cT[m];
+                    Tm[m * MS + (c0 + u) * RS + jp] = v[m];
                 }
+                const float sg = v[0] < 0 ? -1.f : 1.f;
+                ns[0] += fabsf(v[0]);
+                ns[1] += sg * v[1];
+                ns[2] += sg * v[2];
+                ns[3] += sg * v[3];
+            }
         }
         umma::fence_before_sync();
         warp_arrive(&tfree[b]);
         if (vec) umma::mbar_wait(&rfull[b], ph, P.err);
-        epi_bar<E45_THREADS>();
-        // normalisation sums
-        float ns[4] = {0, 0, 0, 0}, nc = 0.f;
-        for (int k = t; k < RR; k += E45_THREADS) {
-            const int ip = k / R, o = ip * RS + (k - ip * R);
-            const float v = Tm[o], sg = v < 0 ? -1.f : 1.f;
-            kahan_add(ns[0], nc, fabsf(v));
-            ns[1] += sg * Tm[MS + o];
-            ns[2] += sg * Tm[2 * MS + o];
-            ns[3] += sg * Tm[3 * MS + o];
-        }
         {
-            const double v0 = warp_sum((double)ns[0] - (double)nc), v1 = warp_sum(ns[1]), v2 = warp_sum(ns[2]),
-                         v3 = warp_sum(ns[3]);
+            const double v0 = warp_sum(ns[0]), v1 = warp_sum(ns[1]), v2 = warp_sum(ns[2]), v3 = warp_sum(ns[3]);
             if (lane == 0) { red[warp][0] = v0; red[warp][1] = v1; red[warp][2] = v2; red[warp][3] = v3; }
         }
         epi_bar<E45_THREADS>();
@@ -1379,9 +1380,11 @@ __global__ void __launch_bounds__(S45_THREADS, 1) k_stage45p(SplitDev P, const f
         const float A = (float)th[3], B = (float)th[4];
         const float* d = vec ? (const float*)(RO + b * 2 * roib) : rois + (size_t)roi * RR;
         const float* sv = !scmos ? nullptr : vec ? (const float*)(RO + b * 2 * roib + roib) : scmos + (size_t)roi * RR;
-        float sg6[6], cg6[6], sh[30];
+        // a thread sums about RR / 384 pixels before the FP64 combination across threads,
+        // so plain FP32 partials suffice here
+        float sg6[6], sh[30];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) { sg6[k] = 0.f; cg6[k] = 0.f; }
+        for (int k = 0; k < 6; ++k) sg6[k] = 0.f;
 #pragma unroll
         for (int k = 0; k < 30; ++k) sh[k] = 0.f;
         bool bad = false;
@@ -1398,10 +1401,10 @@ __global__ void __launch_bounds__(S45_THREADS, 1) k_stage45p(SplitDev P, const f
             const float mu = A * psi + B + (sv ? sv[k] : 0.f);
             if (!(mu > 0.f)) { bad = true; continue; }
             const float dk = d[k];
-            kahan_add(sg6[0], cg6[0], dk > 0.f ? mu - dk - dk * logf(mu / dk) : mu);
-            const float wgt = 1.f - dk / mu, wf = 1.f / mu, wh = dk * wf * wf;
+            sg6[0] += dk > 0.f ? mu - dk - dk * logf(mu / dk) : mu;
+            const float wf = 1.f / mu, wgt = 1.f - dk * wf, wh = dk * wf * wf;
 #pragma unroll
-            for (int q = 0; q < 5; ++q) kahan_add(sg6[1 + q], cg6[1 + q], wgt * jv[q]);
+            for (int q = 0; q < 5; ++q) sg6[1 + q] += wgt * jv[q];
             int o = 0;
 #pragma unroll
             for (int q = 0; q < 5; ++q)
@@ -1418,7 +1421,7 @@ __global__ void __launch_bounds__(S45_THREADS, 1) k_stage45p(SplitDev P, const f
         {
             double v[32];
 #pragma unroll
-            for (int k = 0; k < 6; ++k) v[k] = (double)sg6[k] - (double)cg6[k];
+            for (int k = 0; k < 6; ++k) v[k] = sg6[k];
 #pragma unroll
             for (int k = 0; k < 26; ++k) v[6 + k] = sh[k];
 #pragma unroll
