@@ -98,3 +98,61 @@ def test_fused_and_staged_split_kernels_agree(zpkg, ctx, N, R, zern):
     assert d[:, :3].max() * 1000 < 0.25
     assert np.median(d[:, :3]) * 1000 < 0.02
     assert (d[:, 3] / staged["theta"][ok, 3]).max() < 5e-4
+
+
+def _large_roi_job(psf, zpkg, R, n, seed, scmos=False):
+    """n tetrapod ROIs of side R drawn from the FP64 device model (Poisson noise),
+    with a detection-like start; optionally an sCMOS var/gain^2 map per ROI."""
+    rng = np.random.default_rng(seed)
+    truth = np.c_[rng.uniform(-0.11, 0.11, (n, 2)), rng.uniform(-0.8, 0.8, n), rng.lognormal(np.log(3000.0), 0.5, n),
+                  np.full(n, 25.0)]
+    psi = psf.model(R, truth[:, :3], precision=zpkg.ZOLA_PREC_FP64)
+    mu = truth[:, 3, None, None] * psi + truth[:, 4, None, None]
+    v = None
+    if scmos:
+        v = rng.uniform(0.5, 12.0, (n, R, R)).astype(np.float32)
+        mu = mu + v
+    rois = rng.poisson(mu).astype(np.float32)
+    init = truth.copy()
+    init[:, :2] = 0
+    init[:, 2] = np.round(truth[:, 2] / 0.1) * 0.1
+    init[:, 3] *= 0.9
+    return rois, init, v
+
+
+def _agree(a, b, zern):
+    ok = (a["status"] == 1) & (b["status"] == 1)
+    assert ok.mean() > 0.8
+    d = theta_diff(a["theta"][ok], b["theta"][ok], z_symmetric(zern))
+    assert d[:, :2].max() * 1000 <= 0.5
+    assert d[:, 2].max() * 1000 <= 1.0
+    assert (d[:, 3] / a["theta"][ok, 3]).max() <= 1e-3
+
+
+@pytest.mark.parametrize("R,scmos", [(48, False), (40, False), (48, True)])
+def test_large_roi_fused_likelihood_path(zpkg, ctx, R, scmos):
+    """ROIs of 40 px and more in a pool of at least 1024 slots take the persistent
+    column-blur + likelihood kernel (maps straight from TMEM) and the separate LM
+    kernel.  Its fits must agree with the plain FP64 fit and with the small-pool
+    path (column-blur maps through memory, warp-per-slot likelihood).  R = 40 is
+    the frame pipeline's ROI size (RP = 48 rows of padding); the sCMOS case adds
+    the var/gain^2 map, which the kernel copies beside the ROI."""
+    zern = tetrapod_zernike()
+    psf = make(zpkg, ctx, 128, zern)
+    n = 1100
+    rois, init, v = _large_roi_job(psf, zpkg, R, n, seed=40 + R + (7 if scmos else 0), scmos=scmos)
+    xymax = R * 0.11 / 2
+    p64 = zpkg.PSF.fit_params(-1.5, 1.5, xymax, max_iter=50, tol_xyz=1e-4, precision=zpkg.ZOLA_PREC_FP64)
+    psp = zpkg.PSF.fit_params(-1.5, 1.5, xymax, max_iter=50, tol_xyz=1e-4, precision=zpkg.ZOLA_PREC_SPLIT)
+    try:
+        ctx.set_pool(4096)  # pool = n >= 1024: fused kernel
+        fused = psf.fit(rois, init, psp, scmos=v)
+        ctx.set_pool(512)   # pool 512: maps through memory
+        small = psf.fit(rois, init, psp, scmos=v)
+    finally:
+        ctx.set_pool(0)
+    ref = psf.fit(rois, init, p64, scmos=v)
+    _agree(ref, fused, zern)
+    _agree(ref, small, zern)
+    assert np.all(fused["status"] != 0) and np.all(small["status"] != 0)  # every ROI fitted
+    psf.close()
