@@ -156,3 +156,41 @@ def test_large_roi_fused_likelihood_path(zpkg, ctx, R, scmos):
     _agree(ref, small, zern)
     assert np.all(fused["status"] != 0) and np.all(small["status"] != 0)  # every ROI fitted
     psf.close()
+
+
+def test_host_buffer_fit_streams_inputs_in_chunks(zpkg, ctx):
+    """Host-buffer fits copy the ROIs up in chunks while the fit runs, and the
+    slot pool takes only ROIs that have arrived.  Each ROI's fit does not depend
+    on the slot that runs it, so the result equals the device-buffer call bit for bit."""
+    import torch
+    dev = torch.device("cuda", 0)
+    zern = astig_zernike()
+    psf = make(zpkg, ctx, 64, zern)
+    n, R = 70000, 16  # about 70 MB of ROIs: three chunks
+    rng = np.random.default_rng(77)
+    truth = np.c_[rng.uniform(-0.11, 0.11, (n, 2)), rng.uniform(-0.5, 0.5, n), rng.lognormal(np.log(2000.0), 0.4, n),
+                  np.full(n, 20.0)]
+    psi = torch.empty((n, R, R), dtype=torch.float64, device=dev)
+    psf.model_dev(R, torch.tensor(truth[:, :3], device=dev), psi, stream=ctx.stream)
+    torch.cuda.synchronize()
+    a = torch.tensor(truth[:, 3], device=dev)[:, None, None]
+    g = torch.Generator(device=dev)
+    g.manual_seed(5)
+    rois_d = torch.poisson(a * psi + 20.0, generator=g).float()
+    init = truth.copy()
+    init[:, :2] = 0
+    init[:, 2] = np.round(truth[:, 2] / 0.1) * 0.1
+    prm = zpkg.PSF.fit_params(-1.0, 1.0, 0.88, max_iter=40, tol_xyz=1e-4, precision=zpkg.ZOLA_PREC_SPLIT)
+    rois_pinned = torch.empty(rois_d.shape, dtype=torch.float32, pin_memory=True)
+    rois_pinned.copy_(rois_d)
+    host = psf.fit(rois_pinned.numpy(), init, prm)
+    init_d = torch.tensor(init, device=dev)
+    out = [torch.zeros((n, 5), dtype=torch.float64, device=dev), torch.zeros((n, 5), dtype=torch.float64, device=dev),
+           torch.zeros(n, dtype=torch.float64, device=dev), torch.zeros(n, dtype=torch.int32, device=dev),
+           torch.zeros(n, dtype=torch.int32, device=dev)]
+    psf.fit_dev(rois_d, init_d, prm, *out, stream=ctx.stream)
+    torch.cuda.synchronize()
+    assert np.array_equal(host["theta"], out[0].cpu().numpy())
+    assert np.array_equal(host["status"], out[3].cpu().numpy())
+    assert (host["status"] == 1).mean() > 0.9
+    psf.close()

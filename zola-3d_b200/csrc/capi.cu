@@ -124,6 +124,7 @@ int zola_ctx_create(int device, zola_ctx** out) {
     c->device = device;
     c->num_sms = prop.multiProcessorCount;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&c->d_counter, 64 * sizeof(int)) != cudaSuccess) {
         delete c;
         return ZOLA_E_CUDA;
@@ -143,6 +144,9 @@ int zola_ctx_destroy(zola_ctx* ctx) {
     if (ctx->d_counter) cudaFree(ctx->d_counter);
     if (ctx->h_flags) cudaFreeHost(ctx->h_flags);
     for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
+    for (cudaEvent_t e : ctx->feed_ev) cudaEventDestroy(e);
+    cudaStreamSynchronize(ctx->copy_stream);
+    cudaStreamDestroy(ctx->copy_stream);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return ZOLA_OK;
@@ -284,7 +288,7 @@ namespace {
 
 int fit_dev_impl(zola_ctx* ctx, zola_psf* psf, int R, const float* d_rois, const float* d_scmos,
                  const double* d_init5, int n, const zola_fit_params* prm, double* d_out5, double* d_crlb5,
-                 double* d_nll, int* d_status, int* d_iters, void* stream) {
+                 double* d_nll, int* d_status, int* d_iters, void* stream, const zola::RoiFeed* feed = nullptr) {
     if (!ctx || !psf) return ZOLA_E_ARG;
     if (psf->ctx != ctx) return set_err(ctx, ZOLA_E_ARG, "psf belongs to another context");
     if (!check_fit_params(ctx, prm)) return ZOLA_E_ARG;
@@ -296,7 +300,9 @@ int fit_dev_impl(zola_ctx* ctx, zola_psf* psf, int R, const float* d_rois, const
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
     if (prm->precision == ZOLA_PREC_SPLIT)
         return launch_fit_split(ctx, psf, w, d_rois, d_scmos, d_init5, n, prm, d_out5, d_crlb5, d_nll, d_status, d_iters,
-                                st);
+                                st, feed);
+    if (feed && feed->n_chunks > 0)  // the FP64 form needs every input before it starts
+        ZOLA_CUDA_CHECK(cudaStreamWaitEvent(st, feed->ev[feed->n_chunks - 1], 0), ctx);
     return launch_fit_f64(ctx, psf, w, d_rois, d_scmos, d_init5, n, prm, d_out5, d_crlb5, d_nll, d_status, d_iters, st);
 }
 
@@ -325,10 +331,39 @@ int fit_host_impl(zola_ctx* ctx, zola_psf* psf, int R, const float* rois, const 
     int* dst = status ? (int*)(base + off_s) : nullptr;
     int* dit = iters ? (int*)(base + off_t) : nullptr;
     float* dv = scmos ? (float*)(base + off_v) : nullptr;
-    ZOLA_CUDA_CHECK(cudaMemcpyAsync(dr, rois, rr * nn * sizeof(float), cudaMemcpyHostToDevice, ctx->stream), ctx);
-    ZOLA_CUDA_CHECK(cudaMemcpyAsync(di, init5, 5 * nn * sizeof(double), cudaMemcpyHostToDevice, ctx->stream), ctx);
-    if (scmos) ZOLA_CUDA_CHECK(cudaMemcpyAsync(dv, scmos, rr * nn * sizeof(float), cudaMemcpyHostToDevice, ctx->stream), ctx);
-    int rc = fit_dev_impl(ctx, psf, R, dr, dv, di, n, prm, dout, dcr, dnll, dst, dit, ctx->stream);
+    // Inputs go up in chunks of about 32 MB on the copy stream (at most 64 chunks); the
+    // split fit starts on the first chunk and takes the others as they land.
+    constexpr int MAX_CHUNKS = 64;
+    while ((int)ctx->feed_ev.size() < MAX_CHUNKS) {
+        cudaEvent_t e;
+        ZOLA_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), ctx);
+        ctx->feed_ev.push_back(e);
+    }
+    size_t per = std::max<size_t>(1024, ((size_t)32 << 20) / (rr * sizeof(float) * (scmos ? 2 : 1)));
+    per = std::max(per, (nn + MAX_CHUNKS - 1) / MAX_CHUNKS);
+    int chunk_end[MAX_CHUNKS];
+    int nch = 0;
+    cudaStream_t cs = ctx->copy_stream;
+    ZOLA_CUDA_CHECK(cudaMemcpyAsync(di, init5, 5 * nn * sizeof(double), cudaMemcpyHostToDevice, cs), ctx);
+    for (size_t a = 0; a < nn; a += per, ++nch) {
+        const size_t b = std::min(nn, a + per);
+        ZOLA_CUDA_CHECK(cudaMemcpyAsync(dr + a * rr, rois + a * rr, (b - a) * rr * sizeof(float), cudaMemcpyHostToDevice,
+                                        cs), ctx);
+        if (scmos)
+            ZOLA_CUDA_CHECK(cudaMemcpyAsync(dv + a * rr, scmos + a * rr, (b - a) * rr * sizeof(float),
+                                            cudaMemcpyHostToDevice, cs), ctx);
+        ZOLA_CUDA_CHECK(cudaEventRecord(ctx->feed_ev[nch], cs), ctx);
+        chunk_end[nch] = (int)b;
+    }
+    zola::RoiFeed feed;
+    feed.n_chunks = nch;
+    feed.chunk_end = chunk_end;
+    feed.ev = ctx->feed_ev.data();
+    int rc = fit_dev_impl(ctx, psf, R, dr, dv, di, n, prm, dout, dcr, dnll, dst, dit, ctx->stream, &feed);
+    if (rc) {
+        cudaStreamSynchronize(cs);  // no copy may still write the staging area
+        return rc;
+    }
     if (rc) return rc;
     ZOLA_CUDA_CHECK(cudaMemcpyAsync(out5, dout, 5 * nn * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), ctx);
     if (crlb5) ZOLA_CUDA_CHECK(cudaMemcpyAsync(crlb5, dcr, 5 * nn * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), ctx);

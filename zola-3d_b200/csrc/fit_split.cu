@@ -97,6 +97,7 @@ struct SplitDev {
     int* queue;    // next ROI to hand out
     int* active;   // occupied slots
     int* err;      // bounded-wait timeout flag
+    int* navail;   // ROIs [0, *navail) are on the device (all n unless the inputs are still arriving)
     SplitScales sc;
 };
 
@@ -433,6 +434,39 @@ __device__ __forceinline__ bool tile_live(const SplitDev& P, int s0, int g) {
     bool live = false;
     for (int k = 0; k < g; ++k) live |= P.slot_roi[s0 + k] >= 0;
     return live;
+}
+
+// The next ROI of the queue among those already on the device, or -1.  With
+// every input on the device this is one atomicAdd.  While inputs are still
+// arriving, one lane of the warp takes a run of indices below the available
+// count for all the lanes that ask (compare-and-swap; the queue only advances,
+// so the loop ends), which keeps the contention per warp, not per slot.
+__device__ __forceinline__ int take_roi(const SplitDev& P, int n) {
+    const int avail = min(*(volatile const int*)P.navail, n);
+    if (avail >= n) {
+        const int q = atomicAdd(P.queue, 1);
+        return q < n ? q : -1;
+    }
+    const unsigned m = __activemask();
+    const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+    const int rank = __popc(m & ((1u << lane) - 1u)), cnt = __popc(m);
+    int base = 0, got = 0;
+    if (lane == leader) {
+        int q = *(volatile int*)P.queue;
+        while (q < avail) {
+            const int k = min(cnt, avail - q);
+            const int old = atomicCAS(P.queue, q, q + k);
+            if (old == q) {
+                base = q;
+                got = k;
+                break;
+            }
+            q = old;
+        }
+    }
+    base = __shfl_sync(m, base, leader);
+    got = __shfl_sync(m, got, leader);
+    return rank < got ? base + rank : -1;
 }
 
 // ----------------------------------------------- persistent-kernel helpers ----
@@ -1499,8 +1533,8 @@ __global__ void k_lm(SplitDev P, const double* init, int n, FitParamsDev prm, do
     if (it_out) it_out[roi] = st.evals;
     if (crlb5) lm_crlb(st.F, crlb5 + 5 * roi);
     // refill from the queue
-    const int next = atomicAdd(P.queue, 1);
-    if (next < n) {
+    const int next = take_roi(P, n);
+    if (next >= 0) {
         P.slot_roi[slot] = next;
         P.slot_phase[slot] = 0;
         double* tr = P.lm[slot].trial;
@@ -1830,8 +1864,8 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_fused25(SplitDev P, const 
             if (st_out) st_out[roi] = st.status;
             if (it_out) it_out[roi] = st.evals;
             if (crlb5) lm_crlb(st.F, crlb5 + 5 * roi);
-            const int nx = atomicAdd(P.queue, 1);
-            if (nx < n) {
+            const int nx = take_roi(P, n);
+            if (nx >= 0) {
                 P.slot_roi[slot] = nx;
                 P.slot_phase[slot] = 0;
                 for (int q = 0; q < 5; ++q) st.trial[q] = init[5 * nx + q];
@@ -1847,9 +1881,10 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_fused25(SplitDev P, const 
 }
 
 // Fill the pool from the queue.
-__global__ void k_init_slots(SplitDev P, const double* init, int n, FitParamsDev prm) {
+__global__ void k_init_slots(SplitDev P, const double* init, int n, int navail, FitParamsDev prm) {
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= P.P) return;
+    n = n < navail ? n : navail;
     if (slot < n) {
         P.slot_roi[slot] = slot;
         P.slot_phase[slot] = 0;
@@ -1862,8 +1897,26 @@ __global__ void k_init_slots(SplitDev P, const double* init, int n, FitParamsDev
         *P.queue = P.P < n ? P.P : n;
         *P.active = P.P < n ? P.P : n;
         *P.err = 0;
+        *P.navail = navail;
     }
 }
+
+// Idle slots (their last ROI retired while the queue had reached the ROIs on
+// the device) take ROIs that have arrived since.
+__global__ void k_refill(SplitDev P, const double* init, int n, FitParamsDev prm) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= P.P || P.slot_roi[slot] >= 0) return;
+    const int r = take_roi(P, n);
+    if (r < 0) return;
+    P.slot_roi[slot] = r;
+    P.slot_phase[slot] = 0;
+    double* tr = P.lm[slot].trial;
+    for (int q = 0; q < 5; ++q) tr[q] = init[5 * r + q];
+    lm_clamp(tr, prm);
+    atomicAdd(P.active, 1);
+}
+
+__global__ void k_set_int(int* p, int v) { *p = v; }
 
 // ---------------------------------------------------------------- host -----
 static size_t smem_stage1p(const SplitPlanHost& pl) {
@@ -2040,6 +2093,7 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
     D.queue = D.slot_phase + P;
     D.active = D.queue + 1;
     D.err = D.queue + 2;
+    D.navail = D.queue + 3;
     D.sc = pl->sc;
     ZOLA_CUDA_CHECK(cudaMemsetAsync(D.a4, 0, b_a4, st), ctx);
     ZOLA_CUDA_CHECK(stage1_attr(pl->W, sp.s1), ctx);
@@ -2078,13 +2132,14 @@ static void launch_model_stages(zola_ctx* ctx, const SplitPool& sp, cudaStream_t
     ctx->launches += 1;
 }
 
-static int read_flags(zola_ctx* ctx, const SplitDev& D, cudaStream_t st, int* active, int* err) {
+static int read_flags(zola_ctx* ctx, const SplitDev& D, cudaStream_t st, int* active, int* err, int* queue = nullptr) {
     if (!ctx->h_flags) ZOLA_CUDA_CHECK(cudaMallocHost(&ctx->h_flags, 4 * sizeof(int)), ctx);
-    ZOLA_CUDA_CHECK(cudaMemcpyAsync(ctx->h_flags, D.active, 2 * sizeof(int), cudaMemcpyDeviceToHost, st), ctx);
+    ZOLA_CUDA_CHECK(cudaMemcpyAsync(ctx->h_flags, D.queue, 3 * sizeof(int), cudaMemcpyDeviceToHost, st), ctx);
     ZOLA_CUDA_CHECK(cudaStreamSynchronize(st), ctx);
     prof_collect(ctx);
-    *active = ctx->h_flags[0];
-    *err = ctx->h_flags[1];
+    if (queue) *queue = ctx->h_flags[0];
+    *active = ctx->h_flags[1];
+    *err = ctx->h_flags[2];
     return ZOLA_OK;
 }
 
@@ -2113,17 +2168,41 @@ int launch_model_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const double
 int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_rois, const float* d_scmos,
                      const double* d_init, int n,
                      const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll, int* d_status,
-                     int* d_iters, cudaStream_t st) {
+                     int* d_iters, cudaStream_t st, const RoiFeed* feed) {
     SplitPool sp;
     int rc = setup_pool(ctx, p, w, n, ctx->split_pool_max, sp, st);
     if (rc) return rc;
     const SplitDev& D = sp.D;
     const int P = D.P;
     FitParamsDev fp{prm->zmin, prm->zmax, prm->xymax, prm->tol_xyz, prm->step_xy, prm->step_z, prm->max_iter};
-    k_init_slots<<<(P + 127) / 128, 128, 0, st>>>(D, d_init, n, fp);
+    // inputs still arriving: the fit starts on the first chunk, and chunks are
+    // handed to the pool as their copies complete
+    int chunk = 0, navail = n, queue = 0;
+    if (feed && feed->n_chunks > 0) {
+        ZOLA_CUDA_CHECK(cudaStreamWaitEvent(st, feed->ev[0], 0), ctx);
+        navail = feed->chunk_end[0];
+    }
+    auto poll_feed = [&](bool block) -> int {
+        const int before = navail;
+        while (feed && chunk + 1 < feed->n_chunks) {
+            if (block) {
+                ZOLA_CUDA_CHECK(cudaEventSynchronize(feed->ev[chunk + 1]), ctx);
+                block = false;
+            } else if (cudaEventQuery(feed->ev[chunk + 1]) != cudaSuccess) {
+                break;
+            }
+            navail = feed->chunk_end[++chunk];
+        }
+        if (navail != before) {
+            k_set_int<<<1, 1, 0, st>>>(D.navail, navail);
+            ctx->launches++;
+        }
+        return ZOLA_OK;
+    };
+    k_init_slots<<<(P + 127) / 128, 128, 0, st>>>(D, d_init, n, navail, fp);
     ctx->launches++;
     ZOLA_CUDA_CHECK(cudaGetLastError(), ctx);
-    const int max_rounds = (prm->max_iter + 2) * ((n + P - 1) / P + 1) + 8;
+    const int max_rounds = (prm->max_iter + 2) * ((n + P - 1) / P + 1) + 8 + 4 * (feed ? feed->n_chunks : 0);
     int rounds = 0;
     const bool fused = ctx->split_fused && fused_fits(*sp.pl);
     // Large ROIs in large pools: column blur and likelihood sums in one
@@ -2133,6 +2212,10 @@ int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d
     const bool fused45 = sp.pl->R >= S45_MIN_R && P >= S45_MIN_POOL;
     while (true) {
         for (int k = 0; k < 4; ++k) {
+            if (feed && queue < n) {  // idle slots take ROIs that arrived since
+                k_refill<<<(P + 127) / 128, 128, 0, st>>>(D, d_init, n, fp);
+                ctx->launches++;
+            }
             if (fused) {
                 prof_begin(ctx, 0, st);
                 launch_stage1(ctx, sp, P / sp.pl->G1, st);
@@ -2167,10 +2250,15 @@ int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d
         rounds += 4;
         ZOLA_CUDA_CHECK(cudaGetLastError(), ctx);
         int active, err;
-        rc = read_flags(ctx, D, st, &active, &err);
+        rc = read_flags(ctx, D, st, &active, &err, &queue);
         if (rc) return rc;
         if (err) { ctx->err = "split fit: a bounded device wait timed out"; return ZOLA_E_TIMEOUT; }
-        if (active <= 0) break;
+        if ((rc = poll_feed(false))) return rc;
+        if (active <= 0) {
+            if (queue >= n) break;
+            // every slot idle and the queue at the arrived ROIs: wait for the next chunk
+            if (navail <= queue && (rc = poll_feed(true))) return rc;
+        }
         if (rounds > max_rounds) { ctx->err = "split fit: did not drain the ROI queue"; return ZOLA_E_TIMEOUT; }
     }
     return ZOLA_OK;

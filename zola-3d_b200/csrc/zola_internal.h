@@ -61,6 +61,8 @@ struct WindowTables {
 struct zola_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;    // host-to-device input copies that overlap the fit
+    std::vector<cudaEvent_t> feed_ev;      // completion of each input chunk of a host-buffer fit
     std::string err;
     long long launches = 0;
     int num_sms = 0;
@@ -142,9 +144,17 @@ int launch_fit_f64(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_r
 int launch_model_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const double* d_xyz, int n, double* d_out,
                        double* d_dout, cudaStream_t st);
 void free_split_plan(void* plan);
+// ROIs that reach the device while a split fit runs (host-buffer calls): chunk
+// c holds ROIs [chunk_end[c - 1], chunk_end[c]) and is on the device once ev[c]
+// has completed.  The slot pool refills only from ROIs that have arrived.
+struct RoiFeed {
+    int n_chunks = 0;
+    const int* chunk_end = nullptr;
+    const cudaEvent_t* ev = nullptr;
+};
 int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_rois, const float* d_scmos,
                      const double* d_init, int n, const zola_fit_params* prm, double* d_out5, double* d_crlb5,
-                     double* d_nll, int* d_status, int* d_iters, cudaStream_t st);
+                     double* d_nll, int* d_status, int* d_iters, cudaStream_t st, const RoiFeed* feed = nullptr);
 
 int ensure_scratch(zola_ctx* ctx, size_t bytes, std::string& err);
 int ensure_io(zola_ctx* ctx, size_t bytes);
