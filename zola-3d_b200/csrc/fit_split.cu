@@ -529,7 +529,7 @@ __global__ void __launch_bounds__(S1_THREADS, 1) k_stage1p(SplitDev P, int ntile
     if (t < 32) umma::tmem_alloc(&tmem_base, NCOLS);
     if (t == 0) {
         umma::mbar_init(&cfull, 1);
-        for (int b = 0; b < NBQ; ++b) { umma::mbar_init(&qfull[b], SPLIT_THREADS); umma::mbar_init(&qfree[b], 1); }
+        for (int b = 0; b < NBQ; ++b) { umma::mbar_init(&qfull[b], SPLIT_THREADS / 32); umma::mbar_init(&qfree[b], 1); }
         umma::mbar_init(&accA, 1);
         umma::mbar_init(&accB, 1);
         umma::mbar_init(&tfree, SPLIT_THREADS / 32);
@@ -620,11 +620,13 @@ __global__ void __launch_bounds__(S1_THREADS, 1) k_stage1p(SplitDev P, int ntile
         // the next step are issued before this step's arithmetic
         struct QTab { double2 p0, kz, ky; float2 pu; };
         auto qtab = [&](int s) {
+            const size_t i2 = (((size_t)s * 4 + bp) * DP + ba) * 2;
+            const size_t i4 = (((size_t)s * 2 + (bp >> 1)) * DP + ba) * 4 + (bp & 1) * 2;
             QTab q2;
-            q2.p0 = *(const double2*)(P.phase0 + (((size_t)s * 4 + bp) * DP + ba) * 2);
-            q2.kz = *(const double2*)(P.kz + (((size_t)s * 4 + bp) * DP + ba) * 2);
+            q2.p0 = *(const double2*)(P.phase0 + i2);
+            q2.kz = *(const double2*)(P.kz + i2);
+            q2.pu = *(const float2*)(P.pupf + i4);
             q2.ky = *(const double2*)(P.ky + 8 * s + 2 * bp);
-            q2.pu = *(const float2*)(P.pupf + (((size_t)s * 2 + (bp >> 1)) * DP + ba) * 4 + (bp & 1) * 2);
             return q2;
         };
         const uint32_t ore = kmajor_off(brow, 2 * bp, 16), oim = kmajor_off(brow, 8 + 2 * bp, 16);
@@ -634,9 +636,9 @@ __global__ void __launch_bounds__(S1_THREADS, 1) k_stage1p(SplitDev P, int ntile
             ++q;
             return QR + buf * QRING;
         };
-        auto slot_done = [&](char* qs) {
+        auto slot_done = [&](char* qs) {  // every writer fences its stores; one arrive per warp
             umma::fence_proxy_async();
-            umma::mbar_arrive(&qfull[(qs - QR) / QRING]);
+            warp_arrive(&qfull[(qs - QR) / QRING]);
         };
         uint32_t zkeep[TWO ? 8 : 1][2] = {};  // pass A's Q_z of each K step (W = 128)
         auto build = [&](int s, const QTab& tb, uint32_t& zr, uint32_t& zi) {
