@@ -258,26 +258,36 @@ class PSF:
         return FitParams(float(zmin), float(zmax), float(xymax), int(max_iter), float(tol_xyz), float(step_xy),
                          float(step_z), int(precision))
 
-    def fit(self, rois, init, prm, crlb=True, scmos=None):
+    def fit(self, rois, init, prm, crlb=True, scmos=None, out=None):
         """Batched MLE fit of host ROIs (n, R, R) photons from init (n, 5) = x, y, z, A, B.
-        scmos (n, R, R), optional: var/gain^2 of each ROI pixel, added to the model mean."""
+        scmos (n, R, R), optional: var/gain^2 of each ROI pixel, added to the model mean.
+        out, optional: the result arrays to fill in place, a dict with theta (n, 5) and crlb
+        (n, 5) float64 (crlb may be None), nll (n,) float64, status and iters (n,) int32, all
+        C-contiguous; views of pinned host memory make the device-to-host copy direct."""
         rois = np.ascontiguousarray(rois, dtype=np.float32)
         init = np.ascontiguousarray(init, dtype=np.float64)
         n, R = rois.shape[0], rois.shape[1]
-        out = np.zeros((n, 5))
-        cr = np.zeros((n, 5)) if crlb else None
-        nll = np.zeros(n)
-        st = np.zeros(n, np.int32)
-        it = np.zeros(n, np.int32)
+        if out is None:
+            res = dict(theta=np.zeros((n, 5)), crlb=np.zeros((n, 5)) if crlb else None, nll=np.zeros(n),
+                       status=np.zeros(n, np.int32), iters=np.zeros(n, np.int32))
+        else:
+            res = out
+            for k, shape, dt in (("theta", (n, 5), np.float64), ("crlb", (n, 5), np.float64),
+                                 ("nll", (n,), np.float64), ("status", (n,), np.int32), ("iters", (n,), np.int32)):
+                a = res.get(k)
+                if a is None and k == "crlb":
+                    continue
+                if a is None or a.shape != shape or a.dtype != dt or not a.flags["C_CONTIGUOUS"]:
+                    raise ValueError(f"out[{k!r}] must be a C-contiguous {np.dtype(dt).name} array of shape {shape}")
+        args = (_ptr(res["theta"]), _ptr(res["crlb"]), _ptr(res["nll"]), _ptr(res["status"]), _ptr(res["iters"]))
         if scmos is None:
             self.ctx.check(lib().zola_fit_batch(self.ctx.h, self.h, R, _ptr(rois), _ptr(init), n, ctypes.byref(prm),
-                                                _ptr(out), _ptr(cr), _ptr(nll), _ptr(st), _ptr(it)), "zola_fit_batch")
+                                                *args), "zola_fit_batch")
         else:
             v = np.ascontiguousarray(scmos, dtype=np.float32)
             self.ctx.check(lib().zola_fit_batch_scmos(self.ctx.h, self.h, R, _ptr(rois), _ptr(v), _ptr(init), n,
-                                                      ctypes.byref(prm), _ptr(out), _ptr(cr), _ptr(nll), _ptr(st),
-                                                      _ptr(it)), "zola_fit_batch_scmos")
-        return dict(theta=out, crlb=cr, nll=nll, status=st, iters=it)
+                                                      ctypes.byref(prm), *args), "zola_fit_batch_scmos")
+        return res
 
     def fit_dev(self, rois, init, prm, out, crlb=None, nll=None, status=None, iters=None, stream=None):
         """Device form over torch CUDA tensors (rois float32, init/out float64)."""
