@@ -1124,6 +1124,21 @@ __device__ __forceinline__ double warp_sum(double x) {
     return x;
 }
 
+// Butterfly reduce-scatter of 32 per-lane values: after 31 shuffles lane k
+// holds the warp total of value k (the plain form needs 5 shuffles per value).
+__device__ __forceinline__ double warp_reduce_scatter32(double (&v)[32], int lane) {
+#pragma unroll
+    for (int h = 16; h >= 1; h >>= 1) {
+        const bool up = (lane & h) != 0;
+#pragma unroll
+        for (int i = 0; i < h; ++i) {
+            const double send = up ? v[i] : v[i + h], keep = up ? v[i + h] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, h);
+        }
+    }
+    return v[0];
+}
+
 constexpr int NSUM = NRED + 1;  // sums per slot: NRED + the non-positive-model flag
 constexpr int S5_THREADS = 128;
 constexpr int S5_SLOTS = S5_THREADS / 32;  // one warp per slot
@@ -1218,15 +1233,21 @@ __global__ void __launch_bounds__(S5_THREADS) k_stage5(SplitDev P, const float* 
                 }
         }
     }
-    double tot[NRED];
+    // sums 0..31: butterfly reduce-scatter (lane k ends with sum k); 32..35 plainly
+    double v[32];
 #pragma unroll
-    for (int k = 0; k < 6; ++k) tot[k] = warp_sum((double)sg6[k] - (double)cg6[k]);
+    for (int k = 0; k < 6; ++k) v[k] = (double)sg6[k] - (double)cg6[k];
 #pragma unroll
-    for (int k = 0; k < 30; ++k) tot[6 + k] = warp_sum((double)sh[k]);
+    for (int k = 0; k < 26; ++k) v[6 + k] = sh[k];
+    const double mine = warp_reduce_scatter32(v, lane);
+    double rest[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) rest[k] = warp_sum((double)sh[26 + k]);
     const bool anybad = __any_sync(0xffffffffu, bad);
-    if (lane != 0) return;
     double* out = P.sums + (size_t)slot * NSUM;
-    for (int q = 0; q < NRED; ++q) out[q] = tot[q];
+    out[lane] = mine;
+    if (lane != 0) return;
+    for (int k = 0; k < 4; ++k) out[32 + k] = rest[k];
     out[NRED] = anybad ? 1.0 : 0.0;
 }
 
@@ -1460,16 +1481,7 @@ __global__ void __launch_bounds__(S45_THREADS, 1) k_stage45p(SplitDev P, const f
             for (int k = 0; k < 6; ++k) v[k] = sg6[k];
 #pragma unroll
             for (int k = 0; k < 26; ++k) v[6 + k] = sh[k];
-#pragma unroll
-            for (int h = 16; h >= 1; h >>= 1) {
-                const bool up = (lane & h) != 0;
-#pragma unroll
-                for (int i = 0; i < h; ++i) {
-                    const double send = up ? v[i] : v[i + h], keep = up ? v[i + h] : v[i];
-                    v[i] = keep + __shfl_xor_sync(0xffffffffu, send, h);
-                }
-            }
-            red[warp][lane] = v[0];
+            red[warp][lane] = warp_reduce_scatter32(v, lane);
 #pragma unroll
             for (int k = 26; k < 30; ++k) {
                 const double x = warp_sum((double)sh[k]);
