@@ -470,6 +470,20 @@ __device__ __forceinline__ int take_roi(const SplitDev& P, int n) {
 }
 
 // ----------------------------------------------- persistent-kernel helpers ----
+// True in every thread when any of the tiles blockIdx.x, + gridDim.x, ... (of g
+// slots each) holds a ROI.  A CTA without one leaves before it allocates TMEM
+// or loads constants (a draining pool's last rounds).
+__device__ __forceinline__ bool cta_has_live_tile(const SplitDev& P, int ntiles, int g) {
+    __shared__ int s_any;
+    if (threadIdx.x == 0) {
+        int any = 0;
+        for (int tile = blockIdx.x; tile < ntiles && !any; tile += gridDim.x) any = tile_live(P, tile * g, g);
+        s_any = any;
+    }
+    __syncthreads();
+    return s_any != 0;
+}
+
 // Named barrier 1 over the first N threads of the CTA (the epilogue warps).
 template <int N = SPLIT_THREADS>
 __device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, %0;" ::"n"(N) : "memory"); }
@@ -526,6 +540,7 @@ __global__ void __launch_bounds__(S1_THREADS, 1) k_stage1p(SplitDev P, int ntile
     char* QR = smem + NS * SLAB;   // ring of Q K-slabs
     __shared__ __align__(8) uint64_t cfull, qfull[NBQ], qfree[NBQ], accA, accB, tfree, fin;
     __shared__ uint32_t tmem_base;
+    if (!cta_has_live_tile(P, ntiles, G1)) return;
     if (t < 32) umma::tmem_alloc(&tmem_base, NCOLS);
     if (t == 0) {
         umma::mbar_init(&cfull, 1);
@@ -800,6 +815,7 @@ __global__ void __launch_bounds__(S2_THREADS, 1) k_stage2p(SplitDev P, int ntile
     char* RB = smem + NS * SLAB;     // ring of A2 K-slabs
     __shared__ __align__(8) uint64_t cfull, full[NBUF], freed[NBUF], accA, accB;
     __shared__ uint32_t tmem_base;
+    if (!cta_has_live_tile(P, ntiles, G2)) return;
     if (t < 32) umma::tmem_alloc(&tmem_base, NCOLS);
     if (t == 0) {
         umma::mbar_init(&cfull, 1);
@@ -1289,6 +1305,7 @@ __global__ void __launch_bounds__(S45_THREADS, 1) k_stage45p(SplitDev P, const f
     __shared__ double red[E45_THREADS / 32][NRED];
     __shared__ int bad_w[E45_THREADS / 32];
     const int ncols = tmem_cols_pow2(2 * NT);
+    if (!cta_has_live_tile(P, P.P, 1)) return;
     if (t < 32) umma::tmem_alloc(&tmem_base, ncols);
     if (t == 0) {
         umma::mbar_init(&gfull, 1);
