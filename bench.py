@@ -311,7 +311,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--classes", default="", help="comma list of ROI classes to run (profiling); default all")
-    ap.add_argument("--pool", type=int, default=4096, help="max ROIs in flight per fit call (0: library default)")
+    ap.add_argument("--pool", type=int, default=16384, help="max ROIs in flight per fit call (0: library default)")
     ap.add_argument("--detect-frames", type=int, default=200,
                     help="frames of the detect -> fit pipeline measurement (0: skip)")
     ap.add_argument("--split-mode", default="staged", choices=["staged", "fused"],

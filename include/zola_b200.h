@@ -306,8 +306,9 @@ ZOLA_API int zola_fit_batch_noalloc(zola_psf* psf, int R, const float* d_rois, c
                                     const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll,
                                     int* d_status, int* d_iters, void* stream);
 
-/* Upper bound on the split fit's slot pool (ROIs in flight); 0 = automatic.
- * Smaller pools keep the stage intermediates resident in L2. */
+/* Upper bound on the split fit's slot pool (ROIs in flight); 0 = automatic
+ * (pool state up to 8 GB, at most 32768 slots).  Larger pools amortise each
+ * launch's fixed work and shorten the draining tail of a batch. */
 ZOLA_API int zola_ctx_set_pool(zola_ctx* ctx, int max_slots);
 /* Split fit kernel layout: ZOLA_SPLIT_STAGED (default) runs the five stages
  * as separate kernels through global memory; ZOLA_SPLIT_FUSED runs stage 1

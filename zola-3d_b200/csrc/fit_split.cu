@@ -2090,7 +2090,7 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
     }
     const size_t per_slot = a2_tile_bytes(pl->K1) / pl->G2 + a3_tile_bytes(pl->W) / pl->G2 +
                             (size_t)pl->NT4 * a4_tile_bytes(pl->W) + (size_t)4 * pl->R * pl->R * 4 + sizeof(LMState) + NSUM * 8 + 16;
-    int Pmax = (int)std::min<size_t>(32768, ((size_t)3 << 30) / per_slot);
+    int Pmax = (int)std::min<size_t>(32768, ((size_t)8 << 30) / per_slot);  // at most 8 GB of pool state
     if (pmax_override > 0) Pmax = std::min(Pmax, pmax_override);
     Pmax = std::max(4, Pmax / 4 * 4);
     const int P = std::min(Pmax, (n + 3) / 4 * 4);
