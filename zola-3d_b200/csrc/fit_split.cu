@@ -194,10 +194,11 @@ static SplitPlanHost* get_plan(zola_psf* p, WindowTables* w, std::string& err) {
         sc.cT[m] = (float)(1.0 / (sJ * sG));
     }
 
-    // BC chunks.  Rows n' = part * IC + ii of chunk c (output index c*IC + ii):
+    // DFT constant rows, four parts per output index i:
     // part 0: [Re C ; -Im C], 1: [Im C ; Re C], 2: [Re CK ; -Im CK], 3: [Im CK ; Re CK]
-    // with columns k < DP multiplying the real and k >= DP the imaginary part
-    // of the data; CK[i][b] = C[i][b] * (i k_b).
+    // with data columns k < DP (natural order) multiplying the real and k >= DP
+    // the imaginary part of the data; CK[i][b] = C[i][b] * (i k_b).  The packs
+    // below place column k at its kperm position.
     auto C = [&](int i, int b, double& re, double& im) {
         re = w->C[((size_t)i * D + b) * 2];
         im = w->C[((size_t)i * D + b) * 2 + 1];
