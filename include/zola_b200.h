@@ -157,11 +157,18 @@ ZOLA_API int zola_detector_free(zola_detector* det);
  * (nslices x R x R, sum 1), as Predetection.getRange / getPSFNonNormalized. */
 ZOLA_API int zola_detector_info(const zola_detector* det, int* nslices, double* range, double* psfs);
 /* frames: nframes x SX x SY photons (double, first index x).  out: nframes x
- * cap rows of 7 doubles (score, slice r, i, j, dz, dx, dy), sorted by
- * descending score with ties in the reference's order; counts[f] = number of
- * candidates of frame f (if it exceeds cap the list is truncated: retry with
- * a larger cap). */
+ * cap rows of 7 doubles (score, slice r, i, j, dz, dx, dy): the first
+ * min(counts[f], cap) entries of frame f's whole candidate list, sorted by
+ * descending score with ties in the reference's insertion order (slice r,
+ * then j, then i; Predetection.getVectMaxPosition).  counts[f] = length of the
+ * whole list (at 0.1, the reference's threshold, a 256 x 256 frame against a
+ * 41-slice library gives several thousand). */
+#define ZOLA_DETECT_MAX_CAP (1 << 20)
 ZOLA_API int zola_detect(zola_detector* det, const double* frames, int nframes, int cap, double* out, int* counts);
+/* Device form, asynchronous on stream: cap is also the number of candidates
+ * stored per frame, so a frame with counts[f] > cap gets the sorted first cap
+ * of its list in insertion order -- the same rows on every run, but not the
+ * first cap of the sorted whole.  Call again with cap >= counts[f] for those. */
 ZOLA_API int zola_detect_dev(zola_detector* det, const double* d_frames, int nframes, int cap, double* d_out,
                              int* d_counts, void* stream);
 
@@ -184,7 +191,8 @@ typedef struct {
     int max_iter;             /* LM evaluations per ROI */
     double tol_xyz;           /* LM stopping distance, um */
     int precision;            /* ZOLA_PREC_FP64 or ZOLA_PREC_SPLIT for the fits */
-    int cand_cap;             /* max candidates per frame (0: 1024) */
+    int cand_cap;             /* candidates stored per frame at the start (0: 4096); it grows to the
+                                 longest list so that every frame walks its whole list */
     int frames_per_batch;     /* frames per device batch (0: 1024) */
     int wave_fits;            /* candidates fitted ahead per frame and wave (0: 16); any value gives the
                                  same rows as the reference's one-at-a-time walk */

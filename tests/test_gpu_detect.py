@@ -59,3 +59,33 @@ def test_detection_empty_and_flat_frames(zpkg, ctx):
     got, counts = det.detect(frames, cap=64)
     assert list(counts) == [0, 0]
     det.close()
+
+
+def test_detection_whole_lists_at_the_reference_threshold(zpkg, ctx):
+    """256 x 256 frames against a 41-slice tetrapod library at the reference's
+    threshold (0.1) give thousands of candidates per frame.  The lists are the
+    oracle's whole sorted lists, the same on every run; a small cap returns
+    their first rows, and a cap past the shared-memory sort takes the
+    global-memory sort to the same rows."""
+    zern = tetrapod_zernike()
+    S, R, N = 256, 40, 128
+    psf = zpkg.PSF(ctx, zpkg.optics(size_fft=N, kz_reset=True, **OPTICS), zern)
+    ref = O.OraclePSF(N, 0.11, 1.4, 0.66, 1.518, 1.518, 0.9, zern, gauss_f32=False, kz_reset=True)
+    frames = make_frames(ref.model, S, 2, seed=5, emitters=5, R=64, zr=2.0, bg=30.0)
+    det = zpkg.Detector(psf, S, S, R, -2.0, 2.0, 0.1, 0.1)
+    odet = O.OracleDetector(ref, S, S, R, -2.0, 2.0, 0.1, 0.1)
+    want = odet.detect(frames, cap=100000, threads=8)
+    got, counts = det.detect(frames, cap=16384)
+    again, _ = det.detect(frames, cap=16384)
+    small, counts_small = det.detect(frames, cap=500)
+    wide, _ = det.detect(frames, cap=20000)
+    for f in range(len(frames)):
+        g, w = got[f], want[f]
+        assert len(w) > 2000
+        assert counts[f] == len(w) and counts_small[f] == len(w)
+        assert np.array_equal(g, again[f])
+        assert np.array_equal(g[:, 1:4].astype(int), w[:, 1:4].astype(int)), f"frame {f}: candidate order differs"
+        assert np.allclose(g[:, 0], w[:, 0], rtol=1e-10, atol=0)
+        assert np.array_equal(small[f], g[:500])
+        assert np.array_equal(wide[f], g)
+    det.close()

@@ -473,7 +473,7 @@ LOC_COLUMNS = ["id", "frame", "x_nm", "y_nm", "z_nm", "intensity", "background",
 
 
 def localize_frames(ctx, det, fit_psf, frames, minZ, maxZ, photon_threshold=500.0, max_snr=1.0, max_iter=30,
-                    tol_xyz=1e-4, precision=ZOLA_PREC_FP64, frame0=0, cand_cap=1024, frames_per_batch=1024, wave_fits=0):
+                    tol_xyz=1e-4, precision=ZOLA_PREC_FP64, frame0=0, cand_cap=0, frames_per_batch=1024, wave_fits=0):
     """Detect and localize every frame (LocalizationPipeline): returns a
     structured numpy array with LOC_COLUMNS, one row per localization."""
     frames = np.ascontiguousarray(frames, dtype=np.float64)
@@ -493,7 +493,7 @@ def localize_frames(ctx, det, fit_psf, frames, minZ, maxZ, photon_threshold=500.
     return arr
 
 def localize_frames_scmos(ctx, det, fit_psf, adu, offset, gain, variance, minZ, maxZ, photon_threshold=500.0,
-                          max_snr=1.0, max_iter=30, tol_xyz=1e-4, precision=ZOLA_PREC_FP64, frame0=0, cand_cap=1024,
+                          max_snr=1.0, max_iter=30, tol_xyz=1e-4, precision=ZOLA_PREC_FP64, frame0=0, cand_cap=0,
                           frames_per_batch=1024, wave_fits=0):
     """sCMOS pipeline: ADU frames (n, SX, SY) and offset / gain / variance maps (SX, SY)."""
     adu = np.ascontiguousarray(adu, dtype=np.float32)

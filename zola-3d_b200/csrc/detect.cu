@@ -15,11 +15,15 @@
 //                (tmp keeps the previous slice's value elsewhere, as the
 //                reference reuses it), then peaks with score > thr equal to
 //                tmp and to the max of tmp over i +- 3, with parabolic x/y/z
-//                refinement (:480-560).  Rows: score, r, i, j, topZ, topX, topY.
+//                refinement (:480-560).  Rows: score, r, i, j, topZ, topX, topY,
+//                appended in the reference's insertion order (r, then j, then
+//                i) by an ordered block scan, so the stored list is the same
+//                on every run.
 //   k_det_sort   stable sort by descending score (Arrays.sort of the rows in
-//                insertion order r, j, i; :447-454).
+//                insertion order r, j, i; :447-454): ties keep list order.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -135,20 +139,51 @@ __device__ inline double parabola_top(double xa, double ya, double xb, double yb
     return -b / (2 * a);
 }
 
+// Exclusive prefix sum of one int per thread over the block, in thread order;
+// *total = the block's sum.  wtot: 32 ints of shared memory.
+__device__ int block_exclusive_scan(int v, int* wtot, int* total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wtot[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int y = lane < nw ? wtot[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, y, o);
+            if (lane >= o) y += u;
+        }
+        if (lane < nw) wtot[lane] = y;
+    }
+    __syncthreads();
+    const int base = w ? wtot[w - 1] : 0;
+    *total = wtot[nw - 1];
+    __syncthreads();  // wtot is reused by the next call
+    return base + x - v;
+}
+
 // One CTA per frame; slices in order because tmp carries over between them.
-__global__ void __launch_bounds__(1024) k_det_nms(DetView V, const double* score, double* tmp, double* cand,
-                                                  long long* keys, int* counts) {
+// flags: SX x SY bytes per frame of scratch (the peaks of the current slice).
+// The first V.cap rows of the frame's list (in insertion order) are stored;
+// counts[f] = the length of the whole list.
+__global__ void __launch_bounds__(1024) k_det_nms(DetView V, const double* score, double* tmp, unsigned char* flags,
+                                                  double* cand, int* counts) {
     const int f = blockIdx.x, SX = V.SX, SY = V.SY, Z = V.Z, dec = 3;
     const int lo = max(dec, V.R / 2);
     const double* sc = score + (size_t)f * Z * SX * SY;
     double* tm = tmp + (size_t)f * SX * SY;
+    unsigned char* fl = flags + (size_t)f * SX * SY;
     double* out = cand + (size_t)f * V.cap * 7;
-    long long* key = keys + (size_t)f * V.cap;
-    __shared__ int cnt;
-    if (threadIdx.x == 0) cnt = 0;
+    __shared__ int wtot[32];
     for (int k = threadIdx.x; k < SX * SY; k += blockDim.x) tm[k] = 0.0;
     __syncthreads();
     auto S = [&](int r, int i, int j) { return sc[((size_t)r * SX + i) * SY + j]; };
+    int total = 0;
     for (int r = 0; r < Z; ++r) {
         for (int k = threadIdx.x; k < SX * SY; k += blockDim.x) {
             const int i = k / SY, j = k % SY;
@@ -162,57 +197,86 @@ __global__ void __launch_bounds__(1024) k_det_nms(DetView V, const double* score
         __syncthreads();
         for (int k = threadIdx.x; k < SX * SY; k += blockDim.x) {
             const int i = k / SY, j = k % SY;
-            if (i < lo || i >= SX - lo || j < lo || j >= SY - lo) continue;
-            const double v = S(r, i, j);
-            if (!(v > V.thr) || v != tm[k]) continue;
-            double mx = -INFINITY;
-            for (int a = -dec; a <= dec; ++a) mx = fmax(tm[(size_t)(i + a) * SY + j], mx);
-            if (mx != v) continue;
-            double tz = 0, tx = 0, ty = 0;
-            if (r > 1 && r < Z - 1) tz = parabola_top(-V.zstep, S(r - 1, i, j), 0, v, V.zstep, S(r + 1, i, j));
-            if (i > 1 && i < SX - 1) tx = parabola_top(-V.dx, S(r, i - 1, j), 0, v, V.dx, S(r, i + 1, j));
-            if (j > 1 && j < SY - 1) ty = parabola_top(-V.dx, S(r, i, j - 1), 0, v, V.dx, S(r, i, j + 1));
-            const int slot = atomicAdd(&cnt, 1);
-            if (slot < V.cap) {
-                double* row = out + (size_t)slot * 7;
-                row[0] = v; row[1] = r; row[2] = i; row[3] = j; row[4] = tz; row[5] = tx; row[6] = ty;
-                key[slot] = ((long long)r * SY + j) * SX + i;  // the reference's insertion order
+            unsigned char peak = 0;
+            if (i >= lo && i < SX - lo && j >= lo && j < SY - lo) {
+                const double v = S(r, i, j);
+                if (v > V.thr && v == tm[k]) {
+                    double mx = -INFINITY;
+                    for (int a = -dec; a <= dec; ++a) mx = fmax(tm[(size_t)(i + a) * SY + j], mx);
+                    peak = mx == v;
+                }
             }
+            fl[k] = peak;
         }
         __syncthreads();
+        // append the slice's peaks column by column (thread = column j), rows i in order
+        for (int j0 = lo; j0 < SY - lo; j0 += blockDim.x) {
+            const int j = j0 + threadIdx.x;
+            const bool col = j < SY - lo;
+            int c = 0;
+            if (col)
+                for (int i = lo; i < SX - lo; ++i) c += fl[(size_t)i * SY + j];
+            int tot;
+            int o = total + block_exclusive_scan(c, wtot, &tot);
+            if (col && c)
+                for (int i = lo; i < SX - lo; ++i) {
+                    if (!fl[(size_t)i * SY + j]) continue;
+                    if (o < V.cap) {
+                        const double v = S(r, i, j);
+                        double tz = 0, tx = 0, ty = 0;
+                        if (r > 1 && r < Z - 1) tz = parabola_top(-V.zstep, S(r - 1, i, j), 0, v, V.zstep, S(r + 1, i, j));
+                        if (i > 1 && i < SX - 1) tx = parabola_top(-V.dx, S(r, i - 1, j), 0, v, V.dx, S(r, i + 1, j));
+                        if (j > 1 && j < SY - 1) ty = parabola_top(-V.dx, S(r, i, j - 1), 0, v, V.dx, S(r, i, j + 1));
+                        double* row = out + (size_t)o * 7;
+                        row[0] = v; row[1] = r; row[2] = i; row[3] = j; row[4] = tz; row[5] = tx; row[6] = ty;
+                    }
+                    ++o;
+                }
+            total += tot;
+        }
+        __syncthreads();  // tm and the flags change with the next slice
     }
-    if (threadIdx.x == 0) counts[f] = cnt;
+    if (threadIdx.x == 0) counts[f] = total;
 }
 
-// Sort one frame's candidates by (score descending, insertion order ascending).
-__global__ void __launch_bounds__(1024) k_det_sort(DetView V, double* cand, long long* keys, const int* counts,
-                                                   double* out) {
-    extern __shared__ char smraw[];
+// Sort keys of up to DET_SORT_SMEM candidates per frame live in shared memory;
+// longer lists sort in global scratch (same network).
+constexpr int DET_SORT_SMEM = 16384;
+
+__host__ __device__ inline int det_pow2(int n) {
+    int p = 1;
+    while (p < n) p <<= 1;
+    return p;
+}
+
+// Sort one frame's stored candidates by (score descending, list position
+// ascending) -- a stable sort of the insertion-ordered list -- and write the
+// first min(n, cap) rows.  gs / gid: global sort keys (det_pow2(cap) per
+// frame) or nullptr for the shared-memory form.
+__global__ void __launch_bounds__(1024) k_det_sort(DetView V, const double* cand, const int* counts, double* out,
+                                                   double* gs, int* gid) {
+    extern __shared__ double smraw[];
     const int f = blockIdx.x, n = min(counts[f], V.cap);
-    int P2 = 1;
-    while (P2 < n) P2 <<= 1;
-    double* s = (double*)smraw;
-    long long* k = (long long*)(s + P2);
-    int* id = (int*)(k + P2);
+    const int P2 = det_pow2(n);
+    double* s = gs ? gs + (size_t)f * det_pow2(V.cap) : smraw;
+    int* id = gs ? gid + (size_t)f * det_pow2(V.cap) : (int*)(smraw + P2);
     const double* c = cand + (size_t)f * V.cap * 7;
-    const long long* kk = keys + (size_t)f * V.cap;
     for (int t = threadIdx.x; t < P2; t += blockDim.x) {
-        if (t < n) { s[t] = c[(size_t)t * 7]; k[t] = kk[t]; id[t] = t; }
-        else { s[t] = -INFINITY; k[t] = 0x7fffffffffffffffll; id[t] = -1; }
+        if (t < n) { s[t] = c[(size_t)t * 7]; id[t] = t; }
+        else { s[t] = -INFINITY; id[t] = 0x7fffffff; }
     }
     __syncthreads();
-    // bitonic sort: "before" = higher score, then smaller key
+    // bitonic network: "before" = higher score, then earlier in the list
     for (int size = 2; size <= P2; size <<= 1)
         for (int stride = size >> 1; stride > 0; stride >>= 1) {
             for (int t = threadIdx.x; t < P2; t += blockDim.x) {
                 const int o = t ^ stride;
                 if (o > t) {
                     const bool up = (t & size) == 0;
-                    const bool t_before = s[t] > s[o] || (s[t] == s[o] && k[t] < k[o]);
+                    const bool t_before = s[t] > s[o] || (s[t] == s[o] && id[t] < id[o]);
                     if (up != t_before) {
-                        double ts = s[t]; s[t] = s[o]; s[o] = ts;
-                        long long tk = k[t]; k[t] = k[o]; k[o] = tk;
-                        int ti = id[t]; id[t] = id[o]; id[o] = ti;
+                        const double ts = s[t]; s[t] = s[o]; s[o] = ts;
+                        const int ti = id[t]; id[t] = id[o]; id[o] = ti;
                     }
                 }
             }
@@ -324,8 +388,8 @@ int zola_detect_dev(zola_detector* d, const double* d_frames, int nframes, int c
                     void* stream) {
     if (!d) return ZOLA_E_ARG;
     zola_ctx* ctx = d->psf->ctx;
-    if (nframes < 0 || cap < 1 || cap > 8192 || (nframes > 0 && (!d_frames || !d_out || !d_counts))) {
-        ctx->err = "zola_detect: bad nframes / cap (1..8192) or null buffer";
+    if (nframes < 0 || cap < 1 || cap > ZOLA_DETECT_MAX_CAP || (nframes > 0 && (!d_frames || !d_out || !d_counts))) {
+        ctx->err = "zola_detect: bad nframes / cap (1..2^20) or null buffer";
         return ZOLA_E_ARG;
     }
     if (nframes == 0) return ZOLA_OK;
@@ -333,9 +397,12 @@ int zola_detect_dev(zola_detector* d, const double* d_frames, int nframes, int c
     DetView v = d->v;
     v.cap = cap;
     const size_t SS = (size_t)v.SX * v.SY;
-    // scratch: rowsum, rowsq, var, tmp (4 x SS per frame), scores (Z x SS), candidates, keys
-    const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)nframes, ((size_t)1 << 31) / ((4 + v.Z) * SS * 8 + (size_t)cap * 64)));
-    const size_t per = (4 + v.Z) * SS * 8 + (size_t)cap * 7 * 8 + (size_t)cap * 8;
+    const int p2 = det_pow2(cap);
+    const bool gsort = p2 > DET_SORT_SMEM;
+    // scratch per frame: rowsum (later the peak flags), rowsq, var, tmp, scores (Z x SS),
+    // candidates, and the sort keys when they do not fit in shared memory
+    const size_t per = (4 + (size_t)v.Z) * SS * 8 + (size_t)cap * 7 * 8 + (gsort ? (size_t)p2 * 12 : 0);
+    const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)nframes, ((size_t)1 << 31) / per));
     if (ensure_scratch(ctx, per * chunk + 1024, ctx->err)) return ZOLA_E_CUDA;
     for (int f0 = 0; f0 < nframes; f0 += chunk) {
         const int nf = std::min(chunk, nframes - f0);
@@ -346,7 +413,8 @@ int zola_detect_dev(zola_detector* d, const double* d_frames, int nframes, int c
         double* tmp = (double*)b; b += nf * SS * 8;
         double* score = (double*)b; b += nf * v.Z * SS * 8;
         double* cand = (double*)b; b += (size_t)nf * cap * 7 * 8;
-        long long* keys = (long long*)b;
+        double* gs = gsort ? (double*)b : nullptr;
+        int* gid = gsort ? (int*)(gs + (size_t)nf * p2) : nullptr;
         const double* fr = d_frames + (size_t)f0 * SS;
         prof_begin(ctx, 7, st);
         k_det_var<<<nf, 256, 0, st>>>(v, fr, rowsum, rowsq, var);
@@ -357,12 +425,11 @@ int zola_detect_dev(zola_detector* d, const double* d_frames, int nframes, int c
         cudaFuncSetAttribute(k_det_corr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         dim3 grid(tiles, (v.Z + zc - 1) / zc, nf);
         k_det_corr<<<grid, 256, smem, st>>>(v, zc, fr, var, score);
-        k_det_nms<<<nf, 1024, 0, st>>>(v, score, tmp, cand, keys, d_counts + f0);
-        int p2 = 1;
-        while (p2 < cap) p2 <<= 1;
-        const size_t ssort = (size_t)p2 * (8 + 8 + 4);
+        // the row sums are dead after k_det_var: their space holds the peak flags
+        k_det_nms<<<nf, 1024, 0, st>>>(v, score, tmp, (unsigned char*)rowsum, cand, d_counts + f0);
+        const size_t ssort = gsort ? 0 : (size_t)p2 * 12;
         cudaFuncSetAttribute(k_det_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssort);
-        k_det_sort<<<nf, 1024, ssort, st>>>(v, cand, keys, d_counts + f0, d_out + (size_t)f0 * cap * 7);
+        k_det_sort<<<nf, 1024, ssort, st>>>(v, cand, d_counts + f0, d_out + (size_t)f0 * cap * 7, gs, gid);
         prof_end(ctx, st);
         ctx->launches += 4;
         cudaError_t e = cudaGetLastError();
@@ -374,8 +441,8 @@ int zola_detect_dev(zola_detector* d, const double* d_frames, int nframes, int c
 int zola_detect(zola_detector* d, const double* frames, int nframes, int cap, double* out, int* counts) {
     if (!d) return ZOLA_E_ARG;
     zola_ctx* ctx = d->psf->ctx;
-    if (nframes < 0 || cap < 1 || cap > 8192 || (nframes > 0 && (!frames || !out || !counts))) {
-        ctx->err = "zola_detect: bad nframes / cap (1..8192) or null buffer";
+    if (nframes < 0 || cap < 1 || cap > ZOLA_DETECT_MAX_CAP || (nframes > 0 && (!frames || !out || !counts))) {
+        ctx->err = "zola_detect: bad nframes / cap (1..2^20) or null buffer";
         return ZOLA_E_ARG;
     }
     if (nframes == 0) return ZOLA_OK;
@@ -383,15 +450,34 @@ int zola_detect(zola_detector* d, const double* frames, int nframes, int cap, do
     double* df = nullptr;
     double* dout = nullptr;
     int* dc = nullptr;
+    int room = cap;  // candidates stored per frame on the device
     cudaError_t e = cudaMalloc(&df, SS * nframes * 8);
-    if (e == cudaSuccess) e = cudaMalloc(&dout, (size_t)nframes * cap * 7 * 8);
     if (e == cudaSuccess) e = cudaMalloc(&dc, (size_t)nframes * 4);
     if (e == cudaSuccess) e = cudaMemcpyAsync(df, frames, SS * nframes * 8, cudaMemcpyHostToDevice, ctx->stream);
     int rc = ZOLA_OK;
-    if (e == cudaSuccess) rc = zola_detect_dev(d, df, nframes, cap, dout, dc, ctx->stream);
-    if (e == cudaSuccess && rc == ZOLA_OK) {
+    // A frame whose list is longer than the room is detected again with room for
+    // all of it, so that its rows are the first cap of the whole sorted list.
+    for (int pass = 0; pass < 2 && e == cudaSuccess && rc == ZOLA_OK; ++pass) {
+        if (dout) cudaFree(dout);
+        dout = nullptr;
+        e = cudaMalloc(&dout, (size_t)nframes * room * 7 * 8);
+        if (e == cudaSuccess) rc = zola_detect_dev(d, df, nframes, room, dout, dc, ctx->stream);
+        if (e != cudaSuccess || rc != ZOLA_OK) break;
         e = cudaMemcpyAsync(counts, dc, (size_t)nframes * 4, cudaMemcpyDeviceToHost, ctx->stream);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, (size_t)nframes * cap * 7 * 8, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) break;
+        const int longest = *std::max_element(counts, counts + nframes);
+        if (longest <= room || pass == 1) break;
+        if (longest > ZOLA_DETECT_MAX_CAP) {
+            ctx->err = "zola_detect: a frame has more than 2^20 candidates";
+            rc = ZOLA_E_ARG;
+            break;
+        }
+        room = longest;
+    }
+    if (e == cudaSuccess && rc == ZOLA_OK) {
+        e = cudaMemcpy2DAsync(out, (size_t)cap * 7 * 8, dout, (size_t)room * 7 * 8, (size_t)cap * 7 * 8, nframes,
+                              cudaMemcpyDeviceToHost, ctx->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     }
     if (df) cudaFree(df);

@@ -379,7 +379,10 @@ int localize_impl(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const do
     if (fit_psf->o.kz_reset) { ctx->err = "zola_localize_frames: the fit PSF needs kz_reset = 0"; return ZOLA_E_ARG; }
     const std::vector<double>& range = det->range;
     const std::vector<double>& lib = det->h_psf;
-    const int cap = prm->cand_cap > 0 ? prm->cand_cap : 1024;
+    // candidates stored per frame: grows to the longest list met, so that every
+    // frame walks its whole list as the reference does
+    int cap = prm->cand_cap > 0 ? prm->cand_cap : std::max(4096, det->cand_room);
+    if (cap > ZOLA_DETECT_MAX_CAP) { ctx->err = "zola_localize_frames: cand_cap above 2^20"; return ZOLA_E_ARG; }
     const int FB = std::max(1, std::min(nframes, prm->frames_per_batch > 0 ? prm->frames_per_batch : 1024));
     const size_t SS = (size_t)SX * SY, RR = (size_t)R * R;
     cudaStream_t st = ctx->stream;
@@ -450,6 +453,25 @@ int localize_impl(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const do
         if (e != cudaSuccess) return fail(e);
         int rc = zola_detect_dev(det, (double*)b_img.p, nf, cap, (double*)b_cand.p, (int*)b_cnt.p, st);
         if (rc) return rc;
+        std::vector<int> counts(nf);
+        e = cudaMemcpyAsync(counts.data(), b_cnt.p, (size_t)nf * 4, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return fail(e);
+        const int longest = *std::max_element(counts.begin(), counts.end());
+        det->cand_room = std::max(det->cand_room, longest);
+        if (longest > cap) {  // room for every candidate, then detect this batch again
+            if (longest > ZOLA_DETECT_MAX_CAP) {
+                ctx->err = "zola_localize_frames: a frame has more than 2^20 candidates";
+                return ZOLA_E_ARG;
+            }
+            cap = longest;
+            A(b_cand, (size_t)FB * cap * 7 * 8); A(b_cslot, (size_t)FB * cap * 4); A(b_cmax, (size_t)FB * cap * 8);
+            if (e != cudaSuccess) return fail(e);
+            V.cap = cap;
+            V.cand = (double*)b_cand.p; V.cand_slot = (int*)b_cslot.p; V.cand_maxp = (double*)b_cmax.p;
+            rc = zola_detect_dev(det, (double*)b_img.p, nf, cap, (double*)b_cand.p, (int*)b_cnt.p, st);
+            if (rc) return rc;
+        }
         for (int wave = 0;; ++wave) {
             e = cudaMemsetAsync(b_ns.p, 0, 4, st);
             if (e == cudaSuccess) e = cudaMemsetAsync(b_nacc.p, 0, 4, st);

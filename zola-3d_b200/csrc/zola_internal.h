@@ -104,6 +104,7 @@ struct zola_detector {
     std::vector<double> range;
     double* d_lib = nullptr;    // psf0 | varpsf | norm
     std::vector<double> h_psf;  // Z x R x R normalised library PSFs (pipeline initialisation)
+    int cand_room = 0;          // longest candidate list the pipeline has met (its next starting room)
 };
 
 namespace zola {
