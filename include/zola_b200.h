@@ -93,7 +93,12 @@ typedef struct {
 ZOLA_API int zola_ctx_create(int device, zola_ctx** out);
 ZOLA_API int zola_ctx_destroy(zola_ctx* ctx);
 ZOLA_API const char* zola_last_error(const zola_ctx* ctx);
-/* Stream the context launches on (cudaStream_t as void*). */
+/* Stream the context launches on (cudaStream_t as void*).  The *_dev entry
+ * points take a stream argument; NULL means this stream.  It is a blocking
+ * stream, so CUDA orders it with the legacy default stream (stream 0, torch's
+ * default stream): device inputs written there before the call are complete
+ * when the call reads them, and work queued there after the call waits for it.
+ * With any other stream of the caller's, pass that stream. */
 ZOLA_API void* zola_ctx_stream(zola_ctx* ctx);
 
 /* --- PSF (replaces DataPhase_ + PSFmany_float_ construction; the Java side
@@ -194,7 +199,7 @@ typedef struct {
     int cand_cap;             /* candidates stored per frame at the start (0: 4096); it grows to the
                                  longest list so that every frame walks its whole list */
     int frames_per_batch;     /* frames per device batch (0: 1024) */
-    int wave_fits;            /* candidates fitted ahead per frame and wave (0: 16); any value gives the
+    int wave_fits;            /* candidates fitted ahead per frame and wave (0: 8); any value gives the
                                  same rows as the reference's one-at-a-time walk */
 } zola_loc_params;
 

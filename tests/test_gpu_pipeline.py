@@ -59,15 +59,17 @@ def test_pipeline_matches_reference_pipeline(zpkg, ctx, precision):
     det.close()
 
 
-def test_wave_size_does_not_change_the_rows(zpkg, ctx):
+@pytest.mark.parametrize("S,R,N", [(96, 16, 64), (160, 40, 128)])
+def test_wave_size_does_not_change_the_rows(zpkg, ctx, S, R, N):
     """Fitting K candidates ahead per frame and wave replays the reference's
-    one-candidate-at-a-time walk exactly: K = 1, 16 and 64 give the same rows."""
+    one-candidate-at-a-time walk exactly: K = 1, 16 and 64 give the same rows
+    (a split fit does not depend on the batch it is in; 40 px ROIs take the
+    fused likelihood kernel whatever the wave's size)."""
     zern = astig_zernike()
-    S, R = 96, 16
-    psf_det = zpkg.PSF(ctx, zpkg.optics(size_fft=64, kz_reset=True, **OPTICS), zern)
-    psf_fit = zpkg.PSF(ctx, zpkg.optics(size_fft=64, **OPTICS), zern)
-    ref_fit = O.OraclePSF(64, 0.11, 1.4, 0.66, 1.518, 1.518, 0.9, zern)
-    frames = make_frames(ref_fit.model, S, 6, seed=91, emitters=8, R=32)
+    psf_det = zpkg.PSF(ctx, zpkg.optics(size_fft=N, kz_reset=True, **OPTICS), zern)
+    psf_fit = zpkg.PSF(ctx, zpkg.optics(size_fft=N, **OPTICS), zern)
+    ref_fit = O.OraclePSF(N, 0.11, 1.4, 0.66, 1.518, 1.518, 0.9, zern)
+    frames = make_frames(ref_fit.model, S, 6, seed=91, emitters=8, R=2 * R)
     det = zpkg.Detector(psf_det, S, S, R, -0.6, 0.6, 0.11, 0.1)
     runs = [zpkg.localize_frames(ctx, det, psf_fit, frames, -0.6, 0.6, photon_threshold=300.0, precision=1,
                                  max_iter=40, wave_fits=k) for k in (1, 16, 64)]

@@ -123,7 +123,12 @@ int zola_ctx_create(int device, zola_ctx** out) {
     if (!c) return ZOLA_E_ARG;
     c->device = device;
     c->num_sms = prop.multiProcessorCount;
-    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+    // The context's stream is a blocking stream: CUDA orders it with the legacy
+    // default stream, so device buffers that default-stream work (torch's
+    // default stream, plain cudaMemcpy) wrote before a call are complete when the
+    // call reads them.  The copy stream only carries host-to-device copies of
+    // the host-buffer calls and stays non-blocking.
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamDefault) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&c->d_counter, 64 * sizeof(int)) != cudaSuccess) {
         delete c;

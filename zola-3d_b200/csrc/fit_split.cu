@@ -1284,8 +1284,9 @@ __global__ void __launch_bounds__(S5_THREADS) k_stage5(SplitDev P, const float* 
 constexpr int E45_THREADS = 384;                 // 12 epilogue warps: three per TMEM lane quadrant
 constexpr int S45_THREADS = E45_THREADS + 64;    // + producer warp + MMA warp
 constexpr int S45_NBUF = 4;
-constexpr int S45_MIN_R = 40;       // ROI side from which the fused form is faster
-constexpr int S45_MIN_POOL = 1024;  // and the pool size (small batches favour many short kernels)
+// ROI side from which the fused form is faster.  The choice depends on R only,
+// never on the batch, so a ROI's fit is the same bit for bit in any batch.
+constexpr int S45_MIN_R = 40;
 
 __host__ __device__ inline size_t s45_roi_bytes(int R) { return ((size_t)R * R * 4 + 127) / 128 * 128; }
 
@@ -2237,11 +2238,12 @@ int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d
     const int max_rounds = (prm->max_iter + 2) * ((n + P - 1) / P + 1) + 8 + 4 * (feed ? feed->n_chunks : 0);
     int rounds = 0;
     const bool fused = ctx->split_fused && fused_fits(*sp.pl);
-    // Large ROIs in large pools: column blur and likelihood sums in one
-    // persistent kernel (the maps never leave the SM).  Otherwise the
-    // column-blur maps go through memory to the warp-per-slot likelihood
-    // kernel, which keeps many slots in flight per SM.
-    const bool fused45 = sp.pl->R >= S45_MIN_R && P >= S45_MIN_POOL;
+    // Large ROIs: column blur and likelihood sums in one persistent kernel (the
+    // maps never leave the SM).  Small ROIs: the column-blur maps go through
+    // memory to the warp-per-slot likelihood kernel, which keeps many slots in
+    // flight per SM.  The two sum in different orders; the choice depends on R
+    // alone so that a fit never depends on the batch it is in.
+    const bool fused45 = sp.pl->R >= S45_MIN_R;
     while (true) {
         for (int k = 0; k < 4; ++k) {
             if (feed && queue < n) {  // idle slots take ROIs that arrived since

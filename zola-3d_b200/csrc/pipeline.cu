@@ -343,7 +343,7 @@ struct Buf {
     }
 };
 
-constexpr int PIPE_WAVE_FITS = 16;  // speculative fits per frame and wave
+constexpr int PIPE_WAVE_FITS = 8;  // speculative fits per frame and wave
 
 }  // namespace
 
