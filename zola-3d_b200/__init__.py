@@ -290,7 +290,9 @@ class PSF:
         return res
 
     def fit_dev(self, rois, init, prm, out, crlb=None, nll=None, status=None, iters=None, stream=None):
-        """Device form over torch CUDA tensors (rois float32, init/out float64)."""
+        """Device form over torch CUDA tensors (rois float32, init/out float64).
+        stream: a cudaStream_t handle; None runs on the context's stream, which
+        CUDA orders with the default stream (torch's default stream)."""
         n, R = rois.shape[0], rois.shape[1]
         self.ctx.check(lib().zola_fit_batch_dev(self.ctx.h, self.h, R, _ptr(rois), _ptr(init), n, ctypes.byref(prm),
                                                 _ptr(out), _ptr(crlb), _ptr(nll), _ptr(status), _ptr(iters), stream),
