@@ -468,7 +468,7 @@ def main():
     peak_gbs = peaks.get("hbm_gbs", 6650.0)
     peak_src = "of measured" if "bf16_tflops_sustained" in peaks and "hbm_gbs" in peaks else "of fallback"
     flops, nbytes = {}, {}
-    fused45 = lambda R: R >= 40 and (args.pool or 4096) >= 1024  # noqa: E731  (the library's path choice)
+    fused45 = lambda R: R >= 40  # noqa: E731  (the library's path choice: by ROI side alone)
     for j in job:
         R, N = j["cls"]["R"], j["cls"]["N"]
         W, D = window(R, N), disk_rows(N)
