@@ -186,6 +186,7 @@ typedef struct {
     double intensity, background;   /* photons, photons / px */
     double chi2;                    /* scoreCompute: mean (patch - model)^2 / model */
     double crlb_x_nm, crlb_y_nm, crlb_z_nm;
+    int candidate;                  /* index of the row's candidate in its frame's sorted candidate list */
 } zola_localization;
 
 typedef struct {
@@ -310,9 +311,11 @@ ZOLA_API int zola_drift(zola_ctx* ctx, const double* xyz_nm, const double* crlb_
  * Device buffers and stream as in zola_fit_batch_dev; prm->precision must be
  * ZOLA_PREC_FP64.  The PSF's tables for this ROI size must exist (any model or
  * fit call with this R, e.g. zola_psf_model_dev(psf, R, NULL, 0, NULL, NULL, s),
- * prepares them); the call itself allocates nothing.  Its first call on a
- * device looks up the array's device address; make that first call before any
- * stream capture.  ROI sizes whose per-block work area exceeds the array are
+ * prepares them); the call itself allocates nothing.  It makes the PSF's
+ * device current, as the other entry points do.  Its first call on a device
+ * (and its first call after that device's context was destroyed and created
+ * again, e.g. by cudaDeviceReset) looks up the array's device address; make
+ * that first call before any stream capture.  ROI sizes whose per-block work area exceeds the array are
  * rejected with ZOLA_E_ARG; large windows run on fewer blocks.  All calls share
  * the array: calls that overlap on the GPU race, so serialise them. */
 ZOLA_API int zola_fit_batch_noalloc(zola_psf* psf, int R, const float* d_rois, const double* d_init5, int n,

@@ -46,6 +46,7 @@ def lib():
         L.orc_psf_model.argtypes = [vp, i, i, vp, vp, vp]
         L.orc_psf_model_oil.argtypes = [vp, i, d, d, d, d, vp]
         L.orc_localize_cd.argtypes = [vp, i, i, vp, vp, d, d, i, d, vp, vp, vp, vp, i]
+        L.orc_localize_cd_eps.argtypes = [vp, i, i, vp, vp, d, d, i, d, d, vp, vp, vp, vp, i]
         L.orc_fit_lm.argtypes = [vp, i, i, vp, vp, vp, i, vp, vp, vp, vp, vp, i]
         L.orc_fit_lm_scmos.argtypes = [vp, i, i, vp, vp, vp, vp, i, vp, vp, vp, vp, vp, i]
         L.orc_nll_grad.restype = d
@@ -62,6 +63,8 @@ def lib():
         L.orc_detect.argtypes = [vp, i, vp, i, vp, vp, i]
         L.orc_localize_frames.restype = i
         L.orc_localize_frames.argtypes = [vp, vp, i, vp, d, d, d, d, i, vp, i]
+        L.orc_localize_frames_lm.restype = i
+        L.orc_localize_frames_lm.argtypes = [vp, vp, i, vp, d, d, d, d, i, d, i, vp, i]
         L.orc_localize_frames_scmos.restype = i
         L.orc_localize_frames_scmos.argtypes = [vp, vp, i, vp, vp, vp, vp, d, d, d, d, i, vp, i]
         L.orc_calib_nll.restype = d
@@ -121,7 +124,8 @@ class OraclePSF:
         lib().orc_psf_model_oil(self.h, R, x, y, zoil, zwat, _p(out))
         return out
 
-    def localize_cd(self, patches, init_abxyz, minZ, maxZ, iter_max=20, photon_thr=0.0, threads=1):
+    def localize_cd(self, patches, init_abxyz, minZ, maxZ, iter_max=20, photon_thr=0.0, threads=1, eps=None):
+        """The reference coordinate descent; eps (um) replaces its stopping distance 1e-4 when given."""
         patches = _f64(patches)
         n, R = patches.shape[0], patches.shape[1]
         init = _f64(init_abxyz)
@@ -129,8 +133,12 @@ class OraclePSF:
         crlb = np.zeros((n, 3))
         st = np.zeros(n, np.int32)
         ev = np.zeros(n, np.int32)
-        lib().orc_localize_cd(self.h, R, n, _p(patches), _p(init), minZ, maxZ, iter_max, photon_thr,
-                              _p(out), _p(crlb), _p(st), _p(ev), threads)
+        if eps is None:
+            lib().orc_localize_cd(self.h, R, n, _p(patches), _p(init), minZ, maxZ, iter_max, photon_thr,
+                                  _p(out), _p(crlb), _p(st), _p(ev), threads)
+        else:
+            lib().orc_localize_cd_eps(self.h, R, n, _p(patches), _p(init), minZ, maxZ, iter_max, photon_thr, eps,
+                                      _p(out), _p(crlb), _p(st), _p(ev), threads)
         return out, crlb, st, ev
 
     def fit_lm(self, patches, init_xyzab, zmin, zmax, xymax, tol_xyz=1e-5, step_xy=0.11, step_z=0.22,
@@ -231,6 +239,17 @@ class OracleDetector:
         rows = np.zeros((cap, 10))
         n = lib().orc_localize_frames(self.h, fit_psf.h, frames.shape[0], _p(frames), minZ, maxZ, photon_thr, max_snr,
                                       cap, _p(rows), threads)
+        return rows[:min(n, cap)]
+
+    def localize_frames_lm(self, fit_psf, frames, minZ, maxZ, photon_thr=500.0, max_snr=1.0, max_iter=40,
+                           tol_xyz=1e-4, threads=1, cap=100000):
+        """The same frame loop with the FP64 LM fit of the library (the oracle of
+        zola_localize_frames).  Rows: frame, x_nm, y_nm, z_nm, A, B, chi2, crlbx,
+        crlby, crlbz, candidate index."""
+        frames = _f64(frames)
+        rows = np.zeros((cap, 11))
+        n = lib().orc_localize_frames_lm(self.h, fit_psf.h, frames.shape[0], _p(frames), minZ, maxZ, photon_thr,
+                                         max_snr, max_iter, tol_xyz, cap, _p(rows), threads)
         return rows[:min(n, cap)]
 
     def localize_frames_scmos(self, fit_psf, adu, offset, gain, variance, minZ, maxZ, photon_thr=500.0, max_snr=1.0,

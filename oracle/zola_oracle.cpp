@@ -904,12 +904,15 @@ extern "C" {
 // Reference coordinate-descent localisation (+ finite-difference CRLB) of n
 // patches.  init: n*5 (A, B, x, y, z) in the order Localization.init takes.
 // out: n*5 (x, y, z, A, B); crlb: n*3 (um); status: 1 ok, 0 photon break, -1 NaN.
-void orc_localize_cd(void* h, int R, int n, const double* patches, const double* init,
-                     double minZ, double maxZ, int iterMax, double photonThr,
-                     double* out, double* crlb, int* status, int* evals, int threads) {
+// eps is the stopping distance of the x/y/z move per sweep (the reference's
+// 1e-4 um, Localization.java:31); orc_localize_cd_eps takes another one.
+void orc_localize_cd_eps(void* h, int R, int n, const double* patches, const double* init,
+                         double minZ, double maxZ, int iterMax, double photonThr, double eps,
+                         double* out, double* crlb, int* status, int* evals, int threads) {
     const Psf* p = (const Psf*)h;
     parallel_for(n, threads, [&](int i) {
         CD cd;
+        cd.eps = eps;
         cd.p = p; cd.R = R; cd.d = patches + (size_t)i * R * R;
         cd.minZ = minZ; cd.maxZ = maxZ; cd.iterMax = iterMax; cd.photonThreshold = photonThr;
         cd.maxShift = p->dx / 2.;
@@ -921,6 +924,13 @@ void orc_localize_cd(void* h, int R, int n, const double* patches, const double*
         status[i] = st;
         if (evals) evals[i] = cd.nevals;
     });
+}
+
+void orc_localize_cd(void* h, int R, int n, const double* patches, const double* init,
+                     double minZ, double maxZ, int iterMax, double photonThr,
+                     double* out, double* crlb, int* status, int* evals, int threads) {
+    orc_localize_cd_eps(h, R, n, patches, init, minZ, maxZ, iterMax, photonThr, 1e-4, out, crlb, status, evals,
+                        threads);
 }
 
 // FP64 LM fit of n patches.  init/out: n*5 (x, y, z, A, B).  params:
@@ -1011,11 +1021,17 @@ namespace {
 // the patches; vmap (SX x SY, nullable) is the sCMOS var/gain^2 map: getAandB
 // then uses patch - v (:1168-1211), the fit and the model add v, and the
 // Fisher matrix leaves it out (Localization.java:317-451).
+//
+// lmp (nullable): fit each candidate with the FP64 LM (lm_fit, the oracle of
+// the library's own fit) instead of the reference coordinate descent, on the
+// patch rounded to float as the library stages it; a fit is then used unless
+// its model went non-positive.  Rows hold ncol values: 10, or 11 with the
+// candidate's index in its frame's sorted candidate list last.
 int localize_frames_impl(Detector* D, const Psf* p, int nframes, const double* det_frames, const double* fit_frames,
                          const double* vmap, double minZ, double maxZ, double photonThr, double maxSNR, int rows_cap,
-                         double* rows, int threads) {
+                         double* rows, int threads, const LMParams* lmp = nullptr, int ncol = 10) {
     const int SX = D->SX, SY = D->SY, R = D->R, h = R / 2;
-    std::vector<std::vector<std::array<double, 10>>> per(nframes);
+    std::vector<std::vector<std::array<double, 11>>> per(nframes);
     parallel_for(nframes, threads, [&](int f) {
         const double* img = fit_frames + (size_t)f * SX * SY;
         std::vector<std::array<double, 7>> v;
@@ -1057,7 +1073,22 @@ int localize_frames_impl(Detector* D, const Psf* p, int nframes, const double* d
                 cd.maxShift = p->dx / 2.;
                 cd.psi.resize(R * R); cd.mu.resize(R * R);
                 cd.ta = A; cd.tb = B; cd.tx = -v[sel][5]; cd.ty = -v[sel][6]; cd.tz = D->range[r] + v[sel][4];
-                int st = cd.run();
+                int st;
+                if (lmp) {
+                    std::vector<double> pf((size_t)R * R), vf;
+                    for (int k = 0; k < R * R; ++k) pf[k] = (double)(float)patch[k];
+                    if (vmap) {
+                        vf.resize((size_t)R * R);
+                        for (int k = 0; k < R * R; ++k) vf[k] = (double)(float)sv[k];
+                    }
+                    const double init[5] = {cd.tx, cd.ty, cd.tz, cd.ta, cd.tb};
+                    double o[5], nll;
+                    int ev;
+                    st = lm_fit(p, R, pf.data(), init, *lmp, o, &nll, &ev, nullptr, vmap ? vf.data() : nullptr) != -1;
+                    cd.tx = o[0]; cd.ty = o[1]; cd.tz = o[2]; cd.ta = o[3]; cd.tb = o[4];
+                } else {
+                    st = cd.run();
+                }
                 if (st == 1) {
                     psf_model(p, R, cd.tx, cd.ty, p->zfocus, cd.tz, psi.data(), nullptr);
                     double mthr = 0;
@@ -1075,7 +1106,8 @@ int localize_frames_impl(Detector* D, const Psf* p, int nframes, const double* d
                             double cr[3];
                             fisher_crlb_fd(p, R, cd.tx, cd.ty, cd.tz, cd.ta, cd.tb, cr);
                             per[f].push_back({(double)f, 1000 * (ci * p->dx - cd.tx), 1000 * (cj * p->dx - cd.ty), 1000 * cd.tz,
-                                              cd.ta, cd.tb, chi, 1000 * cr[0], 1000 * cr[1], 1000 * cr[2]});
+                                              cd.ta, cd.tb, chi, 1000 * cr[0], 1000 * cr[1], 1000 * cr[2],
+                                              (double)sel});
                             for (int a = 0; a < R; ++a)
                                 for (int b = 0; b < R; ++b)
                                     if (psi[(size_t)a * R + b] * cd.ta + cd.tb + sv[(size_t)a * R + b] - cd.tb > mthr)
@@ -1095,7 +1127,7 @@ int localize_frames_impl(Detector* D, const Psf* p, int nframes, const double* d
     for (int f = 0; f < nframes; ++f)
         for (auto& row : per[f]) {
             if (n < rows_cap)
-                for (int c = 0; c < 10; ++c) rows[(size_t)n * 10 + c] = row[c];
+                for (int c = 0; c < ncol; ++c) rows[(size_t)n * ncol + c] = row[c];
             ++n;
         }
     return n;
@@ -1109,6 +1141,20 @@ int orc_localize_frames(void* dh, void* ph, int nframes, const double* frames, d
                         double photonThr, double maxSNR, int rows_cap, double* rows, int threads) {
     return localize_frames_impl((Detector*)dh, (const Psf*)ph, nframes, frames, frames, nullptr, minZ, maxZ,
                                 photonThr, maxSNR, rows_cap, rows, threads);
+}
+
+// The same frame loop with every candidate fitted by the FP64 LM of the
+// library's fit (lm_fit): the oracle of zola_localize_frames.  params: max_iter
+// evaluations and tol_xyz (um); the fit box and step caps as the library sets
+// them (z in [minZ - 0.3, maxZ + 0.3], |x|, |y| <= 10 dx + 1e-3, steps dx and
+// 2 dx).  Rows of 11: the 10 columns above and the candidate index.
+int orc_localize_frames_lm(void* dh, void* ph, int nframes, const double* frames, double minZ, double maxZ,
+                           double photonThr, double maxSNR, int max_iter, double tol_xyz, int rows_cap, double* rows,
+                           int threads) {
+    const Psf* p = (const Psf*)ph;
+    const LMParams P{minZ - 0.3, maxZ + 0.3, 10 * p->dx + 1e-3, max_iter, tol_xyz, p->dx, 2 * p->dx};
+    return localize_frames_impl((Detector*)dh, p, nframes, frames, frames, nullptr, minZ, maxZ, photonThr, maxSNR,
+                                rows_cap, rows, threads, &P, 11);
 }
 
 // sCMOS form (LocalizationPipeline.java:588-640): detection on

@@ -85,28 +85,42 @@ def test_fp64_fit_matches_oracle_lm(zpkg, ctx, N, R, zern):
     assert np.median(rel) < 1e-9 and rel.max() < 1e-2
 
 
-def test_fp64_fit_matches_reference_coordinate_descent(zpkg, ctx):
-    """The reference's own CPU algorithm (coordinate descent) reaches the same
-    optimum within the north_star tolerances."""
-    zern = astig_zernike()
-    psf, ref = pair(zpkg, ctx, 64, zern)
-    ref_f32 = O.OraclePSF(64, 0.11, 1.4, 0.66, 1.518, 1.518, 0.9, zern, gauss_f32=True)
-    rois, truth = synth_rois(ref.model, 16, 16, seed=11, zrange=0.5, photons=3000)
+@pytest.mark.parametrize("N,R,zern", CASES[:3])
+def test_fp64_fit_matches_reference_coordinate_descent(zpkg, ctx, N, R, zern):
+    """The reference's own CPU algorithm (coordinate descent with its float
+    spectral Gaussian, Localization.java:491-653) reaches the same optimum from
+    a detection-like start (x = y = 0, z on the 0.1 um library grid): within
+    0.5 nm x/y, 1 nm z and 1e-3 in photons with the reference's stopping
+    distance (x/y/z move per sweep below 1e-4 um; its photon count carries the
+    remaining convergence error of a sweep that stops on x/y/z alone), and
+    within 0.05 nm and 2e-4 when the descent is run to a tighter stop (1e-6 um)."""
+    import os
+    psf, ref = pair(zpkg, ctx, N, zern)
+    ref_f32 = O.OraclePSF(N, 0.11, 1.4, 0.66, 1.518, 1.518, 0.9, zern, gauss_f32=True)
+    rois, truth = synth_rois(ref.model, R, 16, seed=11 + R, zrange=0.5, photons=3000)
     init = truth.copy()
-    init[:, :3] = 0
-    prm = zpkg.PSF.fit_params(-0.9, 0.9, 0.88, max_iter=40, precision=zpkg.ZOLA_PREC_FP64)
+    init[:, :2] = 0
+    init[:, 2] = np.round(truth[:, 2] / 0.1) * 0.1
+    xymax = R * 0.11 / 2
+    prm = zpkg.PSF.fit_params(-0.9, 0.9, xymax, max_iter=40, precision=zpkg.ZOLA_PREC_FP64)
     res = psf.fit(rois, init, prm)
-    cd, crlb, stc, _ = ref_f32.localize_cd(rois.astype(np.float64), np.c_[init[:, 3], init[:, 4], init[:, :3]],
-                                           -0.9, 0.9, 20)
+    threads = os.cpu_count() or 1
+    abxyz = np.c_[init[:, 3], init[:, 4], init[:, :3]]
+    zs = z_symmetric(zern)
+    cd, _, stc, _ = ref_f32.localize_cd(rois.astype(np.float64), abxyz, -0.9, 0.9, 20, threads=threads)
     good = (stc == 1) & (res["status"] == 1)
-    assert good.mean() > 0.8
-    d = np.abs(res["theta"][good] - cd[good]) * 1000
+    assert good.mean() > 0.75
+    d = theta_diff(res["theta"][good], cd[good], zs) * 1000
     assert d[:, :2].max() < 0.5
     assert d[:, 2].max() < 1.0
-    # photons: the coordinate descent stops on the x/y/z move alone, so its A
-    # carries its own convergence error; most fits agree to 1e-3
-    rel = np.abs(res["theta"][good, 3] - cd[good, 3]) / cd[good, 3]
-    assert np.median(rel) < 1e-3 and rel.max() < 3e-3
+    assert (d[:, 3] / 1000 / cd[good, 3]).max() < 1e-3
+    # the same descent run to a tighter stop
+    cdt, _, stt, _ = ref_f32.localize_cd(rois.astype(np.float64), abxyz, -0.9, 0.9, 400, threads=threads, eps=1e-6)
+    good = (stt == 1) & (res["status"] == 1)
+    assert good.mean() > 0.75
+    d = theta_diff(res["theta"][good], cdt[good], zs) * 1000
+    assert d[:, :3].max() < 0.05
+    assert (d[:, 3] / 1000 / cdt[good, 3]).max() < 2e-4
 
 
 def test_fit_rejects_bad_arguments(zpkg, ctx):

@@ -3,8 +3,10 @@ restatement of LocalizationPipeline with the reference coordinate descent."""
 import numpy as np
 import pytest
 
+import os
+
 import oracle as O
-from common import OPTICS, astig_zernike
+from common import OPTICS, astig_zernike, tetrapod_zernike
 from test_gpu_detect import make_frames
 
 pytestmark = pytest.mark.gpu
@@ -76,4 +78,52 @@ def test_wave_size_does_not_change_the_rows(zpkg, ctx, S, R, N):
     assert len(runs[0]) > 10
     for r in runs[1:]:
         assert np.array_equal(r, runs[0])
+    det.close()
+
+
+ROW_CASES = [
+    # 96 x 96 frames, 16 px ROIs, astigmatic PSF (pupil 64^2), +-0.6 um
+    (96, 16, 64, astig_zernike(), 8, 4, 0.6, 20.0),
+    # the frame-pipeline configuration: 256 x 256 frames, 40 px ROIs, 45-mode
+    # tetrapod (pupil 128^2), +-2 um, 0.1 um library, background 30
+    (256, 40, 128, tetrapod_zernike(), 3, 5, 2.0, 30.0),
+]
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("S,R,N,zern,nf,emitters,zr,bg", ROW_CASES)
+def test_pipeline_rows_match_oracle_lm_pipeline(zpkg, ctx, S, R, N, zern, nf, emitters, zr, bg, precision):
+    """Row by row against the oracle's frame loop driven by the FP64 LM of the
+    same fit (LocalizationPipeline.java:766-945 with lm_fit): the same accepted
+    candidates in the same order (joined on frame and candidate index), and per
+    row x/y within 0.5 nm, z within 1 nm, photons within 1e-3 (FP64 fits:
+    within 1e-3 nm and 1e-6), chi2 and CRLB to the model's precision."""
+    psf_det = zpkg.PSF(ctx, zpkg.optics(size_fft=N, kz_reset=True, **OPTICS), zern)
+    psf_fit = zpkg.PSF(ctx, zpkg.optics(size_fft=N, **OPTICS), zern)
+    ref_det = O.OraclePSF(N, 0.11, 1.4, 0.66, 1.518, 1.518, 0.9, zern, kz_reset=True)
+    ref_fit = O.OraclePSF(N, 0.11, 1.4, 0.66, 1.518, 1.518, 0.9, zern)
+    frames = make_frames(ref_fit.model, S, nf, seed=500 + S, emitters=emitters, R=64 if R > 20 else 32, zr=zr * 0.9,
+                         bg=bg)
+    minZ, maxZ, step = -zr, zr, 0.1
+    det = zpkg.Detector(psf_det, S, S, R, minZ, maxZ, step, 0.1)
+    odet = O.OracleDetector(ref_det, S, S, R, minZ, maxZ, step, 0.1)
+    got = zpkg.localize_frames(ctx, det, psf_fit, frames, minZ, maxZ, photon_threshold=500.0, precision=precision,
+                               max_iter=50, tol_xyz=1e-4)
+    want = odet.localize_frames_lm(ref_fit, frames, minZ, maxZ, photon_thr=500.0, max_iter=50, tol_xyz=1e-4,
+                                   threads=os.cpu_count() or 1)
+    assert len(want) >= 2 * nf
+    kg = list(zip(got["frame"].tolist(), got["candidate"].tolist()))
+    kw = list(zip(want[:, 0].astype(int).tolist(), want[:, 10].astype(int).tolist()))
+    assert kg == kw, "accepted candidates differ"
+    dxy = np.maximum(np.abs(got["x_nm"] - want[:, 1]), np.abs(got["y_nm"] - want[:, 2]))
+    dz = np.abs(got["z_nm"] - want[:, 3])
+    dA = np.abs(got["intensity"] - want[:, 4]) / want[:, 4]
+    if precision == 0:
+        assert dxy.max() < 1e-3 and dz.max() < 1e-3 and dA.max() < 1e-6
+    else:
+        assert dxy.max() <= 0.5 and dz.max() <= 1.0 and dA.max() <= 1e-3
+    assert np.allclose(got["chi2"], want[:, 6], rtol=1e-3 if precision else 1e-6)
+    for c, k in (("crlb_x_nm", 7), ("crlb_y_nm", 8), ("crlb_z_nm", 9)):
+        assert np.allclose(got[c], want[:, k], rtol=2e-3)
+    assert list(got["id"]) == list(range(len(got)))
     det.close()

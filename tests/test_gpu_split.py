@@ -55,6 +55,63 @@ def test_split_fit_matches_fp64_fit(zpkg, ctx, N, R, zern):
     assert np.allclose(a["crlb"][ok, :3], b["crlb"][ok, :3], rtol=2e-2)
 
 
+ORACLE_CASES = CASES + [(128, 40, tetrapod_zernike())]
+
+
+@pytest.mark.parametrize("N,R,zern", ORACLE_CASES)
+def test_split_fit_matches_oracle_every_roi(zpkg, ctx, N, R, zern):
+    """The split-precision fit against the FP64 oracle of the same fit
+    (oracle.fit_lm: the same LM algorithm, FP64 model through FFTs), ROI by
+    ROI, every status included.  Fits that end with the same status agree
+    within the north_star tolerances (0.5 nm x/y, 1 nm z, 1e-3 photons) when
+    converged; status disagreements are rare (the model differs by ~2^-22, so
+    an accept/reject decision on a flat likelihood can flip) and their
+    parameter difference stays below 0.5 nm / 1 nm / 1e-3 too once both fits
+    are continued to convergence."""
+    import os
+    psf = make(zpkg, ctx, N, zern)
+    ref = O.OraclePSF(N, 0.11, 1.4, 0.66, 1.518, 1.518, 0.9, zern, gauss_f32=False)
+    n = 48
+    rois, truth = synth_rois(ref.model, R, n, seed=101 + R + N, zrange=0.6, photons=3000, sigma_ln=0.6)
+    init = truth.copy()
+    init[:, :2] = 0
+    init[:, 2] = np.round(truth[:, 2] / 0.1) * 0.1
+    init[:, 3] *= 0.85
+    xymax = R * 0.11 / 2
+    psp = zpkg.PSF.fit_params(-1.0, 1.0, xymax, max_iter=50, tol_xyz=1e-4, precision=zpkg.ZOLA_PREC_SPLIT)
+    b = psf.fit(rois, init, psp)
+    threads = os.cpu_count() or 1
+    o, _, st, _ = ref.fit_lm(rois.astype(np.float64), init, -1.0, 1.0, xymax, tol_xyz=1e-4, max_iter=50,
+                             threads=threads)
+    zs = z_symmetric(zern)
+
+    def within(d, a):
+        return (d[:, :2].max(1) <= 0.5e-3) & (d[:, 2] <= 1e-3) & (d[:, 3] / a[:, 3] <= 1e-3)
+
+    same = b["status"] == st
+    assert same.mean() >= 0.9, f"status agreement {same.mean():.3f}"
+    d = theta_diff(b["theta"], o, zs)
+    ok = within(d, o)
+    conv = same & (st == 1)
+    assert conv.mean() >= 0.8
+    assert ok[conv].all(), f"converged fits outside tolerance: {d[conv & ~ok]}"
+    # every other ROI (different status, or both stopped at the evaluation cap):
+    # continue both from where they stopped with a larger budget; they must then agree
+    rest = np.where(~(conv & ok))[0]
+    if rest.size:
+        p2 = zpkg.PSF.fit_params(-1.0, 1.0, xymax, max_iter=200, tol_xyz=1e-4, precision=zpkg.ZOLA_PREC_SPLIT)
+        b2 = psf.fit(rois[rest], b["theta"][rest], p2)
+        o2, _, st2, _ = ref.fit_lm(rois[rest].astype(np.float64), o[rest], -1.0, 1.0, xymax, tol_xyz=1e-4,
+                                   max_iter=200, threads=threads)
+        both = (b2["status"] == 1) & (st2 == 1)
+        d2 = theta_diff(b2["theta"][both], o2[both], zs)
+        assert within(d2, o2[both]).all(), f"continued fits outside tolerance: {d2}"
+        # anything still unconverged after 200 evaluations sits on a flat likelihood:
+        # allow it but keep it rare
+        assert (~both).sum() <= max(1, n // 24)
+    psf.close()
+
+
 def test_split_fit_small_pool_refills(zpkg, ctx):
     """A pool much smaller than the batch retires and refills slots; every ROI is fitted once."""
     psf = make(zpkg, ctx, 64, astig_zernike())

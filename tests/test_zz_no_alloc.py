@@ -42,10 +42,14 @@ def test_noalloc_fit_matches_regular_fp64_fit(zpkg, ctx, N, R, zern):
     want = buffers()
     psf.fit_dev(rois, init, prm, *want, stream=ctx.stream)   # regular path (also prepares the tables for R)
     torch.cuda.synchronize()
-    for _ in range(2):
+    for call in range(2):
         got = buffers()
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info(dev)[0]
         zpkg.fit_noalloc_dev(psf, rois, init, prm, *got, stream=ctx.stream)
         torch.cuda.synchronize()
+        if call == 1:  # the first call looked the array up; the second must not allocate
+            assert torch.cuda.mem_get_info(dev)[0] == free_before
         assert torch.equal(got[3], want[3])          # status
         assert torch.equal(got[4], want[4])          # evaluations
         for g, w in zip(got[:3], want[:3]):

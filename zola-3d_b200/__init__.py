@@ -47,7 +47,7 @@ class Localization(ctypes.Structure):
     _fields_ = [("id", ctypes.c_int), ("frame", ctypes.c_int), ("x_nm", ctypes.c_double), ("y_nm", ctypes.c_double),
                 ("z_nm", ctypes.c_double), ("intensity", ctypes.c_double), ("background", ctypes.c_double),
                 ("chi2", ctypes.c_double), ("crlb_x_nm", ctypes.c_double), ("crlb_y_nm", ctypes.c_double),
-                ("crlb_z_nm", ctypes.c_double)]
+                ("crlb_z_nm", ctypes.c_double), ("candidate", ctypes.c_int)]
 
 
 class LocParams(ctypes.Structure):
@@ -471,7 +471,7 @@ class Calibration:
 
 
 LOC_COLUMNS = ["id", "frame", "x_nm", "y_nm", "z_nm", "intensity", "background", "chi2", "crlb_x_nm", "crlb_y_nm",
-               "crlb_z_nm"]
+               "crlb_z_nm", "candidate"]
 
 
 def localize_frames(ctx, det, fit_psf, frames, minZ, maxZ, photon_threshold=500.0, max_snr=1.0, max_iter=30,
@@ -488,7 +488,7 @@ def localize_frames(ctx, det, fit_psf, frames, minZ, maxZ, photon_threshold=500.
     ctx.check(lib().zola_localize_frames(ctx.h, det.h, fit_psf.h, _ptr(frames), nf, int(frame0), ctypes.byref(prm),
                                          ctypes.cast(out, ctypes.c_void_p), cap, ctypes.byref(n)),
               "zola_localize_frames")
-    dt = np.dtype([(c, np.int32 if c in ("id", "frame") else np.float64) for c in LOC_COLUMNS])
+    dt = np.dtype([(c, np.int32 if c in ("id", "frame", "candidate") else np.float64) for c in LOC_COLUMNS])
     arr = np.zeros(n.value, dtype=dt)
     for k in range(n.value):
         arr[k] = tuple(getattr(out[k], c) for c in LOC_COLUMNS)
@@ -510,7 +510,7 @@ def localize_frames_scmos(ctx, det, fit_psf, adu, offset, gain, variance, minZ, 
                                                _ptr(maps[0]), _ptr(maps[1]), _ptr(maps[2]),
                                                ctypes.cast(out, ctypes.c_void_p), cap, ctypes.byref(n)),
               "zola_localize_frames_scmos")
-    dt = np.dtype([(c, np.int32 if c in ("id", "frame") else np.float64) for c in LOC_COLUMNS])
+    dt = np.dtype([(c, np.int32 if c in ("id", "frame", "candidate") else np.float64) for c in LOC_COLUMNS])
     arr = np.zeros(n.value, dtype=dt)
     for k in range(n.value):
         arr[k] = tuple(getattr(out[k], c) for c in LOC_COLUMNS)

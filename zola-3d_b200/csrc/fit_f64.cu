@@ -419,26 +419,56 @@ static __device__ __align__(256) unsigned char g_fit_noalloc_scratch[zola::NOALL
 
 namespace {
 std::mutex g_noalloc_mu;
-void* g_noalloc_ptr[64] = {};
+// One cached device address per (device, CUDA context): a context that was
+// destroyed and created again (cudaDeviceReset, or the primary context
+// released and retained again) gets its address looked up afresh.
+struct NoallocEntry {
+    void* context = nullptr;
+    void* ptr = nullptr;
+};
+NoallocEntry g_noalloc[64];
 
-// Device address of the scratch array on the current device, looked up once
-// per device (host code must not use the array's name as a device pointer).
+// The current CUDA context of the calling thread, through the driver entry
+// point the runtime exposes (no link against the driver library).
+void* current_context() {
+    typedef int (*CtxGetCurrent)(void**);
+    static CtxGetCurrent fn = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (CtxGetCurrent)f;
+        looked = true;
+    }
+    void* c = nullptr;
+    if (fn && fn(&c) != 0) c = nullptr;
+    return c;
+}
+
+// Device address of the scratch array in the current context (host code must
+// not use the array's name as a device pointer).  Looked up once per device
+// and context; the caller has made the device current.
 void* noalloc_scratch(int device, std::string& err) {
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
     if (device < 0 || device >= 64) {
         err = "zola_fit_batch_noalloc: device index out of range";
         return nullptr;
     }
-    if (!g_noalloc_ptr[device]) {
+    void* c = current_context();
+    NoallocEntry& e = g_noalloc[device];
+    if (!e.ptr || c != e.context) {
         void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_fit_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            err = std::string("zola_fit_batch_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+        cudaError_t rc = cudaGetSymbolAddress(&p, g_fit_noalloc_scratch);
+        if (rc != cudaSuccess || !p) {
+            err = std::string("zola_fit_batch_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(rc);
             return nullptr;
         }
-        g_noalloc_ptr[device] = p;
+        e.ptr = p;
+        e.context = c;
     }
-    return g_noalloc_ptr[device];
+    return e.ptr;
 }
 }  // namespace
 
@@ -471,12 +501,12 @@ extern "C" int zola_fit_batch_noalloc(zola_psf* psf, int R, const float* d_rois,
     }
     WindowTables* w = &it->second;
     if (n == 0) return ZOLA_OK;
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev != ctx->device) {
-        ctx->err = "zola_fit_batch_noalloc: make the PSF's device current first";
-        return ZOLA_E_ARG;
+    // the PSF's device, as every other entry point (no allocation once its context exists)
+    if (cudaSetDevice(ctx->device) != cudaSuccess) {
+        ctx->err = "zola_fit_batch_noalloc: cudaSetDevice failed";
+        return ZOLA_E_CUDA;
     }
-    char* base = (char*)noalloc_scratch(dev, ctx->err);
+    char* base = (char*)noalloc_scratch(ctx->device, ctx->err);
     if (!base) return ZOLA_E_CUDA;
     const size_t per_cta = f64_work_bytes(psf->D, w->W, w->R);
     const int use_smem = per_cta + 8192 <= 200 * 1024;

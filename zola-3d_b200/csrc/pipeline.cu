@@ -541,6 +541,7 @@ int localize_impl(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const do
         L.frame = frame0 + r.frame;
         L.x_nm = r.x; L.y_nm = r.y; L.z_nm = r.z; L.intensity = r.A; L.background = r.B; L.chi2 = r.chi2;
         L.crlb_x_nm = r.cx; L.crlb_y_nm = r.cy; L.crlb_z_nm = r.cz;
+        L.candidate = r.seq;
     }
     *nout = (int)all.size();
     return ZOLA_OK;
