@@ -136,6 +136,20 @@ ZOLA_API int zola_fit_batch(zola_ctx* ctx, zola_psf* psf, int R, const float* ro
 ZOLA_API int zola_fit_batch_dev(zola_ctx* ctx, zola_psf* psf, int R, const float* d_rois, const double* d_init5,
                        int n, const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll,
                        int* d_status, int* d_iters, void* stream);
+/* Streaming form of zola_fit_batch_dev for a producer that writes ROIs into
+ * d_rois while the fit runs (replaces the detection -> localization hand-off of
+ * LocalizationPipeline_'s producer and consumer threads,
+ * process/gpu/LocalizationPipeline_.java:164-441): ROIs [0, *d_avail) are on
+ * the device, and the producer raises the device int *d_avail (never lowers
+ * it, up to n) as it writes more, with its writes made visible before the count
+ * (e.g. a stream-ordered copy, or a release store).  Split precision; runs the
+ * dataflow kernel.  If the count stops short of n, the call ends with
+ * ZOLA_E_TIMEOUT once no ROI has arrived for the wait limit
+ * (zola_ctx_set_wait_limit); every ROI below the count is fitted by then. */
+ZOLA_API int zola_fit_batch_stream_dev(zola_ctx* ctx, zola_psf* psf, int R, const float* d_rois,
+                                       const double* d_init5, const int* d_avail, int n, const zola_fit_params* prm,
+                                       double* d_out5, double* d_crlb5, double* d_nll, int* d_status, int* d_iters,
+                                       void* stream);
 
 /* sCMOS form (process/cpu/Localization.java:1132, utils/SCMOScamera.java):
  * scmos holds, per ROI pixel, var/gain^2 of the camera pixel; it is added to
@@ -187,6 +201,7 @@ typedef struct {
     double chi2;                    /* scoreCompute: mean (patch - model)^2 / model */
     double crlb_x_nm, crlb_y_nm, crlb_z_nm;
     int candidate;                  /* index of the row's candidate in its frame's sorted candidate list */
+    int fit_status;                 /* the fit's status: 1 converged, 2 evaluation cap, 3 stalled */
 } zola_localization;
 
 typedef struct {
@@ -326,14 +341,40 @@ ZOLA_API int zola_fit_batch_noalloc(zola_psf* psf, int R, const float* d_rois, c
  * (pool state up to 8 GB, at most 32768 slots).  Larger pools amortise each
  * launch's fixed work and shorten the draining tail of a batch. */
 ZOLA_API int zola_ctx_set_pool(zola_ctx* ctx, int max_slots);
-/* Split fit kernel layout: ZOLA_SPLIT_STAGED (default) runs the five stages
- * as separate kernels through global memory; ZOLA_SPLIT_FUSED runs stage 1
- * plus one kernel for stages 2-5 per LM round (same arithmetic, FP32 sums in
- * another order).  Windows whose fused plan does not fit in shared memory
- * always run staged. */
+/* Split fit kernel layout.  ZOLA_SPLIT_FLOW (default) runs the whole fit as
+ * one cooperative kernel: the four stages (pupil DFT, window DFT, row blur,
+ * column blur + likelihood sums + LM step) run at once on their own SMs and
+ * each unit of slots moves to the next stage as soon as it is done, with no
+ * host round trip.  ZOLA_SPLIT_STAGED runs the same stage code as four
+ * kernels per LM round over the whole slot pool (the same results bit for
+ * bit).  ZOLA_SPLIT_FUSED runs stage 1 plus one kernel for stages 2-5 per
+ * round (same arithmetic, FP32 sums in another order); windows whose fused
+ * plan does not fit in shared memory run staged. */
 #define ZOLA_SPLIT_STAGED 0
 #define ZOLA_SPLIT_FUSED 1
+#define ZOLA_SPLIT_FLOW 2
 ZOLA_API int zola_ctx_set_split_mode(zola_ctx* ctx, int mode);
+/* Dataflow kernel shape: units = units of slots in flight (0: two per SM),
+ * ctas[4] = CTAs per stage (all 0: a split by window size; otherwise they must
+ * add up to the SM count).  Results do not depend on either. */
+ZOLA_API int zola_ctx_set_flow(zola_ctx* ctx, int units, const int* ctas);
+/* Autotuner of the dataflow kernel (enable = 1): the first large fits of each
+ * class (pupil grid, ROI side) try a few shapes (CTAs per stage rebalanced
+ * from each stage's measured busy time; 1.5, 2 and 3 units per SM) and keep the
+ * fastest in device time per model evaluation.  Tuned shapes are read from and
+ * written to cache_path (JSON, nullable).  A fit's results do not depend on the
+ * shape, so tuning changes timings only. */
+ZOLA_API int zola_ctx_set_tuning(zola_ctx* ctx, int enable, const char* cache_path);
+/* Shape the dataflow kernel uses for psf's fits of R x R ROIs: units, ctas[4]
+ * and, when tuned, the measured ns per model evaluation (nullable pointers).
+ * Returns 1 when tuned, 0 for the default shape, < 0 on error. */
+ZOLA_API int zola_fit_flow_shape(zola_psf* psf, int R, int* units, int* ctas, double* ns_per_eval);
+/* Upper bound, in GPU clocks, on any single device-side wait of the split fit
+ * (a bulk copy or MMA completion, or the dataflow kernel waiting for a unit to
+ * become ready, e.g. for inputs to arrive); 0 restores the default (2^31, about
+ * a second).  A wait that runs out ends the call with ZOLA_E_TIMEOUT and leaves
+ * the context usable. */
+ZOLA_API int zola_ctx_set_wait_limit(zola_ctx* ctx, long long clocks);
 
 /* ---- CRLB curves and the z-centre search ------------------------------- */
 /* Cramer-Rao bounds (x, y, z, A, B) of an emitter at (0, 0, z[i]) (um), zoil =
@@ -360,10 +401,12 @@ ZOLA_API int zola_psf_center_search(zola_psf* psf, int R, double axial_range, in
 
 /* Per-kernel timing.  With profiling on, every kernel launch of a fit or model
  * call is bracketed by CUDA events on its stream and the elapsed device time is
- * accumulated per kernel kind: 0..4 the split stages 1..5, 5 the FP64 fit,
- * 6 the FP64 model, 7 other.  zola_ctx_stage_stats copies ZOLA_NSTAGES
+ * accumulated per kernel kind: 0..3 the split stages (pupil DFT, window DFT,
+ * row blur, column blur with likelihood sums and LM step; the model-only
+ * column blur), 4 the fused stages 2-5, 5 the FP64 fit, 6 the FP64 model, 7
+ * other, 8 the dataflow split fit.  zola_ctx_stage_stats copies ZOLA_NSTAGES
  * millisecond totals and launch counts (either pointer may be null). */
-#define ZOLA_NSTAGES 8
+#define ZOLA_NSTAGES 9
 ZOLA_API int zola_ctx_profile(zola_ctx* ctx, int enable);
 ZOLA_API int zola_ctx_stage_stats(zola_ctx* ctx, double* ms, long long* launches, int reset);
 

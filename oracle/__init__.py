@@ -245,9 +245,9 @@ class OracleDetector:
                            tol_xyz=1e-4, threads=1, cap=100000):
         """The same frame loop with the FP64 LM fit of the library (the oracle of
         zola_localize_frames).  Rows: frame, x_nm, y_nm, z_nm, A, B, chi2, crlbx,
-        crlby, crlbz, candidate index."""
+        crlby, crlbz, candidate index, LM status (1 converged, 2 evaluation cap, 3 stalled)."""
         frames = _f64(frames)
-        rows = np.zeros((cap, 11))
+        rows = np.zeros((cap, 12))
         n = lib().orc_localize_frames_lm(self.h, fit_psf.h, frames.shape[0], _p(frames), minZ, maxZ, photon_thr,
                                          max_snr, max_iter, tol_xyz, cap, _p(rows), threads)
         return rows[:min(n, cap)]

@@ -1025,13 +1025,14 @@ namespace {
 // lmp (nullable): fit each candidate with the FP64 LM (lm_fit, the oracle of
 // the library's own fit) instead of the reference coordinate descent, on the
 // patch rounded to float as the library stages it; a fit is then used unless
-// its model went non-positive.  Rows hold ncol values: 10, or 11 with the
-// candidate's index in its frame's sorted candidate list last.
+// its model went non-positive.  Rows hold ncol values: 10, or 12 with the
+// candidate's index in its frame's sorted candidate list and the LM status
+// (1 converged, 2 evaluation cap, 3 stalled) last.
 int localize_frames_impl(Detector* D, const Psf* p, int nframes, const double* det_frames, const double* fit_frames,
                          const double* vmap, double minZ, double maxZ, double photonThr, double maxSNR, int rows_cap,
                          double* rows, int threads, const LMParams* lmp = nullptr, int ncol = 10) {
     const int SX = D->SX, SY = D->SY, R = D->R, h = R / 2;
-    std::vector<std::vector<std::array<double, 11>>> per(nframes);
+    std::vector<std::vector<std::array<double, 12>>> per(nframes);
     parallel_for(nframes, threads, [&](int f) {
         const double* img = fit_frames + (size_t)f * SX * SY;
         std::vector<std::array<double, 7>> v;
@@ -1073,7 +1074,7 @@ int localize_frames_impl(Detector* D, const Psf* p, int nframes, const double* d
                 cd.maxShift = p->dx / 2.;
                 cd.psi.resize(R * R); cd.mu.resize(R * R);
                 cd.ta = A; cd.tb = B; cd.tx = -v[sel][5]; cd.ty = -v[sel][6]; cd.tz = D->range[r] + v[sel][4];
-                int st;
+                int st, lm_status = 0;
                 if (lmp) {
                     std::vector<double> pf((size_t)R * R), vf;
                     for (int k = 0; k < R * R; ++k) pf[k] = (double)(float)patch[k];
@@ -1084,7 +1085,8 @@ int localize_frames_impl(Detector* D, const Psf* p, int nframes, const double* d
                     const double init[5] = {cd.tx, cd.ty, cd.tz, cd.ta, cd.tb};
                     double o[5], nll;
                     int ev;
-                    st = lm_fit(p, R, pf.data(), init, *lmp, o, &nll, &ev, nullptr, vmap ? vf.data() : nullptr) != -1;
+                    lm_status = lm_fit(p, R, pf.data(), init, *lmp, o, &nll, &ev, nullptr, vmap ? vf.data() : nullptr);
+                    st = lm_status != -1;
                     cd.tx = o[0]; cd.ty = o[1]; cd.tz = o[2]; cd.ta = o[3]; cd.tb = o[4];
                 } else {
                     st = cd.run();
@@ -1107,7 +1109,7 @@ int localize_frames_impl(Detector* D, const Psf* p, int nframes, const double* d
                             fisher_crlb_fd(p, R, cd.tx, cd.ty, cd.tz, cd.ta, cd.tb, cr);
                             per[f].push_back({(double)f, 1000 * (ci * p->dx - cd.tx), 1000 * (cj * p->dx - cd.ty), 1000 * cd.tz,
                                               cd.ta, cd.tb, chi, 1000 * cr[0], 1000 * cr[1], 1000 * cr[2],
-                                              (double)sel});
+                                              (double)sel, (double)lm_status});
                             for (int a = 0; a < R; ++a)
                                 for (int b = 0; b < R; ++b)
                                     if (psi[(size_t)a * R + b] * cd.ta + cd.tb + sv[(size_t)a * R + b] - cd.tb > mthr)
@@ -1147,14 +1149,14 @@ int orc_localize_frames(void* dh, void* ph, int nframes, const double* frames, d
 // library's fit (lm_fit): the oracle of zola_localize_frames.  params: max_iter
 // evaluations and tol_xyz (um); the fit box and step caps as the library sets
 // them (z in [minZ - 0.3, maxZ + 0.3], |x|, |y| <= 10 dx + 1e-3, steps dx and
-// 2 dx).  Rows of 11: the 10 columns above and the candidate index.
+// 2 dx).  Rows of 12: the 10 columns above, the candidate index and the LM status.
 int orc_localize_frames_lm(void* dh, void* ph, int nframes, const double* frames, double minZ, double maxZ,
                            double photonThr, double maxSNR, int max_iter, double tol_xyz, int rows_cap, double* rows,
                            int threads) {
     const Psf* p = (const Psf*)ph;
     const LMParams P{minZ - 0.3, maxZ + 0.3, 10 * p->dx + 1e-3, max_iter, tol_xyz, p->dx, 2 * p->dx};
     return localize_frames_impl((Detector*)dh, p, nframes, frames, frames, nullptr, minZ, maxZ, photonThr, maxSNR,
-                                rows_cap, rows, threads, &P, 11);
+                                rows_cap, rows, threads, &P, 12);
 }
 
 // sCMOS form (LocalizationPipeline.java:588-640): detection on

@@ -16,11 +16,12 @@ def test_java_double_format(zpkg):
 
 
 def test_csv_header_rows_and_flooring(zpkg, tmp_path):
-    dt = np.dtype([(c, np.int32 if c in ("id", "frame", "candidate") else np.float64) for c in zpkg.LOC_COLUMNS])
+    dt = np.dtype([(c, np.int32 if c in ("id", "frame", "candidate", "fit_status") else np.float64)
+                   for c in zpkg.LOC_COLUMNS])
     locs = np.zeros(2, dtype=dt)
-    # the last field (the candidate index) is not a CSV column
-    locs[0] = (0, 3, 1234.56789, -0.0004, 250.0, 2999.9999, 20.5, 1.02345, 5.5555, 6.0, 12.34567, 17)
-    locs[1] = (1, 4, 0.0, 0.0, -100.0, 100.0, 1.0, 0.5, 1.0, 1.0, 1.0, 2)
+    # the last two fields (candidate index, fit status) are not CSV columns
+    locs[0] = (0, 3, 1234.56789, -0.0004, 250.0, 2999.9999, 20.5, 1.02345, 5.5555, 6.0, 12.34567, 17, 1)
+    locs[1] = (1, 4, 0.0, 0.0, -100.0, 100.0, 1.0, 0.5, 1.0, 1.0, 1.0, 2, 2)
     path = str(tmp_path / "loc.csv")
     zpkg.write_csv(path, locs)
     lines = open(path).read().splitlines()

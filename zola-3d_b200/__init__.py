@@ -27,6 +27,7 @@ ZOLA_PREC_FP64 = 0
 ZOLA_PREC_SPLIT = 1
 ZOLA_SPLIT_STAGED = 0
 ZOLA_SPLIT_FUSED = 1
+ZOLA_SPLIT_FLOW = 2
 ZOLA_CENTER_CPU = 0
 ZOLA_CENTER_GPU = 1
 FIT_STATUS = {1: "converged", 2: "max_iter", 3: "stalled", -1: "nan"}
@@ -47,7 +48,7 @@ class Localization(ctypes.Structure):
     _fields_ = [("id", ctypes.c_int), ("frame", ctypes.c_int), ("x_nm", ctypes.c_double), ("y_nm", ctypes.c_double),
                 ("z_nm", ctypes.c_double), ("intensity", ctypes.c_double), ("background", ctypes.c_double),
                 ("chi2", ctypes.c_double), ("crlb_x_nm", ctypes.c_double), ("crlb_y_nm", ctypes.c_double),
-                ("crlb_z_nm", ctypes.c_double), ("candidate", ctypes.c_int)]
+                ("crlb_z_nm", ctypes.c_double), ("candidate", ctypes.c_int), ("fit_status", ctypes.c_int)]
 
 
 class LocParams(ctypes.Structure):
@@ -71,9 +72,11 @@ EXPORTS = ["zola_ctx_create", "zola_ctx_destroy", "zola_last_error", "zola_ctx_s
            "zola_localize_frames", "zola_write_csv", "zola_format_double_java", "zola_calib_forward",
            "zola_calib_backward", "zola_calib_fit", "zola_ctx_set_split_mode", "zola_crlb_curve",
            "zola_psf_center_search", "zola_calib_init", "zola_drift", "zola_fit_batch_scmos",
-           "zola_fit_batch_scmos_dev", "zola_localize_frames_scmos"]
-STAGES = ["split_stage1_pupil_dft", "split_stage2_window_dft", "split_stage3_blur_rows", "split_stage4_blur_cols",
-          "split_stage5_likelihood_lm", "fp64_fit", "fp64_model", "other"]
+           "zola_fit_batch_scmos_dev", "zola_localize_frames_scmos", "zola_ctx_set_flow", "zola_ctx_set_wait_limit",
+           "zola_fit_batch_stream_dev", "zola_ctx_set_tuning", "zola_fit_flow_shape"]
+STAGES = ["split_stage1_pupil_dft", "split_stage2_window_dft", "split_stage3_blur_rows",
+          "split_stage4_blur_cols_sums_lm", "split_fused_stages2_5", "fp64_fit", "fp64_model", "other",
+          "split_dataflow"]
 
 _lib = None
 
@@ -103,6 +106,10 @@ def lib():
         L.zola_psf_model_prec_dev.argtypes = [vp, i, vp, i, vp, vp, i, vp]
         L.zola_ctx_set_pool.argtypes = [vp, i]
         L.zola_ctx_set_split_mode.argtypes = [vp, i]
+        L.zola_ctx_set_flow.argtypes = [vp, i, vp]
+        L.zola_ctx_set_wait_limit.argtypes = [vp, ctypes.c_longlong]
+        L.zola_ctx_set_tuning.argtypes = [vp, i, ctypes.c_char_p]
+        L.zola_fit_flow_shape.argtypes = [vp, i, vp, vp, vp]
         L.zola_crlb_curve.argtypes = [vp, i, vp, i, d, d, d, d, vp]
         L.zola_psf_center_search.argtypes = [vp, i, d, i, ctypes.POINTER(d)]
         L.zola_ctx_profile.argtypes = [vp, i]
@@ -128,6 +135,8 @@ def lib():
         L.zola_ctx_stage_stats.argtypes = [vp, vp, vp, i]
         L.zola_fit_batch.argtypes = [vp, vp, i, vp, vp, i, ctypes.POINTER(FitParams), vp, vp, vp, vp, vp]
         L.zola_fit_batch_dev.argtypes = [vp, vp, i, vp, vp, i, ctypes.POINTER(FitParams), vp, vp, vp, vp, vp, vp]
+        L.zola_fit_batch_stream_dev.argtypes = [vp, vp, i, vp, vp, vp, i, ctypes.POINTER(FitParams), vp, vp, vp, vp, vp,
+                                                vp]
         _lib = L
     return _lib
 
@@ -166,9 +175,25 @@ class Context:
         self.check(lib().zola_ctx_set_pool(self.h, int(max_slots)), "zola_ctx_set_pool")
 
     def set_split_mode(self, mode):
-        """"staged" (default): five stage kernels per LM round; "fused": stage 1 + one kernel for stages 2-5."""
-        code = {"staged": ZOLA_SPLIT_STAGED, "fused": ZOLA_SPLIT_FUSED}[mode]
+        """"flow" (default): the whole split fit as one dataflow kernel; "staged": four stage kernels per
+        LM round (the same results bit for bit); "fused": stage 1 + one kernel for stages 2-5."""
+        code = {"staged": ZOLA_SPLIT_STAGED, "fused": ZOLA_SPLIT_FUSED, "flow": ZOLA_SPLIT_FLOW}[mode]
         self.check(lib().zola_ctx_set_split_mode(self.h, code), "zola_ctx_set_split_mode")
+
+    def set_flow(self, units=0, ctas=None):
+        """Dataflow kernel shape: units of slots in flight (0: automatic) and CTAs per stage (None:
+        automatic; else four counts adding up to the SM count).  Results do not depend on either."""
+        arr = None if ctas is None else (ctypes.c_int * 4)(*[int(c) for c in ctas])
+        self.check(lib().zola_ctx_set_flow(self.h, int(units), arr), "zola_ctx_set_flow")
+
+    def set_tuning(self, enable=True, cache_path=None):
+        """Autotune the dataflow kernel's shape per (pupil grid, ROI side) on large fits; cache_path: JSON cache."""
+        self.check(lib().zola_ctx_set_tuning(self.h, int(bool(enable)), cache_path.encode() if cache_path else None),
+                   "zola_ctx_set_tuning")
+
+    def set_wait_limit(self, clocks):
+        """Upper bound (GPU clocks) on any device-side wait of the split fit; 0 = default (2^31)."""
+        self.check(lib().zola_ctx_set_wait_limit(self.h, int(clocks)), "zola_ctx_set_wait_limit")
 
     def profile(self, enable=True):
         """Time every library kernel launch with CUDA events on its stream."""
@@ -297,6 +322,25 @@ class PSF:
         self.ctx.check(lib().zola_fit_batch_dev(self.ctx.h, self.h, R, _ptr(rois), _ptr(init), n, ctypes.byref(prm),
                                                 _ptr(out), _ptr(crlb), _ptr(nll), _ptr(status), _ptr(iters), stream),
                        "zola_fit_batch_dev")
+
+    def flow_shape(self, R):
+        """(tuned, units, [CTAs per stage], ns per evaluation) of the dataflow kernel for R x R ROIs."""
+        u = ctypes.c_int()
+        c = (ctypes.c_int * 4)()
+        ns = ctypes.c_double()
+        rc = lib().zola_fit_flow_shape(self.h, int(R), ctypes.byref(u), c, ctypes.byref(ns))
+        if rc < 0:
+            self.ctx.check(rc, "zola_fit_flow_shape")
+        return bool(rc), u.value, list(c), ns.value
+
+    def fit_stream_dev(self, rois, init, avail, prm, out, crlb=None, nll=None, status=None, iters=None, stream=None):
+        """Streaming device form (zola_fit_batch_stream_dev): avail is a one-element int32 CUDA tensor holding
+        how many leading ROIs of rois are already written; the producer raises it while the fit runs."""
+        n, R = rois.shape[0], rois.shape[1]
+        self.ctx.check(lib().zola_fit_batch_stream_dev(self.ctx.h, self.h, R, _ptr(rois), _ptr(init), _ptr(avail), n,
+                                                       ctypes.byref(prm), _ptr(out), _ptr(crlb), _ptr(nll),
+                                                       _ptr(status), _ptr(iters), stream),
+                       "zola_fit_batch_stream_dev")
 
     def crlb_curve(self, R, z, photons=3000.0, background=50.0, h=0.0005, a_step=0.0005):
         """CRLB (x, y, z, A, B) at (0, 0, z) for each depth, finite-difference
@@ -471,7 +515,7 @@ class Calibration:
 
 
 LOC_COLUMNS = ["id", "frame", "x_nm", "y_nm", "z_nm", "intensity", "background", "chi2", "crlb_x_nm", "crlb_y_nm",
-               "crlb_z_nm", "candidate"]
+               "crlb_z_nm", "candidate", "fit_status"]
 
 
 def localize_frames(ctx, det, fit_psf, frames, minZ, maxZ, photon_threshold=500.0, max_snr=1.0, max_iter=30,
@@ -488,7 +532,7 @@ def localize_frames(ctx, det, fit_psf, frames, minZ, maxZ, photon_threshold=500.
     ctx.check(lib().zola_localize_frames(ctx.h, det.h, fit_psf.h, _ptr(frames), nf, int(frame0), ctypes.byref(prm),
                                          ctypes.cast(out, ctypes.c_void_p), cap, ctypes.byref(n)),
               "zola_localize_frames")
-    dt = np.dtype([(c, np.int32 if c in ("id", "frame", "candidate") else np.float64) for c in LOC_COLUMNS])
+    dt = np.dtype([(c, np.int32 if c in ("id", "frame", "candidate", "fit_status") else np.float64) for c in LOC_COLUMNS])
     arr = np.zeros(n.value, dtype=dt)
     for k in range(n.value):
         arr[k] = tuple(getattr(out[k], c) for c in LOC_COLUMNS)
@@ -510,7 +554,7 @@ def localize_frames_scmos(ctx, det, fit_psf, adu, offset, gain, variance, minZ, 
                                                _ptr(maps[0]), _ptr(maps[1]), _ptr(maps[2]),
                                                ctypes.cast(out, ctypes.c_void_p), cap, ctypes.byref(n)),
               "zola_localize_frames_scmos")
-    dt = np.dtype([(c, np.int32 if c in ("id", "frame", "candidate") else np.float64) for c in LOC_COLUMNS])
+    dt = np.dtype([(c, np.int32 if c in ("id", "frame", "candidate", "fit_status") else np.float64) for c in LOC_COLUMNS])
     arr = np.zeros(n.value, dtype=dt)
     for k in range(n.value):
         arr[k] = tuple(getattr(out[k], c) for c in LOC_COLUMNS)

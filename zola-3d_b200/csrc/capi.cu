@@ -130,6 +130,7 @@ int zola_ctx_create(int device, zola_ctx** out) {
     // the host-buffer calls and stays non-blocking.
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamDefault) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->feed_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&c->d_counter, 64 * sizeof(int)) != cudaSuccess) {
         delete c;
         return ZOLA_E_CUDA;
@@ -148,6 +149,13 @@ int zola_ctx_destroy(zola_ctx* ctx) {
     if (ctx->io) cudaFree(ctx->io);
     if (ctx->d_counter) cudaFree(ctx->d_counter);
     if (ctx->h_flags) cudaFreeHost(ctx->h_flags);
+    if (ctx->h_feed) cudaFreeHost(ctx->h_feed);
+    if (ctx->h_tune) cudaFreeHost(ctx->h_tune);
+    for (cudaEvent_t e : ctx->tune_ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->ev_init) cudaEventDestroy(ctx->ev_init);
+    cudaStreamSynchronize(ctx->feed_stream);
+    cudaStreamDestroy(ctx->feed_stream);
     for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : ctx->feed_ev) cudaEventDestroy(e);
     cudaStreamSynchronize(ctx->copy_stream);
@@ -282,8 +290,52 @@ int zola_ctx_set_pool(zola_ctx* ctx, int max_slots) {
 }
 
 int zola_ctx_set_split_mode(zola_ctx* ctx, int mode) {
-    if (!ctx || (mode != ZOLA_SPLIT_STAGED && mode != ZOLA_SPLIT_FUSED)) return ZOLA_E_ARG;
-    ctx->split_fused = mode == ZOLA_SPLIT_FUSED;
+    if (!ctx || (mode != ZOLA_SPLIT_STAGED && mode != ZOLA_SPLIT_FUSED && mode != ZOLA_SPLIT_FLOW)) return ZOLA_E_ARG;
+    ctx->split_mode = mode;
+    return ZOLA_OK;
+}
+
+int zola_ctx_set_flow(zola_ctx* ctx, int units, const int* ctas) {
+    if (!ctx || units < 0) return ZOLA_E_ARG;
+    int sum = 0;
+    if (ctas) {
+        for (int s = 0; s < 4; ++s) {
+            if (ctas[s] < 0 || (ctas[s] == 0 && (ctas[0] | ctas[1] | ctas[2] | ctas[3]) != 0))
+                return set_err(ctx, ZOLA_E_ARG, "zola_ctx_set_flow: every stage needs at least one CTA");
+            sum += ctas[s];
+        }
+        if (sum != 0 && sum != ctx->num_sms)
+            return set_err(ctx, ZOLA_E_ARG, "zola_ctx_set_flow: the CTAs per stage must add up to the SM count");
+    }
+    ctx->flow_units = units;
+    for (int s = 0; s < 4; ++s) ctx->flow_ctas[s] = ctas ? ctas[s] : 0;
+    return ZOLA_OK;
+}
+
+int zola_ctx_set_tuning(zola_ctx* ctx, int enable, const char* cache_path) {
+    if (!ctx) return ZOLA_E_ARG;
+    ctx->tune = enable ? 1 : 0;
+    ctx->tune_path = cache_path ? cache_path : "";
+    tune_load(ctx);
+    return ZOLA_OK;
+}
+
+int zola_fit_flow_shape(zola_psf* psf, int R, int* units, int* ctas, double* ns_per_eval) {
+    if (!psf) return ZOLA_E_ARG;
+    zola_ctx* ctx = psf->ctx;
+    WindowTables* w = get_window(psf, R, ctx->err);
+    if (!w) return ZOLA_E_ARG;
+    FlowShape f;
+    const bool tuned = flow_shape(ctx, psf, w, &f, ns_per_eval);
+    if (units) *units = f.units;
+    if (ctas)
+        for (int s = 0; s < 4; ++s) ctas[s] = f.ctas[s];
+    return tuned ? 1 : 0;
+}
+
+int zola_ctx_set_wait_limit(zola_ctx* ctx, long long clocks) {
+    if (!ctx || clocks < 0) return ZOLA_E_ARG;
+    ctx->wait_limit = clocks;
     return ZOLA_OK;
 }
 
@@ -293,7 +345,8 @@ namespace {
 
 int fit_dev_impl(zola_ctx* ctx, zola_psf* psf, int R, const float* d_rois, const float* d_scmos,
                  const double* d_init5, int n, const zola_fit_params* prm, double* d_out5, double* d_crlb5,
-                 double* d_nll, int* d_status, int* d_iters, void* stream, const zola::RoiFeed* feed = nullptr) {
+                 double* d_nll, int* d_status, int* d_iters, void* stream, const zola::RoiFeed* feed = nullptr,
+                 const int* d_avail = nullptr) {
     if (!ctx || !psf) return ZOLA_E_ARG;
     if (psf->ctx != ctx) return set_err(ctx, ZOLA_E_ARG, "psf belongs to another context");
     if (!check_fit_params(ctx, prm)) return ZOLA_E_ARG;
@@ -303,9 +356,11 @@ int fit_dev_impl(zola_ctx* ctx, zola_psf* psf, int R, const float* d_rois, const
     if (!w) return ZOLA_E_ARG;
     if (n == 0) return ZOLA_OK;
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    if (d_avail && prm->precision != ZOLA_PREC_SPLIT)
+        return set_err(ctx, ZOLA_E_ARG, "zola_fit_batch_stream_dev: streaming inputs need split precision");
     if (prm->precision == ZOLA_PREC_SPLIT)
         return launch_fit_split(ctx, psf, w, d_rois, d_scmos, d_init5, n, prm, d_out5, d_crlb5, d_nll, d_status, d_iters,
-                                st, feed);
+                                st, feed, d_avail);
     if (feed && feed->n_chunks > 0)  // the FP64 form needs every input before it starts
         ZOLA_CUDA_CHECK(cudaStreamWaitEvent(st, feed->ev[feed->n_chunks - 1], 0), ctx);
     return launch_fit_f64(ctx, psf, w, d_rois, d_scmos, d_init5, n, prm, d_out5, d_crlb5, d_nll, d_status, d_iters, st);
@@ -387,6 +442,14 @@ int zola_fit_batch_dev(zola_ctx* ctx, zola_psf* psf, int R, const float* d_rois,
                        const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll, int* d_status,
                        int* d_iters, void* stream) {
     return fit_dev_impl(ctx, psf, R, d_rois, nullptr, d_init5, n, prm, d_out5, d_crlb5, d_nll, d_status, d_iters, stream);
+}
+
+int zola_fit_batch_stream_dev(zola_ctx* ctx, zola_psf* psf, int R, const float* d_rois, const double* d_init5,
+                              const int* d_avail, int n, const zola_fit_params* prm, double* d_out5, double* d_crlb5,
+                              double* d_nll, int* d_status, int* d_iters, void* stream) {
+    if (ctx && n > 0 && !d_avail) return set_err(ctx, ZOLA_E_ARG, "zola_fit_batch_stream_dev: null ROI count");
+    return fit_dev_impl(ctx, psf, R, d_rois, nullptr, d_init5, n, prm, d_out5, d_crlb5, d_nll, d_status, d_iters, stream,
+                        nullptr, d_avail);
 }
 
 int zola_fit_batch(zola_ctx* ctx, zola_psf* psf, int R, const float* rois, const double* init5, int n,

@@ -13,7 +13,8 @@
 //   stage 5  likelihood, gradient, Gauss-Newton Hessian and Fisher sums in
 //            FP32 with Kahan compensation, then the FP64 5x5 LM solve, damping
 //            and convergence test; converged slots are retired and refilled
-//            from the ROI queue (a device counter).
+//            from the ROI queue (a device counter).  Stages 4 and 5 run in one
+//            kernel.
 //
 // C is the W x D partial-DFT matrix, CK = C diag(i k) its x/y derivative, Q the
 // pupil field (built from the pupil tables and the slot's trial x, y, z), G
@@ -26,18 +27,28 @@
 // rounding moves the optimum by about 2^-11 x CRLB (~0.01 nm), far below the
 // 0.5 nm budget.
 //
-// Stages 1 and 2 are persistent kernels that keep the DFT constants in shared
-// memory and issue N = 256 MMAs; for large ROIs stages 4 and 5 run as one
-// persistent kernel plus an LM kernel.  All operands use the canonical
-// no-swizzle layouts of umma.h.  Intermediate operands travel through global
-// slabs laid out as the shared-memory tiles (or K-slabs of them), fetched with
-// 1-D bulk (TMA) copies.  Scales are powers of two chosen from host-side
-// bounds so no FP16 value overflows; they are exact and undone in FP32.
+// Every stage is a persistent body that walks "units" of slots (whole stage-1
+// and window tiles).  ZOLA_SPLIT_STAGED launches the four bodies (pupil DFT,
+// window DFT, row blur, column blur + sums + LM step) as four kernels per LM
+// round over the whole pool.  ZOLA_SPLIT_FLOW launches them once, together, as
+// one cooperative kernel (k_flow): each stage runs on its own CTAs, a unit
+// moves to the next stage as soon as it is done (a state word per unit, one
+// scheduler thread per CTA), its operands pass between stages through global
+// memory while they are still in L2, and converged fits retire and refill from
+// the ROI queue on the device.  Stages 1 and 2 keep the DFT constants in shared
+// memory and issue N = 256 MMAs.  All operands use the canonical no-swizzle
+// layouts of umma.h.  Intermediate operands travel through global slabs laid
+// out as the shared-memory tiles (or K-slabs of them), fetched with 1-D bulk
+// (TMA) copies.  Scales are powers of two chosen from host-side bounds so no
+// FP16 value overflows; they are exact and undone in FP32.
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
+#include <string>
 
 #include "lm.h"
 #include "umma.h"
@@ -52,7 +63,6 @@ using umma::mnmajor_off;
 // quadrant = warp % 4, so thread t owns tile row t % 128) and split the column
 // work of every epilogue and of the Q build; the LM step runs one thread per slot.
 constexpr int SPLIT_THREADS = 512;
-constexpr int LM_THREADS = 32;  // one warp per block: the FP64 LM step of 4096 slots spreads over 128 SMs
 
 // ---------------------------------------------------------------- plan ------
 struct SplitScales {
@@ -98,6 +108,10 @@ struct SplitDev {
     int* active;   // occupied slots
     int* err;      // bounded-wait timeout flag
     int* navail;   // ROIs [0, *navail) are on the device (all n unless the inputs are still arriving)
+    int* ustate;   // per unit of slots: 4 e + s (ready for stage s of evaluation e), or UNIT_DEAD
+    long long wait_limit;  // clocks a dataflow scheduler waits for a ready unit before it gives up
+    unsigned long long* evals;  // dataflow kernel: model evaluations (LM steps) done
+    unsigned long long* clk;    // dataflow kernel: per CTA, clocks without a ready unit and clocks in all
     SplitScales sc;
 };
 
@@ -510,6 +524,218 @@ __device__ __forceinline__ void warp_arrive(uint64_t* mbar) {
     if ((threadIdx.x & 31) == 0) umma::mbar_arrive(mbar);
 }
 
+// ------------------------------------------------------------- work units ----
+// The persistent stage kernels work in units of UG = max(G1, G2) consecutive
+// slots, so that a unit is made of whole pupil-DFT tiles (G1 slots) and whole
+// window tiles (G2 slots).  The round-based kernels walk the units statically
+// (blockIdx.x, + gridDim.x, ...).  The dataflow kernel (k_flow) runs all four
+// stages at once, each on its own CTAs: a unit's state word counts its
+// finished stages (4 e + s: ready for stage s of its evaluation e; UNIT_DEAD
+// once its slots have retired and the ROI queue is empty), and in every CTA one
+// scheduler thread hands the units of its share that are ready for its stage to
+// the CTA's warps through a ring in shared memory.
+constexpr int UNIT_DEAD = -1;
+// Set in a unit's state word by the scheduler that handed it out, until the
+// stage releases it: a unit is never handed out twice at once.
+constexpr int UNIT_CLAIMED = 1 << 30;
+constexpr int URING = 4;
+
+__host__ __device__ inline int unit_slots(int G1, int G2) { return G1 > G2 ? G1 : G2; }
+
+// The ROIs, start points and outputs of a fit.
+struct FitIO {
+    const float* rois;
+    const float* scmos;  // sCMOS var/gain^2 per pixel (Localization.java:1132), or null
+    const double* init;
+    int n;
+    FitParamsDev prm;
+    double* out5;
+    double* crlb5;
+    double* nll;
+    int* status;
+    int* iters;
+};
+
+__device__ __forceinline__ void st_release(int* p, int v) {
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ int ld_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Slot s takes ROI r: fresh LM state at the ROI's (clamped) start point.
+__device__ __forceinline__ void slot_take(const SplitDev& P, const FitIO& F, int s, int r) {
+    P.slot_roi[s] = r;
+    P.slot_phase[s] = 0;
+    double* tr = P.lm[s].trial;
+    for (int q = 0; q < 5; ++q) tr[q] = F.init[5 * r + q];
+    lm_clamp(tr, F.prm);
+}
+
+// Stage 1's scheduler prepares unit u: its idle slots take ROIs that have
+// arrived.  1: the unit has a live slot; 0: not yet (inputs still arriving);
+// -1: none and the queue is exhausted (the unit is marked dead).
+__device__ int unit_refill(const SplitDev& P, const FitIO& F, int u) {
+    const int UG = unit_slots(P.G1, P.G2);
+    bool live = false;
+    for (int g = 0; g < UG; ++g) {
+        const int s = u * UG + g;
+        if (P.slot_roi[s] < 0 && *(volatile int*)P.queue < F.n) {
+            const int r = take_roi(P, F.n);
+            if (r >= 0) {
+                slot_take(P, F, s, r);
+                atomicAdd(P.active, 1);
+            }
+        }
+        live |= P.slot_roi[s] >= 0;
+    }
+    if (live) return 1;
+    if (*(volatile int*)P.queue >= F.n) {
+        st_release(P.ustate + u, UNIT_DEAD);
+        return -1;
+    }
+    return 0;
+}
+
+// State word of unit u after its LM step: its next evaluation, or dead when
+// no slot holds a ROI and the queue is exhausted.
+__device__ int unit_after_lm(const SplitDev& P, const FitIO& F, int u, int tag) {
+    const int UG = unit_slots(P.G1, P.G2);
+    bool live = false;
+    for (int g = 0; g < UG; ++g) live |= P.slot_roi[u * UG + g] >= 0;
+    if (!live && *(volatile int*)P.queue >= F.n) return UNIT_DEAD;
+    return tag + 1;
+}
+
+struct StaticUnits {
+    static constexpr bool flow = false;
+    int u = -1;
+    // The next unit with a live slot, or -1.  Every calling thread walks the
+    // same sequence.
+    __device__ int next(const SplitDev& P, int& tag, bool = false) {
+        const int UG = unit_slots(P.G1, P.G2), U = P.P / UG;
+        for (u = u < 0 ? (int)blockIdx.x : u + (int)gridDim.x; u < U; u += gridDim.x)
+            if (tile_live(P, u * UG, UG)) {
+                tag = 0;
+                return u;
+            }
+        return -1;
+    }
+    __device__ void fence_writes() {}
+    __device__ void release(const SplitDev&, int, int) {}
+    __device__ void schedule(const SplitDev&, const FitIO&) {}
+};
+
+struct UnitRing {
+    int unit[URING], tag[URING];
+    uint64_t full[URING], freed[URING];
+};
+
+struct FlowUnits {
+    static constexpr bool flow = true;
+    UnitRing* r;
+    int stage, first, stride;  // this CTA serves units first, first + stride, ... at stage `stage`
+    int q;
+    // The next unit handed out, or -1 when there is none left (or a wait gave
+    // up).  Called by every lane of a warp, or by one lane (single); each
+    // caller group arrives once on the ring entry.
+    __device__ int next(const SplitDev& P, int& tag, bool single = false) {
+        const int b = q % URING;
+        const uint32_t par = (uint32_t)((q / URING) & 1);
+        ++q;
+        int u = -1;
+        if (umma::mbar_wait(&r->full[b], par, P.err)) {
+            u = r->unit[b];
+            tag = r->tag[b];
+        }
+        if (single) {
+            umma::mbar_arrive(&r->freed[b]);
+        } else {
+            __syncwarp();
+            if ((threadIdx.x & 31) == 0) umma::mbar_arrive(&r->freed[b]);
+        }
+        // the unit's operands, written by other CTAs, are seen by this CTA's loads and bulk copies
+        asm volatile("fence.acq_rel.gpu;" ::: "memory");
+        asm volatile("fence.proxy.async.global;" ::: "memory");
+        return u;
+    }
+    // Every thread that wrote a unit's operands: its generic-proxy writes are
+    // made visible to the next stage's bulk (async-proxy) copies.
+    __device__ void fence_writes() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+    // One thread, once every writer of the unit has passed a barrier behind
+    // fence_writes: publish the unit's next state.
+    __device__ void release(const SplitDev& P, int u, int v) {
+        __threadfence();
+        st_release(P.ustate + u, v);
+    }
+    // The scheduler thread: scan this CTA's units round-robin and hand out
+    // those ready for its stage; stage 1's scheduler refills idle slots first.
+    // Ends (handing out -1) when all its units are dead, when an error was
+    // raised, or after P.wait_limit clocks without a ready unit (then it
+    // raises the error word: 2).
+    __device__ void schedule(const SplitDev& P, const FitIO& F) {
+        const int UG = unit_slots(P.G1, P.G2), U = P.P / UG;
+        const int mine = first < U ? (U - first + stride - 1) / stride : 0;
+        int qq = 0, cur = 0;
+        auto push = [&](int u, int tag) {
+            const int b = qq % URING;
+            if (qq >= URING && !umma::mbar_wait(&r->freed[b], (uint32_t)(((qq / URING) - 1) & 1), P.err)) return false;
+            r->unit[b] = u;
+            r->tag[b] = tag;
+            umma::mbar_arrive(&r->full[b]);
+            ++qq;
+            return true;
+        };
+        const long long start = clock64();
+        long long t0 = start, idle = 0, idle_since = -1;
+        while (*(volatile int*)P.err == 0) {
+            int found = -1, tag = 0, dead = 0;
+            for (int k = 0; k < mine; ++k) {
+                const int i = cur + k < mine ? cur + k : cur + k - mine;
+                const int u = first + i * stride;
+                const int v = ld_acquire(P.ustate + u);
+                if (v < 0) {
+                    ++dead;
+                    continue;
+                }
+                if ((v & 3) != stage || (v & UNIT_CLAIMED)) continue;
+                if (stage == 0) {
+                    const int ok = unit_refill(P, F, u);
+                    if (ok < 0) ++dead;
+                    if (ok <= 0) continue;
+                }
+                found = u;
+                tag = v;
+                cur = i + 1 < mine ? i + 1 : 0;
+                break;
+            }
+            if (found >= 0) {
+                if (idle_since >= 0) idle += clock64() - idle_since;
+                idle_since = -1;
+                P.ustate[found] = tag | UNIT_CLAIMED;  // only this thread reads the claim
+                if (!push(found, tag)) break;
+                t0 = clock64();
+                continue;
+            }
+            if (dead == mine) break;
+            if (idle_since < 0) idle_since = clock64();
+            if (clock64() - t0 > P.wait_limit) {
+                atomicExch(P.err, 2);
+                break;
+            }
+            __nanosleep(100);
+        }
+        push(-1, 0);
+        const long long end = clock64();
+        if (idle_since >= 0) idle += end - idle_since;
+        P.clk[2 * blockIdx.x] = (unsigned long long)idle;
+        P.clk[2 * blockIdx.x + 1] = (unsigned long long)(end - start);
+    }
+};
+
+
 // ------------------------------------------------- stage 1 (persistent) -----
 // One CTA per SM walks the stage-1 tiles (G1 slots x DP pupil rows a) with the
 // DFT constants resident in shared memory (the K-slabs the window stage uses).
@@ -527,8 +753,8 @@ constexpr int S1_QB = 128 * 32;  // one Q array for one K step: 128 rows x 16 k,
 
 __host__ __device__ constexpr int s1_qring_bytes(int W) { return (W > 64 ? 2 : 3) * S1_QB; }
 
-template <int W>
-__global__ void __launch_bounds__(S1_THREADS, 1) k_stage1p(SplitDev P, int ntiles) {
+template <int W, class UNITS>
+__device__ __forceinline__ void stage1_body(const SplitDev& P, const FitIO& F, UNITS units) {
     extern __shared__ __align__(1024) char smem[];
     constexpr bool TWO = W > 64;
     constexpr int SLAB = s2_slab_bytes(W), QRING = s1_qring_bytes(W), NBQ = S1_NBQ, QB = S1_QB;
@@ -537,11 +763,11 @@ __global__ void __launch_bounds__(S1_THREADS, 1) k_stage1p(SplitDev P, int ntile
     // W = 128 comes with K1 = 128 (64 pupil rows): 8 K steps, known here so that the
     // Q_z values of pass A stay in registers for pass B
     const int NS = TWO ? 8 : K1 / 16;
+    const int T1 = unit_slots(G1, P.G2) / G1;  // stage-1 tiles per unit
     char* CS = smem;               // NS constant K-slabs
     char* QR = smem + NS * SLAB;   // ring of Q K-slabs
     __shared__ __align__(8) uint64_t cfull, qfull[NBQ], qfree[NBQ], accA, accB, tfree, fin;
     __shared__ uint32_t tmem_base;
-    if (!cta_has_live_tile(P, ntiles, G1)) return;
     if (t < 32) umma::tmem_alloc(&tmem_base, NCOLS);
     if (t == 0) {
         umma::mbar_init(&cfull, 1);
@@ -561,7 +787,12 @@ __global__ void __launch_bounds__(S1_THREADS, 1) k_stage1p(SplitDev P, int ntile
             umma::bulk_g2s(CS + s * SLAB, (const char*)P.bcs + (size_t)s * SLAB, SLAB, &cfull);
     }
 
-    if (warp == SPLIT_THREADS / 32) {  // ---------------- MMA issuer
+    if (warp == SPLIT_THREADS / 32) {  // ---------------- MMA issuer (lane 0), scheduler (lane 1)
+        if constexpr (UNITS::flow)
+            if (lane == 1) {
+                units.schedule(P, F);
+                return;
+            }
         if (lane != 0) return;
         bool ok = umma::mbar_wait(&cfull, 0, P.err);
         int q = 0, nwait = 0, nphase = 0;
@@ -596,13 +827,18 @@ __global__ void __launch_bounds__(S1_THREADS, 1) k_stage1p(SplitDev P, int ntile
             }
             return true;
         };
-        for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-            if (!tile_live(P, tile * G1, G1)) continue;
-            ok = tmem_ready() && steps(false);
-            umma::mma_commit(&accA);
-            if (TWO && ok) {
-                ok = tmem_ready() && steps(true);
-                umma::mma_commit(&accB);
+        for (int tag = 0; ok;) {
+            const int unit = units.next(P, tag, true);
+            if (unit < 0) break;
+            for (int k = 0; k < T1 && ok; ++k) {
+                const int tile = unit * T1 + k;
+                if (!tile_live(P, tile * G1, G1)) continue;
+                ok = tmem_ready() && steps(false);
+                umma::mma_commit(&accA);
+                if (TWO && ok) {
+                    ok = tmem_ready() && steps(true);
+                    umma::mma_commit(&accB);
+                }
             }
         }
         umma::mma_commit(&fin);
@@ -621,162 +857,169 @@ __global__ void __launch_bounds__(S1_THREADS, 1) k_stage1p(SplitDev P, int ntile
     constexpr int CW = W / 4;
     int q = 0, ntile = 0;
     bool abort = false;
-    for (int tile = blockIdx.x; tile < ntiles && !abort; tile += gridDim.x) {
-        if (!tile_live(P, tile * G1, G1)) continue;
-        const uint32_t ph = (uint32_t)(ntile & 1);
-        ++ntile;
-        const int bslot = tile * G1 + bg;
-        const bool blive = P.slot_roi[bslot] >= 0;
-        double x = 0, y = 0, z = 0;
-        if (blive) {
-            x = P.lm[bslot].trial[0]; y = P.lm[bslot].trial[1]; z = P.lm[bslot].trial[2];
-        }
-        const double kxa = P.kx[ba];
-        // one K step of Q (columns b = 8 s + 2 bp + {0, 1} of row brow); the table loads of
-        // the next step are issued before this step's arithmetic
-        struct QTab { double2 p0, kz, ky; float2 pu; };
-        auto qtab = [&](int s) {
-            const size_t i2 = (((size_t)s * 4 + bp) * DP + ba) * 2;
-            const size_t i4 = (((size_t)s * 2 + (bp >> 1)) * DP + ba) * 4 + (bp & 1) * 2;
-            QTab q2;
-            q2.p0 = *(const double2*)(P.phase0 + i2);
-            q2.kz = *(const double2*)(P.kz + i2);
-            q2.pu = *(const float2*)(P.pupf + i4);
-            q2.ky = *(const double2*)(P.ky + 8 * s + 2 * bp);
-            return q2;
-        };
-        const uint32_t ore = kmajor_off(brow, 2 * bp, 16), oim = kmajor_off(brow, 8 + 2 * bp, 16);
-        auto slot_wait = [&]() {  // ring slot for the next K step
-            const int buf = q % NBQ;
-            if (q >= NBQ) umma::mbar_wait(&qfree[buf], (uint32_t)((q / NBQ - 1) & 1), P.err);
-            ++q;
-            return QR + buf * QRING;
-        };
-        auto slot_done = [&](char* qs) {  // every writer fences its stores; one arrive per warp
-            umma::fence_proxy_async();
-            warp_arrive(&qfull[(qs - QR) / QRING]);
-        };
-        uint32_t zkeep[TWO ? 8 : 1][2] = {};  // pass A's Q_z of each K step (W = 128)
-        auto build = [&](int s, const QTab& tb, uint32_t& zr, uint32_t& zi) {
-            const double ph0[2] = {tb.p0.x, tb.p0.y}, kzr[2] = {tb.kz.x, tb.kz.y}, kyr[2] = {tb.ky.x, tb.ky.y};
-            const float pu[2] = {tb.pu.x, tb.pu.y};
-            float qr[2], qi[2], kzv[2];
+    for (int tag = 0; !abort;) {
+        const int unit = units.next(P, tag);
+        if (unit < 0) break;
+        for (int k = 0; k < T1 && !abort; ++k) {
+            const int tile = unit * T1 + k;
+            if (!tile_live(P, tile * G1, G1)) continue;
+            const uint32_t ph = (uint32_t)(ntile & 1);
+            ++ntile;
+            const int bslot = tile * G1 + bg;
+            const bool blive = P.slot_roi[bslot] >= 0;
+            double x = 0, y = 0, z = 0;
+            if (blive) {
+                x = P.lm[bslot].trial[0]; y = P.lm[bslot].trial[1]; z = P.lm[bslot].trial[2];
+            }
+            const double kxa = P.kx[ba];
+            // one K step of Q (columns b = 8 s + 2 bp + {0, 1} of row brow); the table loads of
+            // the next step are issued before this step's arithmetic
+            struct QTab { double2 p0, kz, ky; float2 pu; };
+            auto qtab = [&](int s) {
+                const size_t i2 = (((size_t)s * 4 + bp) * DP + ba) * 2;
+                const size_t i4 = (((size_t)s * 2 + (bp >> 1)) * DP + ba) * 4 + (bp & 1) * 2;
+                QTab q2;
+                q2.p0 = *(const double2*)(P.phase0 + i2);
+                q2.kz = *(const double2*)(P.kz + i2);
+                q2.pu = *(const float2*)(P.pupf + i4);
+                q2.ky = *(const double2*)(P.ky + 8 * s + 2 * bp);
+                return q2;
+            };
+            const uint32_t ore = kmajor_off(brow, 2 * bp, 16), oim = kmajor_off(brow, 8 + 2 * bp, 16);
+            auto slot_wait = [&]() {  // ring slot for the next K step
+                const int buf = q % NBQ;
+                if (q >= NBQ) umma::mbar_wait(&qfree[buf], (uint32_t)((q / NBQ - 1) & 1), P.err);
+                ++q;
+                return QR + buf * QRING;
+            };
+            auto slot_done = [&](char* qs) {  // every writer fences its stores; one arrive per warp
+                umma::fence_proxy_async();
+                warp_arrive(&qfull[(qs - QR) / QRING]);
+            };
+            uint32_t zkeep[TWO ? 8 : 1][2] = {};  // pass A's Q_z of each K step (W = 128)
+            auto build = [&](int s, const QTab& tb, uint32_t& zr, uint32_t& zi) {
+                const double ph0[2] = {tb.p0.x, tb.p0.y}, kzr[2] = {tb.kz.x, tb.kz.y}, kyr[2] = {tb.ky.x, tb.ky.y};
+                const float pu[2] = {tb.pu.x, tb.pu.y};
+                float qr[2], qi[2], kzv[2];
 #pragma unroll
-            for (int e = 0; e < 2; ++e) {
-                qr[e] = 0.f; qi[e] = 0.f; kzv[e] = 0.f;
-                if (blive && pu[e] != 0.f) {
-                    float sn, cs;
-                    sincos_phase(ph0[e] + kxa * x + kyr[e] * y + kzr[e] * z, sn, cs);
-                    qr[e] = pu[e] * cs;
-                    qi[e] = pu[e] * sn;
-                    kzv[e] = (float)kzr[e];
+                for (int e = 0; e < 2; ++e) {
+                    qr[e] = 0.f; qi[e] = 0.f; kzv[e] = 0.f;
+                    if (blive && pu[e] != 0.f) {
+                        float sn, cs;
+                        sincos_phase(ph0[e] + kxa * x + kyr[e] * y + kzr[e] * z, sn, cs);
+                        qr[e] = pu[e] * cs;
+                        qi[e] = pu[e] * sn;
+                        kzv[e] = (float)kzr[e];
+                    }
                 }
-            }
-            zr = pack_h2(-kzv[0] * qi[0] * P.sc.qz, -kzv[1] * qi[1] * P.sc.qz);  // Q_z = i kz Q
-            zi = pack_h2(kzv[0] * qr[0] * P.sc.qz, kzv[1] * qr[1] * P.sc.qz);
-            uint32_t rh, rl, ih, il;
-            split2(qr[0] * P.sc.q, qr[1] * P.sc.q, rh, rl);
-            split2(qi[0] * P.sc.q, qi[1] * P.sc.q, ih, il);
-            char* qs = slot_wait();
-            *(uint32_t*)(qs + ore) = rh;
-            *(uint32_t*)(qs + oim) = ih;
-            *(uint32_t*)(qs + QB + ore) = rl;
-            *(uint32_t*)(qs + QB + oim) = il;
-            if (!TWO) {
-                *(uint32_t*)(qs + 2 * QB + ore) = zr;
-                *(uint32_t*)(qs + 2 * QB + oim) = zi;
-            }
-            slot_done(qs);
-        };
-        auto build_z = [&](int s) {  // pass B (W = 128): the kept Q_z of step s
-            char* qs = slot_wait();
-            *(uint32_t*)(qs + ore) = zkeep[TWO ? s : 0][0];
-            *(uint32_t*)(qs + oim) = zkeep[TWO ? s : 0][1];
-            slot_done(qs);
-        };
-        // A2 destination of this thread's TMEM row: stage-2 tile of the slot, K positions of a
-        const int slot = tile * G1 + g;
-        const bool live = P.slot_roi[slot] >= 0;
-        const int tile2 = slot / P.G2, mrow0 = (slot % P.G2) * W;
-        char* a2t = P.a2 + (size_t)tile2 * a2_tile_bytes(K1);
-        // epilogue of one pass: maps at TMEM columns c0 (S), c0 + 2W (S_y), zc (S_z; < 0: none)
-        auto epilogue = [&](bool sy, int zc, uint32_t phase, uint64_t* accb) {
-            umma::mbar_wait(accb, phase, P.err);
-            umma::fence_after_sync();
+                zr = pack_h2(-kzv[0] * qi[0] * P.sc.qz, -kzv[1] * qi[1] * P.sc.qz);  // Q_z = i kz Q
+                zi = pack_h2(kzv[0] * qr[0] * P.sc.qz, kzv[1] * qr[1] * P.sc.qz);
+                uint32_t rh, rl, ih, il;
+                split2(qr[0] * P.sc.q, qr[1] * P.sc.q, rh, rl);
+                split2(qi[0] * P.sc.q, qi[1] * P.sc.q, ih, il);
+                char* qs = slot_wait();
+                *(uint32_t*)(qs + ore) = rh;
+                *(uint32_t*)(qs + oim) = ih;
+                *(uint32_t*)(qs + QB + ore) = rl;
+                *(uint32_t*)(qs + QB + oim) = il;
+                if (!TWO) {
+                    *(uint32_t*)(qs + 2 * QB + ore) = zr;
+                    *(uint32_t*)(qs + 2 * QB + oim) = zi;
+                }
+                slot_done(qs);
+            };
+            auto build_z = [&](int s) {  // pass B (W = 128): the kept Q_z of step s
+                char* qs = slot_wait();
+                *(uint32_t*)(qs + ore) = zkeep[TWO ? s : 0][0];
+                *(uint32_t*)(qs + oim) = zkeep[TWO ? s : 0][1];
+                slot_done(qs);
+            };
+            // A2 destination of this thread's TMEM row: stage-2 tile of the slot, K positions of a
+            const int slot = tile * G1 + g;
+            const bool live = P.slot_roi[slot] >= 0;
+            const int tile2 = slot / P.G2, mrow0 = (slot % P.G2) * W;
+            char* a2t = P.a2 + (size_t)tile2 * a2_tile_bytes(K1);
+            // epilogue of one pass: maps at TMEM columns c0 (S), c0 + 2W (S_y), zc (S_z; < 0: none)
+            auto epilogue = [&](bool sy, int zc, uint32_t phase, uint64_t* accb) {
+                umma::mbar_wait(accb, phase, P.err);
+                umma::fence_after_sync();
 #pragma unroll 1
-            for (int h = wg * CW; h < (wg + 1) * CW; h += 8) {
-                const int m = mrow0 + h;
-                if (sy) {
-                    float v4[4][8];
-                    const uint32_t ad[4] = {tmem_lane_addr(tbase, h), tmem_lane_addr(tbase, W + h),
-                                            tmem_lane_addr(tbase, 2 * W + h), tmem_lane_addr(tbase, 3 * W + h)};
-                    tmem_ld8_multi<4>(ad, v4);
-                    const float *sr = v4[0], *si = v4[1], *yr = v4[2], *yi = v4[3];
-                    if (live) {
-                        uint32_t shr[4], slr[4], shi[4], sli[4], wyr[4], wyi[4];
+                for (int h = wg * CW; h < (wg + 1) * CW; h += 8) {
+                    const int m = mrow0 + h;
+                    if (sy) {
+                        float v4[4][8];
+                        const uint32_t ad[4] = {tmem_lane_addr(tbase, h), tmem_lane_addr(tbase, W + h),
+                                                tmem_lane_addr(tbase, 2 * W + h), tmem_lane_addr(tbase, 3 * W + h)};
+                        tmem_ld8_multi<4>(ad, v4);
+                        const float *sr = v4[0], *si = v4[1], *yr = v4[2], *yi = v4[3];
+                        if (live) {
+                            uint32_t shr[4], slr[4], shi[4], sli[4], wyr[4], wyi[4];
 #pragma unroll
-                        for (int u = 0; u < 8; u += 2) {
-                            split2(sr[u] * P.sc.c2, sr[u + 1] * P.sc.c2, shr[u / 2], slr[u / 2]);
-                            split2(si[u] * P.sc.c2, si[u + 1] * P.sc.c2, shi[u / 2], sli[u / 2]);
-                            wyr[u / 2] = pack_h2(yr[u] * P.sc.c2y, yr[u + 1] * P.sc.c2y);
-                            wyi[u / 2] = pack_h2(yi[u] * P.sc.c2y, yi[u + 1] * P.sc.c2y);
+                            for (int u = 0; u < 8; u += 2) {
+                                split2(sr[u] * P.sc.c2, sr[u + 1] * P.sc.c2, shr[u / 2], slr[u / 2]);
+                                split2(si[u] * P.sc.c2, si[u + 1] * P.sc.c2, shi[u / 2], sli[u / 2]);
+                                wyr[u / 2] = pack_h2(yr[u] * P.sc.c2y, yr[u + 1] * P.sc.c2y);
+                                wyi[u / 2] = pack_h2(yi[u] * P.sc.c2y, yi[u + 1] * P.sc.c2y);
+                            }
+                            store4w(a2t + 0 * arr + mnmajor_off(m, kre, 128), shr);
+                            store4w(a2t + 1 * arr + mnmajor_off(m, kre, 128), slr);
+                            store4w(a2t + 0 * arr + mnmajor_off(m, kim, 128), shi);
+                            store4w(a2t + 1 * arr + mnmajor_off(m, kim, 128), sli);
+                            store4w(a2t + 2 * arr + mnmajor_off(m, kre, 128), wyr);
+                            store4w(a2t + 2 * arr + mnmajor_off(m, kim, 128), wyi);
                         }
-                        store4w(a2t + 0 * arr + mnmajor_off(m, kre, 128), shr);
-                        store4w(a2t + 1 * arr + mnmajor_off(m, kre, 128), slr);
-                        store4w(a2t + 0 * arr + mnmajor_off(m, kim, 128), shi);
-                        store4w(a2t + 1 * arr + mnmajor_off(m, kim, 128), sli);
-                        store4w(a2t + 2 * arr + mnmajor_off(m, kre, 128), wyr);
-                        store4w(a2t + 2 * arr + mnmajor_off(m, kim, 128), wyi);
+                    }
+                    if (zc >= 0) {
+                        float v2[2][8];
+                        const uint32_t ad[2] = {tmem_lane_addr(tbase, zc + h), tmem_lane_addr(tbase, zc + W + h)};
+                        tmem_ld8_multi<2>(ad, v2);
+                        const float *zr8 = v2[0], *zi8 = v2[1];
+                        if (live) {
+                            uint32_t wzr[4], wzi[4];
+#pragma unroll
+                            for (int u = 0; u < 8; u += 2) {
+                                wzr[u / 2] = pack_h2(zr8[u] * P.sc.c2z, zr8[u + 1] * P.sc.c2z);
+                                wzi[u / 2] = pack_h2(zi8[u] * P.sc.c2z, zi8[u + 1] * P.sc.c2z);
+                            }
+                            store4w(a2t + 3 * arr + mnmajor_off(m, kre, 128), wzr);
+                            store4w(a2t + 3 * arr + mnmajor_off(m, kim, 128), wzi);
+                        }
                     }
                 }
-                if (zc >= 0) {
-                    float v2[2][8];
-                    const uint32_t ad[2] = {tmem_lane_addr(tbase, zc + h), tmem_lane_addr(tbase, zc + W + h)};
-                    tmem_ld8_multi<2>(ad, v2);
-                    const float *zr8 = v2[0], *zi8 = v2[1];
-                    if (live) {
-                        uint32_t wzr[4], wzi[4];
+                umma::fence_before_sync();
+                warp_arrive(&tfree);
+            };
+            if constexpr (TWO) {
+                QTab cur = qtab(0);
 #pragma unroll
-                        for (int u = 0; u < 8; u += 2) {
-                            wzr[u / 2] = pack_h2(zr8[u] * P.sc.c2z, zr8[u + 1] * P.sc.c2z);
-                            wzi[u / 2] = pack_h2(zi8[u] * P.sc.c2z, zi8[u + 1] * P.sc.c2z);
-                        }
-                        store4w(a2t + 3 * arr + mnmajor_off(m, kre, 128), wzr);
-                        store4w(a2t + 3 * arr + mnmajor_off(m, kim, 128), wzi);
-                    }
+                for (int s = 0; s < 8; ++s) {
+                    QTab nxt;
+                    if (s + 1 < 8) nxt = qtab(s + 1);
+                    build(s, cur, zkeep[s][0], zkeep[s][1]);
+                    if (s + 1 < 8) cur = nxt;
                 }
-            }
-            umma::fence_before_sync();
-            warp_arrive(&tfree);
-        };
-        if constexpr (TWO) {
-            QTab cur = qtab(0);
 #pragma unroll
-            for (int s = 0; s < 8; ++s) {
-                QTab nxt;
-                if (s + 1 < 8) nxt = qtab(s + 1);
-                build(s, cur, zkeep[s][0], zkeep[s][1]);
-                if (s + 1 < 8) cur = nxt;
-            }
+                for (int s = 0; s < NBQ; ++s) build_z(s);
+                epilogue(true, -1, ph, &accA);
 #pragma unroll
-            for (int s = 0; s < NBQ; ++s) build_z(s);
-            epilogue(true, -1, ph, &accA);
-#pragma unroll
-            for (int s = NBQ; s < 8; ++s) build_z(s);
-            epilogue(false, 0, ph, &accB);
-        } else {
-            QTab cur = qtab(0);
-            for (int s = 0; s < NS; ++s) {
-                QTab nxt;
-                if (s + 1 < NS) nxt = qtab(s + 1);
-                uint32_t zr, zi;
-                build(s, cur, zr, zi);
-                if (s + 1 < NS) cur = nxt;
+                for (int s = NBQ; s < 8; ++s) build_z(s);
+                epilogue(false, 0, ph, &accB);
+            } else {
+                QTab cur = qtab(0);
+                for (int s = 0; s < NS; ++s) {
+                    QTab nxt;
+                    if (s + 1 < NS) nxt = qtab(s + 1);
+                    uint32_t zr, zi;
+                    build(s, cur, zr, zi);
+                    if (s + 1 < NS) cur = nxt;
+                }
+                epilogue(true, 4 * W, ph, &accA);
             }
-            epilogue(true, 4 * W, ph, &accA);
+            // (a bounded wait that gave up makes every builder leave the loop together)
+            units.fence_writes();
+            abort = epi_bar_or(t == 0 && *(volatile int*)P.err != 0);
         }
-        // (a bounded wait that gave up makes every builder leave the loop together)
-        abort = epi_bar_or(t == 0 && *(volatile int*)P.err != 0);
+        if (!abort && t == 0) units.release(P, unit, tag + 1);
     }
     if (t == 0) {
         umma::mbar_wait(&fin, 0, P.err);    // every MMA of this CTA has completed
@@ -785,6 +1028,13 @@ __global__ void __launch_bounds__(S1_THREADS, 1) k_stage1p(SplitDev P, int ntile
     epi_bar();
     if (t < 32) umma::tmem_dealloc(tbase, NCOLS);
 }
+
+template <int W>
+__global__ void __launch_bounds__(S1_THREADS, 1) k_stage1p(SplitDev P, FitIO F) {
+    if (!cta_has_live_tile(P, P.P / unit_slots(P.G1, P.G2), unit_slots(P.G1, P.G2))) return;
+    stage1_body<W>(P, F, StaticUnits{});
+}
+
 
 // ------------------------------------------------- stage 2 (persistent) -----
 // One CTA per SM walks the stage-2 tiles (G2 slots x W rows j) with the
@@ -802,8 +1052,8 @@ __global__ void __launch_bounds__(S1_THREADS, 1) k_stage1p(SplitDev P, int ntile
 constexpr int S2_THREADS = SPLIT_THREADS + 32;
 constexpr int S2_NBUF = 4;
 
-template <int W>
-__global__ void __launch_bounds__(S2_THREADS, 1) k_stage2p(SplitDev P, int ntiles) {
+template <int W, class UNITS>
+__device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, UNITS units) {
     extern __shared__ __align__(1024) char smem[];
     constexpr bool TWO = W > 64;
     constexpr int SLAB = s2_slab_bytes(W), RING = s2_ring_bytes(W), NBUF = S2_NBUF;
@@ -811,12 +1061,12 @@ __global__ void __launch_bounds__(S2_THREADS, 1) k_stage2p(SplitDev P, int ntile
     constexpr int NARR = TWO ? 2 : 4;  // A2 arrays per ring step
     const int K1 = P.K1, G2 = P.G2, t = threadIdx.x;
     const int NS = K1 / 16, NSTEP = TWO ? 2 * NS : NS;
+    const int T2 = unit_slots(P.G1, G2) / G2;  // window tiles per unit
     const uint32_t arr = 128u * K1 * 2;
     char* CS = smem;                 // NS constant K-slabs
     char* RB = smem + NS * SLAB;     // ring of A2 K-slabs
     __shared__ __align__(8) uint64_t cfull, full[NBUF], freed[NBUF], accA, accB;
     __shared__ uint32_t tmem_base;
-    if (!cta_has_live_tile(P, ntiles, G2)) return;
     if (t < 32) umma::tmem_alloc(&tmem_base, NCOLS);
     if (t == 0) {
         umma::mbar_init(&cfull, 1);
@@ -829,25 +1079,35 @@ __global__ void __launch_bounds__(S2_THREADS, 1) k_stage2p(SplitDev P, int ntile
     umma::fence_after_sync();
     const uint32_t tbase = tmem_base;
 
-    if (t >= SPLIT_THREADS) {  // ---------------- producer warp
+    if (t >= SPLIT_THREADS) {  // ---------------- producer (lane 0), scheduler (lane 1)
+        if constexpr (UNITS::flow)
+            if (t == SPLIT_THREADS + 1) {
+                units.schedule(P, F);
+                return;
+            }
         if (t != SPLIT_THREADS) return;
         umma::mbar_expect_tx(&cfull, (uint32_t)(NS * SLAB));
         for (int s = 0; s < NS; ++s)
             umma::bulk_g2s(CS + s * SLAB, (const char*)P.bcs + (size_t)s * SLAB, SLAB, &cfull);
         int q = 0;
-        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-            if (!tile_live(P, tile * G2, G2)) continue;
-            const char* src = P.a2 + (size_t)tile * a2_tile_bytes(K1);
-            for (int n = 0; n < NSTEP; ++n, ++q) {
-                const int buf = q % NBUF;
-                if (q >= NBUF && !umma::mbar_wait(&freed[buf], (uint32_t)((q / NBUF - 1) & 1), P.err)) return;
-                const bool pb = TWO && n >= NS;
-                const int s = pb ? n - NS : n;
-                const int a0 = pb ? 2 : 0;  // phase B streams the y and z arrays
-                umma::mbar_expect_tx(&full[buf], RING);
-                for (int j = 0; j < NARR; ++j)
-                    umma::bulk_g2s(RB + buf * RING + j * 4096, src + (size_t)(a0 + j) * arr + (size_t)s * 4096, 4096,
-                                   &full[buf]);
+        for (int tag = 0;;) {
+            const int unit = units.next(P, tag, true);
+            if (unit < 0) break;
+            for (int k = 0; k < T2; ++k) {
+                const int tile = unit * T2 + k;
+                if (!tile_live(P, tile * G2, G2)) continue;
+                const char* src = P.a2 + (size_t)tile * a2_tile_bytes(K1);
+                for (int n = 0; n < NSTEP; ++n, ++q) {
+                    const int buf = q % NBUF;
+                    if (q >= NBUF && !umma::mbar_wait(&freed[buf], (uint32_t)((q / NBUF - 1) & 1), P.err)) return;
+                    const bool pb = TWO && n >= NS;
+                    const int s = pb ? n - NS : n;
+                    const int a0 = pb ? 2 : 0;  // phase B streams the y and z arrays
+                    umma::mbar_expect_tx(&full[buf], RING);
+                    for (int j = 0; j < NARR; ++j)
+                        umma::bulk_g2s(RB + buf * RING + j * 4096, src + (size_t)(a0 + j) * arr + (size_t)s * 4096, 4096,
+                                       &full[buf]);
+                }
             }
         }
         return;
@@ -893,180 +1153,260 @@ __global__ void __launch_bounds__(S2_THREADS, 1) k_stage2p(SplitDev P, int ntile
         return (er[u] * xr[u] + ei[u] * xi[u]) * cf;
     };
     if (t == 0) umma::mbar_wait(&cfull, 0, P.err);
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        if (!tile_live(P, tile * G2, G2)) continue;
-        char* a3t = P.a3 + (size_t)tile * a3_tile_bytes(W);
-        if (t == 0) {
-            issue_steps(0, NS);
-            umma::mma_commit(&accA);
-        }
-        umma::mbar_wait(&accA, (uint32_t)ph, P.err);
-        umma::fence_after_sync();
-        if constexpr (TWO) {
-            float er[CW], ei[CW];
-#pragma unroll
-            for (int h = 0; h < CW; h += 8) {
-                const int i0 = wg * CW + h;
-                float v4[4][8];
-                const uint32_t ad[4] = {tmem_lane_addr(tbase, i0), tmem_lane_addr(tbase, W + i0),
-                                        tmem_lane_addr(tbase, 2 * W + i0), tmem_lane_addr(tbase, 3 * W + i0)};
-                tmem_ld8_multi<4>(ad, v4);
-#pragma unroll
-                for (int u = 0; u < 8; ++u) { er[h + u] = v4[0][u]; ei[h + u] = v4[1][u]; }
-                const float *xr = v4[2], *xi = v4[3];
-                uint32_t hh[4], ll[4], dx[4];
-#pragma unroll
-                for (int u = 0; u < 8; u += 2) {
-                    split2((er[h + u] * er[h + u] + ei[h + u] * ei[h + u]) * P.sc.cI,
-                           (er[h + u + 1] * er[h + u + 1] + ei[h + u + 1] * ei[h + u + 1]) * P.sc.cI, hh[u / 2],
-                           ll[u / 2]);
-                    dx[u / 2] = pack_h2(ipx(er + h, ei + h, xr, xi, u, P.sc.cIx),
-                                        ipx(er + h, ei + h, xr, xi, u + 1, P.sc.cIx));
-                }
-                const uint32_t off = kmajor_off(row, i0, W);
-                store4w(a3t + 0 * arr3 + off, hh);
-                store4w(a3t + 1 * arr3 + off, ll);
-                store4w(a3t + 2 * arr3 + off, dx);
-            }
-            umma::fence_before_sync();
-            epi_bar();
+    bool abort = false;
+    for (int tag = 0; !abort;) {
+        const int unit = units.next(P, tag);
+        if (unit < 0) break;
+        for (int k = 0; k < T2 && !abort; ++k) {
+            const int tile = unit * T2 + k;
+            if (!tile_live(P, tile * G2, G2)) continue;
+            char* a3t = P.a3 + (size_t)tile * a3_tile_bytes(W);
             if (t == 0) {
-                umma::fence_after_sync();
-                issue_steps(NS, NSTEP);
-                umma::mma_commit(&accB);
+                issue_steps(0, NS);
+                umma::mma_commit(&accA);
             }
-            umma::mbar_wait(&accB, (uint32_t)ph, P.err);
+            umma::mbar_wait(&accA, (uint32_t)ph, P.err);
             umma::fence_after_sync();
+            if constexpr (TWO) {
+                float er[CW], ei[CW];
 #pragma unroll
-            for (int h = 0; h < CW; h += 8) {
-                const int i0 = wg * CW + h;
-                float v4[4][8];
-                const uint32_t ad[4] = {tmem_lane_addr(tbase, i0), tmem_lane_addr(tbase, W + i0),
-                                        tmem_lane_addr(tbase, 2 * W + i0), tmem_lane_addr(tbase, 3 * W + i0)};
-                tmem_ld8_multi<4>(ad, v4);
-                uint32_t dy[4], dz[4];
+                for (int h = 0; h < CW; h += 8) {
+                    const int i0 = wg * CW + h;
+                    float v4[4][8];
+                    const uint32_t ad[4] = {tmem_lane_addr(tbase, i0), tmem_lane_addr(tbase, W + i0),
+                                            tmem_lane_addr(tbase, 2 * W + i0), tmem_lane_addr(tbase, 3 * W + i0)};
+                    tmem_ld8_multi<4>(ad, v4);
 #pragma unroll
-                for (int u = 0; u < 8; u += 2) {
-                    dy[u / 2] = pack_h2(ipx(er + h, ei + h, v4[0], v4[1], u, P.sc.cIy),
-                                        ipx(er + h, ei + h, v4[0], v4[1], u + 1, P.sc.cIy));
-                    dz[u / 2] = pack_h2(ipx(er + h, ei + h, v4[2], v4[3], u, P.sc.cIz),
-                                        ipx(er + h, ei + h, v4[2], v4[3], u + 1, P.sc.cIz));
+                    for (int u = 0; u < 8; ++u) { er[h + u] = v4[0][u]; ei[h + u] = v4[1][u]; }
+                    const float *xr = v4[2], *xi = v4[3];
+                    uint32_t hh[4], ll[4], dx[4];
+#pragma unroll
+                    for (int u = 0; u < 8; u += 2) {
+                        split2((er[h + u] * er[h + u] + ei[h + u] * ei[h + u]) * P.sc.cI,
+                               (er[h + u + 1] * er[h + u + 1] + ei[h + u + 1] * ei[h + u + 1]) * P.sc.cI, hh[u / 2],
+                               ll[u / 2]);
+                        dx[u / 2] = pack_h2(ipx(er + h, ei + h, xr, xi, u, P.sc.cIx),
+                                            ipx(er + h, ei + h, xr, xi, u + 1, P.sc.cIx));
+                    }
+                    const uint32_t off = kmajor_off(row, i0, W);
+                    store4w(a3t + 0 * arr3 + off, hh);
+                    store4w(a3t + 1 * arr3 + off, ll);
+                    store4w(a3t + 2 * arr3 + off, dx);
                 }
-                const uint32_t off = kmajor_off(row, i0, W);
-                store4w(a3t + 3 * arr3 + off, dy);
-                store4w(a3t + 4 * arr3 + off, dz);
+                umma::fence_before_sync();
+                epi_bar();
+                if (t == 0) {
+                    umma::fence_after_sync();
+                    issue_steps(NS, NSTEP);
+                    umma::mma_commit(&accB);
+                }
+                umma::mbar_wait(&accB, (uint32_t)ph, P.err);
+                umma::fence_after_sync();
+#pragma unroll
+                for (int h = 0; h < CW; h += 8) {
+                    const int i0 = wg * CW + h;
+                    float v4[4][8];
+                    const uint32_t ad[4] = {tmem_lane_addr(tbase, i0), tmem_lane_addr(tbase, W + i0),
+                                            tmem_lane_addr(tbase, 2 * W + i0), tmem_lane_addr(tbase, 3 * W + i0)};
+                    tmem_ld8_multi<4>(ad, v4);
+                    uint32_t dy[4], dz[4];
+#pragma unroll
+                    for (int u = 0; u < 8; u += 2) {
+                        dy[u / 2] = pack_h2(ipx(er + h, ei + h, v4[0], v4[1], u, P.sc.cIy),
+                                            ipx(er + h, ei + h, v4[0], v4[1], u + 1, P.sc.cIy));
+                        dz[u / 2] = pack_h2(ipx(er + h, ei + h, v4[2], v4[3], u, P.sc.cIz),
+                                            ipx(er + h, ei + h, v4[2], v4[3], u + 1, P.sc.cIz));
+                    }
+                    const uint32_t off = kmajor_off(row, i0, W);
+                    store4w(a3t + 3 * arr3 + off, dy);
+                    store4w(a3t + 4 * arr3 + off, dz);
+                }
+            } else {
+#pragma unroll
+                for (int h = 0; h < CW; h += 8) {
+                    const int i0 = wg * CW + h;
+                    float v4[4][8];
+                    const uint32_t ad[4] = {tmem_lane_addr(tbase, i0), tmem_lane_addr(tbase, W + i0),
+                                            tmem_lane_addr(tbase, 2 * W + i0), tmem_lane_addr(tbase, 3 * W + i0)};
+                    tmem_ld8_multi<4>(ad, v4);
+                    const float *er = v4[0], *ei = v4[1], *xr = v4[2], *xi = v4[3];
+                    uint32_t hh[4], ll[4], dx[4], dy[4], dz[4];
+#pragma unroll
+                    for (int u = 0; u < 8; u += 2) {
+                        split2((er[u] * er[u] + ei[u] * ei[u]) * P.sc.cI,
+                               (er[u + 1] * er[u + 1] + ei[u + 1] * ei[u + 1]) * P.sc.cI, hh[u / 2], ll[u / 2]);
+                        dx[u / 2] = pack_h2(ipx(er, ei, xr, xi, u, P.sc.cIx), ipx(er, ei, xr, xi, u + 1, P.sc.cIx));
+                    }
+                    float w4[4][8];
+                    const uint32_t bd[4] = {tmem_lane_addr(tbase, 4 * W + i0), tmem_lane_addr(tbase, 5 * W + i0),
+                                            tmem_lane_addr(tbase, 6 * W + i0), tmem_lane_addr(tbase, 7 * W + i0)};
+                    tmem_ld8_multi<4>(bd, w4);
+#pragma unroll
+                    for (int u = 0; u < 8; u += 2) {
+                        dy[u / 2] = pack_h2(ipx(er, ei, w4[0], w4[1], u, P.sc.cIy), ipx(er, ei, w4[0], w4[1], u + 1, P.sc.cIy));
+                        dz[u / 2] = pack_h2(ipx(er, ei, w4[2], w4[3], u, P.sc.cIz), ipx(er, ei, w4[2], w4[3], u + 1, P.sc.cIz));
+                    }
+                    const uint32_t off = kmajor_off(row, i0, W);
+                    store4w(a3t + 0 * arr3 + off, hh);
+                    store4w(a3t + 1 * arr3 + off, ll);
+                    store4w(a3t + 2 * arr3 + off, dx);
+                    store4w(a3t + 3 * arr3 + off, dy);
+                    store4w(a3t + 4 * arr3 + off, dz);
+                }
             }
-        } else {
-#pragma unroll
-            for (int h = 0; h < CW; h += 8) {
-                const int i0 = wg * CW + h;
-                float v4[4][8];
-                const uint32_t ad[4] = {tmem_lane_addr(tbase, i0), tmem_lane_addr(tbase, W + i0),
-                                        tmem_lane_addr(tbase, 2 * W + i0), tmem_lane_addr(tbase, 3 * W + i0)};
-                tmem_ld8_multi<4>(ad, v4);
-                const float *er = v4[0], *ei = v4[1], *xr = v4[2], *xi = v4[3];
-                uint32_t hh[4], ll[4], dx[4], dy[4], dz[4];
-#pragma unroll
-                for (int u = 0; u < 8; u += 2) {
-                    split2((er[u] * er[u] + ei[u] * ei[u]) * P.sc.cI,
-                           (er[u + 1] * er[u + 1] + ei[u + 1] * ei[u + 1]) * P.sc.cI, hh[u / 2], ll[u / 2]);
-                    dx[u / 2] = pack_h2(ipx(er, ei, xr, xi, u, P.sc.cIx), ipx(er, ei, xr, xi, u + 1, P.sc.cIx));
-                }
-                float w4[4][8];
-                const uint32_t bd[4] = {tmem_lane_addr(tbase, 4 * W + i0), tmem_lane_addr(tbase, 5 * W + i0),
-                                        tmem_lane_addr(tbase, 6 * W + i0), tmem_lane_addr(tbase, 7 * W + i0)};
-                tmem_ld8_multi<4>(bd, w4);
-#pragma unroll
-                for (int u = 0; u < 8; u += 2) {
-                    dy[u / 2] = pack_h2(ipx(er, ei, w4[0], w4[1], u, P.sc.cIy), ipx(er, ei, w4[0], w4[1], u + 1, P.sc.cIy));
-                    dz[u / 2] = pack_h2(ipx(er, ei, w4[2], w4[3], u, P.sc.cIz), ipx(er, ei, w4[2], w4[3], u + 1, P.sc.cIz));
-                }
-                const uint32_t off = kmajor_off(row, i0, W);
-                store4w(a3t + 0 * arr3 + off, hh);
-                store4w(a3t + 1 * arr3 + off, ll);
-                store4w(a3t + 2 * arr3 + off, dx);
-                store4w(a3t + 3 * arr3 + off, dy);
-                store4w(a3t + 4 * arr3 + off, dz);
-            }
+            // all TMEM reads of this tile done before the next tile's MMAs
+            // (a bounded wait that gave up makes every epilogue thread leave the loop together)
+            umma::fence_before_sync();
+            units.fence_writes();
+            abort = epi_bar_or(t == 0 && *(volatile int*)P.err != 0);
+            if (t == 0) umma::fence_after_sync();
+            ph ^= 1;
         }
-        // all TMEM reads of this tile done before the next tile's MMAs
-        // (a bounded wait that gave up makes every epilogue thread leave the loop together)
-        umma::fence_before_sync();
-        const bool abort = epi_bar_or(t == 0 && *(volatile int*)P.err != 0);
-        if (t == 0) umma::fence_after_sync();
-        ph ^= 1;
-        if (abort) break;
+        if (!abort && t == 0) units.release(P, unit, tag + 1);
     }
     epi_bar();
     if (t < 32) umma::tmem_dealloc(tbase, NCOLS);
 }
 
-// ----------------------------------------------------------- stage 3 -------
-// Blur along the first image index: J^T[(g2, j)][i'] = sum_i I[j][i] G[i'][i].
-__global__ void __launch_bounds__(SPLIT_THREADS, 1) k_stage3(SplitDev P) {
+template <int W>
+__global__ void __launch_bounds__(S2_THREADS, 1) k_stage2p(SplitDev P, FitIO F) {
+    if (!cta_has_live_tile(P, P.P / unit_slots(P.G1, P.G2), unit_slots(P.G1, P.G2))) return;
+    stage2_body<W>(P, F, StaticUnits{});
+}
+
+
+// ------------------------------------------------- stage 3 (persistent) -----
+// Blur along the first image index: J^T[(g2, j)][i'] = sum_i I[j][i] G[i'][i]
+// for each window tile (G2 slots x W rows j).  One CTA per SM keeps G^T in
+// shared memory; warp 16 loads a tile's five intensity arrays (A3) and issues
+// its MMAs into one of two TMEM accumulators, so that the next tile's load and
+// MMAs overlap this tile's epilogue (warps 0-15), which writes the row-blurred
+// maps as the column-blur B operand (hi, lo; N = 4 RP rows (map, i'), K = j).
+constexpr int S3_THREADS = SPLIT_THREADS + 32;
+
+template <class UNITS>
+__device__ __forceinline__ void stage3_body(const SplitDev& P, const FitIO& F, UNITS units) {
     extern __shared__ __align__(1024) char smem[];
-    const int W = P.W, RP = P.RP, t = threadIdx.x;
+    const int W = P.W, RP = P.RP, G2 = P.G2, t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int T2 = unit_slots(P.G1, G2) / G2;
     const size_t arr3 = (size_t)128 * W * 2, gbytes = (size_t)RP * W * 2;
-    char* A3 = smem;
-    char* GT = A3 + 5 * arr3;  // hi, lo
-    __shared__ __align__(8) uint64_t full, done;
+    char* A3 = smem;            // one window tile: I hi, I lo, I_x, I_y, I_z
+    char* GT = A3 + 5 * arr3;   // G^T hi, lo
+    __shared__ __align__(8) uint64_t gfull, full, acc[2], tfree[2], fin;
     __shared__ uint32_t tmem_base;
-    const int ncols = tmem_cols_pow2(4 * RP);
-    if (!tile_live(P, blockIdx.x * P.G2, P.G2)) return;
-    if (t < 32) umma::tmem_alloc(&tmem_base, ncols);
+    const int nc = tmem_cols_pow2(4 * RP);  // one accumulator
+    if (t < 32) umma::tmem_alloc(&tmem_base, 2 * nc);
     if (t == 0) {
+        umma::mbar_init(&gfull, 1);
         umma::mbar_init(&full, 1);
-        umma::mbar_init(&done, 1);
+        for (int b = 0; b < 2; ++b) {
+            umma::mbar_init(&acc[b], 1);
+            umma::mbar_init(&tfree[b], SPLIT_THREADS / 32);
+        }
+        umma::mbar_init(&fin, 1);
         umma::mbar_fence_init();
     }
     __syncthreads();
     umma::fence_after_sync();
     const uint32_t tbase = tmem_base;
-    if (t == 0) {
-        umma::mbar_expect_tx(&full, (uint32_t)(5 * arr3 + 2 * gbytes));
-        const char* src = P.a3 + (size_t)blockIdx.x * a3_tile_bytes(W);
-        for (int q = 0; q < 5; ++q) umma::bulk_g2s(A3 + q * arr3, src + q * arr3, (uint32_t)arr3, &full);
-        umma::bulk_g2s(GT, P.gt_hi, (uint32_t)gbytes, &full);
-        umma::bulk_g2s(GT + gbytes, P.gt_lo, (uint32_t)gbytes, &full);
-        umma::mbar_wait(&full, 0, P.err);
-        umma::fence_after_sync();
+
+    if (warp == SPLIT_THREADS / 32) {  // ---------------- loads + MMAs (lane 0), scheduler (lane 1)
+        if constexpr (UNITS::flow)
+            if (lane == 1) {
+                units.schedule(P, F);
+                return;
+            }
+        if (lane != 0) return;
+        umma::mbar_expect_tx(&gfull, (uint32_t)(2 * gbytes));
+        umma::bulk_g2s(GT, P.gt_hi, (uint32_t)gbytes, &gfull);
+        umma::bulk_g2s(GT + gbytes, P.gt_lo, (uint32_t)gbytes, &gfull);
+        bool ok = umma::mbar_wait(&gfull, 0, P.err);
         const uint32_t sbo = (W / 8) * 128;
         const uint32_t id = umma::idesc_f16(128, RP, false, false);
         const uint32_t a0 = umma::smem_u32(A3), ghi = umma::smem_u32(GT), glo = ghi + (uint32_t)gbytes;
-        mma_chain(tbase, a0, 128, sbo, 256, ghi, 128, sbo, 256, W, id, false);
-        mma_chain(tbase, a0, 128, sbo, 256, glo, 128, sbo, 256, W, id, true);
-        mma_chain(tbase, a0 + (uint32_t)arr3, 128, sbo, 256, ghi, 128, sbo, 256, W, id, true);
-        for (int m = 1; m < 4; ++m)
-            mma_chain(tbase + m * RP, a0 + (uint32_t)((m + 1) * arr3), 128, sbo, 256, ghi, 128, sbo, 256, W, id, false);
-        umma::mma_commit(&done);
+        int n = 0;
+        for (int tag = 0; ok;) {
+            const int unit = units.next(P, tag, true);
+            if (unit < 0) break;
+            for (int k = 0; k < T2 && ok; ++k) {
+                const int tile = unit * T2 + k;
+                if (!tile_live(P, tile * G2, G2)) continue;
+                const int b = n & 1;
+                // the A3 buffer is free once the previous tile's MMAs have completed, and
+                // accumulator b once the epilogue has read tile n - 2 out of it
+                if (n >= 1 && !umma::mbar_wait(&acc[(n - 1) & 1], (uint32_t)(((n - 1) >> 1) & 1), P.err)) { ok = false; break; }
+                if (n >= 2 && !umma::mbar_wait(&tfree[b], (uint32_t)(((n >> 1) - 1) & 1), P.err)) { ok = false; break; }
+                umma::mbar_expect_tx(&full, (uint32_t)(5 * arr3));
+                const char* src = P.a3 + (size_t)tile * a3_tile_bytes(W);
+                for (int q = 0; q < 5; ++q) umma::bulk_g2s(A3 + q * arr3, src + q * arr3, (uint32_t)arr3, &full);
+                if (!umma::mbar_wait(&full, (uint32_t)(n & 1), P.err)) { ok = false; break; }
+                umma::fence_after_sync();
+                const uint32_t td = tbase + (uint32_t)(b * nc);
+                mma_chain(td, a0, 128, sbo, 256, ghi, 128, sbo, 256, W, id, false);
+                mma_chain(td, a0, 128, sbo, 256, glo, 128, sbo, 256, W, id, true);
+                mma_chain(td, a0 + (uint32_t)arr3, 128, sbo, 256, ghi, 128, sbo, 256, W, id, true);
+                for (int m = 1; m < 4; ++m)
+                    mma_chain(td + m * RP, a0 + (uint32_t)((m + 1) * arr3), 128, sbo, 256, ghi, 128, sbo, 256, W, id,
+                              false);
+                umma::mma_commit(&acc[b]);
+                ++n;
+            }
+        }
+        umma::mma_commit(&fin);
+        return;
     }
-    umma::mbar_wait(&done, 0, P.err);
-    umma::fence_after_sync();
-    // epilogue: thread row (g2, j) = t % 128 -> A4 column k = j of the slot's
-    // (map, i') rows; warpgroup = map
+
+    // ---------------- epilogue: thread row (g2, j) = t % 128 -> J column k = j of
+    // the slot's (map, i') rows; warpgroup = map
     const int row = t & 127, m = t >> 7;
     const int g2 = row / W, j = row % W;
-    const int slot = blockIdx.x * P.G2 + g2;
     const int NT = 4 * RP;
-    char* a4s = P.a4 + (size_t)slot * a4_slot_bytes(W, RP);
     const size_t arrJ = (size_t)NT * W * 2;
-    for (int h = 0; h < RP; h += 16) {
-        float v[16];
-        umma::tmem_ld16(tmem_lane_addr(tbase, m * RP + h), v);
-        for (int i8 = 0; i8 < 16; i8 += 8) {
-            const int r = m * RP + h + i8;  // n = (map, i')
-            uint32_t hh[4], ll[4];
+    int n = 0;
+    bool abort = false;
+    for (int tag = 0; !abort;) {
+        const int unit = units.next(P, tag);
+        if (unit < 0) break;
+        for (int k = 0; k < T2 && !abort; ++k) {
+            const int tile = unit * T2 + k;
+            if (!tile_live(P, tile * G2, G2)) continue;
+            const int b = n & 1;
+            umma::mbar_wait(&acc[b], (uint32_t)((n >> 1) & 1), P.err);
+            umma::fence_after_sync();
+            ++n;
+            char* a4s = P.a4 + (size_t)(tile * G2 + g2) * a4_slot_bytes(W, RP);
+            for (int h = 0; h < RP; h += 16) {
+                float v[16];
+                umma::tmem_ld16(tmem_lane_addr(tbase, b * nc + m * RP + h), v);
+                for (int i8 = 0; i8 < 16; i8 += 8) {
+                    const int r = m * RP + h + i8;  // n = (map, i')
+                    uint32_t hh[4], ll[4];
 #pragma unroll
-            for (int u = 0; u < 8; u += 2) split2(v[i8 + u] * P.sc.cJ[m], v[i8 + u + 1] * P.sc.cJ[m], hh[u / 2], ll[u / 2]);
-            const uint32_t off = mnmajor_off(r, j, NT);
-            store4w(a4s + off, hh);
-            store4w(a4s + arrJ + off, ll);
+                    for (int u = 0; u < 8; u += 2)
+                        split2(v[i8 + u] * P.sc.cJ[m], v[i8 + u + 1] * P.sc.cJ[m], hh[u / 2], ll[u / 2]);
+                    const uint32_t off = mnmajor_off(r, j, NT);
+                    store4w(a4s + off, hh);
+                    store4w(a4s + arrJ + off, ll);
+                }
+            }
+            umma::fence_before_sync();
+            warp_arrive(&tfree[b]);
+            units.fence_writes();
+            // (a bounded wait that gave up makes every epilogue thread leave the loop together)
+            abort = epi_bar_or(t == 0 && *(volatile int*)P.err != 0);
         }
+        if (!abort && t == 0) units.release(P, unit, tag + 1);
     }
-    umma::fence_before_sync();
-    __syncthreads();
-    if (t < 32) umma::tmem_dealloc(tbase, ncols);
+    if (t == 0) umma::mbar_wait(&fin, 0, P.err);  // every MMA of this CTA has completed
+    epi_bar();
+    if (t < 32) umma::tmem_dealloc(tbase, 2 * nc);
 }
+
+__global__ void __launch_bounds__(S3_THREADS, 1) k_stage3(SplitDev P, FitIO F) {
+    if (!cta_has_live_tile(P, P.P / unit_slots(P.G1, P.G2), unit_slots(P.G1, P.G2))) return;
+    stage3_body(P, F, StaticUnits{});
+}
+
 
 // ----------------------------------------------------------- stage 4 -------
 // Blur along the second index, transposed so that one pixel column lands in
@@ -1157,24 +1497,19 @@ __device__ __forceinline__ double warp_reduce_scatter32(double (&v)[32], int lan
 }
 
 constexpr int NSUM = NRED + 1;  // sums per slot: NRED + the non-positive-model flag
-constexpr int S5_THREADS = 128;
-constexpr int S5_SLOTS = S5_THREADS / 32;  // one warp per slot
 constexpr int S5_UNROLL = 4;               // pixels per lane whose loads are in flight together
 
-// One warp per slot: likelihood sums at the trial point (per-pixel terms in
-// FP32; the likelihood and gradient with Kahan compensation, the Hessian and
-// Fisher terms plain; lane partials combined in FP64), written to P.sums for
-// the LM step (k_lm).
-__global__ void __launch_bounds__(S5_THREADS) k_stage5(SplitDev P, const float* rois, const float* scmos) {
+// One warp, one slot: likelihood sums at the trial point from the slot's four
+// blurred maps T0 (map m at T0 + m R^2, row-major) (per-pixel terms in FP32;
+// the likelihood and gradient with Kahan compensation, the Hessian and Fisher
+// terms plain; lane partials combined in FP64), written to P.sums for the LM
+// step.  Used for ROIs below 33 px, whose maps sit in shared memory.
+__device__ __noinline__ void slot_sums_warp(const SplitDev& P, const FitIO& F, int slot, const float* T0) {
     const int lane = threadIdx.x & 31;
-    const int slot = blockIdx.x * S5_SLOTS + (threadIdx.x >> 5);
-    if (slot >= P.P) return;
     const int roi = P.slot_roi[slot];
-    if (roi < 0) return;
     const int R = P.R, RR = R * R;
-    const float* T0 = P.tmaps + (size_t)slot * 4 * RR;
-    const float* d = rois + (size_t)roi * RR;
-    const float* sv = scmos ? scmos + (size_t)roi * RR : nullptr;  // sCMOS var/gain^2 (Localization.java:1132)
+    const float* d = F.rois + (size_t)roi * RR;
+    const float* sv = F.scmos ? F.scmos + (size_t)roi * RR : nullptr;  // sCMOS var/gain^2 (Localization.java:1132)
     // normalisation sums.  Each lane walks its pixels k = lane, lane + 32, ...
     // in order; the loads of S5_UNROLL consecutive pixels are issued together
     // so that several memory round trips overlap.
@@ -1268,275 +1603,14 @@ __global__ void __launch_bounds__(S5_THREADS) k_stage5(SplitDev P, const float* 
     out[NRED] = anybad ? 1.0 : 0.0;
 }
 
-// ---------------------------------- stages 4 + 5 sums (persistent) -----
-// One CTA per SM walks the occupied slots.  The column blur is computed
-// transposed, T^T[j'][(map, i')] = sum_j G[j'][j] J[(map, i')][j] (A = G
-// padded to 128 rows, resident in shared memory; B = the slot's J, N = 4 RP,
-// streamed in K-slabs by a producer warp; three FP16 products per K step
-// issued by an MMA warp into one of two TMEM buffers), so TMEM lane j' holds
-// all four maps of pixel column j'.  The epilogue warps read them straight
-// from TMEM and form the normalisation, likelihood, gradient, Gauss-Newton
-// Hessian and Fisher sums (process/cpu/Localization.java:1125-1143 with the
-// Jacobian of psi = |T|/sum|T| of PSFPhase.java:602-629): per-pixel terms in
-// FP32 (a thread sums a few pixels), thread partials combined in FP64.  The
-// next slot's MMAs run in the other TMEM buffer meanwhile.  The sums and a non-positive-model flag go to P.sums; k_lm
-// applies the FP64 LM step.
-constexpr int E45_THREADS = 384;                 // 12 epilogue warps: three per TMEM lane quadrant
-constexpr int S45_THREADS = E45_THREADS + 64;    // + producer warp + MMA warp
-constexpr int S45_NBUF = 4;
-// ROI side from which the fused form is faster.  The choice depends on R only,
-// never on the batch, so a ROI's fit is the same bit for bit in any batch.
-constexpr int S45_MIN_R = 40;
-
-__host__ __device__ inline size_t s45_roi_bytes(int R) { return ((size_t)R * R * 4 + 127) / 128 * 128; }
-
-
-__global__ void __launch_bounds__(S45_THREADS, 1) k_stage45p(SplitDev P, const float* rois, const float* scmos) {
-    extern __shared__ __align__(1024) char smem[];
-    const int W = P.W, RP = P.RP, R = P.R, NT = 4 * RP, RR = R * R, t = threadIdx.x;
-    const int warp = t >> 5, lane = t & 31, NS4 = W / 16;
-    const uint32_t garr = 128u * W * 2, kslab = 32u * NT, ringb = 2 * kslab, roib = (uint32_t)s45_roi_bytes(R);
-    char* G = smem;                      // G hi, lo
-    char* RG = G + 2 * garr;             // ring of J K-slabs (hi, lo)
-    char* RO = RG + S45_NBUF * ringb;    // two buffers of (ROI, sCMOS variance)
-    float* Tm = (float*)(RO + 4 * roib); // the slot's four FP32 maps, row stride RS
-    const int RS = tm_stride(R), MS = R * RS;
-    const bool vec = (R % 2) == 0;       // whole 16-byte units: ROI copies by TMA
-    __shared__ __align__(8) uint64_t gfull, full[S45_NBUF], freed[S45_NBUF], acc[2], tfree[2], rfull[2], rfree[2], fin;
-    __shared__ uint32_t tmem_base;
-    __shared__ double red[E45_THREADS / 32][NRED];
-    __shared__ int bad_w[E45_THREADS / 32];
-    const int ncols = tmem_cols_pow2(2 * NT);
-    if (!cta_has_live_tile(P, P.P, 1)) return;
-    if (t < 32) umma::tmem_alloc(&tmem_base, ncols);
-    if (t == 0) {
-        umma::mbar_init(&gfull, 1);
-        for (int b = 0; b < S45_NBUF; ++b) { umma::mbar_init(&full[b], 1); umma::mbar_init(&freed[b], 1); }
-        for (int b = 0; b < 2; ++b) {
-            umma::mbar_init(&acc[b], 1);
-            umma::mbar_init(&tfree[b], E45_THREADS / 32);
-            umma::mbar_init(&rfull[b], 1);
-            umma::mbar_init(&rfree[b], E45_THREADS / 32);
-        }
-        umma::mbar_init(&fin, 1);
-        umma::mbar_fence_init();
-    }
-    __syncthreads();
-    umma::fence_after_sync();
-    const uint32_t tbase = tmem_base;
-
-    if (warp == E45_THREADS / 32) {  // ---------------- producer
-        if (lane != 0) return;
-        umma::mbar_expect_tx(&gfull, 2 * garr);
-        umma::bulk_g2s(G, P.g128_hi, garr, &gfull);
-        umma::bulk_g2s(G + garr, P.g128_lo, garr, &gfull);
-        int q = 0, n = 0;
-        bool ok = true;
-        for (int slot = blockIdx.x; slot < P.P && ok; slot += gridDim.x) {
-            const int roi = P.slot_roi[slot];
-            if (roi < 0) continue;
-            const int b = n & 1;
-            if (vec) {
-                if (n >= 2 && !umma::mbar_wait(&rfree[b], (uint32_t)(((n >> 1) - 1) & 1), P.err)) break;
-                char* dst = RO + b * 2 * roib;
-                umma::mbar_expect_tx(&rfull[b], (scmos ? 2u : 1u) * RR * 4);
-                umma::bulk_g2s(dst, rois + (size_t)roi * RR, RR * 4, &rfull[b]);
-                if (scmos) umma::bulk_g2s(dst + roib, scmos + (size_t)roi * RR, RR * 4, &rfull[b]);
-            }
-            ++n;
-            const char* src = P.a4 + (size_t)slot * a4_slot_bytes(W, RP);
-            for (int s = 0; s < NS4; ++s, ++q) {
-                const int buf = q % S45_NBUF;
-                if (q >= S45_NBUF && !umma::mbar_wait(&freed[buf], (uint32_t)((q / S45_NBUF - 1) & 1), P.err)) {
-                    ok = false;
-                    break;
-                }
-                umma::mbar_expect_tx(&full[buf], ringb);
-                umma::bulk_g2s(RG + buf * ringb, src + (size_t)s * kslab, kslab, &full[buf]);
-                umma::bulk_g2s(RG + buf * ringb + kslab, src + (size_t)NT * W * 2 + (size_t)s * kslab, kslab, &full[buf]);
-            }
-        }
-        // copies still in flight land before the CTA can exit
-        umma::mbar_wait(&gfull, 0, P.err);
-        for (int j = q > S45_NBUF ? q - S45_NBUF : 0; j < q; ++j)
-            umma::mbar_wait(&full[j % S45_NBUF], (uint32_t)((j / S45_NBUF) & 1), P.err);
-        if (vec)
-            for (int m = n > 2 ? n - 2 : 0; m < n; ++m) umma::mbar_wait(&rfull[m & 1], (uint32_t)((m >> 1) & 1), P.err);
-        return;
-    }
-    if (warp == E45_THREADS / 32 + 1) {  // ---------------- MMA issuer
-        if (lane != 0) return;
-        const uint32_t id = umma::idesc_f16(128, NT, false, true);
-        const uint32_t sbo_g = (W / 8) * 128, lbo_j = (NT / 8) * 128;
-        const uint32_t ghi = umma::smem_u32(G), glo = ghi + garr;
-        bool ok = umma::mbar_wait(&gfull, 0, P.err);
-        int q = 0, n = 0;
-        for (int slot = blockIdx.x; slot < P.P && ok; slot += gridDim.x) {
-            if (P.slot_roi[slot] < 0) continue;
-            const int b = n & 1;
-            if (n >= 2 && !umma::mbar_wait(&tfree[b], (uint32_t)(((n >> 1) - 1) & 1), P.err)) break;
-            umma::fence_after_sync();
-            const uint32_t td = tbase + b * NT;
-            for (int s = 0; s < NS4; ++s, ++q) {
-                const int buf = q % S45_NBUF;
-                if (!umma::mbar_wait(&full[buf], (uint32_t)((q / S45_NBUF) & 1), P.err)) { ok = false; break; }
-                umma::fence_after_sync();
-                const uint32_t jhi = umma::smem_u32(RG + buf * ringb), jlo = jhi + kslab;
-                const uint64_t gh = umma::smem_desc(ghi + s * 256, 128, sbo_g), gl = umma::smem_desc(glo + s * 256, 128, sbo_g);
-                const uint64_t bh = umma::smem_desc(jhi, lbo_j, 128), bl = umma::smem_desc(jlo, lbo_j, 128);
-                umma::mma_f16(td, gh, bh, id, s > 0 ? 1u : 0u);
-                umma::mma_f16(td, gl, bh, id, 1u);
-                umma::mma_f16(td, gh, bl, id, 1u);
-                umma::mma_commit(&freed[buf]);
-            }
-            umma::mma_commit(&acc[b]);
-            ++n;
-        }
-        umma::mma_commit(&fin);
-        return;
-    }
-
-    // ---------------- epilogue warps.  The maps go from TMEM (lane = pixel column j') to
-    // shared memory, which frees the TMEM buffer for the slot after next; the pixel sums
-    // then run over all epilogue threads.
-    const int jp = (warp & 3) * 32 + lane, wg = warp >> 2;
-    constexpr int NWG = E45_THREADS / 128, NW = E45_THREADS / 32;
-    int n = 0;
-    for (int slot = blockIdx.x; slot < P.P; slot += gridDim.x) {
-        const int roi = P.slot_roi[slot];
-        if (roi < 0) continue;
-        const int b = n & 1;
-        const uint32_t ph = (uint32_t)((n >> 1) & 1);
-        ++n;
-        umma::mbar_wait(&acc[b], ph, P.err);
-        umma::fence_after_sync();
-        const uint32_t tb = tbase + b * NT;
-        // the normalisation sums accumulate over the values this thread copies
-        float ns[4] = {0, 0, 0, 0};
-        for (int c0 = 4 * wg; c0 < RP; c0 += 4 * NWG) {
-            uint32_t r[4][4];
-#pragma unroll
-            for (int m = 0; m < 4; ++m) umma::tmem_ld4_nw(tmem_lane_addr(tb, m * RP + c0), r[m]);
-            umma::tmem_wait_ld();
-#pragma unroll
-            for (int m = 0; m < 4; ++m)
-#pragma unroll
-                for (int u = 0; u < 4; ++u) asm volatile("" : "+r"(r[m][u]));
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                if (jp >= R || c0 + u >= R) continue;
-                float v[4];
-#pragma unroll
-                for (int m = 0; m < 4; ++m) {
-                    v[m] = __uint_as_float(r[m][u]) * P.sc.cT[m];
-                    Tm[m * MS + (c0 + u) * RS + jp] = v[m];
-                }
-                const float sg = v[0] < 0 ? -1.f : 1.f;
-                ns[0] += fabsf(v[0]);
-                ns[1] += sg * v[1];
-                ns[2] += sg * v[2];
-                ns[3] += sg * v[3];
-            }
-        }
-        umma::fence_before_sync();
-        warp_arrive(&tfree[b]);
-        if (vec) umma::mbar_wait(&rfull[b], ph, P.err);
-        {
-            const double v0 = warp_sum(ns[0]), v1 = warp_sum(ns[1]), v2 = warp_sum(ns[2]), v3 = warp_sum(ns[3]);
-            if (lane == 0) { red[warp][0] = v0; red[warp][1] = v1; red[warp][2] = v2; red[warp][3] = v3; }
-        }
-        epi_bar<E45_THREADS>();
-        double sum4[4] = {0, 0, 0, 0};
-        for (int w = 0; w < NW; ++w)
-            for (int q = 0; q < 4; ++q) sum4[q] += red[w][q];
-        epi_bar<E45_THREADS>();
-        const float S = (float)sum4[0], Dx = (float)sum4[1], Dy = (float)sum4[2], Dz = (float)sum4[3];
-        const float invS = 1.f / S;
-        const double* th = P.lm[slot].trial;
-        const float A = (float)th[3], B = (float)th[4];
-        const float* d = vec ? (const float*)(RO + b * 2 * roib) : rois + (size_t)roi * RR;
-        const float* sv = !scmos ? nullptr : vec ? (const float*)(RO + b * 2 * roib + roib) : scmos + (size_t)roi * RR;
-        // a thread sums about RR / 384 pixels before the FP64 combination across threads,
-        // so plain FP32 partials suffice here
-        float sg6[6], sh[30];
-#pragma unroll
-        for (int k = 0; k < 6; ++k) sg6[k] = 0.f;
-#pragma unroll
-        for (int k = 0; k < 30; ++k) sh[k] = 0.f;
-        bool bad = false;
-#pragma unroll 2
-        for (int k = t; k < RR; k += E45_THREADS) {
-            const int ip = k / R, to = ip * RS + (k - ip * R);
-            const float v = Tm[to], sgn = v < 0 ? -1.f : 1.f, psi = fabsf(v) * invS;
-            float jv[5];
-            jv[0] = A * (sgn * Tm[MS + to] - psi * Dx) * invS;
-            jv[1] = A * (sgn * Tm[2 * MS + to] - psi * Dy) * invS;
-            jv[2] = A * (sgn * Tm[3 * MS + to] - psi * Dz) * invS;
-            jv[3] = psi;
-            jv[4] = 1.f;
-            const float mu = A * psi + B + (sv ? sv[k] : 0.f);
-            if (!(mu > 0.f)) { bad = true; continue; }
-            const float dk = d[k];
-            sg6[0] += dk > 0.f ? mu - dk - dk * logf(mu / dk) : mu;
-            const float wf = 1.f / mu, wgt = 1.f - dk * wf, wh = dk * wf * wf;
-#pragma unroll
-            for (int q = 0; q < 5; ++q) sg6[1 + q] += wgt * jv[q];
-            int o = 0;
-#pragma unroll
-            for (int q = 0; q < 5; ++q)
-#pragma unroll
-                for (int r2 = 0; r2 <= q; ++r2) {
-                    sh[o] += wh * jv[q] * jv[r2];
-                    sh[o + 15] += wf * jv[q] * jv[r2];
-                    ++o;
-                }
-        }
-        if (vec) warp_arrive(&rfree[b]);  // this slot's ROI buffer is free for the slot after next
-        // 36 sums per thread -> per warp: a butterfly reduce-scatter leaves sum k on lane k
-        // (k < 32); the last four reduce plainly
-        {
-            double v[32];
-#pragma unroll
-            for (int k = 0; k < 6; ++k) v[k] = sg6[k];
-#pragma unroll
-            for (int k = 0; k < 26; ++k) v[6 + k] = sh[k];
-            red[warp][lane] = warp_reduce_scatter32(v, lane);
-#pragma unroll
-            for (int k = 26; k < 30; ++k) {
-                const double x = warp_sum((double)sh[k]);
-                if (lane == 0) red[warp][6 + k] = x;
-            }
-        }
-        const bool wbad = __any_sync(0xffffffffu, bad);
-        if (lane == 0) bad_w[warp] = wbad;
-        epi_bar<E45_THREADS>();
-        if (t < NRED) {
-            double v = 0;
-            for (int w = 0; w < NW; ++w) v += red[w][t];
-            P.sums[(size_t)slot * NSUM + t] = v;
-        }
-        if (t == NRED) {
-            int any = 0;
-            for (int w = 0; w < NW; ++w) any |= bad_w[w];
-            P.sums[(size_t)slot * NSUM + NRED] = any ? 1.0 : 0.0;
-        }
-        // (a bounded wait that gave up makes every epilogue thread leave the loop together)
-        if (epi_bar_or<E45_THREADS>(t == 0 && *(volatile int*)P.err != 0)) break;
-    }
-    if (t == 0) umma::mbar_wait(&fin, 0, P.err);  // every MMA of this CTA has completed
-    epi_bar<E45_THREADS>();
-    if (t < 32) umma::tmem_dealloc(tbase, ncols);
-}
-
-// The FP64 LM step of every occupied slot from its sums (one thread per slot):
-// start or update the damped Gauss-Newton iteration, propose the next trial
-// point, or retire the ROI and refill the slot from the queue.
-__global__ void k_lm(SplitDev P, const double* init, int n, FitParamsDev prm, double* out5, double* crlb5,
-                     double* nll_out, int* st_out, int* it_out) {
-    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= P.P) return;
+// The FP64 LM step of one slot from its sums: start or update the damped
+// Gauss-Newton iteration, propose the next trial point, or retire the ROI and
+// refill the slot from the queue.
+__device__ __noinline__ void lm_slot(const SplitDev& P, const FitIO& io, int slot) {
+    const FitParamsDev& prm = io.prm;
     const int roi = P.slot_roi[slot];
     if (roi < 0) return;
+    if (P.evals) atomicAdd(P.evals, 1ull);
     const double* tot = P.sums + (size_t)slot * NSUM;
     double nll = tot[NRED] != 0.0 ? INFINITY : tot[0], g[5], H[25], F[25];
     for (int q = 0; q < 5; ++q) g[q] = tot[1 + q];
@@ -1560,24 +1634,461 @@ __global__ void k_lm(SplitDev P, const double* init, int n, FitParamsDev prm, do
     P.lm[slot] = st;
     if (more) return;
     // retire
-    for (int q = 0; q < 5; ++q) out5[5 * roi + q] = st.th[q];
-    if (nll_out) nll_out[roi] = st.nll;
-    if (st_out) st_out[roi] = st.status;
-    if (it_out) it_out[roi] = st.evals;
-    if (crlb5) lm_crlb(st.F, crlb5 + 5 * roi);
+    for (int q = 0; q < 5; ++q) io.out5[5 * roi + q] = st.th[q];
+    if (io.nll) io.nll[roi] = st.nll;
+    if (io.status) io.status[roi] = st.status;
+    if (io.iters) io.iters[roi] = st.evals;
+    if (io.crlb5) lm_crlb(st.F, io.crlb5 + 5 * roi);
     // refill from the queue
-    const int next = take_roi(P, n);
+    const int next = take_roi(P, io.n);
     if (next >= 0) {
-        P.slot_roi[slot] = next;
-        P.slot_phase[slot] = 0;
-        double* tr = P.lm[slot].trial;
-        for (int q = 0; q < 5; ++q) tr[q] = init[5 * next + q];
-        lm_clamp(tr, prm);
+        slot_take(P, io, slot, next);
     } else {
         P.slot_roi[slot] = -1;
         atomicSub(P.active, 1);
     }
 }
+
+// ---------------------------------- stages 4 + 5 sums (persistent) -----
+// ROIs of 33 px and more (window 128).  One CTA per SM walks the occupied slots.  The column blur is computed
+// transposed, T^T[j'][(map, i')] = sum_j G[j'][j] J[(map, i')][j] (A = G
+// padded to 128 rows, resident in shared memory; B = the slot's J, N = 4 RP,
+// streamed in K-slabs by a producer warp; three FP16 products per K step
+// issued by an MMA warp into one of two TMEM buffers), so TMEM lane j' holds
+// all four maps of pixel column j'.  The epilogue warps read them straight
+// from TMEM and form the normalisation, likelihood, gradient, Gauss-Newton
+// Hessian and Fisher sums (process/cpu/Localization.java:1125-1143 with the
+// Jacobian of psi = |T|/sum|T| of PSFPhase.java:602-629): per-pixel terms in
+// FP32 (a thread sums a few pixels), thread partials combined in FP64.  The
+// next slot's MMAs run in the other TMEM buffer meanwhile.  The sums and a
+// non-positive-model flag go to P.sums; once a unit's slots are summed, one
+// lane per slot applies the FP64 LM step.
+constexpr int E45_THREADS = 384;                 // 12 epilogue warps: three per TMEM lane quadrant
+constexpr int S45_THREADS = E45_THREADS + 64;    // + producer warp + MMA warp
+constexpr int S45_NBUF = 4;
+// ROIs whose window is 128 take this kernel, smaller ones the warp-per-slot
+// sums (stage45s).  The choice depends on R only, never on the batch, so a
+// ROI's fit is the same bit for bit in any batch.
+constexpr int S45_MIN_W = 128;
+
+__host__ __device__ inline size_t s45_roi_bytes(int R) { return ((size_t)R * R * 4 + 127) / 128 * 128; }
+
+
+template <class UNITS>
+__device__ __forceinline__ void stage45_body(const SplitDev& P, const FitIO& F, UNITS units) {
+    extern __shared__ __align__(1024) char smem[];
+    const int W = P.W, RP = P.RP, R = P.R, NT = 4 * RP, RR = R * R, t = threadIdx.x;
+    const int warp = t >> 5, lane = t & 31, NS4 = W / 16, UG = unit_slots(P.G1, P.G2);
+    const float* rois = F.rois;
+    const float* scmos = F.scmos;
+    if (t >= S45_THREADS) {  // (a dataflow CTA has more threads than this stage uses)
+        __syncthreads();
+        return;
+    }
+    const uint32_t garr = 128u * W * 2, kslab = 32u * NT, ringb = 2 * kslab, roib = (uint32_t)s45_roi_bytes(R);
+    char* G = smem;                      // G hi, lo
+    char* RG = G + 2 * garr;             // ring of J K-slabs (hi, lo)
+    char* RO = RG + S45_NBUF * ringb;    // two buffers of (ROI, sCMOS variance)
+    float* Tm = (float*)(RO + 4 * roib); // the slot's four FP32 maps, row stride RS
+    const int RS = tm_stride(R), MS = R * RS;
+    double (*red)[NRED] = (double (*)[NRED])(((uintptr_t)(Tm + 4 * MS) + 15) & ~(uintptr_t)15);  // per-warp sums
+    int* bad_w = (int*)(red + E45_THREADS / 32);
+    const bool vec = (R % 2) == 0;       // whole 16-byte units: ROI copies by TMA
+    __shared__ __align__(8) uint64_t gfull, full[S45_NBUF], freed[S45_NBUF], acc[2], tfree[2], rfull[2], rfree[2], fin;
+    __shared__ uint32_t tmem_base;
+    const int ncols = tmem_cols_pow2(2 * NT);
+    if (t < 32) umma::tmem_alloc(&tmem_base, ncols);
+    if (t == 0) {
+        umma::mbar_init(&gfull, 1);
+        for (int b = 0; b < S45_NBUF; ++b) { umma::mbar_init(&full[b], 1); umma::mbar_init(&freed[b], 1); }
+        for (int b = 0; b < 2; ++b) {
+            umma::mbar_init(&acc[b], 1);
+            umma::mbar_init(&tfree[b], E45_THREADS / 32);
+            umma::mbar_init(&rfull[b], 1);
+            umma::mbar_init(&rfree[b], E45_THREADS / 32);
+        }
+        umma::mbar_init(&fin, 1);
+        umma::mbar_fence_init();
+    }
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tbase = tmem_base;
+
+    if (warp == E45_THREADS / 32) {  // ---------------- producer (lane 0), scheduler (lane 1)
+        if constexpr (UNITS::flow)
+            if (lane == 1) {
+                units.schedule(P, F);
+                return;
+            }
+        if (lane != 0) return;
+        umma::mbar_expect_tx(&gfull, 2 * garr);
+        umma::bulk_g2s(G, P.g128_hi, garr, &gfull);
+        umma::bulk_g2s(G + garr, P.g128_lo, garr, &gfull);
+        int q = 0, n = 0;
+        bool ok = true;
+        for (int tag = 0; ok;) {
+            const int unit = units.next(P, tag, true);
+            if (unit < 0) break;
+            for (int slot = unit * UG; slot < (unit + 1) * UG && ok; ++slot) {
+                const int roi = P.slot_roi[slot];
+                if (roi < 0) continue;
+                const int b = n & 1;
+                if (vec) {
+                    if (n >= 2 && !umma::mbar_wait(&rfree[b], (uint32_t)(((n >> 1) - 1) & 1), P.err)) {
+                        ok = false;
+                        break;
+                    }
+                    char* dst = RO + b * 2 * roib;
+                    umma::mbar_expect_tx(&rfull[b], (scmos ? 2u : 1u) * RR * 4);
+                    umma::bulk_g2s(dst, rois + (size_t)roi * RR, RR * 4, &rfull[b]);
+                    if (scmos) umma::bulk_g2s(dst + roib, scmos + (size_t)roi * RR, RR * 4, &rfull[b]);
+                }
+                ++n;
+                const char* src = P.a4 + (size_t)slot * a4_slot_bytes(W, RP);
+                for (int s = 0; s < NS4; ++s, ++q) {
+                    const int buf = q % S45_NBUF;
+                    if (q >= S45_NBUF && !umma::mbar_wait(&freed[buf], (uint32_t)((q / S45_NBUF - 1) & 1), P.err)) {
+                        ok = false;
+                        break;
+                    }
+                    umma::mbar_expect_tx(&full[buf], ringb);
+                    umma::bulk_g2s(RG + buf * ringb, src + (size_t)s * kslab, kslab, &full[buf]);
+                    umma::bulk_g2s(RG + buf * ringb + kslab, src + (size_t)NT * W * 2 + (size_t)s * kslab, kslab, &full[buf]);
+                }
+            }
+        }
+        // copies still in flight land before the CTA can exit
+        umma::mbar_wait(&gfull, 0, P.err);
+        for (int j = q > S45_NBUF ? q - S45_NBUF : 0; j < q; ++j)
+            umma::mbar_wait(&full[j % S45_NBUF], (uint32_t)((j / S45_NBUF) & 1), P.err);
+        if (vec)
+            for (int m = n > 2 ? n - 2 : 0; m < n; ++m) umma::mbar_wait(&rfull[m & 1], (uint32_t)((m >> 1) & 1), P.err);
+        return;
+    }
+    if (warp == E45_THREADS / 32 + 1) {  // ---------------- MMA issuer (lane 0)
+        if (lane != 0) return;
+        const uint32_t id = umma::idesc_f16(128, NT, false, true);
+        const uint32_t sbo_g = (W / 8) * 128, lbo_j = (NT / 8) * 128;
+        const uint32_t ghi = umma::smem_u32(G), glo = ghi + garr;
+        bool ok = umma::mbar_wait(&gfull, 0, P.err);
+        int q = 0, n = 0;
+        for (int tag = 0; ok;) {
+            const int unit = units.next(P, tag, true);
+            if (unit < 0) break;
+            for (int slot = unit * UG; slot < (unit + 1) * UG && ok; ++slot) {
+                if (P.slot_roi[slot] < 0) continue;
+                const int b = n & 1;
+                if (n >= 2 && !umma::mbar_wait(&tfree[b], (uint32_t)(((n >> 1) - 1) & 1), P.err)) {
+                    ok = false;
+                    break;
+                }
+                umma::fence_after_sync();
+                const uint32_t td = tbase + b * NT;
+                for (int s = 0; s < NS4; ++s, ++q) {
+                    const int buf = q % S45_NBUF;
+                    if (!umma::mbar_wait(&full[buf], (uint32_t)((q / S45_NBUF) & 1), P.err)) { ok = false; break; }
+                    umma::fence_after_sync();
+                    const uint32_t jhi = umma::smem_u32(RG + buf * ringb), jlo = jhi + kslab;
+                    const uint64_t gh = umma::smem_desc(ghi + s * 256, 128, sbo_g), gl = umma::smem_desc(glo + s * 256, 128, sbo_g);
+                    const uint64_t bh = umma::smem_desc(jhi, lbo_j, 128), bl = umma::smem_desc(jlo, lbo_j, 128);
+                    umma::mma_f16(td, gh, bh, id, s > 0 ? 1u : 0u);
+                    umma::mma_f16(td, gl, bh, id, 1u);
+                    umma::mma_f16(td, gh, bl, id, 1u);
+                    umma::mma_commit(&freed[buf]);
+                }
+                umma::mma_commit(&acc[b]);
+                ++n;
+            }
+        }
+        umma::mma_commit(&fin);
+        return;
+    }
+
+    // ---------------- epilogue warps.  The maps go from TMEM (lane = pixel column j') to
+    // shared memory, which frees the TMEM buffer for the slot after next; the pixel sums
+    // then run over all epilogue threads.
+    const int jp = (warp & 3) * 32 + lane, wg = warp >> 2;
+    constexpr int NWG = E45_THREADS / 128, NW = E45_THREADS / 32;
+    int n = 0;
+    bool abort = false;
+    for (int tag = 0; !abort;) {
+        const int unit = units.next(P, tag);
+        if (unit < 0) break;
+        for (int slot = unit * UG; slot < (unit + 1) * UG; ++slot) {
+            const int roi = P.slot_roi[slot];
+            if (roi < 0) continue;
+            const int b = n & 1;
+            const uint32_t ph = (uint32_t)((n >> 1) & 1);
+            ++n;
+            umma::mbar_wait(&acc[b], ph, P.err);
+            umma::fence_after_sync();
+            const uint32_t tb = tbase + b * NT;
+            // the normalisation sums accumulate over the values this thread copies
+            float ns[4] = {0, 0, 0, 0};
+            for (int c0 = 4 * wg; c0 < RP; c0 += 4 * NWG) {
+                uint32_t r[4][4];
+#pragma unroll
+                for (int m = 0; m < 4; ++m) umma::tmem_ld4_nw(tmem_lane_addr(tb, m * RP + c0), r[m]);
+                umma::tmem_wait_ld();
+#pragma unroll
+                for (int m = 0; m < 4; ++m)
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) asm volatile("" : "+r"(r[m][u]));
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    if (jp >= R || c0 + u >= R) continue;
+                    float v[4];
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) {
+                        v[m] = __uint_as_float(r[m][u]) * P.sc.cT[m];
+                        Tm[m * MS + (c0 + u) * RS + jp] = v[m];
+                    }
+                    const float sg = v[0] < 0 ? -1.f : 1.f;
+                    ns[0] += fabsf(v[0]);
+                    ns[1] += sg * v[1];
+                    ns[2] += sg * v[2];
+                    ns[3] += sg * v[3];
+                }
+            }
+            umma::fence_before_sync();
+            warp_arrive(&tfree[b]);
+            if (vec) umma::mbar_wait(&rfull[b], ph, P.err);
+            {
+                const double v0 = warp_sum(ns[0]), v1 = warp_sum(ns[1]), v2 = warp_sum(ns[2]), v3 = warp_sum(ns[3]);
+                if (lane == 0) { red[warp][0] = v0; red[warp][1] = v1; red[warp][2] = v2; red[warp][3] = v3; }
+            }
+            epi_bar<E45_THREADS>();
+            double sum4[4] = {0, 0, 0, 0};
+            for (int w = 0; w < NW; ++w)
+                for (int q = 0; q < 4; ++q) sum4[q] += red[w][q];
+            epi_bar<E45_THREADS>();
+            const float S = (float)sum4[0], Dx = (float)sum4[1], Dy = (float)sum4[2], Dz = (float)sum4[3];
+            const float invS = 1.f / S;
+            const double* th = P.lm[slot].trial;
+            const float A = (float)th[3], B = (float)th[4];
+            const float* d = vec ? (const float*)(RO + b * 2 * roib) : rois + (size_t)roi * RR;
+            const float* sv = !scmos ? nullptr : vec ? (const float*)(RO + b * 2 * roib + roib) : scmos + (size_t)roi * RR;
+            // a thread sums about RR / 384 pixels before the FP64 combination across threads,
+            // so plain FP32 partials suffice here
+            float sg6[6], sh[30];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) sg6[k] = 0.f;
+#pragma unroll
+            for (int k = 0; k < 30; ++k) sh[k] = 0.f;
+            bool bad = false;
+#pragma unroll 2
+            for (int k = t; k < RR; k += E45_THREADS) {
+                const int ip = k / R, to = ip * RS + (k - ip * R);
+                const float v = Tm[to], sgn = v < 0 ? -1.f : 1.f, psi = fabsf(v) * invS;
+                float jv[5];
+                jv[0] = A * (sgn * Tm[MS + to] - psi * Dx) * invS;
+                jv[1] = A * (sgn * Tm[2 * MS + to] - psi * Dy) * invS;
+                jv[2] = A * (sgn * Tm[3 * MS + to] - psi * Dz) * invS;
+                jv[3] = psi;
+                jv[4] = 1.f;
+                const float mu = A * psi + B + (sv ? sv[k] : 0.f);
+                if (!(mu > 0.f)) { bad = true; continue; }
+                const float dk = d[k];
+                sg6[0] += dk > 0.f ? mu - dk - dk * logf(mu / dk) : mu;
+                const float wf = 1.f / mu, wgt = 1.f - dk * wf, wh = dk * wf * wf;
+#pragma unroll
+                for (int q = 0; q < 5; ++q) sg6[1 + q] += wgt * jv[q];
+                int o = 0;
+#pragma unroll
+                for (int q = 0; q < 5; ++q)
+#pragma unroll
+                    for (int r2 = 0; r2 <= q; ++r2) {
+                        sh[o] += wh * jv[q] * jv[r2];
+                        sh[o + 15] += wf * jv[q] * jv[r2];
+                        ++o;
+                    }
+            }
+            if (vec) warp_arrive(&rfree[b]);  // this slot's ROI buffer is free for the slot after next
+            // 36 sums per thread -> per warp: a butterfly reduce-scatter leaves sum k on lane k
+            // (k < 32); the last four reduce plainly
+            {
+                double v[32];
+#pragma unroll
+                for (int k = 0; k < 6; ++k) v[k] = sg6[k];
+#pragma unroll
+                for (int k = 0; k < 26; ++k) v[6 + k] = sh[k];
+                red[warp][lane] = warp_reduce_scatter32(v, lane);
+#pragma unroll
+                for (int k = 26; k < 30; ++k) {
+                    const double x = warp_sum((double)sh[k]);
+                    if (lane == 0) red[warp][6 + k] = x;
+                }
+            }
+            const bool wbad = __any_sync(0xffffffffu, bad);
+            if (lane == 0) bad_w[warp] = wbad;
+            epi_bar<E45_THREADS>();
+            if (t < NRED) {
+                double v = 0;
+                for (int w = 0; w < NW; ++w) v += red[w][t];
+                P.sums[(size_t)slot * NSUM + t] = v;
+            }
+            if (t == NRED) {
+                int any = 0;
+                for (int w = 0; w < NW; ++w) any |= bad_w[w];
+                P.sums[(size_t)slot * NSUM + NRED] = any ? 1.0 : 0.0;
+            }
+            // (a bounded wait that gave up makes every epilogue thread leave the loop together)
+            if (epi_bar_or<E45_THREADS>(t == 0 && *(volatile int*)P.err != 0)) {
+                abort = true;
+                break;
+            }
+        }
+        if (abort) break;
+        // the unit's LM steps, one lane per slot, then its next state
+        if (warp == 0 && lane < UG) lm_slot(P, F, unit * UG + lane);
+        epi_bar<E45_THREADS>();
+        if (t == 0) units.release(P, unit, unit_after_lm(P, F, unit, tag));
+    }
+    if (t == 0) umma::mbar_wait(&fin, 0, P.err);  // every MMA of this CTA has completed
+    epi_bar<E45_THREADS>();
+    if (t < 32) umma::tmem_dealloc(tbase, ncols);
+}
+
+__global__ void __launch_bounds__(S45_THREADS, 1) k_stage45p(SplitDev P, FitIO F) {
+    if (!cta_has_live_tile(P, P.P / unit_slots(P.G1, P.G2), unit_slots(P.G1, P.G2))) return;
+    stage45_body(P, F, StaticUnits{});
+}
+
+// ------------------------------ stages 4 + 5 for small ROIs (persistent) -----
+// ROIs whose window is 32 or 64.  One CTA per SM walks the units: warp 16
+// loads a unit's row-blurred maps J (hi, lo; all UG slots at once) into one
+// of two buffers and issues the column blur of each live slot,
+// T^T[j'][(map, i')] = sum_j G[j'][j] J[(map, i')][j] (A = G padded to 128
+// rows, resident), into one of two TMEM accumulators.  The epilogue warps copy
+// the maps to shared memory (lane = pixel column j', warpgroup = map), then
+// one warp per slot forms the likelihood sums (slot_sums_warp) and one lane
+// per slot applies the FP64 LM step.
+constexpr int S45S_THREADS = SPLIT_THREADS + 32;
+
+__host__ __device__ inline size_t s45s_smem(int W, int RP, int R, int UG, int nb) {
+    return (size_t)2 * 128 * W * 2 + (size_t)nb * UG * a4_slot_bytes(W, RP) + (size_t)UG * 4 * R * R * 4;
+}
+// J buffers and TMEM accumulators: two when they fit (the next unit's load and
+// MMAs overlap this unit's epilogue), else one.
+__host__ __device__ inline int s45s_nbuf(int W, int RP, int R, int UG) {
+    return 2 * UG * 4 * RP <= 512 && s45s_smem(W, RP, R, UG, 2) <= 225 * 1024 ? 2 : 1;
+}
+
+template <class UNITS>
+__device__ __forceinline__ void stage45s_body(const SplitDev& P, const FitIO& F, UNITS units) {
+    extern __shared__ __align__(1024) char smem[];
+    const int W = P.W, RP = P.RP, R = P.R, NT = 4 * RP, RR = R * R, t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int UG = unit_slots(P.G1, P.G2);
+    const uint32_t garr = 128u * W * 2, jslot = (uint32_t)a4_slot_bytes(W, RP), jarr = jslot / 2;
+    char* G = smem;                                      // G hi, lo (128 rows, rows >= R zero)
+    const int NB = s45s_nbuf(W, RP, R, UG);
+    char* JB = G + 2 * garr;                             // NB buffers of a unit's J
+    float* Tm = (float*)(JB + (size_t)NB * UG * jslot);  // the unit's maps: slot g, map m at (4 g + m) R^2
+    __shared__ __align__(8) uint64_t gfull, full[2], acc[2], tfree[2], fin;
+    __shared__ uint32_t tmem_base;
+    const int nc = UG * NT;  // TMEM columns of one unit
+    const int ncols = tmem_cols_pow2(NB * nc);
+    if (t < 32) umma::tmem_alloc(&tmem_base, ncols);
+    if (t == 0) {
+        umma::mbar_init(&gfull, 1);
+        for (int b = 0; b < 2; ++b) {
+            umma::mbar_init(&full[b], 1);
+            umma::mbar_init(&acc[b], 1);
+            umma::mbar_init(&tfree[b], SPLIT_THREADS / 32);
+        }
+        umma::mbar_init(&fin, 1);
+        umma::mbar_fence_init();
+    }
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tbase = tmem_base;
+
+    if (warp == SPLIT_THREADS / 32) {  // ---------------- loads + MMAs (lane 0), scheduler (lane 1)
+        if constexpr (UNITS::flow)
+            if (lane == 1) {
+                units.schedule(P, F);
+                return;
+            }
+        if (lane != 0) return;
+        umma::mbar_expect_tx(&gfull, 2 * garr);
+        umma::bulk_g2s(G, P.g128_hi, garr, &gfull);
+        umma::bulk_g2s(G + garr, P.g128_lo, garr, &gfull);
+        bool ok = umma::mbar_wait(&gfull, 0, P.err);
+        const uint32_t id = umma::idesc_f16(128, NT, false, true);
+        const uint32_t ghi = umma::smem_u32(G), glo = ghi + garr;
+        const uint32_t sbo_g = (W / 8) * 128, lbo_j = (NT / 8) * 128, kstep_j = 2 * lbo_j;
+        int n = 0;
+        for (int tag = 0; ok;) {
+            const int unit = units.next(P, tag, true);
+            if (unit < 0) break;
+            const int b = n % NB, use = n / NB;
+            const uint32_t par = (uint32_t)((use - 1) & 1);
+            // buffer b was last used by unit n - NB: its MMAs (and so its J reads) are done
+            // once acc[b] completed, and its accumulator is free once the epilogue read it
+            if (use >= 1 && (!umma::mbar_wait(&acc[b], par, P.err) || !umma::mbar_wait(&tfree[b], par, P.err))) break;
+            char* jb = JB + (size_t)b * UG * jslot;
+            umma::mbar_expect_tx(&full[b], (uint32_t)UG * jslot);
+            umma::bulk_g2s(jb, P.a4 + (size_t)unit * UG * jslot, (uint32_t)UG * jslot, &full[b]);
+            if (!umma::mbar_wait(&full[b], (uint32_t)(use & 1), P.err)) break;
+            umma::fence_after_sync();
+            for (int g = 0; g < UG; ++g) {
+                if (P.slot_roi[unit * UG + g] < 0) continue;
+                const uint32_t td = tbase + (uint32_t)(b * nc + g * NT);
+                const uint32_t jhi = umma::smem_u32(jb + (size_t)g * jslot), jlo = jhi + jarr;
+                mma_chain(td, ghi, 128, sbo_g, 256, jhi, lbo_j, 128, kstep_j, W, id, false);
+                mma_chain(td, glo, 128, sbo_g, 256, jhi, lbo_j, 128, kstep_j, W, id, true);
+                mma_chain(td, ghi, 128, sbo_g, 256, jlo, lbo_j, 128, kstep_j, W, id, true);
+            }
+            umma::mma_commit(&acc[b]);
+            ++n;
+        }
+        umma::mma_commit(&fin);
+        return;
+    }
+
+    // ---------------- epilogue: pixel column j' = TMEM lane, map = warpgroup
+    const int jp = t & 127, map = t >> 7;
+    int n = 0;
+    bool abort = false;
+    for (int tag = 0; !abort;) {
+        const int unit = units.next(P, tag);
+        if (unit < 0) break;
+        const int b = n % NB;
+        umma::mbar_wait(&acc[b], (uint32_t)((n / NB) & 1), P.err);
+        umma::fence_after_sync();
+        ++n;
+        for (int g = 0; g < UG; ++g) {
+            if (P.slot_roi[unit * UG + g] < 0) continue;
+            float* dst = Tm + (size_t)(g * 4 + map) * RR;
+            for (int h = 0; h < RP; h += 4) {
+                float v[4];
+                umma::tmem_ld4(tmem_lane_addr(tbase, b * nc + g * NT + map * RP + h), v);
+                if (jp < R)
+                    for (int u = 0; u < 4 && h + u < R; ++u) dst[(h + u) * R + jp] = v[u] * P.sc.cT[map];
+            }
+        }
+        umma::fence_before_sync();
+        warp_arrive(&tfree[b]);
+        epi_bar();
+        if (warp < UG && P.slot_roi[unit * UG + warp] >= 0) slot_sums_warp(P, F, unit * UG + warp, Tm + (size_t)warp * 4 * RR);
+        // (a bounded wait that gave up makes every epilogue thread leave the loop together)
+        abort = epi_bar_or(t == 0 && *(volatile int*)P.err != 0);
+        if (abort) break;
+        // the unit's LM steps, one lane per slot, then its next state
+        if (warp == 0 && lane < UG) lm_slot(P, F, unit * UG + lane);
+        epi_bar();
+        if (t == 0) units.release(P, unit, unit_after_lm(P, F, unit, tag));
+    }
+    if (t == 0) umma::mbar_wait(&fin, 0, P.err);  // every MMA of this CTA has completed
+    epi_bar();
+    if (t < 32) umma::tmem_dealloc(tbase, ncols);
+}
+
+__global__ void __launch_bounds__(S45S_THREADS, 1) k_stage45s(SplitDev P, FitIO F) {
+    if (!cta_has_live_tile(P, P.P / unit_slots(P.G1, P.G2), unit_slots(P.G1, P.G2))) return;
+    stage45s_body(P, F, StaticUnits{});
+}
+
 
 // ------------------------------------------------- fused stages 2 to 5 ------
 // One CTA per stage-2 tile (G2 slots x W rows j).  The window DFT runs over
@@ -1913,12 +2424,17 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_fused25(SplitDev P, const 
     if (t < 32) umma::tmem_dealloc(tbase, ncols);
 }
 
-// Fill the pool from the queue.
-__global__ void k_init_slots(SplitDev P, const double* init, int n, int navail, FitParamsDev prm) {
+// Fill the pool from the queue.  Units with a ROI are ready for stage 1 of
+// their first evaluation (state 0); units without one are dead unless more
+// ROIs are still to arrive.  avail: the caller's device count of ROIs on the
+// device (P.navail points at it), else navail.
+__global__ void k_init_slots(SplitDev P, const double* init, int n, int navail, FitParamsDev prm,
+                             const int* avail = nullptr) {
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= P.P) return;
-    n = n < navail ? n : navail;
-    if (slot < n) {
+    if (avail) navail = *(volatile const int*)avail;
+    const int m = n < navail ? n : navail;
+    if (slot < m) {
         P.slot_roi[slot] = slot;
         P.slot_phase[slot] = 0;
         for (int q = 0; q < 5; ++q) P.lm[slot].trial[q] = init[5 * slot + q];
@@ -1926,11 +2442,14 @@ __global__ void k_init_slots(SplitDev P, const double* init, int n, int navail, 
     } else {
         P.slot_roi[slot] = -1;
     }
+    const int UG = unit_slots(P.G1, P.G2);
+    if (slot % UG == 0) P.ustate[slot / UG] = slot < m || navail < n ? 0 : UNIT_DEAD;
     if (slot == 0) {
-        *P.queue = P.P < n ? P.P : n;
-        *P.active = P.P < n ? P.P : n;
+        *P.queue = P.P < m ? P.P : m;
+        *P.active = P.P < m ? P.P : m;
         *P.err = 0;
-        *P.navail = navail;
+        *P.evals = 0;
+        if (!avail) *P.navail = navail;
     }
 }
 
@@ -1951,6 +2470,47 @@ __global__ void k_refill(SplitDev P, const double* init, int n, FitParamsDev prm
 
 __global__ void k_set_int(int* p, int v) { *p = v; }
 
+// ------------------------------------------------------- dataflow kernel ----
+// The whole fit in one cooperative launch: CTAs [first[s], first[s + 1]) run
+// stage s (pupil DFT, window DFT, row blur, column blur + sums + LM) on the
+// units u with u = (CTA index within the stage) mod (CTAs of the stage).  A unit
+// cycles through the four stages once per evaluation; its operands pass from
+// one stage to the next through global memory while they are still in L2 (the
+// pool is small enough), and no stage waits for a round of the whole pool.
+// Converged fits retire and their slots refill from the ROI queue in the LM
+// step; the kernel ends when every unit is dead.
+constexpr int FLOW_THREADS = SPLIT_THREADS + 32;
+
+struct FlowRoles {
+    int first[5];
+};
+
+template <int W>
+__global__ void __launch_bounds__(FLOW_THREADS, 1) k_flow(SplitDev P, FitIO F, FlowRoles roles) {
+    __shared__ UnitRing ring;
+    int s = 0;
+    while (s < 3 && (int)blockIdx.x >= roles.first[s + 1]) ++s;
+    FlowUnits units{&ring, s, (int)blockIdx.x - roles.first[s], roles.first[s + 1] - roles.first[s], 0};
+    if (threadIdx.x == 0) {  // (each stage body publishes these with its own barrier set-up)
+        const int readers = s == 3 && W >= S45_MIN_W ? E45_THREADS / 32 + 2 : SPLIT_THREADS / 32 + 1;
+        for (int b = 0; b < URING; ++b) {
+            umma::mbar_init(&ring.full[b], 1);
+            umma::mbar_init(&ring.freed[b], readers);
+        }
+    }
+    if (s == 0) {
+        stage1_body<W>(P, F, units);
+    } else if (s == 1) {
+        stage2_body<W>(P, F, units);
+    } else if (s == 2) {
+        stage3_body(P, F, units);
+    } else {
+        if constexpr (W >= S45_MIN_W) stage45_body(P, F, units);
+        else stage45s_body(P, F, units);
+    }
+}
+
+
 // ---------------------------------------------------------------- host -----
 static size_t smem_stage1p(const SplitPlanHost& pl) {
     return (size_t)(pl.K1 / 16) * s2_slab_bytes(pl.W) + (size_t)S1_NBQ * s1_qring_bytes(pl.W);
@@ -1960,6 +2520,14 @@ static size_t smem_stage2p(const SplitPlanHost& pl) {
 }
 static size_t smem_stage3(const SplitPlanHost& pl) { return (size_t)5 * 128 * pl.W * 2 + (size_t)4 * pl.RP * pl.W; }
 static size_t smem_stage4(const SplitPlanHost& pl) { return a4_slot_bytes(pl.W, pl.RP) + (size_t)2 * 128 * pl.W * 2; }
+static size_t smem_stage45(const SplitPlanHost& pl) {
+    return (size_t)2 * 128 * pl.W * 2 + (size_t)S45_NBUF * 2 * 32 * 4 * pl.RP + 4 * s45_roi_bytes(pl.R) +
+           (size_t)4 * pl.R * tm_stride(pl.R) * 4 + 16 + (size_t)(E45_THREADS / 32) * (NRED * 8 + 4);
+}
+static size_t smem_stage45s(const SplitPlanHost& pl) {
+    const int UG = unit_slots(pl.G1, pl.G2);
+    return s45s_smem(pl.W, pl.RP, pl.R, UG, s45s_nbuf(pl.W, pl.RP, pl.R, UG));
+}
 static size_t smem_fused(const SplitPlanHost& pl) {
     const int nbuf = pl.W >= 64 ? 2 : 1;
     return (size_t)4 * 128 * pl.K1 * 2 + (size_t)nbuf * 12 * 16 * pl.K1 + (size_t)5 * 128 * 16 * 2 +
@@ -2024,45 +2592,51 @@ __global__ void k_init_points(SplitDev P, const double* xyz, int n) {
 struct SplitPool {
     SplitPlanHost* pl = nullptr;
     SplitDev D{};
-    size_t s1 = 0, s2 = 0, s3 = 0, s4 = 0, s45 = 0, sf = 0;
+    int U = 0;  // units of UG slots
+    size_t s1 = 0, s2 = 0, s3 = 0, s4 = 0, s45 = 0, sf = 0, sflow = 0;
 };
 
-static cudaError_t stage1_attr(int W, size_t smem) {
+template <int W>
+static cudaError_t set_smem_attrs(const SplitPool& sp) {
     const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    if (W == 32) return cudaFuncSetAttribute(k_stage1p<32>, a, (int)smem);
-    if (W == 64) return cudaFuncSetAttribute(k_stage1p<64>, a, (int)smem);
-    return cudaFuncSetAttribute(k_stage1p<128>, a, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k_stage1p<W>, a, (int)sp.s1);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage2p<W>, a, (int)sp.s2);
+    if (e == cudaSuccess && sp.sflow) e = cudaFuncSetAttribute(k_flow<W>, a, (int)sp.sflow);
+    return e;
 }
 
-static void launch_stage1(zola_ctx* ctx, const SplitPool& sp, int ntiles, cudaStream_t st) {
-    const int grid = std::min(ntiles, ctx->num_sms);
+static cudaError_t smem_attrs(int W, const SplitPool& sp) {
+    if (W == 32) return set_smem_attrs<32>(sp);
+    if (W == 64) return set_smem_attrs<64>(sp);
+    return set_smem_attrs<128>(sp);
+}
+
+static int unit_grid(zola_ctx* ctx, const SplitPool& sp) { return std::min(sp.U, ctx->num_sms); }
+
+static void launch_stage1(zola_ctx* ctx, const SplitPool& sp, const FitIO& F, cudaStream_t st) {
+    const int grid = unit_grid(ctx, sp);
     if (sp.D.W == 32)
-        k_stage1p<32><<<grid, S1_THREADS, sp.s1, st>>>(sp.D, ntiles);
+        k_stage1p<32><<<grid, S1_THREADS, sp.s1, st>>>(sp.D, F);
     else if (sp.D.W == 64)
-        k_stage1p<64><<<grid, S1_THREADS, sp.s1, st>>>(sp.D, ntiles);
+        k_stage1p<64><<<grid, S1_THREADS, sp.s1, st>>>(sp.D, F);
     else
-        k_stage1p<128><<<grid, S1_THREADS, sp.s1, st>>>(sp.D, ntiles);
+        k_stage1p<128><<<grid, S1_THREADS, sp.s1, st>>>(sp.D, F);
 }
 
-static cudaError_t stage2_attr(int W, size_t smem) {
-    const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    if (W == 32) return cudaFuncSetAttribute(k_stage2p<32>, a, (int)smem);
-    if (W == 64) return cudaFuncSetAttribute(k_stage2p<64>, a, (int)smem);
-    return cudaFuncSetAttribute(k_stage2p<128>, a, (int)smem);
-}
-
-static void launch_stage2(zola_ctx* ctx, const SplitPool& sp, int ntiles, cudaStream_t st) {
-    const int grid = std::min(ntiles, ctx->num_sms);
+static void launch_stage2(zola_ctx* ctx, const SplitPool& sp, const FitIO& F, cudaStream_t st) {
+    const int grid = unit_grid(ctx, sp);
     if (sp.D.W == 32)
-        k_stage2p<32><<<grid, S2_THREADS, sp.s2, st>>>(sp.D, ntiles);
+        k_stage2p<32><<<grid, S2_THREADS, sp.s2, st>>>(sp.D, F);
     else if (sp.D.W == 64)
-        k_stage2p<64><<<grid, S2_THREADS, sp.s2, st>>>(sp.D, ntiles);
+        k_stage2p<64><<<grid, S2_THREADS, sp.s2, st>>>(sp.D, F);
     else
-        k_stage2p<128><<<grid, S2_THREADS, sp.s2, st>>>(sp.D, ntiles);
+        k_stage2p<128><<<grid, S2_THREADS, sp.s2, st>>>(sp.D, F);
 }
 
+// Pool of slots for n ROIs: at most pmax slots (0: state up to 8 GB, at most
+// 32768), in whole units; for the dataflow kernel at most max_units units.
 static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pmax_override, SplitPool& sp,
-                      cudaStream_t st) {
+                      cudaStream_t st, int max_units = 0) {
     if (p->D > 64) {
         ctx->err = "split path: pupil disk wider than 64 rows (grid too large for this optics)";
         return ZOLA_E_UNSUPPORTED;
@@ -2082,20 +2656,26 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
         ctx->err = "split path: window sizes 32, 64 and 128 only";
         return ZOLA_E_UNSUPPORTED;
     }
-    sp.s1 = smem_stage1p(*pl); sp.s2 = smem_stage2p(*pl); sp.s3 = smem_stage3(*pl); sp.s4 = smem_stage4(*pl);
-    sp.s45 = (size_t)2 * 128 * pl->W * 2 + (size_t)S45_NBUF * 2 * 32 * 4 * pl->RP + 4 * s45_roi_bytes(pl->R) +
-             (size_t)4 * pl->R * tm_stride(pl->R) * 4;
-    if (sp.s1 > 227 * 1024 || sp.s2 > 227 * 1024 || sp.s3 > 227 * 1024 || sp.s4 > 227 * 1024 ||
-        sp.s45 > 227 * 1024) {
-        ctx->err = "split path: shared-memory plan exceeds 227 KB";
+    const int UG = unit_slots(pl->G1, pl->G2);
+    sp.s1 = smem_stage1p(*pl);
+    sp.s2 = smem_stage2p(*pl);
+    sp.s3 = smem_stage3(*pl);
+    sp.s4 = smem_stage4(*pl);
+    sp.s45 = pl->W >= S45_MIN_W ? smem_stage45(*pl) : smem_stage45s(*pl);
+    sp.sflow = max_units > 0 ? std::max(std::max(sp.s1, sp.s2), std::max(sp.s3, sp.s45)) : 0;
+    const size_t lim = 225 * 1024;
+    if (sp.s1 > lim || sp.s2 > lim || sp.s3 > lim || sp.s4 > lim || sp.s45 > lim || sp.sflow > lim) {
+        ctx->err = "split path: shared-memory plan exceeds 225 KB";
         return ZOLA_E_UNSUPPORTED;
     }
     const size_t per_slot = a2_tile_bytes(pl->K1) / pl->G2 + a3_tile_bytes(pl->W) / pl->G2 +
                             (size_t)pl->NT4 * a4_tile_bytes(pl->W) + (size_t)4 * pl->R * pl->R * 4 + sizeof(LMState) + NSUM * 8 + 16;
     int Pmax = (int)std::min<size_t>(32768, ((size_t)8 << 30) / per_slot);  // at most 8 GB of pool state
     if (pmax_override > 0) Pmax = std::min(Pmax, pmax_override);
-    Pmax = std::max(4, Pmax / 4 * 4);
-    const int P = std::min(Pmax, (n + 3) / 4 * 4);
+    if (max_units > 0) Pmax = std::min(Pmax, max_units * UG);
+    Pmax = std::max(UG, Pmax / UG * UG);
+    const int P = std::min(Pmax, (n + UG - 1) / UG * UG);
+    sp.U = P / UG;
     auto al = [](size_t v) { return (v + 1023) / 1024 * 1024; };
     const size_t b_a2 = al((size_t)(P / pl->G2) * a2_tile_bytes(pl->K1));
     const size_t b_a3 = al((size_t)(P / pl->G2) * a3_tile_bytes(pl->W));
@@ -2103,8 +2683,9 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
     const size_t b_t = al((size_t)P * 4 * pl->R * pl->R * 4);
     const size_t b_lm = al((size_t)P * sizeof(LMState));
     const size_t b_sums = al((size_t)P * NSUM * 8);
-    const size_t b_int = al((size_t)P * 8 + 64);
-    if (ensure_scratch(ctx, b_a2 + b_a3 + b_a4 + b_t + b_lm + b_sums + b_int, ctx->err)) return ZOLA_E_CUDA;
+    const size_t b_int = al((size_t)P * 8 + (size_t)sp.U * 4 + 64);
+    const size_t b_clk = al(((size_t)2 * ctx->num_sms + 1) * 8);
+    if (ensure_scratch(ctx, b_a2 + b_a3 + b_a4 + b_t + b_lm + b_sums + b_clk + b_int, ctx->err)) return ZOLA_E_CUDA;
     char* base = (char*)ctx->scratch;
     SplitDev& D = sp.D;
     D = SplitDev{};
@@ -2121,48 +2702,44 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
     D.tmaps = (float*)base; base += b_t;
     D.lm = (LMState*)base; base += b_lm;
     D.sums = (double*)base; base += b_sums;
+    D.evals = (unsigned long long*)base;
+    D.clk = D.evals + 1;
+    base += b_clk;
     D.slot_roi = (int*)base;
     D.slot_phase = D.slot_roi + P;
     D.queue = D.slot_phase + P;
     D.active = D.queue + 1;
     D.err = D.queue + 2;
     D.navail = D.queue + 3;
+    D.ustate = D.queue + 16;
+    D.wait_limit = ctx->wait_limit > 0 ? ctx->wait_limit : (1ll << 31);
     D.sc = pl->sc;
     ZOLA_CUDA_CHECK(cudaMemsetAsync(D.a4, 0, b_a4, st), ctx);
-    ZOLA_CUDA_CHECK(stage1_attr(pl->W, sp.s1), ctx);
-    ZOLA_CUDA_CHECK(stage2_attr(pl->W, sp.s2), ctx);
-    ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_stage3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.s3), ctx);
-    ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_stage4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.s4), ctx);
-    ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_stage45p, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.s45), ctx);
+    ZOLA_CUDA_CHECK(smem_attrs(pl->W, sp), ctx);
+    const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_stage3, a, (int)sp.s3), ctx);
+    ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_stage4, a, (int)sp.s4), ctx);
+    if (pl->W >= S45_MIN_W)
+        ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_stage45p, a, (int)sp.s45), ctx);
+    else
+        ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_stage45s, a, (int)sp.s45), ctx);
     sp.sf = smem_fused(*pl);
-    if (fused_fits(*pl))
-        ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_fused25, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.sf), ctx);
+    if (fused_fits(*pl)) ZOLA_CUDA_CHECK(cudaFuncSetAttribute(k_fused25, a, (int)sp.sf), ctx);
     return ZOLA_OK;
 }
 
 // Stages 1-3 (pupil DFT, window DFT, row blur) of every occupied slot.
-static void launch_stages123(zola_ctx* ctx, const SplitPool& sp, cudaStream_t st) {
-    const SplitPlanHost& pl = *sp.pl;
-    const int P = sp.D.P;
+static void launch_stages123(zola_ctx* ctx, const SplitPool& sp, const FitIO& F, cudaStream_t st) {
     prof_begin(ctx, 0, st);
-    launch_stage1(ctx, sp, P / pl.G1, st);
+    launch_stage1(ctx, sp, F, st);
     prof_end(ctx, st);
     prof_begin(ctx, 1, st);
-    launch_stage2(ctx, sp, P / pl.G2, st);
+    launch_stage2(ctx, sp, F, st);
     prof_end(ctx, st);
     prof_begin(ctx, 2, st);
-    k_stage3<<<P / pl.G2, SPLIT_THREADS, sp.s3, st>>>(sp.D);
+    k_stage3<<<unit_grid(ctx, sp), S3_THREADS, sp.s3, st>>>(sp.D, F);
     prof_end(ctx, st);
     ctx->launches += 3;
-}
-
-// Model-only evaluation: stages 1-3 and the column blur into FP32 maps.
-static void launch_model_stages(zola_ctx* ctx, const SplitPool& sp, cudaStream_t st) {
-    launch_stages123(ctx, sp, st);
-    prof_begin(ctx, 3, st);
-    k_stage4<<<sp.D.P, SPLIT_THREADS, sp.s4, st>>>(sp.D);
-    prof_end(ctx, st);
-    ctx->launches += 1;
 }
 
 static int read_flags(zola_ctx* ctx, const SplitDev& D, cudaStream_t st, int* active, int* err, int* queue = nullptr) {
@@ -2178,16 +2755,20 @@ static int read_flags(zola_ctx* ctx, const SplitDev& D, cudaStream_t st, int* ac
 
 int launch_model_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const double* d_xyz, int n, double* d_out,
                        double* d_dout, cudaStream_t st) {
+    const FitIO none{};
     for (int done = 0; done < n;) {
         SplitPool sp;
         int rc = setup_pool(ctx, p, w, n - done, 0, sp, st);
         if (rc) return rc;
         const int m = std::min(sp.D.P, n - done);
         k_init_points<<<(sp.D.P + 127) / 128, 128, 0, st>>>(sp.D, d_xyz + 3 * (size_t)done, m);
-        launch_model_stages(ctx, sp, st);
+        launch_stages123(ctx, sp, none, st);
+        prof_begin(ctx, 3, st);
+        k_stage4<<<sp.D.P, SPLIT_THREADS, sp.s4, st>>>(sp.D);
+        prof_end(ctx, st);
         const size_t RR = (size_t)w->R * w->R;
         k_model_out<<<m, 128, 0, st>>>(sp.D, m, d_out + RR * done, d_dout ? d_dout + 3 * RR * done : nullptr);
-        ctx->launches += 2;
+        ctx->launches += 3;
         ZOLA_CUDA_CHECK(cudaGetLastError(), ctx);
         int active, err;
         rc = read_flags(ctx, sp.D, st, &active, &err);
@@ -2198,16 +2779,245 @@ int launch_model_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const double
     return ZOLA_OK;
 }
 
+// Default shape of the dataflow kernel: two units per SM, and the SMs split
+// between the stages in proportion to each stage's share of a unit's device
+// time for this window size (measured on B200 with the round-based kernels).
+static FlowShape default_shape(int W, int grid) {
+    static const double share[3][4] = {{0.40, 0.25, 0.17, 0.18},   // W = 32
+                                       {0.38, 0.27, 0.17, 0.18},   // W = 64
+                                       {0.21, 0.30, 0.21, 0.28}};  // W = 128
+    const int wi = W == 32 ? 0 : W == 64 ? 1 : 2;
+    FlowShape f;
+    f.units = 2 * grid;
+    double w[4];
+    for (int s = 0; s < 4; ++s) w[s] = share[wi][s];
+    // CTAs in proportion to w, at least one each, adding up to grid
+    int sum = 0;
+    for (int s = 0; s < 4; ++s) sum += f.ctas[s] = std::max(1, (int)std::lround(w[s] * grid));
+    for (int s = 0; sum != grid; s = (s + 1) % 4) {
+        if (sum > grid && f.ctas[s] > 1) { --f.ctas[s]; --sum; }
+        else if (sum < grid) { ++f.ctas[s]; ++sum; }
+    }
+    return f;
+}
+
+// CTAs in proportion to the busy time each stage had in a measured launch.
+static void rebalance(FlowShape& f, const unsigned long long* clk, int grid) {
+    double work[4] = {0, 0, 0, 0}, tot = 0;
+    int b = 0;
+    for (int s = 0; s < 4; ++s)
+        for (int k = 0; k < f.ctas[s]; ++k, ++b) work[s] += (double)(clk[2 * b + 1] - std::min(clk[2 * b], clk[2 * b + 1]));
+    for (int s = 0; s < 4; ++s) tot += work[s];
+    if (!(tot > 0)) return;
+    int sum = 0;
+    for (int s = 0; s < 4; ++s) sum += f.ctas[s] = std::max(1, (int)std::lround(work[s] / tot * grid));
+    for (int s = 0; sum != grid; s = (s + 1) % 4) {
+        if (sum > grid && f.ctas[s] > 1) { --f.ctas[s]; --sum; }
+        else if (sum < grid) { ++f.ctas[s]; ++sum; }
+    }
+}
+
+static std::string tune_key(const zola_psf* p, const WindowTables* w) {
+    return "N" + std::to_string(p->N) + "_D" + std::to_string(p->D) + "_R" + std::to_string(w->R) + "_W" +
+           std::to_string(w->W);
+}
+
+// The autotuner's cache: {"<class>": {"units": U, "ctas": [a, b, c, d], "ns_per_eval": t}, ...}
+static void tune_save(zola_ctx* ctx) {
+    if (ctx->tune_path.empty()) return;
+    FILE* f = std::fopen(ctx->tune_path.c_str(), "w");
+    if (!f) return;
+    std::fprintf(f, "{");
+    bool first = true;
+    for (const auto& kv : ctx->tunes) {
+        if (!kv.second.done) continue;
+        const FlowShape& b = kv.second.best;
+        std::fprintf(f, "%s\n  \"%s\": {\"units\": %d, \"ctas\": [%d, %d, %d, %d], \"ns_per_eval\": %.3f}",
+                     first ? "" : ",", kv.first.c_str(), b.units, b.ctas[0], b.ctas[1], b.ctas[2], b.ctas[3],
+                     kv.second.best_ns);
+        first = false;
+    }
+    std::fprintf(f, "\n}\n");
+    std::fclose(f);
+}
+
+void tune_load(zola_ctx* ctx) {
+    if (ctx->tune_path.empty()) return;
+    FILE* f = std::fopen(ctx->tune_path.c_str(), "r");
+    if (!f) return;
+    std::string txt;
+    char buf[4096];
+    size_t k;
+    while ((k = std::fread(buf, 1, sizeof buf, f)) > 0) txt.append(buf, k);
+    std::fclose(f);
+    size_t pos = 0;
+    while ((pos = txt.find('"', pos)) != std::string::npos) {
+        const size_t end = txt.find('"', pos + 1);
+        if (end == std::string::npos) break;
+        const std::string key = txt.substr(pos + 1, end - pos - 1);
+        pos = end + 1;
+        if (key.empty() || key[0] != 'N') continue;
+        FlowTune t;
+        if (std::sscanf(txt.c_str() + pos, " : {\"units\": %d, \"ctas\": [%d, %d, %d, %d], \"ns_per_eval\": %lf",
+                        &t.best.units, &t.best.ctas[0], &t.best.ctas[1], &t.best.ctas[2], &t.best.ctas[3],
+                        &t.best_ns) == 6) {
+            int sum = 0;
+            for (int s = 0; s < 4; ++s) sum += t.best.ctas[s] > 0 ? t.best.ctas[s] : -100000;
+            if (sum == ctx->num_sms && t.best.units > 0) {
+                t.done = true;
+                ctx->tunes[key] = t;
+            }
+        }
+    }
+}
+
+// Shape of this launch: the context's explicit setting, a tuned shape, the
+// tuner's next trial (large batches of an untuned class while tuning is on),
+// or the default.  *trial: the launch is to be measured for the tuner.
+static FlowShape pick_shape(zola_ctx* ctx, const std::string& key, int W, int n, int UG, bool* trial) {
+    const int grid = ctx->num_sms;
+    *trial = false;
+    FlowShape f = default_shape(W, grid);
+    if (ctx->flow_ctas[0] > 0)
+        for (int s = 0; s < 4; ++s) f.ctas[s] = ctx->flow_ctas[s];
+    if (ctx->flow_units > 0) f.units = ctx->flow_units;
+    if (ctx->flow_units > 0 || ctx->flow_ctas[0] > 0) return f;
+    auto it = ctx->tunes.find(key);
+    if (it != ctx->tunes.end() && it->second.done) return it->second.best;
+    // tuning needs a batch that keeps the pool busy for many evaluations
+    if (!ctx->tune || n < 16 * 3 * grid * UG) return f;
+    FlowTune& t = ctx->tunes[key];
+    *trial = true;
+    return t.trials == 0 ? f : t.next;
+}
+
+// After a measured launch: record it and choose the next trial.  Trials 0-2
+// rebalance the CTAs per stage from the measured busy times at two units per
+// SM; trials 3 and 4 try three and one and a half units per SM with the best
+// split; then the best shape is kept (and written to the cache file).
+static void tune_record(zola_ctx* ctx, const std::string& key, const FlowShape& used, double ns_per_eval,
+                        const unsigned long long* clk) {
+    FlowTune& t = ctx->tunes[key];
+    if (t.trials == 0 || ns_per_eval < t.best_ns) {
+        t.best = used;
+        t.best_ns = ns_per_eval;
+    }
+    ++t.trials;
+    const int grid = ctx->num_sms;
+    t.next = used;
+    if (t.trials < 3) {
+        rebalance(t.next, clk, grid);
+    } else if (t.trials == 3) {
+        t.next = t.best;
+        t.next.units = 3 * grid;
+    } else if (t.trials == 4) {
+        t.next = t.best;
+        t.next.units = 3 * grid / 2;
+    } else {
+        t.done = true;
+        tune_save(ctx);
+    }
+}
+
+static int launch_fit_flow(zola_ctx* ctx, zola_psf* p, WindowTables* w, const FitIO& F, cudaStream_t st,
+                           const RoiFeed* feed, const int* d_avail) {
+    SplitPool sp;
+    const int grid = ctx->num_sms;
+    SplitPlanHost* pl = get_plan(p, w, ctx->err);
+    if (!pl) return ZOLA_E_CUDA;
+    const std::string key = tune_key(p, w);
+    bool trial = false;
+    const FlowShape shape = pick_shape(ctx, key, w->W, F.n, unit_slots(pl->G1, pl->G2), &trial);
+    int rc = setup_pool(ctx, p, w, F.n, ctx->split_pool_max, sp, st, shape.units);
+    if (rc) return rc;
+    if (d_avail) sp.D.navail = const_cast<int*>(d_avail);  // read only
+    const SplitDev& D = sp.D;
+    int navail = F.n;
+    if (feed && feed->n_chunks > 0) {
+        ZOLA_CUDA_CHECK(cudaStreamWaitEvent(st, feed->ev[0], 0), ctx);
+        navail = feed->chunk_end[0];
+    }
+    k_init_slots<<<(D.P + 127) / 128, 128, 0, st>>>(D, F.init, F.n, navail, F.prm, d_avail);
+    ctx->launches++;
+    ZOLA_CUDA_CHECK(cudaGetLastError(), ctx);
+    if (feed && feed->n_chunks > 1) {
+        // the ROI count on the device follows the input chunks as they land (a
+        // copy per chunk, after the pool was filled), while the kernel runs
+        if (!ctx->h_feed) ZOLA_CUDA_CHECK(cudaMallocHost(&ctx->h_feed, 64 * sizeof(int)), ctx);
+        if (!ctx->ev_init) ZOLA_CUDA_CHECK(cudaEventCreateWithFlags(&ctx->ev_init, cudaEventDisableTiming), ctx);
+        ZOLA_CUDA_CHECK(cudaStreamSynchronize(ctx->feed_stream), ctx);  // the previous call's count copies are done
+        ZOLA_CUDA_CHECK(cudaEventRecord(ctx->ev_init, st), ctx);
+        ZOLA_CUDA_CHECK(cudaStreamWaitEvent(ctx->feed_stream, ctx->ev_init, 0), ctx);
+        for (int c = 1; c < feed->n_chunks && c < 64; ++c) {
+            ctx->h_feed[c] = feed->chunk_end[c];
+            ZOLA_CUDA_CHECK(cudaStreamWaitEvent(ctx->feed_stream, feed->ev[c], 0), ctx);
+            ZOLA_CUDA_CHECK(cudaMemcpyAsync(D.navail, ctx->h_feed + c, sizeof(int), cudaMemcpyHostToDevice,
+                                            ctx->feed_stream), ctx);
+        }
+    }
+    FlowRoles roles;
+    roles.first[0] = 0;
+    for (int s = 0; s < 4; ++s) roles.first[s + 1] = roles.first[s] + shape.ctas[s];
+    SplitDev dv = D;
+    FitIO io = F;
+    void* args[] = {&dv, &io, &roles};
+    const void* fn = D.W == 32 ? (const void*)k_flow<32> : D.W == 64 ? (const void*)k_flow<64> : (const void*)k_flow<128>;
+    if (trial) {
+        for (auto& e : ctx->tune_ev)
+            if (!e) ZOLA_CUDA_CHECK(cudaEventCreate(&e), ctx);
+        ZOLA_CUDA_CHECK(cudaEventRecord(ctx->tune_ev[0], st), ctx);
+    }
+    prof_begin(ctx, 8, st);
+    cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(FLOW_THREADS), args, sp.sflow, st);
+    prof_end(ctx, st);
+    ctx->launches++;
+    if (e != cudaSuccess) {
+        ctx->err = std::string("split fit (dataflow kernel): ") + cudaGetErrorString(e);
+        return ZOLA_E_CUDA;
+    }
+    if (trial) ZOLA_CUDA_CHECK(cudaEventRecord(ctx->tune_ev[1], st), ctx);
+    int active, err;
+    rc = read_flags(ctx, D, st, &active, &err);
+    if (rc) return rc;
+    if (err == 2) {
+        ctx->err = "split fit: no unit became ready within the wait limit (inputs did not arrive)";
+        return ZOLA_E_TIMEOUT;
+    }
+    if (err) {
+        ctx->err = "split fit: a bounded device wait timed out";
+        return ZOLA_E_TIMEOUT;
+    }
+    if (trial) {
+        if (!ctx->h_tune) ZOLA_CUDA_CHECK(cudaMallocHost(&ctx->h_tune, (2 * (size_t)grid + 1) * 8), ctx);
+        ZOLA_CUDA_CHECK(cudaMemcpy(ctx->h_tune, D.evals, (2 * (size_t)grid + 1) * 8, cudaMemcpyDeviceToHost), ctx);
+        float ms = 0;
+        ZOLA_CUDA_CHECK(cudaEventElapsedTime(&ms, ctx->tune_ev[0], ctx->tune_ev[1]), ctx);
+        if (ctx->h_tune[0] > 0) tune_record(ctx, key, shape, ms * 1e6 / (double)ctx->h_tune[0], ctx->h_tune + 1);
+    }
+    return ZOLA_OK;
+}
+
+// The shape the dataflow kernel uses for this PSF and window; true when it was tuned.
+bool flow_shape(zola_ctx* ctx, zola_psf* p, WindowTables* w, FlowShape* out, double* ns_per_eval) {
+    auto it = ctx->tunes.find(tune_key(p, w));
+    const bool tuned = it != ctx->tunes.end() && it->second.done;
+    *out = tuned ? it->second.best : default_shape(w->W, ctx->num_sms);
+    if (ns_per_eval) *ns_per_eval = tuned ? it->second.best_ns : 0.0;
+    return tuned;
+}
+
 int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_rois, const float* d_scmos,
                      const double* d_init, int n,
                      const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll, int* d_status,
-                     int* d_iters, cudaStream_t st, const RoiFeed* feed) {
+                     int* d_iters, cudaStream_t st, const RoiFeed* feed, const int* d_avail) {
+    FitParamsDev fp{prm->zmin, prm->zmax, prm->xymax, prm->tol_xyz, prm->step_xy, prm->step_z, prm->max_iter};
+    const FitIO F{d_rois, d_scmos, d_init, n, fp, d_out5, d_crlb5, d_nll, d_status, d_iters};
+    if (ctx->split_mode == ZOLA_SPLIT_FLOW || d_avail) return launch_fit_flow(ctx, p, w, F, st, feed, d_avail);
     SplitPool sp;
     int rc = setup_pool(ctx, p, w, n, ctx->split_pool_max, sp, st);
     if (rc) return rc;
     const SplitDev& D = sp.D;
     const int P = D.P;
-    FitParamsDev fp{prm->zmin, prm->zmax, prm->xymax, prm->tol_xyz, prm->step_xy, prm->step_z, prm->max_iter};
     // inputs still arriving: the fit starts on the first chunk, and chunks are
     // handed to the pool as their copies complete
     int chunk = 0, navail = n, queue = 0;
@@ -2237,13 +3047,13 @@ int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d
     ZOLA_CUDA_CHECK(cudaGetLastError(), ctx);
     const int max_rounds = (prm->max_iter + 2) * ((n + P - 1) / P + 1) + 8 + 4 * (feed ? feed->n_chunks : 0);
     int rounds = 0;
-    const bool fused = ctx->split_fused && fused_fits(*sp.pl);
-    // Large ROIs: column blur and likelihood sums in one persistent kernel (the
-    // maps never leave the SM).  Small ROIs: the column-blur maps go through
-    // memory to the warp-per-slot likelihood kernel, which keeps many slots in
-    // flight per SM.  The two sum in different orders; the choice depends on R
-    // alone so that a fit never depends on the batch it is in.
-    const bool fused45 = sp.pl->R >= S45_MIN_R;
+    const bool fused = ctx->split_mode == ZOLA_SPLIT_FUSED && fused_fits(*sp.pl);
+    // Window 128: column blur and likelihood sums in one persistent kernel (the
+    // maps never leave the SM).  Smaller windows: one warp per slot forms the
+    // sums from the unit's maps in shared memory.  The two sum in different
+    // orders; the choice depends on R alone so that a fit never depends on the
+    // batch it is in.
+    const bool big = sp.pl->W >= S45_MIN_W;
     while (true) {
         for (int k = 0; k < 4; ++k) {
             if (feed && queue < n) {  // idle slots take ROIs that arrived since
@@ -2252,34 +3062,23 @@ int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d
             }
             if (fused) {
                 prof_begin(ctx, 0, st);
-                launch_stage1(ctx, sp, P / sp.pl->G1, st);
+                launch_stage1(ctx, sp, F, st);
                 prof_end(ctx, st);
-                prof_begin(ctx, 1, st);
+                prof_begin(ctx, 4, st);
                 k_fused25<<<P / sp.pl->G2, SPLIT_THREADS, sp.sf, st>>>(D, d_rois, d_scmos, d_init, n, fp, d_out5, d_crlb5, d_nll,
                                                                       d_status, d_iters);
                 prof_end(ctx, st);
                 ctx->launches += 2;
                 continue;
             }
-            if (fused45) {
-                launch_stages123(ctx, sp, st);
-                prof_begin(ctx, 3, st);
-                k_stage45p<<<std::min(P, ctx->num_sms), S45_THREADS, sp.s45, st>>>(D, d_rois, d_scmos);
-                prof_end(ctx, st);
-                prof_begin(ctx, 4, st);
-                k_lm<<<(P + LM_THREADS - 1) / LM_THREADS, LM_THREADS, 0, st>>>(D, d_init, n, fp, d_out5, d_crlb5,
-                                                                            d_nll, d_status, d_iters);
-                prof_end(ctx, st);
-                ctx->launches += 2;
-            } else {
-                launch_model_stages(ctx, sp, st);
-                prof_begin(ctx, 4, st);
-                k_stage5<<<(P + S5_SLOTS - 1) / S5_SLOTS, S5_THREADS, 0, st>>>(D, d_rois, d_scmos);
-                k_lm<<<(P + LM_THREADS - 1) / LM_THREADS, LM_THREADS, 0, st>>>(D, d_init, n, fp, d_out5, d_crlb5,
-                                                                            d_nll, d_status, d_iters);
-                prof_end(ctx, st);
-                ctx->launches += 2;
-            }
+            launch_stages123(ctx, sp, F, st);
+            prof_begin(ctx, 3, st);
+            if (big)
+                k_stage45p<<<unit_grid(ctx, sp), S45_THREADS, sp.s45, st>>>(D, F);
+            else
+                k_stage45s<<<unit_grid(ctx, sp), S45S_THREADS, sp.s45, st>>>(D, F);
+            prof_end(ctx, st);
+            ctx->launches += 1;
         }
         rounds += 4;
         ZOLA_CUDA_CHECK(cudaGetLastError(), ctx);

@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(256) k_pipe_replay(PipeView V, const double* t
 }
 
 struct LocRow {
-    int frame, seq;
+    int frame, seq, status;
     double x, y, z, A, B, chi2, cx, cy, cz;
 };
 
@@ -279,7 +279,8 @@ __global__ void k_take_acc(int n, const int* acc_slot, const double* theta, doub
 
 // chi2 and CRLB of the accepted localizations (psi, dpsi evaluated at their
 // fitted positions, in acceptance-list order).
-__global__ void k_pipe_rows(PipeView V, int n, const int* acc_slot, const int* acc_seq, const double* theta,
+__global__ void k_pipe_rows(PipeView V, int n, const int* acc_slot, const int* acc_seq, const int* status,
+                            const double* theta,
                             const double* psi, const double* dpsi, LocRow* rows) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
@@ -313,7 +314,7 @@ __global__ void k_pipe_rows(PipeView V, int n, const int* acc_slot, const int* a
     for (int q = 0; q < 3; ++q)
         if (!(cr[q] == cr[q])) cr[q] = F[q * 5 + q] != 0 ? sqrt(1.0 / F[q * 5 + q]) : 1.79769313486231570e308;
     LocRow& L = rows[k];
-    L.frame = f; L.seq = acc_seq[k];
+    L.frame = f; L.seq = acc_seq[k]; L.status = status[s];
     L.x = 1000 * (ci * V.dx - x); L.y = 1000 * (cj * V.dx - y); L.z = 1000 * z;
     L.A = A; L.B = B; L.chi2 = chi;
     L.cx = 1000 * cr[0]; L.cy = 1000 * cr[1]; L.cz = 1000 * cr[2];
@@ -516,7 +517,7 @@ int localize_impl(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const do
                 // the walk has used psi; its buffer now takes the accepted positions' models
                 rc = zola_psf_model_dev(fit_psf, R, (double*)b_xyz.p, nacc, (double*)b_psi.p, (double*)b_dpsi.p, st);
                 if (rc) return rc;
-                k_pipe_rows<<<(nacc + 127) / 128, 128, 0, st>>>(V, nacc, (int*)b_acc.p, (int*)b_seq.p,
+                k_pipe_rows<<<(nacc + 127) / 128, 128, 0, st>>>(V, nacc, (int*)b_acc.p, (int*)b_seq.p, (int*)b_st.p,
                                                                 (double*)b_out5.p, (double*)b_psi.p,
                                                                 (double*)b_dpsi.p, (LocRow*)b_rows.p);
                 ctx->launches++;
@@ -542,6 +543,7 @@ int localize_impl(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const do
         L.x_nm = r.x; L.y_nm = r.y; L.z_nm = r.z; L.intensity = r.A; L.background = r.B; L.chi2 = r.chi2;
         L.crlb_x_nm = r.cx; L.crlb_y_nm = r.cy; L.crlb_z_nm = r.cz;
         L.candidate = r.seq;
+        L.fit_status = r.status;
     }
     *nout = (int)all.size();
     return ZOLA_OK;

@@ -58,6 +58,24 @@ struct WindowTables {
 
 }  // namespace zola
 
+namespace zola {
+// Shape of the dataflow split-fit kernel: units of slots in flight and CTAs per
+// stage (pupil DFT, window DFT, row blur, column blur + sums + LM).
+struct FlowShape {
+    int units = 0;
+    int ctas[4] = {0, 0, 0, 0};
+};
+// Autotuning state of one (pupil grid, disk rows, ROI side, window) class: the
+// trials made so far and the best shape measured, in device ns per model
+// evaluation.
+struct FlowTune {
+    FlowShape best, next;
+    double best_ns = 0;
+    int trials = 0;
+    bool done = false;
+};
+}  // namespace zola
+
 struct zola_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -77,7 +95,19 @@ struct zola_ctx {
     int* d_status_word = nullptr;
     int* h_flags = nullptr;      // pinned host words read back by the split fit loop
     int split_pool_max = 0;      // 0: size the split slot pool automatically
-    int split_fused = 0;         // 1: stage 1 + one fused kernel for stages 2-5 per LM round
+    int split_mode = ZOLA_SPLIT_FLOW;  // ZOLA_SPLIT_STAGED, _FUSED or _FLOW
+    int flow_units = 0;          // dataflow kernel: units of slots in flight (0: automatic)
+    int flow_ctas[4] = {};       // dataflow kernel: CTAs per stage (all 0: automatic)
+    long long wait_limit = 0;    // clocks a device wait may take before the call fails (0: about a second)
+    cudaStream_t feed_stream = nullptr;  // copies of the arrived-ROI count of a host-buffer fit
+    cudaEvent_t ev_init = nullptr;
+    int* h_feed = nullptr;       // pinned chunk ends for those copies
+    // dataflow-kernel autotuner: on (1) / off (0), JSON cache file, state per class
+    int tune = 0;
+    std::string tune_path;
+    std::map<std::string, zola::FlowTune> tunes;
+    cudaEvent_t tune_ev[2] = {nullptr, nullptr};
+    unsigned long long* h_tune = nullptr;  // pinned: evaluations, then (idle, total) clocks per CTA
     // optional per-kernel timing with CUDA events on the launch stream
     int profile = 0;
     std::vector<cudaEvent_t> ev_pool;
@@ -145,6 +175,8 @@ int launch_fit_f64(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_r
 int launch_model_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const double* d_xyz, int n, double* d_out,
                        double* d_dout, cudaStream_t st);
 void free_split_plan(void* plan);
+void tune_load(zola_ctx* ctx);  // read the autotuner's cache file (zola_ctx::tune_path)
+bool flow_shape(zola_ctx* ctx, zola_psf* p, WindowTables* w, FlowShape* out, double* ns_per_eval);
 // ROIs that reach the device while a split fit runs (host-buffer calls): chunk
 // c holds ROIs [chunk_end[c - 1], chunk_end[c]) and is on the device once ev[c]
 // has completed.  The slot pool refills only from ROIs that have arrived.
@@ -155,7 +187,8 @@ struct RoiFeed {
 };
 int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_rois, const float* d_scmos,
                      const double* d_init, int n, const zola_fit_params* prm, double* d_out5, double* d_crlb5,
-                     double* d_nll, int* d_status, int* d_iters, cudaStream_t st, const RoiFeed* feed = nullptr);
+                     double* d_nll, int* d_status, int* d_iters, cudaStream_t st, const RoiFeed* feed = nullptr,
+                     const int* d_avail = nullptr);
 
 int ensure_scratch(zola_ctx* ctx, size_t bytes, std::string& err);
 int ensure_io(zola_ctx* ctx, size_t bytes);
