@@ -23,14 +23,10 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# DRAM bytes per slot of one launch (ncu dram__bytes_read.sum + dram__bytes_write.sum
-# of one launch per kernel, 48x48 tetrapod class, full pool of 4096 slots; stage 4 is
-# the fused column-blur/likelihood kernel and stage 5 the LM step for this class).
-NCU_TRAFFIC = {("tetra48", "split_stage1_pupil_dft"): (1.070080e6 + 476.936448e6) / 4096,
-               ("tetra48", "split_stage2_window_dft"): (537.341952e6 + 624.652288e6) / 4096,
-               ("tetra48", "split_stage3_blur_rows"): (671.155456e6 + 363.580928e6) / 4096,
-               ("tetra48", "split_stage4_blur_cols"): (441.092608e6 + 1.092864e6) / 4096,
-               ("tetra48", "split_stage5_likelihood_lm"): (2.430720e6 + 0.0) / 4096}
+# DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per model
+# evaluation of the dataflow kernel, from one capture of that kernel on a
+# smaller batch of the class (see profiles/); None until measured.
+NCU_TRAFFIC = {}
 
 METRIC = "MLE ROI fits/sec at ≤0.5 nm vs FP64 oracle (batched split-prec vs plain GPU)"
 UNIT = "ROI fits/s"
@@ -300,6 +296,38 @@ def config_block(n):
 
 
 # ----------------------------------------------------------------- main ----
+def flops_per_eval(R, N):
+    """model evaluation with x/y/z derivatives, complex MAC = 8 flops."""
+    W, D = window(R, N), disk_rows(N)
+    return 3 * 8 * W * D * D + 4 * 8 * W * W * D
+
+
+def theta_err(a, b, zsym):
+    """|a - b| per ROI and parameter, |z| compared for z-symmetric PSFs."""
+    d = np.abs(a - b)
+    if zsym:
+        d[:, 2] = np.abs(np.abs(a[:, 2]) - np.abs(b[:, 2]))
+    return d
+
+
+def accuracy_block(a, sa, b, sb, zsym):
+    """Per-ROI error of fits b against reference fits a, over every ROI compared
+    (all statuses) and over the ROIs both fits report converged."""
+    d = theta_err(a, b, zsym)
+    rel = d[:, 3] / np.abs(a[:, 3])
+    within = (d[:, :2].max(1) <= 0.5e-3) & (d[:, 2] <= 1e-3) & (rel <= 1e-3)
+    conv = (sa == 1) & (sb == 1)
+    out = {"compared": int(len(a)), "within_tolerance": float(within.mean()),
+           "status_agreement": float((sa == sb).mean()), "both_converged": float(conv.mean()),
+           "max_dxy_nm": float(d[:, :2].max() * 1000), "max_dz_nm": float(d[:, 2].max() * 1000),
+           "max_dA_rel": float(rel.max()), "p99_dxy_nm": float(np.percentile(d[:, :2].max(1), 99) * 1000),
+           "p99_dz_nm": float(np.percentile(d[:, 2], 99) * 1000), "p99_dA_rel": float(np.percentile(rel, 99))}
+    if conv.any():
+        out.update(converged_max_dxy_nm=float(d[conv, :2].max() * 1000), converged_max_dz_nm=float(d[conv, 2].max() * 1000),
+                   converged_max_dA_rel=float(rel[conv].max()), converged_within_tolerance=float(within[conv].mean()))
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -308,14 +336,18 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--rois", type=int, default=1_000_000)
     ap.add_argument("--fp64-sample", type=int, default=20_000)
+    ap.add_argument("--oracle-sample", type=int, default=48, help="ROIs per class fitted by the FP64 oracle")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--classes", default="", help="comma list of ROI classes to run (profiling); default all")
     ap.add_argument("--pool", type=int, default=16384, help="max ROIs in flight per fit call (0: library default)")
     ap.add_argument("--detect-frames", type=int, default=200,
                     help="frames of the detect -> fit pipeline measurement (0: skip)")
-    ap.add_argument("--split-mode", default="staged", choices=["staged", "fused"],
-                    help="split fit kernels: five stage kernels, or stage 1 + fused stages 2-5")
+    ap.add_argument("--split-mode", default="staged", choices=["staged", "flow", "fused"],
+                    help="split fit kernels: one dataflow kernel, four stage kernels per round, or stage 1 + fused 2-5")
+    ap.add_argument("--no-tune", action="store_true", help="skip the dataflow-kernel autotuning pass")
+    ap.add_argument("--stage-breakdown", action="store_true",
+                    help="also time the round-based stage kernels per stage (explains the dataflow kernel)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -326,6 +358,7 @@ def main():
     import torch
     import torch.distributed as dist
     import __graft_entry__ as ge
+    import oracle as O
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -346,6 +379,28 @@ def main():
     job = make_job(z, ctx, torch, args.rois, seed=2 + rank, device=device, only=only)
     n_total = sum(j["rois"].shape[0] for j in job)
     torch.cuda.synchronize()
+
+    def fit_class(j, precision=None):
+        p = z.PSF.fit_params(precision=z.ZOLA_PREC_SPLIT if precision is None else precision, **j["prm_kw"])
+        j["psf"].fit_dev(j["rois"], j["init"], p, j["out"], j["crlb"], j["nll"], j["status"], j["iters"],
+                         stream=ctx.stream)
+
+    # autotuning pass (outside the timed region): the dataflow kernel's shape per
+    # class; fits do not depend on the shape, so this changes timings only
+    tuned = {}
+    if args.split_mode == "flow" and not args.no_tune:
+        ctx.set_tuning(True)
+        for j in job:
+            for _ in range(10):
+                fit_class(j)
+                ext.synchronize()
+                if j["psf"].flow_shape(j["cls"]["R"])[0]:
+                    break
+        ctx.set_tuning(False)
+    if args.split_mode == "flow":
+        for j in job:
+            t, units, ctas, ns = j["psf"].flow_shape(j["cls"]["R"])
+            tuned[j["cls"]["name"]] = {"tuned": t, "units": units, "ctas_per_stage": ctas, "ns_per_eval": ns}
 
     # warm-up (split path), also primes tables and the slot pool
     for _ in range(args.warmup):
@@ -373,53 +428,59 @@ def main():
     ms_step = ms / args.steps
     value = n_total * world / (ms_step / 1000.0)
 
-    # per-class split timing (one extra pass outside the timed region), then a
-    # pass with every launch bracketed by CUDA events for the per-kernel times
-    per_class = {}
-    class_stats = {}
+    # per class: time (CUDA events around the call), then the kernel time of a
+    # profiled pass (every launch bracketed by events), evaluations logged per ROI
+    per_class, kern_ms = {}, {}
     for j in job:
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(ext)
-        p = z.PSF.fit_params(precision=z.ZOLA_PREC_SPLIT, **j["prm_kw"])
-        j["psf"].fit_dev(j["rois"], j["init"], p, j["out"], j["crlb"], j["nll"], j["status"], j["iters"],
-                         stream=ctx.stream)
+        fit_class(j)
         e1.record(ext)
         e1.synchronize()
         t = e0.elapsed_time(e1) / 1000.0
-        per_class[j["cls"]["name"]] = {"rois": int(j["rois"].shape[0]), "seconds": t,
-                                       "fits_per_s": j["rois"].shape[0] / t,
-                                       "mean_evals": float(j["iters"].double().mean().item())}
-    stats = None
-    for j in job:
+        name = j["cls"]["name"]
+        per_class[name] = {"rois": int(j["rois"].shape[0]), "seconds": t, "fits_per_s": j["rois"].shape[0] / t,
+                           "mean_evals": float(j["iters"].double().mean().item())}
         ctx.profile(True)
         ctx.stage_stats(reset=True)
-        p = z.PSF.fit_params(precision=z.ZOLA_PREC_SPLIT, **j["prm_kw"])
-        j["psf"].fit_dev(j["rois"], j["init"], p, j["out"], j["crlb"], j["nll"], j["status"], j["iters"],
-                         stream=ctx.stream)
-        class_stats[j["cls"]["name"]] = st = ctx.stage_stats(reset=True)
+        fit_class(j)
+        st = ctx.stage_stats(reset=True)
         ctx.profile(False)
-        stats = st if stats is None else {k: (stats[k][0] + v[0], stats[k][1] + v[1]) for k, v in st.items()}
-
-    # per-class useful evaluations for the roofline
+        kern_ms[name] = {k: v for k, v in st.items() if v[1]}
     iters = {j["cls"]["name"]: int(j["iters"].sum().item()) for j in job}
     split_res = {j["cls"]["name"]: (j["out"].cpu().numpy(), j["status"].cpu().numpy()) for j in job}
 
-    # plain FP64 GPU form on a sample of the same job (and the accuracy check)
-    fp64 = {}
-    acc = {"max_dxy_nm": 0.0, "max_dz_nm": 0.0, "max_dA_rel": 0.0, "compared": 0, "converged_frac": 0.0}
+    # the round-based stage kernels per stage, for the explanation (optional)
+    breakdown = None
+    if args.stage_breakdown:
+        ctx.set_split_mode("staged")
+        ctx.set_pool(16384)
+        breakdown = {}
+        for j in job:
+            ctx.profile(True)
+            ctx.stage_stats(reset=True)
+            fit_class(j)
+            st = ctx.stage_stats(reset=True)
+            ctx.profile(False)
+            ev = iters[j["cls"]["name"]]
+            breakdown[j["cls"]["name"]] = {k: {"ms": round(v[0], 3), "launches": v[1],
+                                               "sm_clocks_per_eval": round(v[0] * 1e-3 * 1.965e9 * 148 / max(1, ev))}
+                                           for k, v in st.items() if v[1]}
+        ctx.set_pool(args.pool)
+        ctx.set_split_mode(args.split_mode)
+
+    # plain FP64 GPU form on a sample of the same job (speed-up and accuracy, every status)
+    fp64, acc64 = {}, {}
     t_job64 = 0.0
-    conv = []
     for j in job:
         cnt = j["rois"].shape[0]
-        m = max(64, int(args.fp64_sample * j["cls"]["frac"]))
-        m = min(m, cnt)
+        m = min(cnt, max(64, int(args.fp64_sample * j["cls"]["frac"])))
         sl = slice(0, m)
         p64 = z.PSF.fit_params(precision=z.ZOLA_PREC_FP64, **j["prm_kw"])
         out64 = torch.empty((m, 5), dtype=torch.float64, device=device)
         st64 = torch.empty(m, dtype=torch.int32, device=device)
         it64 = torch.empty(m, dtype=torch.int32, device=device)
-        # warm-up then timed pass on the library stream
         j["psf"].fit_dev(j["rois"][:64], j["init"][:64], p64, out64[:64], None, None, st64[:64], it64[:64],
                          stream=ctx.stream)
         e0 = torch.cuda.Event(enable_timing=True)
@@ -430,34 +491,34 @@ def main():
         e1.synchronize()
         t = e0.elapsed_time(e1) / 1000.0
         t_job64 += t / m * cnt
-        fp64[j["cls"]["name"]] = {"sample": m, "seconds": t, "fits_per_s": m / t}
-        a = out64.cpu().numpy()
-        sa = st64.cpu().numpy()
-        b, sb = split_res[j["cls"]["name"]]
-        b, sb = b[:m], sb[:m]
-        ok = (sa == 1) & (sb == 1)
-        conv.append(ok.mean())
-        d = np.abs(a[ok] - b[ok])
-        if j["cls"]["zsym"]:
-            d[:, 2] = np.abs(np.abs(a[ok, 2]) - np.abs(b[ok, 2]))
-        acc["max_dxy_nm"] = max(acc["max_dxy_nm"], float(d[:, :2].max() * 1000) if ok.any() else 0.0)
-        acc["max_dz_nm"] = max(acc["max_dz_nm"], float(d[:, 2].max() * 1000) if ok.any() else 0.0)
-        acc["max_dA_rel"] = max(acc["max_dA_rel"], float((d[:, 3] / a[ok, 3]).max()) if ok.any() else 0.0)
-        acc["compared"] += int(ok.sum())
-        if ok.any():
-            within = (d[:, :2].max(1) <= 0.5e-3) & (d[:, 2] <= 1e-3) & (d[:, 3] / a[ok, 3] <= 1e-3)
-            acc.setdefault("per_class", {})[j["cls"]["name"]] = {
-                "compared": int(ok.sum()), "within_tolerance": float(within.mean()),
-                "p99_dxy_nm": float(np.percentile(d[:, :2].max(1), 99) * 1000),
-                "p99_dz_nm": float(np.percentile(d[:, 2], 99) * 1000),
-                "p99_dA_rel": float(np.percentile(d[:, 3] / a[ok, 3], 99))}
-    acc["converged_frac"] = float(np.mean(conv))
+        name = j["cls"]["name"]
+        ev64 = int(it64.sum().item())
+        fp64[name] = {"sample": m, "seconds": t, "fits_per_s": m / t,
+                      "fp64_tflops": round(ev64 * (flops_per_eval(j["cls"]["R"], j["cls"]["N"]) +
+                                                   8 * (j["cls"]["R"] * window(j["cls"]["R"], j["cls"]["N"]) ** 2 +
+                                                        j["cls"]["R"] ** 2 * window(j["cls"]["R"], j["cls"]["N"])))
+                                           / t / 1e12, 3)}
+        b, sb = split_res[name]
+        acc64[name] = accuracy_block(out64.cpu().numpy(), st64.cpu().numpy(), b[:m], sb[:m], j["cls"]["zsym"])
     fp64_value = n_total / t_job64
 
-    # roofline of the dominant kernel.  Each split stage has an algorithmic flop
-    # count (a complex MAC = 8 flops) and an algorithmic DRAM byte count (the
-    # operands it must read and write per evaluation); its bound is the larger
-    # of the two time floors at the measured peaks.
+    # against the FP64 oracle of the same fit (CPU, all host threads) on a sample, every status
+    acc_oracle = {}
+    if rank == 0 and args.oracle_sample > 0:
+        threads = os.cpu_count() or 1
+        for j in job:
+            cls = j["cls"]
+            m = min(args.oracle_sample, j["rois"].shape[0])
+            ref = O.OraclePSF(cls["N"], DX, 1.4, 0.66, 1.518, 1.518, 0.9, j["zern"], gauss_f32=False)
+            kw = j["prm_kw"]
+            o, _, so, _ = ref.fit_lm(j["rois"][:m].double().cpu().numpy(), j["init_np"][:m], kw["zmin"], kw["zmax"],
+                                     kw["xymax"], tol_xyz=kw["tol_xyz"], max_iter=kw["max_iter"], threads=threads)
+            b, sb = split_res[cls["name"]]
+            acc_oracle[cls["name"]] = accuracy_block(o, so, b[:m], sb[:m], cls["zsym"])
+
+    # roofline: the dataflow kernel (the whole fit) of the class with the most
+    # device time, tensor-bound by SURVEY 8(d): flops of the model evaluations it
+    # made / its CUDA-event duration, against the sustained measured bf16 peak
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -467,66 +528,35 @@ def main():
     peak_tf = peaks.get("bf16_tflops_sustained", 1400.0)
     peak_gbs = peaks.get("hbm_gbs", 6650.0)
     peak_src = "of measured" if "bf16_tflops_sustained" in peaks and "hbm_gbs" in peaks else "of fallback"
-    flops, nbytes = {}, {}
-    fused45 = lambda R: R >= 40  # noqa: E731  (the library's path choice: by ROI side alone)
-    for j in job:
-        R, N = j["cls"]["R"], j["cls"]["N"]
-        W, D = window(R, N), disk_rows(N)
-        DP = 32 if D <= 32 else 64
-        K1, RP = 2 * DP, (R + 15) // 16 * 16
-        ev = iters[j["cls"]["name"]]
-        a2, a3, jb, roi, maps = 8 * W * K1, 10 * W * W, 16 * RP * W, 4 * R * R, 16 * R * R
-        flops[j["cls"]["name"]] = {"split_stage1_pupil_dft": ev * 3 * 8 * W * D * D,
-                                   "split_stage2_window_dft": ev * 4 * 8 * W * W * D,
-                                   "split_stage3_blur_rows": ev * 4 * 2 * R * W * W,
-                                   "split_stage4_blur_cols": ev * 4 * 2 * R * R * W}
-        nbytes[j["cls"]["name"]] = {"split_stage1_pupil_dft": ev * a2,
-                                    "split_stage2_window_dft": ev * (a2 + a3),
-                                    "split_stage3_blur_rows": ev * (a3 + jb),
-                                    "split_stage4_blur_cols": ev * (jb + (roi if fused45(R) else maps)),
-                                    "split_stage5_likelihood_lm": ev * (0 if fused45(R) else maps + roi)}
+    kernel_key = "split_dataflow" if args.split_mode == "flow" else None
     by_class = {}
-    best = None
-    for name, st in class_stats.items():
-        by_class[name] = {}
-        for k, (ms_k, n_k) in st.items():
-            if not n_k:
-                continue
-            e = {"ms": round(ms_k, 3), "launches": n_k}
-            sec = ms_k / 1000.0
-            if ms_k > 0 and k in flops[name]:
-                tf = flops[name][k] / sec / 1e12
-                e.update(tflops=round(tf, 2), tensor_frac=round(tf / peak_tf, 4))
-            if ms_k > 0 and k in nbytes[name]:
-                gbs = nbytes[name][k] / sec / 1e9
-                e.update(gbs=round(gbs, 1), hbm_frac=round(gbs / peak_gbs, 4))
-            if ms_k > 0 and k in nbytes[name] and (best is None or ms_k > best[2]):
-                best = (name, k, ms_k)
-            by_class[name][k] = e
-    stage_table = {k: {"ms": round(v[0], 3), "launches": v[1]} for k, v in stats.items() if v[1]}
-    name, dom, _ = best
-    ent = by_class[name][dom]
-    hbm_floor = nbytes[name].get(dom, 0) / (peak_gbs * 1e9)
-    tensor_floor = flops[name].get(dom, 0) / (peak_tf * 1e12)
-    traffic = NCU_TRAFFIC.get((name, dom))
-    if hbm_floor >= tensor_floor:
-        roofline = {"bound": "hbm", "achieved": ent["gbs"], "peak": peak_gbs, "unit": "GB/s", "frac": ent["hbm_frac"],
-                    "tensor_achieved_tflops": ent.get("tflops"), "tensor_frac": ent.get("tensor_frac")}
-    else:
-        roofline = {"bound": "tensor", "achieved": ent["tflops"], "peak": peak_tf, "unit": "TFLOP/s",
-                    "frac": ent["tensor_frac"], "hbm_achieved_gbs": ent.get("gbs"), "hbm_frac": ent.get("hbm_frac")}
-    roofline.update({
-        "kernel": dom, "class": name, "peak_source": peak_src,
-        "traffic": None if traffic is None else int(traffic * min(args.pool or 4096, 32768)),
-        "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu launch of this kernel on "
-                        "this class (4096 slots), scaled to the pool by slots",
-        "algorithmic_bytes_per_launch": None if dom not in nbytes[name] else
-        int(nbytes[name][dom] / max(1, iters[name]) * min(args.pool or 4096, 32768)),
-        "stages_all_classes": stage_table, "per_class": by_class,
-        "note": "achieved = algorithmic bytes (operands each evaluation must read and write: A2 8*W*K1, A3 "
-                "10*W^2, J 16*RP*W, ROI 4*R^2, maps 16*R^2 bytes) or algorithmic flops (complex MAC = 8 flops) of "
-                "the useful model evaluations / summed CUDA-event duration of that kernel's launches for that "
-                "class; the bound is the larger floor at the measured peaks (copy GB/s, sustained bf16 TFLOP/s)"})
+    tot_flops = tot_s = 0.0
+    for j in job:
+        name, R, N = j["cls"]["name"], j["cls"]["R"], j["cls"]["N"]
+        km = kern_ms[name]
+        ms_k = km[kernel_key][0] if kernel_key in km else sum(v[0] for v in km.values())
+        fl = iters[name] * flops_per_eval(R, N)
+        tf = fl / (ms_k / 1000.0) / 1e12
+        by_class[name] = {"kernel_ms": round(ms_k, 3), "evaluations": iters[name], "flops_per_eval": flops_per_eval(R, N),
+                          "tflops": round(tf, 2), "tensor_frac": round(tf / peak_tf, 4),
+                          "input_gbs": round(iters[name] * 4 * R * R / (ms_k / 1000.0) / 1e9, 1)}
+        tot_flops += fl
+        tot_s += ms_k / 1000.0
+    dom = max(by_class, key=lambda k: by_class[k]["kernel_ms"])
+    ent = by_class[dom]
+    traffic = NCU_TRAFFIC.get((dom, kernel_key))
+    roofline = {"bound": "tensor", "achieved": ent["tflops"], "peak": peak_tf, "unit": "TFLOP/s",
+                "frac": ent["tensor_frac"], "kernel": "k_flow (dataflow split fit)" if kernel_key else args.split_mode,
+                "class": dom, "peak_source": peak_src + " (sustained bf16)",
+                "traffic": None if traffic is None else int(traffic * iters[dom]),
+                "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum per launch from one ncu capture of this "
+                                "kernel on a smaller batch of this class, scaled by model evaluations",
+                "whole_job_tflops": round(tot_flops / tot_s / 1e12, 2),
+                "whole_job_tensor_frac": round(tot_flops / tot_s / 1e12 / peak_tf, 4),
+                "per_class": by_class, "hbm_peak_gbs": peak_gbs,
+                "note": "achieved = SURVEY 8(d) algorithmic flops of the model evaluations made (3*8*W*D^2 + 4*8*W^2*D "
+                        "per evaluation, complex MAC = 8 flops; evaluations logged per ROI) / CUDA-event duration of the "
+                        "kernel launch; peak = sustained measured bf16 (FP16 runs at the same rate)"}
 
     # end to end through the host C-ABI (pinned host buffers, H2D + D2H inside the call)
     e2e = None
@@ -572,13 +602,15 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f16x3 (split) / f32 sums / f64 solve", "data": "synthetic",
-                "config": dict(config_block(args.rois), parallelism=f"replicas x{world}", split_kernels=args.split_mode, pool=args.pool),
+                "config": dict(config_block(args.rois), parallelism=f"replicas x{world}", split_kernels=args.split_mode,
+                               pool=args.pool or "library default"),
                 "e2e": e2e, "gpu_launches": int(launches), "clocks": clk, "roofline": roofline,
                 "cpu_baseline": cpu,
-                "split_per_class": per_class,
+                "split_per_class": per_class, "dataflow_shape": tuned,
                 "fp64_plain_gpu": {"value": fp64_value, "unit": UNIT, "per_class": fp64},
                 "speedup_vs_fp64_plain": value / world / fp64_value,
-                "accuracy_vs_fp64": acc,
+                "accuracy_vs_oracle": acc_oracle, "accuracy_vs_fp64_gpu": acc64,
+                "stage_breakdown_round_based": breakdown,
                 "detect_fit_pipeline": detect}
         print(json.dumps(line), flush=True)
     for j in job:

@@ -341,22 +341,24 @@ ZOLA_API int zola_fit_batch_noalloc(zola_psf* psf, int R, const float* d_rois, c
  * (pool state up to 8 GB, at most 32768 slots).  Larger pools amortise each
  * launch's fixed work and shorten the draining tail of a batch. */
 ZOLA_API int zola_ctx_set_pool(zola_ctx* ctx, int max_slots);
-/* Split fit kernel layout.  ZOLA_SPLIT_FLOW (default) runs the whole fit as
- * one cooperative kernel: the four stages (pupil DFT, window DFT, row blur,
- * column blur + likelihood sums + LM step) run at once on their own SMs and
- * each unit of slots moves to the next stage as soon as it is done, with no
- * host round trip.  ZOLA_SPLIT_STAGED runs the same stage code as four
- * kernels per LM round over the whole slot pool (the same results bit for
- * bit).  ZOLA_SPLIT_FUSED runs stage 1 plus one kernel for stages 2-5 per
- * round (same arithmetic, FP32 sums in another order); windows whose fused
- * plan does not fit in shared memory run staged. */
+/* Split fit kernel layout.  ZOLA_SPLIT_STAGED (default) runs the five stages
+ * (pupil DFT, window DFT, row blur, column blur + likelihood sums, FP64 LM
+ * step) as five kernels per LM round over the whole slot pool.
+ * ZOLA_SPLIT_FLOW runs the same stage code as one cooperative kernel: the
+ * stages run at once on their own SMs, each unit of slots moves to the next
+ * stage as soon as it is done, converged fits retire and refill from a device
+ * queue, and there is no host round trip (the same results bit for bit; it
+ * also takes inputs that are still arriving, zola_fit_batch_stream_dev).
+ * ZOLA_SPLIT_FUSED runs stage 1 plus one kernel for stages 2-5 per round (same
+ * arithmetic, FP32 sums in another order); windows whose fused plan does not
+ * fit in shared memory run staged. */
 #define ZOLA_SPLIT_STAGED 0
 #define ZOLA_SPLIT_FUSED 1
 #define ZOLA_SPLIT_FLOW 2
 ZOLA_API int zola_ctx_set_split_mode(zola_ctx* ctx, int mode);
 /* Dataflow kernel shape: units = units of slots in flight (0: two per SM),
- * ctas[4] = CTAs per stage (all 0: a split by window size; otherwise they must
- * add up to the SM count).  Results do not depend on either. */
+ * ctas[5] = CTAs per stage (null or all 0: a split by window size; otherwise
+ * each at least 1, adding up to the SM count).  Results do not depend on either. */
 ZOLA_API int zola_ctx_set_flow(zola_ctx* ctx, int units, const int* ctas);
 /* Autotuner of the dataflow kernel (enable = 1): the first large fits of each
  * class (pupil grid, ROI side) try a few shapes (CTAs per stage rebalanced
@@ -365,10 +367,15 @@ ZOLA_API int zola_ctx_set_flow(zola_ctx* ctx, int units, const int* ctas);
  * written to cache_path (JSON, nullable).  A fit's results do not depend on the
  * shape, so tuning changes timings only. */
 ZOLA_API int zola_ctx_set_tuning(zola_ctx* ctx, int enable, const char* cache_path);
-/* Shape the dataflow kernel uses for psf's fits of R x R ROIs: units, ctas[4]
+/* Shape the dataflow kernel uses for psf's fits of R x R ROIs: units, ctas[5]
  * and, when tuned, the measured ns per model evaluation (nullable pointers).
  * Returns 1 when tuned, 0 for the default shape, < 0 on error. */
 ZOLA_API int zola_fit_flow_shape(zola_psf* psf, int R, int* units, int* ctas, double* ns_per_eval);
+/* Bookkeeping of the last dataflow fit on this context, per stage (pupil DFT,
+ * window DFT, row blur, column blur + sums, LM step): the fraction of time its
+ * CTAs had a unit to work on, and the busy GPU clocks one CTA spent per unit;
+ * and the model evaluations made (nullable pointers, 5 values each). */
+ZOLA_API int zola_ctx_flow_stats(zola_ctx* ctx, double* busy, double* clocks_per_unit, double* evaluations);
 /* Upper bound, in GPU clocks, on any single device-side wait of the split fit
  * (a bulk copy or MMA completion, or the dataflow kernel waiting for a unit to
  * become ready, e.g. for inputs to arrive); 0 restores the default (2^31, about

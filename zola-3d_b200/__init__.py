@@ -73,7 +73,7 @@ EXPORTS = ["zola_ctx_create", "zola_ctx_destroy", "zola_last_error", "zola_ctx_s
            "zola_calib_backward", "zola_calib_fit", "zola_ctx_set_split_mode", "zola_crlb_curve",
            "zola_psf_center_search", "zola_calib_init", "zola_drift", "zola_fit_batch_scmos",
            "zola_fit_batch_scmos_dev", "zola_localize_frames_scmos", "zola_ctx_set_flow", "zola_ctx_set_wait_limit",
-           "zola_fit_batch_stream_dev", "zola_ctx_set_tuning", "zola_fit_flow_shape"]
+           "zola_fit_batch_stream_dev", "zola_ctx_set_tuning", "zola_fit_flow_shape", "zola_ctx_flow_stats"]
 STAGES = ["split_stage1_pupil_dft", "split_stage2_window_dft", "split_stage3_blur_rows",
           "split_stage4_blur_cols_sums_lm", "split_fused_stages2_5", "fp64_fit", "fp64_model", "other",
           "split_dataflow"]
@@ -110,6 +110,7 @@ def lib():
         L.zola_ctx_set_wait_limit.argtypes = [vp, ctypes.c_longlong]
         L.zola_ctx_set_tuning.argtypes = [vp, i, ctypes.c_char_p]
         L.zola_fit_flow_shape.argtypes = [vp, i, vp, vp, vp]
+        L.zola_ctx_flow_stats.argtypes = [vp, vp, vp, vp]
         L.zola_crlb_curve.argtypes = [vp, i, vp, i, d, d, d, d, vp]
         L.zola_psf_center_search.argtypes = [vp, i, d, i, ctypes.POINTER(d)]
         L.zola_ctx_profile.argtypes = [vp, i]
@@ -175,21 +176,29 @@ class Context:
         self.check(lib().zola_ctx_set_pool(self.h, int(max_slots)), "zola_ctx_set_pool")
 
     def set_split_mode(self, mode):
-        """"flow" (default): the whole split fit as one dataflow kernel; "staged": four stage kernels per
-        LM round (the same results bit for bit); "fused": stage 1 + one kernel for stages 2-5."""
+        """"staged" (default): five stage kernels per LM round; "flow": the whole split fit as one dataflow
+        kernel (the same results bit for bit); "fused": stage 1 + one kernel for stages 2-5."""
         code = {"staged": ZOLA_SPLIT_STAGED, "fused": ZOLA_SPLIT_FUSED, "flow": ZOLA_SPLIT_FLOW}[mode]
         self.check(lib().zola_ctx_set_split_mode(self.h, code), "zola_ctx_set_split_mode")
 
     def set_flow(self, units=0, ctas=None):
         """Dataflow kernel shape: units of slots in flight (0: automatic) and CTAs per stage (None:
-        automatic; else four counts adding up to the SM count).  Results do not depend on either."""
-        arr = None if ctas is None else (ctypes.c_int * 4)(*[int(c) for c in ctas])
+        automatic; else five counts adding up to the SM count).  Results do not depend on either."""
+        arr = None if ctas is None else (ctypes.c_int * 5)(*[int(c) for c in ctas])
         self.check(lib().zola_ctx_set_flow(self.h, int(units), arr), "zola_ctx_set_flow")
 
     def set_tuning(self, enable=True, cache_path=None):
         """Autotune the dataflow kernel's shape per (pupil grid, ROI side) on large fits; cache_path: JSON cache."""
         self.check(lib().zola_ctx_set_tuning(self.h, int(bool(enable)), cache_path.encode() if cache_path else None),
                    "zola_ctx_set_tuning")
+
+    def flow_stats(self):
+        """Last dataflow fit: per stage busy fraction and busy clocks per unit, and the evaluations made."""
+        busy = np.zeros(5)
+        cpu = np.zeros(5)
+        ev = ctypes.c_double()
+        self.check(lib().zola_ctx_flow_stats(self.h, _ptr(busy), _ptr(cpu), ctypes.byref(ev)), "zola_ctx_flow_stats")
+        return {"busy": busy.tolist(), "clocks_per_unit": cpu.tolist(), "evaluations": ev.value}
 
     def set_wait_limit(self, clocks):
         """Upper bound (GPU clocks) on any device-side wait of the split fit; 0 = default (2^31)."""
@@ -326,7 +335,7 @@ class PSF:
     def flow_shape(self, R):
         """(tuned, units, [CTAs per stage], ns per evaluation) of the dataflow kernel for R x R ROIs."""
         u = ctypes.c_int()
-        c = (ctypes.c_int * 4)()
+        c = (ctypes.c_int * 5)()
         ns = ctypes.c_double()
         rc = lib().zola_fit_flow_shape(self.h, int(R), ctypes.byref(u), c, ctypes.byref(ns))
         if rc < 0:

@@ -297,18 +297,19 @@ int zola_ctx_set_split_mode(zola_ctx* ctx, int mode) {
 
 int zola_ctx_set_flow(zola_ctx* ctx, int units, const int* ctas) {
     if (!ctx || units < 0) return ZOLA_E_ARG;
-    int sum = 0;
+    int sum = 0, zeros = 0;
     if (ctas) {
-        for (int s = 0; s < 4; ++s) {
-            if (ctas[s] < 0 || (ctas[s] == 0 && (ctas[0] | ctas[1] | ctas[2] | ctas[3]) != 0))
-                return set_err(ctx, ZOLA_E_ARG, "zola_ctx_set_flow: every stage needs at least one CTA");
+        for (int s = 0; s < zola::FLOW_STAGES; ++s) {
+            if (ctas[s] < 0) return set_err(ctx, ZOLA_E_ARG, "zola_ctx_set_flow: negative CTA count");
+            zeros += ctas[s] == 0;
             sum += ctas[s];
         }
-        if (sum != 0 && sum != ctx->num_sms)
-            return set_err(ctx, ZOLA_E_ARG, "zola_ctx_set_flow: the CTAs per stage must add up to the SM count");
+        if (sum != 0 && (zeros || sum != ctx->num_sms))
+            return set_err(ctx, ZOLA_E_ARG,
+                           "zola_ctx_set_flow: every stage needs a CTA, and the counts must add up to the SM count");
     }
     ctx->flow_units = units;
-    for (int s = 0; s < 4; ++s) ctx->flow_ctas[s] = ctas ? ctas[s] : 0;
+    for (int s = 0; s < zola::FLOW_STAGES; ++s) ctx->flow_ctas[s] = ctas ? ctas[s] : 0;
     return ZOLA_OK;
 }
 
@@ -329,8 +330,18 @@ int zola_fit_flow_shape(zola_psf* psf, int R, int* units, int* ctas, double* ns_
     const bool tuned = flow_shape(ctx, psf, w, &f, ns_per_eval);
     if (units) *units = f.units;
     if (ctas)
-        for (int s = 0; s < 4; ++s) ctas[s] = f.ctas[s];
+        for (int s = 0; s < zola::FLOW_STAGES; ++s) ctas[s] = f.ctas[s];
     return tuned ? 1 : 0;
+}
+
+int zola_ctx_flow_stats(zola_ctx* ctx, double* busy, double* clocks_per_unit, double* evaluations) {
+    if (!ctx) return ZOLA_E_ARG;
+    for (int s = 0; s < zola::FLOW_STAGES; ++s) {
+        if (busy) busy[s] = ctx->flow_busy[s];
+        if (clocks_per_unit) clocks_per_unit[s] = ctx->flow_clk_per_unit[s];
+    }
+    if (evaluations) *evaluations = ctx->flow_evals;
+    return ZOLA_OK;
 }
 
 int zola_ctx_set_wait_limit(zola_ctx* ctx, long long clocks) {

@@ -108,10 +108,10 @@ struct SplitDev {
     int* active;   // occupied slots
     int* err;      // bounded-wait timeout flag
     int* navail;   // ROIs [0, *navail) are on the device (all n unless the inputs are still arriving)
-    int* ustate;   // per unit of slots: 4 e + s (ready for stage s of evaluation e), or UNIT_DEAD
+    int* ustate;   // per unit of slots: 5 e + s (ready for stage s of evaluation e), or UNIT_DEAD
     long long wait_limit;  // clocks a dataflow scheduler waits for a ready unit before it gives up
     unsigned long long* evals;  // dataflow kernel: model evaluations (LM steps) done
-    unsigned long long* clk;    // dataflow kernel: per CTA, clocks without a ready unit and clocks in all
+    unsigned long long* clk;    // dataflow kernel: per CTA, clocks without a ready unit, clocks in all, units done
     SplitScales sc;
 };
 
@@ -528,9 +528,10 @@ __device__ __forceinline__ void warp_arrive(uint64_t* mbar) {
 // The persistent stage kernels work in units of UG = max(G1, G2) consecutive
 // slots, so that a unit is made of whole pupil-DFT tiles (G1 slots) and whole
 // window tiles (G2 slots).  The round-based kernels walk the units statically
-// (blockIdx.x, + gridDim.x, ...).  The dataflow kernel (k_flow) runs all four
-// stages at once, each on its own CTAs: a unit's state word counts its
-// finished stages (4 e + s: ready for stage s of its evaluation e; UNIT_DEAD
+// (blockIdx.x, + gridDim.x, ...).  The dataflow kernel (k_flow) runs all five
+// stages at once (the four model stages and the LM step), each on its own
+// CTAs: a unit's state word counts its finished stages (5 e + s: ready for
+// stage s of its evaluation e; UNIT_DEAD
 // once its slots have retired and the ROI queue is empty), and in every CTA one
 // scheduler thread hands the units of its share that are ready for its stage to
 // the CTA's warps through a ring in shared memory.
@@ -562,6 +563,13 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 __device__ __forceinline__ int ld_acquire(const int* p) {
     int v;
     asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+// Relaxed loads of several state words can be in flight together; a unit found
+// ready is then acquired with one fence.
+__device__ __forceinline__ int ld_relaxed(const int* p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
 
@@ -630,6 +638,7 @@ struct StaticUnits {
 
 struct UnitRing {
     int unit[URING], tag[URING];
+    int released;  // units this CTA has finished (for the scheduler's bookkeeping)
     uint64_t full[URING], freed[URING];
 };
 
@@ -669,6 +678,7 @@ struct FlowUnits {
     __device__ void release(const SplitDev& P, int u, int v) {
         __threadfence();
         st_release(P.ustate + u, v);
+        atomicAdd(&r->released, 1);
     }
     // The scheduler thread: scan this CTA's units round-robin and hand out
     // those ready for its stage; stage 1's scheduler refills idle slots first.
@@ -690,48 +700,62 @@ struct FlowUnits {
         };
         const long long start = clock64();
         long long t0 = start, idle = 0, idle_since = -1;
+        constexpr int SCAN = 8;  // state words loaded together
         while (*(volatile int*)P.err == 0) {
             int found = -1, tag = 0, dead = 0;
-            for (int k = 0; k < mine; ++k) {
-                const int i = cur + k < mine ? cur + k : cur + k - mine;
-                const int u = first + i * stride;
-                const int v = ld_acquire(P.ustate + u);
-                if (v < 0) {
-                    ++dead;
-                    continue;
+            for (int k0 = 0; k0 < mine && found < 0; k0 += SCAN) {
+                int vv[SCAN], uu[SCAN];
+#pragma unroll
+                for (int j = 0; j < SCAN; ++j) {
+                    const int k = k0 + j, i = cur + k < mine ? cur + k : cur + k - mine;
+                    uu[j] = first + i * stride;
+                    vv[j] = k < mine ? ld_relaxed(P.ustate + uu[j]) : UNIT_CLAIMED;
                 }
-                if ((v & 3) != stage || (v & UNIT_CLAIMED)) continue;
-                if (stage == 0) {
-                    const int ok = unit_refill(P, F, u);
-                    if (ok < 0) ++dead;
-                    if (ok <= 0) continue;
+                for (int j = 0; j < SCAN && k0 + j < mine; ++j) {
+                    const int v = vv[j], u = uu[j];
+                    if (v < 0) {
+                        ++dead;
+                        continue;
+                    }
+                    if ((v & UNIT_CLAIMED) || v % FLOW_STAGES != stage) continue;
+                    asm volatile("fence.acq_rel.gpu;" ::: "memory");  // acquire what the unit's last stage wrote
+                    if (stage == 0) {
+                        const int ok = unit_refill(P, F, u);
+                        if (ok < 0) ++dead;
+                        if (ok <= 0) continue;
+                    }
+                    found = u;
+                    tag = v;
+                    const int i = k0 + j + cur < mine ? k0 + j + cur : k0 + j + cur - mine;
+                    cur = i + 1 < mine ? i + 1 : 0;
+                    break;
                 }
-                found = u;
-                tag = v;
-                cur = i + 1 < mine ? i + 1 : 0;
-                break;
             }
             if (found >= 0) {
                 if (idle_since >= 0) idle += clock64() - idle_since;
                 idle_since = -1;
+                t0 = clock64();
                 P.ustate[found] = tag | UNIT_CLAIMED;  // only this thread reads the claim
                 if (!push(found, tag)) break;
                 t0 = clock64();
                 continue;
             }
             if (dead == mine) break;
-            if (idle_since < 0) idle_since = clock64();
+            // the CTA is idle once every unit handed out has been finished
+            const bool drained = *(volatile int*)&r->released >= qq;
+            if (idle_since < 0 && drained) idle_since = clock64();
             if (clock64() - t0 > P.wait_limit) {
                 atomicExch(P.err, 2);
                 break;
             }
-            __nanosleep(100);
+            __nanosleep(32);
         }
         push(-1, 0);
         const long long end = clock64();
         if (idle_since >= 0) idle += end - idle_since;
-        P.clk[2 * blockIdx.x] = (unsigned long long)idle;
-        P.clk[2 * blockIdx.x + 1] = (unsigned long long)(end - start);
+        P.clk[3 * blockIdx.x] = (unsigned long long)idle;
+        P.clk[3 * blockIdx.x + 1] = (unsigned long long)(end - start);
+        P.clk[3 * blockIdx.x + 2] = (unsigned long long)(qq > 0 ? qq - 1 : 0);
     }
 };
 
@@ -1497,111 +1521,6 @@ __device__ __forceinline__ double warp_reduce_scatter32(double (&v)[32], int lan
 }
 
 constexpr int NSUM = NRED + 1;  // sums per slot: NRED + the non-positive-model flag
-constexpr int S5_UNROLL = 4;               // pixels per lane whose loads are in flight together
-
-// One warp, one slot: likelihood sums at the trial point from the slot's four
-// blurred maps T0 (map m at T0 + m R^2, row-major) (per-pixel terms in FP32;
-// the likelihood and gradient with Kahan compensation, the Hessian and Fisher
-// terms plain; lane partials combined in FP64), written to P.sums for the LM
-// step.  Used for ROIs below 33 px, whose maps sit in shared memory.
-__device__ __noinline__ void slot_sums_warp(const SplitDev& P, const FitIO& F, int slot, const float* T0) {
-    const int lane = threadIdx.x & 31;
-    const int roi = P.slot_roi[slot];
-    const int R = P.R, RR = R * R;
-    const float* d = F.rois + (size_t)roi * RR;
-    const float* sv = F.scmos ? F.scmos + (size_t)roi * RR : nullptr;  // sCMOS var/gain^2 (Localization.java:1132)
-    // normalisation sums.  Each lane walks its pixels k = lane, lane + 32, ...
-    // in order; the loads of S5_UNROLL consecutive pixels are issued together
-    // so that several memory round trips overlap.
-    float ns[4] = {0, 0, 0, 0}, nc = 0.f;
-    for (int k0 = lane; k0 < RR; k0 += 32 * S5_UNROLL) {
-        float tv[S5_UNROLL][4];
-#pragma unroll
-        for (int j = 0; j < S5_UNROLL; ++j) {
-            const int k = k0 + 32 * j;
-            if (k < RR)
-                for (int m = 0; m < 4; ++m) tv[j][m] = T0[m * RR + k];
-        }
-#pragma unroll
-        for (int j = 0; j < S5_UNROLL; ++j) {
-            if (k0 + 32 * j >= RR) continue;
-            const float v = tv[j][0];
-            const float sg = v < 0 ? -1.f : 1.f;
-            kahan_add(ns[0], nc, fabsf(v));
-            ns[1] += sg * tv[j][1];
-            ns[2] += sg * tv[j][2];
-            ns[3] += sg * tv[j][3];
-        }
-    }
-    const float S = (float)warp_sum((double)ns[0] - (double)nc);
-    const float Dx = (float)warp_sum(ns[1]), Dy = (float)warp_sum(ns[2]), Dz = (float)warp_sum(ns[3]);
-    const float invS = 1.f / S;
-    const double* th = P.lm[slot].trial;
-    const float A = (float)th[3], B = (float)th[4];
-    float sg6[6], cg6[6], sh[30];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) { sg6[k] = 0.f; cg6[k] = 0.f; }
-#pragma unroll
-    for (int k = 0; k < 30; ++k) sh[k] = 0.f;
-    bool bad = false;
-    for (int k0 = lane; k0 < RR; k0 += 32 * S5_UNROLL) {
-        float tv[S5_UNROLL][4], dv[S5_UNROLL], vv[S5_UNROLL];
-#pragma unroll
-        for (int jj = 0; jj < S5_UNROLL; ++jj) {
-            const int k = k0 + 32 * jj;
-            if (k < RR) {
-                for (int m = 0; m < 4; ++m) tv[jj][m] = T0[m * RR + k];
-                dv[jj] = d[k];
-                vv[jj] = sv ? sv[k] : 0.f;
-            }
-        }
-#pragma unroll
-        for (int jj = 0; jj < S5_UNROLL; ++jj) {
-            if (k0 + 32 * jj >= RR) continue;
-            const float v = tv[jj][0];
-            const float sgn = v < 0 ? -1.f : 1.f;
-            const float psi = fabsf(v) * invS;
-            float j[5];
-            j[0] = A * (sgn * tv[jj][1] - psi * Dx) * invS;
-            j[1] = A * (sgn * tv[jj][2] - psi * Dy) * invS;
-            j[2] = A * (sgn * tv[jj][3] - psi * Dz) * invS;
-            j[3] = psi;
-            j[4] = 1.f;
-            const float mu = A * psi + B + vv[jj];
-            if (!(mu > 0.f)) { bad = true; continue; }
-            const float dk = dv[jj];
-            kahan_add(sg6[0], cg6[0], dk > 0.f ? mu - dk - dk * logf(mu / dk) : mu);
-            const float wg = 1.f - dk / mu, wf = 1.f / mu, wh = dk * wf * wf;
-#pragma unroll
-            for (int q = 0; q < 5; ++q) kahan_add(sg6[1 + q], cg6[1 + q], wg * j[q]);
-            int o = 0;
-#pragma unroll
-            for (int q = 0; q < 5; ++q)
-#pragma unroll
-                for (int r2 = 0; r2 <= q; ++r2) {
-                    sh[o] += wh * j[q] * j[r2];
-                    sh[o + 15] += wf * j[q] * j[r2];
-                    ++o;
-                }
-        }
-    }
-    // sums 0..31: butterfly reduce-scatter (lane k ends with sum k); 32..35 plainly
-    double v[32];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) v[k] = (double)sg6[k] - (double)cg6[k];
-#pragma unroll
-    for (int k = 0; k < 26; ++k) v[6 + k] = sh[k];
-    const double mine = warp_reduce_scatter32(v, lane);
-    double rest[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) rest[k] = warp_sum((double)sh[26 + k]);
-    const bool anybad = __any_sync(0xffffffffu, bad);
-    double* out = P.sums + (size_t)slot * NSUM;
-    out[lane] = mine;
-    if (lane != 0) return;
-    for (int k = 0; k < 4; ++k) out[32 + k] = rest[k];
-    out[NRED] = anybad ? 1.0 : 0.0;
-}
 
 // The FP64 LM step of one slot from its sums: start or update the damped
 // Gauss-Newton iteration, propose the next trial point, or retire the ROI and
@@ -1646,6 +1565,103 @@ __device__ __noinline__ void lm_slot(const SplitDev& P, const FitIO& io, int slo
     } else {
         P.slot_roi[slot] = -1;
         atomicSub(P.active, 1);
+    }
+}
+
+// The round-based fit's LM step: every occupied slot of the pool, one thread each.
+__global__ void k_lm(SplitDev P, FitIO F) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot < P.P) lm_slot(P, F, slot);
+}
+
+// ------------------------------------------------- LM stage (dataflow) -----
+// The FP64 LM steps of the dataflow kernel.  Warp k of an LM CTA owns the
+// units first + (k + i warps) stride and polls their state words; when a
+// unit's sums are done, lanes 0 .. UG - 1 apply the LM step to the unit's slots
+// (retiring converged fits and refilling their slots) and lane 0 publishes the
+// unit's next state.  One unit per warp, so the LM steps of different units
+// overlap, and many units are stepped at once: the FP64 work never holds up
+// the tensor-core stages.
+__device__ void lm_role(const SplitDev& P, const FitIO& F, int first, int stride) {
+    const int UG = unit_slots(P.G1, P.G2), U = P.P / UG;
+    const int lane = threadIdx.x & 31, g = lane, lead = 0;
+    const unsigned gmask = 0xffffffffu;
+    const int group = (int)threadIdx.x >> 5, ngroups = (int)blockDim.x >> 5;
+    __shared__ unsigned long long busy_sum, units_done;
+    __shared__ int owners;
+    if (threadIdx.x == 0) {
+        busy_sum = 0;
+        units_done = 0;
+        owners = 0;
+    }
+    __syncthreads();
+    const long long start = clock64();
+    long long busy = 0, idle_since = start;
+    int mine = 0, done_units = 0;
+    for (int u = first + group * stride; u < U; u += ngroups * stride) ++mine;
+    if (mine && g == 0) atomicAdd(&owners, 1);
+    // every decision that ends a loop is taken by the group's first lane and
+    // broadcast, so the lanes of a group stay together
+    const unsigned long long cap = (unsigned long long)F.n * (F.prm.max_iter + 1) + 2ull * P.P;
+    for (;;) {
+        int ctl = 0;
+        if (g == 0) ctl = *(volatile int*)P.err != 0;
+        if (__shfl_sync(gmask, ctl, lead)) break;
+        bool any = false;
+        int dead = 0;
+        for (int u = first + group * stride; u < U; u += ngroups * stride) {
+            int v = 0;
+            if (g == 0) v = ld_acquire(P.ustate + u);
+            v = __shfl_sync(gmask, v, lead);
+            if (v < 0) {
+                ++dead;
+                continue;
+            }
+            // (a unit another stage handed out carries the claim bit; this stage claims none)
+            if ((v & UNIT_CLAIMED) || v % FLOW_STAGES != FLOW_STAGES - 1) continue;
+            const long long b0 = clock64();
+            if (g < UG) lm_slot(P, F, u * UG + g);
+            __syncwarp(gmask);
+            // every ROI takes at most max_iter evaluations: more means the fit lost
+            // track of its slots, and the whole kernel stops with an error
+            int stop = 0;
+            if (g == 0) stop = *(volatile unsigned long long*)P.evals > cap;
+            if (__shfl_sync(gmask, stop, lead)) {
+                if (g == 0) atomicExch(P.err, 3);
+                break;
+            }
+            if (g == 0) {
+                __threadfence();
+                st_release(P.ustate + u, unit_after_lm(P, F, u, v));
+                ++done_units;
+            }
+            busy += clock64() - b0;
+            any = true;
+        }
+        if (dead == mine) break;
+        if (any) {
+            idle_since = clock64();
+            continue;
+        }
+        int late = 0;
+        if (g == 0) late = clock64() - idle_since > P.wait_limit;
+        if (__shfl_sync(gmask, late, lead)) {
+            if (g == 0) atomicExch(P.err, 2);
+            break;
+        }
+        __nanosleep(200);
+    }
+    if (g == 0) {
+        atomicAdd(&busy_sum, (unsigned long long)busy);
+        atomicAdd(&units_done, (unsigned long long)done_units);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const long long total = clock64() - start;
+        const long long used = owners ? (long long)(busy_sum / (unsigned long long)owners) : 0;
+        P.clk[3 * blockIdx.x] = (unsigned long long)(total > used ? total - used : 0);
+        P.clk[3 * blockIdx.x + 1] = (unsigned long long)total;
+        P.clk[3 * blockIdx.x + 2] = units_done;
     }
 }
 
@@ -1939,10 +1955,7 @@ __device__ __forceinline__ void stage45_body(const SplitDev& P, const FitIO& F, 
             }
         }
         if (abort) break;
-        // the unit's LM steps, one lane per slot, then its next state
-        if (warp == 0 && lane < UG) lm_slot(P, F, unit * UG + lane);
-        epi_bar<E45_THREADS>();
-        if (t == 0) units.release(P, unit, unit_after_lm(P, F, unit, tag));
+        if (t == 0) units.release(P, unit, tag + 1);  // (the sums were written before the last barrier)
     }
     if (t == 0) umma::mbar_wait(&fin, 0, P.err);  // every MMA of this CTA has completed
     epi_bar<E45_THREADS>();
@@ -1954,6 +1967,109 @@ __global__ void __launch_bounds__(S45_THREADS, 1) k_stage45p(SplitDev P, FitIO F
     stage45_body(P, F, StaticUnits{});
 }
 
+// Likelihood sums of a unit's live slots from their maps in shared memory (slot
+// g, map m at Tm + (4 g + m) R^2, row-major), all 16 epilogue warps at once:
+// 16 / UG warps per slot, each thread summing strided pixels (per-pixel terms
+// in FP32; the normalisation, likelihood and gradient with Kahan
+// compensation), warp partials combined in FP64 in a fixed order.  Writes
+// P.sums; the caller's next barrier publishes them.
+__device__ __noinline__ void unit_sums(const SplitDev& P, const FitIO& F, int unit, const float* Tm,
+                                       double (*red)[NRED], double (*nrm)[4], int* badw) {
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31, UG = unit_slots(P.G1, P.G2);
+    const int wps = (SPLIT_THREADS / 32) / UG, g = warp / wps, ws = warp - g * wps;
+    const int tid = ws * 32 + lane, nts = wps * 32, R = P.R, RR = R * R;
+    const int slot = unit * UG + g, roi = P.slot_roi[slot];
+    const float* T0 = Tm + (size_t)g * 4 * RR;
+    {
+        float ns[4] = {0, 0, 0, 0}, nc = 0.f;
+        if (roi >= 0)
+            for (int k = tid; k < RR; k += nts) {
+                const float v = T0[k], sg = v < 0 ? -1.f : 1.f;
+                kahan_add(ns[0], nc, fabsf(v));
+                ns[1] += sg * T0[RR + k];
+                ns[2] += sg * T0[2 * RR + k];
+                ns[3] += sg * T0[3 * RR + k];
+            }
+        const double v0 = warp_sum((double)ns[0] - (double)nc), v1 = warp_sum(ns[1]), v2 = warp_sum(ns[2]),
+                     v3 = warp_sum(ns[3]);
+        if (lane == 0) { nrm[warp][0] = v0; nrm[warp][1] = v1; nrm[warp][2] = v2; nrm[warp][3] = v3; }
+    }
+    epi_bar();
+    double s4[4] = {0, 0, 0, 0};
+    for (int w = g * wps; w < (g + 1) * wps; ++w)
+        for (int q = 0; q < 4; ++q) s4[q] += nrm[w][q];
+    const float S = (float)s4[0], Dx = (float)s4[1], Dy = (float)s4[2], Dz = (float)s4[3];
+    const float invS = 1.f / S;
+    float sg6[6], cg6[6], sh[30];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) { sg6[k] = 0.f; cg6[k] = 0.f; }
+#pragma unroll
+    for (int k = 0; k < 30; ++k) sh[k] = 0.f;
+    bool bad = false;
+    if (roi >= 0) {
+        const double* th = P.lm[slot].trial;
+        const float A = (float)th[3], B = (float)th[4];
+        const float* d = F.rois + (size_t)roi * RR;
+        const float* sv = F.scmos ? F.scmos + (size_t)roi * RR : nullptr;  // sCMOS var/gain^2 (Localization.java:1132)
+        for (int k = tid; k < RR; k += nts) {
+            const float v = T0[k], sgn = v < 0 ? -1.f : 1.f, psi = fabsf(v) * invS;
+            float j[5];
+            j[0] = A * (sgn * T0[RR + k] - psi * Dx) * invS;
+            j[1] = A * (sgn * T0[2 * RR + k] - psi * Dy) * invS;
+            j[2] = A * (sgn * T0[3 * RR + k] - psi * Dz) * invS;
+            j[3] = psi;
+            j[4] = 1.f;
+            const float mu = A * psi + B + (sv ? sv[k] : 0.f);
+            if (!(mu > 0.f)) { bad = true; continue; }
+            const float dk = d[k];
+            kahan_add(sg6[0], cg6[0], dk > 0.f ? mu - dk - dk * logf(mu / dk) : mu);
+            const float wgt = 1.f - dk / mu, wf = 1.f / mu, wh = dk * wf * wf;
+#pragma unroll
+            for (int q = 0; q < 5; ++q) kahan_add(sg6[1 + q], cg6[1 + q], wgt * j[q]);
+            int o = 0;
+#pragma unroll
+            for (int q = 0; q < 5; ++q)
+#pragma unroll
+                for (int r2 = 0; r2 <= q; ++r2) {
+                    sh[o] += wh * j[q] * j[r2];
+                    sh[o + 15] += wf * j[q] * j[r2];
+                    ++o;
+                }
+        }
+    }
+    // 36 sums per thread -> per warp: a butterfly reduce-scatter leaves sum k on lane k
+    // (k < 32); the last four reduce plainly
+    {
+        double v[32];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) v[k] = (double)sg6[k] - (double)cg6[k];
+#pragma unroll
+        for (int k = 0; k < 26; ++k) v[6 + k] = sh[k];
+        red[warp][lane] = warp_reduce_scatter32(v, lane);
+#pragma unroll
+        for (int k = 26; k < 30; ++k) {
+            const double x = warp_sum((double)sh[k]);
+            if (lane == 0) red[warp][6 + k] = x;
+        }
+    }
+    const bool wbad = __any_sync(0xffffffffu, bad);
+    if (lane == 0) badw[warp] = wbad;
+    epi_bar();
+    for (int i = t; i < UG * (NRED + 1); i += SPLIT_THREADS) {
+        const int gg = i / (NRED + 1), k = i - gg * (NRED + 1), sl = unit * UG + gg;
+        if (P.slot_roi[sl] < 0) continue;
+        if (k < NRED) {
+            double v = 0;
+            for (int w = gg * wps; w < (gg + 1) * wps; ++w) v += red[w][k];
+            P.sums[(size_t)sl * NSUM + k] = v;
+        } else {
+            int any = 0;
+            for (int w = gg * wps; w < (gg + 1) * wps; ++w) any |= badw[w];
+            P.sums[(size_t)sl * NSUM + NRED] = any ? 1.0 : 0.0;
+        }
+    }
+}
+
 // ------------------------------ stages 4 + 5 for small ROIs (persistent) -----
 // ROIs whose window is 32 or 64.  One CTA per SM walks the units: warp 16
 // loads a unit's row-blurred maps J (hi, lo; all UG slots at once) into one
@@ -1961,12 +2077,13 @@ __global__ void __launch_bounds__(S45_THREADS, 1) k_stage45p(SplitDev P, FitIO F
 // T^T[j'][(map, i')] = sum_j G[j'][j] J[(map, i')][j] (A = G padded to 128
 // rows, resident), into one of two TMEM accumulators.  The epilogue warps copy
 // the maps to shared memory (lane = pixel column j', warpgroup = map), then
-// one warp per slot forms the likelihood sums (slot_sums_warp) and one lane
-// per slot applies the FP64 LM step.
+// form the likelihood sums of the unit's slots (unit_sums); the LM step
+// follows in its own stage.
 constexpr int S45S_THREADS = SPLIT_THREADS + 32;
 
 __host__ __device__ inline size_t s45s_smem(int W, int RP, int R, int UG, int nb) {
-    return (size_t)2 * 128 * W * 2 + (size_t)nb * UG * a4_slot_bytes(W, RP) + (size_t)UG * 4 * R * R * 4;
+    return (size_t)2 * 128 * W * 2 + (size_t)nb * UG * a4_slot_bytes(W, RP) + (size_t)UG * 4 * R * R * 4 + 16 +
+           (size_t)(SPLIT_THREADS / 32) * ((NRED + 4) * 8 + 4);
 }
 // J buffers and TMEM accumulators: two when they fit (the next unit's load and
 // MMAs overlap this unit's epilogue), else one.
@@ -1984,6 +2101,9 @@ __device__ __forceinline__ void stage45s_body(const SplitDev& P, const FitIO& F,
     const int NB = s45s_nbuf(W, RP, R, UG);
     char* JB = G + 2 * garr;                             // NB buffers of a unit's J
     float* Tm = (float*)(JB + (size_t)NB * UG * jslot);  // the unit's maps: slot g, map m at (4 g + m) R^2
+    double (*red)[NRED] = (double (*)[NRED])(((uintptr_t)(Tm + (size_t)UG * 4 * RR) + 15) & ~(uintptr_t)15);
+    double (*nrm)[4] = (double (*)[4])(red + SPLIT_THREADS / 32);  // per-warp sums: likelihood terms, normalisation
+    int* badw = (int*)(nrm + SPLIT_THREADS / 32);
     __shared__ __align__(8) uint64_t gfull, full[2], acc[2], tfree[2], fin;
     __shared__ uint32_t tmem_base;
     const int nc = UG * NT;  // TMEM columns of one unit
@@ -2070,14 +2190,10 @@ __device__ __forceinline__ void stage45s_body(const SplitDev& P, const FitIO& F,
         umma::fence_before_sync();
         warp_arrive(&tfree[b]);
         epi_bar();
-        if (warp < UG && P.slot_roi[unit * UG + warp] >= 0) slot_sums_warp(P, F, unit * UG + warp, Tm + (size_t)warp * 4 * RR);
+        unit_sums(P, F, unit, Tm, red, nrm, badw);
         // (a bounded wait that gave up makes every epilogue thread leave the loop together)
         abort = epi_bar_or(t == 0 && *(volatile int*)P.err != 0);
-        if (abort) break;
-        // the unit's LM steps, one lane per slot, then its next state
-        if (warp == 0 && lane < UG) lm_slot(P, F, unit * UG + lane);
-        epi_bar();
-        if (t == 0) units.release(P, unit, unit_after_lm(P, F, unit, tag));
+        if (!abort && t == 0) units.release(P, unit, tag + 1);
     }
     if (t == 0) umma::mbar_wait(&fin, 0, P.err);  // every MMA of this CTA has completed
     epi_bar();
@@ -2472,9 +2588,9 @@ __global__ void k_set_int(int* p, int v) { *p = v; }
 
 // ------------------------------------------------------- dataflow kernel ----
 // The whole fit in one cooperative launch: CTAs [first[s], first[s + 1]) run
-// stage s (pupil DFT, window DFT, row blur, column blur + sums + LM) on the
+// stage s (pupil DFT, window DFT, row blur, column blur + sums, LM step) on the
 // units u with u = (CTA index within the stage) mod (CTAs of the stage).  A unit
-// cycles through the four stages once per evaluation; its operands pass from
+// cycles through the five stages once per evaluation; its operands pass from
 // one stage to the next through global memory while they are still in L2 (the
 // pool is small enough), and no stage waits for a round of the whole pool.
 // Converged fits retire and their slots refill from the ROI queue in the LM
@@ -2482,21 +2598,26 @@ __global__ void k_set_int(int* p, int v) { *p = v; }
 constexpr int FLOW_THREADS = SPLIT_THREADS + 32;
 
 struct FlowRoles {
-    int first[5];
+    int first[FLOW_STAGES + 1];
 };
 
 template <int W>
 __global__ void __launch_bounds__(FLOW_THREADS, 1) k_flow(SplitDev P, FitIO F, FlowRoles roles) {
     __shared__ UnitRing ring;
     int s = 0;
-    while (s < 3 && (int)blockIdx.x >= roles.first[s + 1]) ++s;
+    while (s < FLOW_STAGES - 1 && (int)blockIdx.x >= roles.first[s + 1]) ++s;
     FlowUnits units{&ring, s, (int)blockIdx.x - roles.first[s], roles.first[s + 1] - roles.first[s], 0};
+    if (s == FLOW_STAGES - 1) {
+        lm_role(P, F, units.first, units.stride);
+        return;
+    }
     if (threadIdx.x == 0) {  // (each stage body publishes these with its own barrier set-up)
         const int readers = s == 3 && W >= S45_MIN_W ? E45_THREADS / 32 + 2 : SPLIT_THREADS / 32 + 1;
         for (int b = 0; b < URING; ++b) {
             umma::mbar_init(&ring.full[b], 1);
             umma::mbar_init(&ring.freed[b], readers);
         }
+        ring.released = 0;
     }
     if (s == 0) {
         stage1_body<W>(P, F, units);
@@ -2684,7 +2805,7 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
     const size_t b_lm = al((size_t)P * sizeof(LMState));
     const size_t b_sums = al((size_t)P * NSUM * 8);
     const size_t b_int = al((size_t)P * 8 + (size_t)sp.U * 4 + 64);
-    const size_t b_clk = al(((size_t)2 * ctx->num_sms + 1) * 8);
+    const size_t b_clk = al(((size_t)3 * ctx->num_sms + 1) * 8);
     if (ensure_scratch(ctx, b_a2 + b_a3 + b_a4 + b_t + b_lm + b_sums + b_clk + b_int, ctx->err)) return ZOLA_E_CUDA;
     char* base = (char*)ctx->scratch;
     SplitDev& D = sp.D;
@@ -2783,35 +2904,35 @@ int launch_model_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const double
 // between the stages in proportion to each stage's share of a unit's device
 // time for this window size (measured on B200 with the round-based kernels).
 static FlowShape default_shape(int W, int grid) {
-    static const double share[3][4] = {{0.40, 0.25, 0.17, 0.18},   // W = 32
-                                       {0.38, 0.27, 0.17, 0.18},   // W = 64
-                                       {0.21, 0.30, 0.21, 0.28}};  // W = 128
+    static const double share[3][FLOW_STAGES] = {{0.33, 0.20, 0.17, 0.25, 0.05},   // W = 32
+                                                 {0.38, 0.23, 0.16, 0.19, 0.04},   // W = 64
+                                                 {0.22, 0.31, 0.18, 0.26, 0.03}};  // W = 128
     const int wi = W == 32 ? 0 : W == 64 ? 1 : 2;
     FlowShape f;
     f.units = 2 * grid;
-    double w[4];
-    for (int s = 0; s < 4; ++s) w[s] = share[wi][s];
-    // CTAs in proportion to w, at least one each, adding up to grid
+    // CTAs in proportion to the shares, at least one each, adding up to grid
     int sum = 0;
-    for (int s = 0; s < 4; ++s) sum += f.ctas[s] = std::max(1, (int)std::lround(w[s] * grid));
-    for (int s = 0; sum != grid; s = (s + 1) % 4) {
+    for (int s = 0; s < FLOW_STAGES; ++s) sum += f.ctas[s] = std::max(1, (int)std::lround(share[wi][s] * grid));
+    for (int s = 0; sum != grid; s = (s + 1) % FLOW_STAGES) {
         if (sum > grid && f.ctas[s] > 1) { --f.ctas[s]; --sum; }
         else if (sum < grid) { ++f.ctas[s]; ++sum; }
     }
     return f;
 }
 
-// CTAs in proportion to the busy time each stage had in a measured launch.
+// CTAs in proportion to the busy time (time with a unit in flight) each stage
+// had in a measured launch, moved half way from the current split.
 static void rebalance(FlowShape& f, const unsigned long long* clk, int grid) {
-    double work[4] = {0, 0, 0, 0}, tot = 0;
+    double work[FLOW_STAGES] = {}, tot = 0;
     int b = 0;
-    for (int s = 0; s < 4; ++s)
-        for (int k = 0; k < f.ctas[s]; ++k, ++b) work[s] += (double)(clk[2 * b + 1] - std::min(clk[2 * b], clk[2 * b + 1]));
-    for (int s = 0; s < 4; ++s) tot += work[s];
+    for (int s = 0; s < FLOW_STAGES; ++s)
+        for (int k = 0; k < f.ctas[s]; ++k, ++b) work[s] += (double)(clk[3 * b + 1] - std::min(clk[3 * b], clk[3 * b + 1]));
+    for (int s = 0; s < FLOW_STAGES; ++s) tot += work[s];
     if (!(tot > 0)) return;
     int sum = 0;
-    for (int s = 0; s < 4; ++s) sum += f.ctas[s] = std::max(1, (int)std::lround(work[s] / tot * grid));
-    for (int s = 0; sum != grid; s = (s + 1) % 4) {
+    for (int s = 0; s < FLOW_STAGES; ++s)
+        sum += f.ctas[s] = std::max(1, (int)std::lround(0.5 * f.ctas[s] + 0.5 * work[s] / tot * grid));
+    for (int s = 0; sum != grid; s = (s + 1) % FLOW_STAGES) {
         if (sum > grid && f.ctas[s] > 1) { --f.ctas[s]; --sum; }
         else if (sum < grid) { ++f.ctas[s]; ++sum; }
     }
@@ -2832,9 +2953,9 @@ static void tune_save(zola_ctx* ctx) {
     for (const auto& kv : ctx->tunes) {
         if (!kv.second.done) continue;
         const FlowShape& b = kv.second.best;
-        std::fprintf(f, "%s\n  \"%s\": {\"units\": %d, \"ctas\": [%d, %d, %d, %d], \"ns_per_eval\": %.3f}",
+        std::fprintf(f, "%s\n  \"%s\": {\"units\": %d, \"ctas\": [%d, %d, %d, %d, %d], \"ns_per_eval\": %.3f}",
                      first ? "" : ",", kv.first.c_str(), b.units, b.ctas[0], b.ctas[1], b.ctas[2], b.ctas[3],
-                     kv.second.best_ns);
+                     b.ctas[4], kv.second.best_ns);
         first = false;
     }
     std::fprintf(f, "\n}\n");
@@ -2858,11 +2979,11 @@ void tune_load(zola_ctx* ctx) {
         pos = end + 1;
         if (key.empty() || key[0] != 'N') continue;
         FlowTune t;
-        if (std::sscanf(txt.c_str() + pos, " : {\"units\": %d, \"ctas\": [%d, %d, %d, %d], \"ns_per_eval\": %lf",
+        if (std::sscanf(txt.c_str() + pos, " : {\"units\": %d, \"ctas\": [%d, %d, %d, %d, %d], \"ns_per_eval\": %lf",
                         &t.best.units, &t.best.ctas[0], &t.best.ctas[1], &t.best.ctas[2], &t.best.ctas[3],
-                        &t.best_ns) == 6) {
+                        &t.best.ctas[4], &t.best_ns) == 7) {
             int sum = 0;
-            for (int s = 0; s < 4; ++s) sum += t.best.ctas[s] > 0 ? t.best.ctas[s] : -100000;
+            for (int s = 0; s < FLOW_STAGES; ++s) sum += t.best.ctas[s] > 0 ? t.best.ctas[s] : -100000;
             if (sum == ctx->num_sms && t.best.units > 0) {
                 t.done = true;
                 ctx->tunes[key] = t;
@@ -2879,7 +3000,7 @@ static FlowShape pick_shape(zola_ctx* ctx, const std::string& key, int W, int n,
     *trial = false;
     FlowShape f = default_shape(W, grid);
     if (ctx->flow_ctas[0] > 0)
-        for (int s = 0; s < 4; ++s) f.ctas[s] = ctx->flow_ctas[s];
+        for (int s = 0; s < FLOW_STAGES; ++s) f.ctas[s] = ctx->flow_ctas[s];
     if (ctx->flow_units > 0) f.units = ctx->flow_units;
     if (ctx->flow_units > 0 || ctx->flow_ctas[0] > 0) return f;
     auto it = ctx->tunes.find(key);
@@ -2891,9 +3012,9 @@ static FlowShape pick_shape(zola_ctx* ctx, const std::string& key, int W, int n,
     return t.trials == 0 ? f : t.next;
 }
 
-// After a measured launch: record it and choose the next trial.  Trials 0-2
+// After a measured launch: record it and choose the next trial.  Trials 0-4
 // rebalance the CTAs per stage from the measured busy times at two units per
-// SM; trials 3 and 4 try three and one and a half units per SM with the best
+// SM; trials 5 and 6 try three and one and a half units per SM with the best
 // split; then the best shape is kept (and written to the cache file).
 static void tune_record(zola_ctx* ctx, const std::string& key, const FlowShape& used, double ns_per_eval,
                         const unsigned long long* clk) {
@@ -2905,12 +3026,12 @@ static void tune_record(zola_ctx* ctx, const std::string& key, const FlowShape& 
     ++t.trials;
     const int grid = ctx->num_sms;
     t.next = used;
-    if (t.trials < 3) {
+    if (t.trials < 5) {
         rebalance(t.next, clk, grid);
-    } else if (t.trials == 3) {
+    } else if (t.trials == 5) {
         t.next = t.best;
         t.next.units = 3 * grid;
-    } else if (t.trials == 4) {
+    } else if (t.trials == 6) {
         t.next = t.best;
         t.next.units = 3 * grid / 2;
     } else {
@@ -2957,7 +3078,7 @@ static int launch_fit_flow(zola_ctx* ctx, zola_psf* p, WindowTables* w, const Fi
     }
     FlowRoles roles;
     roles.first[0] = 0;
-    for (int s = 0; s < 4; ++s) roles.first[s + 1] = roles.first[s] + shape.ctas[s];
+    for (int s = 0; s < FLOW_STAGES; ++s) roles.first[s + 1] = roles.first[s] + shape.ctas[s];
     SplitDev dv = D;
     FitIO io = F;
     void* args[] = {&dv, &io, &roles};
@@ -2983,13 +3104,33 @@ static int launch_fit_flow(zola_ctx* ctx, zola_psf* p, WindowTables* w, const Fi
         ctx->err = "split fit: no unit became ready within the wait limit (inputs did not arrive)";
         return ZOLA_E_TIMEOUT;
     }
+    if (err == 3) {
+        ctx->err = "split fit: more model evaluations than the ROIs allow (internal error)";
+        return ZOLA_E_CUDA;
+    }
     if (err) {
         ctx->err = "split fit: a bounded device wait timed out";
         return ZOLA_E_TIMEOUT;
     }
+    // per stage: busy fraction and device clocks per unit (bookkeeping of the last launch)
+    if (!ctx->h_tune) ZOLA_CUDA_CHECK(cudaMallocHost(&ctx->h_tune, (3 * (size_t)grid + 1) * 8), ctx);
+    ZOLA_CUDA_CHECK(cudaMemcpy(ctx->h_tune, D.evals, (3 * (size_t)grid + 1) * 8, cudaMemcpyDeviceToHost), ctx);
+    {
+        const unsigned long long* clk = ctx->h_tune + 1;
+        int b = 0;
+        for (int s = 0; s < FLOW_STAGES; ++s) {
+            double idle = 0, tot = 0, units = 0;
+            for (int k = 0; k < shape.ctas[s]; ++k, ++b) {
+                idle += (double)clk[3 * b];
+                tot += (double)clk[3 * b + 1];
+                units += (double)clk[3 * b + 2];
+            }
+            ctx->flow_busy[s] = tot > 0 ? 1.0 - idle / tot : 0.0;
+            ctx->flow_clk_per_unit[s] = units > 0 ? (tot - idle) / units : 0.0;
+        }
+        ctx->flow_evals = (double)ctx->h_tune[0];
+    }
     if (trial) {
-        if (!ctx->h_tune) ZOLA_CUDA_CHECK(cudaMallocHost(&ctx->h_tune, (2 * (size_t)grid + 1) * 8), ctx);
-        ZOLA_CUDA_CHECK(cudaMemcpy(ctx->h_tune, D.evals, (2 * (size_t)grid + 1) * 8, cudaMemcpyDeviceToHost), ctx);
         float ms = 0;
         ZOLA_CUDA_CHECK(cudaEventElapsedTime(&ms, ctx->tune_ev[0], ctx->tune_ev[1]), ctx);
         if (ctx->h_tune[0] > 0) tune_record(ctx, key, shape, ms * 1e6 / (double)ctx->h_tune[0], ctx->h_tune + 1);
@@ -3010,7 +3151,9 @@ int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d
                      const double* d_init, int n,
                      const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll, int* d_status,
                      int* d_iters, cudaStream_t st, const RoiFeed* feed, const int* d_avail) {
-    FitParamsDev fp{prm->zmin, prm->zmax, prm->xymax, prm->tol_xyz, prm->step_xy, prm->step_z, prm->max_iter};
+    // the likelihood is summed in FP32 and the model is good to about 2^-22:
+    // likelihood changes below 1e-3 are not resolved (lm_update)
+    FitParamsDev fp{prm->zmin, prm->zmax, prm->xymax, prm->tol_xyz, prm->step_xy, prm->step_z, prm->max_iter, 1e-3};
     const FitIO F{d_rois, d_scmos, d_init, n, fp, d_out5, d_crlb5, d_nll, d_status, d_iters};
     if (ctx->split_mode == ZOLA_SPLIT_FLOW || d_avail) return launch_fit_flow(ctx, p, w, F, st, feed, d_avail);
     SplitPool sp;
@@ -3048,11 +3191,11 @@ int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d
     const int max_rounds = (prm->max_iter + 2) * ((n + P - 1) / P + 1) + 8 + 4 * (feed ? feed->n_chunks : 0);
     int rounds = 0;
     const bool fused = ctx->split_mode == ZOLA_SPLIT_FUSED && fused_fits(*sp.pl);
-    // Window 128: column blur and likelihood sums in one persistent kernel (the
-    // maps never leave the SM).  Smaller windows: one warp per slot forms the
-    // sums from the unit's maps in shared memory.  The two sum in different
-    // orders; the choice depends on R alone so that a fit never depends on the
-    // batch it is in.
+    // Window 128: column blur and likelihood sums in one persistent kernel, one
+    // slot at a time over all its threads (the maps never leave the SM).  Smaller
+    // windows: the unit's maps go to shared memory and its slots are summed
+    // together.  The two sum in different orders; the choice depends on R alone
+    // so that a fit never depends on the batch it is in.
     const bool big = sp.pl->W >= S45_MIN_W;
     while (true) {
         for (int k = 0; k < 4; ++k) {
@@ -3078,7 +3221,10 @@ int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d
             else
                 k_stage45s<<<unit_grid(ctx, sp), S45S_THREADS, sp.s45, st>>>(D, F);
             prof_end(ctx, st);
-            ctx->launches += 1;
+            prof_begin(ctx, 7, st);
+            k_lm<<<(P + 127) / 128, 128, 0, st>>>(D, F);
+            prof_end(ctx, st);
+            ctx->launches += 2;
         }
         rounds += 4;
         ZOLA_CUDA_CHECK(cudaGetLastError(), ctx);

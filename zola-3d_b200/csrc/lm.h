@@ -27,6 +27,7 @@ struct LMState {
     double lambda;
     double trial[5];   // proposed point
     double step;       // max |trial - th| over x, y, z
+    double pred;       // decrease of the likelihood the quadratic model predicts for the trial step
     int evals;
     int status;        // 2 running, 1 converged, 3 stalled, -1 NaN / non-positive model
 };
@@ -117,17 +118,30 @@ __host__ __device__ inline bool lm_propose(LMState& s, const FitParamsDev& P) {
         for (int q = 0; q < 5; ++q) s.trial[q] = s.th[q] + scale * d[q];
         lm_clamp(s.trial, P);
         s.step = fmax(fabs(s.trial[0] - s.th[0]), fmax(fabs(s.trial[1] - s.th[1]), fabs(s.trial[2] - s.th[2])));
+        double dl[5], hd = 0, gd = 0;
+        for (int q = 0; q < 5; ++q) dl[q] = s.trial[q] - s.th[q];
+        for (int q = 0; q < 5; ++q) {
+            gd += s.g[q] * dl[q];
+            for (int r = 0; r < 5; ++r) hd += dl[q] * s.H[q * 5 + r] * dl[r];
+        }
+        s.pred = -(gd + 0.5 * hd);
         return true;
     }
     if (s.status == 2) s.status = 2;  // max evaluations reached: stays "max iter"
     return false;
 }
 
-// Accept or reject the evaluated trial point.
+// Accept or reject the evaluated trial point.  Near the optimum of a flat
+// likelihood (a faint or defocused emitter) the decrease of the last steps is
+// below the rounding of a likelihood summed in FP32.  So when the quadratic
+// model predicts a decrease of at most P.accept_nll, the step is accepted
+// unless the likelihood rose by more than that; the next Gauss-Newton step
+// from the accepted point decides convergence.  (P.accept_nll = 0: a step is
+// accepted only when the likelihood did not rise.)
 __host__ __device__ inline void lm_update(LMState& s, double nll, const double* g, const double* H, const double* F,
                                           const FitParamsDev& P) {
     s.evals += 1;
-    if (nll <= s.nll) {
+    if (nll <= s.nll || (s.pred <= P.accept_nll && nll <= s.nll + P.accept_nll)) {
         for (int q = 0; q < 5; ++q) { s.th[q] = s.trial[q]; s.g[q] = g[q]; }
         for (int q = 0; q < 25; ++q) { s.H[q] = H[q]; s.F[q] = F[q]; }
         s.nll = nll;

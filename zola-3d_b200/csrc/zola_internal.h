@@ -42,6 +42,10 @@ struct WinView {
 struct FitParamsDev {
     double zmin, zmax, xymax, tol_xyz, step_xy, step_z;
     int max_iter;
+    // Likelihood resolution of the fit: a step whose predicted decrease is at
+    // most this is accepted unless the likelihood rose by more than this (0:
+    // a step is accepted only when the likelihood did not rise).
+    double accept_nll = 0.0;
 };
 
 // Host-side tables of one window size (FP64 and the split-precision packs).
@@ -60,10 +64,11 @@ struct WindowTables {
 
 namespace zola {
 // Shape of the dataflow split-fit kernel: units of slots in flight and CTAs per
-// stage (pupil DFT, window DFT, row blur, column blur + sums + LM).
+// stage (pupil DFT, window DFT, row blur, column blur + sums, LM step).
+constexpr int FLOW_STAGES = 5;
 struct FlowShape {
     int units = 0;
-    int ctas[4] = {0, 0, 0, 0};
+    int ctas[FLOW_STAGES] = {0, 0, 0, 0, 0};
 };
 // Autotuning state of one (pupil grid, disk rows, ROI side, window) class: the
 // trials made so far and the best shape measured, in device ns per model
@@ -95,9 +100,9 @@ struct zola_ctx {
     int* d_status_word = nullptr;
     int* h_flags = nullptr;      // pinned host words read back by the split fit loop
     int split_pool_max = 0;      // 0: size the split slot pool automatically
-    int split_mode = ZOLA_SPLIT_FLOW;  // ZOLA_SPLIT_STAGED, _FUSED or _FLOW
+    int split_mode = ZOLA_SPLIT_STAGED;  // ZOLA_SPLIT_STAGED, _FUSED or _FLOW
     int flow_units = 0;          // dataflow kernel: units of slots in flight (0: automatic)
-    int flow_ctas[4] = {};       // dataflow kernel: CTAs per stage (all 0: automatic)
+    int flow_ctas[5] = {};       // dataflow kernel: CTAs per stage (all 0: automatic)
     long long wait_limit = 0;    // clocks a device wait may take before the call fails (0: about a second)
     cudaStream_t feed_stream = nullptr;  // copies of the arrived-ROI count of a host-buffer fit
     cudaEvent_t ev_init = nullptr;
@@ -107,7 +112,10 @@ struct zola_ctx {
     std::string tune_path;
     std::map<std::string, zola::FlowTune> tunes;
     cudaEvent_t tune_ev[2] = {nullptr, nullptr};
-    unsigned long long* h_tune = nullptr;  // pinned: evaluations, then (idle, total) clocks per CTA
+    unsigned long long* h_tune = nullptr;  // pinned: evaluations, then (idle, total clocks, units) per CTA
+    double flow_busy[5] = {};              // last dataflow launch: busy fraction per stage
+    double flow_clk_per_unit[5] = {};      // last dataflow launch: busy clocks per unit per stage (one CTA)
+    double flow_evals = 0;                 // last dataflow launch: model evaluations
     // optional per-kernel timing with CUDA events on the launch stream
     int profile = 0;
     std::vector<cudaEvent_t> ev_pool;
