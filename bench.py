@@ -181,12 +181,79 @@ def detect_fit_config(z, ctx, nframes, seed=1, precision=None):
                         "split-precision fits, host frames in and localization rows out"}
 
 
-def run_step(z, job, precision, stream_ptr, sl=None):
+def calibration_config(z, ctx, seed=3, fit_iters=10):
+    """Calibration benchmark: 5 beads x 61 slices (50 nm, +-1.5 um) x 32^2 px, PSF
+    from 45 Zernike coefficients ~ N(0, 0.05 lambda) + 0.1 lambda astigmatism,
+    n_sample 1.33 at depth 0, 20,000 photons, background 50, Poisson noise.
+    Times the stack NLL (forward), NLL + adjoint gradient (backward) and LM
+    iterations of the Zernike fit on the GPU, and the oracle's restatement of
+    the reference stack NLL (ZernikePhaseRetrieval.java:1843-1874) on the CPU;
+    the reference's coordinate-wise finite-difference update takes about 8
+    stack NLLs per coefficient per iteration."""
+    import oracle as O
+    rng = np.random.default_rng(seed)
+    nz, nb, ns, R = 45, 5, 61, 32
+    zern = rng.normal(0, 0.05, nz) * TWO_PI
+    zern[:3] = 0
+    zern[5] += 0.1 * TWO_PI
+    dz = (np.arange(ns) - ns // 2) * 0.05
+    xyz = np.c_[rng.uniform(-0.05, 0.05, (nb, 2)), rng.uniform(-0.05, 0.05, nb)]
+    photons = np.full((nb, ns), 20000.0)
+    ref = O.OraclePSF(128, DX, 1.4, 0.66, 1.518, 1.33, 1.0, zern, gauss_f32=False)
+    stacks = np.zeros((nb, ns, R, R))
+    for b in range(nb):
+        for k in range(ns):
+            stacks[b, k] = rng.poisson(photons[b, k] * ref.model_oil(R, xyz[b, 0], xyz[b, 1], dz[k] + xyz[b, 2], 0.0)
+                                       + 50.0)
+    bead = np.zeros((nb, 3 + ns + 6))
+    bead[:, 3 + ns] = 50.0
+    psf = z.PSF(ctx, z.optics(size_fft=128, xystep=DX, na=1.4, wavelength=0.66, n_oil=1.518, n_wat=1.33, sigma=0.9),
+                np.zeros(nz))
+    cal = z.Calibration(psf, stacks, dz, photons=photons)
+    z0 = np.zeros(nz)
+    cal.forward(z0, 0.9, bead)
+    cal.backward(z0, 0.9, bead)
+    reps = 20
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        cal.forward(z0, 0.9, bead)
+    t_fwd = (time.perf_counter() - t0) / reps
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        cal.backward(z0, 0.9, bead)
+    t_bwd = (time.perf_counter() - t0) / reps
+    t0 = time.perf_counter()
+    _, _, _, nll, it = cal.fit(z0, 0.9, bead, max_iter=fit_iters)
+    t_fit = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    oref = O.OraclePSF(128, DX, 1.4, 0.66, 1.518, 1.33, 0.9, z0, gauss_f32=False)
+    for b in range(nb):
+        oref.calib_nll_full(R, dz, stacks[b], photons[b], 0.9, bead[b, :3], bead[b, 3:3 + ns], bead[b, 3 + ns:])
+    t_cpu = time.perf_counter() - t0
+    psf.close()
+    return {"workload": "5 beads x 61 slices x 32^2 px, 45 Zernike coefficients, n_sample 1.33, pupil 128^2",
+            "forward_nll_per_s": 1.0 / t_fwd, "adjoint_gradient_per_s": 1.0 / t_bwd,
+            "lm_iterations": int(it), "lm_iterations_per_s": it / t_fit, "final_nll": float(nll),
+            "cpu_oracle_stack_nll_s": t_cpu, "cpu_cores": 1,
+            "reference_fd_iteration_s_estimate": t_cpu * 8 * (nz - 3),
+            "note": "host C-ABI calls (stacks resident on the device); the reference's finite-difference "
+                    "coordinate update needs about 8 stack NLLs per coefficient per iteration (estimate from the "
+                    "oracle's single-thread NLL time)"}
+
+
+def run_step(z, ctx, job, precision, stream_ptr, mixed=True):
+    """One step: the whole mixed job, in one zola_fit_batch_mixed_dev call (split precision), or one
+    call per class."""
+    if mixed and precision == z.ZOLA_PREC_SPLIT:
+        z.fit_mixed_dev(ctx, [dict(psf=j["psf"], rois=j["rois"], init=j["init"],
+                                   prm=z.PSF.fit_params(precision=precision, **j["prm_kw"]), out=j["out"],
+                                   crlb=j["crlb"], nll=j["nll"], status=j["status"], iters=j["iters"]) for j in job],
+                        stream=stream_ptr)
+        return
     for j in job:
         p = z.PSF.fit_params(precision=precision, **j["prm_kw"])
-        s = sl if sl is not None else slice(None)
-        j["psf"].fit_dev(j["rois"][s], j["init"][s], p, j["out"][s], j["crlb"][s], j["nll"][s], j["status"][s],
-                         j["iters"][s], stream=stream_ptr)
+        j["psf"].fit_dev(j["rois"], j["init"], p, j["out"], j["crlb"], j["nll"], j["status"], j["iters"],
+                         stream=stream_ptr)
 
 
 # --------------------------------------------------------------- clocks ----
@@ -346,6 +413,8 @@ def main():
     ap.add_argument("--split-mode", default="staged", choices=["staged", "flow", "fused"],
                     help="split fit kernels: one dataflow kernel, four stage kernels per round, or stage 1 + fused 2-5")
     ap.add_argument("--no-tune", action="store_true", help="skip the dataflow-kernel autotuning pass")
+    ap.add_argument("--no-calibration", dest="calibration", action="store_false",
+                    help="skip the Zernike calibration measurement")
     ap.add_argument("--stage-breakdown", action="store_true",
                     help="also time the round-based stage kernels per stage (explains the dataflow kernel)")
     args = ap.parse_args()
@@ -404,7 +473,7 @@ def main():
 
     # warm-up (split path), also primes tables and the slot pool
     for _ in range(args.warmup):
-        run_step(z, job, z.ZOLA_PREC_SPLIT, ctx.stream)
+        run_step(z, ctx, job, z.ZOLA_PREC_SPLIT, ctx.stream, mixed=args.split_mode == "staged")
     ext.synchronize()
 
     # timed steps (device time on the library stream; max over ranks)
@@ -416,7 +485,7 @@ def main():
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(ext)
     for _ in range(args.steps):
-        run_step(z, job, z.ZOLA_PREC_SPLIT, ctx.stream)
+        run_step(z, ctx, job, z.ZOLA_PREC_SPLIT, ctx.stream, mixed=args.split_mode == "staged")
     ev1.record(ext)
     ev1.synchronize()
     torch.cuda.synchronize()
@@ -528,35 +597,51 @@ def main():
     peak_tf = peaks.get("bf16_tflops_sustained", 1400.0)
     peak_gbs = peaks.get("hbm_gbs", 6650.0)
     peak_src = "of measured" if "bf16_tflops_sustained" in peaks and "hbm_gbs" in peaks else "of fallback"
-    kernel_key = "split_dataflow" if args.split_mode == "flow" else None
+    # SURVEY 8(d) flops of each kernel per model evaluation: stage 1 the pupil DFT
+    # (3*8*W*D^2), stage 2 the window DFT (4*8*W^2*D), the dataflow kernel both
+    def stage_flops(R, N):
+        W, D = window(R, N), disk_rows(N)
+        return {"split_stage1_pupil_dft": 3 * 8 * W * D * D, "split_stage2_window_dft": 4 * 8 * W * W * D,
+                "split_dataflow": flops_per_eval(R, N)}
     by_class = {}
     tot_flops = tot_s = 0.0
+    best = None
     for j in job:
         name, R, N = j["cls"]["name"], j["cls"]["R"], j["cls"]["N"]
-        km = kern_ms[name]
-        ms_k = km[kernel_key][0] if kernel_key in km else sum(v[0] for v in km.values())
+        km, sf = kern_ms[name], stage_flops(R, N)
+        ms_all = sum(v[0] for v in km.values())
+        ent = {"kernels": {}}
+        for k, (ms_k, n_k) in km.items():
+            e = {"ms": round(ms_k, 3), "launches": n_k}
+            if k in sf and ms_k > 0:
+                tf = iters[name] * sf[k] / (ms_k / 1000.0) / 1e12
+                e.update(tflops=round(tf, 2), tensor_frac=round(tf / peak_tf, 4))
+                if best is None or ms_k > best[2]:
+                    best = (name, k, ms_k)
+            ent["kernels"][k] = e
         fl = iters[name] * flops_per_eval(R, N)
-        tf = fl / (ms_k / 1000.0) / 1e12
-        by_class[name] = {"kernel_ms": round(ms_k, 3), "evaluations": iters[name], "flops_per_eval": flops_per_eval(R, N),
-                          "tflops": round(tf, 2), "tensor_frac": round(tf / peak_tf, 4),
-                          "input_gbs": round(iters[name] * 4 * R * R / (ms_k / 1000.0) / 1e9, 1)}
+        ent.update(evaluations=iters[name], fit_ms=round(ms_all, 3),
+                   fit_tflops=round(fl / (ms_all / 1000.0) / 1e12, 2),
+                   fit_tensor_frac=round(fl / (ms_all / 1000.0) / 1e12 / peak_tf, 4))
+        by_class[name] = ent
         tot_flops += fl
-        tot_s += ms_k / 1000.0
-    dom = max(by_class, key=lambda k: by_class[k]["kernel_ms"])
-    ent = by_class[dom]
-    traffic = NCU_TRAFFIC.get((dom, kernel_key))
+        tot_s += ms_all / 1000.0
+    dom_cls, dom_k, _ = best
+    ent = by_class[dom_cls]["kernels"][dom_k]
+    traffic = NCU_TRAFFIC.get((dom_cls, dom_k))
     roofline = {"bound": "tensor", "achieved": ent["tflops"], "peak": peak_tf, "unit": "TFLOP/s",
-                "frac": ent["tensor_frac"], "kernel": "k_flow (dataflow split fit)" if kernel_key else args.split_mode,
-                "class": dom, "peak_source": peak_src + " (sustained bf16)",
-                "traffic": None if traffic is None else int(traffic * iters[dom]),
-                "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum per launch from one ncu capture of this "
-                                "kernel on a smaller batch of this class, scaled by model evaluations",
+                "frac": ent["tensor_frac"], "kernel": dom_k, "class": dom_cls,
+                "peak_source": peak_src + " (sustained bf16)",
+                "traffic": None if traffic is None else int(traffic * iters[dom_cls] / max(1, ent["launches"])),
+                "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum per launch: ncu bytes per model "
+                                "evaluation of this kernel on this class (profiles/), times the evaluations per launch",
                 "whole_job_tflops": round(tot_flops / tot_s / 1e12, 2),
                 "whole_job_tensor_frac": round(tot_flops / tot_s / 1e12 / peak_tf, 4),
                 "per_class": by_class, "hbm_peak_gbs": peak_gbs,
-                "note": "achieved = SURVEY 8(d) algorithmic flops of the model evaluations made (3*8*W*D^2 + 4*8*W^2*D "
-                        "per evaluation, complex MAC = 8 flops; evaluations logged per ROI) / CUDA-event duration of the "
-                        "kernel launch; peak = sustained measured bf16 (FP16 runs at the same rate)"}
+                "note": "achieved = SURVEY 8(d) algorithmic flops of the model evaluations made (pupil DFT 3*8*W*D^2, "
+                        "window DFT 4*8*W^2*D per evaluation, complex MAC = 8 flops; evaluations logged per ROI) / "
+                        "summed CUDA-event duration of that kernel's launches for that class; whole_job = all SURVEY "
+                        "8(d) flops / all fit kernels' time; peak = sustained measured bf16 (FP16 runs at the same rate)"}
 
     # end to end through the host C-ABI (pinned host buffers, H2D + D2H inside the call)
     e2e = None
@@ -590,6 +675,7 @@ def main():
            "d2h_bytes_per_step": int(d2h)}
 
     detect = detect_fit_config(z, ctx, args.detect_frames, seed=1 + rank) if args.detect_frames > 0 else None
+    calib = calibration_config(z, ctx) if args.calibration and rank == 0 else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -611,7 +697,7 @@ def main():
                 "speedup_vs_fp64_plain": value / world / fp64_value,
                 "accuracy_vs_oracle": acc_oracle, "accuracy_vs_fp64_gpu": acc64,
                 "stage_breakdown_round_based": breakdown,
-                "detect_fit_pipeline": detect}
+                "detect_fit_pipeline": detect, "calibration": calib}
         print(json.dumps(line), flush=True)
     for j in job:
         j["psf"].close()

@@ -151,6 +151,26 @@ ZOLA_API int zola_fit_batch_stream_dev(zola_ctx* ctx, zola_psf* psf, int R, cons
                                        double* d_out5, double* d_crlb5, double* d_nll, int* d_status, int* d_iters,
                                        void* stream);
 
+/* Mixed batch: several ROI classes (PSF and ROI side, e.g. 16 x 16 astigmatic,
+ * 24 x 24 saddle and 48 x 48 tetrapod ROIs) fitted in one call (replaces the
+ * reference's per-size Modelmany_double_ batches run side by side by its
+ * worker threads, process/gpu/Modelmany_double_.java:865-940).  Each class has
+ * its own slot pool and stream, and the classes' LM rounds are interleaved so
+ * that one class's draining tail overlaps the others' work; each ROI's fit is
+ * the same bit for bit as in a call of its class alone.  Device buffers as in
+ * zola_fit_batch_dev; every class must use split precision. */
+#define ZOLA_MAX_CLASSES 8
+typedef struct {
+    zola_psf* psf;
+    int R, n;
+    const float* d_rois;
+    const double* d_init5;
+    zola_fit_params prm;
+    double *d_out5, *d_crlb5, *d_nll;  /* d_crlb5, d_nll nullable */
+    int *d_status, *d_iters;           /* nullable */
+} zola_fit_class;
+ZOLA_API int zola_fit_batch_mixed_dev(zola_ctx* ctx, const zola_fit_class* classes, int nclass, void* stream);
+
 /* sCMOS form (process/cpu/Localization.java:1132, utils/SCMOScamera.java):
  * scmos holds, per ROI pixel, var/gain^2 of the camera pixel; it is added to
  * the model mean (mu = A psi + B + scmos), and rois are then

@@ -162,3 +162,73 @@ def test_calibration_fit_recovers_aberrations_and_sigma(zpkg, ctx):
     _, m_true = cal.forward(zern, 1.0, bead, model=True)
     # the fitted stack model stays within the Poisson noise of the true one at every pixel
     assert (np.abs(m_fit - m_true) / np.sqrt(m_true)).max() < 3.0
+
+
+def config4_data(seed=3):
+    """Bead z-stacks of the calibration benchmark: 5 beads x 61 slices (50 nm
+    steps over +-1.5 um) x 32 x 32 px, a PSF from 45 Zernike coefficients
+    ~ N(0, 0.05 lambda) plus 0.1 lambda astigmatism, sample index 1.33 with the
+    beads at depth 0, 20,000 photons per bead, background 50 / px, Poisson
+    noise."""
+    rng = np.random.default_rng(seed)
+    nz, nb, ns, R = 45, 5, 61, 32
+    zern = rng.normal(0, 0.05, nz) * TWO_PI
+    zern[:3] = 0
+    zern[5] += 0.1 * TWO_PI
+    dz = (np.arange(ns) - ns // 2) * 0.05
+    xyz = np.c_[rng.uniform(-0.05, 0.05, (nb, 2)), rng.uniform(-0.05, 0.05, nb)]
+    photons = np.full((nb, ns), 20000.0)
+    a = rng.normal(0, 200.0, (nb, ns))
+    c = np.zeros((nb, NP))
+    c[:, 0] = 50.0
+    ref = O.OraclePSF(128, 0.11, 1.4, 0.66, 1.518, 1.33, 1.0, zern, gauss_f32=False)
+    stacks = np.zeros((nb, ns, R, R))
+    for b in range(nb):
+        for s in range(ns):
+            mu = (photons[b, s] + a[b, s]) * ref.model_oil(R, xyz[b, 0], xyz[b, 1], dz[s] + xyz[b, 2], 0.0) + c[b, 0]
+            stacks[b, s] = rng.poisson(mu)
+    return zern, dz, np.c_[xyz, a, c], stacks, photons
+
+
+def test_calibration_benchmark_scale_nll_and_adjoint(zpkg, ctx):
+    """At the calibration benchmark's scale (45 coefficients, 5 beads x 61
+    slices x 32^2, n_sample 1.33): the forward NLL equals the oracle's
+    restatement of ZernikePhaseRetrieval's stack likelihood to 1e-9, and the
+    hand-written adjoint is within 1e-4 of central finite differences
+    (h = 1e-4 lambda for the phase) for every Zernike coefficient, the blur
+    width and each bead's x, y, z, photometry and background terms."""
+    zern, dz, bead, stacks, photons = config4_data()
+    ns, nb = len(dz), len(bead)
+    o = dict(OPTICS)
+    psf = zpkg.PSF(ctx, zpkg.optics(size_fft=128, n_wat=1.33, **o), np.zeros(45))
+    cal = zpkg.Calibration(psf, stacks, dz, photons=photons)
+    z0 = zern * 0.8
+    s0 = 0.95
+    b0 = bead.copy()
+    b0[:, :3] += [0.01, -0.01, 0.02]
+    b0[:, 3 + ns] += 2.0
+    ref = O.OraclePSF(128, 0.11, 1.4, 0.66, 1.518, 1.33, 0.9, z0, gauss_f32=False)
+    want = sum(ref.calib_nll_full(32, dz, stacks[b], photons[b], s0, b0[b, :3], b0[b, 3:3 + ns], b0[b, 3 + ns:])
+               for b in range(nb))
+    got = cal.forward(z0, s0, b0)
+    assert abs(got - want) <= 1e-9 * abs(want)
+    _, gz, gs, gb = cal.backward(z0, s0, b0)
+    h = 1e-4 * TWO_PI
+    for i in range(3, 45):
+        e = np.zeros(45)
+        e[i] = h
+        fd = (cal.forward(z0 + e, s0, b0) - cal.forward(z0 - e, s0, b0)) / (2 * h)
+        assert abs(gz[i] - fd) <= 1e-4 * max(abs(fd), 1e-2 * np.abs(gz[3:]).max()), (i, gz[i], fd)
+    fd = (cal.forward(z0, s0 + 1e-5, b0) - cal.forward(z0, s0 - 1e-5, b0)) / 2e-5
+    assert abs(gs - fd) <= 1e-4 * abs(fd), (gs, fd)
+    cols = [0, 1, 2, 3, 3 + ns // 2, 2 + ns] + list(range(3 + ns, 3 + ns + NP))
+    steps = {0: 1e-5, 1: 1e-5, 2: 1e-5}
+    for b in range(nb):
+        for q in cols:
+            hq = steps.get(q, 1e-2 if q < 3 + ns else 1e-4)
+            e = np.zeros_like(b0)
+            e[b, q] = hq
+            fd = (cal.forward(z0, s0, b0 + e) - cal.forward(z0, s0, b0 - e)) / (2 * hq)
+            scale = np.abs(gb[:, q]).max()
+            assert abs(gb[b, q] - fd) <= 1e-4 * max(abs(fd), 1e-3 * scale) + 1e-6, (b, q, gb[b, q], fd)
+    assert np.all(gz[:3] == 0)

@@ -285,3 +285,39 @@ def test_host_buffer_fit_streams_inputs_in_chunks(zpkg, ctx):
     assert np.array_equal(host["status"], out[3].cpu().numpy())
     assert (host["status"] == 1).mean() > 0.9
     psf.close()
+
+
+def test_mixed_batch_equals_per_class_calls(zpkg, ctx):
+    """Three ROI classes (16 x 16 astigmatic with a 64^2 pupil, 24 x 24 saddle and
+    48 x 48 tetrapod with 128^2 pupils) fitted in one zola_fit_batch_mixed_dev
+    call give, ROI by ROI and bit for bit, the fits of one call per class: each
+    class runs its own slot pool on its own stream, and a fit does not depend on
+    its batch.  A small pool makes the classes refill their slots many times."""
+    import torch
+    dev = torch.device("cuda", 0)
+    specs = [(64, 16, astig_zernike(), 1500), (128, 24, saddle_zernike(), 900), (128, 48, tetrapod_zernike(), 500)]
+    classes, want = [], []
+    ctx.set_pool(256)
+    try:
+        for N, R, zern, n in specs:
+            psf = make(zpkg, ctx, N, zern)
+            rois, init, _ = _large_roi_job(psf, zpkg, R, n, seed=700 + R)
+            prm = zpkg.PSF.fit_params(-1.5, 1.5, R * 0.11 / 2, max_iter=50, tol_xyz=1e-4,
+                                      precision=zpkg.ZOLA_PREC_SPLIT)
+            want.append(psf.fit(rois, init, prm))
+            classes.append(dict(psf=psf, rois=torch.tensor(rois, device=dev), init=torch.tensor(init, device=dev),
+                                prm=prm, out=torch.zeros((n, 5), dtype=torch.float64, device=dev),
+                                crlb=torch.zeros((n, 5), dtype=torch.float64, device=dev),
+                                status=torch.zeros(n, dtype=torch.int32, device=dev),
+                                iters=torch.zeros(n, dtype=torch.int32, device=dev)))
+        torch.cuda.synchronize()
+        zpkg.fit_mixed_dev(ctx, classes, stream=ctx.stream)
+        torch.cuda.synchronize()
+    finally:
+        ctx.set_pool(0)
+    for c, w in zip(classes, want):
+        assert np.array_equal(c["out"].cpu().numpy(), w["theta"])
+        assert np.array_equal(np.nan_to_num(c["crlb"].cpu().numpy()), np.nan_to_num(w["crlb"]))
+        assert np.array_equal(c["status"].cpu().numpy(), w["status"])
+        assert np.array_equal(c["iters"].cpu().numpy(), w["iters"])
+        c["psf"].close()

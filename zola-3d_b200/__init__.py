@@ -64,6 +64,13 @@ class FitParams(ctypes.Structure):
                 ("step_z", ctypes.c_double), ("precision", ctypes.c_int)]
 
 
+class FitClass(ctypes.Structure):
+    _fields_ = [("psf", ctypes.c_void_p), ("R", ctypes.c_int), ("n", ctypes.c_int), ("d_rois", ctypes.c_void_p),
+                ("d_init5", ctypes.c_void_p), ("prm", FitParams), ("d_out5", ctypes.c_void_p),
+                ("d_crlb5", ctypes.c_void_p), ("d_nll", ctypes.c_void_p), ("d_status", ctypes.c_void_p),
+                ("d_iters", ctypes.c_void_p)]
+
+
 EXPORTS = ["zola_ctx_create", "zola_ctx_destroy", "zola_last_error", "zola_ctx_stream", "zola_ctx_launches",
            "zola_ctx_set_pool", "zola_psf_load", "zola_psf_free", "zola_psf_info", "zola_psf_model",
            "zola_psf_model_dev", "zola_psf_model_prec", "zola_psf_model_prec_dev", "zola_fit_batch",
@@ -73,7 +80,8 @@ EXPORTS = ["zola_ctx_create", "zola_ctx_destroy", "zola_last_error", "zola_ctx_s
            "zola_calib_backward", "zola_calib_fit", "zola_ctx_set_split_mode", "zola_crlb_curve",
            "zola_psf_center_search", "zola_calib_init", "zola_drift", "zola_fit_batch_scmos",
            "zola_fit_batch_scmos_dev", "zola_localize_frames_scmos", "zola_ctx_set_flow", "zola_ctx_set_wait_limit",
-           "zola_fit_batch_stream_dev", "zola_ctx_set_tuning", "zola_fit_flow_shape", "zola_ctx_flow_stats"]
+           "zola_fit_batch_stream_dev", "zola_ctx_set_tuning", "zola_fit_flow_shape", "zola_ctx_flow_stats",
+           "zola_fit_batch_mixed_dev"]
 STAGES = ["split_stage1_pupil_dft", "split_stage2_window_dft", "split_stage3_blur_rows",
           "split_stage4_blur_cols_sums_lm", "split_fused_stages2_5", "fp64_fit", "fp64_model", "other",
           "split_dataflow"]
@@ -111,6 +119,7 @@ def lib():
         L.zola_ctx_set_tuning.argtypes = [vp, i, ctypes.c_char_p]
         L.zola_fit_flow_shape.argtypes = [vp, i, vp, vp, vp]
         L.zola_ctx_flow_stats.argtypes = [vp, vp, vp, vp]
+        L.zola_fit_batch_mixed_dev.argtypes = [vp, vp, i, vp]
         L.zola_crlb_curve.argtypes = [vp, i, vp, i, d, d, d, d, vp]
         L.zola_psf_center_search.argtypes = [vp, i, d, i, ctypes.POINTER(d)]
         L.zola_ctx_profile.argtypes = [vp, i]
@@ -588,6 +597,21 @@ def java_double(v):
     if lib().zola_format_double_java(float(v), b, 64) != 0:
         raise ZolaError("zola_format_double_java failed")
     return b.value.decode()
+
+
+def fit_mixed_dev(ctx, classes, stream=None):
+    """Mixed batch (zola_fit_batch_mixed_dev): classes is a list of dicts with psf, rois (n, R, R) float32,
+    init (n, 5) float64, prm (split precision), out (n, 5) and optional crlb, nll, status, iters, all torch
+    CUDA tensors; every class is fitted in one call."""
+    arr = (FitClass * max(1, len(classes)))()
+    for k, c in enumerate(classes):
+        rois = c["rois"]
+        arr[k] = FitClass(c["psf"].h.value if hasattr(c["psf"].h, "value") else c["psf"].h, int(rois.shape[1]),
+                          int(rois.shape[0]), rois.data_ptr(), c["init"].data_ptr(), c["prm"], c["out"].data_ptr(),
+                          *[c[x].data_ptr() if c.get(x) is not None else None
+                            for x in ("crlb", "nll", "status", "iters")])
+    ctx.check(lib().zola_fit_batch_mixed_dev(ctx.h, ctypes.cast(arr, ctypes.c_void_p), len(classes), stream),
+              "zola_fit_batch_mixed_dev")
 
 
 def fit_noalloc_dev(psf, rois, init, prm, out, crlb=None, nll=None, status=None, iters=None, stream=None):

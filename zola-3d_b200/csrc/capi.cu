@@ -151,6 +151,14 @@ int zola_ctx_destroy(zola_ctx* ctx) {
     if (ctx->h_flags) cudaFreeHost(ctx->h_flags);
     if (ctx->h_feed) cudaFreeHost(ctx->h_feed);
     if (ctx->h_tune) cudaFreeHost(ctx->h_tune);
+    if (ctx->h_mix) cudaFreeHost(ctx->h_mix);
+    for (cudaEvent_t e : ctx->mix_ev)
+        if (e) cudaEventDestroy(e);
+    for (cudaStream_t x : ctx->mix_stream)
+        if (x) {
+            cudaStreamSynchronize(x);
+            cudaStreamDestroy(x);
+        }
     for (cudaEvent_t e : ctx->tune_ev)
         if (e) cudaEventDestroy(e);
     if (ctx->ev_init) cudaEventDestroy(ctx->ev_init);
@@ -461,6 +469,34 @@ int zola_fit_batch_stream_dev(zola_ctx* ctx, zola_psf* psf, int R, const float* 
     if (ctx && n > 0 && !d_avail) return set_err(ctx, ZOLA_E_ARG, "zola_fit_batch_stream_dev: null ROI count");
     return fit_dev_impl(ctx, psf, R, d_rois, nullptr, d_init5, n, prm, d_out5, d_crlb5, d_nll, d_status, d_iters, stream,
                         nullptr, d_avail);
+}
+
+int zola_fit_batch_mixed_dev(zola_ctx* ctx, const zola_fit_class* classes, int nclass, void* stream) {
+    if (!ctx || nclass < 0 || nclass > ZOLA_MAX_CLASSES || (nclass > 0 && !classes)) return ZOLA_E_ARG;
+    cudaSetDevice(ctx->device);
+    zola::MixedClass mc[ZOLA_MAX_CLASSES];
+    int m = 0;
+    for (int c = 0; c < nclass; ++c) {
+        const zola_fit_class& k = classes[c];
+        if (!k.psf || k.psf->ctx != ctx) return set_err(ctx, ZOLA_E_ARG, "zola_fit_batch_mixed_dev: bad PSF");
+        if (!check_fit_params(ctx, &k.prm)) return ZOLA_E_ARG;
+        if (k.prm.precision != ZOLA_PREC_SPLIT)
+            return set_err(ctx, ZOLA_E_ARG, "zola_fit_batch_mixed_dev: every class needs split precision");
+        if (k.n < 0 || (k.n > 0 && (!k.d_rois || !k.d_init5 || !k.d_out5)))
+            return set_err(ctx, ZOLA_E_ARG, "zola_fit_batch_mixed_dev: bad n or null buffer");
+        if (k.psf->o.kz_reset)
+            return set_err(ctx, ZOLA_E_ARG, "fit needs a PSF built with kz_reset = 0 (the fit model tables)");
+        WindowTables* w = get_window(k.psf, k.R, ctx->err);
+        if (!w) return ZOLA_E_ARG;
+        if (k.n == 0) continue;
+        const zola_fit_params& pr = k.prm;
+        zola::FitParamsDev fp{pr.zmin, pr.zmax, pr.xymax, pr.tol_xyz, pr.step_xy, pr.step_z, pr.max_iter, 1e-3};
+        mc[m++] = zola::MixedClass{k.psf, w,
+                                   zola::FitIO{k.d_rois, nullptr, k.d_init5, k.n, fp, k.d_out5, k.d_crlb5, k.d_nll,
+                                               k.d_status, k.d_iters}};
+    }
+    if (m == 0) return ZOLA_OK;
+    return zola::launch_fit_split_mixed(ctx, m, mc, stream ? (cudaStream_t)stream : ctx->stream);
 }
 
 int zola_fit_batch(zola_ctx* ctx, zola_psf* psf, int R, const float* rois, const double* init5, int n,

@@ -543,19 +543,6 @@ constexpr int URING = 4;
 
 __host__ __device__ inline int unit_slots(int G1, int G2) { return G1 > G2 ? G1 : G2; }
 
-// The ROIs, start points and outputs of a fit.
-struct FitIO {
-    const float* rois;
-    const float* scmos;  // sCMOS var/gain^2 per pixel (Localization.java:1132), or null
-    const double* init;
-    int n;
-    FitParamsDev prm;
-    double* out5;
-    double* crlb5;
-    double* nll;
-    int* status;
-    int* iters;
-};
 
 __device__ __forceinline__ void st_release(int* p, int v) {
     asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
@@ -2755,9 +2742,11 @@ static void launch_stage2(zola_ctx* ctx, const SplitPool& sp, const FitIO& F, cu
 }
 
 // Pool of slots for n ROIs: at most pmax slots (0: state up to 8 GB, at most
-// 32768), in whole units; for the dataflow kernel at most max_units units.
+// 32768), in whole units; for the dataflow kernel at most max_units units.  The
+// pool's device state is carved from base, or from the context's scratch when
+// base is null; with need given, only the bytes it takes are reported.
 static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pmax_override, SplitPool& sp,
-                      cudaStream_t st, int max_units = 0) {
+                      cudaStream_t st, int max_units = 0, char* base_in = nullptr, size_t* need = nullptr) {
     if (p->D > 64) {
         ctx->err = "split path: pupil disk wider than 64 rows (grid too large for this optics)";
         return ZOLA_E_UNSUPPORTED;
@@ -2806,8 +2795,13 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
     const size_t b_sums = al((size_t)P * NSUM * 8);
     const size_t b_int = al((size_t)P * 8 + (size_t)sp.U * 4 + 64);
     const size_t b_clk = al(((size_t)3 * ctx->num_sms + 1) * 8);
-    if (ensure_scratch(ctx, b_a2 + b_a3 + b_a4 + b_t + b_lm + b_sums + b_clk + b_int, ctx->err)) return ZOLA_E_CUDA;
-    char* base = (char*)ctx->scratch;
+    const size_t total = b_a2 + b_a3 + b_a4 + b_t + b_lm + b_sums + b_clk + b_int;
+    if (need) {
+        *need = total;
+        return ZOLA_OK;
+    }
+    if (!base_in && ensure_scratch(ctx, total, ctx->err)) return ZOLA_E_CUDA;
+    char* base = base_in ? base_in : (char*)ctx->scratch;
     SplitDev& D = sp.D;
     D = SplitDev{};
     D.R = pl->R; D.W = pl->W; D.D = pl->D; D.DP = pl->DP; D.K1 = pl->K1;
@@ -3239,6 +3233,96 @@ int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d
             if (navail <= queue && (rc = poll_feed(true))) return rc;
         }
         if (rounds > max_rounds) { ctx->err = "split fit: did not drain the ROI queue"; return ZOLA_E_TIMEOUT; }
+    }
+    return ZOLA_OK;
+}
+
+// ------------------------------------------------------- mixed batches -----
+// Several ROI classes (PSF, ROI side) fitted in one call: each class gets its
+// own slot pool (carved from one scratch area) and its own stream, and the host
+// interleaves the classes' LM rounds, so the draining tail of one class
+// overlaps the others' work.  Each ROI's fit is the same bit for bit as in a
+// call of its class alone (a fit does not depend on its batch).
+int launch_fit_split_mixed(zola_ctx* ctx, int nc, MixedClass* mc, cudaStream_t st) {
+    if (nc > ZOLA_MAX_CLASSES) {
+        ctx->err = "zola_fit_batch_mixed_dev: too many classes";
+        return ZOLA_E_ARG;
+    }
+    std::vector<SplitPool> sp(nc);
+    std::vector<size_t> off(nc + 1, 0);
+    for (int c = 0; c < nc; ++c) {
+        size_t need = 0;
+        int rc = setup_pool(ctx, mc[c].p, mc[c].w, mc[c].F.n, ctx->split_pool_max, sp[c], st, 0, nullptr, &need);
+        if (rc) return rc;
+        off[c + 1] = off[c] + (need + 4095) / 4096 * 4096;
+    }
+    if (ensure_scratch(ctx, off[nc], ctx->err)) return ZOLA_E_CUDA;
+    if (!ctx->mix_ev[0])
+        for (auto& e : ctx->mix_ev) ZOLA_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), ctx);
+    if (!ctx->h_mix) ZOLA_CUDA_CHECK(cudaMallocHost(&ctx->h_mix, 4 * ZOLA_MAX_CLASSES * sizeof(int)), ctx);
+    ZOLA_CUDA_CHECK(cudaEventRecord(ctx->mix_ev[ZOLA_MAX_CLASSES], st), ctx);
+    struct State {
+        int rounds = 0, max_rounds = 0;
+        bool done = false;
+    };
+    std::vector<State> S(nc);
+    for (int c = 0; c < nc; ++c) {
+        if (!ctx->mix_stream[c]) ZOLA_CUDA_CHECK(cudaStreamCreateWithFlags(&ctx->mix_stream[c], cudaStreamNonBlocking), ctx);
+        cudaStream_t cs = ctx->mix_stream[c];
+        ZOLA_CUDA_CHECK(cudaStreamWaitEvent(cs, ctx->mix_ev[ZOLA_MAX_CLASSES], 0), ctx);
+        int rc = setup_pool(ctx, mc[c].p, mc[c].w, mc[c].F.n, ctx->split_pool_max, sp[c], cs, 0,
+                            (char*)ctx->scratch + off[c]);
+        if (rc) return rc;
+        const SplitDev& D = sp[c].D;
+        k_init_slots<<<(D.P + 127) / 128, 128, 0, cs>>>(D, mc[c].F.init, mc[c].F.n, mc[c].F.n, mc[c].F.prm);
+        ctx->launches++;
+        S[c].max_rounds = (mc[c].F.prm.max_iter + 2) * ((mc[c].F.n + D.P - 1) / D.P + 1) + 8;
+        S[c].done = mc[c].F.n == 0;
+    }
+    ZOLA_CUDA_CHECK(cudaGetLastError(), ctx);
+    for (;;) {
+        bool any = false;
+        for (int c = 0; c < nc; ++c) {
+            if (S[c].done) continue;
+            any = true;
+            cudaStream_t cs = ctx->mix_stream[c];
+            const SplitPool& p = sp[c];
+            const FitIO& F = mc[c].F;
+            const bool big = p.pl->W >= S45_MIN_W;
+            for (int k = 0; k < 4; ++k) {
+                launch_stages123(ctx, p, F, cs);
+                if (big)
+                    k_stage45p<<<unit_grid(ctx, p), S45_THREADS, p.s45, cs>>>(p.D, F);
+                else
+                    k_stage45s<<<unit_grid(ctx, p), S45S_THREADS, p.s45, cs>>>(p.D, F);
+                k_lm<<<(p.D.P + 127) / 128, 128, 0, cs>>>(p.D, F);
+                ctx->launches += 2;
+            }
+            S[c].rounds += 4;
+            ZOLA_CUDA_CHECK(cudaMemcpyAsync(ctx->h_mix + 4 * c, p.D.queue, 3 * sizeof(int), cudaMemcpyDeviceToHost, cs),
+                            ctx);
+            ZOLA_CUDA_CHECK(cudaEventRecord(ctx->mix_ev[c], cs), ctx);
+        }
+        if (!any) break;
+        ZOLA_CUDA_CHECK(cudaGetLastError(), ctx);
+        for (int c = 0; c < nc; ++c) {  // the other classes keep running while one is read back
+            if (S[c].done) continue;
+            ZOLA_CUDA_CHECK(cudaEventSynchronize(ctx->mix_ev[c]), ctx);
+            const int queue = ctx->h_mix[4 * c], active = ctx->h_mix[4 * c + 1], err = ctx->h_mix[4 * c + 2];
+            if (err) {
+                ctx->err = "split fit: a bounded device wait timed out";
+                return ZOLA_E_TIMEOUT;
+            }
+            if (active <= 0 && queue >= mc[c].F.n) S[c].done = true;
+            else if (S[c].rounds > S[c].max_rounds) {
+                ctx->err = "split fit: did not drain the ROI queue";
+                return ZOLA_E_TIMEOUT;
+            }
+        }
+    }
+    for (int c = 0; c < nc; ++c) {
+        ZOLA_CUDA_CHECK(cudaEventRecord(ctx->mix_ev[c], ctx->mix_stream[c]), ctx);
+        ZOLA_CUDA_CHECK(cudaStreamWaitEvent(st, ctx->mix_ev[c], 0), ctx);
     }
     return ZOLA_OK;
 }

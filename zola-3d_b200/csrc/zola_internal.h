@@ -48,6 +48,20 @@ struct FitParamsDev {
     double accept_nll = 0.0;
 };
 
+// The ROIs, start points and outputs of a fit.
+struct FitIO {
+    const float* rois;
+    const float* scmos;  // sCMOS var/gain^2 per pixel (Localization.java:1132), or null
+    const double* init;
+    int n;
+    FitParamsDev prm;
+    double* out5;
+    double* crlb5;
+    double* nll;
+    int* status;
+    int* iters;
+};
+
 // Host-side tables of one window size (FP64 and the split-precision packs).
 struct WindowTables {
     int R = 0, W = 0;
@@ -116,6 +130,11 @@ struct zola_ctx {
     double flow_busy[5] = {};              // last dataflow launch: busy fraction per stage
     double flow_clk_per_unit[5] = {};      // last dataflow launch: busy clocks per unit per stage (one CTA)
     double flow_evals = 0;                 // last dataflow launch: model evaluations
+    // mixed batches: a stream and a read-back event per class (the last event
+    // orders the classes after the caller's stream), pinned flag words
+    cudaStream_t mix_stream[ZOLA_MAX_CLASSES] = {};
+    cudaEvent_t mix_ev[ZOLA_MAX_CLASSES + 1] = {};
+    int* h_mix = nullptr;
     // optional per-kernel timing with CUDA events on the launch stream
     int profile = 0;
     std::vector<cudaEvent_t> ev_pool;
@@ -193,6 +212,13 @@ struct RoiFeed {
     const int* chunk_end = nullptr;
     const cudaEvent_t* ev = nullptr;
 };
+// One class of a mixed batch: its PSF, window tables and fit inputs/outputs.
+struct MixedClass {
+    zola_psf* p;
+    WindowTables* w;
+    FitIO F;
+};
+int launch_fit_split_mixed(zola_ctx* ctx, int nc, MixedClass* mc, cudaStream_t st);
 int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_rois, const float* d_scmos,
                      const double* d_init, int n, const zola_fit_params* prm, double* d_out5, double* d_crlb5,
                      double* d_nll, int* d_status, int* d_iters, cudaStream_t st, const RoiFeed* feed = nullptr,
