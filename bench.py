@@ -24,9 +24,14 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per model
-# evaluation of the dataflow kernel, from one capture of that kernel on a
-# smaller batch of the class (see profiles/); None until measured.
-NCU_TRAFFIC = {}
+# evaluation of each round-based kernel of the 48x48 tetrapod class: one launch
+# with all 4096 slots of a pool live (profiles/split_kernels_tetra48_dram_traffic.md).
+NCU_TRAFFIC = {
+    ("tetra48", "split_stage1_pupil_dft"): 117_036,
+    ("tetra48", "split_stage2_window_dft"): 283_487,
+    ("tetra48", "split_stage3_blur_rows"): 251_771,
+    ("tetra48", "split_stage4_blur_cols_sums_lm"): 107_996,
+}
 
 METRIC = "MLE ROI fits/sec at ≤0.5 nm vs FP64 oracle (batched split-prec vs plain GPU)"
 UNIT = "ROI fits/s"
@@ -241,6 +246,157 @@ def calibration_config(z, ctx, seed=3, fit_iters=10):
                     "oracle's single-thread NLL time)"}
 
 
+def small_roi_config(z, ctx, n=1000, seed=0, reps=5):
+    """Plain per-ROI localisation: 1,000 16x16 astigmatic ROIs (pupil 64^2, Z(2,2)
+    0.08 lambda + random Z(3,+-1), Z(4,0)), x, y ~ U(-1, 1) px, z ~ U(-0.6, 0.6) um,
+    photons LogNormal(ln 2000, 0.4), background 20, Poisson noise, seed 0; at most
+    30 evaluations.  The split and FP64 fits run through the host C-ABI (ROIs in
+    host memory, results back); the CPU arm is the oracle's restatement of the
+    reference CPU localisation (coordinate descent, Localization.java) on the same
+    ROIs with all host threads; the FP64 oracle LM of the same fit is the accuracy
+    reference for every ROI."""
+    import oracle as O
+    rng = np.random.default_rng(seed)
+    R, N = 16, 64
+    zern = zern_astig(np.random.default_rng(seed))
+    psf = z.PSF(ctx, z.optics(size_fft=N, xystep=DX, na=1.4, wavelength=0.66, n_oil=1.518, sigma=0.9), zern)
+    truth = np.c_[rng.uniform(-DX, DX, (n, 2)), rng.uniform(-0.6, 0.6, n), rng.lognormal(np.log(2000.0), 0.4, n),
+                  np.full(n, 20.0)]
+    rois = rng.poisson(truth[:, 3, None, None] * psf.model(R, truth[:, :3]) + 20.0).astype(np.float32)
+    init = np.zeros((n, 5))
+    init[:, 2] = np.round(truth[:, 2] / 0.1) * 0.1
+    border = np.concatenate([rois[:, 0, :], rois[:, -1, :], rois[:, 1:-1, 0], rois[:, 1:-1, -1]], axis=1)
+    init[:, 4] = border.mean(axis=1)
+    init[:, 3] = np.maximum(rois.sum(axis=(1, 2)) - init[:, 4] * R * R, 100.0)
+    kw = dict(zmin=-0.9, zmax=0.9, xymax=R * DX / 2, max_iter=30, tol_xyz=1e-4)
+    threads = os.cpu_count() or 1
+    ref = O.OraclePSF(N, DX, 1.4, 0.66, 1.518, 1.518, 0.9, zern, gauss_f32=False)
+    o, _, so, _ = ref.fit_lm(rois.astype(np.float64), init, kw["zmin"], kw["zmax"], kw["xymax"], tol_xyz=kw["tol_xyz"],
+                             max_iter=kw["max_iter"], threads=threads)
+    out = {"workload": "1,000 16x16 astigmatic ROIs, pupil 64^2, 30 evaluations at most, host ROIs in / results out",
+           "rois": n}
+    for name, prec in (("split", z.ZOLA_PREC_SPLIT), ("fp64", z.ZOLA_PREC_FP64)):
+        prm = z.PSF.fit_params(precision=prec, **kw)
+        res = psf.fit(rois, init, prm)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            res = psf.fit(rois, init, prm)
+        dt = (time.perf_counter() - t0) / reps
+        out[name] = {"fits_per_s": n / dt, "ms_per_call": dt * 1000,
+                     "accuracy_vs_oracle": accuracy_block(o, so, res["theta"], res["status"], False)}
+    # the reference CPU path on the same ROIs (its own init: A, B, x, y, z)
+    t0 = time.perf_counter()
+    ref.localize_cd(rois.astype(np.float64), np.c_[init[:, 3], init[:, 4], init[:, :3]], kw["zmin"], kw["zmax"], 20,
+                    0.0, threads=threads)
+    dt = time.perf_counter() - t0
+    out["cpu_port"] = {"fits_per_s": n / dt, "cores": threads, "kind": "port",
+                       "note": "oracle restatement of the reference coordinate descent (Localization.java), FFT model"}
+    out["split_vs_cpu_port"] = out["split"]["fits_per_s"] / out["cpu_port"]["fits_per_s"]
+    psf.close()
+    return out
+
+
+def filaments(rng, n_curves, lo, hi, zr, n_points):
+    """Points on random smooth 3-D curves (cubic Bezier, 4 random control
+    points in the box [lo, hi]^2 x [-zr, zr]) with 25 nm Gaussian jitter:
+    (n_points, 3) in um."""
+    t = rng.uniform(0, 1, n_points)
+    c = rng.integers(0, n_curves, n_points)
+    ctrl = np.concatenate([rng.uniform(lo, hi, (n_curves, 4, 2)), rng.uniform(-zr, zr, (n_curves, 4, 1))], axis=2)
+    b = np.stack([(1 - t) ** 3, 3 * t * (1 - t) ** 2, 3 * t ** 2 * (1 - t), t ** 3], axis=1)
+    pts = np.einsum("nk,nkd->nd", b, ctrl[c])
+    return pts + rng.normal(0, 0.025, pts.shape)
+
+
+def stream_drift_config(z, ctx, torch, device, nframes, seed=4):
+    """End-to-end stream with drift: 512x512 uint16 frames (camera offset 100
+    counts), Poisson(15) emitters a frame on synthetic filaments (random 3-D
+    cubic curves, 25 nm jitter), tetrapod PSF (45 modes, pupil 128^2), photons
+    LogNormal(ln 4000, 0.5), background 30, and an imposed drift: a random walk
+    of 0.5 nm a frame in x, y, z.  The split-precision detect -> fit pipeline
+    runs on the uint16 frames (host frames in, rows out, timed); then the 3-D
+    drift (20 time bins, 10 nm voxels) is estimated from the localizations in
+    a 5.12 x 5.12 um crop at the centre (one emitter a frame on average sits on
+    the crop's filaments; the others on filaments elsewhere in the frame), and
+    compared with the imposed walk."""
+    S, R, N, P = 512, 40, 128, 64
+    rng = np.random.default_rng(seed)
+    zern = zern_tetrapod(np.random.default_rng(seed * 100 + 7))
+    base = dict(size_fft=N, xystep=DX, na=1.4, wavelength=0.66, n_oil=1.518, sigma=0.9)
+    psf_det = z.PSF(ctx, z.optics(kz_reset=True, **base), zern)
+    psf_fit = z.PSF(ctx, z.optics(**base), zern)
+    fov = S * DX
+    c0, c1 = fov / 2 - 2.56, fov / 2 + 2.56
+    inner = filaments(rng, 6, c0 + 0.3, c1 - 0.3, 0.8, 200000)
+    outer = filaments(rng, 40, P * DX / 2, fov - P * DX / 2, 1.5, 800000)
+    outer = outer[(np.abs(outer[:, 0] - fov / 2) > 2.56 + R * DX / 2) | (np.abs(outer[:, 1] - fov / 2) > 2.56 + R * DX / 2)]
+    walk = np.cumsum(rng.normal(0, 0.5e-3, (nframes, 3)), axis=0)  # um
+    emit = []
+    for f in range(nframes):
+        k_in, k_out = rng.poisson(1.0), rng.poisson(14.0)
+        pts = np.concatenate([inner[rng.integers(0, len(inner), k_in)], outer[rng.integers(0, len(outer), k_out)]])
+        for q in pts:
+            emit.append((f, *(q + walk[f]), rng.lognormal(np.log(4000.0), 0.5)))
+    emit = np.array(emit)
+    cx, cy = emit[:, 1] / DX, emit[:, 2] / DX
+    ix, iy = cx.astype(int), cy.astype(int)
+    frames = np.empty((nframes, S, S), dtype=np.uint16)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    fb = 200
+    for f0 in range(0, nframes, fb):
+        f1 = min(nframes, f0 + fb)
+        sel = np.nonzero((emit[:, 0] >= f0) & (emit[:, 0] < f1))[0]
+        img = torch.full(((f1 - f0) * S * S,), 30.0, dtype=torch.float64, device=device)
+        if len(sel):
+            xyz = torch.tensor(np.c_[(ix[sel] - cx[sel]) * DX, (iy[sel] - cy[sel]) * DX, emit[sel, 3]],
+                               dtype=torch.float64, device=device)
+            psi = torch.empty((len(sel), P, P), dtype=torch.float64, device=device)
+            psf_fit.model_dev(P, xyz, psi, stream=torch.cuda.current_stream().cuda_stream)
+            torch.cuda.synchronize()
+            a = torch.arange(P, device=device) - P // 2
+            fr = torch.tensor(emit[sel, 0] - f0, dtype=torch.int64, device=device)
+            ii = torch.tensor(ix[sel], device=device)[:, None, None] + a[None, :, None]
+            jj = torch.tensor(iy[sel], device=device)[:, None, None] + a[None, None, :]
+            ok = (ii >= 0) & (ii < S) & (jj >= 0) & (jj < S)
+            flat = (fr[:, None, None] * S * S + ii.clamp(0, S - 1) * S + jj.clamp(0, S - 1))
+            amp = torch.tensor(emit[sel, 4], dtype=torch.float64, device=device)[:, None, None]
+            img.index_put_((flat[ok],), (amp * psi)[ok], accumulate=True)
+        cnt = torch.poisson(img, generator=gen) + 100.0
+        frames[f0:f1] = cnt.clamp(max=65535).to(torch.int32).cpu().numpy().reshape(f1 - f0, S, S).astype(np.uint16)
+    det = z.Detector(psf_det, S, S, R, -2.0, 2.0, 0.1, 0.1)
+    kw = dict(adu=1.0, gain=1.0, offset=100.0, photon_threshold=500.0, precision=z.ZOLA_PREC_SPLIT, max_iter=50,
+              tol_xyz=1e-4)
+    z.localize_frames_u16(ctx, det, psf_fit, frames[:8], -2.0, 2.0, **kw)  # warm-up: tables, plans
+    t0 = time.perf_counter()
+    rows = z.localize_frames_u16(ctx, det, psf_fit, frames, -2.0, 2.0, **kw)
+    dt = time.perf_counter() - t0
+    out = {"workload": "512x512 uint16 frames, Poisson(15) tetrapod emitters on filaments, drift random walk "
+                       "0.5 nm/frame; split-precision pipeline, host frames in / rows out",
+           "frames": nframes, "emitters": int(len(emit)), "localizations": int(len(rows)), "seconds": dt,
+           "frames_per_s": nframes / dt, "localizations_per_s": len(rows) / dt,
+           "h2d_bytes": int(frames.nbytes)}
+    xyz = np.c_[rows["x_nm"], rows["y_nm"], rows["z_nm"]]
+    crop = (np.abs(xyz[:, 0] / 1000 - fov / 2) < 2.56) & (np.abs(xyz[:, 1] / 1000 - fov / 2) < 2.56) & \
+        (np.abs(xyz[:, 2]) < 1280.0)
+    out["crop_localizations"] = int(crop.sum())
+    if crop.sum() > 100:
+        cr = np.c_[rows["crlb_x_nm"], rows["crlb_y_nm"], rows["crlb_z_nm"]][crop]
+        fr = rows["frame"][crop]
+        t0 = time.perf_counter()
+        b, l, px = z.drift(ctx, xyz[crop], fr, cr, pixel_nm=10.0, bins=20, max_drift_um=0.2)
+        out["drift_seconds"] = time.perf_counter() - t0
+        err = l - walk[fr] * 1000.0
+        err -= err.mean(axis=0)
+        out["drift_rms_error_nm"] = [float(v) for v in np.sqrt((err ** 2).mean(axis=0))]
+        out["imposed_drift_rms_nm"] = [float(v) for v in (walk * 1000.0 - (walk * 1000.0).mean(0)).std(axis=0)]
+        out["drift_voxel_nm"] = px
+    det.close()
+    psf_det.close()
+    psf_fit.close()
+    return out
+
+
 def run_step(z, ctx, job, precision, stream_ptr, mixed=True):
     """One step: the whole mixed job, in one zola_fit_batch_mixed_dev call (split precision), or one
     call per class."""
@@ -364,7 +520,7 @@ def config_block(n):
 
 # ----------------------------------------------------------------- main ----
 def flops_per_eval(R, N):
-    """model evaluation with x/y/z derivatives, complex MAC = 8 flops."""
+    """Algorithmic flops of one model evaluation with x/y/z derivatives (complex MAC = 8 flops)."""
     W, D = window(R, N), disk_rows(N)
     return 3 * 8 * W * D * D + 4 * 8 * W * W * D
 
@@ -415,6 +571,10 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="skip the dataflow-kernel autotuning pass")
     ap.add_argument("--no-calibration", dest="calibration", action="store_false",
                     help="skip the Zernike calibration measurement")
+    ap.add_argument("--stream-frames", type=int, default=0,
+                    help="frames of the 512x512 uint16 stream + drift measurement (0: skip)")
+    ap.add_argument("--no-small-rois", dest="small_rois", action="store_false",
+                    help="skip the 1,000-ROI 16x16 localisation measurement")
     ap.add_argument("--stage-breakdown", action="store_true",
                     help="also time the round-based stage kernels per stage (explains the dataflow kernel)")
     args = ap.parse_args()
@@ -586,7 +746,7 @@ def main():
             acc_oracle[cls["name"]] = accuracy_block(o, so, b[:m], sb[:m], cls["zsym"])
 
     # roofline: the dataflow kernel (the whole fit) of the class with the most
-    # device time, tensor-bound by SURVEY 8(d): flops of the model evaluations it
+    # device time, tensor-bound: algorithmic flops of the model evaluations it
     # made / its CUDA-event duration, against the sustained measured bf16 peak
     peaks = {}
     try:
@@ -597,7 +757,7 @@ def main():
     peak_tf = peaks.get("bf16_tflops_sustained", 1400.0)
     peak_gbs = peaks.get("hbm_gbs", 6650.0)
     peak_src = "of measured" if "bf16_tflops_sustained" in peaks and "hbm_gbs" in peaks else "of fallback"
-    # SURVEY 8(d) flops of each kernel per model evaluation: stage 1 the pupil DFT
+    # algorithmic flops of each kernel per model evaluation: stage 1 the pupil DFT
     # (3*8*W*D^2), stage 2 the window DFT (4*8*W^2*D), the dataflow kernel both
     def stage_flops(R, N):
         W, D = window(R, N), disk_rows(N)
@@ -635,13 +795,17 @@ def main():
                 "traffic": None if traffic is None else int(traffic * iters[dom_cls] / max(1, ent["launches"])),
                 "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum per launch: ncu bytes per model "
                                 "evaluation of this kernel on this class (profiles/), times the evaluations per launch",
+                "hbm_gbs_at_traffic": None if traffic is None else
+                round(traffic * iters[dom_cls] / (ent["ms"] / 1000.0) / 1e9, 1),
+                "hbm_frac_at_traffic": None if traffic is None else
+                round(traffic * iters[dom_cls] / (ent["ms"] / 1000.0) / 1e9 / peak_gbs, 4),
                 "whole_job_tflops": round(tot_flops / tot_s / 1e12, 2),
                 "whole_job_tensor_frac": round(tot_flops / tot_s / 1e12 / peak_tf, 4),
                 "per_class": by_class, "hbm_peak_gbs": peak_gbs,
-                "note": "achieved = SURVEY 8(d) algorithmic flops of the model evaluations made (pupil DFT 3*8*W*D^2, "
+                "note": "achieved = algorithmic flops of the model evaluations made (pupil DFT 3*8*W*D^2, "
                         "window DFT 4*8*W^2*D per evaluation, complex MAC = 8 flops; evaluations logged per ROI) / "
-                        "summed CUDA-event duration of that kernel's launches for that class; whole_job = all SURVEY "
-                        "8(d) flops / all fit kernels' time; peak = sustained measured bf16 (FP16 runs at the same rate)"}
+                        "summed CUDA-event duration of that kernel's launches for that class; whole_job = all "
+                        "algorithmic flops / all fit kernels' time; peak = sustained measured bf16 (FP16 runs at the same rate)"}
 
     # end to end through the host C-ABI (pinned host buffers, H2D + D2H inside the call)
     e2e = None
@@ -676,6 +840,9 @@ def main():
 
     detect = detect_fit_config(z, ctx, args.detect_frames, seed=1 + rank) if args.detect_frames > 0 else None
     calib = calibration_config(z, ctx) if args.calibration and rank == 0 else None
+    small = small_roi_config(z, ctx) if args.small_rois and rank == 0 else None
+    stream = stream_drift_config(z, ctx, torch, device, args.stream_frames) if args.stream_frames > 0 and rank == 0 \
+        else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -697,7 +864,8 @@ def main():
                 "speedup_vs_fp64_plain": value / world / fp64_value,
                 "accuracy_vs_oracle": acc_oracle, "accuracy_vs_fp64_gpu": acc64,
                 "stage_breakdown_round_based": breakdown,
-                "detect_fit_pipeline": detect, "calibration": calib}
+                "detect_fit_pipeline": detect, "calibration": calib, "small_roi_localisation": small,
+                "stream_drift": stream}
         print(json.dumps(line), flush=True)
     for j in job:
         j["psf"].close()

@@ -204,6 +204,13 @@ ZOLA_API int zola_detector_info(const zola_detector* det, int* nslices, double* 
  * 41-slice library gives several thousand). */
 #define ZOLA_DETECT_MAX_CAP (1 << 20)
 ZOLA_API int zola_detect(zola_detector* det, const double* frames, int nframes, int cap, double* out, int* counts);
+/* Camera-count form: frames are nframes x SX x SY uint16 counts as the camera
+ * writes them (2 bytes a pixel over the host link), turned into photons on
+ * the device as LocalizationPipeline.java:601-605 does: count * (adu / gain) +
+ * (-offset * adu / gain), negative values set to 0 (adu, gain, offset: the
+ * arguments of the LocalizationPipeline constructor, :100-107). */
+ZOLA_API int zola_detect_u16(zola_detector* det, const uint16_t* frames, int nframes, int cap, double adu,
+                             double gain, double offset, double* out, int* counts);
 /* Device form, asynchronous on stream: cap is also the number of candidates
  * stored per frame, so a frame with counts[f] > cap gets the sorted first cap
  * of its list in insertion order -- the same rows on every run, but not the
@@ -248,6 +255,13 @@ typedef struct {
 ZOLA_API int zola_localize_frames(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const double* frames,
                                   int nframes, int frame0, const zola_loc_params* prm, zola_localization* out,
                                   int out_cap, int* nout);
+
+/* Camera-count form of the pipeline: uint16 frames converted on the device
+ * with adu, gain and offset exactly as zola_detect_u16 does
+ * (LocalizationPipeline.java:100-107, 601-605); rows as zola_localize_frames. */
+ZOLA_API int zola_localize_frames_u16(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const uint16_t* frames,
+                                      int nframes, int frame0, const zola_loc_params* prm, double adu, double gain,
+                                      double offset, zola_localization* out, int out_cap, int* nout);
 
 /* sCMOS form of the pipeline (LocalizationPipeline.java:588-640, 799-820,
  * utils/SCMOScamera.java): adu frames (float, nframes x SX x SY) and per-pixel

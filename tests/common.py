@@ -1,4 +1,4 @@
-"""Shared optics set-ups for the tests (BASELINE-style configurations, small)."""
+"""Shared optics set-ups for the tests (the benchmark optics, at small sizes)."""
 import numpy as np
 
 TWO_PI = 2 * np.pi

@@ -141,3 +141,32 @@ def test_pipeline_rows_match_oracle_lm_pipeline(zpkg, ctx, S, R, N, zern, nf, em
         assert np.allclose(got[c][conv], want[conv, k], rtol=2e-3)
     assert list(got["id"]) == list(range(len(got)))
     det.close()
+
+
+def test_uint16_frames_equal_photon_frames(zpkg, ctx):
+    """Camera counts converted on the device (count * adu / gain - offset * adu /
+    gain, clamped at 0, as LocalizationPipeline.java:601-605) give the candidate
+    lists and rows of the same photons passed as doubles."""
+    zern = astig_zernike()
+    S, R = 96, 16
+    psf_det = zpkg.PSF(ctx, zpkg.optics(size_fft=64, kz_reset=True, **OPTICS), zern)
+    psf_fit = zpkg.PSF(ctx, zpkg.optics(size_fft=64, **OPTICS), zern)
+    ref_fit = O.OraclePSF(64, 0.11, 1.4, 0.66, 1.518, 1.518, 0.9, zern)
+    photons = make_frames(ref_fit.model, S, 6, seed=123, emitters=4, R=32)
+    adu, gain, offset = 0.47, 2.0, 100.0
+    counts = np.clip(np.round(photons * gain / adu + offset), 0, 65535).astype(np.uint16)
+    counts[0, :6, :6] = 7  # below the offset: these photons clamp to 0
+    ph = counts.astype(np.float64) * (adu / gain) + (-offset * adu / gain)
+    ph[ph < 0] = 0.0
+    det = zpkg.Detector(psf_det, S, S, R, -0.6, 0.6, 0.11, 0.1)
+    g16, c16 = det.detect_u16(counts, adu, gain, offset, cap=1024)
+    g64, c64 = det.detect(ph, cap=1024)
+    assert np.array_equal(c16, c64) and c64.sum() > 0
+    for a, b in zip(g16, g64):
+        assert np.array_equal(a, b)
+    kw = dict(photon_threshold=300.0, precision=1, max_iter=40)
+    r16 = zpkg.localize_frames_u16(ctx, det, psf_fit, counts, -0.6, 0.6, adu=adu, gain=gain, offset=offset, **kw)
+    r64 = zpkg.localize_frames(ctx, det, psf_fit, ph, -0.6, 0.6, **kw)
+    assert len(r64) > 10
+    assert np.array_equal(r16, r64)
+    det.close()

@@ -1,5 +1,5 @@
 """GPU tests of the split-precision tcgen05 path against the FP64 device path
-and the CPU oracle (north_star tolerances: 0.5 nm x/y, 1 nm z, 1e-3 photons)."""
+and the CPU oracle (tolerances: 0.5 nm x/y, 1 nm z, 1e-3 photons)."""
 import numpy as np
 import pytest
 
@@ -63,7 +63,7 @@ def test_split_fit_matches_oracle_every_roi(zpkg, ctx, N, R, zern):
     """The split-precision fit against the FP64 oracle of the same fit
     (oracle.fit_lm: the same LM algorithm, FP64 model through FFTs), ROI by
     ROI, every status included.  Fits that end with the same status agree
-    within the north_star tolerances (0.5 nm x/y, 1 nm z, 1e-3 photons) when
+    within the tolerances (0.5 nm x/y, 1 nm z, 1e-3 photons) when
     converged; status disagreements are rare (the model differs by ~2^-22, so
     an accept/reject decision on a flat likelihood can flip) and their
     parameter difference stays below 0.5 nm / 1 nm / 1e-3 too once both fits

@@ -63,7 +63,7 @@ def test_lm_and_reference_coordinate_descent_agree():
     assert (st == 1).all()
     cd, crlb, stc, _ = p.localize_cd(pat, np.c_[init[:, 3], init[:, 4], init[:, :3]], -0.9, 0.9, 20)
     assert (stc == 1).all()
-    # north_star tolerances: 0.5 nm in x/y, 1 nm in z
+    # accuracy tolerances: 0.5 nm in x/y, 1 nm in z
     assert np.abs(cd[:, :2] - lm[:, :2]).max() < 0.5e-3
     assert np.abs(cd[:, 2] - lm[:, 2]).max() < 1e-3
     assert (crlb > 0).all() and (crlb < 0.1).all()

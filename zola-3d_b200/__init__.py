@@ -81,7 +81,7 @@ EXPORTS = ["zola_ctx_create", "zola_ctx_destroy", "zola_last_error", "zola_ctx_s
            "zola_psf_center_search", "zola_calib_init", "zola_drift", "zola_fit_batch_scmos",
            "zola_fit_batch_scmos_dev", "zola_localize_frames_scmos", "zola_ctx_set_flow", "zola_ctx_set_wait_limit",
            "zola_fit_batch_stream_dev", "zola_ctx_set_tuning", "zola_fit_flow_shape", "zola_ctx_flow_stats",
-           "zola_fit_batch_mixed_dev"]
+           "zola_fit_batch_mixed_dev", "zola_detect_u16", "zola_localize_frames_u16"]
 STAGES = ["split_stage1_pupil_dft", "split_stage2_window_dft", "split_stage3_blur_rows",
           "split_stage4_blur_cols_sums_lm", "split_fused_stages2_5", "fp64_fit", "fp64_model", "other",
           "split_dataflow"]
@@ -140,6 +140,9 @@ def lib():
         L.zola_detector_free.argtypes = [vp]
         L.zola_detector_info.argtypes = [vp, ctypes.POINTER(i), vp, vp]
         L.zola_detect.argtypes = [vp, vp, i, i, vp, vp]
+        L.zola_detect_u16.argtypes = [vp, vp, i, i, d, d, d, vp, vp]
+        L.zola_localize_frames_u16.argtypes = [vp, vp, vp, vp, i, i, ctypes.POINTER(LocParams), d, d, d, vp, i,
+                                               ctypes.POINTER(i)]
         L.zola_detect_dev.argtypes = [vp, vp, i, i, vp, vp, vp]
         L.zola_fit_batch_noalloc.argtypes = [vp, i, vp, vp, i, ctypes.POINTER(FitParams), vp, vp, vp, vp, vp, vp]
         L.zola_ctx_stage_stats.argtypes = [vp, vp, vp, i]
@@ -407,6 +410,16 @@ class Detector:
         self.psf.ctx.check(lib().zola_detect(self.h, _ptr(frames), nf, cap, _ptr(out), _ptr(counts)), "zola_detect")
         return [out[f, :min(cap, counts[f])] for f in range(nf)], counts
 
+    def detect_u16(self, frames, adu=1.0, gain=1.0, offset=0.0, cap=2048):
+        """detect() on uint16 camera frames, converted to photons on the device."""
+        frames = np.ascontiguousarray(frames, dtype=np.uint16)
+        nf = frames.shape[0]
+        out = np.zeros((nf, cap, 7))
+        counts = np.zeros(nf, np.int32)
+        self.psf.ctx.check(lib().zola_detect_u16(self.h, _ptr(frames), nf, cap, float(adu), float(gain), float(offset),
+                                                 _ptr(out), _ptr(counts)), "zola_detect_u16")
+        return [out[f, :min(cap, counts[f])] for f in range(nf)], counts
+
     def detect_dev(self, frames, cap, out, counts, stream=None):
         self.psf.ctx.check(lib().zola_detect_dev(self.h, _ptr(frames), frames.shape[0], cap, _ptr(out), _ptr(counts),
                                                  stream), "zola_detect_dev")
@@ -536,25 +549,53 @@ LOC_COLUMNS = ["id", "frame", "x_nm", "y_nm", "z_nm", "intensity", "background",
                "crlb_z_nm", "candidate", "fit_status"]
 
 
+LOC_DTYPE = np.dtype([(c, np.int32 if c in ("id", "frame", "candidate", "fit_status") else np.float64)
+                      for c in LOC_COLUMNS])
+assert LOC_DTYPE.itemsize == ctypes.sizeof(Localization)  # the packed dtype is the C struct's layout
+
+
+def _loc_params(det, minZ, maxZ, photon_threshold, max_snr, max_iter, tol_xyz, precision, cand_cap,
+                frames_per_batch, wave_fits):
+    return LocParams(det.R, float(minZ), float(maxZ), float(photon_threshold), float(max_snr), int(max_iter),
+                     float(tol_xyz), int(precision), int(cand_cap), int(frames_per_batch), int(wave_fits))
+
+
+def _loc_rows(ctx, nf, call, name):
+    """Run one pipeline entry point into a row buffer and return its rows as a
+    structured array (LOC_DTYPE; the buffer is the C array itself)."""
+    cap = max(64, nf * 64)
+    out = np.empty(cap, dtype=LOC_DTYPE)
+    n = ctypes.c_int()
+    ctx.check(call(out.ctypes.data_as(ctypes.c_void_p), cap, ctypes.byref(n)), name)
+    return out[:n.value].copy()
+
+
 def localize_frames(ctx, det, fit_psf, frames, minZ, maxZ, photon_threshold=500.0, max_snr=1.0, max_iter=30,
                     tol_xyz=1e-4, precision=ZOLA_PREC_FP64, frame0=0, cand_cap=0, frames_per_batch=1024, wave_fits=0):
     """Detect and localize every frame (LocalizationPipeline): returns a
     structured numpy array with LOC_COLUMNS, one row per localization."""
     frames = np.ascontiguousarray(frames, dtype=np.float64)
     nf = frames.shape[0]
-    prm = LocParams(det.R, float(minZ), float(maxZ), float(photon_threshold), float(max_snr), int(max_iter),
-                    float(tol_xyz), int(precision), int(cand_cap), int(frames_per_batch), int(wave_fits))
-    cap = max(64, nf * 64)
-    out = (Localization * cap)()
-    n = ctypes.c_int()
-    ctx.check(lib().zola_localize_frames(ctx.h, det.h, fit_psf.h, _ptr(frames), nf, int(frame0), ctypes.byref(prm),
-                                         ctypes.cast(out, ctypes.c_void_p), cap, ctypes.byref(n)),
-              "zola_localize_frames")
-    dt = np.dtype([(c, np.int32 if c in ("id", "frame", "candidate", "fit_status") else np.float64) for c in LOC_COLUMNS])
-    arr = np.zeros(n.value, dtype=dt)
-    for k in range(n.value):
-        arr[k] = tuple(getattr(out[k], c) for c in LOC_COLUMNS)
-    return arr
+    prm = _loc_params(det, minZ, maxZ, photon_threshold, max_snr, max_iter, tol_xyz, precision, cand_cap,
+                      frames_per_batch, wave_fits)
+    return _loc_rows(ctx, nf, lambda out, cap, n: lib().zola_localize_frames(
+        ctx.h, det.h, fit_psf.h, _ptr(frames), nf, int(frame0), ctypes.byref(prm), out, cap, n),
+        "zola_localize_frames")
+
+
+def localize_frames_u16(ctx, det, fit_psf, frames, minZ, maxZ, adu=1.0, gain=1.0, offset=0.0, photon_threshold=500.0,
+                        max_snr=1.0, max_iter=30, tol_xyz=1e-4, precision=ZOLA_PREC_FP64, frame0=0, cand_cap=0,
+                        frames_per_batch=1024, wave_fits=0):
+    """The pipeline on uint16 camera frames (n, SX, SY), converted to photons on
+    the device as count * adu / gain - offset * adu / gain, clamped at 0."""
+    frames = np.ascontiguousarray(frames, dtype=np.uint16)
+    nf = frames.shape[0]
+    prm = _loc_params(det, minZ, maxZ, photon_threshold, max_snr, max_iter, tol_xyz, precision, cand_cap,
+                      frames_per_batch, wave_fits)
+    return _loc_rows(ctx, nf, lambda out, cap, n: lib().zola_localize_frames_u16(
+        ctx.h, det.h, fit_psf.h, _ptr(frames), nf, int(frame0), ctypes.byref(prm), float(adu), float(gain),
+        float(offset), out, cap, n), "zola_localize_frames_u16")
+
 
 def localize_frames_scmos(ctx, det, fit_psf, adu, offset, gain, variance, minZ, maxZ, photon_threshold=500.0,
                           max_snr=1.0, max_iter=30, tol_xyz=1e-4, precision=ZOLA_PREC_FP64, frame0=0, cand_cap=0,
@@ -563,20 +604,11 @@ def localize_frames_scmos(ctx, det, fit_psf, adu, offset, gain, variance, minZ, 
     adu = np.ascontiguousarray(adu, dtype=np.float32)
     maps = [np.ascontiguousarray(m, dtype=np.float64) for m in (offset, gain, variance)]
     nf = adu.shape[0]
-    prm = LocParams(det.R, float(minZ), float(maxZ), float(photon_threshold), float(max_snr), int(max_iter),
-                    float(tol_xyz), int(precision), int(cand_cap), int(frames_per_batch), int(wave_fits))
-    cap = max(64, nf * 64)
-    out = (Localization * cap)()
-    n = ctypes.c_int()
-    ctx.check(lib().zola_localize_frames_scmos(ctx.h, det.h, fit_psf.h, _ptr(adu), nf, int(frame0), ctypes.byref(prm),
-                                               _ptr(maps[0]), _ptr(maps[1]), _ptr(maps[2]),
-                                               ctypes.cast(out, ctypes.c_void_p), cap, ctypes.byref(n)),
-              "zola_localize_frames_scmos")
-    dt = np.dtype([(c, np.int32 if c in ("id", "frame", "candidate", "fit_status") else np.float64) for c in LOC_COLUMNS])
-    arr = np.zeros(n.value, dtype=dt)
-    for k in range(n.value):
-        arr[k] = tuple(getattr(out[k], c) for c in LOC_COLUMNS)
-    return arr
+    prm = _loc_params(det, minZ, maxZ, photon_threshold, max_snr, max_iter, tol_xyz, precision, cand_cap,
+                      frames_per_batch, wave_fits)
+    return _loc_rows(ctx, nf, lambda out, cap, n: lib().zola_localize_frames_scmos(
+        ctx.h, det.h, fit_psf.h, _ptr(adu), nf, int(frame0), ctypes.byref(prm), _ptr(maps[0]), _ptr(maps[1]),
+        _ptr(maps[2]), out, cap, n), "zola_localize_frames_scmos")
 
 
 def write_csv(path, locs, append=False):

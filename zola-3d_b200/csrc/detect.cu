@@ -133,6 +133,112 @@ __global__ void __launch_bounds__(256) k_det_corr(DetView V, int zc, const doubl
 }
 
 // ---------------------------------------------------------------------------
+// Register-tiled form of the same correlation (same terms, same order per
+// output: u outer, v inner, one FMA each), bound by the FP64 FMA pipe instead
+// of shared-memory loads.  A CTA of 256 threads covers a 32 x 64 output tile
+// and RZC slices; each thread owns 8 consecutive outputs of one row for every
+// slice (32 accumulators).  For each kernel row u a thread keeps an 8-wide
+// window of the image row in registers and slides it along v, so one image
+// load and RZC broadcast library loads feed 8 RZC FMAs.  A half-warp holds
+// 16 consecutive rows of one 8-column group; with an odd row stride their
+// window loads fall in 16 different bank pairs.
+constexpr int RTI = 32, RTJ = 64, RPX = 8, RZC = 4;
+
+__host__ __device__ inline int rt_stride(int R) { return (RTJ + R) | 1; }
+__host__ __device__ inline size_t rt_smem(int R, int zc) {
+    return (size_t)(RTI + R) * rt_stride(R) * 8 + (size_t)zc * R * R * 8;
+}
+
+__global__ void __launch_bounds__(256, 2) k_det_corr_rt(DetView V, int zc, const double* frames, const double* var,
+                                                         double* score) {
+    extern __shared__ double sm[];
+    const int SX = V.SX, SY = V.SY, R = V.R, Z = V.Z, h = R / 2, TS = rt_stride(R), TH = RTI + R;
+    const int f = blockIdx.z, z0 = blockIdx.y * zc;
+    const int tiles_j = (SY + RTJ - 1) / RTJ;
+    const int i0 = (blockIdx.x / tiles_j) * RTI, j0 = (blockIdx.x % tiles_j) * RTJ;
+    double* tile = sm;                    // (RTI + R) rows x TS (RTJ + R used, zero-filled)
+    double* ps = tile + (size_t)TH * TS;  // zc x R x R
+    const double* img = frames + (size_t)f * SX * SY;
+    const int TW = RTJ + R;  // the last window load (v = R - 1) reads column RTJ + R - 1
+    for (int k = threadIdx.x; k < TH * TW; k += blockDim.x) {
+        const int a = k / TW, b = k - a * TW;
+        const int i = i0 - h + a, j = j0 - h + b;
+        tile[a * TS + b] = (i >= 0 && i < SX && j >= 0 && j < SY) ? img[(size_t)i * SY + j] : 0.0;
+    }
+    const int nz = min(zc, Z - z0);
+    for (int k = threadIdx.x; k < nz * R * R; k += blockDim.x) ps[k] = V.psf0[(size_t)z0 * R * R + k];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ti = (lane & 15) + 16 * (warp & 1), tj = 8 * (2 * (warp >> 1) + (lane >> 4));
+    double acc[RZC][RPX];
+#pragma unroll
+    for (int q = 0; q < RZC; ++q)
+#pragma unroll
+        for (int k = 0; k < RPX; ++k) acc[q][k] = 0.0;
+    const int RR = R * R;
+    for (int u = 0; u < R; ++u) {
+        const double* trow = tile + (ti + u) * TS + tj;
+        const double* prow = ps + u * R;
+        double w[RPX];
+#pragma unroll
+        for (int k = 0; k < RPX; ++k) w[k] = trow[k];
+        for (int v = 0; v < R; ++v) {
+            double p[RZC];
+#pragma unroll
+            for (int q = 0; q < RZC; ++q) p[q] = q < nz ? prow[q * RR + v] : 0.0;
+#pragma unroll
+            for (int q = 0; q < RZC; ++q)
+#pragma unroll
+                for (int k = 0; k < RPX; ++k) acc[q][k] = fma(w[k], p[q], acc[q][k]);
+#pragma unroll
+            for (int k = 0; k < RPX - 1; ++k) w[k] = w[k + 1];
+            w[RPX - 1] = trow[v + RPX];
+        }
+    }
+    const int i = i0 + ti;
+    if (i >= SX) return;
+    for (int k = 0; k < RPX; ++k) {
+        const int j = j0 + tj + k;
+        if (j >= SY) break;
+        const double vi = var[(size_t)f * SX * SY + (size_t)i * SY + j];
+#pragma unroll
+        for (int q = 0; q < RZC; ++q) {
+            if (q >= nz) break;
+            const int r = z0 + q;
+            const double vp = V.varpsf[r];
+            const double s = sqrt(vp * vi);
+            double o;
+            if (s > 0) o = (acc[q][k] * V.inv_m) / s;
+            else if (vp <= 0) o = -1.0;
+            else o = -2.0;
+            score[(((size_t)f * Z + r) * SX + i) * SY + j] = o;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Camera counts to photons as LocalizationPipeline.java:601-605 does it:
+// value * (adu / gain) + (-offset * adu / gain), a product then a sum (Java
+// does not contract them), negative results set to 0.
+__global__ void k_u16_photons(const uint16_t* in, size_t n, double slope, double intercept, double* out) {
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+        const double v = __dadd_rn(__dmul_rn((double)in[k], slope), intercept);
+        out[k] = v < 0 ? 0.0 : v;
+    }
+}
+
+void rescale_u16(zola_ctx* ctx, const uint16_t* d_in, size_t n, const double* rescale, double* d_out,
+                 cudaStream_t st) {
+    k_u16_photons<<<ctx->num_sms * 8, 256, 0, st>>>(d_in, n, rescale[0], rescale[1], d_out);
+    ctx->launches++;
+}
+
+void camera_rescale(double adu, double gain, double offset, double* rescale) {
+    rescale[0] = adu / gain;            // rescale_slope (LocalizationPipeline.java:103)
+    rescale[1] = -offset * adu / gain;  // rescale_intercept (:104)
+}
+
+// ---------------------------------------------------------------------------
 __device__ inline double parabola_top(double xa, double ya, double xb, double yb, double xc, double yc) {
     const double a = (yc - ya) / ((xc - xa) * (xc - xb)) - (yb - ya) / ((xb - xa) * (xc - xb));
     const double b = ((yb - ya) / (xb - xa)) - a * (xb + xa);
@@ -418,13 +524,21 @@ int zola_detect_dev(zola_detector* d, const double* d_frames, int nframes, int c
         const double* fr = d_frames + (size_t)f0 * SS;
         prof_begin(ctx, 7, st);
         k_det_var<<<nf, 256, 0, st>>>(v, fr, rowsum, rowsq, var);
-        const int tiles = ((v.SX + DT - 1) / DT) * ((v.SY + DT - 1) / DT);
-        const size_t tile_b = (size_t)(DT + v.R) * (DT + v.R) * 8, slice_b = (size_t)v.R * v.R * 8;
-        const int zc = (int)std::max<size_t>(1, std::min<size_t>(ZC, (200 * 1024 - tile_b) / slice_b));
-        const size_t smem = tile_b + (size_t)zc * slice_b;
-        cudaFuncSetAttribute(k_det_corr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        dim3 grid(tiles, (v.Z + zc - 1) / zc, nf);
-        k_det_corr<<<grid, 256, smem, st>>>(v, zc, fr, var, score);
+        if (rt_smem(v.R, RZC) <= 112 * 1024) {  // two register-tiled CTAs per SM
+            const int tiles = ((v.SX + RTI - 1) / RTI) * ((v.SY + RTJ - 1) / RTJ);
+            const size_t smem = rt_smem(v.R, RZC);
+            cudaFuncSetAttribute(k_det_corr_rt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            dim3 grid(tiles, (v.Z + RZC - 1) / RZC, nf);
+            k_det_corr_rt<<<grid, 256, smem, st>>>(v, RZC, fr, var, score);
+        } else {
+            const int tiles = ((v.SX + DT - 1) / DT) * ((v.SY + DT - 1) / DT);
+            const size_t tile_b = (size_t)(DT + v.R) * (DT + v.R) * 8, slice_b = (size_t)v.R * v.R * 8;
+            const int zc = (int)std::max<size_t>(1, std::min<size_t>(ZC, (200 * 1024 - tile_b) / slice_b));
+            const size_t smem = tile_b + (size_t)zc * slice_b;
+            cudaFuncSetAttribute(k_det_corr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            dim3 grid(tiles, (v.Z + zc - 1) / zc, nf);
+            k_det_corr<<<grid, 256, smem, st>>>(v, zc, fr, var, score);
+        }
         // the row sums are dead after k_det_var: their space holds the peak flags
         k_det_nms<<<nf, 1024, 0, st>>>(v, score, tmp, (unsigned char*)rowsum, cand, d_counts + f0);
         const size_t ssort = gsort ? 0 : (size_t)p2 * 12;
@@ -438,10 +552,17 @@ int zola_detect_dev(zola_detector* d, const double* d_frames, int nframes, int c
     return ZOLA_OK;
 }
 
-int zola_detect(zola_detector* d, const double* frames, int nframes, int cap, double* out, int* counts) {
+}  // extern "C"
+
+namespace {
+
+// frames (photons) or u16 camera counts with rescale = {slope, intercept}
+int detect_impl(zola_detector* d, const double* frames, const uint16_t* u16, const double* rescale, int nframes,
+                int cap, double* out, int* counts) {
     if (!d) return ZOLA_E_ARG;
     zola_ctx* ctx = d->psf->ctx;
-    if (nframes < 0 || cap < 1 || cap > ZOLA_DETECT_MAX_CAP || (nframes > 0 && (!frames || !out || !counts))) {
+    if (nframes < 0 || cap < 1 || cap > ZOLA_DETECT_MAX_CAP ||
+        (nframes > 0 && ((!frames && !u16) || !out || !counts))) {
         ctx->err = "zola_detect: bad nframes / cap (1..2^20) or null buffer";
         return ZOLA_E_ARG;
     }
@@ -450,10 +571,17 @@ int zola_detect(zola_detector* d, const double* frames, int nframes, int cap, do
     double* df = nullptr;
     double* dout = nullptr;
     int* dc = nullptr;
+    uint16_t* du = nullptr;
     int room = cap;  // candidates stored per frame on the device
     cudaError_t e = cudaMalloc(&df, SS * nframes * 8);
     if (e == cudaSuccess) e = cudaMalloc(&dc, (size_t)nframes * 4);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(df, frames, SS * nframes * 8, cudaMemcpyHostToDevice, ctx->stream);
+    if (u16) {
+        if (e == cudaSuccess) e = cudaMalloc(&du, SS * nframes * 2);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(du, u16, SS * nframes * 2, cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess) rescale_u16(ctx, du, SS * nframes, rescale, df, ctx->stream);
+    } else if (e == cudaSuccess) {
+        e = cudaMemcpyAsync(df, frames, SS * nframes * 8, cudaMemcpyHostToDevice, ctx->stream);
+    }
     int rc = ZOLA_OK;
     // A frame whose list is longer than the room is detected again with room for
     // all of it, so that its rows are the first cap of the whole sorted list.
@@ -483,8 +611,29 @@ int zola_detect(zola_detector* d, const double* frames, int nframes, int cap, do
     if (df) cudaFree(df);
     if (dout) cudaFree(dout);
     if (dc) cudaFree(dc);
+    if (du) cudaFree(du);
     if (e != cudaSuccess) { ctx->err = std::string("zola_detect: ") + cudaGetErrorString(e); return ZOLA_E_CUDA; }
     return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int zola_detect(zola_detector* d, const double* frames, int nframes, int cap, double* out, int* counts) {
+    return detect_impl(d, frames, nullptr, nullptr, nframes, cap, out, counts);
+}
+
+int zola_detect_u16(zola_detector* d, const uint16_t* frames, int nframes, int cap, double adu, double gain,
+                    double offset, double* out, int* counts) {
+    if (!d) return ZOLA_E_ARG;
+    if (!(gain != 0) || !std::isfinite(adu) || !std::isfinite(gain) || !std::isfinite(offset)) {
+        d->psf->ctx->err = "zola_detect_u16: adu, gain, offset must be finite and gain non-zero";
+        return ZOLA_E_ARG;
+    }
+    double rescale[2];
+    camera_rescale(adu, gain, offset, rescale);
+    return detect_impl(d, nullptr, frames, rescale, nframes, cap, out, counts);
 }
 
 }  // extern "C"

@@ -368,9 +368,11 @@ __global__ void k_pipe_scmos(const float* adu, const double* offset, const doubl
 namespace {
 
 // frames: photon frames (no sCMOS); or adu + offset/gain/variance maps (sCMOS).
+// u16: camera counts (with rescale = {slope, intercept}) instead of photon frames.
 int localize_impl(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const double* frames, const float* adu,
                   const double* offset, const double* gain, const double* variance, int nframes, int frame0,
-                  const zola_loc_params* prm, zola_localization* out, int out_cap, int* nout) {
+                  const zola_loc_params* prm, zola_localization* out, int out_cap, int* nout,
+                  const uint16_t* u16 = nullptr, const double* rescale = nullptr) {
     const bool scmos = adu != nullptr;
     *nout = 0;
     if (nframes <= 0) return ZOLA_OK;
@@ -391,7 +393,7 @@ int localize_impl(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const do
     const int slot_cap = FB * K;
     Buf b_img, b_mask, b_cand, b_cnt, b_lib, b_rng, b_cslot, b_cmax, b_ptr, b_lim, b_done, b_ns, b_rois, b_init, b_sf,
         b_sc, b_out5, b_st, b_xyz, b_psi, b_mthr, b_acc, b_seq, b_nacc, b_dpsi, b_rows, b_fimg, b_adu, b_off, b_gain,
-        b_vg, b_sv;
+        b_vg, b_sv, b_u16;
     cudaError_t e = cudaSuccess;
     auto A = [&](Buf& b, size_t bytes) { if (e == cudaSuccess) e = b.alloc(bytes); };
     A(b_img, SS * FB * 8); A(b_mask, SS * FB); A(b_cand, (size_t)FB * cap * 7 * 8); A(b_cnt, (size_t)FB * 4);
@@ -402,6 +404,7 @@ int localize_impl(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const do
     A(b_sc, (size_t)slot_cap * 4); A(b_out5, (size_t)slot_cap * 40); A(b_st, (size_t)slot_cap * 4);
     A(b_xyz, (size_t)slot_cap * 24); A(b_psi, RR * slot_cap * 8); A(b_mthr, (size_t)slot_cap * 8);
     A(b_acc, (size_t)slot_cap * 4); A(b_seq, (size_t)slot_cap * 4);
+    if (u16) A(b_u16, SS * FB * 2);
     if (scmos) {
         A(b_fimg, SS * FB * 8); A(b_adu, SS * FB * 4); A(b_off, SS * 8); A(b_gain, SS * 8); A(b_vg, SS * 8);
         A(b_sv, RR * slot_cap * 4);
@@ -445,6 +448,9 @@ int localize_impl(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const do
                                                               (double*)b_fimg.p);
                 ctx->launches++;
             }
+        } else if (u16) {  // 2 bytes a pixel over the host link, photons made on the device
+            e = cudaMemcpyAsync(b_u16.p, u16 + (size_t)f0 * SS, SS * nf * 2, cudaMemcpyHostToDevice, st);
+            if (e == cudaSuccess) rescale_u16(ctx, (const uint16_t*)b_u16.p, SS * nf, rescale, (double*)b_img.p, st);
         } else {
             e = cudaMemcpyAsync(b_img.p, frames + (size_t)f0 * SS, SS * nf * 8, cudaMemcpyHostToDevice, st);
         }
@@ -557,6 +563,20 @@ extern "C" int zola_localize_frames(zola_ctx* ctx, zola_detector* det, zola_psf*
     if (!ctx || !det || !fit_psf || !prm || !nout || (nframes > 0 && (!frames || !out))) return ZOLA_E_ARG;
     return localize_impl(ctx, det, fit_psf, frames, nullptr, nullptr, nullptr, nullptr, nframes, frame0, prm, out,
                          out_cap, nout);
+}
+
+extern "C" int zola_localize_frames_u16(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const uint16_t* frames,
+                                        int nframes, int frame0, const zola_loc_params* prm, double adu, double gain,
+                                        double offset, zola_localization* out, int out_cap, int* nout) {
+    if (!ctx || !det || !fit_psf || !prm || !nout || (nframes > 0 && (!frames || !out))) return ZOLA_E_ARG;
+    if (!(gain != 0) || !std::isfinite(adu) || !std::isfinite(gain) || !std::isfinite(offset)) {
+        ctx->err = "zola_localize_frames_u16: adu, gain, offset must be finite and gain non-zero";
+        return ZOLA_E_ARG;
+    }
+    double rescale[2];
+    camera_rescale(adu, gain, offset, rescale);
+    return localize_impl(ctx, det, fit_psf, nullptr, nullptr, nullptr, nullptr, nullptr, nframes, frame0, prm, out,
+                         out_cap, nout, frames, rescale);
 }
 
 extern "C" int zola_localize_frames_scmos(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const float* adu,

@@ -225,6 +225,10 @@ int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d
                      const int* d_avail = nullptr);
 
 int ensure_scratch(zola_ctx* ctx, size_t bytes, std::string& err);
+// camera counts -> photons (LocalizationPipeline.java:601-605): rescale = {adu / gain, -offset adu / gain}
+void camera_rescale(double adu, double gain, double offset, double* rescale);
+void rescale_u16(zola_ctx* ctx, const uint16_t* d_in, size_t n, const double* rescale, double* d_out,
+                 cudaStream_t st);
 int ensure_io(zola_ctx* ctx, size_t bytes);
 
 // Owned device allocation released on scope exit (one-time host paths).
