@@ -42,7 +42,7 @@ def build(force=False, verbose=False, ptxas_v=False):
                 print(" ".join(cmd), flush=True)
             subprocess.check_call(cmd)
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lcufft", "-Xlinker", "-rpath",
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-Xlinker", "-rpath",
                                                               "-Xlinker", "/usr/local/cuda/lib64"]
         if verbose:
             print(" ".join(cmd), flush=True)

@@ -13,15 +13,14 @@
 // mean CRLB (:540-640).  The per-localization drift is the SplineFit of the
 // bin drifts at its frame (:660-700).
 //
-// GPU: histograms by atomic adds, batched 3-D C2C FFTs (cuFFT, single
-// precision like the reference's float transforms), pair products, inverse
-// FFTs and the centring crop in chunks of pairs, and one CTA per pair for the
-// peak centroid.  The circular shift the reference applies before the forward
+// GPU: histograms by atomic adds, batched 3-D C2C FFTs (the hand-written
+// radix-2 transform below, single precision like the reference's float
+// transforms), pair products, inverse FFTs and the centring crop in chunks of
+// pairs, and one CTA per pair for the peak centroid.  The circular shift the reference applies before the forward
 // FFT multiplies every spectrum by the same sign pattern, which cancels in
 // F_t conj(F_s), so it is left out.  The least squares and the spline run on
 // the host.
 #include <cuda_runtime.h>
-#include <cufft.h>
 
 #include <algorithm>
 #include <cmath>
@@ -64,6 +63,77 @@ __global__ void k_drift_gauss(DriftDev D, float2* spec, double sf0, double sf1, 
         const float g = (float)exp(-.5 * (dx * dx / sf2 + dy * dy / sf1 + dz * dz / sf0));
         spec[k].x *= g;
         spec[k].y *= g;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Batched complex FFT along one axis of [outer][L][inner] data (L a power of
+// two, 2 .. 256): line (o, i) holds the elements (o L + k) inner + i.  A CTA
+// takes TL consecutive lines into shared memory (bit-reversed), runs the
+// log2(L) radix-2 decimation-in-time stages there and writes them back in
+// place.  Loads and stores run along the line (inner = 1) or across lines
+// (inner > 1), whichever is contiguous in memory.  Unnormalised; sign -1 is
+// exp(-2 pi i j k / L) (forward), +1 the inverse.  tw[m] = exp(-2 pi i m / 256),
+// m < 128, rounded from double; length L uses every (256 / L)-th entry.
+constexpr int FFT_LMAX = 256, FFT_THREADS = 256;
+
+__global__ void __launch_bounds__(FFT_THREADS) k_fft_lines(float2* data, int L, int lg, long long inner,
+                                                           long long lines, int TL, const float2* tw, float sign) {
+    extern __shared__ float2 sbuf[];
+    const int LS = L + 1;
+    const long long q0 = (long long)blockIdx.x * TL;
+    const int nl = (int)min((long long)TL, lines - q0);
+    auto addr = [&](int q, int k) {
+        const long long line = q0 + q, o = line / inner, i = line - o * inner;
+        return (o * L + k) * inner + i;
+    };
+    for (int e = threadIdx.x; e < nl * L; e += FFT_THREADS) {
+        int q, k;
+        if (inner == 1) { q = e / L; k = e - q * L; } else { k = e / nl; q = e - k * nl; }
+        sbuf[q * LS + (int)(__brev((unsigned)k) >> (32 - lg))] = data[addr(q, k)];
+    }
+    __syncthreads();
+    const int H = L / 2;
+    for (int half = 1; half < L; half <<= 1) {
+        const int ts = (FFT_LMAX / 2) / half;
+        for (int b = threadIdx.x; b < nl * H; b += FFT_THREADS) {
+            const int q = b / H, j = b - q * H, m = j & (half - 1);
+            const int i0 = q * LS + 2 * (j - m) + m, i1 = i0 + half;
+            float2 w = tw[m * ts];
+            w.y *= -sign;
+            const float2 a = sbuf[i0], c = sbuf[i1];
+            const float2 t = make_float2(w.x * c.x - w.y * c.y, w.x * c.y + w.y * c.x);
+            sbuf[i0] = make_float2(a.x + t.x, a.y + t.y);
+            sbuf[i1] = make_float2(a.x - t.x, a.y - t.y);
+        }
+        __syncthreads();
+    }
+    for (int e = threadIdx.x; e < nl * L; e += FFT_THREADS) {
+        int q, k;
+        if (inner == 1) { q = e / L; k = e - q * L; } else { k = e / nl; q = e - k * nl; }
+        data[addr(q, k)] = sbuf[q * LS + k];
+    }
+}
+
+// In-place 3-D FFTs of `batch` cubes [P0][P1][P2] (x = P2 fastest), one pass per axis.
+static void fft3d(zola_ctx* ctx, float2* d, int batch, int P0, int P1, int P2, float sign, const float2* tw,
+                  cudaStream_t st) {
+    const int dims[3] = {P0, P1, P2};
+    const long long total = (long long)batch * P0 * P1 * P2;
+    long long inner = 1;
+    for (int ax = 2; ax >= 0; --ax) {
+        const int L = dims[ax];
+        if (L > 1) {
+            int lg = 0;
+            while ((1 << lg) < L) ++lg;
+            const long long lines = total / L;
+            const int TL = (int)std::max<long long>(1, std::min<long long>(lines, 4096 / (L + 1)));  // <= 32 KB
+            const size_t smem = (size_t)TL * (L + 1) * sizeof(float2);
+            k_fft_lines<<<(unsigned)((lines + TL - 1) / TL), FFT_THREADS, smem, st>>>(d, L, lg, inner, lines, TL, tw,
+                                                                                     sign);
+            ctx->launches++;
+        }
+        inner *= L;
     }
 }
 
@@ -278,15 +348,6 @@ struct DriftSpline {
     }
 };
 
-struct CufftPlan {
-    cufftHandle h = 0;
-    bool ok = false;
-    CufftPlan() = default;
-    CufftPlan(const CufftPlan&) = delete;
-    CufftPlan& operator=(const CufftPlan&) = delete;
-    ~CufftPlan() { if (ok) cufftDestroy(h); }
-};
-
 }  // namespace
 
 extern "C" int zola_drift(zola_ctx* ctx, const double* xyz_nm, const double* crlb_nm, const int* frame, int n,
@@ -368,14 +429,16 @@ extern "C" int zola_drift(zola_ctx* ctx, const double* xyz_nm, const double* crl
         ZOLA_CUDA_CHECK(cudaMemcpyAsync(d_p2.p, p2.data(), (size_t)4 * tot, cudaMemcpyHostToDevice, st), ctx);
         ZOLA_CUDA_CHECK(cudaMemsetAsync(d_res.p, 0, RV * tot * sizeof(float), st), ctx);
     }
-    CufftPlan fwd, inv;
-    int dims[3] = {D.P0, D.P1, D.P2};
-    fwd.ok = cufftPlanMany(&fwd.h, 3, dims, nullptr, 1, (int)PV, nullptr, 1, (int)PV, CUFFT_C2C, bin) == CUFFT_SUCCESS;
-    if (fwd.ok) inv.ok = cufftPlanMany(&inv.h, 3, dims, nullptr, 1, (int)PV, nullptr, 1, (int)PV, CUFFT_C2C, CH) ==
-                         CUFFT_SUCCESS;
-    if (!fwd.ok || !inv.ok || cufftSetStream(fwd.h, st) != CUFFT_SUCCESS || cufftSetStream(inv.h, st) != CUFFT_SUCCESS) {
-        ctx->err = "zola_drift: cuFFT plan failed";
-        return ZOLA_E_CUDA;
+    // twiddles exp(-2 pi i m / 256), m < 128, for every transform length
+    DevBuf<float2> d_tw;
+    {
+        std::vector<float2> tw(FFT_LMAX / 2);
+        for (int m = 0; m < FFT_LMAX / 2; ++m)
+            tw[m] = make_float2((float)std::cos(2 * M_PI * m / FFT_LMAX), (float)-std::sin(2 * M_PI * m / FFT_LMAX));
+        ZOLA_CUDA_CHECK(d_tw.alloc(tw.size()), ctx);
+        ZOLA_CUDA_CHECK(cudaMemcpyAsync(d_tw.p, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice, st),
+                        ctx);
+        ZOLA_CUDA_CHECK(cudaStreamSynchronize(st), ctx);  // tw is a host temporary
     }
     const int grid = ctx->num_sms * 8;
     for (int u = 0; u < nbw[0]; ++u)
@@ -388,20 +451,13 @@ extern "C" int zola_drift(zola_ctx* ctx, const double* xyz_nm, const double* crl
                 }
                 ZOLA_CUDA_CHECK(cudaMemsetAsync(d_spec.p, 0, PV * bin * sizeof(float2), st), ctx);
                 k_drift_hist<<<(n + 255) / 256, 256, 0, st>>>(D, d_xyz.p, d_frame.p, n, d_spec.p);
-                if (cufftExecC2C(fwd.h, (cufftComplex*)d_spec.p, (cufftComplex*)d_spec.p, CUFFT_FORWARD) != CUFFT_SUCCESS) {
-                    ctx->err = "zola_drift: forward FFT failed";
-                    return ZOLA_E_CUDA;
-                }
+                fft3d(ctx, d_spec.p, bin, D.P0, D.P1, D.P2, -1.f, d_tw.p, st);
                 k_drift_gauss<<<grid, 256, 0, st>>>(D, d_spec.p, sfp[2], sfp[1], sfp[0]);
                 ctx->launches += 2;
                 for (int first = 0; first < tot; first += CH) {
                     const int np = std::min(CH, tot - first);
                     k_drift_pairs<<<grid, 256, 0, st>>>(D, d_spec.p, d_p1.p, d_p2.p, first, np, d_corr.p);
-                    if (cufftExecC2C(inv.h, (cufftComplex*)d_corr.p, (cufftComplex*)d_corr.p, CUFFT_INVERSE) !=
-                        CUFFT_SUCCESS) {
-                        ctx->err = "zola_drift: inverse FFT failed";
-                        return ZOLA_E_CUDA;
-                    }
+                    fft3d(ctx, d_corr.p, np, D.P0, D.P1, D.P2, 1.f, d_tw.p, st);
                     k_drift_crop<<<grid, 256, 0, st>>>(D, d_corr.p, first, np, d_res.p);
                     ctx->launches += 2;
                 }
