@@ -563,12 +563,13 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--classes", default="", help="comma list of ROI classes to run (profiling); default all")
-    ap.add_argument("--pool", type=int, default=16384, help="max ROIs in flight per fit call (0: library default)")
+    ap.add_argument("--pool", type=int, default=0,
+                    help="slots of the split fit's pool per class (0: chosen by the library's autotuner)")
     ap.add_argument("--detect-frames", type=int, default=200,
                     help="frames of the detect -> fit pipeline measurement (0: skip)")
     ap.add_argument("--split-mode", default="staged", choices=["staged", "flow", "fused"],
                     help="split fit kernels: one dataflow kernel, four stage kernels per round, or stage 1 + fused 2-5")
-    ap.add_argument("--no-tune", action="store_true", help="skip the dataflow-kernel autotuning pass")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuning pass (slot pool per class, or the dataflow kernel shape)")
     ap.add_argument("--no-calibration", dest="calibration", action="store_false",
                     help="skip the Zernike calibration measurement")
     ap.add_argument("--stream-frames", type=int, default=0,
@@ -630,6 +631,19 @@ def main():
         for j in job:
             t, units, ctas, ns = j["psf"].flow_shape(j["cls"]["R"])
             tuned[j["cls"]["name"]] = {"tuned": t, "units": units, "ctas_per_stage": ctas, "ns_per_eval": ns}
+    # round-based kernels: the slot pool per class (four trial fits of each class
+    # alone; the fits are the same bit for bit whatever the pool)
+    if args.split_mode == "staged" and not args.no_tune and args.pool == 0:
+        ctx.set_tuning(True)
+        for j in job:
+            for _ in range(4):
+                fit_class(j)
+                ext.synchronize()
+        ctx.set_tuning(False)
+    if args.split_mode == "staged":
+        for j in job:
+            t, pool, ns = j["psf"].split_pool(j["cls"]["R"])
+            tuned[j["cls"]["name"]] = {"tuned": t, "pool": pool, "ns_per_eval": ns}
 
     # warm-up (split path), also primes tables and the slot pool
     for _ in range(args.warmup):
@@ -856,10 +870,10 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f16x3 (split) / f32 sums / f64 solve", "data": "synthetic",
                 "config": dict(config_block(args.rois), parallelism=f"replicas x{world}", split_kernels=args.split_mode,
-                               pool=args.pool or "library default"),
+                               pool=args.pool or "autotuned per class (tuned_shapes)"),
                 "e2e": e2e, "gpu_launches": int(launches), "clocks": clk, "roofline": roofline,
                 "cpu_baseline": cpu,
-                "split_per_class": per_class, "dataflow_shape": tuned,
+                "split_per_class": per_class, "tuned_shapes": tuned,
                 "fp64_plain_gpu": {"value": fp64_value, "unit": UNIT, "per_class": fp64},
                 "speedup_vs_fp64_plain": value / world / fp64_value,
                 "accuracy_vs_oracle": acc_oracle, "accuracy_vs_fp64_gpu": acc64,

@@ -405,6 +405,16 @@ ZOLA_API int zola_ctx_set_tuning(zola_ctx* ctx, int enable, const char* cache_pa
  * and, when tuned, the measured ns per model evaluation (nullable pointers).
  * Returns 1 when tuned, 0 for the default shape, < 0 on error. */
 ZOLA_API int zola_fit_flow_shape(zola_psf* psf, int R, int* units, int* ctas, double* ns_per_eval);
+/* Slot pool of the round-based split fit (ZOLA_SPLIT_STAGED) for psf's R x R
+ * ROIs.  With tuning on (zola_ctx_set_tuning) and no explicit pool
+ * (zola_ctx_set_pool 0), the first four fits of a class with at least 131072
+ * ROIs try pools of 4096, 8192, 16384 and 32768 slots (each capped at 8 GB of
+ * pool state) and keep the fastest in device time per model evaluation; the
+ * choice goes to the tuning cache file with the dataflow shapes, and mixed
+ * batches use it too.  Returns 1 and the tuned pool (and its ns per
+ * evaluation) when tuned, 0 and the context's setting (0: automatic) when not.
+ * A fit's results do not depend on the pool. */
+ZOLA_API int zola_fit_split_pool(zola_psf* psf, int R, int* pool, double* ns_per_eval);
 /* Bookkeeping of the last dataflow fit on this context, per stage (pupil DFT,
  * window DFT, row blur, column blur + sums, LM step): the fraction of time its
  * CTAs had a unit to work on, and the busy GPU clocks one CTA spent per unit;

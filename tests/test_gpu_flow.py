@@ -150,3 +150,68 @@ def test_autotuner_changes_timings_only(zpkg, ctx, tmp_path):
     finally:
         c2.close()
     psf.close()
+
+
+def test_pool_tuner_changes_timings_only(zpkg, tmp_path):
+    """With tuning on and an automatic pool, the round-based split fit tries
+    four slot pools on the first large fits of a class and keeps the fastest;
+    every trial gives the fits of the default pool bit for bit (a fit does not
+    depend on its batch), and the choice goes to the cache file and back."""
+    import json
+    import torch
+    dev = torch.device("cuda", 0)
+    c = zpkg.Context(0)
+    try:
+        psf = zpkg.PSF(c, zpkg.optics(size_fft=64, **OPTICS), astig_zernike())
+        m, rep, R = 8192, 16, 16
+        n = m * rep
+        rng = np.random.default_rng(8)
+        truth = np.c_[rng.uniform(-0.11, 0.11, (m, 2)), rng.uniform(-0.5, 0.5, m),
+                      rng.lognormal(np.log(2500.0), 0.5, m), np.full(m, 20.0)]
+        psi = torch.empty((m, R, R), dtype=torch.float64, device=dev)
+        psf.model_dev(R, torch.tensor(truth[:, :3], device=dev), psi, stream=c.stream)
+        torch.cuda.synchronize()
+        g = torch.Generator(device=dev)
+        g.manual_seed(12)
+        rois = torch.poisson(torch.tensor(truth[:, 3], device=dev)[:, None, None] * psi + 20.0,
+                             generator=g).float().repeat(rep, 1, 1).contiguous()
+        init = np.tile(truth, (rep, 1))
+        init[:, :2] = 0
+        init[:, 2] = np.round(init[:, 2] / 0.1) * 0.1
+        d_init = torch.tensor(init, device=dev)
+        prm = zpkg.PSF.fit_params(-1.0, 1.0, 0.88, max_iter=50, tol_xyz=1e-4, precision=zpkg.ZOLA_PREC_SPLIT)
+
+        def run():
+            out = [torch.zeros((n, 5), dtype=torch.float64, device=dev), torch.zeros(n, dtype=torch.int32, device=dev)]
+            psf.fit_dev(rois, d_init, prm, out[0], None, None, out[1], None, stream=c.stream)
+            torch.cuda.synchronize()
+            return out[0].cpu().numpy(), out[1].cpu().numpy()
+
+        c.set_pool(0)
+        base = run()
+        assert psf.split_pool(R)[0] is False
+        cache = str(tmp_path / "pool_tune.json")
+        c.set_tuning(True, cache)
+        try:
+            for _ in range(4):
+                got = run()
+                assert np.array_equal(got[0], base[0]) and np.array_equal(got[1], base[1])
+        finally:
+            c.set_tuning(False)
+        tuned, pool, ns = psf.split_pool(R)
+        assert tuned and pool in (4096, 8192, 16384, 32768) and ns > 0
+        got = run()  # the tuned pool
+        assert np.array_equal(got[0], base[0]) and np.array_equal(got[1], base[1])
+        entries = {k: v for k, v in json.load(open(cache)).items() if k.endswith("_pool")}
+        assert list(entries.values())[0]["pool"] == pool
+        psf.close()
+    finally:
+        c.close()
+    c2 = zpkg.Context(0)
+    try:
+        c2.set_tuning(False, cache)
+        p2 = zpkg.PSF(c2, zpkg.optics(size_fft=64, **OPTICS), astig_zernike())
+        assert p2.split_pool(R)[:2] == (True, pool)
+        p2.close()
+    finally:
+        c2.close()

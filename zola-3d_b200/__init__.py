@@ -81,7 +81,7 @@ EXPORTS = ["zola_ctx_create", "zola_ctx_destroy", "zola_last_error", "zola_ctx_s
            "zola_psf_center_search", "zola_calib_init", "zola_drift", "zola_fit_batch_scmos",
            "zola_fit_batch_scmos_dev", "zola_localize_frames_scmos", "zola_ctx_set_flow", "zola_ctx_set_wait_limit",
            "zola_fit_batch_stream_dev", "zola_ctx_set_tuning", "zola_fit_flow_shape", "zola_ctx_flow_stats",
-           "zola_fit_batch_mixed_dev", "zola_detect_u16", "zola_localize_frames_u16"]
+           "zola_fit_batch_mixed_dev", "zola_detect_u16", "zola_localize_frames_u16", "zola_fit_split_pool"]
 STAGES = ["split_stage1_pupil_dft", "split_stage2_window_dft", "split_stage3_blur_rows",
           "split_stage4_blur_cols_sums_lm", "split_fused_stages2_5", "fp64_fit", "fp64_model", "other",
           "split_dataflow"]
@@ -119,6 +119,7 @@ def lib():
         L.zola_ctx_set_tuning.argtypes = [vp, i, ctypes.c_char_p]
         L.zola_fit_flow_shape.argtypes = [vp, i, vp, vp, vp]
         L.zola_ctx_flow_stats.argtypes = [vp, vp, vp, vp]
+        L.zola_fit_split_pool.argtypes = [vp, i, vp, vp]
         L.zola_fit_batch_mixed_dev.argtypes = [vp, vp, i, vp]
         L.zola_crlb_curve.argtypes = [vp, i, vp, i, d, d, d, d, vp]
         L.zola_psf_center_search.argtypes = [vp, i, d, i, ctypes.POINTER(d)]
@@ -353,6 +354,15 @@ class PSF:
         if rc < 0:
             self.ctx.check(rc, "zola_fit_flow_shape")
         return bool(rc), u.value, list(c), ns.value
+
+    def split_pool(self, R):
+        """(tuned, pool slots, ns per evaluation) of the round-based split fit for R x R ROIs."""
+        pool = ctypes.c_int()
+        ns = ctypes.c_double()
+        rc = lib().zola_fit_split_pool(self.h, int(R), ctypes.byref(pool), ctypes.byref(ns))
+        if rc < 0:
+            self.ctx.check(rc, "zola_fit_split_pool")
+        return bool(rc), pool.value, ns.value
 
     def fit_stream_dev(self, rois, init, avail, prm, out, crlb=None, nll=None, status=None, iters=None, stream=None):
         """Streaming device form (zola_fit_batch_stream_dev): avail is a one-element int32 CUDA tensor holding

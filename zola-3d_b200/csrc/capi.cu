@@ -342,6 +342,13 @@ int zola_fit_flow_shape(zola_psf* psf, int R, int* units, int* ctas, double* ns_
     return tuned ? 1 : 0;
 }
 
+int zola_fit_split_pool(zola_psf* psf, int R, int* pool, double* ns_per_eval) {
+    if (!psf) return ZOLA_E_ARG;
+    WindowTables* w = get_window(psf, R, psf->ctx->err);
+    if (!w) return ZOLA_E_ARG;
+    return split_pool_choice(psf, w, pool, ns_per_eval);
+}
+
 int zola_ctx_flow_stats(zola_ctx* ctx, double* busy, double* clocks_per_unit, double* evaluations) {
     if (!ctx) return ZOLA_E_ARG;
     for (int s = 0; s < zola::FLOW_STAGES; ++s) {

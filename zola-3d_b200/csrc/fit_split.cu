@@ -1516,7 +1516,6 @@ __device__ __noinline__ void lm_slot(const SplitDev& P, const FitIO& io, int slo
     const FitParamsDev& prm = io.prm;
     const int roi = P.slot_roi[slot];
     if (roi < 0) return;
-    if (P.evals) atomicAdd(P.evals, 1ull);
     const double* tot = P.sums + (size_t)slot * NSUM;
     double nll = tot[NRED] != 0.0 ? INFINITY : tot[0], g[5], H[25], F[25];
     for (int q = 0; q < 5; ++q) g[q] = tot[1 + q];
@@ -1558,7 +1557,10 @@ __device__ __noinline__ void lm_slot(const SplitDev& P, const FitIO& io, int slo
 // The round-based fit's LM step: every occupied slot of the pool, one thread each.
 __global__ void k_lm(SplitDev P, FitIO F) {
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot < P.P) lm_slot(P, F, slot);
+    const bool live = slot < P.P && P.slot_roi[slot] >= 0;
+    const unsigned m = __ballot_sync(0xffffffffu, live);  // model evaluations: one atomic per warp
+    if (P.evals && (threadIdx.x & 31) == 0 && m) atomicAdd(P.evals, (unsigned long long)__popc(m));
+    if (live) lm_slot(P, F, slot);
 }
 
 // ------------------------------------------------- LM stage (dataflow) -----
@@ -1607,7 +1609,10 @@ __device__ void lm_role(const SplitDev& P, const FitIO& F, int first, int stride
             // (a unit another stage handed out carries the claim bit; this stage claims none)
             if ((v & UNIT_CLAIMED) || v % FLOW_STAGES != FLOW_STAGES - 1) continue;
             const long long b0 = clock64();
-            if (g < UG) lm_slot(P, F, u * UG + g);
+            const bool lv = g < UG && P.slot_roi[u * UG + g] >= 0;
+            const unsigned lmask = __ballot_sync(gmask, lv);
+            if (g == 0 && lmask) atomicAdd(P.evals, (unsigned long long)__popc(lmask));
+            if (lv) lm_slot(P, F, u * UG + g);
             __syncwarp(gmask);
             // every ROI takes at most max_iter evaluations: more means the fit lost
             // track of its slots, and the whole kernel stops with an error
@@ -2937,7 +2942,8 @@ static std::string tune_key(const zola_psf* p, const WindowTables* w) {
            std::to_string(w->W);
 }
 
-// The autotuner's cache: {"<class>": {"units": U, "ctas": [a, b, c, d], "ns_per_eval": t}, ...}
+// The autotuner's cache: {"<class>": {"units": U, "ctas": [a, b, c, d, e], "ns_per_eval": t}, ...} for the
+// dataflow kernel, {"<class>_pool": {"pool": P, "ns_per_eval": t}, ...} for the round-based kernels.
 static void tune_save(zola_ctx* ctx) {
     if (ctx->tune_path.empty()) return;
     FILE* f = std::fopen(ctx->tune_path.c_str(), "w");
@@ -2950,6 +2956,12 @@ static void tune_save(zola_ctx* ctx) {
         std::fprintf(f, "%s\n  \"%s\": {\"units\": %d, \"ctas\": [%d, %d, %d, %d, %d], \"ns_per_eval\": %.3f}",
                      first ? "" : ",", kv.first.c_str(), b.units, b.ctas[0], b.ctas[1], b.ctas[2], b.ctas[3],
                      b.ctas[4], kv.second.best_ns);
+        first = false;
+    }
+    for (const auto& kv : ctx->pool_tunes) {
+        if (!kv.second.done) continue;
+        std::fprintf(f, "%s\n  \"%s\": {\"pool\": %d, \"ns_per_eval\": %.3f}", first ? "" : ",", kv.first.c_str(),
+                     kv.second.best, kv.second.best_ns);
         first = false;
     }
     std::fprintf(f, "\n}\n");
@@ -2972,6 +2984,14 @@ void tune_load(zola_ctx* ctx) {
         const std::string key = txt.substr(pos + 1, end - pos - 1);
         pos = end + 1;
         if (key.empty() || key[0] != 'N') continue;
+        PoolTune pt;
+        if (std::sscanf(txt.c_str() + pos, " : {\"pool\": %d, \"ns_per_eval\": %lf", &pt.best, &pt.best_ns) == 2) {
+            if (pt.best > 0) {
+                pt.done = true;
+                ctx->pool_tunes[key] = pt;
+            }
+            continue;
+        }
         FlowTune t;
         if (std::sscanf(txt.c_str() + pos, " : {\"units\": %d, \"ctas\": [%d, %d, %d, %d, %d], \"ns_per_eval\": %lf",
                         &t.best.units, &t.best.ctas[0], &t.best.ctas[1], &t.best.ctas[2], &t.best.ctas[3],
@@ -3033,6 +3053,38 @@ static void tune_record(zola_ctx* ctx, const std::string& key, const FlowShape& 
         tune_save(ctx);
     }
 }
+
+// Slot pools the round-based tuner tries, in this order (each capped by the
+// 8 GB pool-state limit of setup_pool).
+static const int POOL_TRIALS[] = {4096, 8192, 16384, 32768};
+constexpr int N_POOL_TRIALS = 4;
+
+// Pool of a round-based fit: the context's explicit setting, the tuned pool,
+// the tuner's next trial (large batches of an untuned class while tuning is
+// on), or 0 (automatic).  *trial: the fit is to be measured for the tuner.
+static int pick_pool(zola_ctx* ctx, const std::string& key, int n, bool* trial) {
+    *trial = false;
+    if (ctx->split_pool_max > 0) return ctx->split_pool_max;
+    auto it = ctx->pool_tunes.find(key);
+    if (it != ctx->pool_tunes.end() && it->second.done) return it->second.best;
+    if (!ctx->tune || n < 4 * POOL_TRIALS[N_POOL_TRIALS - 1]) return 0;
+    *trial = true;
+    return POOL_TRIALS[ctx->pool_tunes[key].trials];
+}
+
+static void pool_record(zola_ctx* ctx, const std::string& key, int pool, double ns_per_eval) {
+    PoolTune& t = ctx->pool_tunes[key];
+    if (t.trials == 0 || ns_per_eval < t.best_ns) {
+        t.best = pool;
+        t.best_ns = ns_per_eval;
+    }
+    if (++t.trials == N_POOL_TRIALS) {
+        t.done = true;
+        tune_save(ctx);
+    }
+}
+
+static std::string pool_key(const zola_psf* p, const WindowTables* w) { return tune_key(p, w) + "_pool"; }
 
 static int launch_fit_flow(zola_ctx* ctx, zola_psf* p, WindowTables* w, const FitIO& F, cudaStream_t st,
                            const RoiFeed* feed, const int* d_avail) {
@@ -3151,10 +3203,19 @@ int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d
     const FitIO F{d_rois, d_scmos, d_init, n, fp, d_out5, d_crlb5, d_nll, d_status, d_iters};
     if (ctx->split_mode == ZOLA_SPLIT_FLOW || d_avail) return launch_fit_flow(ctx, p, w, F, st, feed, d_avail);
     SplitPool sp;
-    int rc = setup_pool(ctx, p, w, n, ctx->split_pool_max, sp, st);
+    const std::string pkey = pool_key(p, w);
+    bool trial = false;
+    const int pool = pick_pool(ctx, pkey, n, &trial);
+    trial = trial && !feed && ctx->split_mode == ZOLA_SPLIT_STAGED;
+    int rc = setup_pool(ctx, p, w, n, pool, sp, st);
     if (rc) return rc;
     const SplitDev& D = sp.D;
     const int P = D.P;
+    if (trial) {
+        if (!ctx->tune_ev[0])
+            for (auto& e : ctx->tune_ev) ZOLA_CUDA_CHECK(cudaEventCreate(&e), ctx);
+        ZOLA_CUDA_CHECK(cudaEventRecord(ctx->tune_ev[0], st), ctx);
+    }
     // inputs still arriving: the fit starts on the first chunk, and chunks are
     // handed to the pool as their copies complete
     int chunk = 0, navail = n, queue = 0;
@@ -3234,7 +3295,24 @@ int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d
         }
         if (rounds > max_rounds) { ctx->err = "split fit: did not drain the ROI queue"; return ZOLA_E_TIMEOUT; }
     }
+    if (trial) {  // device time per model evaluation of this pool size
+        unsigned long long evals = 0;
+        float ms = 0;
+        ZOLA_CUDA_CHECK(cudaEventRecord(ctx->tune_ev[1], st), ctx);
+        ZOLA_CUDA_CHECK(cudaMemcpyAsync(&evals, D.evals, sizeof evals, cudaMemcpyDeviceToHost, st), ctx);
+        ZOLA_CUDA_CHECK(cudaEventSynchronize(ctx->tune_ev[1]), ctx);
+        ZOLA_CUDA_CHECK(cudaEventElapsedTime(&ms, ctx->tune_ev[0], ctx->tune_ev[1]), ctx);
+        if (evals > 0) pool_record(ctx, pkey, pool, ms * 1e6 / (double)evals);
+    }
     return ZOLA_OK;
+}
+
+int split_pool_choice(zola_psf* p, WindowTables* w, int* pool, double* ns_per_eval) {
+    const auto it = p->ctx->pool_tunes.find(pool_key(p, w));
+    const bool tuned = it != p->ctx->pool_tunes.end() && it->second.done;
+    if (pool) *pool = tuned ? it->second.best : p->ctx->split_pool_max;
+    if (ns_per_eval) *ns_per_eval = tuned ? it->second.best_ns : 0.0;
+    return tuned ? 1 : 0;
 }
 
 // ------------------------------------------------------- mixed batches -----
@@ -3250,9 +3328,12 @@ int launch_fit_split_mixed(zola_ctx* ctx, int nc, MixedClass* mc, cudaStream_t s
     }
     std::vector<SplitPool> sp(nc);
     std::vector<size_t> off(nc + 1, 0);
+    std::vector<int> pool(nc, 0);
     for (int c = 0; c < nc; ++c) {
         size_t need = 0;
-        int rc = setup_pool(ctx, mc[c].p, mc[c].w, mc[c].F.n, ctx->split_pool_max, sp[c], st, 0, nullptr, &need);
+        bool trial = false;
+        pool[c] = pick_pool(ctx, pool_key(mc[c].p, mc[c].w), 0, &trial);  // explicit, tuned or automatic
+        int rc = setup_pool(ctx, mc[c].p, mc[c].w, mc[c].F.n, pool[c], sp[c], st, 0, nullptr, &need);
         if (rc) return rc;
         off[c + 1] = off[c] + (need + 4095) / 4096 * 4096;
     }
@@ -3270,8 +3351,7 @@ int launch_fit_split_mixed(zola_ctx* ctx, int nc, MixedClass* mc, cudaStream_t s
         if (!ctx->mix_stream[c]) ZOLA_CUDA_CHECK(cudaStreamCreateWithFlags(&ctx->mix_stream[c], cudaStreamNonBlocking), ctx);
         cudaStream_t cs = ctx->mix_stream[c];
         ZOLA_CUDA_CHECK(cudaStreamWaitEvent(cs, ctx->mix_ev[ZOLA_MAX_CLASSES], 0), ctx);
-        int rc = setup_pool(ctx, mc[c].p, mc[c].w, mc[c].F.n, ctx->split_pool_max, sp[c], cs, 0,
-                            (char*)ctx->scratch + off[c]);
+        int rc = setup_pool(ctx, mc[c].p, mc[c].w, mc[c].F.n, pool[c], sp[c], cs, 0, (char*)ctx->scratch + off[c]);
         if (rc) return rc;
         const SplitDev& D = sp[c].D;
         k_init_slots<<<(D.P + 127) / 128, 128, 0, cs>>>(D, mc[c].F.init, mc[c].F.n, mc[c].F.n, mc[c].F.prm);

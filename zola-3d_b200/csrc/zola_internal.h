@@ -93,6 +93,14 @@ struct FlowTune {
     int trials = 0;
     bool done = false;
 };
+// Autotuning state of the round-based split fit of one class: the slot pool
+// size, tried from small to large, kept by device ns per model evaluation.
+struct PoolTune {
+    int best = 0;
+    double best_ns = 0;
+    int trials = 0;
+    bool done = false;
+};
 }  // namespace zola
 
 struct zola_ctx {
@@ -125,6 +133,7 @@ struct zola_ctx {
     int tune = 0;
     std::string tune_path;
     std::map<std::string, zola::FlowTune> tunes;
+    std::map<std::string, zola::PoolTune> pool_tunes;
     cudaEvent_t tune_ev[2] = {nullptr, nullptr};
     unsigned long long* h_tune = nullptr;  // pinned: evaluations, then (idle, total clocks, units) per CTA
     double flow_busy[5] = {};              // last dataflow launch: busy fraction per stage
@@ -219,6 +228,9 @@ struct MixedClass {
     FitIO F;
 };
 int launch_fit_split_mixed(zola_ctx* ctx, int nc, MixedClass* mc, cudaStream_t st);
+// The round-based split fit's pool for psf's R x R ROIs: 1 and the tuned pool
+// (and its ns per evaluation) when tuned, else 0 and the context's setting.
+int split_pool_choice(zola_psf* p, WindowTables* w, int* pool, double* ns_per_eval);
 int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_rois, const float* d_scmos,
                      const double* d_init, int n, const zola_fit_params* prm, double* d_out5, double* d_crlb5,
                      double* d_nll, int* d_status, int* d_iters, cudaStream_t st, const RoiFeed* feed = nullptr,
