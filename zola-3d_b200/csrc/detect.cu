@@ -524,12 +524,15 @@ int zola_detect_dev(zola_detector* d, const double* d_frames, int nframes, int c
         const double* fr = d_frames + (size_t)f0 * SS;
         prof_begin(ctx, 7, st);
         k_det_var<<<nf, 256, 0, st>>>(v, fr, rowsum, rowsq, var);
-        if (rt_smem(v.R, RZC) <= 112 * 1024) {  // two register-tiled CTAs per SM
+        // slices per register-tiled CTA: as many (up to RZC) as keep two CTAs per SM
+        int zrt = RZC;
+        while (zrt > 0 && rt_smem(v.R, zrt) > 112 * 1024) --zrt;
+        if (zrt > 0) {
             const int tiles = ((v.SX + RTI - 1) / RTI) * ((v.SY + RTJ - 1) / RTJ);
-            const size_t smem = rt_smem(v.R, RZC);
+            const size_t smem = rt_smem(v.R, zrt);
             cudaFuncSetAttribute(k_det_corr_rt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            dim3 grid(tiles, (v.Z + RZC - 1) / RZC, nf);
-            k_det_corr_rt<<<grid, 256, smem, st>>>(v, RZC, fr, var, score);
+            dim3 grid(tiles, (v.Z + zrt - 1) / zrt, nf);
+            k_det_corr_rt<<<grid, 256, smem, st>>>(v, zrt, fr, var, score);
         } else {
             const int tiles = ((v.SX + DT - 1) / DT) * ((v.SY + DT - 1) / DT);
             const size_t tile_b = (size_t)(DT + v.R) * (DT + v.R) * 8, slice_b = (size_t)v.R * v.R * 8;
