@@ -405,6 +405,11 @@ ZOLA_API int zola_ctx_set_tuning(zola_ctx* ctx, int enable, const char* cache_pa
  * and, when tuned, the measured ns per model evaluation (nullable pointers).
  * Returns 1 when tuned, 0 for the default shape, < 0 on error. */
 ZOLA_API int zola_fit_flow_shape(zola_psf* psf, int R, int* units, int* ctas, double* ns_per_eval);
+/* The round-based split fit issues its kernels in blocks of four LM rounds (20
+ * launches with the same arguments for the whole fit); enable = 1 (default)
+ * captures a block once per fit as a CUDA graph and replays it, 0 launches
+ * the kernels one by one.  Results are the same either way. */
+ZOLA_API int zola_ctx_set_round_graphs(zola_ctx* ctx, int enable);
 /* Slot pool of the round-based split fit (ZOLA_SPLIT_STAGED) for psf's R x R
  * ROIs.  With tuning on (zola_ctx_set_tuning) and no explicit pool
  * (zola_ctx_set_pool 0), the first four fits of a class with at least 131072

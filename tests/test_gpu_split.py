@@ -321,3 +321,27 @@ def test_mixed_batch_equals_per_class_calls(zpkg, ctx):
         assert np.array_equal(c["status"].cpu().numpy(), w["status"])
         assert np.array_equal(c["iters"].cpu().numpy(), w["iters"])
         c["psf"].close()
+
+
+def test_round_graphs_equal_direct_launches(zpkg, ctx):
+    """The round-based kernels replayed as a captured 4-round CUDA graph give the
+    fits of the same kernels launched one by one, bit for bit."""
+    import torch
+    dev = torch.device("cuda", 0)
+    psf = make(zpkg, ctx, 128, tetrapod_zernike())
+    rois, init, _ = _large_roi_job(psf, zpkg, 48, 600, seed=777)
+    prm = zpkg.PSF.fit_params(-1.5, 1.5, 48 * 0.11 / 2, max_iter=50, tol_xyz=1e-4, precision=zpkg.ZOLA_PREC_SPLIT)
+    d_rois, d_init = torch.tensor(rois, device=dev), torch.tensor(init, device=dev)
+    res = []
+    try:
+        for graphs in (True, False):
+            ctx.set_round_graphs(graphs)
+            out = torch.zeros((600, 5), dtype=torch.float64, device=dev)
+            st = torch.zeros(600, dtype=torch.int32, device=dev)
+            psf.fit_dev(d_rois, d_init, prm, out, None, None, st, None, stream=ctx.stream)
+            torch.cuda.synchronize()
+            res.append((out.cpu().numpy(), st.cpu().numpy()))
+    finally:
+        ctx.set_round_graphs(True)
+    assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])
+    psf.close()

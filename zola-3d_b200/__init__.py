@@ -81,7 +81,8 @@ EXPORTS = ["zola_ctx_create", "zola_ctx_destroy", "zola_last_error", "zola_ctx_s
            "zola_psf_center_search", "zola_calib_init", "zola_drift", "zola_fit_batch_scmos",
            "zola_fit_batch_scmos_dev", "zola_localize_frames_scmos", "zola_ctx_set_flow", "zola_ctx_set_wait_limit",
            "zola_fit_batch_stream_dev", "zola_ctx_set_tuning", "zola_fit_flow_shape", "zola_ctx_flow_stats",
-           "zola_fit_batch_mixed_dev", "zola_detect_u16", "zola_localize_frames_u16", "zola_fit_split_pool"]
+           "zola_fit_batch_mixed_dev", "zola_detect_u16", "zola_localize_frames_u16", "zola_fit_split_pool",
+           "zola_ctx_set_round_graphs"]
 STAGES = ["split_stage1_pupil_dft", "split_stage2_window_dft", "split_stage3_blur_rows",
           "split_stage4_blur_cols_sums_lm", "split_fused_stages2_5", "fp64_fit", "fp64_model", "other",
           "split_dataflow"]
@@ -120,6 +121,7 @@ def lib():
         L.zola_fit_flow_shape.argtypes = [vp, i, vp, vp, vp]
         L.zola_ctx_flow_stats.argtypes = [vp, vp, vp, vp]
         L.zola_fit_split_pool.argtypes = [vp, i, vp, vp]
+        L.zola_ctx_set_round_graphs.argtypes = [vp, i]
         L.zola_fit_batch_mixed_dev.argtypes = [vp, vp, i, vp]
         L.zola_crlb_curve.argtypes = [vp, i, vp, i, d, d, d, d, vp]
         L.zola_psf_center_search.argtypes = [vp, i, d, i, ctypes.POINTER(d)]
@@ -199,6 +201,10 @@ class Context:
         automatic; else five counts adding up to the SM count).  Results do not depend on either."""
         arr = None if ctas is None else (ctypes.c_int * 5)(*[int(c) for c in ctas])
         self.check(lib().zola_ctx_set_flow(self.h, int(units), arr), "zola_ctx_set_flow")
+
+    def set_round_graphs(self, enable=True):
+        """Replay the round-based split kernels' 4-round blocks as CUDA graphs (default) or launch them one by one."""
+        self.check(lib().zola_ctx_set_round_graphs(self.h, int(bool(enable))), "zola_ctx_set_round_graphs")
 
     def set_tuning(self, enable=True, cache_path=None):
         """Autotune the dataflow kernel's shape per (pupil grid, ROI side) on large fits; cache_path: JSON cache."""

@@ -342,6 +342,12 @@ int zola_fit_flow_shape(zola_psf* psf, int R, int* units, int* ctas, double* ns_
     return tuned ? 1 : 0;
 }
 
+int zola_ctx_set_round_graphs(zola_ctx* ctx, int enable) {
+    if (!ctx) return ZOLA_E_ARG;
+    ctx->round_graphs = enable != 0;
+    return ZOLA_OK;
+}
+
 int zola_fit_split_pool(zola_psf* psf, int R, int* pool, double* ns_per_eval) {
     if (!psf) return ZOLA_E_ARG;
     WindowTables* w = get_window(psf, R, psf->ctx->err);

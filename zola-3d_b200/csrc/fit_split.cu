@@ -3193,6 +3193,70 @@ bool flow_shape(zola_ctx* ctx, zola_psf* p, WindowTables* w, FlowShape* out, dou
     return tuned;
 }
 
+// One LM round of the round-based kernels: pupil DFT, window DFT, row blur,
+// column blur + sums, LM step.  Window 128: column blur and likelihood sums in
+// one persistent kernel, one slot at a time over all its threads (the maps
+// never leave the SM).  Smaller windows: the unit's maps go to shared memory
+// and its slots are summed together.  The two sum in different orders; the
+// choice depends on R alone so that a fit never depends on the batch it is in.
+static void issue_round(zola_ctx* ctx, const SplitPool& sp, const FitIO& F, cudaStream_t st) {
+    launch_stages123(ctx, sp, F, st);
+    prof_begin(ctx, 3, st);
+    if (sp.pl->W >= S45_MIN_W)
+        k_stage45p<<<unit_grid(ctx, sp), S45_THREADS, sp.s45, st>>>(sp.D, F);
+    else
+        k_stage45s<<<unit_grid(ctx, sp), S45S_THREADS, sp.s45, st>>>(sp.D, F);
+    prof_end(ctx, st);
+    prof_begin(ctx, 7, st);
+    k_lm<<<(sp.D.P + 127) / 128, 128, 0, st>>>(sp.D, F);
+    prof_end(ctx, st);
+    ctx->launches += 2;
+}
+
+// Four rounds: 20 launches whose arguments stay the same for the whole fit.
+static void issue_rounds(zola_ctx* ctx, const SplitPool& sp, const FitIO& F, cudaStream_t st) {
+    for (int k = 0; k < 4; ++k) issue_round(ctx, sp, F, st);
+}
+
+// The four rounds captured once per fit as a CUDA graph and replayed between
+// the host's flag reads: one launch instead of 20 per block.  Not with the
+// context's kernel profiling on (its events bracket single launches); if the
+// capture fails the rounds are issued directly.
+struct RoundGraph {
+    cudaGraphExec_t exec = nullptr;
+    RoundGraph() = default;
+    RoundGraph(const RoundGraph&) = delete;
+    RoundGraph& operator=(const RoundGraph&) = delete;
+    ~RoundGraph() { if (exec) cudaGraphExecDestroy(exec); }
+    void capture(zola_ctx* ctx, const SplitPool& sp, const FitIO& F, cudaStream_t st) {
+        if (ctx->profile || !ctx->round_graphs) return;
+        cudaGraph_t g = nullptr;
+        if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+        const long long l0 = ctx->launches;
+        issue_rounds(ctx, sp, F, st);
+        ctx->launches = l0;
+        if (cudaStreamEndCapture(st, &g) != cudaSuccess || !g) {
+            cudaGetLastError();
+            return;
+        }
+        if (cudaGraphInstantiate(&exec, g, 0) != cudaSuccess) {
+            exec = nullptr;
+            cudaGetLastError();
+        }
+        cudaGraphDestroy(g);
+    }
+    void run(zola_ctx* ctx, const SplitPool& sp, const FitIO& F, cudaStream_t st) {
+        if (exec && cudaGraphLaunch(exec, st) == cudaSuccess) {
+            ctx->launches += 20;
+            return;
+        }
+        issue_rounds(ctx, sp, F, st);
+    }
+};
+
 int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_rois, const float* d_scmos,
                      const double* d_init, int n,
                      const zola_fit_params* prm, double* d_out5, double* d_crlb5, double* d_nll, int* d_status,
@@ -3246,14 +3310,12 @@ int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d
     const int max_rounds = (prm->max_iter + 2) * ((n + P - 1) / P + 1) + 8 + 4 * (feed ? feed->n_chunks : 0);
     int rounds = 0;
     const bool fused = ctx->split_mode == ZOLA_SPLIT_FUSED && fused_fits(*sp.pl);
-    // Window 128: column blur and likelihood sums in one persistent kernel, one
-    // slot at a time over all its threads (the maps never leave the SM).  Smaller
-    // windows: the unit's maps go to shared memory and its slots are summed
-    // together.  The two sum in different orders; the choice depends on R alone
-    // so that a fit never depends on the batch it is in.
-    const bool big = sp.pl->W >= S45_MIN_W;
+    RoundGraph graph;
+    if (!fused && !feed) graph.capture(ctx, sp, F, st);
     while (true) {
-        for (int k = 0; k < 4; ++k) {
+        if (!fused && !feed) {
+            graph.run(ctx, sp, F, st);
+        } else for (int k = 0; k < 4; ++k) {
             if (feed && queue < n) {  // idle slots take ROIs that arrived since
                 k_refill<<<(P + 127) / 128, 128, 0, st>>>(D, d_init, n, fp);
                 ctx->launches++;
@@ -3269,17 +3331,7 @@ int launch_fit_split(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d
                 ctx->launches += 2;
                 continue;
             }
-            launch_stages123(ctx, sp, F, st);
-            prof_begin(ctx, 3, st);
-            if (big)
-                k_stage45p<<<unit_grid(ctx, sp), S45_THREADS, sp.s45, st>>>(D, F);
-            else
-                k_stage45s<<<unit_grid(ctx, sp), S45S_THREADS, sp.s45, st>>>(D, F);
-            prof_end(ctx, st);
-            prof_begin(ctx, 7, st);
-            k_lm<<<(P + 127) / 128, 128, 0, st>>>(D, F);
-            prof_end(ctx, st);
-            ctx->launches += 2;
+            issue_round(ctx, sp, F, st);
         }
         rounds += 4;
         ZOLA_CUDA_CHECK(cudaGetLastError(), ctx);
@@ -3347,6 +3399,7 @@ int launch_fit_split_mixed(zola_ctx* ctx, int nc, MixedClass* mc, cudaStream_t s
         bool done = false;
     };
     std::vector<State> S(nc);
+    RoundGraph graphs[ZOLA_MAX_CLASSES];
     for (int c = 0; c < nc; ++c) {
         if (!ctx->mix_stream[c]) ZOLA_CUDA_CHECK(cudaStreamCreateWithFlags(&ctx->mix_stream[c], cudaStreamNonBlocking), ctx);
         cudaStream_t cs = ctx->mix_stream[c];
@@ -3358,6 +3411,7 @@ int launch_fit_split_mixed(zola_ctx* ctx, int nc, MixedClass* mc, cudaStream_t s
         ctx->launches++;
         S[c].max_rounds = (mc[c].F.prm.max_iter + 2) * ((mc[c].F.n + D.P - 1) / D.P + 1) + 8;
         S[c].done = mc[c].F.n == 0;
+        if (!S[c].done) graphs[c].capture(ctx, sp[c], mc[c].F, cs);
     }
     ZOLA_CUDA_CHECK(cudaGetLastError(), ctx);
     for (;;) {
@@ -3367,17 +3421,7 @@ int launch_fit_split_mixed(zola_ctx* ctx, int nc, MixedClass* mc, cudaStream_t s
             any = true;
             cudaStream_t cs = ctx->mix_stream[c];
             const SplitPool& p = sp[c];
-            const FitIO& F = mc[c].F;
-            const bool big = p.pl->W >= S45_MIN_W;
-            for (int k = 0; k < 4; ++k) {
-                launch_stages123(ctx, p, F, cs);
-                if (big)
-                    k_stage45p<<<unit_grid(ctx, p), S45_THREADS, p.s45, cs>>>(p.D, F);
-                else
-                    k_stage45s<<<unit_grid(ctx, p), S45S_THREADS, p.s45, cs>>>(p.D, F);
-                k_lm<<<(p.D.P + 127) / 128, 128, 0, cs>>>(p.D, F);
-                ctx->launches += 2;
-            }
+            graphs[c].run(ctx, p, mc[c].F, cs);
             S[c].rounds += 4;
             ZOLA_CUDA_CHECK(cudaMemcpyAsync(ctx->h_mix + 4 * c, p.D.queue, 3 * sizeof(int), cudaMemcpyDeviceToHost, cs),
                             ctx);

@@ -122,6 +122,7 @@ struct zola_ctx {
     int* d_status_word = nullptr;
     int* h_flags = nullptr;      // pinned host words read back by the split fit loop
     int split_pool_max = 0;      // 0: size the split slot pool automatically
+    bool round_graphs = true;    // replay the round-based split kernels as CUDA graphs
     int split_mode = ZOLA_SPLIT_STAGED;  // ZOLA_SPLIT_STAGED, _FUSED or _FLOW
     int flow_units = 0;          // dataflow kernel: units of slots in flight (0: automatic)
     int flow_ctas[5] = {};       // dataflow kernel: CTAs per stage (all 0: automatic)
