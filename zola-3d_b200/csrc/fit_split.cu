@@ -2169,14 +2169,39 @@ __device__ __forceinline__ void stage45s_body(const SplitDev& P, const FitIO& F,
         umma::mbar_wait(&acc[b], (uint32_t)((n / NB) & 1), P.err);
         umma::fence_after_sync();
         ++n;
-        for (int g = 0; g < UG; ++g) {
-            if (P.slot_roi[unit * UG + g] < 0) continue;
-            float* dst = Tm + (size_t)(g * 4 + map) * RR;
-            for (int h = 0; h < RP; h += 4) {
-                float v[4];
-                umma::tmem_ld4(tmem_lane_addr(tbase, b * nc + g * NT + map * RP + h), v);
-                if (jp < R)
-                    for (int u = 0; u < 4 && h + u < R; ++u) dst[(h + u) * R + jp] = v[u] * P.sc.cT[map];
+        const float cT = P.sc.cT[map];
+        if (UG * RP == 64) {
+            // the whole unit's map columns of this lane (8 groups of 8) in flight before one wait
+            uint32_t ad[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int g = q / (RP / 8), h = (q - g * (RP / 8)) * 8;
+                ad[q] = tmem_lane_addr(tbase, b * nc + g * NT + map * RP + h);
+            }
+            float v[8][8];
+            tmem_ld8_multi<8>(ad, v);
+            if (jp < R)
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const int g = q / (RP / 8), h = (q - g * (RP / 8)) * 8;
+                    if (P.slot_roi[unit * UG + g] < 0) continue;
+                    float* dst = Tm + (size_t)(g * 4 + map) * RR;
+#pragma unroll
+                    for (int u = 0; u < 8; ++u)
+                        if (h + u < R) dst[(h + u) * R + jp] = v[q][u] * cT;
+                }
+        } else {
+            for (int g = 0; g < UG; ++g) {
+                if (P.slot_roi[unit * UG + g] < 0) continue;
+                float* dst = Tm + (size_t)(g * 4 + map) * RR;
+                for (int h = 0; h < RP; h += 16) {  // 16 columns a wait
+                    const uint32_t ad[2] = {tmem_lane_addr(tbase, b * nc + g * NT + map * RP + h),
+                                            tmem_lane_addr(tbase, b * nc + g * NT + map * RP + h + 8)};
+                    float v[2][8];
+                    tmem_ld8_multi<2>(ad, v);
+                    if (jp < R)
+                        for (int u = 0; u < 16 && h + u < R; ++u) dst[(h + u) * R + jp] = v[u >> 3][u & 7] * cT;
+                }
             }
         }
         umma::fence_before_sync();
