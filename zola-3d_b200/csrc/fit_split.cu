@@ -1494,17 +1494,38 @@ __device__ __forceinline__ double warp_sum(double x) {
 
 // Butterfly reduce-scatter of 32 per-lane values: after 31 shuffles lane k
 // holds the warp total of value k (the plain form needs 5 shuffles per value).
-__device__ __forceinline__ double warp_reduce_scatter32(double (&v)[32], int lane) {
+__device__ __forceinline__ float warp_reduce_scatter32f(float (&v)[32], int lane) {
 #pragma unroll
     for (int h = 16; h >= 1; h >>= 1) {
         const bool up = (lane & h) != 0;
 #pragma unroll
         for (int i = 0; i < h; ++i) {
-            const double send = up ? v[i] : v[i + h], keep = up ? v[i + h] : v[i];
+            const float send = up ? v[i] : v[i + h], keep = up ? v[i + h] : v[i];
             v[i] = keep + __shfl_xor_sync(0xffffffffu, send, h);
         }
     }
     return v[0];
+}
+
+// A warp's totals of the 36 per-thread likelihood sums into red[0..35]: the
+// likelihood and gradient (s6 - c6, the caller's compensated FP32 sums) in
+// FP64, the 30 Gauss-Newton Hessian and Fisher terms by the FP32 butterfly
+// (their relative rounding, about 2^-21, is far below what the LM step and
+// the CRLB need), so that no per-thread FP64 array is held.
+__device__ __forceinline__ void warp_sums36(const float (&s6)[6], const float (&c6)[6], const float (&sh)[30],
+                                            double* red, int lane) {
+    float w[32];
+#pragma unroll
+    for (int k = 0; k < 30; ++k) w[k] = sh[k];
+    w[30] = 0.f;
+    w[31] = 0.f;
+    const float hk = warp_reduce_scatter32f(w, lane);
+    if (lane < 30) red[6 + lane] = (double)hk;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const double x = warp_sum((double)s6[k] - (double)c6[k]);
+        if (lane == k) red[k] = x;
+    }
 }
 
 constexpr int NSUM = NRED + 1;  // sums per slot: NRED + the non-positive-model flag
@@ -1912,20 +1933,9 @@ __device__ __forceinline__ void stage45_body(const SplitDev& P, const FitIO& F, 
                     }
             }
             if (vec) warp_arrive(&rfree[b]);  // this slot's ROI buffer is free for the slot after next
-            // 36 sums per thread -> per warp: a butterfly reduce-scatter leaves sum k on lane k
-            // (k < 32); the last four reduce plainly
             {
-                double v[32];
-#pragma unroll
-                for (int k = 0; k < 6; ++k) v[k] = sg6[k];
-#pragma unroll
-                for (int k = 0; k < 26; ++k) v[6 + k] = sh[k];
-                red[warp][lane] = warp_reduce_scatter32(v, lane);
-#pragma unroll
-                for (int k = 26; k < 30; ++k) {
-                    const double x = warp_sum((double)sh[k]);
-                    if (lane == 0) red[warp][6 + k] = x;
-                }
+                const float zero6[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                warp_sums36(sg6, zero6, sh, red[warp], lane);
             }
             const bool wbad = __any_sync(0xffffffffu, bad);
             if (lane == 0) bad_w[warp] = wbad;
@@ -2029,21 +2039,7 @@ __device__ __noinline__ void unit_sums(const SplitDev& P, const FitIO& F, int un
                 }
         }
     }
-    // 36 sums per thread -> per warp: a butterfly reduce-scatter leaves sum k on lane k
-    // (k < 32); the last four reduce plainly
-    {
-        double v[32];
-#pragma unroll
-        for (int k = 0; k < 6; ++k) v[k] = (double)sg6[k] - (double)cg6[k];
-#pragma unroll
-        for (int k = 0; k < 26; ++k) v[6 + k] = sh[k];
-        red[warp][lane] = warp_reduce_scatter32(v, lane);
-#pragma unroll
-        for (int k = 26; k < 30; ++k) {
-            const double x = warp_sum((double)sh[k]);
-            if (lane == 0) red[warp][6 + k] = x;
-        }
-    }
+    warp_sums36(sg6, cg6, sh, red[warp], lane);
     const bool wbad = __any_sync(0xffffffffu, bad);
     if (lane == 0) badw[warp] = wbad;
     epi_bar();
@@ -2200,7 +2196,9 @@ __device__ __forceinline__ void stage45s_body(const SplitDev& P, const FitIO& F,
                     float v[2][8];
                     tmem_ld8_multi<2>(ad, v);
                     if (jp < R)
-                        for (int u = 0; u < 16 && h + u < R; ++u) dst[(h + u) * R + jp] = v[u >> 3][u & 7] * cT;
+#pragma unroll
+                        for (int u = 0; u < 16; ++u)
+                            if (h + u < R) dst[(h + u) * R + jp] = v[u >> 3][u & 7] * cT;
                 }
             }
         }
