@@ -207,17 +207,22 @@ __device__ inline void norm_sums(const F64Work& w, int R, bool derivs, double* r
     for (int k = 0; k < 4; ++k) s[k] = v[k];
 }
 
-// Writes psi (and dpsi) of n models; one CTA per model.
+// Writes psi (and dpsi) of n models; one CTA per model.  With a list, only
+// the models list[0 .. *n_dev) are evaluated (position list[m] of xyz, written
+// at the same index of out).
 __global__ void __launch_bounds__(F64_THREADS) model_f64_kernel(PsfView P, WinView Wn, const double* xyz, int n,
                                                                 double* out, double* dout, char* gscratch,
-                                                                size_t per_cta, int use_smem) {
+                                                                size_t per_cta, int use_smem, const int* list,
+                                                                const int* n_dev) {
     extern __shared__ __align__(256) char smem_raw[];
     double* red = (double*)smem_raw;
     char* base = use_smem ? smem_raw + 8192 : gscratch + (size_t)blockIdx.x * per_cta;
     F64Work w = f64_carve(base, P.D, Wn.W, Wn.R);
     const int R = Wn.R;
     const bool derivs = dout != nullptr;
-    for (int m = blockIdx.x; m < n; m += gridDim.x) {
+    const int nn = n_dev ? min(n, *n_dev) : n;
+    for (int mi = blockIdx.x; mi < nn; mi += gridDim.x) {
+        const int m = list ? list[mi] : mi;
         eval_maps_f64(P, Wn, w, xyz[3 * m], xyz[3 * m + 1], P.zfocus, xyz[3 * m + 2], derivs);
         double s[4];
         norm_sums(w, R, derivs, red, s);
@@ -353,7 +358,7 @@ static int f64_layout(zola_ctx* ctx, zola_psf* p, WindowTables* w, int nblocks, 
 }
 
 int launch_model_f64(zola_ctx* ctx, zola_psf* p, WindowTables* w, const double* d_xyz, int n, double* d_out,
-                     double* d_dout, cudaStream_t st) {
+                     double* d_dout, cudaStream_t st, const int* d_list, const int* d_count) {
     if (n <= 0) return ZOLA_OK;
     int nblocks = std::min(n, ctx->num_sms * 2);
     size_t per_cta, smem;
@@ -363,7 +368,7 @@ int launch_model_f64(zola_ctx* ctx, zola_psf* p, WindowTables* w, const double* 
     WinView wv{w->R, w->W, w->d_C, w->d_G};
     prof_begin(ctx, 6, st);
     model_f64_kernel<<<nblocks, F64_THREADS, smem, st>>>(p->view, wv, d_xyz, n, d_out, d_dout, (char*)ctx->scratch,
-                                                         per_cta, use_smem);
+                                                         per_cta, use_smem, d_list, d_count);
     prof_end(ctx, st);
     ctx->launches++;
     ZOLA_CUDA_CHECK(cudaGetLastError(), ctx);

@@ -188,11 +188,34 @@ __global__ void __launch_bounds__(128) k_pipe_wave(PipeView V, int K) {
     if (threadIdx.x == 0) V.limit[f] = limit;
 }
 
-// Model threshold of each fitted slot: 0.2 max(0, max(model - B)), model =
-// psi A + B (+ sCMOS v) (maxModelThreshold, LocalizationPipeline.java:860-880).
-__global__ void k_pipe_mthr(int n, int RR, const double* theta, const double* psi, const float* slot_v, double* mthr) {
+// The fitted slots that can be accepted whatever the mask: every test of the
+// walk's acceptance (k_pipe_replay) but the mask's, with the same arithmetic.
+// Only these need the model at their fit (the walk masks by the model only
+// where it accepts); they are listed in list[0 .. *count).
+__device__ __forceinline__ bool pipe_static_pass(const PipeView& V, const double* theta, const int* status, int slot,
+                                                 int ci, int cj) {
+    if (status[slot] == ZOLA_FIT_NAN) return false;
+    const double* th = theta + (size_t)slot * 5;
+    const double x = th[0], y = th[1], z = th[2], A = th[3];
+    if (!(A > V.photon_thr && fabs(x) < 10 * V.dx && fabs(y) < 10 * V.dx)) return false;
+    const int px = (int)(ci - x / V.dx), py = (int)(cj - y / V.dx);
+    return px >= 0 && px < V.SX && py >= 0 && py < V.SY && z > V.minZ && z < V.maxZ;
+}
+
+__global__ void k_pipe_need(PipeView V, int n, const double* theta, const int* status, int* list, int* count) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
+    const double* row = V.cand + ((size_t)V.slot_frame[s] * V.cap + V.slot_cand[s]) * 7;
+    if (pipe_static_pass(V, theta, status, s, (int)llrint(row[2]), (int)llrint(row[3]))) list[atomicAdd(count, 1)] = s;
+}
+
+// Model threshold of each listed slot: 0.2 max(0, max(model - B)), model =
+// psi A + B (+ sCMOS v) (maxModelThreshold, LocalizationPipeline.java:860-880).
+__global__ void k_pipe_mthr(int n, int RR, const double* theta, const double* psi, const float* slot_v, double* mthr,
+                            const int* list, const int* count) {
+    const int li = blockIdx.x * blockDim.x + threadIdx.x;
+    if (li >= min(n, *count)) return;
+    const int s = list[li];
     const double A = theta[5 * s + 3], B = theta[5 * s + 4];
     const double* ps = psi + (size_t)s * RR;
     const float* sv = slot_v ? slot_v + (size_t)s * RR : nullptr;
@@ -224,14 +247,10 @@ __global__ void __launch_bounds__(256) k_pipe_replay(PipeView V, const double* t
         if (__syncthreads_or(mine)) continue;  // alreadyTreated
         const double maxp = V.cand_maxp[(size_t)f * V.cap + i];
         bool accepted = false;
-        if (slot >= 0 && status[slot] != ZOLA_FIT_NAN) {
+        if (slot >= 0 && pipe_static_pass(V, theta, status, slot, ci, cj)) {
             const double* th = theta + (size_t)slot * 5;
-            const double x = th[0], y = th[1], z = th[2], A = th[3];
-            if (A > V.photon_thr && fabs(x) < 10 * V.dx && fabs(y) < 10 * V.dx) {
-                const int px = (int)(ci - x / V.dx), py = (int)(cj - y / V.dx);
-                accepted = px >= 0 && px < SX && py >= 0 && py < SY && !mk[(size_t)px * SY + py] && z > V.minZ &&
-                           z < V.maxZ;
-            }
+            const int px = (int)(ci - th[0] / V.dx), py = (int)(cj - th[1] / V.dx);
+            accepted = !mk[(size_t)px * SY + py];
         }
         __syncthreads();  // every thread has read the mask before it changes
         if (accepted) {
@@ -393,7 +412,7 @@ int localize_impl(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const do
     const int slot_cap = FB * K;
     Buf b_img, b_mask, b_cand, b_cnt, b_lib, b_rng, b_cslot, b_cmax, b_ptr, b_lim, b_done, b_ns, b_rois, b_init, b_sf,
         b_sc, b_out5, b_st, b_xyz, b_psi, b_mthr, b_acc, b_seq, b_nacc, b_dpsi, b_rows, b_fimg, b_adu, b_off, b_gain,
-        b_vg, b_sv, b_u16;
+        b_vg, b_sv, b_u16, b_list, b_nlist;
     cudaError_t e = cudaSuccess;
     auto A = [&](Buf& b, size_t bytes) { if (e == cudaSuccess) e = b.alloc(bytes); };
     A(b_img, SS * FB * 8); A(b_mask, SS * FB); A(b_cand, (size_t)FB * cap * 7 * 8); A(b_cnt, (size_t)FB * 4);
@@ -405,6 +424,7 @@ int localize_impl(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const do
     A(b_xyz, (size_t)slot_cap * 24); A(b_psi, RR * slot_cap * 8); A(b_mthr, (size_t)slot_cap * 8);
     A(b_acc, (size_t)slot_cap * 4); A(b_seq, (size_t)slot_cap * 4);
     if (u16) A(b_u16, SS * FB * 2);
+    A(b_list, (size_t)slot_cap * 4); A(b_nlist, 64);
     if (scmos) {
         A(b_fimg, SS * FB * 8); A(b_adu, SS * FB * 4); A(b_off, SS * 8); A(b_gain, SS * 8); A(b_vg, SS * 8);
         A(b_sv, RR * slot_cap * 4);
@@ -496,13 +516,21 @@ int localize_impl(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const do
                            : zola_fit_batch_dev(ctx, fit_psf, R, (float*)b_rois.p, (double*)b_init.p, nslot, &fp,
                                                 (double*)b_out5.p, nullptr, nullptr, (int*)b_st.p, nullptr, st);
                 if (rc) return rc;
-                // psi at every fitted position (mask updates of the walk)
+                // psi at the fitted positions the walk may accept (its model masks)
                 k_take_xyz<<<(nslot + 127) / 128, 128, 0, st>>>(nslot, (double*)b_out5.p, (double*)b_xyz.p);
-                ctx->launches++;
-                rc = zola_psf_model_dev(fit_psf, R, (double*)b_xyz.p, nslot, (double*)b_psi.p, nullptr, st);
+                e = cudaMemsetAsync(b_nlist.p, 0, 4, st);
+                if (e != cudaSuccess) return fail(e);
+                k_pipe_need<<<(nslot + 127) / 128, 128, 0, st>>>(V, nslot, (double*)b_out5.p, (int*)b_st.p,
+                                                                 (int*)b_list.p, (int*)b_nlist.p);
+                ctx->launches += 2;
+                WindowTables* wt = get_window(fit_psf, R, ctx->err);
+                if (!wt) return ZOLA_E_ARG;
+                rc = launch_model_f64(ctx, fit_psf, wt, (double*)b_xyz.p, nslot, (double*)b_psi.p, nullptr, st,
+                                      (const int*)b_list.p, (const int*)b_nlist.p);
                 if (rc) return rc;
                 k_pipe_mthr<<<(nslot + 127) / 128, 128, 0, st>>>(nslot, (int)RR, (double*)b_out5.p,
-                                                                 (double*)b_psi.p, V.slot_v, (double*)b_mthr.p);
+                                                                 (double*)b_psi.p, V.slot_v, (double*)b_mthr.p,
+                                                                 (const int*)b_list.p, (const int*)b_nlist.p);
                 ctx->launches++;
             }
             k_pipe_replay<<<nf, 256, 0, st>>>(V, (double*)b_out5.p, (int*)b_st.p, (double*)b_psi.p,

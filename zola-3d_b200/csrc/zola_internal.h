@@ -202,8 +202,10 @@ WindowTables* get_window(zola_psf* p, int R, std::string& err);
 void blur_matrix(int R, int W, double sigma, std::vector<double>& G, std::vector<double>* dG);
 
 // fit_f64.cu
+// d_list / d_count (nullable): evaluate only the models d_list[0 .. *d_count) (at most n).
 int launch_model_f64(zola_ctx* ctx, zola_psf* p, WindowTables* w, const double* d_xyz, int n,
-                     double* d_out, double* d_dout, cudaStream_t st);
+                     double* d_out, double* d_dout, cudaStream_t st, const int* d_list = nullptr,
+                     const int* d_count = nullptr);
 int launch_fit_f64(zola_ctx* ctx, zola_psf* p, WindowTables* w, const float* d_rois, const float* d_scmos,
                    const double* d_init, int n, const zola_fit_params* prm, double* d_out5, double* d_crlb5,
                    double* d_nll, int* d_status, int* d_iters, cudaStream_t st);
