@@ -141,11 +141,48 @@ def make_job(z, ctx, torch, n, seed, device, only=None):
     return job
 
 
-def detect_fit_config(z, ctx, nframes, seed=1, precision=None):
-    """Frames of 256^2 px with Poisson(5) tetrapod emitters (45 modes, pupil 128^2,
-    z in +-2 um, A ~ LogNormal(ln 4000, 0.5), B = 30), detected against a 41-slice
-    library (0.1 um) with 40 x 40 ROIs and fitted through the frame pipeline.
-    Returns the frames/s of zola_localize_frames (host frames in, rows out)."""
+def render_frames(z, torch, device, psf, emit, nframes, S, P=64, bg=30.0, offset=0.0, seed=1, batch=200):
+    """uint16 camera frames (n, S, S): background + emitters (rows frame, x px,
+    y px, z um, photons; the FP64 device model on a P x P patch) with Poisson
+    noise, plus a camera offset, rendered on the device in batches of frames."""
+    cx, cy = emit[:, 1], emit[:, 2]
+    ix, iy = cx.astype(int), cy.astype(int)
+    frames = np.empty((nframes, S, S), dtype=np.uint16)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    a = torch.arange(P, device=device) - P // 2
+    for f0 in range(0, nframes, batch):
+        f1 = min(nframes, f0 + batch)
+        sel = np.nonzero((emit[:, 0] >= f0) & (emit[:, 0] < f1))[0]
+        img = torch.full(((f1 - f0) * S * S,), bg, dtype=torch.float64, device=device)
+        if len(sel):
+            # a positive model x moves the PSF towards lower pixel indices
+            xyz = torch.tensor(np.c_[(ix[sel] - cx[sel]) * DX, (iy[sel] - cy[sel]) * DX, emit[sel, 3]],
+                               dtype=torch.float64, device=device)
+            psi = torch.empty((len(sel), P, P), dtype=torch.float64, device=device)
+            psf.model_dev(P, xyz, psi, stream=torch.cuda.current_stream().cuda_stream)
+            torch.cuda.synchronize()
+            fr = torch.tensor(emit[sel, 0] - f0, dtype=torch.int64, device=device)
+            ii = torch.tensor(ix[sel], device=device)[:, None, None] + a[None, :, None]
+            jj = torch.tensor(iy[sel], device=device)[:, None, None] + a[None, None, :]
+            ok = (ii >= 0) & (ii < S) & (jj >= 0) & (jj < S)
+            flat = fr[:, None, None] * S * S + ii.clamp(0, S - 1) * S + jj.clamp(0, S - 1)
+            amp = torch.tensor(emit[sel, 4], dtype=torch.float64, device=device)[:, None, None]
+            img.index_put_((flat[ok],), (amp * psi)[ok], accumulate=True)
+        cnt = torch.poisson(img, generator=gen) + offset
+        frames[f0:f1] = cnt.clamp(max=65535).to(torch.int32).cpu().numpy().reshape(f1 - f0, S, S).astype(np.uint16)
+    return frames
+
+
+def detect_fit_config(z, ctx, torch, device, nframes, fp64_frames=0, seed=1):
+    """Full-frame detect + fit: 256^2 uint16 frames of photon counts with
+    Poisson(5) tetrapod emitters (45 modes, pupil 128^2, z in +-2 um,
+    A ~ LogNormal(ln 4000, 0.5), B = 30), detected against a 41-slice library
+    (0.1 um) with 40 x 40 ROIs and fitted through the frame pipeline
+    (zola_localize_frames_u16: host frames in, localization rows out).  The
+    split-precision arm runs nframes frames, the plain FP64 arm the first
+    fp64_frames of them; the rows of the two arms are joined on (frame,
+    candidate index)."""
     S, R, N = 256, 40, 128
     rng = np.random.default_rng(seed)
     zern = zern_tetrapod(np.random.default_rng(seed * 100 + 7))
@@ -153,37 +190,52 @@ def detect_fit_config(z, ctx, nframes, seed=1, precision=None):
     psf_det = z.PSF(ctx, z.optics(kz_reset=True, **base), zern)
     psf_fit = z.PSF(ctx, z.optics(**base), zern)
     P = 64  # rendering patch
-    emit = []
-    for f in range(nframes):
-        for _ in range(rng.poisson(5)):
-            cx, cy = rng.uniform(P / 2, S - P / 2, 2)
-            emit.append((f, cx, cy, rng.uniform(-2.0, 2.0), rng.lognormal(np.log(4000.0), 0.5)))
-    emit = np.array(emit)
-    ix, iy = emit[:, 1].astype(int), emit[:, 2].astype(int)
-    # a positive model x moves the PSF towards lower pixel indices
-    xyz = np.c_[(ix - emit[:, 1]) * DX, (iy - emit[:, 2]) * DX, emit[:, 3]]
-    psi = psf_fit.model(P, xyz)
-    img = np.full((nframes, S, S), 30.0)
-    for k in range(len(emit)):
-        f = int(emit[k, 0])
-        img[f, ix[k] - P // 2:ix[k] + P // 2, iy[k] - P // 2:iy[k] + P // 2] += emit[k, 4] * psi[k]
-    frames = rng.poisson(img).astype(np.float64)
+    k = rng.poisson(5, nframes)
+    fr = np.repeat(np.arange(nframes), k)
+    m = len(fr)
+    emit = np.c_[fr, rng.uniform(P / 2, S - P / 2, (m, 2)), rng.uniform(-2.0, 2.0, m),
+                 rng.lognormal(np.log(4000.0), 0.5, m)]
+    frames = render_frames(z, torch, device, psf_fit, emit, nframes, S, P, seed=seed)
     det = z.Detector(psf_det, S, S, R, -2.0, 2.0, 0.1, 0.1)
-    prec = z.ZOLA_PREC_SPLIT if precision is None else precision
-    kw = dict(photon_threshold=500.0, precision=prec, max_iter=50, tol_xyz=1e-4)
-    z.localize_frames(ctx, det, psf_fit, frames, -2.0, 2.0, **kw)  # warm-up: tables, plans, scratch sizes
-    t0 = time.perf_counter()
-    rows = z.localize_frames(ctx, det, psf_fit, frames, -2.0, 2.0, **kw)
-    dt = time.perf_counter() - t0
-    nz = det.nz
+    out = {"workload": "256x256 uint16 frames, Poisson(5) tetrapod emitters, R = 40, 0.1 um library over +-2 um; "
+                       "host frames in and localization rows out",
+           "frames": nframes, "emitters": int(m), "library_slices": det.nz,
+           "detect_fp64_flops_per_frame": 2.0 * S * S * R * R * det.nz, "h2d_bytes_per_frame": S * S * 2}
+    rows = {}
+    for name, prec, nf in (("split", z.ZOLA_PREC_SPLIT, nframes), ("fp64", z.ZOLA_PREC_FP64, fp64_frames)):
+        if nf <= 0:
+            continue
+        kw = dict(photon_threshold=500.0, precision=prec, max_iter=50, tol_xyz=1e-4)
+        z.localize_frames_u16(ctx, det, psf_fit, frames[:min(nf, 64)], -2.0, 2.0, **kw)  # tables, plans, scratch
+        t0 = time.perf_counter()
+        r = z.localize_frames_u16(ctx, det, psf_fit, frames[:nf], -2.0, 2.0, **kw)
+        dt = time.perf_counter() - t0
+        rows[name] = r
+        out[name] = {"frames": nf, "seconds": dt, "frames_per_s": nf / dt, "localizations": int(len(r)),
+                     "localizations_per_s": len(r) / dt}
+    if "fp64" in rows:
+        a, b = rows["fp64"], rows["split"]
+        b = b[b["frame"] < fp64_frames]
+        ka = {(int(f), int(c)): i for i, (f, c) in enumerate(zip(a["frame"], a["candidate"]))}
+        kb = {(int(f), int(c)): i for i, (f, c) in enumerate(zip(b["frame"], b["candidate"]))}
+        both = sorted(set(ka) & set(kb))
+        ia, ib = [ka[q] for q in both], [kb[q] for q in both]
+        conv = (a["fit_status"][ia] == 1) & (b["fit_status"][ib] == 1)
+        dxy = np.maximum(np.abs(a["x_nm"][ia] - b["x_nm"][ib]), np.abs(a["y_nm"][ia] - b["y_nm"][ib]))
+        dz = np.abs(a["z_nm"][ia] - b["z_nm"][ib])
+        da = np.abs(a["intensity"][ia] - b["intensity"][ib]) / np.abs(a["intensity"][ia])
+        out["split_vs_fp64_rows"] = {
+            "fp64_rows": int(len(a)), "split_rows": int(len(b)), "same_candidate": len(both),
+            "both_converged": int(conv.sum()),
+            "converged_within_tolerance": float(((dxy <= 0.5) & (dz <= 1.0) & (da <= 1e-3))[conv].mean())
+            if conv.any() else None,
+            "converged_max_dxy_nm": float(dxy[conv].max()) if conv.any() else None,
+            "converged_max_dz_nm": float(dz[conv].max()) if conv.any() else None}
+        out["split_vs_fp64_speedup"] = out["split"]["frames_per_s"] / out["fp64"]["frames_per_s"]
     det.close()
     psf_det.close()
     psf_fit.close()
-    return {"frames": nframes, "seconds": dt, "frames_per_s": nframes / dt, "emitters": int(len(emit)),
-            "localizations": int(len(rows)), "library_slices": nz,
-            "detect_fp64_flops_per_frame": 2.0 * S * S * R * R * nz,
-            "workload": "256x256 frames, Poisson(5) tetrapod emitters, R = 40, 0.1 um library over +-2 um, "
-                        "split-precision fits, host frames in and localization rows out"}
+    return out
 
 
 def calibration_config(z, ctx, seed=3, fit_iters=10):
@@ -338,32 +390,8 @@ def stream_drift_config(z, ctx, torch, device, nframes, seed=4):
         for q in pts:
             emit.append((f, *(q + walk[f]), rng.lognormal(np.log(4000.0), 0.5)))
     emit = np.array(emit)
-    cx, cy = emit[:, 1] / DX, emit[:, 2] / DX
-    ix, iy = cx.astype(int), cy.astype(int)
-    frames = np.empty((nframes, S, S), dtype=np.uint16)
-    gen = torch.Generator(device=device)
-    gen.manual_seed(seed)
-    fb = 200
-    for f0 in range(0, nframes, fb):
-        f1 = min(nframes, f0 + fb)
-        sel = np.nonzero((emit[:, 0] >= f0) & (emit[:, 0] < f1))[0]
-        img = torch.full(((f1 - f0) * S * S,), 30.0, dtype=torch.float64, device=device)
-        if len(sel):
-            xyz = torch.tensor(np.c_[(ix[sel] - cx[sel]) * DX, (iy[sel] - cy[sel]) * DX, emit[sel, 3]],
-                               dtype=torch.float64, device=device)
-            psi = torch.empty((len(sel), P, P), dtype=torch.float64, device=device)
-            psf_fit.model_dev(P, xyz, psi, stream=torch.cuda.current_stream().cuda_stream)
-            torch.cuda.synchronize()
-            a = torch.arange(P, device=device) - P // 2
-            fr = torch.tensor(emit[sel, 0] - f0, dtype=torch.int64, device=device)
-            ii = torch.tensor(ix[sel], device=device)[:, None, None] + a[None, :, None]
-            jj = torch.tensor(iy[sel], device=device)[:, None, None] + a[None, None, :]
-            ok = (ii >= 0) & (ii < S) & (jj >= 0) & (jj < S)
-            flat = (fr[:, None, None] * S * S + ii.clamp(0, S - 1) * S + jj.clamp(0, S - 1))
-            amp = torch.tensor(emit[sel, 4], dtype=torch.float64, device=device)[:, None, None]
-            img.index_put_((flat[ok],), (amp * psi)[ok], accumulate=True)
-        cnt = torch.poisson(img, generator=gen) + 100.0
-        frames[f0:f1] = cnt.clamp(max=65535).to(torch.int32).cpu().numpy().reshape(f1 - f0, S, S).astype(np.uint16)
+    emit[:, 1:3] /= DX  # um -> px
+    frames = render_frames(z, torch, device, psf_fit, emit, nframes, S, P, offset=100.0, seed=seed)
     det = z.Detector(psf_det, S, S, R, -2.0, 2.0, 0.1, 0.1)
     kw = dict(adu=1.0, gain=1.0, offset=100.0, photon_threshold=500.0, precision=z.ZOLA_PREC_SPLIT, max_iter=50,
               tol_xyz=1e-4)
@@ -572,6 +600,8 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuning pass (slot pool per class, or the dataflow kernel shape)")
     ap.add_argument("--no-calibration", dest="calibration", action="store_false",
                     help="skip the Zernike calibration measurement")
+    ap.add_argument("--detect-fp64-frames", type=int, default=50,
+                    help="frames of the detect -> fit pipeline's plain FP64 arm (0: skip)")
     ap.add_argument("--stream-frames", type=int, default=0,
                     help="frames of the 512x512 uint16 stream + drift measurement (0: skip)")
     ap.add_argument("--no-small-rois", dest="small_rois", action="store_false",
@@ -852,7 +882,8 @@ def main():
     e2e = {"value": n_total * world / t_e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h)}
 
-    detect = detect_fit_config(z, ctx, args.detect_frames, seed=1 + rank) if args.detect_frames > 0 else None
+    detect = detect_fit_config(z, ctx, torch, device, args.detect_frames, args.detect_fp64_frames, seed=1 + rank) \
+        if args.detect_frames > 0 else None
     calib = calibration_config(z, ctx) if args.calibration and rank == 0 else None
     small = small_roi_config(z, ctx) if args.small_rois and rank == 0 else None
     stream = stream_drift_config(z, ctx, torch, device, args.stream_frames) if args.stream_frames > 0 and rank == 0 \
