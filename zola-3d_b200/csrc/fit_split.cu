@@ -1294,6 +1294,11 @@ __global__ void __launch_bounds__(S2_THREADS, 1) k_stage2p(SplitDev P, FitIO F) 
 // MMAs overlap this tile's epilogue (warps 0-15), which writes the row-blurred
 // maps as the column-blur B operand (hi, lo; N = 4 RP rows (map, i'), K = j).
 constexpr int S3_THREADS = SPLIT_THREADS + 32;
+// Window tiles of the row blur in shared memory: two (a loader lane fills one
+// while the MMAs read the other) for windows up to 64 in the round-based
+// kernel, one otherwise (160 KB at W = 128; the dataflow kernel's stage CTAs
+// keep the smaller plan).
+__host__ __device__ constexpr int s3_nbuf(int W, bool flow) { return !flow && W <= 64 ? 2 : 1; }
 
 template <class UNITS>
 __device__ __forceinline__ void stage3_body(const SplitDev& P, const FitIO& F, UNITS units) {
@@ -1301,15 +1306,17 @@ __device__ __forceinline__ void stage3_body(const SplitDev& P, const FitIO& F, U
     const int W = P.W, RP = P.RP, G2 = P.G2, t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int T2 = unit_slots(P.G1, G2) / G2;
     const size_t arr3 = (size_t)128 * W * 2, gbytes = (size_t)RP * W * 2;
-    char* A3 = smem;            // one window tile: I hi, I lo, I_x, I_y, I_z
-    char* GT = A3 + 5 * arr3;   // G^T hi, lo
-    __shared__ __align__(8) uint64_t gfull, full, acc[2], tfree[2], fin;
+    const int NB3 = s3_nbuf(W, UNITS::flow);
+    char* A3 = smem;                  // NB3 window tiles: I hi, I lo, I_x, I_y, I_z
+    char* GT = A3 + NB3 * 5 * arr3;   // G^T hi, lo
+    __shared__ __align__(8) uint64_t gfull, full[2], acc[2], tfree[2], fin;
     __shared__ uint32_t tmem_base;
     const int nc = tmem_cols_pow2(4 * RP);  // one accumulator
     if (t < 32) umma::tmem_alloc(&tmem_base, 2 * nc);
     if (t == 0) {
         umma::mbar_init(&gfull, 1);
-        umma::mbar_init(&full, 1);
+        umma::mbar_init(&full[0], 1);
+        umma::mbar_init(&full[1], 1);
         for (int b = 0; b < 2; ++b) {
             umma::mbar_init(&acc[b], 1);
             umma::mbar_init(&tfree[b], SPLIT_THREADS / 32);
@@ -1321,12 +1328,38 @@ __device__ __forceinline__ void stage3_body(const SplitDev& P, const FitIO& F, U
     umma::fence_after_sync();
     const uint32_t tbase = tmem_base;
 
-    if (warp == SPLIT_THREADS / 32) {  // ---------------- loads + MMAs (lane 0), scheduler (lane 1)
+    if (warp == SPLIT_THREADS / 32) {  // ------- MMAs (lane 0), scheduler (lane 1) or A3 loader (lane 1, two buffers)
         if constexpr (UNITS::flow)
             if (lane == 1) {
                 units.schedule(P, F);
                 return;
             }
+        if (NB3 == 2 && lane == 1) {
+            // the loader: tile n goes to buffer n & 1 once the MMAs of tile n - 2 (the
+            // buffer's last reader) have completed; the MMA lane walks the same tiles
+            int n = 0;
+            for (int tag = 0;;) {
+                const int unit = units.next(P, tag, true);
+                if (unit < 0) break;
+                bool ok = true;
+                for (int k = 0; k < T2; ++k) {
+                    const int tile = unit * T2 + k;
+                    if (!tile_live(P, tile * G2, G2)) continue;
+                    const int b = n & 1;
+                    if (n >= 2 && !umma::mbar_wait(&acc[b], (uint32_t)(((n >> 1) - 1) & 1), P.err)) { ok = false; break; }
+                    umma::mbar_expect_tx(&full[b], (uint32_t)(5 * arr3));
+                    const char* src = P.a3 + (size_t)tile * a3_tile_bytes(W);
+                    char* dst = A3 + (size_t)b * 5 * arr3;
+                    for (int q = 0; q < 5; ++q) umma::bulk_g2s(dst + q * arr3, src + q * arr3, (uint32_t)arr3, &full[b]);
+                    ++n;
+                }
+                if (!ok) break;
+            }
+            // (normally the MMA lane has waited for every copy; after a wait that gave up,
+            // the copies still in flight land before the CTA leaves)
+            for (int q = n - 2 < 0 ? 0 : n - 2; q < n; ++q) umma::mbar_wait(&full[q & 1], (uint32_t)((q >> 1) & 1), P.err);
+            return;
+        }
         if (lane != 0) return;
         umma::mbar_expect_tx(&gfull, (uint32_t)(2 * gbytes));
         umma::bulk_g2s(GT, P.gt_hi, (uint32_t)gbytes, &gfull);
@@ -1334,7 +1367,7 @@ __device__ __forceinline__ void stage3_body(const SplitDev& P, const FitIO& F, U
         bool ok = umma::mbar_wait(&gfull, 0, P.err);
         const uint32_t sbo = (W / 8) * 128;
         const uint32_t id = umma::idesc_f16(128, RP, false, false);
-        const uint32_t a0 = umma::smem_u32(A3), ghi = umma::smem_u32(GT), glo = ghi + (uint32_t)gbytes;
+        const uint32_t ghi = umma::smem_u32(GT), glo = ghi + (uint32_t)gbytes;
         int n = 0;
         for (int tag = 0; ok;) {
             const int unit = units.next(P, tag, true);
@@ -1343,14 +1376,21 @@ __device__ __forceinline__ void stage3_body(const SplitDev& P, const FitIO& F, U
                 const int tile = unit * T2 + k;
                 if (!tile_live(P, tile * G2, G2)) continue;
                 const int b = n & 1;
-                // the A3 buffer is free once the previous tile's MMAs have completed, and
-                // accumulator b once the epilogue has read tile n - 2 out of it
-                if (n >= 1 && !umma::mbar_wait(&acc[(n - 1) & 1], (uint32_t)(((n - 1) >> 1) & 1), P.err)) { ok = false; break; }
+                // accumulator b is free once the epilogue has read tile n - 2 out of it
                 if (n >= 2 && !umma::mbar_wait(&tfree[b], (uint32_t)(((n >> 1) - 1) & 1), P.err)) { ok = false; break; }
-                umma::mbar_expect_tx(&full, (uint32_t)(5 * arr3));
-                const char* src = P.a3 + (size_t)tile * a3_tile_bytes(W);
-                for (int q = 0; q < 5; ++q) umma::bulk_g2s(A3 + q * arr3, src + q * arr3, (uint32_t)arr3, &full);
-                if (!umma::mbar_wait(&full, (uint32_t)(n & 1), P.err)) { ok = false; break; }
+                uint32_t a0;
+                if (NB3 == 2) {  // the loader filled buffer b
+                    if (!umma::mbar_wait(&full[b], (uint32_t)((n >> 1) & 1), P.err)) { ok = false; break; }
+                    a0 = umma::smem_u32(A3 + (size_t)b * 5 * arr3);
+                } else {
+                    // the one A3 buffer is free once the previous tile's MMAs have completed
+                    if (n >= 1 && !umma::mbar_wait(&acc[(n - 1) & 1], (uint32_t)(((n - 1) >> 1) & 1), P.err)) { ok = false; break; }
+                    umma::mbar_expect_tx(&full[0], (uint32_t)(5 * arr3));
+                    const char* src = P.a3 + (size_t)tile * a3_tile_bytes(W);
+                    for (int q = 0; q < 5; ++q) umma::bulk_g2s(A3 + q * arr3, src + q * arr3, (uint32_t)arr3, &full[0]);
+                    if (!umma::mbar_wait(&full[0], (uint32_t)(n & 1), P.err)) { ok = false; break; }
+                    a0 = umma::smem_u32(A3);
+                }
                 umma::fence_after_sync();
                 const uint32_t td = tbase + (uint32_t)(b * nc);
                 mma_chain(td, a0, 128, sbo, 256, ghi, 128, sbo, 256, W, id, false);
@@ -2654,7 +2694,9 @@ static size_t smem_stage1p(const SplitPlanHost& pl) {
 static size_t smem_stage2p(const SplitPlanHost& pl) {
     return (size_t)(pl.K1 / 16) * s2_slab_bytes(pl.W) + (size_t)S2_NBUF * s2_ring_bytes(pl.W);
 }
-static size_t smem_stage3(const SplitPlanHost& pl) { return (size_t)5 * 128 * pl.W * 2 + (size_t)4 * pl.RP * pl.W; }
+static size_t smem_stage3(const SplitPlanHost& pl, bool flow = false) {
+    return (size_t)s3_nbuf(pl.W, flow) * 5 * 128 * pl.W * 2 + (size_t)4 * pl.RP * pl.W;
+}
 static size_t smem_stage4(const SplitPlanHost& pl) { return a4_slot_bytes(pl.W, pl.RP) + (size_t)2 * 128 * pl.W * 2; }
 static size_t smem_stage45(const SplitPlanHost& pl) {
     return (size_t)2 * 128 * pl.W * 2 + (size_t)S45_NBUF * 2 * 32 * 4 * pl.RP + 4 * s45_roi_bytes(pl.R) +
@@ -2800,7 +2842,7 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
     sp.s3 = smem_stage3(*pl);
     sp.s4 = smem_stage4(*pl);
     sp.s45 = pl->W >= S45_MIN_W ? smem_stage45(*pl) : smem_stage45s(*pl);
-    sp.sflow = max_units > 0 ? std::max(std::max(sp.s1, sp.s2), std::max(sp.s3, sp.s45)) : 0;
+    sp.sflow = max_units > 0 ? std::max(std::max(sp.s1, sp.s2), std::max(smem_stage3(*pl, true), sp.s45)) : 0;
     const size_t lim = 225 * 1024;
     if (sp.s1 > lim || sp.s2 > lim || sp.s3 > lim || sp.s4 > lim || sp.s45 > lim || sp.sflow > lim) {
         ctx->err = "split path: shared-memory plan exceeds 225 KB";
