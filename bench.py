@@ -365,12 +365,14 @@ def stream_drift_config(z, ctx, torch, device, nframes, seed=4):
     counts), Poisson(15) emitters a frame on synthetic filaments (random 3-D
     cubic curves, 25 nm jitter), tetrapod PSF (45 modes, pupil 128^2), photons
     LogNormal(ln 4000, 0.5), background 30, and an imposed drift: a random walk
-    of 0.5 nm a frame in x, y, z.  The split-precision detect -> fit pipeline
-    runs on the uint16 frames (host frames in, rows out, timed); then the 3-D
-    drift (20 time bins, 10 nm voxels) is estimated from the localizations in
-    a 5.12 x 5.12 um crop at the centre (one emitter a frame on average sits on
-    the crop's filaments; the others on filaments elsewhere in the frame), and
-    compared with the imposed walk."""
+    of 0.5 nm a frame in x, y, z over 100,000 frames (a run of fewer frames
+    takes proportionally larger steps, so that it spans the same excursion).
+    The split-precision detect -> fit pipeline runs on the uint16 frames (host
+    frames in, rows out, timed); then the 3-D drift (20 time bins, 10 nm
+    voxels) is estimated from the localizations in a 5.12 x 5.12 um crop at the
+    centre (1.5 emitters a frame on average sit on the crop's filaments; the
+    others on filaments elsewhere in the frame), and compared with the imposed
+    walk."""
     S, R, N, P = 512, 40, 128, 64
     rng = np.random.default_rng(seed)
     zern = zern_tetrapod(np.random.default_rng(seed * 100 + 7))
@@ -382,10 +384,12 @@ def stream_drift_config(z, ctx, torch, device, nframes, seed=4):
     inner = filaments(rng, 6, c0 + 0.3, c1 - 0.3, 0.8, 200000)
     outer = filaments(rng, 40, P * DX / 2, fov - P * DX / 2, 1.5, 800000)
     outer = outer[(np.abs(outer[:, 0] - fov / 2) > 2.56 + R * DX / 2) | (np.abs(outer[:, 1] - fov / 2) > 2.56 + R * DX / 2)]
-    walk = np.cumsum(rng.normal(0, 0.5e-3, (nframes, 3)), axis=0)  # um
+    # the walk's step is scaled so that the run spans the excursion of 100,000 frames at 0.5 nm a frame
+    step = 0.5e-3 * np.sqrt(max(1.0, 100000.0 / nframes))
+    walk = np.cumsum(rng.normal(0, step, (nframes, 3)), axis=0)  # um
     emit = []
     for f in range(nframes):
-        k_in, k_out = rng.poisson(1.0), rng.poisson(14.0)
+        k_in, k_out = rng.poisson(1.5), rng.poisson(13.5)
         pts = np.concatenate([inner[rng.integers(0, len(inner), k_in)], outer[rng.integers(0, len(outer), k_out)]])
         for q in pts:
             emit.append((f, *(q + walk[f]), rng.lognormal(np.log(4000.0), 0.5)))
@@ -403,7 +407,7 @@ def stream_drift_config(z, ctx, torch, device, nframes, seed=4):
                        "0.5 nm/frame; split-precision pipeline, host frames in / rows out",
            "frames": nframes, "emitters": int(len(emit)), "localizations": int(len(rows)), "seconds": dt,
            "frames_per_s": nframes / dt, "localizations_per_s": len(rows) / dt,
-           "h2d_bytes": int(frames.nbytes)}
+           "h2d_bytes": int(frames.nbytes), "walk_step_nm": step * 1000.0}
     xyz = np.c_[rows["x_nm"], rows["y_nm"], rows["z_nm"]]
     crop = (np.abs(xyz[:, 0] / 1000 - fov / 2) < 2.56) & (np.abs(xyz[:, 1] / 1000 - fov / 2) < 2.56) & \
         (np.abs(xyz[:, 2]) < 1280.0)
@@ -593,7 +597,7 @@ def main():
     ap.add_argument("--classes", default="", help="comma list of ROI classes to run (profiling); default all")
     ap.add_argument("--pool", type=int, default=0,
                     help="slots of the split fit's pool per class (0: chosen by the library's autotuner)")
-    ap.add_argument("--detect-frames", type=int, default=200,
+    ap.add_argument("--detect-frames", type=int, default=1024,
                     help="frames of the detect -> fit pipeline measurement (0: skip)")
     ap.add_argument("--split-mode", default="staged", choices=["staged", "flow", "fused"],
                     help="split fit kernels: one dataflow kernel, four stage kernels per round, or stage 1 + fused 2-5")
