@@ -515,6 +515,21 @@ __device__ __forceinline__ bool epi_bar_or(bool p) {
     return r != 0;
 }
 
+// Named barrier `id` over N threads (a warp group's own barrier), and its OR form.
+template <int N>
+__device__ __forceinline__ void group_bar(int id) { asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(N) : "memory"); }
+template <int N>
+__device__ __forceinline__ bool group_bar_or(int id, bool p) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred P, Q;\n\tsetp.ne.u32 P, %1, 0;\n\t"
+        "bar.red.or.pred Q, %2, %3, P;\n\tselp.u32 %0, 1, 0, Q;\n\t}\n"
+        : "=r"(r)
+        : "r"((uint32_t)p), "r"(id), "n"(N)
+        : "memory");
+    return r != 0;
+}
+
 __host__ __device__ constexpr int s2_slab_bytes(int W) { return 6 * W * 32; }
 
 __host__ __device__ constexpr int s2_ring_bytes(int W) { return (W > 64 ? 2 : 4) * 4096; }
@@ -2015,10 +2030,11 @@ __global__ void __launch_bounds__(S45_THREADS, 1) k_stage45p(SplitDev P, FitIO F
 // in FP32; the normalisation, likelihood and gradient with Kahan
 // compensation), warp partials combined in FP64 in a fixed order.  Writes
 // P.sums; the caller's next barrier publishes them.
+template <int NTG>
 __device__ __noinline__ void unit_sums(const SplitDev& P, const FitIO& F, int unit, const float* Tm,
-                                       double (*red)[NRED], double (*nrm)[4], int* badw) {
-    const int t = threadIdx.x, warp = t >> 5, lane = t & 31, UG = unit_slots(P.G1, P.G2);
-    const int wps = (SPLIT_THREADS / 32) / UG, g = warp / wps, ws = warp - g * wps;
+                                       double (*red)[NRED], double (*nrm)[4], int* badw, int t, int bar_id) {
+    const int warp = t >> 5, lane = t & 31, UG = unit_slots(P.G1, P.G2);
+    const int wps = (NTG / 32) / UG, g = warp / wps, ws = warp - g * wps;
     const int tid = ws * 32 + lane, nts = wps * 32, R = P.R, RR = R * R;
     const int slot = unit * UG + g, roi = P.slot_roi[slot];
     const float* T0 = Tm + (size_t)g * 4 * RR;
@@ -2036,7 +2052,7 @@ __device__ __noinline__ void unit_sums(const SplitDev& P, const FitIO& F, int un
                      v3 = warp_sum(ns[3]);
         if (lane == 0) { nrm[warp][0] = v0; nrm[warp][1] = v1; nrm[warp][2] = v2; nrm[warp][3] = v3; }
     }
-    epi_bar();
+    group_bar<NTG>(bar_id);
     double s4[4] = {0, 0, 0, 0};
     for (int w = g * wps; w < (g + 1) * wps; ++w)
         for (int q = 0; q < 4; ++q) s4[q] += nrm[w][q];
@@ -2082,8 +2098,8 @@ __device__ __noinline__ void unit_sums(const SplitDev& P, const FitIO& F, int un
     warp_sums36(sg6, cg6, sh, red[warp], lane);
     const bool wbad = __any_sync(0xffffffffu, bad);
     if (lane == 0) badw[warp] = wbad;
-    epi_bar();
-    for (int i = t; i < UG * (NRED + 1); i += SPLIT_THREADS) {
+    group_bar<NTG>(bar_id);
+    for (int i = t; i < UG * (NRED + 1); i += NTG) {
         const int gg = i / (NRED + 1), k = i - gg * (NRED + 1), sl = unit * UG + gg;
         if (P.slot_roi[sl] < 0) continue;
         if (k < NRED) {
@@ -2109,14 +2125,92 @@ __device__ __noinline__ void unit_sums(const SplitDev& P, const FitIO& F, int un
 // follows in its own stage.
 constexpr int S45S_THREADS = SPLIT_THREADS + 32;
 
-__host__ __device__ inline size_t s45s_smem(int W, int RP, int R, int UG, int nb) {
-    return (size_t)2 * 128 * W * 2 + (size_t)nb * UG * a4_slot_bytes(W, RP) + (size_t)UG * 4 * R * R * 4 + 16 +
-           (size_t)(SPLIT_THREADS / 32) * ((NRED + 4) * 8 + 4);
+// Map areas of the epilogue: two warp groups of 256 threads, each summing its
+// own unit (units alternate between them, with the J buffers and TMEM
+// accumulators), when there are two buffers; one group of 512 threads
+// otherwise.  The choice depends on the class alone, so the round-based and
+// dataflow kernels sum in the same order.
+__host__ __device__ inline int s45s_groups(int nb) { return nb == 2 ? 2 : 1; }
+__host__ __device__ inline size_t s45s_smem(int W, int RP, int R, int UG, int nb, int groups = 1) {
+    return (size_t)2 * 128 * W * 2 + (size_t)nb * UG * a4_slot_bytes(W, RP) + (size_t)groups * UG * 4 * R * R * 4 +
+           16 + (size_t)(SPLIT_THREADS / 32) * ((NRED + 4) * 8 + 4);
 }
 // J buffers and TMEM accumulators: two when they fit (the next unit's load and
 // MMAs overlap this unit's epilogue), else one.
 __host__ __device__ inline int s45s_nbuf(int W, int RP, int R, int UG) {
-    return 2 * UG * 4 * RP <= 512 && s45s_smem(W, RP, R, UG, 2) <= 225 * 1024 ? 2 : 1;
+    return 2 * UG * 4 * RP <= 512 && s45s_smem(W, RP, R, UG, 2, s45s_groups(2)) <= 225 * 1024 ? 2 : 1;
+}
+
+// The epilogue of one group of NTG threads (tg its thread index, bar_id its
+// barrier): the maps of each unit it owns from TMEM to shared memory (pixel
+// column j' = TMEM lane; 4 NTG / 512 maps a thread), then the unit's sums.
+template <int NTG, class UNITS>
+__device__ __forceinline__ void s45s_epilogue(const SplitDev& P, const FitIO& F, UNITS& units, int NB, int grp,
+                                              int tg, int bar_id, uint32_t tbase, float* Tm, double (*red)[NRED],
+                                              double (*nrm)[4], int* badw, uint64_t* acc, uint64_t* tfree) {
+    constexpr int NG = SPLIT_THREADS / NTG;  // groups
+    const int R = P.R, RP = P.RP, NT = 4 * RP, RR = R * R, UG = unit_slots(P.G1, P.G2), nc = UG * NT;
+    const int jp = tg & 127;
+    int n = 0;
+    bool abort = false;
+    for (int tag = 0; !abort;) {
+        const int unit = units.next(P, tag);
+        if (unit < 0) break;
+        const int b = n % NB;
+        const uint32_t par = (uint32_t)((n / NB) & 1);
+        ++n;
+        if (NG == 2 && b != grp) continue;  // the other group's unit
+        umma::mbar_wait(&acc[b], par, P.err);
+        umma::fence_after_sync();
+#pragma unroll
+        for (int mi = 0; mi < NG; ++mi) {
+            const int map = NG == 1 ? (tg >> 7) : 2 * (tg >> 7) + mi;
+            const float cT = P.sc.cT[map];
+            if (UG * RP == 64) {
+                // the whole unit's columns of this map and lane (8 groups of 8) in flight before one wait
+                uint32_t ad[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const int g = q / (RP / 8), h = (q - g * (RP / 8)) * 8;
+                    ad[q] = tmem_lane_addr(tbase, b * nc + g * NT + map * RP + h);
+                }
+                float v[8][8];
+                tmem_ld8_multi<8>(ad, v);
+                if (jp < R)
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const int g = q / (RP / 8), h = (q - g * (RP / 8)) * 8;
+                        if (P.slot_roi[unit * UG + g] < 0) continue;
+                        float* dst = Tm + (size_t)(g * 4 + map) * RR;
+#pragma unroll
+                        for (int u = 0; u < 8; ++u)
+                            if (h + u < R) dst[(h + u) * R + jp] = v[q][u] * cT;
+                    }
+            } else {
+                for (int g = 0; g < UG; ++g) {
+                    if (P.slot_roi[unit * UG + g] < 0) continue;
+                    float* dst = Tm + (size_t)(g * 4 + map) * RR;
+                    for (int h = 0; h < RP; h += 16) {  // 16 columns a wait
+                        const uint32_t ad[2] = {tmem_lane_addr(tbase, b * nc + g * NT + map * RP + h),
+                                                tmem_lane_addr(tbase, b * nc + g * NT + map * RP + h + 8)};
+                        float v[2][8];
+                        tmem_ld8_multi<2>(ad, v);
+                        if (jp < R)
+#pragma unroll
+                            for (int u = 0; u < 16; ++u)
+                                if (h + u < R) dst[(h + u) * R + jp] = v[u >> 3][u & 7] * cT;
+                    }
+                }
+            }
+        }
+        umma::fence_before_sync();
+        warp_arrive(&tfree[b]);
+        group_bar<NTG>(bar_id);
+        unit_sums<NTG>(P, F, unit, Tm, red, nrm, badw, tg, bar_id);
+        // (a bounded wait that gave up makes every thread of the group leave the loop together)
+        abort = group_bar_or<NTG>(bar_id, tg == 0 && *(volatile int*)P.err != 0);
+        if (!abort && tg == 0) units.release(P, unit, tag + 1);
+    }
 }
 
 template <class UNITS>
@@ -2127,9 +2221,11 @@ __device__ __forceinline__ void stage45s_body(const SplitDev& P, const FitIO& F,
     const uint32_t garr = 128u * W * 2, jslot = (uint32_t)a4_slot_bytes(W, RP), jarr = jslot / 2;
     char* G = smem;                                      // G hi, lo (128 rows, rows >= R zero)
     const int NB = s45s_nbuf(W, RP, R, UG);
+    const int NGRP = s45s_groups(NB);
     char* JB = G + 2 * garr;                             // NB buffers of a unit's J
-    float* Tm = (float*)(JB + (size_t)NB * UG * jslot);  // the unit's maps: slot g, map m at (4 g + m) R^2
-    double (*red)[NRED] = (double (*)[NRED])(((uintptr_t)(Tm + (size_t)UG * 4 * RR) + 15) & ~(uintptr_t)15);
+    float* Tm = (float*)(JB + (size_t)NB * UG * jslot);  // per group, a unit's maps: slot g, map m at (4 g + m) R^2
+    double (*red)[NRED] =
+        (double (*)[NRED])(((uintptr_t)(Tm + (size_t)NGRP * UG * 4 * RR) + 15) & ~(uintptr_t)15);
     double (*nrm)[4] = (double (*)[4])(red + SPLIT_THREADS / 32);  // per-warp sums: likelihood terms, normalisation
     int* badw = (int*)(nrm + SPLIT_THREADS / 32);
     __shared__ __align__(8) uint64_t gfull, full[2], acc[2], tfree[2], fin;
@@ -2142,7 +2238,7 @@ __device__ __forceinline__ void stage45s_body(const SplitDev& P, const FitIO& F,
         for (int b = 0; b < 2; ++b) {
             umma::mbar_init(&full[b], 1);
             umma::mbar_init(&acc[b], 1);
-            umma::mbar_init(&tfree[b], SPLIT_THREADS / 32);
+            umma::mbar_init(&tfree[b], SPLIT_THREADS / 32 / NGRP);  // the warps of the unit's group
         }
         umma::mbar_init(&fin, 1);
         umma::mbar_fence_init();
@@ -2194,61 +2290,13 @@ __device__ __forceinline__ void stage45s_body(const SplitDev& P, const FitIO& F,
         return;
     }
 
-    // ---------------- epilogue: pixel column j' = TMEM lane, map = warpgroup
-    const int jp = t & 127, map = t >> 7;
-    int n = 0;
-    bool abort = false;
-    for (int tag = 0; !abort;) {
-        const int unit = units.next(P, tag);
-        if (unit < 0) break;
-        const int b = n % NB;
-        umma::mbar_wait(&acc[b], (uint32_t)((n / NB) & 1), P.err);
-        umma::fence_after_sync();
-        ++n;
-        const float cT = P.sc.cT[map];
-        if (UG * RP == 64) {
-            // the whole unit's map columns of this lane (8 groups of 8) in flight before one wait
-            uint32_t ad[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                const int g = q / (RP / 8), h = (q - g * (RP / 8)) * 8;
-                ad[q] = tmem_lane_addr(tbase, b * nc + g * NT + map * RP + h);
-            }
-            float v[8][8];
-            tmem_ld8_multi<8>(ad, v);
-            if (jp < R)
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    const int g = q / (RP / 8), h = (q - g * (RP / 8)) * 8;
-                    if (P.slot_roi[unit * UG + g] < 0) continue;
-                    float* dst = Tm + (size_t)(g * 4 + map) * RR;
-#pragma unroll
-                    for (int u = 0; u < 8; ++u)
-                        if (h + u < R) dst[(h + u) * R + jp] = v[q][u] * cT;
-                }
-        } else {
-            for (int g = 0; g < UG; ++g) {
-                if (P.slot_roi[unit * UG + g] < 0) continue;
-                float* dst = Tm + (size_t)(g * 4 + map) * RR;
-                for (int h = 0; h < RP; h += 16) {  // 16 columns a wait
-                    const uint32_t ad[2] = {tmem_lane_addr(tbase, b * nc + g * NT + map * RP + h),
-                                            tmem_lane_addr(tbase, b * nc + g * NT + map * RP + h + 8)};
-                    float v[2][8];
-                    tmem_ld8_multi<2>(ad, v);
-                    if (jp < R)
-#pragma unroll
-                        for (int u = 0; u < 16; ++u)
-                            if (h + u < R) dst[(h + u) * R + jp] = v[u >> 3][u & 7] * cT;
-                }
-            }
-        }
-        umma::fence_before_sync();
-        warp_arrive(&tfree[b]);
-        epi_bar();
-        unit_sums(P, F, unit, Tm, red, nrm, badw);
-        // (a bounded wait that gave up makes every epilogue thread leave the loop together)
-        abort = epi_bar_or(t == 0 && *(volatile int*)P.err != 0);
-        if (!abort && t == 0) units.release(P, unit, tag + 1);
+    // ---------------- epilogue: one group of 512 threads, or two of 256
+    if (NGRP == 2) {
+        const int grp = t >> 8, tg = t & 255;
+        s45s_epilogue<256>(P, F, units, NB, grp, tg, 2 + grp, tbase, Tm + (size_t)grp * UG * 4 * RR, red + 8 * grp,
+                           nrm + 8 * grp, badw + 8 * grp, acc, tfree);
+    } else {
+        s45s_epilogue<SPLIT_THREADS>(P, F, units, NB, 0, t, 1, tbase, Tm, red, nrm, badw, acc, tfree);
     }
     if (t == 0) umma::mbar_wait(&fin, 0, P.err);  // every MMA of this CTA has completed
     epi_bar();
@@ -2703,8 +2751,8 @@ static size_t smem_stage45(const SplitPlanHost& pl) {
            (size_t)4 * pl.R * tm_stride(pl.R) * 4 + 16 + (size_t)(E45_THREADS / 32) * (NRED * 8 + 4);
 }
 static size_t smem_stage45s(const SplitPlanHost& pl) {
-    const int UG = unit_slots(pl.G1, pl.G2);
-    return s45s_smem(pl.W, pl.RP, pl.R, UG, s45s_nbuf(pl.W, pl.RP, pl.R, UG));
+    const int UG = unit_slots(pl.G1, pl.G2), nb = s45s_nbuf(pl.W, pl.RP, pl.R, UG);
+    return s45s_smem(pl.W, pl.RP, pl.R, UG, nb, s45s_groups(nb));
 }
 static size_t smem_fused(const SplitPlanHost& pl) {
     const int nbuf = pl.W >= 64 ? 2 : 1;
