@@ -1776,7 +1776,8 @@ __device__ __forceinline__ void stage45_body(const SplitDev& P, const FitIO& F, 
     float* Tm = (float*)(RO + 4 * roib); // the slot's four FP32 maps, row stride RS
     const int RS = tm_stride(R), MS = R * RS;
     double (*red)[NRED] = (double (*)[NRED])(((uintptr_t)(Tm + 4 * MS) + 15) & ~(uintptr_t)15);  // per-warp sums
-    int* bad_w = (int*)(red + E45_THREADS / 32);
+    double (*nrm4)[4] = (double (*)[4])(red + E45_THREADS / 32);  // per-warp normalisation sums
+    int* bad_w = (int*)(nrm4 + E45_THREADS / 32);
     const bool vec = (R % 2) == 0;       // whole 16-byte units: ROI copies by TMA
     __shared__ __align__(8) uint64_t gfull, full[S45_NBUF], freed[S45_NBUF], acc[2], tfree[2], rfull[2], rfree[2], fin;
     __shared__ uint32_t tmem_base;
@@ -1939,13 +1940,17 @@ __device__ __forceinline__ void stage45_body(const SplitDev& P, const FitIO& F, 
             if (vec) umma::mbar_wait(&rfull[b], ph, P.err);
             {
                 const double v0 = warp_sum(ns[0]), v1 = warp_sum(ns[1]), v2 = warp_sum(ns[2]), v3 = warp_sum(ns[3]);
-                if (lane == 0) { red[warp][0] = v0; red[warp][1] = v1; red[warp][2] = v2; red[warp][3] = v3; }
+                if (lane == 0) { nrm4[warp][0] = v0; nrm4[warp][1] = v1; nrm4[warp][2] = v2; nrm4[warp][3] = v3; }
             }
-            epi_bar<E45_THREADS>();
+            // the maps and norms are in; in the round-based kernel this barrier also takes the
+            // vote on a bounded wait that gave up (every epilogue thread leaves the loop together)
+            if (epi_bar_or<E45_THREADS>(!UNITS::flow && t == 0 && *(volatile int*)P.err != 0)) {
+                abort = true;
+                break;
+            }
             double sum4[4] = {0, 0, 0, 0};
             for (int w = 0; w < NW; ++w)
-                for (int q = 0; q < 4; ++q) sum4[q] += red[w][q];
-            epi_bar<E45_THREADS>();
+                for (int q = 0; q < 4; ++q) sum4[q] += nrm4[w][q];
             const float S = (float)sum4[0], Dx = (float)sum4[1], Dy = (float)sum4[2], Dz = (float)sum4[3];
             const float invS = 1.f / S;
             const double* th = P.lm[slot].trial;
@@ -2005,14 +2010,19 @@ __device__ __forceinline__ void stage45_body(const SplitDev& P, const FitIO& F, 
                 for (int w = 0; w < NW; ++w) any |= bad_w[w];
                 P.sums[(size_t)slot * NSUM + NRED] = any ? 1.0 : 0.0;
             }
-            // (a bounded wait that gave up makes every epilogue thread leave the loop together)
-            if (epi_bar_or<E45_THREADS>(t == 0 && *(volatile int*)P.err != 0)) {
-                abort = true;
-                break;
+            // The dataflow kernel publishes the unit once its sums are written, behind this
+            // barrier, which also takes the vote on a bounded wait that gave up.  The
+            // round-based kernel needs neither: the next slot's first barrier orders the
+            // sums and maps against their next writers.
+            if constexpr (UNITS::flow) {
+                if (epi_bar_or<E45_THREADS>(t == 0 && *(volatile int*)P.err != 0)) {
+                    abort = true;
+                    break;
+                }
             }
         }
         if (abort) break;
-        if (t == 0) units.release(P, unit, tag + 1);  // (the sums were written before the last barrier)
+        if (t == 0) units.release(P, unit, tag + 1);  // (flow: the sums were written before the last barrier)
     }
     if (t == 0) umma::mbar_wait(&fin, 0, P.err);  // every MMA of this CTA has completed
     epi_bar<E45_THREADS>();
@@ -2205,11 +2215,17 @@ __device__ __forceinline__ void s45s_epilogue(const SplitDev& P, const FitIO& F,
         }
         umma::fence_before_sync();
         warp_arrive(&tfree[b]);
-        group_bar<NTG>(bar_id);
+        // the maps are in; in the round-based kernel this barrier also takes the vote on a
+        // bounded wait that gave up (every thread of the group leaves the loop together)
+        if (group_bar_or<NTG>(bar_id, !UNITS::flow && tg == 0 && *(volatile int*)P.err != 0)) break;
         unit_sums<NTG>(P, F, unit, Tm, red, nrm, badw, tg, bar_id);
-        // (a bounded wait that gave up makes every thread of the group leave the loop together)
-        abort = group_bar_or<NTG>(bar_id, tg == 0 && *(volatile int*)P.err != 0);
-        if (!abort && tg == 0) units.release(P, unit, tag + 1);
+        // The dataflow kernel publishes the unit once its sums are written, behind this
+        // barrier (with the vote); the round-based kernel needs neither: the next unit's
+        // first barrier orders the sums and maps against their next writers.
+        if constexpr (UNITS::flow) {
+            abort = group_bar_or<NTG>(bar_id, tg == 0 && *(volatile int*)P.err != 0);
+            if (!abort && tg == 0) units.release(P, unit, tag + 1);
+        }
     }
 }
 
@@ -2748,7 +2764,7 @@ static size_t smem_stage3(const SplitPlanHost& pl, bool flow = false) {
 static size_t smem_stage4(const SplitPlanHost& pl) { return a4_slot_bytes(pl.W, pl.RP) + (size_t)2 * 128 * pl.W * 2; }
 static size_t smem_stage45(const SplitPlanHost& pl) {
     return (size_t)2 * 128 * pl.W * 2 + (size_t)S45_NBUF * 2 * 32 * 4 * pl.RP + 4 * s45_roi_bytes(pl.R) +
-           (size_t)4 * pl.R * tm_stride(pl.R) * 4 + 16 + (size_t)(E45_THREADS / 32) * (NRED * 8 + 4);
+           (size_t)4 * pl.R * tm_stride(pl.R) * 4 + 16 + (size_t)(E45_THREADS / 32) * (NRED * 8 + 4 * 8 + 4);
 }
 static size_t smem_stage45s(const SplitPlanHost& pl) {
     const int UG = unit_slots(pl.G1, pl.G2), nb = s45s_nbuf(pl.W, pl.RP, pl.R, UG);
