@@ -425,11 +425,12 @@ ZOLA_API int zola_fit_split_pool(zola_psf* psf, int R, int* pool, double* ns_per
  * CTAs had a unit to work on, and the busy GPU clocks one CTA spent per unit;
  * and the model evaluations made (nullable pointers, 5 values each). */
 ZOLA_API int zola_ctx_flow_stats(zola_ctx* ctx, double* busy, double* clocks_per_unit, double* evaluations);
-/* Upper bound, in GPU clocks, on any single device-side wait of the split fit
- * (a bulk copy or MMA completion, or the dataflow kernel waiting for a unit to
- * become ready, e.g. for inputs to arrive); 0 restores the default (2^31, about
- * a second).  A wait that runs out ends the call with ZOLA_E_TIMEOUT and leaves
- * the context usable. */
+/* Upper bound, in GPU clocks, on the dataflow kernel's waits for a unit to
+ * become ready (its schedulers and LM warps; e.g. for inputs still arriving);
+ * 0 restores the default (2^31, about a second).  The mbarrier waits on bulk
+ * copies and MMA completions keep a fixed bound of 2^31 clocks: a shorter one
+ * could give up on a copy still in flight.  A wait that runs out ends the call
+ * with ZOLA_E_TIMEOUT and leaves the context usable. */
 ZOLA_API int zola_ctx_set_wait_limit(zola_ctx* ctx, long long clocks);
 
 /* ---- CRLB curves and the z-centre search ------------------------------- */
