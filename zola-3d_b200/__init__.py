@@ -220,7 +220,7 @@ class Context:
         return {"busy": busy.tolist(), "clocks_per_unit": cpu.tolist(), "evaluations": ev.value}
 
     def set_wait_limit(self, clocks):
-        """Upper bound (GPU clocks) on any device-side wait of the split fit; 0 = default (2^31)."""
+        """Upper bound (GPU clocks) on the dataflow kernel's waits for a ready unit; 0 = default (2^31)."""
         self.check(lib().zola_ctx_set_wait_limit(self.h, int(clocks)), "zola_ctx_set_wait_limit")
 
     def profile(self, enable=True):
