@@ -1086,12 +1086,14 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
     constexpr int NCOLS = W >= 64 ? 512 : 256;
     constexpr int NARR = TWO ? 2 : 4;  // A2 arrays per ring step
     const int K1 = P.K1, G2 = P.G2, t = threadIdx.x;
-    const int NS = K1 / 16, NSTEP = TWO ? 2 * NS : NS;
+    // W = 128: the ring carries, per tile, the K steps of (S hi, S lo) for E and E_x, then
+    // S_y alone, then S_z alone, so that E_y and E_z can be issued separately
+    const int NS = K1 / 16, NSTEP = TWO ? 3 * NS : NS;
     const int T2 = unit_slots(P.G1, G2) / G2;  // window tiles per unit
     const uint32_t arr = 128u * K1 * 2;
     char* CS = smem;                 // NS constant K-slabs
     char* RB = smem + NS * SLAB;     // ring of A2 K-slabs
-    __shared__ __align__(8) uint64_t cfull, full[NBUF], freed[NBUF], accA, accB;
+    __shared__ __align__(8) uint64_t cfull, full[NBUF], freed[NBUF], accA, accB, accZ, tfreeE, tfreeX;
     __shared__ uint32_t tmem_base;
     if (t < 32) umma::tmem_alloc(&tmem_base, NCOLS);
     if (t == 0) {
@@ -1099,6 +1101,9 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
         for (int b = 0; b < NBUF; ++b) { umma::mbar_init(&full[b], 1); umma::mbar_init(&freed[b], 1); }
         umma::mbar_init(&accA, 1);
         umma::mbar_init(&accB, 1);
+        umma::mbar_init(&accZ, 1);
+        umma::mbar_init(&tfreeE, SPLIT_THREADS / 32);
+        umma::mbar_init(&tfreeX, SPLIT_THREADS / 32);
         umma::mbar_fence_init();
     }
     __syncthreads();
@@ -1126,11 +1131,11 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
                 for (int n = 0; n < NSTEP; ++n, ++q) {
                     const int buf = q % NBUF;
                     if (q >= NBUF && !umma::mbar_wait(&freed[buf], (uint32_t)((q / NBUF - 1) & 1), P.err)) return;
-                    const bool pb = TWO && n >= NS;
-                    const int s = pb ? n - NS : n;
-                    const int a0 = pb ? 2 : 0;  // phase B streams the y and z arrays
-                    umma::mbar_expect_tx(&full[buf], RING);
-                    for (int j = 0; j < NARR; ++j)
+                    const int ph3 = TWO ? n / NS : 0;  // W = 128: 0 (hi, lo), 1 (y), 2 (z)
+                    const int s = n - ph3 * NS;
+                    const int a0 = ph3 == 0 ? 0 : ph3 + 1, na = ph3 == 0 ? NARR : 1;
+                    umma::mbar_expect_tx(&full[buf], (uint32_t)(na * 4096));
+                    for (int j = 0; j < na; ++j)
                         umma::bulk_g2s(RB + buf * RING + j * 4096, src + (size_t)(a0 + j) * arr + (size_t)s * 4096, 4096,
                                        &full[buf]);
                 }
@@ -1151,9 +1156,10 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
             if (!umma::mbar_wait(&full[buf], (uint32_t)((q / NBUF) & 1), P.err)) return;
             umma::fence_after_sync();
             const uint32_t rb = umma::smem_u32(RB + buf * RING);
-            const bool pb = TWO && n >= NS;
-            const uint32_t cb = umma::smem_u32(CS + (pb ? n - NS : n) * SLAB);
-            const bool first = (pb ? n - NS : n) == 0;
+            const int ph3 = TWO ? n / NS : 0;
+            const bool pb = ph3 > 0;
+            const uint32_t cb = umma::smem_u32(CS + (n - ph3 * NS) * SLAB);
+            const bool first = n - ph3 * NS == 0;
             auto mma = [&](uint32_t a, int row0, int N, int col, bool acc) {
                 const uint64_t ad = umma::smem_desc(a, lbo_mn, 128);
                 const uint64_t bd = umma::smem_desc(cb + (uint32_t)(row0 / 8) * 256, 128, 256);
@@ -1169,8 +1175,7 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
                     mma(rb + 12288, 0, 2 * W, 6 * W, !first);  // Ez
                 }
             } else {
-                mma(rb, 0, 2 * W, 0, !first);          // Ey
-                mma(rb + 4096, 0, 2 * W, 2 * W, !first);  // Ez
+                mma(rb, 0, 2 * W, ph3 == 1 ? 0 : 2 * W, !first);  // Ey into E's columns, Ez into E_x's
             }
             umma::mma_commit(&freed[buf]);
         }
@@ -1194,17 +1199,37 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
             umma::mbar_wait(&accA, (uint32_t)ph, P.err);
             umma::fence_after_sync();
             if constexpr (TWO) {
+                // E (columns 0 .. 2W) into registers first: its columns then take E_y while
+                // this epilogue forms I and I_x; once E_x has been read, its columns take E_z
                 float er[CW], ei[CW];
 #pragma unroll
-                for (int h = 0; h < CW; h += 8) {
+                for (int h = 0; h < CW; h += 16) {
                     const int i0 = wg * CW + h;
                     float v4[4][8];
                     const uint32_t ad[4] = {tmem_lane_addr(tbase, i0), tmem_lane_addr(tbase, W + i0),
-                                            tmem_lane_addr(tbase, 2 * W + i0), tmem_lane_addr(tbase, 3 * W + i0)};
+                                            tmem_lane_addr(tbase, i0 + 8), tmem_lane_addr(tbase, W + i0 + 8)};
                     tmem_ld8_multi<4>(ad, v4);
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) { er[h + u] = v4[0][u]; ei[h + u] = v4[1][u]; }
-                    const float *xr = v4[2], *xi = v4[3];
+                    for (int u = 0; u < 8; ++u) {
+                        er[h + u] = v4[0][u]; ei[h + u] = v4[1][u];
+                        er[h + 8 + u] = v4[2][u]; ei[h + 8 + u] = v4[3][u];
+                    }
+                }
+                umma::fence_before_sync();
+                warp_arrive(&tfreeE);
+                if (t == 0) {  // E_y into E's columns
+                    umma::mbar_wait(&tfreeE, (uint32_t)ph, P.err);
+                    umma::fence_after_sync();
+                    issue_steps(NS, 2 * NS);
+                    umma::mma_commit(&accB);
+                }
+#pragma unroll
+                for (int h = 0; h < CW; h += 8) {
+                    const int i0 = wg * CW + h;
+                    float v2[2][8];
+                    const uint32_t ad[2] = {tmem_lane_addr(tbase, 2 * W + i0), tmem_lane_addr(tbase, 3 * W + i0)};
+                    tmem_ld8_multi<2>(ad, v2);
+                    const float *xr = v2[0], *xi = v2[1];
                     uint32_t hh[4], ll[4], dx[4];
 #pragma unroll
                     for (int u = 0; u < 8; u += 2) {
@@ -1220,32 +1245,42 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
                     store4w(a3t + 2 * arr3 + off, dx);
                 }
                 umma::fence_before_sync();
-                epi_bar();
-                if (t == 0) {
+                warp_arrive(&tfreeX);
+                if (t == 0) {  // E_z into E_x's columns
+                    umma::mbar_wait(&tfreeX, (uint32_t)ph, P.err);
                     umma::fence_after_sync();
-                    issue_steps(NS, NSTEP);
-                    umma::mma_commit(&accB);
+                    issue_steps(2 * NS, 3 * NS);
+                    umma::mma_commit(&accZ);
                 }
                 umma::mbar_wait(&accB, (uint32_t)ph, P.err);
                 umma::fence_after_sync();
 #pragma unroll
                 for (int h = 0; h < CW; h += 8) {
                     const int i0 = wg * CW + h;
-                    float v4[4][8];
-                    const uint32_t ad[4] = {tmem_lane_addr(tbase, i0), tmem_lane_addr(tbase, W + i0),
-                                            tmem_lane_addr(tbase, 2 * W + i0), tmem_lane_addr(tbase, 3 * W + i0)};
-                    tmem_ld8_multi<4>(ad, v4);
-                    uint32_t dy[4], dz[4];
+                    float v2[2][8];
+                    const uint32_t ad[2] = {tmem_lane_addr(tbase, i0), tmem_lane_addr(tbase, W + i0)};
+                    tmem_ld8_multi<2>(ad, v2);
+                    uint32_t dy[4];
 #pragma unroll
-                    for (int u = 0; u < 8; u += 2) {
-                        dy[u / 2] = pack_h2(ipx(er + h, ei + h, v4[0], v4[1], u, P.sc.cIy),
-                                            ipx(er + h, ei + h, v4[0], v4[1], u + 1, P.sc.cIy));
-                        dz[u / 2] = pack_h2(ipx(er + h, ei + h, v4[2], v4[3], u, P.sc.cIz),
-                                            ipx(er + h, ei + h, v4[2], v4[3], u + 1, P.sc.cIz));
-                    }
-                    const uint32_t off = kmajor_off(row, i0, W);
-                    store4w(a3t + 3 * arr3 + off, dy);
-                    store4w(a3t + 4 * arr3 + off, dz);
+                    for (int u = 0; u < 8; u += 2)
+                        dy[u / 2] = pack_h2(ipx(er + h, ei + h, v2[0], v2[1], u, P.sc.cIy),
+                                            ipx(er + h, ei + h, v2[0], v2[1], u + 1, P.sc.cIy));
+                    store4w(a3t + 3 * arr3 + kmajor_off(row, i0, W), dy);
+                }
+                umma::mbar_wait(&accZ, (uint32_t)ph, P.err);
+                umma::fence_after_sync();
+#pragma unroll
+                for (int h = 0; h < CW; h += 8) {
+                    const int i0 = wg * CW + h;
+                    float v2[2][8];
+                    const uint32_t ad[2] = {tmem_lane_addr(tbase, 2 * W + i0), tmem_lane_addr(tbase, 3 * W + i0)};
+                    tmem_ld8_multi<2>(ad, v2);
+                    uint32_t dz[4];
+#pragma unroll
+                    for (int u = 0; u < 8; u += 2)
+                        dz[u / 2] = pack_h2(ipx(er + h, ei + h, v2[0], v2[1], u, P.sc.cIz),
+                                            ipx(er + h, ei + h, v2[0], v2[1], u + 1, P.sc.cIz));
+                    store4w(a3t + 4 * arr3 + kmajor_off(row, i0, W), dz);
                 }
             } else {
 #pragma unroll
