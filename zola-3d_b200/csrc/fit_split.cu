@@ -1087,8 +1087,9 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
     constexpr int NARR = TWO ? 2 : 4;  // A2 arrays per ring step
     const int K1 = P.K1, G2 = P.G2, t = threadIdx.x;
     // W = 128: the ring carries, per tile, the K steps of (S hi, S lo) for E and E_x, then
-    // S_y alone, then S_z alone, so that E_y and E_z can be issued separately
-    const int NS = K1 / 16, NSTEP = TWO ? 3 * NS : NS;
+    // S_y two K steps an entry, then S_z two K steps an entry, so that E_y and E_z can be
+    // issued separately with as many bytes in flight per entry
+    const int NS = K1 / 16, NSTEP = TWO ? 2 * NS : NS;
     const int T2 = unit_slots(P.G1, G2) / G2;  // window tiles per unit
     const uint32_t arr = 128u * K1 * 2;
     char* CS = smem;                 // NS constant K-slabs
@@ -1131,13 +1132,19 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
                 for (int n = 0; n < NSTEP; ++n, ++q) {
                     const int buf = q % NBUF;
                     if (q >= NBUF && !umma::mbar_wait(&freed[buf], (uint32_t)((q / NBUF - 1) & 1), P.err)) return;
-                    const int ph3 = TWO ? n / NS : 0;  // W = 128: 0 (hi, lo), 1 (y), 2 (z)
-                    const int s = n - ph3 * NS;
-                    const int a0 = ph3 == 0 ? 0 : ph3 + 1, na = ph3 == 0 ? NARR : 1;
-                    umma::mbar_expect_tx(&full[buf], (uint32_t)(na * 4096));
-                    for (int j = 0; j < na; ++j)
-                        umma::bulk_g2s(RB + buf * RING + j * 4096, src + (size_t)(a0 + j) * arr + (size_t)s * 4096, 4096,
-                                       &full[buf]);
+                    // W = 128: kind 0 = (hi, lo) of step n, 1 = y and 2 = z of steps 2e, 2e + 1
+                    const int kind = !TWO || n < NS ? 0 : n < NS + NS / 2 ? 1 : 2;
+                    umma::mbar_expect_tx(&full[buf], RING);
+                    if (kind == 0) {
+                        for (int aj = 0; aj < NARR; ++aj)
+                            umma::bulk_g2s(RB + buf * RING + aj * 4096, src + (size_t)aj * arr + (size_t)n * 4096, 4096,
+                                           &full[buf]);
+                    } else {
+                        const int e = n - NS - (kind == 2 ? NS / 2 : 0);
+                        for (int j = 0; j < 2; ++j)
+                            umma::bulk_g2s(RB + buf * RING + j * 4096,
+                                           src + (size_t)(kind + 1) * arr + (size_t)(2 * e + j) * 4096, 4096, &full[buf]);
+                    }
                 }
             }
         }
@@ -1156,10 +1163,10 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
             if (!umma::mbar_wait(&full[buf], (uint32_t)((q / NBUF) & 1), P.err)) return;
             umma::fence_after_sync();
             const uint32_t rb = umma::smem_u32(RB + buf * RING);
-            const int ph3 = TWO ? n / NS : 0;
-            const bool pb = ph3 > 0;
-            const uint32_t cb = umma::smem_u32(CS + (n - ph3 * NS) * SLAB);
-            const bool first = n - ph3 * NS == 0;
+            const int kind = !TWO || n < NS ? 0 : n < NS + NS / 2 ? 1 : 2;
+            const bool pb = kind > 0;
+            const uint32_t cb = umma::smem_u32(CS + (pb ? 0 : n) * SLAB);
+            const bool first = n == 0;
             auto mma = [&](uint32_t a, int row0, int N, int col, bool acc) {
                 const uint64_t ad = umma::smem_desc(a, lbo_mn, 128);
                 const uint64_t bd = umma::smem_desc(cb + (uint32_t)(row0 / 8) * 256, 128, 256);
@@ -1174,8 +1181,15 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
                     mma(rb + 8192, 0, 2 * W, 4 * W, !first);   // Ey
                     mma(rb + 12288, 0, 2 * W, 6 * W, !first);  // Ez
                 }
-            } else {
-                mma(rb, 0, 2 * W, ph3 == 1 ? 0 : 2 * W, !first);  // Ey into E's columns, Ez into E_x's
+            } else {  // two K steps of E_y (into E's columns) or E_z (into E_x's)
+                const int e = n - NS - (kind == 2 ? NS / 2 : 0);
+                for (int j = 0; j < 2; ++j) {
+                    const int st = 2 * e + j;
+                    const uint64_t ad = umma::smem_desc(rb + (uint32_t)j * 4096, lbo_mn, 128);
+                    const uint64_t bd = umma::smem_desc(umma::smem_u32(CS + st * SLAB), 128, 256);
+                    umma::mma_f16(tbase + (kind == 1 ? 0 : 2 * W), ad, bd, umma::idesc_f16(128, 2 * W, true, false),
+                                  st > 0 ? 1u : 0u);
+                }
             }
             umma::mma_commit(&freed[buf]);
         }
@@ -1220,7 +1234,7 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
                 if (t == 0) {  // E_y into E's columns
                     umma::mbar_wait(&tfreeE, (uint32_t)ph, P.err);
                     umma::fence_after_sync();
-                    issue_steps(NS, 2 * NS);
+                    issue_steps(NS, NS + NS / 2);
                     umma::mma_commit(&accB);
                 }
 #pragma unroll
@@ -1249,7 +1263,7 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
                 if (t == 0) {  // E_z into E_x's columns
                     umma::mbar_wait(&tfreeX, (uint32_t)ph, P.err);
                     umma::fence_after_sync();
-                    issue_steps(2 * NS, 3 * NS);
+                    issue_steps(NS + NS / 2, 2 * NS);
                     umma::mma_commit(&accZ);
                 }
                 umma::mbar_wait(&accB, (uint32_t)ph, P.err);
