@@ -1086,15 +1086,12 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
     constexpr int NCOLS = W >= 64 ? 512 : 256;
     constexpr int NARR = TWO ? 2 : 4;  // A2 arrays per ring step
     const int K1 = P.K1, G2 = P.G2, t = threadIdx.x;
-    // W = 128: the ring carries, per tile, the K steps of (S hi, S lo) for E and E_x, then
-    // S_y two K steps an entry, then S_z two K steps an entry, so that E_y and E_z can be
-    // issued separately with as many bytes in flight per entry
     const int NS = K1 / 16, NSTEP = TWO ? 2 * NS : NS;
     const int T2 = unit_slots(P.G1, G2) / G2;  // window tiles per unit
     const uint32_t arr = 128u * K1 * 2;
     char* CS = smem;                 // NS constant K-slabs
     char* RB = smem + NS * SLAB;     // ring of A2 K-slabs
-    __shared__ __align__(8) uint64_t cfull, full[NBUF], freed[NBUF], accA, accB, accZ, tfreeE, tfreeX;
+    __shared__ __align__(8) uint64_t cfull, full[NBUF], freed[NBUF], accA, accB;
     __shared__ uint32_t tmem_base;
     if (t < 32) umma::tmem_alloc(&tmem_base, NCOLS);
     if (t == 0) {
@@ -1102,9 +1099,6 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
         for (int b = 0; b < NBUF; ++b) { umma::mbar_init(&full[b], 1); umma::mbar_init(&freed[b], 1); }
         umma::mbar_init(&accA, 1);
         umma::mbar_init(&accB, 1);
-        umma::mbar_init(&accZ, 1);
-        umma::mbar_init(&tfreeE, SPLIT_THREADS / 32);
-        umma::mbar_init(&tfreeX, SPLIT_THREADS / 32);
         umma::mbar_fence_init();
     }
     __syncthreads();
@@ -1132,19 +1126,13 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
                 for (int n = 0; n < NSTEP; ++n, ++q) {
                     const int buf = q % NBUF;
                     if (q >= NBUF && !umma::mbar_wait(&freed[buf], (uint32_t)((q / NBUF - 1) & 1), P.err)) return;
-                    // W = 128: kind 0 = (hi, lo) of step n, 1 = y and 2 = z of steps 2e, 2e + 1
-                    const int kind = !TWO || n < NS ? 0 : n < NS + NS / 2 ? 1 : 2;
+                    const bool pb = TWO && n >= NS;
+                    const int s = pb ? n - NS : n;
+                    const int a0 = pb ? 2 : 0;  // phase B streams the y and z arrays
                     umma::mbar_expect_tx(&full[buf], RING);
-                    if (kind == 0) {
-                        for (int aj = 0; aj < NARR; ++aj)
-                            umma::bulk_g2s(RB + buf * RING + aj * 4096, src + (size_t)aj * arr + (size_t)n * 4096, 4096,
-                                           &full[buf]);
-                    } else {
-                        const int e = n - NS - (kind == 2 ? NS / 2 : 0);
-                        for (int j = 0; j < 2; ++j)
-                            umma::bulk_g2s(RB + buf * RING + j * 4096,
-                                           src + (size_t)(kind + 1) * arr + (size_t)(2 * e + j) * 4096, 4096, &full[buf]);
-                    }
+                    for (int j = 0; j < NARR; ++j)
+                        umma::bulk_g2s(RB + buf * RING + j * 4096, src + (size_t)(a0 + j) * arr + (size_t)s * 4096, 4096,
+                                       &full[buf]);
                 }
             }
         }
@@ -1163,10 +1151,9 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
             if (!umma::mbar_wait(&full[buf], (uint32_t)((q / NBUF) & 1), P.err)) return;
             umma::fence_after_sync();
             const uint32_t rb = umma::smem_u32(RB + buf * RING);
-            const int kind = !TWO || n < NS ? 0 : n < NS + NS / 2 ? 1 : 2;
-            const bool pb = kind > 0;
-            const uint32_t cb = umma::smem_u32(CS + (pb ? 0 : n) * SLAB);
-            const bool first = n == 0;
+            const bool pb = TWO && n >= NS;
+            const uint32_t cb = umma::smem_u32(CS + (pb ? n - NS : n) * SLAB);
+            const bool first = (pb ? n - NS : n) == 0;
             auto mma = [&](uint32_t a, int row0, int N, int col, bool acc) {
                 const uint64_t ad = umma::smem_desc(a, lbo_mn, 128);
                 const uint64_t bd = umma::smem_desc(cb + (uint32_t)(row0 / 8) * 256, 128, 256);
@@ -1181,15 +1168,9 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
                     mma(rb + 8192, 0, 2 * W, 4 * W, !first);   // Ey
                     mma(rb + 12288, 0, 2 * W, 6 * W, !first);  // Ez
                 }
-            } else {  // two K steps of E_y (into E's columns) or E_z (into E_x's)
-                const int e = n - NS - (kind == 2 ? NS / 2 : 0);
-                for (int j = 0; j < 2; ++j) {
-                    const int st = 2 * e + j;
-                    const uint64_t ad = umma::smem_desc(rb + (uint32_t)j * 4096, lbo_mn, 128);
-                    const uint64_t bd = umma::smem_desc(umma::smem_u32(CS + st * SLAB), 128, 256);
-                    umma::mma_f16(tbase + (kind == 1 ? 0 : 2 * W), ad, bd, umma::idesc_f16(128, 2 * W, true, false),
-                                  st > 0 ? 1u : 0u);
-                }
+            } else {
+                mma(rb, 0, 2 * W, 0, !first);          // Ey
+                mma(rb + 4096, 0, 2 * W, 2 * W, !first);  // Ez
             }
             umma::mma_commit(&freed[buf]);
         }
@@ -1213,37 +1194,17 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
             umma::mbar_wait(&accA, (uint32_t)ph, P.err);
             umma::fence_after_sync();
             if constexpr (TWO) {
-                // E (columns 0 .. 2W) into registers first: its columns then take E_y while
-                // this epilogue forms I and I_x; once E_x has been read, its columns take E_z
                 float er[CW], ei[CW];
-#pragma unroll
-                for (int h = 0; h < CW; h += 16) {
-                    const int i0 = wg * CW + h;
-                    float v4[4][8];
-                    const uint32_t ad[4] = {tmem_lane_addr(tbase, i0), tmem_lane_addr(tbase, W + i0),
-                                            tmem_lane_addr(tbase, i0 + 8), tmem_lane_addr(tbase, W + i0 + 8)};
-                    tmem_ld8_multi<4>(ad, v4);
-#pragma unroll
-                    for (int u = 0; u < 8; ++u) {
-                        er[h + u] = v4[0][u]; ei[h + u] = v4[1][u];
-                        er[h + 8 + u] = v4[2][u]; ei[h + 8 + u] = v4[3][u];
-                    }
-                }
-                umma::fence_before_sync();
-                warp_arrive(&tfreeE);
-                if (t == 0) {  // E_y into E's columns
-                    umma::mbar_wait(&tfreeE, (uint32_t)ph, P.err);
-                    umma::fence_after_sync();
-                    issue_steps(NS, NS + NS / 2);
-                    umma::mma_commit(&accB);
-                }
 #pragma unroll
                 for (int h = 0; h < CW; h += 8) {
                     const int i0 = wg * CW + h;
-                    float v2[2][8];
-                    const uint32_t ad[2] = {tmem_lane_addr(tbase, 2 * W + i0), tmem_lane_addr(tbase, 3 * W + i0)};
-                    tmem_ld8_multi<2>(ad, v2);
-                    const float *xr = v2[0], *xi = v2[1];
+                    float v4[4][8];
+                    const uint32_t ad[4] = {tmem_lane_addr(tbase, i0), tmem_lane_addr(tbase, W + i0),
+                                            tmem_lane_addr(tbase, 2 * W + i0), tmem_lane_addr(tbase, 3 * W + i0)};
+                    tmem_ld8_multi<4>(ad, v4);
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) { er[h + u] = v4[0][u]; ei[h + u] = v4[1][u]; }
+                    const float *xr = v4[2], *xi = v4[3];
                     uint32_t hh[4], ll[4], dx[4];
 #pragma unroll
                     for (int u = 0; u < 8; u += 2) {
@@ -1259,42 +1220,32 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
                     store4w(a3t + 2 * arr3 + off, dx);
                 }
                 umma::fence_before_sync();
-                warp_arrive(&tfreeX);
-                if (t == 0) {  // E_z into E_x's columns
-                    umma::mbar_wait(&tfreeX, (uint32_t)ph, P.err);
+                epi_bar();
+                if (t == 0) {
                     umma::fence_after_sync();
-                    issue_steps(NS + NS / 2, 2 * NS);
-                    umma::mma_commit(&accZ);
+                    issue_steps(NS, NSTEP);
+                    umma::mma_commit(&accB);
                 }
                 umma::mbar_wait(&accB, (uint32_t)ph, P.err);
                 umma::fence_after_sync();
 #pragma unroll
                 for (int h = 0; h < CW; h += 8) {
                     const int i0 = wg * CW + h;
-                    float v2[2][8];
-                    const uint32_t ad[2] = {tmem_lane_addr(tbase, i0), tmem_lane_addr(tbase, W + i0)};
-                    tmem_ld8_multi<2>(ad, v2);
-                    uint32_t dy[4];
+                    float v4[4][8];
+                    const uint32_t ad[4] = {tmem_lane_addr(tbase, i0), tmem_lane_addr(tbase, W + i0),
+                                            tmem_lane_addr(tbase, 2 * W + i0), tmem_lane_addr(tbase, 3 * W + i0)};
+                    tmem_ld8_multi<4>(ad, v4);
+                    uint32_t dy[4], dz[4];
 #pragma unroll
-                    for (int u = 0; u < 8; u += 2)
-                        dy[u / 2] = pack_h2(ipx(er + h, ei + h, v2[0], v2[1], u, P.sc.cIy),
-                                            ipx(er + h, ei + h, v2[0], v2[1], u + 1, P.sc.cIy));
-                    store4w(a3t + 3 * arr3 + kmajor_off(row, i0, W), dy);
-                }
-                umma::mbar_wait(&accZ, (uint32_t)ph, P.err);
-                umma::fence_after_sync();
-#pragma unroll
-                for (int h = 0; h < CW; h += 8) {
-                    const int i0 = wg * CW + h;
-                    float v2[2][8];
-                    const uint32_t ad[2] = {tmem_lane_addr(tbase, 2 * W + i0), tmem_lane_addr(tbase, 3 * W + i0)};
-                    tmem_ld8_multi<2>(ad, v2);
-                    uint32_t dz[4];
-#pragma unroll
-                    for (int u = 0; u < 8; u += 2)
-                        dz[u / 2] = pack_h2(ipx(er + h, ei + h, v2[0], v2[1], u, P.sc.cIz),
-                                            ipx(er + h, ei + h, v2[0], v2[1], u + 1, P.sc.cIz));
-                    store4w(a3t + 4 * arr3 + kmajor_off(row, i0, W), dz);
+                    for (int u = 0; u < 8; u += 2) {
+                        dy[u / 2] = pack_h2(ipx(er + h, ei + h, v4[0], v4[1], u, P.sc.cIy),
+                                            ipx(er + h, ei + h, v4[0], v4[1], u + 1, P.sc.cIy));
+                        dz[u / 2] = pack_h2(ipx(er + h, ei + h, v4[2], v4[3], u, P.sc.cIz),
+                                            ipx(er + h, ei + h, v4[2], v4[3], u + 1, P.sc.cIz));
+                    }
+                    const uint32_t off = kmajor_off(row, i0, W);
+                    store4w(a3t + 3 * arr3 + off, dy);
+                    store4w(a3t + 4 * arr3 + off, dz);
                 }
             } else {
 #pragma unroll
