@@ -597,15 +597,38 @@ int cal_setup(zola_psf* p, const zola_calib_data* cd, CalRun& run, const CalibCa
     const size_t RR = (size_t)R * R, DD = (size_t)p->D * p->D, nbs = (size_t)nb * ns;
     run.per_cta = cal_work_bytes(p->D, w->W, R);
     run.grid = (int)std::min<size_t>(CAL_GRID, nbs);
+    // The work buffers are carved from one grow-only area of the context, so that repeated
+    // calls (an optimiser's forward / backward evaluations) allocate nothing.
+    struct Piece { void** q; size_t bytes; };
+    const Piece pieces[] = {{(void**)&run.d_phase, DD * 8}, {(void**)&run.d_bead, (size_t)nb * V.pb * 8},
+                            {(void**)&run.d_slice, nbs * NOUT * 8}, {(void**)&run.d_gphi, nbs * DD * 8},
+                            {(void**)&run.d_gsum, DD * 8}, {(void**)&run.d_bgrad, (size_t)nb * V.pb * 8},
+                            {(void**)&run.d_tot, 16}, {(void**)&run.d_stacks, nbs * RR * 8},
+                            {(void**)&run.d_dz, (size_t)ns * 8}, {(void**)&run.d_G, (size_t)R * w->W * 8},
+                            {(void**)&run.d_dG, (size_t)R * w->W * 8},
+                            {(void**)&run.scratch, (size_t)CAL_GRID * run.per_cta},
+                            {(void**)&run.d_A0, cd->photons ? nbs * 8 : 0}};
+    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    size_t total = 0;
+    for (const Piece& q : pieces) total += al(q.bytes);
     cudaError_t e = cudaSuccess;
-    auto A = [&](void** q, size_t bytes) { if (e == cudaSuccess) e = run.alloc(q, bytes); };
-    A((void**)&run.d_phase, DD * 8); A((void**)&run.d_bead, (size_t)nb * V.pb * 8);
-    A((void**)&run.d_slice, nbs * NOUT * 8); A((void**)&run.d_gphi, nbs * DD * 8); A((void**)&run.d_gsum, DD * 8);
-    A((void**)&run.d_bgrad, (size_t)nb * V.pb * 8); A((void**)&run.d_tot, 16);
-    A((void**)&run.d_stacks, nbs * RR * 8); A((void**)&run.d_dz, (size_t)ns * 8);
-    A((void**)&run.d_G, (size_t)R * w->W * 8); A((void**)&run.d_dG, (size_t)R * w->W * 8);
-    A((void**)&run.scratch, (size_t)CAL_GRID * run.per_cta);
-    if (cd->photons) A((void**)&run.d_A0, nbs * 8);
+    if (total > ctx->calib_bytes) {
+        if (ctx->calib_area) {
+            cudaDeviceSynchronize();
+            cudaFree(ctx->calib_area);
+            ctx->calib_area = nullptr;
+            ctx->calib_bytes = 0;
+        }
+        e = cudaMalloc(&ctx->calib_area, total);
+        if (e == cudaSuccess) ctx->calib_bytes = total;
+    }
+    if (e == cudaSuccess) {
+        char* base = (char*)ctx->calib_area;
+        for (const Piece& q : pieces) {
+            *q.q = q.bytes ? base : nullptr;
+            base += al(q.bytes);
+        }
+    }
     if (e == cudaSuccess) e = cudaMemcpy(run.d_stacks, cd->stacks, nbs * RR * 8, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(run.d_dz, cd->dz, (size_t)ns * 8, cudaMemcpyHostToDevice);
     if (e == cudaSuccess && cd->photons) e = cudaMemcpy(run.d_A0, cd->photons, nbs * 8, cudaMemcpyHostToDevice);

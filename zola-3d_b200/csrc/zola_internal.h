@@ -118,6 +118,8 @@ struct zola_ctx {
     // results of one call; never overlaps scratch)
     void* io = nullptr;
     size_t io_bytes = 0;
+    void* calib_area = nullptr;  // calibration work buffers (grow-only, reused by every call)
+    size_t calib_bytes = 0;
     int* d_counter = nullptr;
     int* d_status_word = nullptr;
     int* h_flags = nullptr;      // pinned host words read back by the split fit loop
