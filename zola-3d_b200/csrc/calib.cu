@@ -577,6 +577,31 @@ struct CalRun {
     }
 };
 
+// Carve the buffers q[k] (bytes[k] each, 256-byte aligned) from a grow-only
+// device area of the context; repeated calls of the same size allocate nothing.
+cudaError_t carve(void** area, size_t* cap, void** const* q, const size_t* bytes, int n) {
+    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    size_t total = 0;
+    for (int k = 0; k < n; ++k) total += al(bytes[k]);
+    if (total > *cap) {
+        if (*area) {
+            cudaDeviceSynchronize();
+            cudaFree(*area);
+            *area = nullptr;
+            *cap = 0;
+        }
+        cudaError_t e = cudaMalloc(area, total);
+        if (e != cudaSuccess) return e;
+        *cap = total;
+    }
+    char* base = (char*)*area;
+    for (int k = 0; k < n; ++k) {
+        *q[k] = bytes[k] ? base : nullptr;
+        base += al(bytes[k]);
+    }
+    return cudaSuccess;
+}
+
 int cal_setup(zola_psf* p, const zola_calib_data* cd, CalRun& run, const CalibCache** cache) {
     zola_ctx* ctx = p->ctx;
     if (!cd || !cd->dz || !cd->stacks) { ctx->err = "calibration: null data"; return ZOLA_E_ARG; }
@@ -599,36 +624,14 @@ int cal_setup(zola_psf* p, const zola_calib_data* cd, CalRun& run, const CalibCa
     run.grid = (int)std::min<size_t>(CAL_GRID, nbs);
     // The work buffers are carved from one grow-only area of the context, so that repeated
     // calls (an optimiser's forward / backward evaluations) allocate nothing.
-    struct Piece { void** q; size_t bytes; };
-    const Piece pieces[] = {{(void**)&run.d_phase, DD * 8}, {(void**)&run.d_bead, (size_t)nb * V.pb * 8},
-                            {(void**)&run.d_slice, nbs * NOUT * 8}, {(void**)&run.d_gphi, nbs * DD * 8},
-                            {(void**)&run.d_gsum, DD * 8}, {(void**)&run.d_bgrad, (size_t)nb * V.pb * 8},
-                            {(void**)&run.d_tot, 16}, {(void**)&run.d_stacks, nbs * RR * 8},
-                            {(void**)&run.d_dz, (size_t)ns * 8}, {(void**)&run.d_G, (size_t)R * w->W * 8},
-                            {(void**)&run.d_dG, (size_t)R * w->W * 8},
-                            {(void**)&run.scratch, (size_t)CAL_GRID * run.per_cta},
-                            {(void**)&run.d_A0, cd->photons ? nbs * 8 : 0}};
-    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
-    size_t total = 0;
-    for (const Piece& q : pieces) total += al(q.bytes);
-    cudaError_t e = cudaSuccess;
-    if (total > ctx->calib_bytes) {
-        if (ctx->calib_area) {
-            cudaDeviceSynchronize();
-            cudaFree(ctx->calib_area);
-            ctx->calib_area = nullptr;
-            ctx->calib_bytes = 0;
-        }
-        e = cudaMalloc(&ctx->calib_area, total);
-        if (e == cudaSuccess) ctx->calib_bytes = total;
-    }
-    if (e == cudaSuccess) {
-        char* base = (char*)ctx->calib_area;
-        for (const Piece& q : pieces) {
-            *q.q = q.bytes ? base : nullptr;
-            base += al(q.bytes);
-        }
-    }
+    void** const q[] = {(void**)&run.d_phase, (void**)&run.d_bead, (void**)&run.d_slice, (void**)&run.d_gphi,
+                        (void**)&run.d_gsum, (void**)&run.d_bgrad, (void**)&run.d_tot, (void**)&run.d_stacks,
+                        (void**)&run.d_dz, (void**)&run.d_G, (void**)&run.d_dG, (void**)&run.scratch,
+                        (void**)&run.d_A0};
+    const size_t bytes[] = {DD * 8, (size_t)nb * V.pb * 8, nbs * NOUT * 8, nbs * DD * 8, DD * 8,
+                            (size_t)nb * V.pb * 8, 16, nbs * RR * 8, (size_t)ns * 8, (size_t)R * w->W * 8,
+                            (size_t)R * w->W * 8, (size_t)CAL_GRID * run.per_cta, cd->photons ? nbs * 8 : 0};
+    cudaError_t e = carve(&ctx->calib_area, &ctx->calib_bytes, q, bytes, 13);
     if (e == cudaSuccess) e = cudaMemcpy(run.d_stacks, cd->stacks, nbs * RR * 8, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(run.d_dz, cd->dz, (size_t)ns * 8, cudaMemcpyHostToDevice);
     if (e == cudaSuccess && cd->photons) e = cudaMemcpy(run.d_A0, cd->photons, nbs * 8, cudaMemcpyHostToDevice);
@@ -818,9 +821,11 @@ int zola_calib_fit(zola_psf* psf, const zola_calib_data* data, double* zernike, 
     const int nl = nzr + 4 + 1 + NPOLY, ne = nl * (nl + 1) / 2;
     double *d_dirs = nullptr, *d_tan = nullptr, *d_model = nullptr, *d_psi = nullptr, *d_gram = nullptr;
     int* d_db = nullptr;
-    if (run.alloc((void**)&d_dirs, dirs.size() * 8) || run.alloc((void**)&d_db, (size_t)ndir * 4) ||
-        run.alloc((void**)&d_tan, (size_t)ndir * nbs * RR * 8) || run.alloc((void**)&d_model, (size_t)nbs * RR * 8) ||
-        run.alloc((void**)&d_psi, (size_t)nbs * RR * 8) || run.alloc((void**)&d_gram, (size_t)nbs * ne * 8)) {
+    void** const fq[] = {(void**)&d_dirs, (void**)&d_db, (void**)&d_tan, (void**)&d_model, (void**)&d_psi,
+                         (void**)&d_gram};
+    const size_t fb[] = {dirs.size() * 8, (size_t)ndir * 4, (size_t)ndir * nbs * RR * 8, (size_t)nbs * RR * 8,
+                         (size_t)nbs * RR * 8, (size_t)nbs * ne * 8};
+    if (carve(&ctx->calib_fit_area, &ctx->calib_fit_bytes, fq, fb, 6) != cudaSuccess) {
         ctx->err = "zola_calib_fit: device memory";
         return ZOLA_E_CUDA;
     }

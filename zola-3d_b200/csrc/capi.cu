@@ -148,6 +148,7 @@ int zola_ctx_destroy(zola_ctx* ctx) {
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->io) cudaFree(ctx->io);
     if (ctx->calib_area) cudaFree(ctx->calib_area);
+    if (ctx->calib_fit_area) cudaFree(ctx->calib_fit_area);
     if (ctx->d_counter) cudaFree(ctx->d_counter);
     if (ctx->h_flags) cudaFreeHost(ctx->h_flags);
     if (ctx->h_feed) cudaFreeHost(ctx->h_feed);

@@ -120,6 +120,8 @@ struct zola_ctx {
     size_t io_bytes = 0;
     void* calib_area = nullptr;  // calibration work buffers (grow-only, reused by every call)
     size_t calib_bytes = 0;
+    void* calib_fit_area = nullptr;  // the calibration LM's tangents, Gram blocks and model (grow-only)
+    size_t calib_fit_bytes = 0;
     int* d_counter = nullptr;
     int* d_status_word = nullptr;
     int* h_flags = nullptr;      // pinned host words read back by the split fit loop
