@@ -459,11 +459,12 @@ ZOLA_API int zola_psf_center_search(zola_psf* psf, int R, double axial_range, in
 /* Per-kernel timing.  With profiling on, every kernel launch of a fit or model
  * call is bracketed by CUDA events on its stream and the elapsed device time is
  * accumulated per kernel kind: 0..3 the split stages (pupil DFT, window DFT,
- * row blur, column blur with likelihood sums and LM step; the model-only
- * column blur), 4 the fused stages 2-5, 5 the FP64 fit, 6 the FP64 model, 7
- * other, 8 the dataflow split fit.  zola_ctx_stage_stats copies ZOLA_NSTAGES
- * millisecond totals and launch counts (either pointer may be null). */
-#define ZOLA_NSTAGES 9
+ * row blur, column blur with likelihood sums; the model-only column blur), 4
+ * the fused stages 2-5, 5 the FP64 fit, 6 the FP64 model, 7 the split fit's LM
+ * step and other kernels, 8 the dataflow split fit, 9 detection.
+ * zola_ctx_stage_stats copies ZOLA_NSTAGES millisecond totals and launch
+ * counts (either pointer may be null). */
+#define ZOLA_NSTAGES 10
 ZOLA_API int zola_ctx_profile(zola_ctx* ctx, int enable);
 ZOLA_API int zola_ctx_stage_stats(zola_ctx* ctx, double* ms, long long* launches, int reset);
 

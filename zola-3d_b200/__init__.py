@@ -85,7 +85,7 @@ EXPORTS = ["zola_ctx_create", "zola_ctx_destroy", "zola_last_error", "zola_ctx_s
            "zola_ctx_set_round_graphs"]
 STAGES = ["split_stage1_pupil_dft", "split_stage2_window_dft", "split_stage3_blur_rows",
           "split_stage4_blur_cols_sums_lm", "split_fused_stages2_5", "fp64_fit", "fp64_model", "other",
-          "split_dataflow"]
+          "split_dataflow", "detect"]
 
 _lib = None
 

@@ -522,7 +522,7 @@ int zola_detect_dev(zola_detector* d, const double* d_frames, int nframes, int c
         double* gs = gsort ? (double*)b : nullptr;
         int* gid = gsort ? (int*)(gs + (size_t)nf * p2) : nullptr;
         const double* fr = d_frames + (size_t)f0 * SS;
-        prof_begin(ctx, 7, st);
+        prof_begin(ctx, 9, st);
         k_det_var<<<nf, 256, 0, st>>>(v, fr, rowsum, rowsq, var);
         // slices per register-tiled CTA: as many (up to RZC) as keep two CTAs per SM
         int zrt = RZC;

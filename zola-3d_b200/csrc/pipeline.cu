@@ -486,18 +486,35 @@ int localize_impl(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const do
         if (e != cudaSuccess) return fail(e);
         const int longest = *std::max_element(counts.begin(), counts.end());
         det->cand_room = std::max(det->cand_room, longest);
-        if (longest > cap) {  // room for every candidate, then detect this batch again
+        if (longest > cap) {  // room for every candidate; the frames whose list was cut are detected again
             if (longest > ZOLA_DETECT_MAX_CAP) {
                 ctx->err = "zola_localize_frames: a frame has more than 2^20 candidates";
                 return ZOLA_E_ARG;
             }
+            const int old = cap;
             cap = longest;
-            A(b_cand, (size_t)FB * cap * 7 * 8); A(b_cslot, (size_t)FB * cap * 4); A(b_cmax, (size_t)FB * cap * 8);
+            {
+                // the stored rows move to the wider layout; the frames whose whole list
+                // fitted keep them (detection is per frame, so they would come out the same)
+                Buf wide;
+                e = wide.alloc((size_t)FB * cap * 7 * 8);
+                if (e == cudaSuccess)
+                    e = cudaMemcpy2DAsync(wide.p, (size_t)cap * 7 * 8, b_cand.p, (size_t)old * 7 * 8,
+                                          (size_t)old * 7 * 8, nf, cudaMemcpyDeviceToDevice, st);
+                if (e != cudaSuccess) return fail(e);
+                std::swap(b_cand.p, wide.p);
+                std::swap(b_cand.bytes, wide.bytes);
+            }  // (freeing the old rows waits for the copy)
+            A(b_cslot, (size_t)FB * cap * 4); A(b_cmax, (size_t)FB * cap * 8);
             if (e != cudaSuccess) return fail(e);
             V.cap = cap;
             V.cand = (double*)b_cand.p; V.cand_slot = (int*)b_cslot.p; V.cand_maxp = (double*)b_cmax.p;
-            rc = zola_detect_dev(det, (double*)b_img.p, nf, cap, (double*)b_cand.p, (int*)b_cnt.p, st);
-            if (rc) return rc;
+            for (int f = 0; f < nf; ++f) {
+                if (counts[f] <= old) continue;
+                rc = zola_detect_dev(det, (double*)b_img.p + (size_t)f * SS, 1, cap, (double*)b_cand.p + (size_t)f * cap * 7,
+                                     (int*)b_cnt.p + f, st);
+                if (rc) return rc;
+            }
         }
         for (int wave = 0;; ++wave) {
             e = cudaMemsetAsync(b_ns.p, 0, 4, st);
