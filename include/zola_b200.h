@@ -239,7 +239,7 @@ typedef struct {
     int max_iter;             /* LM evaluations per ROI */
     double tol_xyz;           /* LM stopping distance, um */
     int precision;            /* ZOLA_PREC_FP64 or ZOLA_PREC_SPLIT for the fits */
-    int cand_cap;             /* candidates stored per frame at the start (0: 4096); it grows to the
+    int cand_cap;             /* candidates stored per frame at the start (0: 8192); it grows to the
                                  longest list so that every frame walks its whole list */
     int frames_per_batch;     /* frames per device batch (0: 1024) */
     int wave_fits;            /* candidates fitted ahead per frame and wave (0: 8); any value gives the

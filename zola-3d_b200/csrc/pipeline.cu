@@ -364,6 +364,9 @@ struct Buf {
 };
 
 constexpr int PIPE_WAVE_FITS = 8;  // speculative fits per frame and wave
+// Candidates stored per frame at the start of a call: a 256 x 256 frame against a
+// 41-slice library lists up to about 7,500 at the reference's threshold.
+constexpr int PIPE_CAND_ROOM = 8192;
 
 }  // namespace
 
@@ -403,7 +406,7 @@ int localize_impl(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const do
     const std::vector<double>& lib = det->h_psf;
     // candidates stored per frame: grows to the longest list met, so that every
     // frame walks its whole list as the reference does
-    int cap = prm->cand_cap > 0 ? prm->cand_cap : std::max(4096, det->cand_room);
+    int cap = prm->cand_cap > 0 ? prm->cand_cap : std::max(PIPE_CAND_ROOM, det->cand_room);
     if (cap > ZOLA_DETECT_MAX_CAP) { ctx->err = "zola_localize_frames: cand_cap above 2^20"; return ZOLA_E_ARG; }
     const int FB = std::max(1, std::min(nframes, prm->frames_per_batch > 0 ? prm->frames_per_batch : 1024));
     const size_t SS = (size_t)SX * SY, RR = (size_t)R * R;
@@ -509,13 +512,29 @@ int localize_impl(zola_ctx* ctx, zola_detector* det, zola_psf* fit_psf, const do
             if (e != cudaSuccess) return fail(e);
             V.cap = cap;
             V.cand = (double*)b_cand.p; V.cand_slot = (int*)b_cslot.p; V.cand_maxp = (double*)b_cmax.p;
-            for (int f = 0; f < nf; ++f) {
-                if (counts[f] <= old) continue;
-                rc = zola_detect_dev(det, (double*)b_img.p + (size_t)f * SS, 1, cap, (double*)b_cand.p + (size_t)f * cap * 7,
-                                     (int*)b_cnt.p + f, st);
-                if (rc) return rc;
+            // the cut frames, gathered, are detected again as one batch and their rows scattered back
+            std::vector<int> cut;
+            for (int f = 0; f < nf; ++f)
+                if (counts[f] > old) cut.push_back(f);
+            const size_t nc = cut.size();
+            Buf g_img, g_out, g_cnt;
+            e = g_img.alloc(nc * SS * 8);
+            if (e == cudaSuccess) e = g_out.alloc(nc * (size_t)cap * 7 * 8);
+            if (e == cudaSuccess) e = g_cnt.alloc(nc * 4);
+            for (size_t k = 0; k < nc && e == cudaSuccess; ++k)
+                e = cudaMemcpyAsync((double*)g_img.p + k * SS, (double*)b_img.p + (size_t)cut[k] * SS, SS * 8,
+                                    cudaMemcpyDeviceToDevice, st);
+            if (e != cudaSuccess) return fail(e);
+            rc = zola_detect_dev(det, (double*)g_img.p, (int)nc, cap, (double*)g_out.p, (int*)g_cnt.p, st);
+            if (rc) return rc;
+            for (size_t k = 0; k < nc && e == cudaSuccess; ++k) {
+                e = cudaMemcpyAsync((double*)b_cand.p + (size_t)cut[k] * cap * 7, (double*)g_out.p + k * cap * 7,
+                                    (size_t)cap * 7 * 8, cudaMemcpyDeviceToDevice, st);
+                if (e == cudaSuccess)
+                    e = cudaMemcpyAsync((int*)b_cnt.p + cut[k], (int*)g_cnt.p + k, 4, cudaMemcpyDeviceToDevice, st);
             }
-        }
+            if (e != cudaSuccess) return fail(e);
+        }  // (freeing the gathered buffers waits for the copies)
         for (int wave = 0;; ++wave) {
             e = cudaMemsetAsync(b_ns.p, 0, 4, st);
             if (e == cudaSuccess) e = cudaMemsetAsync(b_nacc.p, 0, 4, st);
