@@ -170,3 +170,25 @@ def test_uint16_frames_equal_photon_frames(zpkg, ctx):
     assert len(r64) >= 5
     assert np.array_equal(r16, r64)
     det.close()
+
+
+def test_candidate_room_growth_does_not_change_the_rows(zpkg, ctx):
+    """A small starting room makes every frame's candidate list outgrow it: the
+    pipeline widens the room and detects only the cut frames again (gathered
+    into one batch), and the rows equal those of a room that fits at once."""
+    zern = astig_zernike()
+    S, R = 96, 16
+    psf_det = zpkg.PSF(ctx, zpkg.optics(size_fft=64, kz_reset=True, **OPTICS), zern)
+    psf_fit = zpkg.PSF(ctx, zpkg.optics(size_fft=64, **OPTICS), zern)
+    ref_fit = O.OraclePSF(64, 0.11, 1.4, 0.66, 1.518, 1.518, 0.9, zern)
+    frames = make_frames(ref_fit.model, S, 5, seed=271, emitters=4, R=32)
+    kw = dict(photon_threshold=300.0, precision=1, max_iter=40)
+    rows = []
+    for room in (16384, 32):
+        det = zpkg.Detector(psf_det, S, S, R, -0.6, 0.6, 0.11, 0.1)  # (a fresh detector keeps no room of its own)
+        _, counts = det.detect(frames, cap=16384)
+        assert counts.max() > 32
+        rows.append(zpkg.localize_frames(ctx, det, psf_fit, frames, -0.6, 0.6, cand_cap=room, **kw))
+        det.close()
+    assert len(rows[0]) >= 5
+    assert np.array_equal(rows[0], rows[1])
