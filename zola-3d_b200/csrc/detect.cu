@@ -182,6 +182,8 @@ __global__ void __launch_bounds__(256, 2) k_det_corr_rt(DetView V, int zc, const
         double w[RPX];
 #pragma unroll
         for (int k = 0; k < RPX; ++k) w[k] = trow[k];
+        // unrolled by the window width: the window's shifts become register renames
+#pragma unroll 8
         for (int v = 0; v < R; ++v) {
             double p[RZC];
 #pragma unroll
