@@ -118,23 +118,39 @@ __device__ void eval_maps_f64(const PsfView& P, const WinView& Wn, const F64Work
     double2* S = w.S;
     double2* Sy = w.S + (size_t)D * W;
     double2* Sz = w.S + (size_t)2 * D * W;
-    for (int idx = tid; idx < D * W; idx += nt) {
-        int a = idx / W, j = idx - a * W;
-        double2 s = make_double2(0, 0), sy = make_double2(0, 0), sz = make_double2(0, 0);
+    // a thread takes 4 rows a of one column j: each C value it loads serves 4 outputs
+    // (every output still sums its terms in the order b = 0, 1, ...)
+    constexpr int TA = 4;
+    const int DA = (D + TA - 1) / TA;
+    for (int idx = tid; idx < DA * W; idx += nt) {
+        const int a0 = (idx / W) * TA, j = idx - (idx / W) * W;
+        double2 s[TA], sy[TA], sz[TA];
+#pragma unroll
+        for (int t = 0; t < TA; ++t) { s[t] = make_double2(0, 0); sy[t] = make_double2(0, 0); sz[t] = make_double2(0, 0); }
         const double2* crow = Wn.C + (size_t)j * D;
-        const double2* qrow = w.Q + (size_t)a * D;
         for (int b = 0; b < D; ++b) {
-            double2 c = crow[b], q = qrow[b];
-            double2 qc = cmul(q, c);
-            s.x += qc.x; s.y += qc.y;
-            if (derivs) {
-                double ky = P.ky[b], kz = P.kz[a * D + b];
-                sy.x -= ky * qc.y; sy.y += ky * qc.x;   // (i ky) q c
-                sz.x -= kz * qc.y; sz.y += kz * qc.x;   // (i kz) q c
+            const double2 c = crow[b];
+            const double ky = P.ky[b];
+#pragma unroll
+            for (int t = 0; t < TA; ++t) {
+                if (a0 + t >= D) break;
+                const double2 q = w.Q[(size_t)(a0 + t) * D + b];
+                const double2 qc = cmul(q, c);
+                s[t].x += qc.x; s[t].y += qc.y;
+                if (derivs) {
+                    const double kz = P.kz[(a0 + t) * D + b];
+                    sy[t].x -= ky * qc.y; sy[t].y += ky * qc.x;   // (i ky) q c
+                    sz[t].x -= kz * qc.y; sz[t].y += kz * qc.x;   // (i kz) q c
+                }
             }
         }
-        S[idx] = s;
-        if (derivs) { Sy[idx] = sy; Sz[idx] = sz; }
+#pragma unroll
+        for (int t = 0; t < TA; ++t) {
+            if (a0 + t >= D) break;
+            const size_t o = (size_t)(a0 + t) * W + j;
+            S[o] = s[t];
+            if (derivs) { Sy[o] = sy[t]; Sz[o] = sz[t]; }
+        }
     }
     __syncthreads();
     // 3. second contraction over pupil rows a, then intensities
@@ -142,39 +158,63 @@ __device__ void eval_maps_f64(const PsfView& P, const WinView& Wn, const F64Work
     double* I1 = w.I + (size_t)W * W;
     double* I2 = w.I + (size_t)2 * W * W;
     double* I3 = w.I + (size_t)3 * W * W;
-    for (int idx = tid; idx < W * W; idx += nt) {
-        int i = idx / W, j = idx - i * W;
-        double2 e = make_double2(0, 0), ex = make_double2(0, 0), ey = make_double2(0, 0), ez = make_double2(0, 0);
-        const double2* crow = Wn.C + (size_t)i * D;
+    // a thread takes 4 rows i of one column j: each S, S_y, S_z value it loads serves 4
+    // outputs (every output still sums its terms in the order a = 0, 1, ...)
+    constexpr int TI = 4;
+    for (int idx = tid; idx < (W / TI) * W; idx += nt) {
+        const int i0 = (idx / W) * TI, j = idx - (idx / W) * W;
+        double2 e[TI], ex[TI], ey[TI], ez[TI];
+#pragma unroll
+        for (int t = 0; t < TI; ++t) {
+            e[t] = make_double2(0, 0); ex[t] = make_double2(0, 0); ey[t] = make_double2(0, 0); ez[t] = make_double2(0, 0);
+        }
         for (int a = 0; a < D; ++a) {
-            double2 c = crow[a];
-            double2 s = S[(size_t)a * W + j];
-            double2 cs = cmul(c, s);
-            e.x += cs.x; e.y += cs.y;
-            if (derivs) {
-                double kx = P.kx[a];
-                ex.x -= kx * cs.y; ex.y += kx * cs.x;
-                ey = cmadd(ey, c, Sy[(size_t)a * W + j]);
-                ez = cmadd(ez, c, Sz[(size_t)a * W + j]);
+            const double2 s = S[(size_t)a * W + j];
+            double2 sy, sz;
+            double kx = 0;
+            if (derivs) { sy = Sy[(size_t)a * W + j]; sz = Sz[(size_t)a * W + j]; kx = P.kx[a]; }
+#pragma unroll
+            for (int t = 0; t < TI; ++t) {
+                const double2 c = Wn.C[(size_t)(i0 + t) * D + a];
+                const double2 cs = cmul(c, s);
+                e[t].x += cs.x; e[t].y += cs.y;
+                if (derivs) {
+                    ex[t].x -= kx * cs.y; ex[t].y += kx * cs.x;
+                    ey[t] = cmadd(ey[t], c, sy);
+                    ez[t] = cmadd(ez[t], c, sz);
+                }
             }
         }
-        I0[idx] = e.x * e.x + e.y * e.y;
-        if (derivs) {
-            I1[idx] = 2.0 * (e.x * ex.x + e.y * ex.y);
-            I2[idx] = 2.0 * (e.x * ey.x + e.y * ey.y);
-            I3[idx] = 2.0 * (e.x * ez.x + e.y * ez.y);
+#pragma unroll
+        for (int t = 0; t < TI; ++t) {
+            const size_t o = (size_t)(i0 + t) * W + j;
+            I0[o] = e[t].x * e[t].x + e[t].y * e[t].y;
+            if (derivs) {
+                I1[o] = 2.0 * (e[t].x * ex[t].x + e[t].y * ex[t].y);
+                I2[o] = 2.0 * (e[t].x * ey[t].x + e[t].y * ey[t].y);
+                I3[o] = 2.0 * (e[t].x * ez[t].x + e[t].y * ez[t].y);
+            }
         }
     }
     __syncthreads();
     // 4. blur along the first index: J[m][i'][j] = sum_i G[i'][i] I[m][i][j]
     const int nm = derivs ? 4 : 1;
-    for (int idx = tid; idx < nm * R * W; idx += nt) {
-        int m = idx / (R * W), rem = idx - m * R * W, ip = rem / W, j = rem - ip * W;
-        const double* g = Wn.G + (size_t)ip * W;
+    // a thread takes 4 rows i' of one column j (each I value loaded serves 4 outputs)
+    constexpr int TR = 4;
+    const int RB = (R + TR - 1) / TR;
+    for (int idx = tid; idx < nm * RB * W; idx += nt) {
+        const int m = idx / (RB * W), rem = idx - m * RB * W, ip0 = (rem / W) * TR, j = rem - (rem / W) * W;
         const double* Im = w.I + (size_t)m * W * W;
-        double acc = 0.0;
-        for (int i = 0; i < W; ++i) acc = fma(g[i], Im[(size_t)i * W + j], acc);
-        w.J[idx] = acc;
+        double acc[TR] = {0.0, 0.0, 0.0, 0.0};
+        for (int i = 0; i < W; ++i) {
+            const double v = Im[(size_t)i * W + j];
+#pragma unroll
+            for (int t = 0; t < TR; ++t)
+                if (ip0 + t < R) acc[t] = fma(Wn.G[(size_t)(ip0 + t) * W + i], v, acc[t]);
+        }
+#pragma unroll
+        for (int t = 0; t < TR; ++t)
+            if (ip0 + t < R) w.J[((size_t)m * R + ip0 + t) * W + j] = acc[t];
     }
     __syncthreads();
     // 5. blur along the second index: T[m][i'][j'] = sum_j G[j'][j] J[m][i'][j]
