@@ -873,18 +873,20 @@ def main():
         host.append((r.numpy(), i0.numpy(), res))
         h2d += r.numel() * 4 + i0.numel() * 8
         d2h += m * (5 * 8 + 5 * 8 + 8 + 4 + 4)
-    # one untimed pass sizes the library's staging area, then the timed pass (inputs
-    # and results in pinned host memory)
-    for j, (r, i0, res) in zip(job, host):
-        j["psf"].fit(r, i0, z.PSF.fit_params(precision=z.ZOLA_PREC_SPLIT, **j["prm_kw"]), out=res)
+    # one mixed call from host memory (zola_fit_batch_mixed: each class's H2D copy on the
+    # copy stream overlaps the fits of the classes copied before it); one untimed pass
+    # sizes the library's staging area, then the timed pass (inputs and results pinned)
+    mixed = [dict(psf=j["psf"], rois=r, init=i0, out=res,
+                  prm=z.PSF.fit_params(precision=z.ZOLA_PREC_SPLIT, **j["prm_kw"]))
+             for j, (r, i0, res) in zip(job, host)]
+    z.fit_mixed(ctx, mixed)
     torch.cuda.synchronize()
     rp.barrier()
     t0 = time.perf_counter()
-    for j, (r, i0, res) in zip(job, host):
-        j["psf"].fit(r, i0, z.PSF.fit_params(precision=z.ZOLA_PREC_SPLIT, **j["prm_kw"]), out=res)
+    z.fit_mixed(ctx, mixed)
     t_e2e = rp.max_over_ranks(time.perf_counter() - t0, device)
     e2e = {"value": n_total * world / t_e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-           "d2h_bytes_per_step": int(d2h)}
+           "d2h_bytes_per_step": int(d2h), "call": "zola_fit_batch_mixed"}
 
     detect = detect_fit_config(z, ctx, torch, device, args.detect_frames, args.detect_fp64_frames, seed=1 + rank) \
         if args.detect_frames > 0 else None

@@ -170,6 +170,12 @@ typedef struct {
     int *d_status, *d_iters;           /* nullable */
 } zola_fit_class;
 ZOLA_API int zola_fit_batch_mixed_dev(zola_ctx* ctx, const zola_fit_class* classes, int nclass, void* stream);
+/* Host-buffer form of the mixed batch: the d_* fields of each class point to
+ * HOST memory here (pinned memory lets the copies overlap the fits).  The
+ * inputs go up on the context's copy stream, the smallest class first, and
+ * each class starts fitting as soon as its own inputs have landed; the results
+ * come back before the call returns. */
+ZOLA_API int zola_fit_batch_mixed(zola_ctx* ctx, const zola_fit_class* classes, int nclass);
 
 /* sCMOS form (process/cpu/Localization.java:1132, utils/SCMOScamera.java):
  * scmos holds, per ROI pixel, var/gain^2 of the camera pixel; it is added to

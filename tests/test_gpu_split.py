@@ -313,14 +313,39 @@ def test_mixed_batch_equals_per_class_calls(zpkg, ctx):
         torch.cuda.synchronize()
         zpkg.fit_mixed_dev(ctx, classes, stream=ctx.stream)
         torch.cuda.synchronize()
+        # the same classes from host memory (zola_fit_batch_mixed): plain numpy inputs and
+        # results, copies staged by the library
+        hosted = []
+        for c in classes:
+            n = c["rois"].shape[0]
+            hosted.append(dict(psf=c["psf"], rois=c["rois"].cpu().numpy(), init=c["init"].cpu().numpy(), prm=c["prm"],
+                               out=dict(theta=np.zeros((n, 5)), crlb=np.zeros((n, 5)), nll=np.zeros(n),
+                                        status=np.zeros(n, np.int32), iters=np.zeros(n, np.int32))))
+        zpkg.fit_mixed(ctx, hosted)
     finally:
         ctx.set_pool(0)
-    for c, w in zip(classes, want):
+    for c, h, w in zip(classes, hosted, want):
         assert np.array_equal(c["out"].cpu().numpy(), w["theta"])
         assert np.array_equal(np.nan_to_num(c["crlb"].cpu().numpy()), np.nan_to_num(w["crlb"]))
         assert np.array_equal(c["status"].cpu().numpy(), w["status"])
         assert np.array_equal(c["iters"].cpu().numpy(), w["iters"])
+        for key in ("theta", "nll", "status", "iters"):
+            assert np.array_equal(h["out"][key], w[key]), key
+        assert np.array_equal(np.nan_to_num(h["out"]["crlb"]), np.nan_to_num(w["crlb"]))
         c["psf"].close()
+
+
+def test_host_mixed_batch_rejects_bad_results(zpkg, ctx):
+    """zola_fit_batch_mixed with a wrong-shaped result array is refused on the host
+    before any copy; a class with no ROIs is accepted and left untouched."""
+    psf = make(zpkg, ctx, 64, astig_zernike())
+    prm = zpkg.PSF.fit_params(-1.5, 1.5, 0.88, precision=zpkg.ZOLA_PREC_SPLIT)
+    rois = np.zeros((4, 16, 16), np.float32)
+    init = np.zeros((4, 5))
+    with pytest.raises(ValueError):
+        zpkg.fit_mixed(ctx, [dict(psf=psf, rois=rois, init=init, prm=prm, out=dict(theta=np.zeros((3, 5))))])
+    zpkg.fit_mixed(ctx, [dict(psf=psf, rois=rois[:0], init=init[:0], prm=prm, out=dict(theta=np.zeros((0, 5))))])
+    psf.close()
 
 
 def test_round_graphs_equal_direct_launches(zpkg, ctx):

@@ -82,7 +82,7 @@ EXPORTS = ["zola_ctx_create", "zola_ctx_destroy", "zola_last_error", "zola_ctx_s
            "zola_fit_batch_scmos_dev", "zola_localize_frames_scmos", "zola_ctx_set_flow", "zola_ctx_set_wait_limit",
            "zola_fit_batch_stream_dev", "zola_ctx_set_tuning", "zola_fit_flow_shape", "zola_ctx_flow_stats",
            "zola_fit_batch_mixed_dev", "zola_detect_u16", "zola_localize_frames_u16", "zola_fit_split_pool",
-           "zola_ctx_set_round_graphs"]
+           "zola_ctx_set_round_graphs", "zola_fit_batch_mixed"]
 STAGES = ["split_stage1_pupil_dft", "split_stage2_window_dft", "split_stage3_blur_rows",
           "split_stage4_blur_cols_sums_lm", "split_fused_stages2_5", "fp64_fit", "fp64_model", "other",
           "split_dataflow", "detect"]
@@ -123,6 +123,7 @@ def lib():
         L.zola_fit_split_pool.argtypes = [vp, i, vp, vp]
         L.zola_ctx_set_round_graphs.argtypes = [vp, i]
         L.zola_fit_batch_mixed_dev.argtypes = [vp, vp, i, vp]
+        L.zola_fit_batch_mixed.argtypes = [vp, vp, i]
         L.zola_crlb_curve.argtypes = [vp, i, vp, i, d, d, d, d, vp]
         L.zola_psf_center_search.argtypes = [vp, i, d, i, ctypes.POINTER(d)]
         L.zola_ctx_profile.argtypes = [vp, i]
@@ -660,6 +661,33 @@ def fit_mixed_dev(ctx, classes, stream=None):
                             for x in ("crlb", "nll", "status", "iters")])
     ctx.check(lib().zola_fit_batch_mixed_dev(ctx.h, ctypes.cast(arr, ctypes.c_void_p), len(classes), stream),
               "zola_fit_batch_mixed_dev")
+
+
+def fit_mixed(ctx, classes):
+    """Mixed batch from host memory (zola_fit_batch_mixed): classes is a list of dicts with psf, rois (n, R, R)
+    float32, init (n, 5) float64, prm (split precision) and out, a dict of host result arrays as PSF.fit takes
+    (theta (n, 5); crlb (n, 5), nll, status, iters optional).  Pinned arrays let the copies overlap the fits."""
+    arr = (FitClass * max(1, len(classes)))()
+    keep = []
+    for k, c in enumerate(classes):
+        rois = np.ascontiguousarray(c["rois"], dtype=np.float32)
+        init = np.ascontiguousarray(c["init"], dtype=np.float64)
+        keep += [rois, init]
+        res = c["out"]
+        n = rois.shape[0]
+        for key, shape, dt in (("theta", (n, 5), np.float64), ("crlb", (n, 5), np.float64), ("nll", (n,), np.float64),
+                               ("status", (n,), np.int32), ("iters", (n,), np.int32)):
+            a = res.get(key)
+            if a is None and key != "theta":
+                continue
+            if a is None or a.shape != shape or a.dtype != dt or not a.flags["C_CONTIGUOUS"]:
+                raise ValueError(f"out[{key!r}] must be a C-contiguous {np.dtype(dt).name} array of shape {shape}")
+        arr[k] = FitClass(c["psf"].h.value if hasattr(c["psf"].h, "value") else c["psf"].h, int(rois.shape[1]), n,
+                          rois.ctypes.data, init.ctypes.data, c["prm"], res["theta"].ctypes.data,
+                          *[res[x].ctypes.data if res.get(x) is not None else None
+                            for x in ("crlb", "nll", "status", "iters")])
+    ctx.check(lib().zola_fit_batch_mixed(ctx.h, ctypes.cast(arr, ctypes.c_void_p), len(classes)),
+              "zola_fit_batch_mixed")
 
 
 def fit_noalloc_dev(psf, rois, init, prm, out, crlb=None, nll=None, status=None, iters=None, stream=None):

@@ -3,6 +3,8 @@
 // arguments and reports failures through the return code and zola_last_error.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include <cstring>
 #include <new>
 
@@ -400,6 +402,9 @@ int fit_dev_impl(zola_ctx* ctx, zola_psf* psf, int R, const float* d_rois, const
     return launch_fit_f64(ctx, psf, w, d_rois, d_scmos, d_init5, n, prm, d_out5, d_crlb5, d_nll, d_status, d_iters, st);
 }
 
+int mixed_dev_impl(zola_ctx* ctx, const zola_fit_class* classes, int nclass, cudaStream_t st,
+                   const cudaEvent_t* ready);
+
 int fit_host_impl(zola_ctx* ctx, zola_psf* psf, int R, const float* rois, const float* scmos, const double* init5,
                   int n, const zola_fit_params* prm, double* out5, double* crlb5, double* nll, int* status,
                   int* iters) {
@@ -489,29 +494,128 @@ int zola_fit_batch_stream_dev(zola_ctx* ctx, zola_psf* psf, int R, const float* 
 int zola_fit_batch_mixed_dev(zola_ctx* ctx, const zola_fit_class* classes, int nclass, void* stream) {
     if (!ctx || nclass < 0 || nclass > ZOLA_MAX_CLASSES || (nclass > 0 && !classes)) return ZOLA_E_ARG;
     cudaSetDevice(ctx->device);
+    return mixed_dev_impl(ctx, classes, nclass, stream ? (cudaStream_t)stream : ctx->stream, nullptr);
+}
+
+}  // extern "C"
+
+namespace {
+
+// ready (nullable): per class, an event after which its inputs are on the device
+// One class of a mixed batch: its PSF, parameters and buffers, and the window
+// tables of its ROI size (built here when missing).
+int check_mixed_class(zola_ctx* ctx, const zola_fit_class& k, WindowTables** w) {
+    if (!k.psf || k.psf->ctx != ctx) return set_err(ctx, ZOLA_E_ARG, "zola_fit_batch_mixed: bad PSF");
+    if (!check_fit_params(ctx, &k.prm)) return ZOLA_E_ARG;
+    if (k.prm.precision != ZOLA_PREC_SPLIT)
+        return set_err(ctx, ZOLA_E_ARG, "zola_fit_batch_mixed: every class needs split precision");
+    if (k.n < 0 || (k.n > 0 && (!k.d_rois || !k.d_init5 || !k.d_out5)))
+        return set_err(ctx, ZOLA_E_ARG, "zola_fit_batch_mixed: bad n or null buffer");
+    if (k.psf->o.kz_reset)
+        return set_err(ctx, ZOLA_E_ARG, "fit needs a PSF built with kz_reset = 0 (the fit model tables)");
+    *w = get_window(k.psf, k.R, ctx->err);
+    return *w ? ZOLA_OK : ZOLA_E_ARG;
+}
+
+int mixed_dev_impl(zola_ctx* ctx, const zola_fit_class* classes, int nclass, cudaStream_t st,
+                   const cudaEvent_t* ready) {
     zola::MixedClass mc[ZOLA_MAX_CLASSES];
+    cudaEvent_t rdy[ZOLA_MAX_CLASSES];
     int m = 0;
     for (int c = 0; c < nclass; ++c) {
         const zola_fit_class& k = classes[c];
-        if (!k.psf || k.psf->ctx != ctx) return set_err(ctx, ZOLA_E_ARG, "zola_fit_batch_mixed_dev: bad PSF");
-        if (!check_fit_params(ctx, &k.prm)) return ZOLA_E_ARG;
-        if (k.prm.precision != ZOLA_PREC_SPLIT)
-            return set_err(ctx, ZOLA_E_ARG, "zola_fit_batch_mixed_dev: every class needs split precision");
-        if (k.n < 0 || (k.n > 0 && (!k.d_rois || !k.d_init5 || !k.d_out5)))
-            return set_err(ctx, ZOLA_E_ARG, "zola_fit_batch_mixed_dev: bad n or null buffer");
-        if (k.psf->o.kz_reset)
-            return set_err(ctx, ZOLA_E_ARG, "fit needs a PSF built with kz_reset = 0 (the fit model tables)");
-        WindowTables* w = get_window(k.psf, k.R, ctx->err);
-        if (!w) return ZOLA_E_ARG;
+        WindowTables* w = nullptr;
+        if (int rc = check_mixed_class(ctx, k, &w)) return rc;
         if (k.n == 0) continue;
         const zola_fit_params& pr = k.prm;
         zola::FitParamsDev fp{pr.zmin, pr.zmax, pr.xymax, pr.tol_xyz, pr.step_xy, pr.step_z, pr.max_iter, 1e-3};
+        if (ready) rdy[m] = ready[c];
         mc[m++] = zola::MixedClass{k.psf, w,
                                    zola::FitIO{k.d_rois, nullptr, k.d_init5, k.n, fp, k.d_out5, k.d_crlb5, k.d_nll,
                                                k.d_status, k.d_iters}};
     }
     if (m == 0) return ZOLA_OK;
-    return zola::launch_fit_split_mixed(ctx, m, mc, stream ? (cudaStream_t)stream : ctx->stream);
+    return zola::launch_fit_split_mixed(ctx, m, mc, st, ready ? rdy : nullptr);
+}
+
+}  // namespace
+
+extern "C" {
+
+int zola_fit_batch_mixed(zola_ctx* ctx, const zola_fit_class* classes, int nclass) {
+    if (!ctx || nclass < 0 || nclass > ZOLA_MAX_CLASSES || (nclass > 0 && !classes)) return ZOLA_E_ARG;
+    cudaSetDevice(ctx->device);
+    // staging layout per class: rois | init | out | crlb | nll | status | iters
+    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    size_t off[ZOLA_MAX_CLASSES][8] = {};
+    size_t total = 0;
+    for (int c = 0; c < nclass; ++c) {
+        const zola_fit_class& k = classes[c];
+        WindowTables* w = nullptr;  // every class is checked before the first copy reads a host buffer
+        if (int rc = check_mixed_class(ctx, k, &w)) return rc;
+        const size_t n = (size_t)k.n, rr = (size_t)k.R * k.R;
+        const size_t sz[7] = {rr * n * 4, n * 40, n * 40, k.d_crlb5 ? n * 40 : 0, k.d_nll ? n * 8 : 0,
+                              k.d_status ? n * 4 : 0, k.d_iters ? n * 4 : 0};
+        for (int q = 0; q < 7; ++q) {
+            off[c][q] = total;
+            total += al(sz[q]);
+        }
+    }
+    if (total == 0) return ZOLA_OK;
+    if (ensure_io(ctx, total)) return ZOLA_E_CUDA;
+    char* base = (char*)ctx->io;
+    while ((int)ctx->feed_ev.size() < ZOLA_MAX_CLASSES) {
+        cudaEvent_t e;
+        ZOLA_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), ctx);
+        ctx->feed_ev.push_back(e);
+    }
+    // inputs go up on the copy stream, the smallest class first, so that the first
+    // classes start fitting while the larger ones are still being copied
+    int order[ZOLA_MAX_CLASSES];
+    for (int c = 0; c < nclass; ++c) order[c] = c;
+    std::sort(order, order + nclass, [&](int x, int y) {
+        return (size_t)classes[x].n * classes[x].R * classes[x].R < (size_t)classes[y].n * classes[y].R * classes[y].R;
+    });
+    cudaStream_t cs = ctx->copy_stream;
+    for (int oc = 0; oc < nclass; ++oc) {
+        const int c = order[oc];
+        const zola_fit_class& k = classes[c];
+        const size_t n = (size_t)k.n, rr = (size_t)k.R * k.R;
+        if (n > 0) {
+            ZOLA_CUDA_CHECK(cudaMemcpyAsync(base + off[c][0], k.d_rois, rr * n * 4, cudaMemcpyHostToDevice, cs), ctx);
+            ZOLA_CUDA_CHECK(cudaMemcpyAsync(base + off[c][1], k.d_init5, n * 40, cudaMemcpyHostToDevice, cs), ctx);
+        }
+        ZOLA_CUDA_CHECK(cudaEventRecord(ctx->feed_ev[c], cs), ctx);
+    }
+    zola_fit_class dev[ZOLA_MAX_CLASSES];
+    for (int c = 0; c < nclass; ++c) {
+        dev[c] = classes[c];
+        dev[c].d_rois = (const float*)(base + off[c][0]);
+        dev[c].d_init5 = (const double*)(base + off[c][1]);
+        dev[c].d_out5 = (double*)(base + off[c][2]);
+        dev[c].d_crlb5 = classes[c].d_crlb5 ? (double*)(base + off[c][3]) : nullptr;
+        dev[c].d_nll = classes[c].d_nll ? (double*)(base + off[c][4]) : nullptr;
+        dev[c].d_status = classes[c].d_status ? (int*)(base + off[c][5]) : nullptr;
+        dev[c].d_iters = classes[c].d_iters ? (int*)(base + off[c][6]) : nullptr;
+    }
+    int rc = mixed_dev_impl(ctx, dev, nclass, ctx->stream, ctx->feed_ev.data());
+    if (rc) {
+        cudaStreamSynchronize(cs);  // no copy may still write the staging area
+        return rc;
+    }
+    cudaStream_t st = ctx->stream;
+    for (int c = 0; c < nclass; ++c) {
+        const zola_fit_class& k = classes[c];
+        const size_t n = (size_t)k.n;
+        if (n == 0) continue;
+        ZOLA_CUDA_CHECK(cudaMemcpyAsync(k.d_out5, dev[c].d_out5, n * 40, cudaMemcpyDeviceToHost, st), ctx);
+        if (k.d_crlb5) ZOLA_CUDA_CHECK(cudaMemcpyAsync(k.d_crlb5, dev[c].d_crlb5, n * 40, cudaMemcpyDeviceToHost, st), ctx);
+        if (k.d_nll) ZOLA_CUDA_CHECK(cudaMemcpyAsync(k.d_nll, dev[c].d_nll, n * 8, cudaMemcpyDeviceToHost, st), ctx);
+        if (k.d_status) ZOLA_CUDA_CHECK(cudaMemcpyAsync(k.d_status, dev[c].d_status, n * 4, cudaMemcpyDeviceToHost, st), ctx);
+        if (k.d_iters) ZOLA_CUDA_CHECK(cudaMemcpyAsync(k.d_iters, dev[c].d_iters, n * 4, cudaMemcpyDeviceToHost, st), ctx);
+    }
+    ZOLA_CUDA_CHECK(cudaStreamSynchronize(st), ctx);
+    return ZOLA_OK;
 }
 
 int zola_fit_batch(zola_ctx* ctx, zola_psf* psf, int R, const float* rois, const double* init5, int n,

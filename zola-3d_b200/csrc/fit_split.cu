@@ -3502,7 +3502,7 @@ int split_pool_choice(zola_psf* p, WindowTables* w, int* pool, double* ns_per_ev
 // interleaves the classes' LM rounds, so the draining tail of one class
 // overlaps the others' work.  Each ROI's fit is the same bit for bit as in a
 // call of its class alone (a fit does not depend on its batch).
-int launch_fit_split_mixed(zola_ctx* ctx, int nc, MixedClass* mc, cudaStream_t st) {
+int launch_fit_split_mixed(zola_ctx* ctx, int nc, MixedClass* mc, cudaStream_t st, const cudaEvent_t* ready) {
     if (nc > ZOLA_MAX_CLASSES) {
         ctx->err = "zola_fit_batch_mixed_dev: too many classes";
         return ZOLA_E_ARG;
@@ -3533,6 +3533,7 @@ int launch_fit_split_mixed(zola_ctx* ctx, int nc, MixedClass* mc, cudaStream_t s
         if (!ctx->mix_stream[c]) ZOLA_CUDA_CHECK(cudaStreamCreateWithFlags(&ctx->mix_stream[c], cudaStreamNonBlocking), ctx);
         cudaStream_t cs = ctx->mix_stream[c];
         ZOLA_CUDA_CHECK(cudaStreamWaitEvent(cs, ctx->mix_ev[ZOLA_MAX_CLASSES], 0), ctx);
+        if (ready) ZOLA_CUDA_CHECK(cudaStreamWaitEvent(cs, ready[c], 0), ctx);  // this class's inputs have landed
         int rc = setup_pool(ctx, mc[c].p, mc[c].w, mc[c].F.n, pool[c], sp[c], cs, 0, (char*)ctx->scratch + off[c]);
         if (rc) return rc;
         const SplitDev& D = sp[c].D;

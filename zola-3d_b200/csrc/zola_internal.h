@@ -234,7 +234,9 @@ struct MixedClass {
     WindowTables* w;
     FitIO F;
 };
-int launch_fit_split_mixed(zola_ctx* ctx, int nc, MixedClass* mc, cudaStream_t st);
+// ready (nullable): per class, an event recorded once its inputs are on the device
+int launch_fit_split_mixed(zola_ctx* ctx, int nc, MixedClass* mc, cudaStream_t st,
+                           const cudaEvent_t* ready = nullptr);
 // The round-based split fit's pool for psf's R x R ROIs: 1 and the tuned pool
 // (and its ns per evaluation) when tuned, else 0 and the context's setting.
 int split_pool_choice(zola_psf* p, WindowTables* w, int* pool, double* ns_per_eval);
