@@ -201,6 +201,17 @@ def detect_fit_config(z, ctx, torch, device, nframes, fp64_frames=0, seed=1):
                        "host frames in and localization rows out",
            "frames": nframes, "emitters": int(m), "library_slices": det.nz,
            "detect_fp64_flops_per_frame": 2.0 * S * S * R * R * det.nz, "h2d_bytes_per_frame": S * S * 2}
+    # detection alone (uint16 frames in, candidate lists out), after a warm-up call
+    det.detect_u16(frames[:min(nframes, 64)])
+    t0 = time.perf_counter()
+    det.detect_u16(frames)
+    dt = time.perf_counter() - t0
+    fp64_issue = 148 * 64 * 2 * 1.965e9  # 148 SMs x 64 DFMA/clk x max SM clock
+    out["detect_only"] = {"frames": nframes, "frames_per_s": nframes / dt,
+                          "fp64_tflops": out["detect_fp64_flops_per_frame"] * nframes / dt / 1e12,
+                          "fp64_frac_of_issue": out["detect_fp64_flops_per_frame"] * nframes / dt / fp64_issue,
+                          "note": "host uint16 frames to candidate lists through zola_detect_u16; FP64 issue rate "
+                                  "= 148 SMs x 64 DFMA/clk x 1965 MHz (nominal)"}
     rows = {}
     for name, prec, nf in (("split", z.ZOLA_PREC_SPLIT, nframes), ("fp64", z.ZOLA_PREC_FP64, fp64_frames)):
         if nf <= 0:
