@@ -201,8 +201,9 @@ def detect_fit_config(z, ctx, torch, device, nframes, fp64_frames=0, seed=1):
                        "host frames in and localization rows out",
            "frames": nframes, "emitters": int(m), "library_slices": det.nz,
            "detect_fp64_flops_per_frame": 2.0 * S * S * R * R * det.nz, "h2d_bytes_per_frame": S * S * 2}
-    # detection alone (uint16 frames in, candidate lists out), after a warm-up call
-    det.detect_u16(frames[:min(nframes, 64)])
+    # detection alone (uint16 frames in, candidate lists out), after a warm-up call of
+    # the same size (it sizes the staging and scratch areas)
+    det.detect_u16(frames)
     t0 = time.perf_counter()
     det.detect_u16(frames)
     dt = time.perf_counter() - t0

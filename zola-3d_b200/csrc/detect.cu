@@ -573,50 +573,63 @@ int detect_impl(zola_detector* d, const double* frames, const uint16_t* u16, con
     }
     if (nframes == 0) return ZOLA_OK;
     const size_t SS = (size_t)d->v.SX * d->v.SY;
-    double* df = nullptr;
-    double* dout = nullptr;
-    int* dc = nullptr;
-    uint16_t* du = nullptr;
-    int room = cap;  // candidates stored per frame on the device
-    cudaError_t e = cudaMalloc(&df, SS * nframes * 8);
-    if (e == cudaSuccess) e = cudaMalloc(&dc, (size_t)nframes * 4);
+    // frames, counts, the uint16 frames and the candidate rows come from the
+    // context's grow-only staging area, so repeated calls allocate nothing
+    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t b_df = al(SS * nframes * 8), b_dc = al((size_t)nframes * 4), b_du = u16 ? al(SS * nframes * 2) : 0;
+    if (ensure_io(ctx, b_df + b_dc + b_du + al((size_t)nframes * cap * 7 * 8))) return ZOLA_E_CUDA;
+    char* io = (char*)ctx->io;
+    double* df = (double*)io;
+    int* dc = (int*)(io + b_df);
+    uint16_t* du = u16 ? (uint16_t*)(io + b_df + b_dc) : nullptr;
+    double* dout = (double*)(io + b_df + b_dc + b_du);
+    cudaError_t e = cudaSuccess;
     if (u16) {
-        if (e == cudaSuccess) e = cudaMalloc(&du, SS * nframes * 2);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(du, u16, SS * nframes * 2, cudaMemcpyHostToDevice, ctx->stream);
+        e = cudaMemcpyAsync(du, u16, SS * nframes * 2, cudaMemcpyHostToDevice, ctx->stream);
         if (e == cudaSuccess) rescale_u16(ctx, du, SS * nframes, rescale, df, ctx->stream);
-    } else if (e == cudaSuccess) {
+    } else {
         e = cudaMemcpyAsync(df, frames, SS * nframes * 8, cudaMemcpyHostToDevice, ctx->stream);
     }
-    int rc = ZOLA_OK;
-    // A frame whose list is longer than the room is detected again with room for
-    // all of it, so that its rows are the first cap of the whole sorted list.
-    for (int pass = 0; pass < 2 && e == cudaSuccess && rc == ZOLA_OK; ++pass) {
-        if (dout) cudaFree(dout);
-        dout = nullptr;
-        e = cudaMalloc(&dout, (size_t)nframes * room * 7 * 8);
-        if (e == cudaSuccess) rc = zola_detect_dev(d, df, nframes, room, dout, dc, ctx->stream);
-        if (e != cudaSuccess || rc != ZOLA_OK) break;
+    int rc = e == cudaSuccess ? zola_detect_dev(d, df, nframes, cap, dout, dc, ctx->stream) : ZOLA_OK;
+    if (e == cudaSuccess && rc == ZOLA_OK) {
         e = cudaMemcpyAsync(counts, dc, (size_t)nframes * 4, cudaMemcpyDeviceToHost, ctx->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-        if (e != cudaSuccess) break;
-        const int longest = *std::max_element(counts, counts + nframes);
-        if (longest <= room || pass == 1) break;
-        if (longest > ZOLA_DETECT_MAX_CAP) {
-            ctx->err = "zola_detect: a frame has more than 2^20 candidates";
-            rc = ZOLA_E_ARG;
-            break;
-        }
-        room = longest;
+    }
+    // A frame whose list is longer than cap kept the first cap candidates in scan
+    // order, not the best cap: such frames are gathered and detected again with
+    // room for their whole lists, and the first cap rows of each replace theirs.
+    std::vector<int> longf;
+    int room = cap;
+    if (e == cudaSuccess && rc == ZOLA_OK)
+        for (int f = 0; f < nframes; ++f)
+            if (counts[f] > cap) {
+                longf.push_back(f);
+                room = std::max(room, counts[f]);
+            }
+    double* g = nullptr;  // gathered frames, their rows, their counts (rare: one allocation)
+    if (!longf.empty() && room > ZOLA_DETECT_MAX_CAP) {
+        ctx->err = "zola_detect: a frame has more than 2^20 candidates";
+        rc = ZOLA_E_ARG;
+    } else if (!longf.empty()) {
+        const size_t nl = longf.size();
+        e = cudaMalloc(&g, nl * SS * 8 + nl * (size_t)room * 7 * 8 + nl * 4);
+        double* g_out = g + nl * SS;
+        int* g_cnt = (int*)(g_out + nl * (size_t)room * 7);
+        for (size_t k = 0; k < nl && e == cudaSuccess; ++k)
+            e = cudaMemcpyAsync(g + k * SS, df + (size_t)longf[k] * SS, SS * 8, cudaMemcpyDeviceToDevice, ctx->stream);
+        if (e == cudaSuccess) rc = zola_detect_dev(d, g, (int)nl, room, g_out, g_cnt, ctx->stream);
+        for (size_t k = 0; k < nl && e == cudaSuccess && rc == ZOLA_OK; ++k)
+            e = cudaMemcpyAsync(dout + (size_t)longf[k] * cap * 7, g_out + k * room * 7, (size_t)cap * 7 * 8,
+                                cudaMemcpyDeviceToDevice, ctx->stream);
     }
     if (e == cudaSuccess && rc == ZOLA_OK) {
-        e = cudaMemcpy2DAsync(out, (size_t)cap * 7 * 8, dout, (size_t)room * 7 * 8, (size_t)cap * 7 * 8, nframes,
-                              cudaMemcpyDeviceToHost, ctx->stream);
+        e = cudaMemcpyAsync(out, dout, (size_t)nframes * cap * 7 * 8, cudaMemcpyDeviceToHost, ctx->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     }
-    if (df) cudaFree(df);
-    if (dout) cudaFree(dout);
-    if (dc) cudaFree(dc);
-    if (du) cudaFree(du);
+    if (g) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(g);
+    }
     if (e != cudaSuccess) { ctx->err = std::string("zola_detect: ") + cudaGetErrorString(e); return ZOLA_E_CUDA; }
     return rc;
 }
