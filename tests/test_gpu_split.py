@@ -335,6 +335,56 @@ def test_mixed_batch_equals_per_class_calls(zpkg, ctx):
         c["psf"].close()
 
 
+def test_host_mixed_batch_streams_chunks(zpkg, ctx):
+    """zola_fit_batch_mixed copies each class up in chunks of about 32 MB,
+    interleaved across the classes, and each class's pool starts on its first
+    chunk and takes the others as they land (idle slots refilled between
+    rounds).  With three chunks per class and a small pool, the fits equal the
+    device-buffer mixed call bit for bit."""
+    import torch
+    dev = torch.device("cuda", 0)
+    specs = [(64, 16, astig_zernike(), 70000, (-0.5, 0.5)), (128, 48, tetrapod_zernike(), 9000, (-0.8, 0.8))]
+    classes, hosted = [], []
+    ctx.set_pool(1024)
+    try:
+        for k, (N, R, zern, n, zr) in enumerate(specs):
+            psf = make(zpkg, ctx, N, zern)
+            rng = np.random.default_rng(90 + k)
+            truth = np.c_[rng.uniform(-0.11, 0.11, (n, 2)), rng.uniform(*zr, n), rng.lognormal(np.log(2500.0), 0.4, n),
+                          np.full(n, 20.0)]
+            psi = torch.empty((n, R, R), dtype=torch.float64, device=dev)
+            psf.model_dev(R, torch.tensor(truth[:, :3], device=dev), psi, stream=ctx.stream)
+            torch.cuda.synchronize()
+            g = torch.Generator(device=dev)
+            g.manual_seed(11 + k)
+            rois_d = torch.poisson(torch.tensor(truth[:, 3], device=dev)[:, None, None] * psi + 20.0, generator=g).float()
+            init = truth.copy()
+            init[:, :2] = 0
+            init[:, 2] = np.round(truth[:, 2] / 0.1) * 0.1
+            prm = zpkg.PSF.fit_params(zr[0] - 0.5, zr[1] + 0.5, R * 0.11 / 2, max_iter=40, tol_xyz=1e-4,
+                                      precision=zpkg.ZOLA_PREC_SPLIT)
+            classes.append(dict(psf=psf, rois=rois_d, init=torch.tensor(init, device=dev), prm=prm,
+                                out=torch.zeros((n, 5), dtype=torch.float64, device=dev),
+                                status=torch.zeros(n, dtype=torch.int32, device=dev),
+                                iters=torch.zeros(n, dtype=torch.int32, device=dev)))
+            pinned = torch.empty(rois_d.shape, dtype=torch.float32, pin_memory=True)
+            pinned.copy_(rois_d)
+            hosted.append(dict(psf=psf, rois=pinned.numpy(), init=init, prm=prm,
+                               out=dict(theta=np.zeros((n, 5)), status=np.zeros(n, np.int32),
+                                        iters=np.zeros(n, np.int32))))
+        zpkg.fit_mixed_dev(ctx, classes, stream=ctx.stream)
+        torch.cuda.synchronize()
+        zpkg.fit_mixed(ctx, hosted)
+    finally:
+        ctx.set_pool(0)
+    for c, h in zip(classes, hosted):
+        assert np.array_equal(h["out"]["theta"], c["out"].cpu().numpy())
+        assert np.array_equal(h["out"]["status"], c["status"].cpu().numpy())
+        assert np.array_equal(h["out"]["iters"], c["iters"].cpu().numpy())
+        assert (h["out"]["status"] == 1).mean() > 0.8
+        c["psf"].close()
+
+
 def test_host_mixed_batch_rejects_bad_results(zpkg, ctx):
     """zola_fit_batch_mixed with a wrong-shaped result array is refused on the host
     before any copy; a class with no ROIs is accepted and left untouched."""

@@ -403,7 +403,7 @@ int fit_dev_impl(zola_ctx* ctx, zola_psf* psf, int R, const float* d_rois, const
 }
 
 int mixed_dev_impl(zola_ctx* ctx, const zola_fit_class* classes, int nclass, cudaStream_t st,
-                   const cudaEvent_t* ready);
+                   const zola::RoiFeed* feeds);
 
 int fit_host_impl(zola_ctx* ctx, zola_psf* psf, int R, const float* rois, const float* scmos, const double* init5,
                   int n, const zola_fit_params* prm, double* out5, double* crlb5, double* nll, int* status,
@@ -501,7 +501,6 @@ int zola_fit_batch_mixed_dev(zola_ctx* ctx, const zola_fit_class* classes, int n
 
 namespace {
 
-// ready (nullable): per class, an event after which its inputs are on the device
 // One class of a mixed batch: its PSF, parameters and buffers, and the window
 // tables of its ROI size (built here when missing).
 int check_mixed_class(zola_ctx* ctx, const zola_fit_class& k, WindowTables** w) {
@@ -517,10 +516,11 @@ int check_mixed_class(zola_ctx* ctx, const zola_fit_class& k, WindowTables** w) 
     return *w ? ZOLA_OK : ZOLA_E_ARG;
 }
 
+// feeds (nullable): per class, its input chunks still arriving on the copy stream
 int mixed_dev_impl(zola_ctx* ctx, const zola_fit_class* classes, int nclass, cudaStream_t st,
-                   const cudaEvent_t* ready) {
+                   const zola::RoiFeed* feeds) {
     zola::MixedClass mc[ZOLA_MAX_CLASSES];
-    cudaEvent_t rdy[ZOLA_MAX_CLASSES];
+    zola::RoiFeed fd[ZOLA_MAX_CLASSES];
     int m = 0;
     for (int c = 0; c < nclass; ++c) {
         const zola_fit_class& k = classes[c];
@@ -529,13 +529,13 @@ int mixed_dev_impl(zola_ctx* ctx, const zola_fit_class* classes, int nclass, cud
         if (k.n == 0) continue;
         const zola_fit_params& pr = k.prm;
         zola::FitParamsDev fp{pr.zmin, pr.zmax, pr.xymax, pr.tol_xyz, pr.step_xy, pr.step_z, pr.max_iter, 1e-3};
-        if (ready) rdy[m] = ready[c];
+        if (feeds) fd[m] = feeds[c];
         mc[m++] = zola::MixedClass{k.psf, w,
                                    zola::FitIO{k.d_rois, nullptr, k.d_init5, k.n, fp, k.d_out5, k.d_crlb5, k.d_nll,
                                                k.d_status, k.d_iters}};
     }
     if (m == 0) return ZOLA_OK;
-    return zola::launch_fit_split_mixed(ctx, m, mc, st, ready ? rdy : nullptr);
+    return zola::launch_fit_split_mixed(ctx, m, mc, st, feeds ? fd : nullptr);
 }
 
 }  // namespace
@@ -564,29 +564,42 @@ int zola_fit_batch_mixed(zola_ctx* ctx, const zola_fit_class* classes, int nclas
     if (total == 0) return ZOLA_OK;
     if (ensure_io(ctx, total)) return ZOLA_E_CUDA;
     char* base = (char*)ctx->io;
-    while ((int)ctx->feed_ev.size() < ZOLA_MAX_CLASSES) {
+    // Inputs go up on the copy stream in chunks of about 32 MB (at most 64 a class),
+    // the classes' chunks interleaved, so that every class starts fitting on its
+    // first chunk while the rest are still crossing the host link.
+    constexpr int MAX_CHUNKS = 64;
+    while ((int)ctx->feed_ev.size() < MAX_CHUNKS * ZOLA_MAX_CLASSES) {
         cudaEvent_t e;
         ZOLA_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), ctx);
         ctx->feed_ev.push_back(e);
     }
-    // inputs go up on the copy stream, the smallest class first, so that the first
-    // classes start fitting while the larger ones are still being copied
-    int order[ZOLA_MAX_CLASSES];
-    for (int c = 0; c < nclass; ++c) order[c] = c;
-    std::sort(order, order + nclass, [&](int x, int y) {
-        return (size_t)classes[x].n * classes[x].R * classes[x].R < (size_t)classes[y].n * classes[y].R * classes[y].R;
-    });
+    int chunk_end[ZOLA_MAX_CLASSES][MAX_CHUNKS];
+    size_t per[ZOLA_MAX_CLASSES];
+    zola::RoiFeed feeds[ZOLA_MAX_CLASSES];
     cudaStream_t cs = ctx->copy_stream;
-    for (int oc = 0; oc < nclass; ++oc) {
-        const int c = order[oc];
+    int most = 0;
+    for (int c = 0; c < nclass; ++c) {
         const zola_fit_class& k = classes[c];
         const size_t n = (size_t)k.n, rr = (size_t)k.R * k.R;
-        if (n > 0) {
-            ZOLA_CUDA_CHECK(cudaMemcpyAsync(base + off[c][0], k.d_rois, rr * n * 4, cudaMemcpyHostToDevice, cs), ctx);
+        per[c] = std::max<size_t>(1024, ((size_t)32 << 20) / (rr * sizeof(float)));
+        per[c] = std::max(per[c], (n + MAX_CHUNKS - 1) / MAX_CHUNKS);
+        feeds[c].n_chunks = (int)((n + per[c] - 1) / per[c]);
+        feeds[c].chunk_end = chunk_end[c];
+        feeds[c].ev = ctx->feed_ev.data() + (size_t)c * MAX_CHUNKS;
+        most = std::max(most, feeds[c].n_chunks);
+        if (n > 0)
             ZOLA_CUDA_CHECK(cudaMemcpyAsync(base + off[c][1], k.d_init5, n * 40, cudaMemcpyHostToDevice, cs), ctx);
-        }
-        ZOLA_CUDA_CHECK(cudaEventRecord(ctx->feed_ev[c], cs), ctx);
     }
+    for (int j = 0; j < most; ++j)
+        for (int c = 0; c < nclass; ++c) {
+            if (j >= feeds[c].n_chunks) continue;
+            const zola_fit_class& k = classes[c];
+            const size_t rr = (size_t)k.R * k.R, a = (size_t)j * per[c], b = std::min((size_t)k.n, a + per[c]);
+            ZOLA_CUDA_CHECK(cudaMemcpyAsync(base + off[c][0] + a * rr * 4, k.d_rois + a * rr, (b - a) * rr * 4,
+                                            cudaMemcpyHostToDevice, cs), ctx);
+            ZOLA_CUDA_CHECK(cudaEventRecord(feeds[c].ev[j], cs), ctx);
+            chunk_end[c][j] = (int)b;
+        }
     zola_fit_class dev[ZOLA_MAX_CLASSES];
     for (int c = 0; c < nclass; ++c) {
         dev[c] = classes[c];
@@ -598,7 +611,7 @@ int zola_fit_batch_mixed(zola_ctx* ctx, const zola_fit_class* classes, int nclas
         dev[c].d_status = classes[c].d_status ? (int*)(base + off[c][5]) : nullptr;
         dev[c].d_iters = classes[c].d_iters ? (int*)(base + off[c][6]) : nullptr;
     }
-    int rc = mixed_dev_impl(ctx, dev, nclass, ctx->stream, ctx->feed_ev.data());
+    int rc = mixed_dev_impl(ctx, dev, nclass, ctx->stream, feeds);
     if (rc) {
         cudaStreamSynchronize(cs);  // no copy may still write the staging area
         return rc;

@@ -573,11 +573,16 @@ int detect_impl(zola_detector* d, const double* frames, const uint16_t* u16, con
     }
     if (nframes == 0) return ZOLA_OK;
     const size_t SS = (size_t)d->v.SX * d->v.SY;
+    // Candidates stored per frame in the first pass: at least DETECT_ROOM, so that the
+    // usual lists (a few thousand at the reference's threshold) are whole and sorted
+    // in one pass whatever cap the caller asks for.
+    constexpr int DETECT_ROOM = 8192;
+    const int room0 = std::max(cap, DETECT_ROOM);
     // frames, counts, the uint16 frames and the candidate rows come from the
     // context's grow-only staging area, so repeated calls allocate nothing
     auto al = [](size_t b) { return (b + 255) / 256 * 256; };
     const size_t b_df = al(SS * nframes * 8), b_dc = al((size_t)nframes * 4), b_du = u16 ? al(SS * nframes * 2) : 0;
-    if (ensure_io(ctx, b_df + b_dc + b_du + al((size_t)nframes * cap * 7 * 8))) return ZOLA_E_CUDA;
+    if (ensure_io(ctx, b_df + b_dc + b_du + al((size_t)nframes * room0 * 7 * 8))) return ZOLA_E_CUDA;
     char* io = (char*)ctx->io;
     double* df = (double*)io;
     int* dc = (int*)(io + b_df);
@@ -590,19 +595,19 @@ int detect_impl(zola_detector* d, const double* frames, const uint16_t* u16, con
     } else {
         e = cudaMemcpyAsync(df, frames, SS * nframes * 8, cudaMemcpyHostToDevice, ctx->stream);
     }
-    int rc = e == cudaSuccess ? zola_detect_dev(d, df, nframes, cap, dout, dc, ctx->stream) : ZOLA_OK;
+    int rc = e == cudaSuccess ? zola_detect_dev(d, df, nframes, room0, dout, dc, ctx->stream) : ZOLA_OK;
     if (e == cudaSuccess && rc == ZOLA_OK) {
         e = cudaMemcpyAsync(counts, dc, (size_t)nframes * 4, cudaMemcpyDeviceToHost, ctx->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     }
-    // A frame whose list is longer than cap kept the first cap candidates in scan
-    // order, not the best cap: such frames are gathered and detected again with
-    // room for their whole lists, and the first cap rows of each replace theirs.
+    // A frame whose list is longer than the room kept the first candidates in scan
+    // order, not the best: such frames are gathered and detected again with room
+    // for their whole lists, and the first cap rows of each replace theirs.
     std::vector<int> longf;
-    int room = cap;
+    int room = room0;
     if (e == cudaSuccess && rc == ZOLA_OK)
         for (int f = 0; f < nframes; ++f)
-            if (counts[f] > cap) {
+            if (counts[f] > room0) {
                 longf.push_back(f);
                 room = std::max(room, counts[f]);
             }
@@ -619,11 +624,12 @@ int detect_impl(zola_detector* d, const double* frames, const uint16_t* u16, con
             e = cudaMemcpyAsync(g + k * SS, df + (size_t)longf[k] * SS, SS * 8, cudaMemcpyDeviceToDevice, ctx->stream);
         if (e == cudaSuccess) rc = zola_detect_dev(d, g, (int)nl, room, g_out, g_cnt, ctx->stream);
         for (size_t k = 0; k < nl && e == cudaSuccess && rc == ZOLA_OK; ++k)
-            e = cudaMemcpyAsync(dout + (size_t)longf[k] * cap * 7, g_out + k * room * 7, (size_t)cap * 7 * 8,
+            e = cudaMemcpyAsync(dout + (size_t)longf[k] * room0 * 7, g_out + k * room * 7, (size_t)cap * 7 * 8,
                                 cudaMemcpyDeviceToDevice, ctx->stream);
     }
     if (e == cudaSuccess && rc == ZOLA_OK) {
-        e = cudaMemcpyAsync(out, dout, (size_t)nframes * cap * 7 * 8, cudaMemcpyDeviceToHost, ctx->stream);
+        e = cudaMemcpy2DAsync(out, (size_t)cap * 7 * 8, dout, (size_t)room0 * 7 * 8, (size_t)cap * 7 * 8, nframes,
+                              cudaMemcpyDeviceToHost, ctx->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     }
     if (g) {

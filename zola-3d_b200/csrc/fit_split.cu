@@ -138,7 +138,10 @@ static double pow2scale(double bound) {
     return std::ldexp(1.0, (int)std::floor(std::log2(16384.0 / bound)));
 }
 
-__host__ __device__ inline size_t a2_tile_bytes(int K1) { return (size_t)4 * 128 * K1 * 2; }
+// A2 arrays of a stage-2 tile: S hi, S lo, S_y, S_z and, for W = 128, S_x = i k_x S
+// (the window DFT then needs only the hi/lo DFT constants, not their x derivative).
+__host__ __device__ constexpr int a2_arrays(int W) { return W > 64 ? 5 : 4; }
+__host__ __device__ inline size_t a2_tile_bytes(int K1, int W) { return (size_t)a2_arrays(W) * 128 * K1 * 2; }
 __host__ __device__ inline size_t a3_tile_bytes(int W) { return (size_t)5 * 128 * W * 2; }
 __host__ __device__ inline size_t a4_tile_bytes(int W) { return (size_t)2 * 128 * W * 2; }
 // Row-blurred maps J of one slot as the column-blur B operand: hi then lo, each
@@ -531,8 +534,13 @@ __device__ __forceinline__ bool group_bar_or(int id, bool p) {
 }
 
 __host__ __device__ constexpr int s2_slab_bytes(int W) { return 6 * W * 32; }
-
-__host__ __device__ constexpr int s2_ring_bytes(int W) { return (W > 64 ? 2 : 4) * 4096; }
+// the window DFT's resident K-slab: all six row groups, or for W = 128 only the hi
+// and lo DFT rows (4W rows: parts 0, 1 hi and their lo)
+__host__ __device__ constexpr int s2_cslab_bytes(int W) { return (W > 64 ? 4 : 6) * W * 32; }
+// one ring step of A2 K-slabs: W = 128 streams S hi, S lo, S_x (phase A) or S_y, S_z
+// (phase B); smaller windows all four arrays at once
+__host__ __device__ constexpr int s2_ring_bytes(int W) { return (W > 64 ? 3 : 4) * 4096; }
+__host__ __device__ constexpr int s2_nbuf(int W) { return W > 64 ? 8 : 4; }
 
 __device__ __forceinline__ void warp_arrive(uint64_t* mbar) {
     __syncwarp();
@@ -629,6 +637,9 @@ struct StaticUnits {
         for (u = u < 0 ? (int)blockIdx.x : u + (int)gridDim.x; u < U; u += gridDim.x)
             if (tile_live(P, u * UG, UG)) {
                 tag = 0;
+                // the next unit's slot states, on their way to L1 while this unit runs
+                if ((threadIdx.x & 31) == 0 && u + (int)gridDim.x < U)
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(P.slot_roi + (size_t)(u + gridDim.x) * UG));
                 return u;
             }
         return -1;
@@ -879,6 +890,7 @@ __device__ __forceinline__ void stage1_body(const SplitDev& P, const FitIO& F, U
     const int row = t & 127, wg = t >> 7;
     const int g = row / DP, a = row % DP;
     const int kre = kperm(a, false), kim = kperm(a, true);
+    const float kxe = TWO ? (float)P.kx[a] : 0.f;  // k_x of this TMEM row's pupil row
     const size_t arr = (size_t)128 * K1 * 2;
     constexpr int CW = W / 4;
     int q = 0, ntile = 0;
@@ -964,7 +976,7 @@ __device__ __forceinline__ void stage1_body(const SplitDev& P, const FitIO& F, U
             const int slot = tile * G1 + g;
             const bool live = P.slot_roi[slot] >= 0;
             const int tile2 = slot / P.G2, mrow0 = (slot % P.G2) * W;
-            char* a2t = P.a2 + (size_t)tile2 * a2_tile_bytes(K1);
+            char* a2t = P.a2 + (size_t)tile2 * a2_tile_bytes(K1, W);
             // epilogue of one pass: maps at TMEM columns c0 (S), c0 + 2W (S_y), zc (S_z; < 0: none)
             auto epilogue = [&](bool sy, int zc, uint32_t phase, uint64_t* accb) {
                 umma::mbar_wait(accb, phase, P.err);
@@ -993,6 +1005,16 @@ __device__ __forceinline__ void stage1_body(const SplitDev& P, const FitIO& F, U
                             store4w(a2t + 1 * arr + mnmajor_off(m, kim, 128), sli);
                             store4w(a2t + 2 * arr + mnmajor_off(m, kre, 128), wyr);
                             store4w(a2t + 2 * arr + mnmajor_off(m, kim, 128), wyi);
+                            if constexpr (TWO) {  // S_x = i k_x(a) S, scaled like S_y
+                                uint32_t wxr[4], wxi[4];
+#pragma unroll
+                                for (int u = 0; u < 8; u += 2) {
+                                    wxr[u / 2] = pack_h2(-kxe * si[u] * P.sc.c2y, -kxe * si[u + 1] * P.sc.c2y);
+                                    wxi[u / 2] = pack_h2(kxe * sr[u] * P.sc.c2y, kxe * sr[u + 1] * P.sc.c2y);
+                                }
+                                store4w(a2t + 4 * arr + mnmajor_off(m, kre, 128), wxr);
+                                store4w(a2t + 4 * arr + mnmajor_off(m, kim, 128), wxi);
+                            }
                         }
                     }
                     if (zc >= 0) {
@@ -1076,15 +1098,13 @@ __global__ void __launch_bounds__(S1_THREADS, 1) k_stage1p(SplitDev P, FitIO F) 
 // Ez.  Warps 0-15 run the epilogues (thread 0 also issues the MMAs), warp 16
 // is the producer.
 constexpr int S2_THREADS = SPLIT_THREADS + 32;
-constexpr int S2_NBUF = 4;
 
 template <int W, class UNITS>
 __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, UNITS units) {
     extern __shared__ __align__(1024) char smem[];
     constexpr bool TWO = W > 64;
-    constexpr int SLAB = s2_slab_bytes(W), RING = s2_ring_bytes(W), NBUF = S2_NBUF;
+    constexpr int SLAB = s2_cslab_bytes(W), RING = s2_ring_bytes(W), NBUF = s2_nbuf(W);
     constexpr int NCOLS = W >= 64 ? 512 : 256;
-    constexpr int NARR = TWO ? 2 : 4;  // A2 arrays per ring step
     const int K1 = P.K1, G2 = P.G2, t = threadIdx.x;
     const int NS = K1 / 16, NSTEP = TWO ? 2 * NS : NS;
     const int T2 = unit_slots(P.G1, G2) / G2;  // window tiles per unit
@@ -1113,8 +1133,15 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
             }
         if (t != SPLIT_THREADS) return;
         umma::mbar_expect_tx(&cfull, (uint32_t)(NS * SLAB));
-        for (int s = 0; s < NS; ++s)
-            umma::bulk_g2s(CS + s * SLAB, (const char*)P.bcs + (size_t)s * SLAB, SLAB, &cfull);
+        for (int s = 0; s < NS; ++s) {
+            const char* src = (const char*)P.bcs + (size_t)s * s2_slab_bytes(W);
+            if constexpr (TWO) {  // rows [0, 2W) (hi) and [4W, 6W) (lo) of the full slab
+                umma::bulk_g2s(CS + s * SLAB, src, 2 * W * 32, &cfull);
+                umma::bulk_g2s(CS + s * SLAB + 2 * W * 32, src + 4 * W * 32, 2 * W * 32, &cfull);
+            } else {
+                umma::bulk_g2s(CS + s * SLAB, src, SLAB, &cfull);
+            }
+        }
         int q = 0;
         for (int tag = 0;;) {
             const int unit = units.next(P, tag, true);
@@ -1122,17 +1149,19 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
             for (int k = 0; k < T2; ++k) {
                 const int tile = unit * T2 + k;
                 if (!tile_live(P, tile * G2, G2)) continue;
-                const char* src = P.a2 + (size_t)tile * a2_tile_bytes(K1);
+                const char* src = P.a2 + (size_t)tile * a2_tile_bytes(K1, W);
                 for (int n = 0; n < NSTEP; ++n, ++q) {
                     const int buf = q % NBUF;
                     if (q >= NBUF && !umma::mbar_wait(&freed[buf], (uint32_t)((q / NBUF - 1) & 1), P.err)) return;
                     const bool pb = TWO && n >= NS;
                     const int s = pb ? n - NS : n;
-                    const int a0 = pb ? 2 : 0;  // phase B streams the y and z arrays
-                    umma::mbar_expect_tx(&full[buf], RING);
-                    for (int j = 0; j < NARR; ++j)
-                        umma::bulk_g2s(RB + buf * RING + j * 4096, src + (size_t)(a0 + j) * arr + (size_t)s * 4096, 4096,
-                                       &full[buf]);
+                    // phase A: S hi, S lo, S_x (W = 128) or all four arrays; phase B: S_y, S_z
+                    constexpr int A_ARR[4] = {0, 1, TWO ? 4 : 2, 3};
+                    const int narr = TWO ? (pb ? 2 : 3) : 4;
+                    umma::mbar_expect_tx(&full[buf], (uint32_t)(narr * 4096));
+                    for (int j = 0; j < narr; ++j)
+                        umma::bulk_g2s(RB + buf * RING + j * 4096,
+                                       src + (size_t)(pb ? 2 + j : A_ARR[j]) * arr + (size_t)s * 4096, 4096, &full[buf]);
                 }
             }
         }
@@ -1145,10 +1174,10 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
     const size_t arr3 = (size_t)128 * W * 2;
     const uint32_t lbo_mn = (128 / 8) * 128;
     int q = 0, ph = 0;
-    auto issue_steps = [&](int n0, int n1) {
+    auto issue_steps = [&](int n0, int n1) -> bool {
         for (int n = n0; n < n1; ++n, ++q) {
             const int buf = q % NBUF;
-            if (!umma::mbar_wait(&full[buf], (uint32_t)((q / NBUF) & 1), P.err)) return;
+            if (!umma::mbar_wait(&full[buf], (uint32_t)((q / NBUF) & 1), P.err)) return false;
             umma::fence_after_sync();
             const uint32_t rb = umma::smem_u32(RB + buf * RING);
             const bool pb = TWO && n >= NS;
@@ -1159,21 +1188,25 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
                 const uint64_t bd = umma::smem_desc(cb + (uint32_t)(row0 / 8) * 256, 128, 256);
                 umma::mma_f16(tbase + col, ad, bd, umma::idesc_f16(128, N, true, false), acc ? 1u : 0u);
             };
-            if (!pb) {
+            if (!pb && TWO) {  // resident rows: [0, 2W) hi(C), [2W, 4W) lo(C)
+                mma(rb, 0, 2 * W, 0, !first);              // E = hi x hi(C)
+                mma(rb, 2 * W, 2 * W, 0, true);            // + hi x lo(C)
+                mma(rb + 4096, 0, 2 * W, 0, true);         // + lo x hi(C)
+                mma(rb + 8192, 0, 2 * W, 2 * W, !first);   // Ex = S_x x hi(C)
+            } else if (!pb) {
 #pragma unroll
                 for (int r = 0; r < 4 * W; r += 256) mma(rb, r, 4 * W < 256 ? 4 * W : 256, r, !first);  // E, Ex
                 mma(rb, 4 * W, 2 * W, 0, true);         // + hi x lo(C)
                 mma(rb + 4096, 0, 2 * W, 0, true);      // + lo x hi(C)
-                if (!TWO) {
-                    mma(rb + 8192, 0, 2 * W, 4 * W, !first);   // Ey
-                    mma(rb + 12288, 0, 2 * W, 6 * W, !first);  // Ez
-                }
+                mma(rb + 8192, 0, 2 * W, 4 * W, !first);   // Ey
+                mma(rb + 12288, 0, 2 * W, 6 * W, !first);  // Ez
             } else {
                 mma(rb, 0, 2 * W, 0, !first);          // Ey
                 mma(rb + 4096, 0, 2 * W, 2 * W, !first);  // Ez
             }
             umma::mma_commit(&freed[buf]);
         }
+        return true;
     };
     auto ipx = [](const float* er, const float* ei, const float* xr, const float* xi, int u, float cf) {
         return (er[u] * xr[u] + ei[u] * xi[u]) * cf;
@@ -1186,12 +1219,16 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
         for (int k = 0; k < T2 && !abort; ++k) {
             const int tile = unit * T2 + k;
             if (!tile_live(P, tile * G2, G2)) continue;
+            // the error flag is read here and voted on at the tile's last barrier (its
+            // latency hides under the tile); a wait that gave up in this tile votes too
+            const int errv = t == 0 ? *(volatile int*)P.err : 0;
+            bool bad = false;
             char* a3t = P.a3 + (size_t)tile * a3_tile_bytes(W);
             if (t == 0) {
-                issue_steps(0, NS);
+                bad = !issue_steps(0, NS);
                 umma::mma_commit(&accA);
             }
-            umma::mbar_wait(&accA, (uint32_t)ph, P.err);
+            bad |= !umma::mbar_wait(&accA, (uint32_t)ph, P.err);
             umma::fence_after_sync();
             if constexpr (TWO) {
                 float er[CW], ei[CW];
@@ -1211,8 +1248,8 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
                         split2((er[h + u] * er[h + u] + ei[h + u] * ei[h + u]) * P.sc.cI,
                                (er[h + u + 1] * er[h + u + 1] + ei[h + u + 1] * ei[h + u + 1]) * P.sc.cI, hh[u / 2],
                                ll[u / 2]);
-                        dx[u / 2] = pack_h2(ipx(er + h, ei + h, xr, xi, u, P.sc.cIx),
-                                            ipx(er + h, ei + h, xr, xi, u + 1, P.sc.cIx));
+                        dx[u / 2] = pack_h2(ipx(er + h, ei + h, xr, xi, u, P.sc.cIy),  // S_x scaled like S_y
+                                            ipx(er + h, ei + h, xr, xi, u + 1, P.sc.cIy));
                     }
                     const uint32_t off = kmajor_off(row, i0, W);
                     store4w(a3t + 0 * arr3 + off, hh);
@@ -1223,10 +1260,10 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
                 epi_bar();
                 if (t == 0) {
                     umma::fence_after_sync();
-                    issue_steps(NS, NSTEP);
+                    bad |= !issue_steps(NS, NSTEP);
                     umma::mma_commit(&accB);
                 }
-                umma::mbar_wait(&accB, (uint32_t)ph, P.err);
+                bad |= !umma::mbar_wait(&accB, (uint32_t)ph, P.err);
                 umma::fence_after_sync();
 #pragma unroll
                 for (int h = 0; h < CW; h += 8) {
@@ -1284,7 +1321,7 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
             // (a bounded wait that gave up makes every epilogue thread leave the loop together)
             umma::fence_before_sync();
             units.fence_writes();
-            abort = epi_bar_or(t == 0 && *(volatile int*)P.err != 0);
+            abort = epi_bar_or(bad || errv != 0);
             if (t == 0) umma::fence_after_sync();
             ph ^= 1;
         }
@@ -2386,7 +2423,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_fused25(SplitDev P, const 
     };
     if (t == 0) {
         umma::mbar_expect_tx(&full_a2, (uint32_t)(4 * arr2 + 2 * gtb));
-        const char* src = P.a2 + (size_t)blockIdx.x * a2_tile_bytes(K1);
+        const char* src = P.a2 + (size_t)blockIdx.x * a2_tile_bytes(K1, W);
         for (int q = 0; q < 4; ++q) umma::bulk_g2s(A2 + q * arr2, src + q * arr2, (uint32_t)arr2, &full_a2);
         umma::bulk_g2s(GT, P.gt_hi, (uint32_t)gtb, &full_a2);
         umma::bulk_g2s(GT + gtb, P.gt_lo, (uint32_t)gtb, &full_a2);
@@ -2756,7 +2793,7 @@ static size_t smem_stage1p(const SplitPlanHost& pl) {
     return (size_t)(pl.K1 / 16) * s2_slab_bytes(pl.W) + (size_t)S1_NBQ * s1_qring_bytes(pl.W);
 }
 static size_t smem_stage2p(const SplitPlanHost& pl) {
-    return (size_t)(pl.K1 / 16) * s2_slab_bytes(pl.W) + (size_t)S2_NBUF * s2_ring_bytes(pl.W);
+    return (size_t)(pl.K1 / 16) * s2_cslab_bytes(pl.W) + (size_t)s2_nbuf(pl.W) * s2_ring_bytes(pl.W);
 }
 static size_t smem_stage3(const SplitPlanHost& pl, bool flow = false) {
     return (size_t)s3_nbuf(pl.W, flow) * 5 * 128 * pl.W * 2 + (size_t)4 * pl.RP * pl.W;
@@ -2912,7 +2949,7 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
         ctx->err = "split path: shared-memory plan exceeds 225 KB";
         return ZOLA_E_UNSUPPORTED;
     }
-    const size_t per_slot = a2_tile_bytes(pl->K1) / pl->G2 + a3_tile_bytes(pl->W) / pl->G2 +
+    const size_t per_slot = a2_tile_bytes(pl->K1, pl->W) / pl->G2 + a3_tile_bytes(pl->W) / pl->G2 +
                             (size_t)pl->NT4 * a4_tile_bytes(pl->W) + (size_t)4 * pl->R * pl->R * 4 + sizeof(LMState) + NSUM * 8 + 16;
     int Pmax = (int)std::min<size_t>(32768, ((size_t)8 << 30) / per_slot);  // at most 8 GB of pool state
     if (pmax_override > 0) Pmax = std::min(Pmax, pmax_override);
@@ -2921,7 +2958,7 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
     const int P = std::min(Pmax, (n + UG - 1) / UG * UG);
     sp.U = P / UG;
     auto al = [](size_t v) { return (v + 1023) / 1024 * 1024; };
-    const size_t b_a2 = al((size_t)(P / pl->G2) * a2_tile_bytes(pl->K1));
+    const size_t b_a2 = al((size_t)(P / pl->G2) * a2_tile_bytes(pl->K1, pl->W));
     const size_t b_a3 = al((size_t)(P / pl->G2) * a3_tile_bytes(pl->W));
     const size_t b_a4 = al((size_t)P * pl->NT4 * a4_tile_bytes(pl->W));
     const size_t b_t = al((size_t)P * 4 * pl->R * pl->R * 4);
@@ -3502,7 +3539,7 @@ int split_pool_choice(zola_psf* p, WindowTables* w, int* pool, double* ns_per_ev
 // interleaves the classes' LM rounds, so the draining tail of one class
 // overlaps the others' work.  Each ROI's fit is the same bit for bit as in a
 // call of its class alone (a fit does not depend on its batch).
-int launch_fit_split_mixed(zola_ctx* ctx, int nc, MixedClass* mc, cudaStream_t st, const cudaEvent_t* ready) {
+int launch_fit_split_mixed(zola_ctx* ctx, int nc, MixedClass* mc, cudaStream_t st, const RoiFeed* feeds) {
     if (nc > ZOLA_MAX_CLASSES) {
         ctx->err = "zola_fit_batch_mixed_dev: too many classes";
         return ZOLA_E_ARG;
@@ -3523,27 +3560,56 @@ int launch_fit_split_mixed(zola_ctx* ctx, int nc, MixedClass* mc, cudaStream_t s
         for (auto& e : ctx->mix_ev) ZOLA_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), ctx);
     if (!ctx->h_mix) ZOLA_CUDA_CHECK(cudaMallocHost(&ctx->h_mix, 4 * ZOLA_MAX_CLASSES * sizeof(int)), ctx);
     ZOLA_CUDA_CHECK(cudaEventRecord(ctx->mix_ev[ZOLA_MAX_CLASSES], st), ctx);
+    // A class whose inputs are still arriving (feeds[c] with chunks) starts on its
+    // first chunk; between blocks of rounds the host hands it the chunks that have
+    // landed (the device count of arrived ROIs), and idle slots take them.
     struct State {
-        int rounds = 0, max_rounds = 0;
-        bool done = false;
+        int rounds = 0, max_rounds = 0, chunk = 0, navail = 0, queue = 0;
+        bool done = false, feed = false;
     };
     std::vector<State> S(nc);
     RoundGraph graphs[ZOLA_MAX_CLASSES];
     for (int c = 0; c < nc; ++c) {
         if (!ctx->mix_stream[c]) ZOLA_CUDA_CHECK(cudaStreamCreateWithFlags(&ctx->mix_stream[c], cudaStreamNonBlocking), ctx);
         cudaStream_t cs = ctx->mix_stream[c];
+        const FitIO& F = mc[c].F;
         ZOLA_CUDA_CHECK(cudaStreamWaitEvent(cs, ctx->mix_ev[ZOLA_MAX_CLASSES], 0), ctx);
-        if (ready) ZOLA_CUDA_CHECK(cudaStreamWaitEvent(cs, ready[c], 0), ctx);  // this class's inputs have landed
-        int rc = setup_pool(ctx, mc[c].p, mc[c].w, mc[c].F.n, pool[c], sp[c], cs, 0, (char*)ctx->scratch + off[c]);
+        S[c].feed = feeds && feeds[c].n_chunks > 0;
+        S[c].navail = F.n;
+        if (S[c].feed) {
+            ZOLA_CUDA_CHECK(cudaStreamWaitEvent(cs, feeds[c].ev[0], 0), ctx);  // the first chunk has landed
+            S[c].navail = feeds[c].chunk_end[0];
+        }
+        int rc = setup_pool(ctx, mc[c].p, mc[c].w, F.n, pool[c], sp[c], cs, 0, (char*)ctx->scratch + off[c]);
         if (rc) return rc;
         const SplitDev& D = sp[c].D;
-        k_init_slots<<<(D.P + 127) / 128, 128, 0, cs>>>(D, mc[c].F.init, mc[c].F.n, mc[c].F.n, mc[c].F.prm);
+        k_init_slots<<<(D.P + 127) / 128, 128, 0, cs>>>(D, F.init, F.n, S[c].navail, F.prm);
         ctx->launches++;
-        S[c].max_rounds = (mc[c].F.prm.max_iter + 2) * ((mc[c].F.n + D.P - 1) / D.P + 1) + 8;
-        S[c].done = mc[c].F.n == 0;
-        if (!S[c].done) graphs[c].capture(ctx, sp[c], mc[c].F, cs);
+        S[c].max_rounds = (F.prm.max_iter + 2) * ((F.n + D.P - 1) / D.P + 1) + 8 + (S[c].feed ? 4 * feeds[c].n_chunks : 0);
+        S[c].done = F.n == 0;
+        if (!S[c].done && !S[c].feed) graphs[c].capture(ctx, sp[c], F, cs);
     }
     ZOLA_CUDA_CHECK(cudaGetLastError(), ctx);
+    // hand class c the chunks that have landed (block: wait for at least one)
+    auto poll_feed = [&](int c, bool block) -> int {
+        State& q = S[c];
+        const RoiFeed& fd = feeds[c];
+        const int before = q.navail;
+        while (q.chunk + 1 < fd.n_chunks) {
+            if (block) {
+                ZOLA_CUDA_CHECK(cudaEventSynchronize(fd.ev[q.chunk + 1]), ctx);
+                block = false;
+            } else if (cudaEventQuery(fd.ev[q.chunk + 1]) != cudaSuccess) {
+                break;
+            }
+            q.navail = fd.chunk_end[++q.chunk];
+        }
+        if (q.navail != before) {
+            k_set_int<<<1, 1, 0, ctx->mix_stream[c]>>>(sp[c].D.navail, q.navail);
+            ctx->launches++;
+        }
+        return ZOLA_OK;
+    };
     for (;;) {
         bool any = false;
         for (int c = 0; c < nc; ++c) {
@@ -3551,7 +3617,16 @@ int launch_fit_split_mixed(zola_ctx* ctx, int nc, MixedClass* mc, cudaStream_t s
             any = true;
             cudaStream_t cs = ctx->mix_stream[c];
             const SplitPool& p = sp[c];
-            graphs[c].run(ctx, p, mc[c].F, cs);
+            if (S[c].feed && S[c].queue < mc[c].F.n) {
+                for (int k = 0; k < 4; ++k) {  // idle slots take ROIs that arrived since
+                    k_refill<<<(p.D.P + 127) / 128, 128, 0, cs>>>(p.D, mc[c].F.init, mc[c].F.n, mc[c].F.prm);
+                    ctx->launches++;
+                    issue_round(ctx, p, mc[c].F, cs);
+                }
+            } else {
+                if (S[c].feed && !graphs[c].exec) graphs[c].capture(ctx, p, mc[c].F, cs);  // every ROI taken
+                graphs[c].run(ctx, p, mc[c].F, cs);
+            }
             S[c].rounds += 4;
             ZOLA_CUDA_CHECK(cudaMemcpyAsync(ctx->h_mix + 4 * c, p.D.queue, 3 * sizeof(int), cudaMemcpyDeviceToHost, cs),
                             ctx);
@@ -3566,6 +3641,13 @@ int launch_fit_split_mixed(zola_ctx* ctx, int nc, MixedClass* mc, cudaStream_t s
             if (err) {
                 ctx->err = "split fit: a bounded device wait timed out";
                 return ZOLA_E_TIMEOUT;
+            }
+            S[c].queue = queue;
+            if (S[c].feed) {
+                int rc = poll_feed(c, false);
+                // every slot idle and the queue at the arrived ROIs: wait for the next chunk
+                if (!rc && active <= 0 && queue < mc[c].F.n && S[c].navail <= queue) rc = poll_feed(c, true);
+                if (rc) return rc;
             }
             if (active <= 0 && queue >= mc[c].F.n) S[c].done = true;
             else if (S[c].rounds > S[c].max_rounds) {

@@ -234,9 +234,9 @@ struct MixedClass {
     WindowTables* w;
     FitIO F;
 };
-// ready (nullable): per class, an event recorded once its inputs are on the device
+// feeds (nullable): per class, its input chunks still arriving (n_chunks 0: all on the device)
 int launch_fit_split_mixed(zola_ctx* ctx, int nc, MixedClass* mc, cudaStream_t st,
-                           const cudaEvent_t* ready = nullptr);
+                           const RoiFeed* feeds = nullptr);
 // The round-based split fit's pool for psf's R x R ROIs: 1 and the tuned pool
 // (and its ns per evaluation) when tuned, else 0 and the context's setting.
 int split_pool_choice(zola_psf* p, WindowTables* w, int* pool, double* ns_per_eval);
