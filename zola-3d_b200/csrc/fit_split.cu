@@ -138,10 +138,8 @@ static double pow2scale(double bound) {
     return std::ldexp(1.0, (int)std::floor(std::log2(16384.0 / bound)));
 }
 
-// A2 arrays of a stage-2 tile: S hi, S lo, S_y, S_z and, for W = 128, S_x = i k_x S
-// (the window DFT then needs only the hi/lo DFT constants, not their x derivative).
-__host__ __device__ constexpr int a2_arrays(int W) { return W > 64 ? 5 : 4; }
-__host__ __device__ inline size_t a2_tile_bytes(int K1, int W) { return (size_t)a2_arrays(W) * 128 * K1 * 2; }
+// A2 arrays of a stage-2 tile: S hi, S lo, S_y, S_z
+__host__ __device__ inline size_t a2_tile_bytes(int K1) { return (size_t)4 * 128 * K1 * 2; }
 __host__ __device__ inline size_t a3_tile_bytes(int W) { return (size_t)5 * 128 * W * 2; }
 __host__ __device__ inline size_t a4_tile_bytes(int W) { return (size_t)2 * 128 * W * 2; }
 // Row-blurred maps J of one slot as the column-blur B operand: hi then lo, each
@@ -534,13 +532,10 @@ __device__ __forceinline__ bool group_bar_or(int id, bool p) {
 }
 
 __host__ __device__ constexpr int s2_slab_bytes(int W) { return 6 * W * 32; }
-// the window DFT's resident K-slab: all six row groups, or for W = 128 only the hi
-// and lo DFT rows (4W rows: parts 0, 1 hi and their lo)
-__host__ __device__ constexpr int s2_cslab_bytes(int W) { return (W > 64 ? 4 : 6) * W * 32; }
-// one ring step of A2 K-slabs: W = 128 streams S hi, S lo, S_x (phase A) or S_y, S_z
+// one ring step of A2 K-slabs: W = 128 streams S hi, S lo (phase A) or S_y, S_z
 // (phase B); smaller windows all four arrays at once
-__host__ __device__ constexpr int s2_ring_bytes(int W) { return (W > 64 ? 3 : 4) * 4096; }
-__host__ __device__ constexpr int s2_nbuf(int W) { return W > 64 ? 8 : 4; }
+__host__ __device__ constexpr int s2_ring_bytes(int W) { return (W > 64 ? 2 : 4) * 4096; }
+constexpr int S2_NBUF = 4;
 
 __device__ __forceinline__ void warp_arrive(uint64_t* mbar) {
     __syncwarp();
@@ -890,7 +885,6 @@ __device__ __forceinline__ void stage1_body(const SplitDev& P, const FitIO& F, U
     const int row = t & 127, wg = t >> 7;
     const int g = row / DP, a = row % DP;
     const int kre = kperm(a, false), kim = kperm(a, true);
-    const float kxe = TWO ? (float)P.kx[a] : 0.f;  // k_x of this TMEM row's pupil row
     const size_t arr = (size_t)128 * K1 * 2;
     constexpr int CW = W / 4;
     int q = 0, ntile = 0;
@@ -976,7 +970,7 @@ __device__ __forceinline__ void stage1_body(const SplitDev& P, const FitIO& F, U
             const int slot = tile * G1 + g;
             const bool live = P.slot_roi[slot] >= 0;
             const int tile2 = slot / P.G2, mrow0 = (slot % P.G2) * W;
-            char* a2t = P.a2 + (size_t)tile2 * a2_tile_bytes(K1, W);
+            char* a2t = P.a2 + (size_t)tile2 * a2_tile_bytes(K1);
             // epilogue of one pass: maps at TMEM columns c0 (S), c0 + 2W (S_y), zc (S_z; < 0: none)
             auto epilogue = [&](bool sy, int zc, uint32_t phase, uint64_t* accb) {
                 umma::mbar_wait(accb, phase, P.err);
@@ -1005,16 +999,6 @@ __device__ __forceinline__ void stage1_body(const SplitDev& P, const FitIO& F, U
                             store4w(a2t + 1 * arr + mnmajor_off(m, kim, 128), sli);
                             store4w(a2t + 2 * arr + mnmajor_off(m, kre, 128), wyr);
                             store4w(a2t + 2 * arr + mnmajor_off(m, kim, 128), wyi);
-                            if constexpr (TWO) {  // S_x = i k_x(a) S, scaled like S_y
-                                uint32_t wxr[4], wxi[4];
-#pragma unroll
-                                for (int u = 0; u < 8; u += 2) {
-                                    wxr[u / 2] = pack_h2(-kxe * si[u] * P.sc.c2y, -kxe * si[u + 1] * P.sc.c2y);
-                                    wxi[u / 2] = pack_h2(kxe * sr[u] * P.sc.c2y, kxe * sr[u + 1] * P.sc.c2y);
-                                }
-                                store4w(a2t + 4 * arr + mnmajor_off(m, kre, 128), wxr);
-                                store4w(a2t + 4 * arr + mnmajor_off(m, kim, 128), wxi);
-                            }
                         }
                     }
                     if (zc >= 0) {
@@ -1103,7 +1087,7 @@ template <int W, class UNITS>
 __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, UNITS units) {
     extern __shared__ __align__(1024) char smem[];
     constexpr bool TWO = W > 64;
-    constexpr int SLAB = s2_cslab_bytes(W), RING = s2_ring_bytes(W), NBUF = s2_nbuf(W);
+    constexpr int SLAB = s2_slab_bytes(W), RING = s2_ring_bytes(W), NBUF = S2_NBUF;
     constexpr int NCOLS = W >= 64 ? 512 : 256;
     const int K1 = P.K1, G2 = P.G2, t = threadIdx.x;
     const int NS = K1 / 16, NSTEP = TWO ? 2 * NS : NS;
@@ -1133,15 +1117,8 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
             }
         if (t != SPLIT_THREADS) return;
         umma::mbar_expect_tx(&cfull, (uint32_t)(NS * SLAB));
-        for (int s = 0; s < NS; ++s) {
-            const char* src = (const char*)P.bcs + (size_t)s * s2_slab_bytes(W);
-            if constexpr (TWO) {  // rows [0, 2W) (hi) and [4W, 6W) (lo) of the full slab
-                umma::bulk_g2s(CS + s * SLAB, src, 2 * W * 32, &cfull);
-                umma::bulk_g2s(CS + s * SLAB + 2 * W * 32, src + 4 * W * 32, 2 * W * 32, &cfull);
-            } else {
-                umma::bulk_g2s(CS + s * SLAB, src, SLAB, &cfull);
-            }
-        }
+        for (int s = 0; s < NS; ++s)
+            umma::bulk_g2s(CS + s * SLAB, (const char*)P.bcs + (size_t)s * SLAB, SLAB, &cfull);
         int q = 0;
         for (int tag = 0;;) {
             const int unit = units.next(P, tag, true);
@@ -1149,19 +1126,18 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
             for (int k = 0; k < T2; ++k) {
                 const int tile = unit * T2 + k;
                 if (!tile_live(P, tile * G2, G2)) continue;
-                const char* src = P.a2 + (size_t)tile * a2_tile_bytes(K1, W);
+                const char* src = P.a2 + (size_t)tile * a2_tile_bytes(K1);
                 for (int n = 0; n < NSTEP; ++n, ++q) {
                     const int buf = q % NBUF;
                     if (q >= NBUF && !umma::mbar_wait(&freed[buf], (uint32_t)((q / NBUF - 1) & 1), P.err)) return;
                     const bool pb = TWO && n >= NS;
                     const int s = pb ? n - NS : n;
-                    // phase A: S hi, S lo, S_x (W = 128) or all four arrays; phase B: S_y, S_z
-                    constexpr int A_ARR[4] = {0, 1, TWO ? 4 : 2, 3};
-                    const int narr = TWO ? (pb ? 2 : 3) : 4;
-                    umma::mbar_expect_tx(&full[buf], (uint32_t)(narr * 4096));
-                    for (int j = 0; j < narr; ++j)
-                        umma::bulk_g2s(RB + buf * RING + j * 4096,
-                                       src + (size_t)(pb ? 2 + j : A_ARR[j]) * arr + (size_t)s * 4096, 4096, &full[buf]);
+                    const int a0 = pb ? 2 : 0;  // phase B streams the y and z arrays
+                    constexpr int NARR = TWO ? 2 : 4;  // A2 arrays per ring step
+                    umma::mbar_expect_tx(&full[buf], RING);
+                    for (int j = 0; j < NARR; ++j)
+                        umma::bulk_g2s(RB + buf * RING + j * 4096, src + (size_t)(a0 + j) * arr + (size_t)s * 4096, 4096,
+                                       &full[buf]);
                 }
             }
         }
@@ -1188,18 +1164,15 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
                 const uint64_t bd = umma::smem_desc(cb + (uint32_t)(row0 / 8) * 256, 128, 256);
                 umma::mma_f16(tbase + col, ad, bd, umma::idesc_f16(128, N, true, false), acc ? 1u : 0u);
             };
-            if (!pb && TWO) {  // resident rows: [0, 2W) hi(C), [2W, 4W) lo(C)
-                mma(rb, 0, 2 * W, 0, !first);              // E = hi x hi(C)
-                mma(rb, 2 * W, 2 * W, 0, true);            // + hi x lo(C)
-                mma(rb + 4096, 0, 2 * W, 0, true);         // + lo x hi(C)
-                mma(rb + 8192, 0, 2 * W, 2 * W, !first);   // Ex = S_x x hi(C)
-            } else if (!pb) {
+            if (!pb) {
 #pragma unroll
                 for (int r = 0; r < 4 * W; r += 256) mma(rb, r, 4 * W < 256 ? 4 * W : 256, r, !first);  // E, Ex
                 mma(rb, 4 * W, 2 * W, 0, true);         // + hi x lo(C)
                 mma(rb + 4096, 0, 2 * W, 0, true);      // + lo x hi(C)
-                mma(rb + 8192, 0, 2 * W, 4 * W, !first);   // Ey
-                mma(rb + 12288, 0, 2 * W, 6 * W, !first);  // Ez
+                if (!TWO) {
+                    mma(rb + 8192, 0, 2 * W, 4 * W, !first);   // Ey
+                    mma(rb + 12288, 0, 2 * W, 6 * W, !first);  // Ez
+                }
             } else {
                 mma(rb, 0, 2 * W, 0, !first);          // Ey
                 mma(rb + 4096, 0, 2 * W, 2 * W, !first);  // Ez
@@ -1248,8 +1221,8 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
                         split2((er[h + u] * er[h + u] + ei[h + u] * ei[h + u]) * P.sc.cI,
                                (er[h + u + 1] * er[h + u + 1] + ei[h + u + 1] * ei[h + u + 1]) * P.sc.cI, hh[u / 2],
                                ll[u / 2]);
-                        dx[u / 2] = pack_h2(ipx(er + h, ei + h, xr, xi, u, P.sc.cIy),  // S_x scaled like S_y
-                                            ipx(er + h, ei + h, xr, xi, u + 1, P.sc.cIy));
+                        dx[u / 2] = pack_h2(ipx(er + h, ei + h, xr, xi, u, P.sc.cIx),
+                                            ipx(er + h, ei + h, xr, xi, u + 1, P.sc.cIx));
                     }
                     const uint32_t off = kmajor_off(row, i0, W);
                     store4w(a3t + 0 * arr3 + off, hh);
@@ -2423,7 +2396,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) k_fused25(SplitDev P, const 
     };
     if (t == 0) {
         umma::mbar_expect_tx(&full_a2, (uint32_t)(4 * arr2 + 2 * gtb));
-        const char* src = P.a2 + (size_t)blockIdx.x * a2_tile_bytes(K1, W);
+        const char* src = P.a2 + (size_t)blockIdx.x * a2_tile_bytes(K1);
         for (int q = 0; q < 4; ++q) umma::bulk_g2s(A2 + q * arr2, src + q * arr2, (uint32_t)arr2, &full_a2);
         umma::bulk_g2s(GT, P.gt_hi, (uint32_t)gtb, &full_a2);
         umma::bulk_g2s(GT + gtb, P.gt_lo, (uint32_t)gtb, &full_a2);
@@ -2793,7 +2766,7 @@ static size_t smem_stage1p(const SplitPlanHost& pl) {
     return (size_t)(pl.K1 / 16) * s2_slab_bytes(pl.W) + (size_t)S1_NBQ * s1_qring_bytes(pl.W);
 }
 static size_t smem_stage2p(const SplitPlanHost& pl) {
-    return (size_t)(pl.K1 / 16) * s2_cslab_bytes(pl.W) + (size_t)s2_nbuf(pl.W) * s2_ring_bytes(pl.W);
+    return (size_t)(pl.K1 / 16) * s2_slab_bytes(pl.W) + (size_t)S2_NBUF * s2_ring_bytes(pl.W);
 }
 static size_t smem_stage3(const SplitPlanHost& pl, bool flow = false) {
     return (size_t)s3_nbuf(pl.W, flow) * 5 * 128 * pl.W * 2 + (size_t)4 * pl.RP * pl.W;
@@ -2949,7 +2922,7 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
         ctx->err = "split path: shared-memory plan exceeds 225 KB";
         return ZOLA_E_UNSUPPORTED;
     }
-    const size_t per_slot = a2_tile_bytes(pl->K1, pl->W) / pl->G2 + a3_tile_bytes(pl->W) / pl->G2 +
+    const size_t per_slot = a2_tile_bytes(pl->K1) / pl->G2 + a3_tile_bytes(pl->W) / pl->G2 +
                             (size_t)pl->NT4 * a4_tile_bytes(pl->W) + (size_t)4 * pl->R * pl->R * 4 + sizeof(LMState) + NSUM * 8 + 16;
     int Pmax = (int)std::min<size_t>(32768, ((size_t)8 << 30) / per_slot);  // at most 8 GB of pool state
     if (pmax_override > 0) Pmax = std::min(Pmax, pmax_override);
@@ -2958,7 +2931,7 @@ static int setup_pool(zola_ctx* ctx, zola_psf* p, WindowTables* w, int n, int pm
     const int P = std::min(Pmax, (n + UG - 1) / UG * UG);
     sp.U = P / UG;
     auto al = [](size_t v) { return (v + 1023) / 1024 * 1024; };
-    const size_t b_a2 = al((size_t)(P / pl->G2) * a2_tile_bytes(pl->K1, pl->W));
+    const size_t b_a2 = al((size_t)(P / pl->G2) * a2_tile_bytes(pl->K1));
     const size_t b_a3 = al((size_t)(P / pl->G2) * a3_tile_bytes(pl->W));
     const size_t b_a4 = al((size_t)P * pl->NT4 * a4_tile_bytes(pl->W));
     const size_t b_t = al((size_t)P * 4 * pl->R * pl->R * 4);
