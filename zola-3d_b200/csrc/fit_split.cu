@@ -632,9 +632,6 @@ struct StaticUnits {
         for (u = u < 0 ? (int)blockIdx.x : u + (int)gridDim.x; u < U; u += gridDim.x)
             if (tile_live(P, u * UG, UG)) {
                 tag = 0;
-                // the next unit's slot states, on their way to L1 while this unit runs
-                if ((threadIdx.x & 31) == 0 && u + (int)gridDim.x < U)
-                    asm volatile("prefetch.global.L1 [%0];" ::"l"(P.slot_roi + (size_t)(u + gridDim.x) * UG));
                 return u;
             }
         return -1;
@@ -1150,10 +1147,10 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
     const size_t arr3 = (size_t)128 * W * 2;
     const uint32_t lbo_mn = (128 / 8) * 128;
     int q = 0, ph = 0;
-    auto issue_steps = [&](int n0, int n1) -> bool {
+    auto issue_steps = [&](int n0, int n1) {
         for (int n = n0; n < n1; ++n, ++q) {
             const int buf = q % NBUF;
-            if (!umma::mbar_wait(&full[buf], (uint32_t)((q / NBUF) & 1), P.err)) return false;
+            if (!umma::mbar_wait(&full[buf], (uint32_t)((q / NBUF) & 1), P.err)) return;
             umma::fence_after_sync();
             const uint32_t rb = umma::smem_u32(RB + buf * RING);
             const bool pb = TWO && n >= NS;
@@ -1179,7 +1176,6 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
             }
             umma::mma_commit(&freed[buf]);
         }
-        return true;
     };
     auto ipx = [](const float* er, const float* ei, const float* xr, const float* xi, int u, float cf) {
         return (er[u] * xr[u] + ei[u] * xi[u]) * cf;
@@ -1192,16 +1188,12 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
         for (int k = 0; k < T2 && !abort; ++k) {
             const int tile = unit * T2 + k;
             if (!tile_live(P, tile * G2, G2)) continue;
-            // the error flag is read here and voted on at the tile's last barrier (its
-            // latency hides under the tile); a wait that gave up in this tile votes too
-            const int errv = t == 0 ? *(volatile int*)P.err : 0;
-            bool bad = false;
             char* a3t = P.a3 + (size_t)tile * a3_tile_bytes(W);
             if (t == 0) {
-                bad = !issue_steps(0, NS);
+                issue_steps(0, NS);
                 umma::mma_commit(&accA);
             }
-            bad |= !umma::mbar_wait(&accA, (uint32_t)ph, P.err);
+            umma::mbar_wait(&accA, (uint32_t)ph, P.err);
             umma::fence_after_sync();
             if constexpr (TWO) {
                 float er[CW], ei[CW];
@@ -1233,10 +1225,10 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
                 epi_bar();
                 if (t == 0) {
                     umma::fence_after_sync();
-                    bad |= !issue_steps(NS, NSTEP);
+                    issue_steps(NS, NSTEP);
                     umma::mma_commit(&accB);
                 }
-                bad |= !umma::mbar_wait(&accB, (uint32_t)ph, P.err);
+                umma::mbar_wait(&accB, (uint32_t)ph, P.err);
                 umma::fence_after_sync();
 #pragma unroll
                 for (int h = 0; h < CW; h += 8) {
@@ -1294,7 +1286,7 @@ __device__ __forceinline__ void stage2_body(const SplitDev& P, const FitIO& F, U
             // (a bounded wait that gave up makes every epilogue thread leave the loop together)
             umma::fence_before_sync();
             units.fence_writes();
-            abort = epi_bar_or(bad || errv != 0);
+            abort = epi_bar_or(t == 0 && *(volatile int*)P.err != 0);
             if (t == 0) umma::fence_after_sync();
             ph ^= 1;
         }
