@@ -27,10 +27,10 @@ sys.path.insert(0, ROOT)
 # evaluation of each round-based kernel of the 48x48 tetrapod class: one launch
 # with all 4096 slots of a pool live (profiles/split_kernels_tetra48_dram_traffic.md).
 NCU_TRAFFIC = {
-    ("tetra48", "split_stage1_pupil_dft"): 117_036,
-    ("tetra48", "split_stage2_window_dft"): 283_487,
-    ("tetra48", "split_stage3_blur_rows"): 251_771,
-    ("tetra48", "split_stage4_blur_cols_sums_lm"): 107_996,
+    ("tetra48", "split_stage1_pupil_dft"): 117_005,
+    ("tetra48", "split_stage2_window_dft"): 284_238,
+    ("tetra48", "split_stage3_blur_rows"): 252_620,
+    ("tetra48", "split_stage4_blur_cols_sums_lm"): 108_704,
 }
 
 METRIC = "MLE ROI fits/sec at ≤0.5 nm vs FP64 oracle (batched split-prec vs plain GPU)"
