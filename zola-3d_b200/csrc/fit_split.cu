@@ -914,6 +914,14 @@ __device__ __forceinline__ void stage1_body(const SplitDev& P, const FitIO& F, U
                 q2.ky = *(const double2*)(P.ky + 8 * s + 2 * bp);
                 return q2;
             };
+            // the table lines of step s on their way to L1 (the same for every tile)
+            auto qpre = [&](int s) {
+                const size_t i2 = (((size_t)s * 4 + bp) * DP + ba) * 2;
+                const size_t i4 = (((size_t)s * 2 + (bp >> 1)) * DP + ba) * 4 + (bp & 1) * 2;
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(P.phase0 + i2));
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(P.kz + i2));
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(P.pupf + i4));
+            };
             const uint32_t ore = kmajor_off(brow, 2 * bp, 16), oim = kmajor_off(brow, 8 + 2 * bp, 16);
             auto slot_wait = [&]() {  // ring slot for the next K step
                 const int buf = q % NBQ;
@@ -956,6 +964,41 @@ __device__ __forceinline__ void stage1_body(const SplitDev& P, const FitIO& F, U
                     *(uint32_t*)(qs + 2 * QB + oim) = zi;
                 }
                 slot_done(qs);
+            };
+            // W = 128: steps s and s + 1 together, so that four sin/cos chains are in flight
+            auto build_pair = [&](int s, const QTab& ta, const QTab& tc, uint32_t (&za)[2], uint32_t (&zc)[2]) {
+                float qr[4], qi[4], kzv[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const QTab& tb = e < 2 ? ta : tc;
+                    const double ph0 = (e & 1) ? tb.p0.y : tb.p0.x, kzr = (e & 1) ? tb.kz.y : tb.kz.x;
+                    const double kyr = (e & 1) ? tb.ky.y : tb.ky.x;
+                    const float pu = (e & 1) ? tb.pu.y : tb.pu.x;
+                    qr[e] = 0.f; qi[e] = 0.f; kzv[e] = 0.f;
+                    if (blive && pu != 0.f) {
+                        float sn, cs;
+                        sincos_phase(ph0 + kxa * x + kyr * y + kzr * z, sn, cs);
+                        qr[e] = pu * cs;
+                        qi[e] = pu * sn;
+                        kzv[e] = (float)kzr;
+                    }
+                }
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int e = 2 * h;
+                    uint32_t(&zz)[2] = h == 0 ? za : zc;
+                    zz[0] = pack_h2(-kzv[e] * qi[e] * P.sc.qz, -kzv[e + 1] * qi[e + 1] * P.sc.qz);  // Q_z = i kz Q
+                    zz[1] = pack_h2(kzv[e] * qr[e] * P.sc.qz, kzv[e + 1] * qr[e + 1] * P.sc.qz);
+                    uint32_t rh, rl, ih, il;
+                    split2(qr[e] * P.sc.q, qr[e + 1] * P.sc.q, rh, rl);
+                    split2(qi[e] * P.sc.q, qi[e + 1] * P.sc.q, ih, il);
+                    char* qs = slot_wait();
+                    *(uint32_t*)(qs + ore) = rh;
+                    *(uint32_t*)(qs + oim) = ih;
+                    *(uint32_t*)(qs + QB + ore) = rl;
+                    *(uint32_t*)(qs + QB + oim) = il;
+                    slot_done(qs);
+                }
             };
             auto build_z = [&](int s) {  // pass B (W = 128): the kept Q_z of step s
                 char* qs = slot_wait();
@@ -1019,14 +1062,16 @@ __device__ __forceinline__ void stage1_body(const SplitDev& P, const FitIO& F, U
                 warp_arrive(&tfree);
             };
             if constexpr (TWO) {
-                QTab cur = qtab(0);
 #pragma unroll
-                for (int s = 0; s < 8; ++s) {
-                    QTab nxt;
-                    if (s + 1 < 8) nxt = qtab(s + 1);
-                    build(s, cur, zkeep[s][0], zkeep[s][1]);
-                    if (s + 1 < 8) cur = nxt;
+                for (int s = 0; s < 8; s += 2) {
+                    if (s + 2 < 8) {
+                        qpre(s + 2);
+                        qpre(s + 3);
+                    }
+                    build_pair(s, qtab(s), qtab(s + 1), zkeep[s], zkeep[s + 1]);
                 }
+                qpre(0);  // the next tile's first pair
+                qpre(1);
 #pragma unroll
                 for (int s = 0; s < NBQ; ++s) build_z(s);
                 epilogue(true, -1, ph, &accA);
