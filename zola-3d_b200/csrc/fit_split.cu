@@ -2012,9 +2012,18 @@ __device__ __forceinline__ void stage45_body(const SplitDev& P, const FitIO& F, 
 #pragma unroll
             for (int k = 0; k < 30; ++k) sh[k] = 0.f;
             bool bad = false;
-#pragma unroll 2
+            // pixel k = ip R + jc of the maps' rows (stride RS), stepped without a division
+            int ip = t / R, jc = t - (t / R) * R;
+            const int dq = E45_THREADS / R, dr = E45_THREADS - (E45_THREADS / R) * R;
+#pragma unroll 3
             for (int k = t; k < RR; k += E45_THREADS) {
-                const int ip = k / R, to = ip * RS + (k - ip * R);
+                const int to = ip * RS + jc;
+                ip += dq;
+                jc += dr;
+                if (jc >= R) {
+                    jc -= R;
+                    ++ip;
+                }
                 const float v = Tm[to], sgn = v < 0 ? -1.f : 1.f, psi = fabsf(v) * invS;
                 float jv[5];
                 jv[0] = A * (sgn * Tm[MS + to] - psi * Dx) * invS;
