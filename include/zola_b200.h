@@ -171,10 +171,12 @@ typedef struct {
 } zola_fit_class;
 ZOLA_API int zola_fit_batch_mixed_dev(zola_ctx* ctx, const zola_fit_class* classes, int nclass, void* stream);
 /* Host-buffer form of the mixed batch: the d_* fields of each class point to
- * HOST memory here (pinned memory lets the copies overlap the fits).  The
- * inputs go up on the context's copy stream, the smallest class first, and
- * each class starts fitting as soon as its own inputs have landed; the results
- * come back before the call returns. */
+ * HOST memory here (pinned memory lets the copies overlap the fits).  Every
+ * class is checked first; the ROIs then go up on the context's copy stream in
+ * chunks of about 32 MB, interleaved across the classes, and each class starts
+ * fitting on its first chunk and takes the others as they land.  The results
+ * come back before the call returns and equal those of
+ * zola_fit_batch_mixed_dev bit for bit. */
 ZOLA_API int zola_fit_batch_mixed(zola_ctx* ctx, const zola_fit_class* classes, int nclass);
 
 /* sCMOS form (process/cpu/Localization.java:1132, utils/SCMOScamera.java):
