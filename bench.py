@@ -514,7 +514,10 @@ def cpu_baseline(budget_s=15.0, seed=2):
         zern = cls["zern"](np.random.default_rng(seed * 100 + R))
         p = O.OraclePSF(N, DX, 1.4, 0.66, 1.518, 1.518, 0.9, zern)
         rng = np.random.default_rng(seed + 7 * R)
-        n1 = max(threads, 2)
+        # four ROIs a host thread per class (64 a class on 16 cores): a sample that takes
+        # a few seconds a class, with the GPU job's start (x = y = 0, z on the 0.1 um grid,
+        # 0.9 of the photons)
+        n1 = 4 * max(threads, 1)
         truth = np.c_[rng.uniform(-DX, DX, (n1, 2)), rng.uniform(-cls["zr"], cls["zr"], n1),
                       rng.lognormal(np.log(3000.0), 0.6, n1), np.full(n1, cls["bg"])]
         rois = rng.poisson(truth[:, 3, None, None] * p.model(R, truth[:, :3]) + cls["bg"]).astype(float)
