@@ -27,3 +27,34 @@ def test_ctx_create_fails_cleanly_without_gpu(zpkg):
     h = ctypes.c_void_p()
     rc = zpkg.lib().zola_ctx_create(0, ctypes.byref(h))
     assert rc != 0
+
+
+def test_ctypes_structures_match_the_header(zpkg, tmp_path):
+    """The Python mirror's ctypes structures have the sizes and field offsets
+    that a C compiler gives the header's structs (gcc on include/zola_b200.h)."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        return
+    pairs = [("zola_optics", zpkg.Optics), ("zola_localization", zpkg.Localization),
+             ("zola_loc_params", zpkg.LocParams), ("zola_fit_params", zpkg.FitParams),
+             ("zola_fit_class", zpkg.FitClass), ("zola_drift_params", zpkg.DriftParams),
+             ("zola_calib_data", zpkg.CalibData)]
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "zola_b200.h"', "int main(void) {"]
+    for cname, cls in pairs:
+        lines.append(f'    printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f in cls._fields_:
+            lines.append(f'    printf("{cname} {f[0]} %zu\\n", offsetof({cname}, {f[0]}));')
+    lines += ["    return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.check_call(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)])
+    got = {}
+    for ln in subprocess.check_output([str(exe)], text=True).splitlines():
+        cname, key, val = ln.split()
+        got[(cname, key)] = int(val)
+    for cname, cls in pairs:
+        assert got[(cname, "size")] == ctypes.sizeof(cls), cname
+        for f in cls._fields_:
+            assert got[(cname, f[0])] == getattr(cls, f[0]).offset, (cname, f[0])
