@@ -58,3 +58,29 @@ def test_ctypes_structures_match_the_header(zpkg, tmp_path):
         assert got[(cname, "size")] == ctypes.sizeof(cls), cname
         for f in cls._fields_:
             assert got[(cname, f[0])] == getattr(cls, f[0]).offset, (cname, f[0])
+
+
+def declared_arity():
+    """{name: parameter count} of every ZOLA_API function in the header."""
+    src = open(os.path.join(ROOT, "include", "zola_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    out = {}
+    for m in re.finditer(r"ZOLA_API\s+[\w\s\*]+?\b(zola_\w+)\s*\(([^;]*?)\)\s*;", src, flags=re.S):
+        params = m.group(2).strip()
+        out[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_python_argtypes_match_the_header(zpkg):
+    """Every function the Python mirror binds with argtypes takes as many
+    arguments as the header declares (a mismatch would corrupt the call)."""
+    L = zpkg.lib()
+    arity = declared_arity()
+    checked = 0
+    for name, n in arity.items():
+        fn = getattr(L, name)
+        if fn.argtypes is None:
+            continue
+        assert len(fn.argtypes) == n, (name, len(fn.argtypes), n)
+        checked += 1
+    assert checked >= 20
