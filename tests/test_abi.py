@@ -84,3 +84,15 @@ def test_python_argtypes_match_the_header(zpkg):
         assert len(fn.argtypes) == n, (name, len(fn.argtypes), n)
         checked += 1
     assert checked >= 20
+
+
+def test_wide_return_types_are_declared(zpkg):
+    """Functions that return a pointer or a 64-bit integer have a restype that
+    keeps all 64 bits (ctypes would otherwise truncate them to a C int)."""
+    src = open(os.path.join(ROOT, "include", "zola_b200.h")).read()
+    L = zpkg.lib()
+    wide = re.findall(r"ZOLA_API\s+(?!int\s)([\w\s]+?\*?)\s*\b(zola_\w+)\s*\(", src)
+    assert len(wide) >= 3
+    for ret, name in wide:
+        rt = getattr(L, name).restype
+        assert rt is not None and ctypes.sizeof(rt) == 8, (name, ret, rt)
